@@ -1,0 +1,10 @@
+"""B200-native (sm_100a) MLS-MPM step for emerge-engine, behind the reference's API.
+
+`Simulation`, `SimConfig`, `SpawnRegion`, the constitutive models and `SlipBoundary` keep the
+reference crate's names and semantics; the step runs in libemerge_cuda.so (include/emerge_cuda.h).
+"""
+from .config import BodyState, SimConfig, SlipBoundary, SpawnRegion  # noqa: F401
+from .materials import (DruckerPragerMaterial, FallbackMaterial, NaccMaterial,  # noqa: F401
+                        NeoHookeanMaterial, NewtonianFluidMaterial, StomakhinMaterial,
+                        lame_from_young, to_radians)
+from .simulation import MaterialRegistry, Simulation  # noqa: F401

@@ -1,0 +1,64 @@
+// kernels.h -- host-side launchers of the device kernels (step_kernels.cu, sort.cu).
+#pragma once
+
+#include <cstddef>
+#include <cstdint>
+#include <cstring>
+#include <cuda_runtime.h>
+
+#include "device_state.cuh"
+
+namespace emerge {
+
+struct LoadFlagsHost {
+    int temperature = 0;
+    int activation = 0;
+    int pinned = 0;
+};
+
+// step_kernels.cu
+void launch_particle_pass(const StepLaunch &L, const LoadFlagsHost &lf, int mode_g2p);
+void launch_density_pass(const StepLaunch &L, const LoadFlagsHost &lf);
+void launch_grid_update(const StepLaunch &L);
+void launch_step_begin(const StepLaunch &L);
+void launch_substep_begin(const StepLaunch &L, int use_cond, unsigned long long handle,
+                          int kernels_per_substep);
+void launch_prime_setup(const StepLaunch &L);
+void launch_region_state(const DevParticles &P, int n, float cx, float cy, float r2, void *acc,
+                         cudaStream_t stream);
+size_t region_acc_bytes();
+void region_acc_finalize(const void *acc, emerge_body_state *out);
+void launch_gather_aos(const DevParticles &P, int n, emerge_particle *out, cudaStream_t stream);
+void launch_scatter_aos(const DevParticles &P, int n, const emerge_particle *in, cudaStream_t stream);
+void launch_append_aos(const DevParticles &P, int n_old, int n_new, const emerge_particle *in,
+                       cudaStream_t stream);
+void launch_reinit(const DevParticles &P, int n, const MatP *mats, int n_mats, cudaStream_t stream);
+void launch_mass_scatter(const DevParticles &P, int n, const GridView &g, int filter, float lox,
+                         float loy, float hix, float hiy, cudaStream_t stream);
+void launch_mass_gather(const DevParticles &P, int lo, int hi, const GridView &g, int write_initial,
+                        cudaStream_t stream);
+
+// sort.cu
+// Scratch for a stable LSD radix sort of up to `capacity` (key, value) pairs.
+struct SortScratch {
+    size_t capacity = 0;
+    uint32_t *keys[2] = {nullptr, nullptr};
+    uint32_t *vals[2] = {nullptr, nullptr};
+    uint32_t *hist = nullptr;      // 256 * blocks
+    uint32_t *partials = nullptr;  // scan partials
+    size_t hist_capacity = 0;
+};
+size_t sort_scratch_bytes(size_t n);
+// Carves the scratch arrays out of one device allocation of sort_scratch_bytes(n).
+void sort_scratch_bind(SortScratch &s, void *base, size_t n);
+// Keys of the particle positions: key_mode 0 = tile key, 1 = block_index key.
+void launch_sort_keys(const float2 *x, int n, int res, int key_mode, uint32_t *keys, uint32_t *vals,
+                      cudaStream_t stream);
+int sort_key_bits(int res, int key_mode);
+// Sorts (keys[0], vals[0]) stably by key; result lands in (keys[r], vals[r]), r returned.
+int radix_sort_pairs(SortScratch &s, int n, int key_bits, cudaStream_t stream);
+// dst[j] = src[perm[j]] for every particle array.
+void launch_permute(const DevParticles &src, const DevParticles &dst, const uint32_t *perm, int n,
+                    cudaStream_t stream);
+
+}  // namespace emerge

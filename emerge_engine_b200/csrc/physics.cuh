@@ -1,0 +1,659 @@
+// physics.cuh -- per-particle MLS-MPM math on the device.
+//
+// Each function restates one reference item (path:line inside the reference
+// crate M1thieu/emerge-engine) in f32, in the reference's expression order.
+// Translation units including this header are compiled with -fmad=false so
+// a*b+c is never contracted into an FMA (the Rust reference never contracts),
+// and with IEEE division/sqrt (nvcc defaults).  expf/logf/sinf/sinhf/powf are
+// CUDA's libdevice-free intrinsics-by-default implementations, whose last-ulp
+// behaviour differs from glibc: results agree with the CPU reference to
+// tolerance, not bit for bit.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "../../include/emerge_cuda.h"
+
+namespace emerge {
+
+constexpr float F32_EPS = 1.1920929e-7f;     // f32::EPSILON
+constexpr float KERNEL_D_INVERSE = 4.0f;     // spacetime/solver/config.rs:22
+constexpr float MIN_J = 1e-6f;               // matter/materials/utils.rs:11
+constexpr float LOG_CLAMP = 1e-10f;          // matter/materials/utils.rs:6
+
+enum Model : uint32_t {
+    M_FALLBACK = 0, M_FLUID = 1, M_NEOHOOKEAN = 2, M_COROTATED = 3, M_SNOW = 4,
+    M_DRUCKER_PRAGER = 5, M_VON_MISES = 6, M_RANKINE = 7, M_DP_MUI = 8,
+    M_VISCOELASTIC = 9, M_NACC = 10, M_GRANULAR_FLUID = 11
+};
+
+struct M2 { float2 xa, ya; };  // glam Mat2: columns x_axis, y_axis
+
+#define EM_HD __host__ __device__ __forceinline__
+
+EM_HD float2 v2(float x, float y) { return make_float2(x, y); }
+EM_HD float2 vadd(float2 a, float2 b) { return v2(a.x + b.x, a.y + b.y); }
+EM_HD float2 vsub(float2 a, float2 b) { return v2(a.x - b.x, a.y - b.y); }
+EM_HD float2 vmulv(float2 a, float2 b) { return v2(a.x * b.x, a.y * b.y); }
+EM_HD float2 vmuls(float2 a, float s) { return v2(a.x * s, a.y * s); }
+EM_HD float2 svmul(float s, float2 a) { return v2(s * a.x, s * a.y); }
+EM_HD float2 vdivs(float2 a, float s) { return v2(a.x / s, a.y / s); }
+EM_HD float2 splat(float s) { return v2(s, s); }
+EM_HD float vdot(float2 a, float2 b) { return a.x * b.x + a.y * b.y; }
+EM_HD float vlen(float2 a) { return sqrtf(vdot(a, a)); }
+EM_HD float vlen2(float2 a) { return vdot(a, a); }
+EM_HD bool vfinite(float2 a) { return isfinite(a.x) && isfinite(a.y); }
+EM_HD float2 vabs2(float2 a) { return v2(fabsf(a.x), fabsf(a.y)); }
+EM_HD float2 vmax2(float2 a, float2 b) { return v2(fmaxf(a.x, b.x), fmaxf(a.y, b.y)); }
+EM_HD float2 vmin2(float2 a, float2 b) { return v2(fminf(a.x, b.x), fminf(a.y, b.y)); }
+// glam Vec2::clamp: self.max(min).min(max)
+EM_HD float2 vclamp2(float2 a, float2 lo, float2 hi) { return vmin2(vmax2(a, lo), hi); }
+// f32::clamp keeps NaN
+EM_HD float fclampf(float x, float lo, float hi) {
+    if (x < lo) x = lo;
+    if (x > hi) x = hi;
+    return x;
+}
+// glam normalize_or_zero
+EM_HD float2 normalize_or_zero(float2 a) {
+    float rcp = 1.0f / vlen(a);
+    if (isfinite(rcp) && rcp > 0.0f) return vmuls(a, rcp);
+    return v2(0.0f, 0.0f);
+}
+
+EM_HD M2 m2(float2 a, float2 b) { M2 r; r.xa = a; r.ya = b; return r; }
+EM_HD M2 mident() { return m2(v2(1.0f, 0.0f), v2(0.0f, 1.0f)); }
+EM_HD M2 mzero() { return m2(v2(0.0f, 0.0f), v2(0.0f, 0.0f)); }
+EM_HD M2 mdiag(float2 d) { return m2(v2(d.x, 0.0f), v2(0.0f, d.y)); }
+EM_HD M2 madd(M2 a, M2 b) { return m2(vadd(a.xa, b.xa), vadd(a.ya, b.ya)); }
+EM_HD M2 msub(M2 a, M2 b) { return m2(vsub(a.xa, b.xa), vsub(a.ya, b.ya)); }
+EM_HD M2 mscale(M2 a, float s) { return m2(vmuls(a.xa, s), vmuls(a.ya, s)); }
+EM_HD M2 smscale(float s, M2 a) { return m2(svmul(s, a.xa), svmul(s, a.ya)); }
+EM_HD float2 mv(M2 a, float2 v) { return vadd(vmuls(a.xa, v.x), vmuls(a.ya, v.y)); }
+EM_HD M2 mm(M2 a, M2 b) { return m2(mv(a, b.xa), mv(a, b.ya)); }
+EM_HD M2 mtrans(M2 a) { return m2(v2(a.xa.x, a.ya.x), v2(a.xa.y, a.ya.y)); }
+EM_HD float mdet(M2 a) { return a.xa.x * a.ya.y - a.ya.x * a.xa.y; }
+EM_HD bool mfinite(M2 a) { return vfinite(a.xa) && vfinite(a.ya); }
+EM_HD M2 m_from4(float4 f) { return m2(v2(f.x, f.y), v2(f.z, f.w)); }
+EM_HD float4 m_to4(M2 a) { return make_float4(a.xa.x, a.xa.y, a.ya.x, a.ya.y); }
+
+// Rust `f32 as i32` (saturating, NaN -> 0); cvt.rzi.s32.f32 has the same semantics.
+EM_HD int f2i(float f) { return static_cast<int>(f); }
+
+// axis_weights (spacetime/grid/kernel.rs:20-25)
+EM_HD void axis_weights(float d, float w[3]) {
+    float a = 0.5f - d;
+    float b = 0.5f + d;
+    w[0] = 0.5f * (a * a);
+    w[1] = 0.75f - d * d;
+    w[2] = 0.5f * (b * b);
+}
+
+// quadratic_weights (spacetime/grid/kernel.rs:10-18)
+struct QW { int bx, by; float wx[3], wy[3]; };
+EM_HD QW quadratic_weights(float2 p) {
+    QW q;
+    q.bx = f2i(floorf(p.x));
+    q.by = f2i(floorf(p.y));
+    float dx = (p.x - static_cast<float>(q.bx)) - 0.5f;
+    float dy = (p.y - static_cast<float>(q.by)) - 0.5f;
+    axis_weights(dx, q.wx);
+    axis_weights(dy, q.wy);
+    return q;
+}
+
+// ---------------------------------------------------------------- svd / polar
+EM_HD float2 orthogonal_complement(float2 v) {  // materials/svd.rs:81-85
+    float2 perp = v2(-v.y, v.x);
+    float len = vlen(perp);
+    if (len > 1e-10f) return vdivs(perp, len);
+    return v2(1.0f, 0.0f);
+}
+
+// svd2 (matter/materials/svd.rs:14-76): F = U diag(sigma) Vt, det U = det V = +1,
+// reflection carried by a negative sigma.y.
+EM_HD void svd2(M2 f, M2 &u_out, float2 &sigma_out, M2 &vt_out) {
+    float f00 = f.xa.x, f10 = f.xa.y, f01 = f.ya.x, f11 = f.ya.y;
+    float c00 = f00 * f00 + f10 * f10;
+    float c01 = f00 * f01 + f10 * f11;
+    float c11 = f01 * f01 + f11 * f11;
+    float mean = (c00 + c11) * 0.5f;
+    float half_diff = (c00 - c11) * 0.5f;
+    float disc = sqrtf(half_diff * half_diff + c01 * c01);
+    float lambda1 = mean + disc;
+    float lambda2 = mean - disc;
+    float2 v1;
+    if (fabsf(c01) > 1e-10f * fmaxf(c00 + c11, 1e-30f)) {
+        float2 raw = v2(c01, lambda1 - c00);
+        v1 = vdivs(raw, vlen(raw));
+    } else {
+        v1 = (c00 >= c11) ? v2(1.0f, 0.0f) : v2(0.0f, 1.0f);
+    }
+    float2 vv2 = v2(-v1.y, v1.x);
+    M2 vt = mtrans(m2(v1, vv2));
+    float2 sigma = v2(sqrtf(fmaxf(lambda1, 0.0f)), sqrtf(fmaxf(lambda2, 0.0f)));
+    float2 fv1 = mv(f, v1);
+    float2 fv2 = mv(f, vv2);
+    float2 u1 = (sigma.x > 1e-10f) ? vdivs(fv1, sigma.x) : orthogonal_complement(fv2);
+    float2 u2 = (sigma.y > 1e-10f) ? vdivs(fv2, sigma.y) : orthogonal_complement(u1);
+    M2 u = m2(u1, u2);
+    if (mdet(u) < 0.0f) {
+        u.ya = v2(-u.ya.x, -u.ya.y);
+        sigma.y = -sigma.y;
+    }
+    u_out = u;
+    sigma_out = sigma;
+    vt_out = vt;
+}
+
+// polar_decomposition_2d (matter/materials/utils.rs:129-138)
+EM_HD M2 polar(M2 f) {
+    float x = f.xa.x + f.ya.y;
+    float y = f.xa.y - f.ya.x;
+    float norm = sqrtf(x * x + y * y);
+    if (norm > F32_EPS) return m2(vdivs(v2(x, y), norm), vdivs(v2(-y, x), norm));
+    return mident();
+}
+
+// elastic_wave_dt (matter/materials/utils.rs:145-163)
+EM_HD float elastic_wave_dt(float lambda, float mu, float hardening, float density,
+                            float min_density, float cell_width, float material_cfl) {
+    float rho = fmaxf(density, min_density);
+    float modulus = fmaxf((lambda + 2.0f * mu) * hardening, 0.0f);
+    if (modulus <= F32_EPS) return INFINITY;
+    float c = sqrtf(modulus / rho);
+    if (c <= F32_EPS) return INFINITY;
+    return material_cfl * cell_width / c;
+}
+
+// ---------------------------------------------------------------- material view
+// Device view of one MaterialParams slot.  The fields each model reads follow
+// that model's params() packing (elastic.rs:275-288, fluid.rs:209-226,
+// sand.rs:321-343, snow.rs:178-191, nacc.rs:300-314).  Constructor-only fields
+// that params() does not carry are fixed at the reference constructors' values:
+// NeoHookean min_density 1e-6 (elastic.rs:55), Fluid min_density/min_volume 1e-6
+// (fluid.rs:60-61), DP volume_correction 1.0 (sand.rs:89), NACC min_density 1e-6
+// (nacc.rs:71) and hardening_enabled = hardening_factor > 0 (nacc.rs:70).
+typedef emerge_material_params MatP;
+
+EM_HD float nacc_kappa(const MatP &m) { return m.lambda + m.mu; }  // inverse of nacc.rs:304
+
+// DruckerPragerMaterial::alpha (sand.rs:135-141); dp_h0..3 = phi0, h1, h2, phi_r
+EM_HD float dp_alpha(const MatP &m, float q) {
+    float phi = m.dp_h0 + (m.dp_h1 * q - m.dp_h3) * expf(-m.dp_h2 * q);
+    float s = sinf(phi);
+    return sqrtf(2.0f / 3.0f) * (2.0f * s) / (3.0f - s);
+}
+
+// DruckerPragerMaterial::project (sand.rs:156-194); cohesion in stretch_limit (sand.rs:335)
+EM_HD bool dp_project(const MatP &m, float2 sigma_in, float lvs, float q, float2 &out,
+                      float &dq) {
+    float2 sigma = vmax2(vabs2(sigma_in), splat(LOG_CLAMP));
+    float2 eps = v2(logf(sigma.x) + lvs * 0.5f, logf(sigma.y) + lvs * 0.5f);
+    float trace = eps.x + eps.y;
+    float2 dev = vsub(eps, splat(trace * 0.5f));
+    float dev_norm = vlen(dev);
+    if (dev_norm == 0.0f || trace > 0.0f) {
+        out = v2(1.0f, 1.0f);
+        dq = dev_norm;
+        return true;
+    }
+    float ratio = (m.lambda + m.mu) / m.mu;
+    float alpha = dp_alpha(m, q);
+    float cohesion_term = m.stretch_limit / (2.0f * m.mu);
+    float gamma = dev_norm + ratio * trace * alpha - cohesion_term;
+    if (gamma <= 0.0f) return false;
+    float2 h = vsub(eps, svmul(gamma, vdivs(dev, dev_norm)));
+    out = v2(expf(h.x), expf(h.y));
+    dq = gamma;
+    return true;
+}
+
+EM_HD M2 reconstruct(M2 u, float2 s, M2 vt) { return mm(mm(u, mdiag(s)), vt); }
+
+// NaccMaterial::project (nacc.rs:129-223).  params(): hardening_exponent = xi,
+// compression_limit = beta, stretch_limit = M (nacc.rs:309-311).
+EM_HD void nacc_project(const MatP &m, M2 f, float alpha, M2 &f_out, float &alpha_out) {
+    const float kappa = nacc_kappa(m);
+    float xi = m.hardening_exponent;
+    float beta = m.compression_limit;
+    float mm_ = m.stretch_limit;
+    bool hard = xi > 0.0f;
+    M2 u, vt;
+    float2 sv;
+    svd2(f, u, sv, vt);
+    float2 sv_sq = vmulv(sv, sv);
+    float sv_sq_trace = sv_sq.x + sv_sq.y;
+    float p0 = kappa * (1.0e-5f + sinhf(xi * fmaxf(-alpha, 0.0f)));
+    float j_e_tr = fmaxf(sv.x * sv.y, 1.0e-6f);
+    float2 s_tr = svmul(m.mu * (1.0f / j_e_tr), vsub(sv_sq, splat(sv_sq_trace * 0.5f)));
+    float psi_kappa = kappa * 0.5f * (j_e_tr - 1.0f / j_e_tr);
+    float p_tr = -psi_kappa * j_e_tr;
+    if (p_tr > p0) {
+        float j_n1 = sqrtf(fmaxf(-2.0f * p0 / kappa + 1.0f, 1.0e-8f));
+        float sv_new = powf(j_n1, 0.5f);
+        if (hard) alpha += logf(j_e_tr / j_n1);
+        f_out = reconstruct(u, splat(sv_new), vt);
+        alpha_out = alpha;
+        return;
+    }
+    if (p_tr < -beta * p0) {
+        float j_n1 = sqrtf(fmaxf(2.0f * beta * p0 / kappa + 1.0f, 1.0e-8f));
+        float sv_new = powf(j_n1, 0.5f);
+        if (hard) alpha += logf(j_e_tr / j_n1);
+        f_out = reconstruct(u, splat(sv_new), vt);
+        alpha_out = alpha;
+        return;
+    }
+    float y0 = (1.0f + 2.0f * beta) * 2.0f;
+    float y1 = mm_ * mm_ * (p_tr + beta * p0) * (p_tr - p0);
+    float s_norm_sq = s_tr.x * s_tr.x + s_tr.y * s_tr.y;
+    float y = y0 * s_norm_sq + y1;
+    if (y < 1.0e-4f) {
+        f_out = f;
+        alpha_out = alpha;
+        return;
+    }
+    if (hard && p0 > 1.0e-4f && p_tr < p0 - 1.0e-4f && p_tr > -beta * p0 + 1.0e-4f) {
+        float p_c = (1.0f - beta) * p0 * 0.5f;
+        float q_tr = sqrtf(2.0f) * vlen(s_tr);
+        float2 dir = normalize_or_zero(v2(p_c - p_tr, -q_tr));
+        float c = mm_ * mm_ * (p_c + beta * p0) * (p_c - p0);
+        float b = mm_ * mm_ * dir.x * (2.0f * p_c - p0 + beta * p0);
+        float a = mm_ * mm_ * dir.x * dir.x + (1.0f + 2.0f * beta) * dir.y * dir.y;
+        float discr = sqrtf(fmaxf(b * b - 4.0f * a * c, 0.0f));
+        float l1 = (-b + discr) / (2.0f * a);
+        float l2 = (-b - discr) / (2.0f * a);
+        float p1 = p_c + l1 * dir.x;
+        float p2 = p_c + l2 * dir.x;
+        float p_x = ((p_tr - p_c) * (p1 - p_c) > 0.0f) ? p1 : p2;
+        float j_e_x = sqrtf(fmaxf(fabsf(-2.0f * p_x / kappa + 1.0f), 1.0e-8f));
+        if (j_e_x > 1.0e-4f) alpha += logf(j_e_tr / j_e_x);
+    }
+    float scale = sqrtf(fmaxf(-y1 / fmaxf(y0, 1.0e-10f), 0.0f)) * (j_e_tr / m.mu);
+    float2 b_n1 = vadd(svmul(scale, normalize_or_zero(s_tr)), splat(sv_sq_trace / 2.0f));
+    float2 sv_new = v2(sqrtf(fmaxf(b_n1.x, 1.0e-8f)), sqrtf(fmaxf(b_n1.y, 1.0e-8f)));
+    f_out = reconstruct(u, sv_new, vt);
+    alpha_out = alpha;
+}
+
+// ---------------------------------------------------------------- particle view
+// Registers of one particle while a kernel works on it.
+struct PState {
+    float2 x, v;
+    M2 c, f;
+    float mass, v0, vol, rho;
+    uint32_t mat;
+    float jp, h, q, lvs;
+    float temperature, activation;
+    float2 act_dir;
+    uint32_t pinned;
+};
+
+// MaterialModel::kirchhoff_stress per model.
+EM_HD M2 kirchhoff_stress(const MatP &m, const PState &p) {
+    const M2 f = p.f;
+    switch (m.model) {
+    case M_NEOHOOKEAN: {  // elastic.rs:180-255; damage rate in cohesion_coeff (elastic.rs:284)
+        float j = mdet(f);
+        if (j <= MIN_J) return mzero();
+        float t_scale = 1.0f + m.thermal_expansion * p.temperature;
+        float damage_scale = expf(-m.cohesion_coeff * p.q);
+        float mu = m.mu * t_scale * damage_scale;
+        float lambda = m.lambda * t_scale * damage_scale;
+        M2 b = mm(f, mtrans(f));
+        float tr_b = b.xa.x + b.ya.y;
+        M2 dev_b = msub(b, mdiag(splat(tr_b * 0.5f)));
+        float k = lambda + mu;
+        M2 dev_stress = smscale(mu / j, dev_b);
+        M2 vol_stress = smscale(k * logf(j), mident());
+        M2 viscous = mzero();
+        if (m.dynamic_viscosity > 0.0f) {  // viscosity in dynamic_viscosity (elastic.rs:285)
+            M2 sym = madd(p.c, mtrans(p.c));
+            M2 d = mscale(sym, 0.5f);
+            float d_trace = d.xa.x + d.ya.y;
+            M2 d_dev = msub(d, mdiag(splat(d_trace * 0.5f)));
+            viscous = smscale(m.dynamic_viscosity, d_dev);
+        }
+        return madd(madd(dev_stress, vol_stress), viscous);
+    }
+    case M_FLUID: {  // fluid.rs:135-191 (min_density 1e-6, fluid.rs:60)
+        float density = fminf(fmaxf(p.rho, 1.0e-6f), m.rest_density * 2.0f);
+        float pressure = fmaxf(
+            m.eos_stiffness * (powf(density / m.rest_density, m.eos_power) - 1.0f),
+            m.pressure_floor);
+        M2 stress = mdiag(splat(-pressure));
+        float eff_visc = m.dynamic_viscosity;
+        if (m.thermal_viscosity_coeff > 0.0f)
+            eff_visc = m.dynamic_viscosity * expf(-m.thermal_viscosity_coeff * p.temperature);
+        M2 sym = madd(p.c, mtrans(p.c));
+        float div_v = sym.xa.x + sym.ya.y;
+        M2 strain_dev = msub(sym, mdiag(splat(div_v * 0.5f)));
+        stress = madd(stress, smscale(eff_visc, strain_dev));
+        if (m.bulk_viscosity > 0.0f)
+            stress = madd(stress, mdiag(splat(m.bulk_viscosity * div_v * 0.5f)));
+        if (m.surface_tension_coeff != 0.0f) {
+            float j = f.xa.x * f.ya.y - f.xa.y * f.ya.x;
+            stress = madd(stress, mdiag(splat(m.surface_tension_coeff * j)));
+        }
+        return stress;
+    }
+    case M_DRUCKER_PRAGER: {  // sand.rs:220-231
+        float j = mdet(f);
+        if (j <= MIN_J) return mzero();
+        M2 r = polar(f);
+        M2 a = mm(smscale(2.0f * m.mu, msub(f, r)), mtrans(f));
+        M2 b = smscale(m.lambda * (j - 1.0f) * j, mident());
+        return madd(a, b);
+    }
+    case M_SNOW: {  // snow.rs:109-136
+        float j = mdet(f);
+        if (j <= MIN_J) return mzero();
+        M2 r = polar(f);
+        float mu_eff = m.mu * p.h;
+        float lambda_eff = m.lambda * p.h;
+        M2 tau = madd(mm(smscale(2.0f * mu_eff, msub(f, r)), mtrans(f)),
+                      smscale(lambda_eff * (j - 1.0f) * j, mident()));
+        if (m.cohesion_coeff > 0.0f && p.jp < 1.0f && j > 1.0f)
+            tau = madd(tau, smscale(m.cohesion_coeff * p.jp * (j - 1.0f) * j, mident()));
+        return tau;
+    }
+    case M_NACC: {  // nacc.rs:236-249
+        float j = fmaxf(mdet(f), MIN_J);
+        M2 b = mm(f, mtrans(f));
+        float tr_b = b.xa.x + b.ya.y;
+        M2 dev_b = msub(b, mdiag(splat(tr_b * 0.5f)));
+        M2 dev_stress = smscale(m.mu / j, dev_b);
+        M2 vol_stress = smscale(nacc_kappa(m) * 0.5f * (j * j - 1.0f), mident());
+        return madd(dev_stress, vol_stress);
+    }
+    default:  // FallbackMaterial: zero stress (materials/mod.rs:362-366)
+        return mzero();
+    }
+}
+
+// combined_kirchhoff_stress (spacetime/transfer.rs:77-104).  Only NeoHookean has a
+// non-zero activation_scale among the supported models (elastic.rs:271-273).
+EM_HD M2 combined_kirchhoff_stress(const MatP &m, const PState &p) {
+    M2 tau = kirchhoff_stress(m, p);
+    float coeff = (m.model == M_NEOHOOKEAN) ? m.active_stress_coeff : 0.0f;
+    if (p.activation <= 0.0f || coeff <= 0.0f) return tau;
+    M2 tau_active;
+    float2 n = p.act_dir;
+    float len_sq = vdot(n, n);
+    if (len_sq > F32_EPS) {
+        float2 n0 = vdivs(n, sqrtf(len_sq));
+        M2 n_outer = m2(vmuls(n0, n0.x), vmuls(n0, n0.y));
+        M2 a_mat = mscale(n_outer, p.activation * coeff);
+        tau_active = mm(mm(p.f, a_mat), mtrans(p.f));
+    } else {
+        tau_active = mdiag(splat(p.activation * coeff));
+    }
+    return madd(tau, tau_active);
+}
+
+// MaterialModel::stress_volume: Fluid uses max(volume, 1e-6) (fluid.rs:193-195),
+// every other supported model the initial volume (materials/mod.rs:114).
+EM_HD float stress_volume(const MatP &m, const PState &p) {
+    if (m.model == M_FLUID) return fmaxf(p.vol, 1.0e-6f);
+    return p.v0;
+}
+
+// MaterialModel::timestep_bound
+EM_HD float timestep_bound(const MatP &m, float density, float h, float cell, float mat_cfl,
+                           float visc_cfl) {
+    switch (m.model) {
+    case M_NEOHOOKEAN: {  // elastic.rs:290-327
+        float elastic_dt = elastic_wave_dt(m.lambda, m.mu, 1.0f, density, 1.0e-6f, cell, mat_cfl);
+        float viscous_dt = INFINITY;
+        if (m.dynamic_viscosity > 0.0f) {
+            float d = fmaxf(density, 1.0e-6f);
+            float kinematic = m.dynamic_viscosity / d;
+            if (kinematic > F32_EPS) viscous_dt = visc_cfl * cell * cell / kinematic;
+        }
+        return fminf(elastic_dt, viscous_dt);
+    }
+    case M_FLUID: {  // fluid.rs:228-259
+        const float MIN_DENSITY_RATIO = 1.0e-6f;
+        float d = fmaxf(density, 1.0e-6f);
+        float ratio = fmaxf(d / fmaxf(m.rest_density, 1.0e-6f), MIN_DENSITY_RATIO);
+        float dt_bound = INFINITY;
+        float c2 = m.eos_stiffness * m.eos_power * powf(ratio, m.eos_power - 1.0f) /
+                   fmaxf(m.rest_density, 1.0e-6f);
+        if (isfinite(c2) && c2 > F32_EPS) dt_bound = fminf(dt_bound, mat_cfl * cell / sqrtf(c2));
+        if (m.dynamic_viscosity > 0.0f) {
+            float kin = m.dynamic_viscosity / d;
+            if (kin > F32_EPS) dt_bound = fminf(dt_bound, visc_cfl * cell * cell / kin);
+        }
+        return dt_bound;
+    }
+    case M_DRUCKER_PRAGER:  // sand.rs:345-362
+        return elastic_wave_dt(m.lambda, m.mu, 1.0f, density, MIN_J, cell, mat_cfl);
+    case M_SNOW:  // snow.rs:193-211
+        return elastic_wave_dt(m.lambda, m.mu, h, density, MIN_J, cell, mat_cfl);
+    case M_NACC: {  // nacc.rs:279-298: lambda = kappa - mu = params().lambda
+        return elastic_wave_dt(m.lambda, m.mu, h, density, 1.0e-6f, cell, mat_cfl);
+    }
+    default:
+        return INFINITY;
+    }
+}
+
+EM_HD void sync_volume_density(PState &p) {
+    float j = fmaxf(mdet(p.f), MIN_J);
+    float v = fmaxf(p.v0 * j, 1.0e-6f);
+    p.vol = v;
+    p.rho = p.mass / v;
+}
+
+// DP update after the return map decision (sand.rs:258-318).
+EM_HD void dp_finish(const MatP &m, PState &p, M2 u, float2 sigma, M2 vt, bool projected,
+                     float2 proj, float dq) {
+    float2 new_sigma = sigma;
+    if (projected) {
+        float2 sigma_abs = vmax2(vabs2(sigma), splat(LOG_CLAMP));
+        float prev_det = sigma_abs.x * sigma_abs.y;
+        float new_det = proj.x * proj.y;
+        float diff = new_det - prev_det;
+        float corrected = diff > 0.0f ? new_det : prev_det + diff * 1.0f;  // volume_correction 1.0
+        p.lvs += logf(prev_det) - logf(corrected);
+        float q_max = 5.0f / fmaxf(m.dp_h2, 1e-6f);
+        p.q = fminf(p.q + dq, q_max);
+        if (m.compression_limit > 0.0f) p.lvs += sinf(m.compression_limit) * dq;  // dilatancy
+        new_sigma = proj;
+    }
+    new_sigma = vabs2(new_sigma);
+    float j_new = new_sigma.x * new_sigma.y;
+    if (j_new < m.volume_ratio_min)
+        new_sigma = vmuls(new_sigma, sqrtf(m.volume_ratio_min / fmaxf(j_new, 1e-6f)));
+    p.f = mm(mm(u, mdiag(new_sigma)), vt);
+    sync_volume_density(p);
+}
+
+// MaterialModel::update_particle
+EM_HD void update_particle(const MatP &m, PState &p, float dt) {
+    switch (m.model) {
+    case M_NEOHOOKEAN: {  // elastic.rs:262-269
+        M2 fp_new = madd(mident(), smscale(dt, p.c));
+        p.f = mm(fp_new, p.f);
+        sync_volume_density(p);
+        break;
+    }
+    case M_FLUID: {  // fluid.rs:197-207; settling_damping in dp_h0 (fluid.rs:223)
+        float j = fclampf(mdet(p.f), 0.5f, 2.0f);
+        float s = sqrtf(j);
+        p.f = m2(v2(s, 0.0f), v2(0.0f, s));
+        if (m.dp_h0 > 0.0f) {
+            float k = 1.0f - fminf(m.dp_h0 * dt, 0.5f);
+            p.v.x *= k;
+            p.v.y *= k;
+        }
+        break;
+    }
+    case M_DRUCKER_PRAGER: {  // sand.rs:248-319
+        M2 f_trial = mm(madd(mident(), smscale(dt, p.c)), p.f);
+        M2 u, vt;
+        float2 sigma;
+        svd2(f_trial, u, sigma, vt);
+        float2 proj;
+        float dq = 0.0f;
+        bool projected = dp_project(m, sigma, p.lvs, p.q, proj, dq);
+        dp_finish(m, p, u, sigma, vt, projected, proj, dq);
+        break;
+    }
+    case M_SNOW: {  // snow.rs:142-176
+        M2 f_trial = mm(madd(mident(), smscale(dt, p.c)), p.f);
+        M2 u, vt;
+        float2 sigma;
+        svd2(f_trial, u, sigma, vt);
+        float lo = 1.0f - m.compression_limit, hi = 1.0f + m.stretch_limit;
+        float2 sigma_c = v2(fclampf(sigma.x, lo, hi), fclampf(sigma.y, lo, hi));
+        float jp_new = p.jp * (sigma.x * sigma.y) / (sigma_c.x * sigma_c.y);
+        p.jp = fclampf(jp_new, m.volume_ratio_min, m.volume_ratio_max);
+        p.h = fclampf(expf(m.hardening_exponent * (1.0f - p.jp)), 0.1f, 7.0f);
+        p.f = mm(mm(u, mdiag(sigma_c)), vt);
+        sync_volume_density(p);
+        break;
+    }
+    case M_NACC: {  // nacc.rs:255-269 (no F advance on the CPU path)
+        M2 nf;
+        float na;
+        nacc_project(m, p.f, p.lvs, nf, na);
+        p.f = nf;
+        p.lvs = na;
+        float j = fmaxf(mdet(nf), MIN_J);
+        float vol = p.v0 * j;
+        p.vol = vol;
+        p.rho = vol > MIN_J ? p.mass / vol : p.rho;
+        break;
+    }
+    default:
+        break;
+    }
+}
+
+// MaterialModel::init_particle
+EM_HD void init_particle(const MatP &m, emerge_particle &p) {
+    switch (m.model) {
+    case M_DRUCKER_PRAGER:  // sand.rs:237-246
+        p.friction_hardening = m.dp_h1 > 0.0f ? m.dp_h3 / m.dp_h1 : 0.0f;
+        break;
+    case M_SNOW:  // snow.rs:104-107
+        p.plastic_volume_ratio = 1.0f;
+        p.hardening_scale = 1.0f;
+        break;
+    case M_NACC:  // nacc.rs:271-273
+        p.log_volume_strain = 0.0f;
+        break;
+    default:
+        break;
+    }
+}
+
+// ---------------------------------------------------------------- solver pieces
+struct DevConfig {
+    int res;                 // grid_res
+    float cell;              // grid_cell_size
+    float dt;                // frame dt
+    int adaptive;
+    int affine_cfl;
+    float cfl, mat_cfl, visc_cfl, min_dt;
+    int project;
+    float min_density, min_volume, min_j;
+    float2 gravity;
+    int thickness;           // config.boundary_thickness
+    float default_v0;
+    float particle_mass;
+    int max_substeps;
+    float apic_blend, j_max;
+    int n_bound;             // slip boundaries in order
+    int bound_t[8];
+};
+
+// affine_cfl_speed_contribution (step.rs:481-488)
+EM_HD float affine_cfl(M2 c, float cell) {
+    const float STENCIL_CORNER_DISTANCE = 1.5f * 1.41421356f;
+    float grad_norm = sqrtf(vlen2(c.xa) + vlen2(c.ya));
+    return grad_norm * STENCIL_CORNER_DISTANCE * cell;
+}
+
+// cfl_bound (step.rs:472-479)
+EM_HD float cfl_bound(const DevConfig &c, float max_speed, float min_mat_dt, float max_dt) {
+    float dt = max_dt;
+    if (max_speed > F32_EPS) dt = fminf(dt, c.cfl * c.cell / max_speed);
+    dt = fminf(dt, min_mat_dt);
+    return fclampf(dt, fminf(c.min_dt, max_dt), max_dt);
+}
+
+EM_HD int sat_sub(int a, int b) { return a > b ? a - b : 0; }
+
+// project_particle_state_to_admissible (step.rs:347-429); returns true if corrected.
+EM_HD bool project_state(const DevConfig &c, PState &q) {
+    bool projected = false;
+    float mn = static_cast<float>(sat_sub(c.thickness, 1));
+    float mx = static_cast<float>(sat_sub(c.res, c.thickness));
+    float2 center = splat((mn + mx) * 0.5f);
+    if (!vfinite(q.x)) {
+        q.x = center;
+        projected = true;
+    } else {
+        q.x = vclamp2(q.x, splat(mn), splat(mx));
+    }
+    if (!vfinite(q.v)) {
+        q.v = v2(0.0f, 0.0f);
+        projected = true;
+    }
+    if (!mfinite(q.c)) {
+        q.c = mzero();
+        projected = true;
+    }
+    if (!mfinite(q.f) || mdet(q.f) <= c.min_j) {
+        q.f = mident();
+        projected = true;
+    } else {
+        float j = mdet(q.f);
+        if (j > c.j_max) {
+            q.f = mscale(q.f, sqrtf(c.j_max / j));
+            projected = true;
+        }
+    }
+    if (!isfinite(q.jp) || q.jp <= 0.0f) { q.jp = 1.0f; projected = true; }
+    if (!isfinite(q.h) || q.h <= 0.0f) { q.h = 1.0f; projected = true; }
+    if (!isfinite(q.q)) { q.q = 0.0f; projected = true; }
+    if (!isfinite(q.lvs)) { q.lvs = 0.0f; projected = true; }
+    if (!isfinite(q.mass) || q.mass <= 0.0f) { q.mass = c.particle_mass; projected = true; }
+    if (!isfinite(q.v0) || q.v0 <= 0.0f) {
+        q.v0 = fmaxf(c.default_v0, c.min_volume);
+        projected = true;
+    }
+    if (!isfinite(q.vol) || q.vol <= 0.0f) {
+        q.vol = fmaxf(q.v0, c.min_volume);
+        projected = true;
+    }
+    if (!isfinite(q.rho) || q.rho <= 0.0f) {
+        q.rho = fmaxf(q.mass / q.vol, c.min_density);
+        projected = true;
+    } else {
+        q.rho = fmaxf(q.rho, c.min_density);
+    }
+    return projected;
+}
+
+// apply_slip_wall_velocity (forces/boundary/mod.rs:78-101) for cell (x, y)
+EM_HD void slip_velocity(int thickness, int x, int y, int res, float2 &v) {
+    int hi = res - (thickness + 1);
+    if (x < thickness) v.x = fmaxf(v.x, 0.0f);
+    if (x > hi) v.x = fminf(v.x, 0.0f);
+    if (y < thickness) v.y = fmaxf(v.y, 0.0f);
+    if (y > hi) v.y = fminf(v.y, 0.0f);
+}
+
+// clamp_position_inside_grid (forces/boundary/mod.rs:103-111)
+EM_HD float2 clamp_position(int thickness, float2 pos, int res) {
+    float mn = static_cast<float>(sat_sub(thickness, 1));
+    float mx = static_cast<float>(sat_sub(res, thickness));
+    return vclamp2(pos, splat(mn), splat(mx));
+}
+
+}  // namespace emerge

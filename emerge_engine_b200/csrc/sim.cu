@@ -1,0 +1,995 @@
+// sim.cu -- host runtime of the CUDA backend and the C ABI (include/emerge_cuda.h).
+//
+// One emerge_sim owns: the particle SoA (two slot-order copies, swapped by the
+// sort), the tiled grid, the sort scratch, the device step controller, an AoS
+// staging buffer for uploads/readbacks, a stream, and a CUDA graph per step.
+// The graph is [k_step_begin] -> while(cont){k_substep_begin, k_grid_update,
+// k_particle, k_density?}: the adaptive substep loop of Simulation::step
+// (spacetime/solver/step.rs:34-49) runs on the device with no host round trip.
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "device_state.cuh"
+#include "kernels.h"
+
+using namespace emerge;
+
+namespace {
+
+thread_local std::string g_global_error;
+
+constexpr float F32_EPSILON = 1.1920929e-7f;
+
+struct Buffer {
+    void *ptr = nullptr;
+    size_t bytes = 0;
+    ~Buffer() { reset(); }
+    void reset() {
+        if (ptr) cudaFree(ptr);
+        ptr = nullptr;
+        bytes = 0;
+    }
+};
+
+// Bump allocator over one device allocation, 256-byte aligned pieces.
+struct Carver {
+    uintptr_t p;
+    explicit Carver(void *base) : p(reinterpret_cast<uintptr_t>(base)) {}
+    template <class T>
+    T *take(size_t n) {
+        p = (p + 255) & ~static_cast<uintptr_t>(255);
+        T *r = reinterpret_cast<T *>(p);
+        p += n * sizeof(T);
+        return r;
+    }
+};
+
+size_t particle_set_bytes(size_t cap) {
+    // 2 float2 + 2 float4 + 12 four-byte scalars + float2 + slot index + rho_dp, + alignment
+    return cap * (8 * 2 + 16 * 2 + 4 * 16 + 8 + 4 + 4) + 32 * 256;
+}
+
+DevParticles carve_particles(Carver &c, size_t cap) {
+    DevParticles P;
+    P.x = c.take<float2>(cap);
+    P.v = c.take<float2>(cap);
+    P.c = c.take<float4>(cap);
+    P.f = c.take<float4>(cap);
+    P.mass = c.take<float>(cap);
+    P.v0 = c.take<float>(cap);
+    P.vol = c.take<float>(cap);
+    P.rho = c.take<float>(cap);
+    P.mat = c.take<uint32_t>(cap);
+    P.jp = c.take<float>(cap);
+    P.h = c.take<float>(cap);
+    P.q = c.take<float>(cap);
+    P.lvs = c.take<float>(cap);
+    P.temperature = c.take<float>(cap);
+    P.activation = c.take<float>(cap);
+    P.act_dir = c.take<float2>(cap);
+    P.pinned = c.take<uint32_t>(cap);
+    P.user_tag = c.take<uint32_t>(cap);
+    P.muscle = c.take<uint32_t>(cap);
+    P.contact = c.take<uint32_t>(cap);
+    P.sleeping = c.take<uint32_t>(cap);
+    P.scalar = c.take<float>(cap);
+    P.slot_to_index = c.take<uint32_t>(cap);
+    P.rho_dp = c.take<float>(cap);
+    return P;
+}
+
+bool model_supported(uint32_t m) {
+    return m == M_FALLBACK || m == M_FLUID || m == M_NEOHOOKEAN || m == M_SNOW ||
+           m == M_DRUCKER_PRAGER || m == M_NACC;
+}
+
+// LcgRng (spacetime/solver/mod.rs:154-175)
+struct Lcg {
+    uint32_t state;
+    uint32_t next_u32() {
+        state = state * 1664525u + 1013904223u;
+        return state;
+    }
+    float next_f32() { return static_cast<float>(next_u32()) / 4294967296.0f; }
+};
+
+size_t sat_sub_sz(size_t a, size_t b) { return a > b ? a - b : 0; }
+
+}  // namespace
+
+struct emerge_sim {
+    emerge_sim_config cfg{};
+    DevConfig dcfg{};
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    std::string error;
+
+    // particles
+    size_t n = 0, cap = 0;
+    Buffer pbuf;             // two particle sets
+    DevParticles P[2];
+    int cur = 0;
+    Buffer staging;          // AoS staging (cap * 128 B)
+    emerge_particle *d_aos = nullptr;
+    uint32_t next_tag = 1;
+    LoadFlagsHost lf;
+    std::vector<uint8_t> host_pinned_flag;  // not used for stepping; kept for add/write scans
+
+    // grid
+    int res = 0, tpd = 0;
+    Buffer gbuf;
+    GridView g{};
+
+    // materials / boundaries
+    std::vector<emerge_material_params> mats;
+    Buffer mbuf;
+    std::vector<uint64_t> bounds;
+
+    // controller
+    Buffer sbuf;
+    StepState *d_state = nullptr;
+    StepState *h_state = nullptr;  // pinned mirror
+    Buffer region_buf;
+
+    // sort
+    Buffer sortbuf;
+    SortScratch sort;
+    size_t sort_cap = 0;
+    uint64_t steps_since_sort = 0;
+    bool sorted_once = false;
+    unsigned long long fallback_at_sort = 0, blocks_at_sort = 0;
+
+    // step pipeline
+    bool pending_valid = false;  // the next substep's P2G (+density) is already on the grid
+    int use_graph = 1;
+    int use_window = 1;
+    int64_t sort_interval = 0;   // 0 = adaptive
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t graph_exec = nullptr;
+    bool graph_dirty = true;
+    unsigned long long host_launches = 0;
+    unsigned long long graph_launches = 0;
+    cudaEvent_t ev[8] = {};
+    emerge_step_timing last_timing{};
+
+    int fail(emerge_status st, const std::string &msg) {
+        error = msg;
+        return st;
+    }
+};
+
+namespace {
+
+bool cuda_ok(emerge_sim *s, cudaError_t e, const char *what, emerge_status *out) {
+    if (e == cudaSuccess) return true;
+    s->error = std::string(what) + ": " + cudaGetErrorString(e);
+    *out = (e == cudaErrorMemoryAllocation) ? EMERGE_ERR_OOM : EMERGE_ERR_CUDA;
+    return false;
+}
+
+#define CK(call)                                                    \
+    do {                                                            \
+        emerge_status st_ = EMERGE_OK;                              \
+        if (!cuda_ok(s, (call), #call, &st_)) return st_;           \
+    } while (0)
+
+// SimConfig::validate (config.rs:247-299) plus the device path's feature gates.
+emerge_status validate_config(const emerge_sim_config &c, std::string &msg) {
+    auto bad = [&](const char *m) {
+        msg = m;
+        return EMERGE_ERR_INVALID_ARG;
+    };
+    if (c.grid_res < 4) return bad("grid_res must be >= 4");
+    if (!(c.grid_cell_size > 0.0f)) return bad("grid_cell_size must be positive");
+    if (!(c.dt > 0.0f)) return bad("dt must be positive");
+    if (!(c.cfl_coefficient > 0.0f)) return bad("cfl_coefficient must be positive");
+    if (!(c.material_cfl_coefficient > 0.0f)) return bad("material_cfl_coefficient must be positive");
+    if (!(c.viscous_timestep_coefficient > 0.0f))
+        return bad("viscous_timestep_coefficient must be positive");
+    if (!(c.min_dt > 0.0f)) return bad("min_dt must be positive");
+    if (!(c.min_dt <= c.dt)) return bad("min_dt must be <= dt");
+    if (!(c.projection_min_density > 0.0f)) return bad("projection_min_density must be positive");
+    if (!(c.projection_min_volume > 0.0f)) return bad("projection_min_volume must be positive");
+    if (!(c.projection_min_deformation_j > 0.0f))
+        return bad("projection_min_deformation_j must be positive");
+    if (!(c.particle_mass > 0.0f)) return bad("particle_mass must be positive");
+    if (!(c.contact_friction >= 0.0f)) return bad("contact_friction must be non-negative");
+    if (c.max_substeps_per_step == 0) return bad("max_substeps_per_step must be > 0");
+    if (!(c.default_initial_volume > 0.0f)) return bad("default_initial_volume must be positive");
+    if (!(c.j_max > 1.0f)) return bad("j_max must be > 1.0");
+    if (!(c.apic_blend >= 0.0f && c.apic_blend <= 1.0f)) return bad("apic_blend must be in [0, 1]");
+    if (!(c.boundary_thickness > 0 && c.boundary_thickness < c.grid_res - 1))
+        return bad("boundary_thickness must be in [1, grid_res-2]");
+    if (c.grid_res > 32768) {
+        msg = "grid_res above 32768 is not supported by the device grid";
+        return EMERGE_ERR_UNSUPPORTED;
+    }
+    if (c.sleep_threshold > 0.0f) {
+        msg = "sleep_threshold > 0 (sleep partition) is not on the device path";
+        return EMERGE_ERR_UNSUPPORTED;
+    }
+    if (c.asflip_blend > 0.0f) {
+        msg = "asflip_blend > 0 (ASFLIP) is not on the device path";
+        return EMERGE_ERR_UNSUPPORTED;
+    }
+    if (c.max_substeps_per_step > 0x7fffffffull) {
+        msg = "max_substeps_per_step too large";
+        return EMERGE_ERR_INVALID_ARG;
+    }
+    return EMERGE_OK;
+}
+
+DevConfig make_dev_config(const emerge_sim_config &c, const std::vector<uint64_t> &bounds) {
+    DevConfig d{};
+    d.res = static_cast<int>(c.grid_res);
+    d.cell = c.grid_cell_size;
+    d.dt = c.dt;
+    d.adaptive = c.adaptive_timestep ? 1 : 0;
+    d.affine_cfl = c.cfl_include_affine_speed ? 1 : 0;
+    d.cfl = c.cfl_coefficient;
+    d.mat_cfl = c.material_cfl_coefficient;
+    d.visc_cfl = c.viscous_timestep_coefficient;
+    d.min_dt = c.min_dt;
+    d.project = c.project_invalid_state ? 1 : 0;
+    d.min_density = c.projection_min_density;
+    d.min_volume = c.projection_min_volume;
+    d.min_j = c.projection_min_deformation_j;
+    d.gravity = make_float2(c.gravity[0], c.gravity[1]);
+    d.thickness = static_cast<int>(c.boundary_thickness);
+    d.default_v0 = c.default_initial_volume;
+    d.particle_mass = c.particle_mass;
+    d.max_substeps = static_cast<int>(c.max_substeps_per_step);
+    d.apic_blend = c.apic_blend;
+    d.j_max = c.j_max;
+    d.n_bound = static_cast<int>(bounds.size());
+    for (size_t k = 0; k < bounds.size() && k < static_cast<size_t>(MAX_BOUNDARIES); ++k)
+        d.bound_t[k] = static_cast<int>(bounds[k]);
+    return d;
+}
+
+StepLaunch make_launch(emerge_sim *s) {
+    StepLaunch L;
+    L.P = s->P[s->cur];
+    L.n = static_cast<int>(s->n);
+    L.mats = static_cast<const MatP *>(s->mbuf.ptr);
+    L.n_mats = static_cast<int>(s->mats.size());
+    L.cfg = s->dcfg;
+    L.st = s->d_state;
+    L.g = s->g;
+    int density = s->cfg.recompute_density_each_step ? 1 : 0;
+    for (const auto &m : s->mats)
+        if (m.model == M_FLUID) density = 1;  // needs_density_recompute (fluid.rs:261-263)
+    L.density_mode = density;
+    L.use_window = s->use_window;
+    L.stream = s->stream;
+    return L;
+}
+
+void update_material_flags(emerge_sim *s) {
+    s->lf.temperature = 0;
+    s->lf.activation = 0;
+    for (const auto &m : s->mats) {
+        if (m.model == M_NEOHOOKEAN && m.thermal_expansion != 0.0f) s->lf.temperature = 1;
+        if (m.model == M_FLUID && m.thermal_viscosity_coeff > 0.0f) s->lf.temperature = 1;
+        if (m.model == M_NEOHOOKEAN && m.active_stress_coeff > 0.0f) s->lf.activation = 1;
+    }
+}
+
+emerge_status ensure_capacity(emerge_sim *s, size_t need) {
+    if (need <= s->cap) return EMERGE_OK;
+    size_t cap = s->cap ? s->cap : 1024;
+    while (cap < need) cap *= 2;
+    size_t bytes = 2 * particle_set_bytes(cap);
+    void *ptr = nullptr;
+    CK(cudaMalloc(&ptr, bytes));
+    Carver c(ptr);
+    DevParticles np[2];
+    np[0] = carve_particles(c, cap);
+    np[1] = carve_particles(c, cap);
+    if (s->n > 0) {
+        // move the live set into np[0] (same slot order)
+        std::vector<uint32_t> ident;  // identity permutation via a device copy of slots
+        uint32_t *d_perm = nullptr;
+        CK(cudaMalloc(&d_perm, s->n * sizeof(uint32_t)));
+        ident.resize(s->n);
+        for (size_t i = 0; i < s->n; ++i) ident[i] = static_cast<uint32_t>(i);
+        CK(cudaMemcpyAsync(d_perm, ident.data(), s->n * sizeof(uint32_t), cudaMemcpyHostToDevice,
+                           s->stream));
+        launch_permute(s->P[s->cur], np[0], d_perm, static_cast<int>(s->n), s->stream);
+        s->host_launches += 1;
+        CK(cudaStreamSynchronize(s->stream));
+        cudaFree(d_perm);
+    }
+    s->pbuf.reset();
+    s->pbuf.ptr = ptr;
+    s->pbuf.bytes = bytes;
+    s->P[0] = np[0];
+    s->P[1] = np[1];
+    s->cur = 0;
+    s->cap = cap;
+    s->staging.reset();
+    CK(cudaMalloc(&s->staging.ptr, cap * sizeof(emerge_particle)));
+    s->staging.bytes = cap * sizeof(emerge_particle);
+    s->d_aos = static_cast<emerge_particle *>(s->staging.ptr);
+    s->sortbuf.reset();
+    size_t sb = sort_scratch_bytes(cap);
+    CK(cudaMalloc(&s->sortbuf.ptr, sb));
+    s->sortbuf.bytes = sb;
+    sort_scratch_bind(s->sort, s->sortbuf.ptr, cap);
+    s->graph_dirty = true;
+    return EMERGE_OK;
+}
+
+emerge_status upload_materials(emerge_sim *s) {
+    CK(cudaMemcpyAsync(s->mbuf.ptr, s->mats.data(), s->mats.size() * sizeof(emerge_material_params),
+                       cudaMemcpyHostToDevice, s->stream));
+    update_material_flags(s);
+    s->graph_dirty = true;
+    return EMERGE_OK;
+}
+
+void destroy_graph(emerge_sim *s) {
+    if (s->graph_exec) cudaGraphExecDestroy(s->graph_exec);
+    if (s->graph) cudaGraphDestroy(s->graph);
+    s->graph_exec = nullptr;
+    s->graph = nullptr;
+}
+
+emerge_status build_graph(emerge_sim *s) {
+    destroy_graph(s);
+    StepLaunch L = make_launch(s);
+    cudaGraph_t graph;
+    CK(cudaGraphCreate(&graph, 0));
+    s->graph = graph;
+    // node 1: k_step_begin (captured into the top-level graph)
+    CK(cudaStreamBeginCaptureToGraph(s->stream, graph, nullptr, nullptr, 0,
+                                     cudaStreamCaptureModeThreadLocal));
+    launch_step_begin(L);
+    CK(cudaStreamEndCapture(s->stream, &graph));
+    size_t nn = 0;
+    CK(cudaGraphGetNodes(graph, nullptr, &nn));
+    std::vector<cudaGraphNode_t> nodes(nn);
+    CK(cudaGraphGetNodes(graph, nodes.data(), &nn));
+    cudaGraphConditionalHandle handle;
+    CK(cudaGraphConditionalHandleCreate(&handle, graph, 1, cudaGraphCondAssignDefault));
+    cudaGraphNodeParams cp = {};
+    cp.type = cudaGraphNodeTypeConditional;
+    cp.conditional.handle = handle;
+    cp.conditional.type = cudaGraphCondTypeWhile;
+    cp.conditional.size = 1;
+    cudaGraphNode_t wnode;
+    CK(cudaGraphAddNode(&wnode, graph, nodes.data(), nn, &cp));
+    cudaGraph_t body = cp.conditional.phGraph_out[0];
+    const int kps = 3 + (L.density_mode ? 1 : 0);
+    CK(cudaStreamBeginCaptureToGraph(s->stream, body, nullptr, nullptr, 0,
+                                     cudaStreamCaptureModeThreadLocal));
+    launch_substep_begin(L, 1, static_cast<unsigned long long>(handle), kps);
+    launch_grid_update(L);
+    launch_particle_pass(L, s->lf, 1);
+    if (L.density_mode) launch_density_pass(L, s->lf);
+    CK(cudaStreamEndCapture(s->stream, &body));
+    CK(cudaGraphInstantiate(&s->graph_exec, graph, 0));
+    s->graph_dirty = false;
+    return EMERGE_OK;
+}
+
+emerge_status prime(emerge_sim *s) {
+    StepLaunch L = make_launch(s);
+    launch_prime_setup(L);
+    launch_particle_pass(L, s->lf, 0);
+    s->host_launches += 2;
+    if (L.density_mode) {
+        launch_density_pass(L, s->lf);
+        s->host_launches += 1;
+    }
+    CK(cudaGetLastError());
+    s->pending_valid = true;
+    return EMERGE_OK;
+}
+
+emerge_status sort_particles(emerge_sim *s, int key_mode) {
+    if (s->n < 2) return EMERGE_OK;
+    int n = static_cast<int>(s->n);
+    launch_sort_keys(s->P[s->cur].x, n, s->res, key_mode, s->sort.keys[0], s->sort.vals[0],
+                     s->stream);
+    int bits = sort_key_bits(s->res, key_mode);
+    int r = radix_sort_pairs(s->sort, n, bits, s->stream);
+    launch_permute(s->P[s->cur], s->P[s->cur ^ 1], s->sort.vals[r], n, s->stream);
+    s->host_launches += 2 + 5 * ((bits + 7) / 8);
+    s->cur ^= 1;
+    s->graph_dirty = true;
+    s->sorted_once = true;
+    s->steps_since_sort = 0;
+    CK(cudaGetLastError());
+    return EMERGE_OK;
+}
+
+// Particle order policy: sort when never sorted, every sort_interval steps when
+// set, else when more than 5% of the particle-pass CTAs since the last sort had
+// to fall back to global reductions (their stencils no longer fit one window).
+emerge_status maybe_sort(emerge_sim *s) {
+    bool need = !s->sorted_once;
+    if (!need && s->sort_interval > 0) need = s->steps_since_sort >= static_cast<uint64_t>(s->sort_interval);
+    if (!need && s->sort_interval == 0 && s->use_window) {
+        // the pinned mirror is refreshed after every step launch (async); use what is there
+        unsigned long long fb = s->h_state->window_fallback - s->fallback_at_sort;
+        unsigned long long bl = s->h_state->window_blocks - s->blocks_at_sort;
+        if (bl > 0 && fb * 20 > bl) need = true;
+    }
+    if (!need) return EMERGE_OK;
+    emerge_status st = sort_particles(s, 0);
+    s->fallback_at_sort = s->h_state->window_fallback;
+    s->blocks_at_sort = s->h_state->window_blocks;
+    return st;
+}
+
+emerge_status run_host_loop_step(emerge_sim *s, bool timed) {
+    StepLaunch L = make_launch(s);
+    float t_cfl = 0, t_grid = 0, t_part = 0, t_dens = 0;
+    if (timed) CK(cudaEventRecord(s->ev[0], s->stream));
+    launch_step_begin(L);
+    s->host_launches += 1;
+    CK(cudaMemcpyAsync(s->h_state, s->d_state, sizeof(StepState), cudaMemcpyDeviceToHost, s->stream));
+    CK(cudaStreamSynchronize(s->stream));
+    while (s->h_state->cont) {
+        CK(cudaEventRecord(s->ev[1], s->stream));
+        launch_substep_begin(L, 0, 0ull, 0);
+        CK(cudaEventRecord(s->ev[2], s->stream));
+        launch_grid_update(L);
+        CK(cudaEventRecord(s->ev[3], s->stream));
+        launch_particle_pass(L, s->lf, 1);
+        CK(cudaEventRecord(s->ev[4], s->stream));
+        s->host_launches += 3;
+        if (L.density_mode) {
+            launch_density_pass(L, s->lf);
+            s->host_launches += 1;
+        }
+        CK(cudaEventRecord(s->ev[5], s->stream));
+        CK(cudaMemcpyAsync(s->h_state, s->d_state, sizeof(StepState), cudaMemcpyDeviceToHost,
+                           s->stream));
+        CK(cudaStreamSynchronize(s->stream));
+        CK(cudaGetLastError());
+        float a, b, c, d;
+        cudaEventElapsedTime(&a, s->ev[1], s->ev[2]);
+        cudaEventElapsedTime(&b, s->ev[2], s->ev[3]);
+        cudaEventElapsedTime(&c, s->ev[3], s->ev[4]);
+        cudaEventElapsedTime(&d, s->ev[4], s->ev[5]);
+        t_cfl += a;
+        t_grid += b;
+        t_part += c;
+        t_dens += d;
+    }
+    if (timed) {
+        CK(cudaEventRecord(s->ev[6], s->stream));
+        CK(cudaEventSynchronize(s->ev[6]));
+        float tot;
+        cudaEventElapsedTime(&tot, s->ev[0], s->ev[6]);
+        emerge_step_timing &t = s->last_timing;
+        std::memset(&t, 0, sizeof(t));
+        t.cfl_us = static_cast<uint64_t>(t_cfl * 1000.0f);
+        t.grid_update_us = static_cast<uint64_t>(t_grid * 1000.0f);
+        t.g2p_us = static_cast<uint64_t>(t_part * 1000.0f);  // fused G2P+update+projection+P2G pass
+        t.density_us = static_cast<uint64_t>(t_dens * 1000.0f);
+        t.total_us = static_cast<uint64_t>(tot * 1000.0f);
+    }
+    return EMERGE_OK;
+}
+
+emerge_status spawn_region(emerge_sim *s, const emerge_spawn_region &sp, uint32_t tag,
+                           std::vector<emerge_particle> &out) {
+    // initialize_particles (spacetime/solver/mod.rs:88-151)
+    if (!(sp.spacing > 0.0f) || sp.box_size[0] <= 0 || sp.box_size[1] <= 0)
+        return static_cast<emerge_status>(s->fail(EMERGE_ERR_INVALID_ARG, "spawn: spacing and box_size must be positive"));
+    float hx = static_cast<float>(sp.box_size[0]) * 0.5f, hy = static_cast<float>(sp.box_size[1]) * 0.5f;
+    float mnx = sp.box_center[0] - hx, mny = sp.box_center[1] - hy;
+    float mxx = sp.box_center[0] + hx, mxy = sp.box_center[1] + hy;
+    // SpawnRegion::fits_in_sim (config.rs:472-482)
+    float dmin = static_cast<float>(s->cfg.boundary_thickness);
+    float dmax = static_cast<float>(sat_sub_sz(s->cfg.grid_res, s->cfg.boundary_thickness));
+    if (!(mnx >= dmin && mny >= dmin && mxx <= dmax && mxy <= dmax))
+        return static_cast<emerge_status>(s->fail(EMERGE_ERR_INVALID_ARG,
+                                                  "spawn region must stay inside the simulation domain"));
+    float mass = sp.has_mass_override ? sp.mass_override : s->cfg.particle_mass;
+    float v0 = s->cfg.default_initial_volume;
+    Lcg rng{sp.rng_seed};
+    const emerge_material_params *mat =
+        sp.material_id < s->mats.size() ? &s->mats[sp.material_id] : nullptr;
+    for (float i = mnx; i < mxx; i += sp.spacing) {
+        for (float j = mny; j < mxy; j += sp.spacing) {
+            bool inside = true;
+            if (sp.shape == 1) {
+                float dx = i - sp.box_center[0], dy = j - sp.box_center[1];
+                inside = std::sqrt(dx * dx + dy * dy) <= sp.disk_radius;
+            }
+            if (!inside) continue;
+            float jitter_mag = sp.position_jitter * sp.spacing;
+            float jx = (rng.next_f32() - 0.5f) * 2.0f * jitter_mag;
+            float jy = (rng.next_f32() - 0.5f) * 2.0f * jitter_mag;
+            float rx = rng.next_f32();
+            float ry = rng.next_f32();
+            emerge_particle q;
+            std::memset(&q, 0, sizeof(q));
+            q.x[0] = i + jx;
+            q.x[1] = j + jy;
+            q.v[0] = (rx - 0.5f) * sp.initial_velocity_scale;
+            q.v[1] = (ry - 0.5f) * sp.initial_velocity_scale;
+            std::memcpy(q.f, sp.initial_deformation_gradient, sizeof(q.f));
+            q.mass = mass;
+            q.initial_volume = v0;
+            q.volume = v0;
+            q.density = mass / v0;
+            q.material_id = sp.material_id;
+            q.plastic_volume_ratio = 1.0f;
+            q.hardening_scale = 1.0f;
+            q.user_tag = tag;
+            if (mat) init_particle(*mat, q);  // add_body stamps + init (particles.rs:383-392)
+            out.push_back(q);
+        }
+    }
+    return EMERGE_OK;
+}
+
+// Appends host particles and optionally runs the local (add_body) or full
+// (Simulation::new) initial-volume estimate on the device.
+emerge_status append_particles(emerge_sim *s, const emerge_particle *src, size_t count,
+                               int volume_mode /*0 none, 1 local, 2 full*/) {
+    for (size_t k = 0; k < count; ++k) {
+        if (src[k].contact_group != 0)
+            return static_cast<emerge_status>(s->fail(
+                EMERGE_ERR_UNSUPPORTED, "contact_group != 0 (multi-field contact) is not on the device path"));
+    }
+    if (s->n + count > 0x7fffffffull)
+        return static_cast<emerge_status>(s->fail(EMERGE_ERR_INVALID_ARG, "too many particles"));
+    emerge_status st = ensure_capacity(s, s->n + count);
+    if (st != EMERGE_OK) return st;
+    for (size_t k = 0; k < count; ++k)
+        if (src[k].pinned) s->lf.pinned = 1;
+    const int n_old = static_cast<int>(s->n), n_new = static_cast<int>(s->n + count);
+    if (count > 0) {
+        CK(cudaMemcpyAsync(s->d_aos, src, count * sizeof(emerge_particle), cudaMemcpyHostToDevice,
+                           s->stream));
+        launch_append_aos(s->P[s->cur], n_old, n_new, s->d_aos, s->stream);
+        s->host_launches += 1;
+    }
+    s->n = static_cast<size_t>(n_new);
+    if (volume_mode != 0 && count > 0) {
+        // estimate_particle_volumes_local (density.rs:81-144) / estimate_particle_volumes (:41-72)
+        int filter = 0;
+        float lox = 0, loy = 0, hix = 0, hiy = 0;
+        if (volume_mode == 1) {
+            float lo[2] = {3.402823466e38f, 3.402823466e38f};
+            float hi[2] = {-3.402823466e38f, -3.402823466e38f};
+            for (size_t k = 0; k < count; ++k)
+                for (int d = 0; d < 2; ++d) {
+                    lo[d] = std::fmin(lo[d], src[k].x[d]);
+                    hi[d] = std::fmax(hi[d], src[k].x[d]);
+                }
+            lox = lo[0] - 3.0f;
+            loy = lo[1] - 3.0f;
+            hix = hi[0] + 3.0f;
+            hiy = hi[1] + 3.0f;
+            filter = 1;
+        }
+        size_t cells = static_cast<size_t>(s->tpd) * s->tpd * TILE_CELLS;
+        CK(cudaMemsetAsync(s->g.acc_a, 0, cells * sizeof(float4), s->stream));
+        launch_mass_scatter(s->P[s->cur], n_new, s->g, filter, lox, loy, hix, hiy, s->stream);
+        launch_mass_gather(s->P[s->cur], volume_mode == 1 ? n_old : 0, n_new, s->g, 1, s->stream);
+        CK(cudaMemsetAsync(s->g.acc_a, 0, cells * sizeof(float4), s->stream));
+        CK(cudaMemsetAsync(s->g.acc_s, 0, cells * sizeof(float2), s->stream));
+        CK(cudaMemsetAsync(s->g.tile_flag, 0, static_cast<size_t>(s->tpd) * s->tpd, s->stream));
+        s->host_launches += 2;
+    }
+    CK(cudaGetLastError());
+    s->pending_valid = false;
+    s->graph_dirty = true;
+    s->sorted_once = false;
+    return EMERGE_OK;
+}
+
+emerge_status invalidate_pending(emerge_sim *s) {
+    if (!s->pending_valid) return EMERGE_OK;
+    size_t cells = static_cast<size_t>(s->tpd) * s->tpd * TILE_CELLS;
+    CK(cudaMemsetAsync(s->g.acc_a, 0, cells * sizeof(float4), s->stream));
+    CK(cudaMemsetAsync(s->g.acc_s, 0, cells * sizeof(float2), s->stream));
+    CK(cudaMemsetAsync(s->g.tile_flag, 0, static_cast<size_t>(s->tpd) * s->tpd, s->stream));
+    s->pending_valid = false;
+    return EMERGE_OK;
+}
+
+}  // namespace
+
+// =============================================================== C ABI
+extern "C" {
+
+const char *emerge_cuda_last_error(const emerge_sim *sim) {
+    return sim ? sim->error.c_str() : "null simulation handle";
+}
+
+const char *emerge_cuda_last_global_error(void) { return g_global_error.c_str(); }
+
+emerge_status emerge_cuda_create(const emerge_sim_config *config, int device, emerge_sim **out) {
+    if (!config || !out) {
+        g_global_error = "null argument";
+        return EMERGE_ERR_INVALID_ARG;
+    }
+    *out = nullptr;
+    std::string msg;
+    emerge_status vs = validate_config(*config, msg);
+    if (vs != EMERGE_OK) {
+        g_global_error = msg;
+        return vs;
+    }
+    int ndev = 0;
+    cudaError_t e = cudaGetDeviceCount(&ndev);
+    if (e != cudaSuccess || ndev == 0) {
+        g_global_error = std::string("no CUDA device available: ") + cudaGetErrorString(e);
+        return EMERGE_ERR_CUDA;
+    }
+    if (device < 0 || device >= ndev) {
+        g_global_error = "device index out of range";
+        return EMERGE_ERR_INVALID_ARG;
+    }
+    e = cudaSetDevice(device);
+    if (e != cudaSuccess) {
+        g_global_error = std::string("cudaSetDevice: ") + cudaGetErrorString(e);
+        return EMERGE_ERR_CUDA;
+    }
+    emerge_sim *s = new emerge_sim();
+    s->cfg = *config;
+    s->device = device;
+    s->bounds.push_back(config->boundary_thickness);  // default SlipBoundary (lifecycle.rs:29-30)
+    s->dcfg = make_dev_config(s->cfg, s->bounds);
+    emerge_material_params fallback;
+    std::memset(&fallback, 0, sizeof(fallback));
+    s->mats.push_back(fallback);
+    auto bail = [&](emerge_status st) {
+        g_global_error = s->error;
+        emerge_cuda_destroy(s);
+        return st;
+    };
+    emerge_status st = EMERGE_OK;
+    if (!cuda_ok(s, cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking), "stream", &st))
+        return bail(st);
+    for (auto &ev : s->ev)
+        if (!cuda_ok(s, cudaEventCreate(&ev), "event", &st)) return bail(st);
+    s->res = static_cast<int>(config->grid_res);
+    s->tpd = (s->res + TILE - 1) / TILE;
+    size_t cells = static_cast<size_t>(s->tpd) * s->tpd * TILE_CELLS;
+    size_t gbytes = cells * (sizeof(float4) + 2 * sizeof(float2)) + static_cast<size_t>(s->tpd) * s->tpd + 4 * 256;
+    if (!cuda_ok(s, cudaMalloc(&s->gbuf.ptr, gbytes), "grid alloc", &st)) return bail(st);
+    s->gbuf.bytes = gbytes;
+    Carver c(s->gbuf.ptr);
+    s->g.res = s->res;
+    s->g.tpd = s->tpd;
+    s->g.acc_a = c.take<float4>(cells);
+    s->g.acc_s = c.take<float2>(cells);
+    s->g.grid_v = c.take<float2>(cells);
+    s->g.tile_flag = c.take<uint8_t>(static_cast<size_t>(s->tpd) * s->tpd);
+    if (!cuda_ok(s, cudaMemsetAsync(s->gbuf.ptr, 0, gbytes, s->stream), "grid clear", &st)) return bail(st);
+    if (!cuda_ok(s, cudaMalloc(&s->mbuf.ptr, MAX_MATERIALS * sizeof(emerge_material_params)), "mat alloc", &st))
+        return bail(st);
+    if (!cuda_ok(s, cudaMalloc(&s->sbuf.ptr, sizeof(StepState)), "state alloc", &st)) return bail(st);
+    s->d_state = static_cast<StepState *>(s->sbuf.ptr);
+    if (!cuda_ok(s, cudaMallocHost(&s->h_state, sizeof(StepState)), "pinned alloc", &st)) return bail(st);
+    std::memset(s->h_state, 0, sizeof(StepState));
+    s->h_state->last_step_dt = config->dt;
+    s->h_state->min_mdt_bits[0] = s->h_state->min_mdt_bits[1] = 0x7f800000u;
+    if (!cuda_ok(s, cudaMemcpyAsync(s->d_state, s->h_state, sizeof(StepState), cudaMemcpyHostToDevice, s->stream),
+                 "state init", &st))
+        return bail(st);
+    if (!cuda_ok(s, cudaMalloc(&s->region_buf.ptr, region_acc_bytes()), "region alloc", &st)) return bail(st);
+    if (upload_materials(s) != EMERGE_OK) return bail(EMERGE_ERR_CUDA);
+    if (ensure_capacity(s, 1024) != EMERGE_OK) return bail(EMERGE_ERR_OOM);
+    if (!cuda_ok(s, cudaStreamSynchronize(s->stream), "create sync", &st)) return bail(st);
+    const char *env = std::getenv("EMERGE_CUDA_USE_GRAPH");
+    if (env) s->use_graph = std::atoi(env) != 0;
+    *out = s;
+    return EMERGE_OK;
+}
+
+emerge_status emerge_cuda_destroy(emerge_sim *s) {
+    if (!s) return EMERGE_OK;
+    if (s->stream) cudaStreamSynchronize(s->stream);
+    destroy_graph(s);
+    for (auto &ev : s->ev)
+        if (ev) cudaEventDestroy(ev);
+    if (s->h_state) cudaFreeHost(s->h_state);
+    s->pbuf.reset();
+    s->staging.reset();
+    s->gbuf.reset();
+    s->mbuf.reset();
+    s->sbuf.reset();
+    s->sortbuf.reset();
+    s->region_buf.reset();
+    if (s->stream) cudaStreamDestroy(s->stream);
+    delete s;
+    return EMERGE_OK;
+}
+
+emerge_status emerge_cuda_set_materials(emerge_sim *s, const emerge_material_params *params,
+                                        uint32_t count) {
+    if (!s || (!params && count)) return EMERGE_ERR_INVALID_ARG;
+    if (count == 0 || count > MAX_MATERIALS)
+        return static_cast<emerge_status>(s->fail(EMERGE_ERR_INVALID_ARG, "material count must be in [1, 64]"));
+    for (uint32_t k = 0; k < count; ++k)
+        if (!model_supported(params[k].model))
+            return static_cast<emerge_status>(
+                s->fail(EMERGE_ERR_UNSUPPORTED, "material " + std::to_string(k) + ": constitutive model " +
+                                                    std::to_string(params[k].model) + " is not on the device path"));
+    bool default_changed = s->mats.empty() || std::memcmp(&s->mats[0], &params[0], sizeof(emerge_material_params)) != 0;
+    s->mats.assign(params, params + count);
+    emerge_status st = upload_materials(s);
+    if (st != EMERGE_OK) return st;
+    if (default_changed && s->n > 0) {
+        launch_reinit(s->P[s->cur], static_cast<int>(s->n), static_cast<const MatP *>(s->mbuf.ptr),
+                      static_cast<int>(count), s->stream);
+        s->host_launches += 1;
+    }
+    st = invalidate_pending(s);
+    CK(cudaGetLastError());
+    return st;
+}
+
+emerge_status emerge_cuda_set_slip_boundaries(emerge_sim *s, const uint64_t *thickness, uint32_t n) {
+    if (!s || (!thickness && n)) return EMERGE_ERR_INVALID_ARG;
+    if (n > static_cast<uint32_t>(MAX_BOUNDARIES))
+        return static_cast<emerge_status>(s->fail(EMERGE_ERR_UNSUPPORTED, "at most 8 boundaries"));
+    for (uint32_t k = 0; k < n; ++k)
+        if (thickness[k] + 1 > s->cfg.grid_res)
+            return static_cast<emerge_status>(s->fail(EMERGE_ERR_INVALID_ARG, "boundary thickness exceeds grid"));
+    s->bounds.assign(thickness, thickness + n);
+    s->dcfg = make_dev_config(s->cfg, s->bounds);
+    s->graph_dirty = true;
+    return EMERGE_OK;
+}
+
+emerge_status emerge_cuda_add_body(emerge_sim *s, const emerge_spawn_region *spawn, uint32_t *tag_out) {
+    if (!s || !spawn) return EMERGE_ERR_INVALID_ARG;
+    std::vector<emerge_particle> ps;
+    uint32_t tag = s->next_tag;
+    emerge_status st = spawn_region(s, *spawn, tag, ps);
+    if (st != EMERGE_OK) return st;
+    s->next_tag += 1;
+    st = append_particles(s, ps.data(), ps.size(), 1);
+    if (st != EMERGE_OK) return st;
+    if (tag_out) *tag_out = tag;
+    return EMERGE_OK;
+}
+
+emerge_status emerge_cuda_init_with_spawn(emerge_sim *s, const emerge_spawn_region *spawn) {
+    if (!s || !spawn) return EMERGE_ERR_INVALID_ARG;
+    if (s->n != 0)
+        return static_cast<emerge_status>(s->fail(EMERGE_ERR_INVALID_ARG, "init_with_spawn needs an empty simulation"));
+    std::vector<emerge_particle> ps;
+    emerge_status st = spawn_region(s, *spawn, 0, ps);
+    if (st != EMERGE_OK) return st;
+    // Simulation::new does not run init_particle (lifecycle.rs:57-99): undo it.
+    for (auto &q : ps) {
+        q.plastic_volume_ratio = 1.0f;
+        q.hardening_scale = 1.0f;
+        q.friction_hardening = 0.0f;
+        q.log_volume_strain = 0.0f;
+    }
+    return append_particles(s, ps.data(), ps.size(), spawn->precompute_initial_volumes ? 2 : 0);
+}
+
+emerge_status emerge_cuda_add_particles(emerge_sim *s, const emerge_particle *particles, uint64_t n,
+                                        int estimate_volumes) {
+    if (!s || (!particles && n)) return EMERGE_ERR_INVALID_ARG;
+    return append_particles(s, particles, static_cast<size_t>(n), estimate_volumes ? 1 : 0);
+}
+
+emerge_status emerge_cuda_particle_count(const emerge_sim *s, uint64_t *n_out) {
+    if (!s || !n_out) return EMERGE_ERR_INVALID_ARG;
+    *n_out = s->n;
+    return EMERGE_OK;
+}
+
+emerge_status emerge_cuda_read_particles(emerge_sim *s, emerge_particle *out, uint64_t n) {
+    if (!s || (!out && n)) return EMERGE_ERR_INVALID_ARG;
+    if (n != s->n) return static_cast<emerge_status>(s->fail(EMERGE_ERR_INVALID_ARG, "n must equal the particle count"));
+    if (n == 0) return EMERGE_OK;
+    launch_gather_aos(s->P[s->cur], static_cast<int>(n), s->d_aos, s->stream);
+    s->host_launches += 1;
+    CK(cudaMemcpyAsync(out, s->d_aos, n * sizeof(emerge_particle), cudaMemcpyDeviceToHost, s->stream));
+    CK(cudaStreamSynchronize(s->stream));
+    return EMERGE_OK;
+}
+
+emerge_status emerge_cuda_write_particles(emerge_sim *s, const emerge_particle *in, uint64_t n) {
+    if (!s || (!in && n)) return EMERGE_ERR_INVALID_ARG;
+    if (n != s->n) return static_cast<emerge_status>(s->fail(EMERGE_ERR_INVALID_ARG, "n must equal the particle count"));
+    for (uint64_t k = 0; k < n; ++k) {
+        if (in[k].contact_group != 0)
+            return static_cast<emerge_status>(s->fail(
+                EMERGE_ERR_UNSUPPORTED, "contact_group != 0 (multi-field contact) is not on the device path"));
+        if (in[k].pinned) s->lf.pinned = 1;
+    }
+    if (n == 0) return EMERGE_OK;
+    CK(cudaMemcpyAsync(s->d_aos, in, n * sizeof(emerge_particle), cudaMemcpyHostToDevice, s->stream));
+    launch_scatter_aos(s->P[s->cur], static_cast<int>(n), s->d_aos, s->stream);
+    s->host_launches += 1;
+    CK(cudaGetLastError());
+    s->graph_dirty = true;  // load flags may have changed
+    return invalidate_pending(s);
+}
+
+emerge_status emerge_cuda_step(emerge_sim *s, uint32_t n_steps, emerge_step_timing *timing) {
+    if (!s) return EMERGE_ERR_INVALID_ARG;
+    if (s->n == 0) {
+        if (timing) std::memset(timing, 0, sizeof(*timing));
+        return EMERGE_OK;
+    }
+    for (uint32_t k = 0; k < n_steps; ++k) {
+        emerge_status st = maybe_sort(s);
+        if (st != EMERGE_OK) return st;
+        if (!s->pending_valid) {
+            st = prime(s);
+            if (st != EMERGE_OK) return st;
+        }
+        if (s->use_graph) {
+            if (s->graph_dirty || !s->graph_exec) {
+                st = build_graph(s);
+                if (st != EMERGE_OK) return st;
+            }
+            bool timed = timing && k + 1 == n_steps;
+            if (timed) CK(cudaEventRecord(s->ev[0], s->stream));
+            CK(cudaGraphLaunch(s->graph_exec, s->stream));
+            s->graph_launches += 1;
+            if (timed) {
+                CK(cudaEventRecord(s->ev[6], s->stream));
+                CK(cudaEventSynchronize(s->ev[6]));
+                float tot;
+                cudaEventElapsedTime(&tot, s->ev[0], s->ev[6]);
+                std::memset(&s->last_timing, 0, sizeof(s->last_timing));
+                s->last_timing.total_us = static_cast<uint64_t>(tot * 1000.0f);
+            }
+        } else {
+            st = run_host_loop_step(s, timing != nullptr);
+            if (st != EMERGE_OK) return st;
+        }
+        CK(cudaMemcpyAsync(s->h_state, s->d_state, sizeof(StepState), cudaMemcpyDeviceToHost, s->stream));
+        s->steps_since_sort += 1;
+    }
+    CK(cudaGetLastError());
+    if (timing) {
+        CK(cudaStreamSynchronize(s->stream));
+        *timing = s->last_timing;
+    }
+    return EMERGE_OK;
+}
+
+static emerge_status sync_state(emerge_sim *s) {
+    CK(cudaMemcpyAsync(s->h_state, s->d_state, sizeof(StepState), cudaMemcpyDeviceToHost, s->stream));
+    CK(cudaStreamSynchronize(s->stream));
+    return EMERGE_OK;
+}
+
+emerge_status emerge_cuda_last_substeps(emerge_sim *s, uint64_t *out) {
+    if (!s || !out) return EMERGE_ERR_INVALID_ARG;
+    emerge_status st = sync_state(s);
+    if (st != EMERGE_OK) return st;
+    *out = s->h_state->substeps;
+    return EMERGE_OK;
+}
+
+emerge_status emerge_cuda_effective_dt(emerge_sim *s, float *out) {
+    if (!s || !out) return EMERGE_ERR_INVALID_ARG;
+    emerge_status st = sync_state(s);
+    if (st != EMERGE_OK) return st;
+    *out = s->h_state->last_step_dt;
+    return EMERGE_OK;
+}
+
+emerge_status emerge_cuda_last_counters(emerge_sim *s, uint64_t *vel_clamp, uint64_t *jproj,
+                                        float *dropped) {
+    if (!s) return EMERGE_ERR_INVALID_ARG;
+    emerge_status st = sync_state(s);
+    if (st != EMERGE_OK) return st;
+    if (vel_clamp) *vel_clamp = s->h_state->vel_clamp;
+    if (jproj) *jproj = s->h_state->jproj;
+    if (dropped) *dropped = s->h_state->dropped;
+    return EMERGE_OK;
+}
+
+emerge_status emerge_cuda_synchronize(emerge_sim *s) {
+    if (!s) return EMERGE_ERR_INVALID_ARG;
+    CK(cudaStreamSynchronize(s->stream));
+    return EMERGE_OK;
+}
+
+emerge_status emerge_cuda_region_state(emerge_sim *s, float cx, float cy, float radius,
+                                       emerge_body_state *out) {
+    if (!s || !out) return EMERGE_ERR_INVALID_ARG;
+    std::vector<unsigned char> acc(region_acc_bytes(), 0);
+    // max_jp starts at the ordered encoding of 0.0f (BodyState::default)
+    CK(cudaMemsetAsync(s->region_buf.ptr, 0, region_acc_bytes(), s->stream));
+    uint32_t zero_ordered = 0x80000000u;
+    CK(cudaMemcpyAsync(static_cast<char *>(s->region_buf.ptr) + region_acc_bytes() - 8, &zero_ordered, 4,
+                       cudaMemcpyHostToDevice, s->stream));
+    launch_region_state(s->P[s->cur], static_cast<int>(s->n), cx, cy, radius * radius, s->region_buf.ptr,
+                        s->stream);
+    s->host_launches += 1;
+    CK(cudaMemcpyAsync(acc.data(), s->region_buf.ptr, acc.size(), cudaMemcpyDeviceToHost, s->stream));
+    CK(cudaStreamSynchronize(s->stream));
+    region_acc_finalize(acc.data(), out);
+    return EMERGE_OK;
+}
+
+emerge_status emerge_cuda_set_option(emerge_sim *s, int option, int64_t value) {
+    if (!s) return EMERGE_ERR_INVALID_ARG;
+    switch (option) {
+    case EMERGE_OPT_USE_GRAPH: s->use_graph = value != 0; return EMERGE_OK;
+    case EMERGE_OPT_SORT_INTERVAL:
+        if (value < 0) return static_cast<emerge_status>(s->fail(EMERGE_ERR_INVALID_ARG, "sort interval < 0"));
+        s->sort_interval = value;
+        return EMERGE_OK;
+    case EMERGE_OPT_P2G_WINDOW:
+        s->use_window = value != 0;
+        s->graph_dirty = true;
+        return EMERGE_OK;
+    default: return static_cast<emerge_status>(s->fail(EMERGE_ERR_INVALID_ARG, "unknown option"));
+    }
+}
+
+emerge_status emerge_cuda_sort_now(emerge_sim *s, int key_mode) {
+    if (!s || (key_mode != 0 && key_mode != 1)) return EMERGE_ERR_INVALID_ARG;
+    emerge_status st = sort_particles(s, key_mode);
+    if (st != EMERGE_OK) return st;
+    CK(cudaStreamSynchronize(s->stream));
+    return EMERGE_OK;
+}
+
+emerge_status emerge_cuda_sort_keys(const float *xy, uint64_t n, uint32_t grid_res, int key_mode,
+                                    uint32_t *keys_out, uint32_t *perm_out) {
+    if ((!xy && n) || (key_mode != 0 && key_mode != 1) || grid_res < 1 || n > 0x7fffffffull) {
+        g_global_error = "invalid argument";
+        return EMERGE_ERR_INVALID_ARG;
+    }
+    if (n == 0) return EMERGE_OK;
+    cudaStream_t stream;
+    if (cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking) != cudaSuccess) {
+        g_global_error = "stream create failed";
+        return EMERGE_ERR_CUDA;
+    }
+    float2 *d_xy = nullptr;
+    void *scratch = nullptr;
+    emerge_status rc = EMERGE_OK;
+    SortScratch sc;
+    int r = 0;
+    if (cudaMalloc(&d_xy, n * sizeof(float2)) != cudaSuccess ||
+        cudaMalloc(&scratch, sort_scratch_bytes(n)) != cudaSuccess) {
+        rc = EMERGE_ERR_OOM;
+        goto done;
+    }
+    sort_scratch_bind(sc, scratch, n);
+    cudaMemcpyAsync(d_xy, xy, n * sizeof(float2), cudaMemcpyHostToDevice, stream);
+    launch_sort_keys(d_xy, static_cast<int>(n), static_cast<int>(grid_res), key_mode, sc.keys[0], sc.vals[0],
+                     stream);
+    cudaMemcpyAsync(keys_out, sc.keys[0], n * sizeof(uint32_t), cudaMemcpyDeviceToHost, stream);
+    r = radix_sort_pairs(sc, static_cast<int>(n), sort_key_bits(static_cast<int>(grid_res), key_mode), stream);
+    cudaMemcpyAsync(perm_out, sc.vals[r], n * sizeof(uint32_t), cudaMemcpyDeviceToHost, stream);
+    if (cudaStreamSynchronize(stream) != cudaSuccess || cudaGetLastError() != cudaSuccess) rc = EMERGE_ERR_CUDA;
+done:
+    if (rc != EMERGE_OK) g_global_error = "sort_keys failed";
+    if (d_xy) cudaFree(d_xy);
+    if (scratch) cudaFree(scratch);
+    cudaStreamDestroy(stream);
+    return rc;
+}
+
+void *emerge_cuda_stream(emerge_sim *s) { return s ? static_cast<void *>(s->stream) : nullptr; }
+
+emerge_status emerge_cuda_kernel_launches(emerge_sim *s, uint64_t *out) {
+    if (!s || !out) return EMERGE_ERR_INVALID_ARG;
+    emerge_status st = sync_state(s);
+    if (st != EMERGE_OK) return st;
+    *out = s->host_launches + s->graph_launches + s->h_state->graph_kernels;
+    return EMERGE_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,924 @@
+// step_kernels.cu -- the MLS-MPM substep on sm_100a.
+//
+// One substep k of the reference (spacetime/solver/step.rs:62-317) runs as:
+//   k_substep_begin   1 thread: dt(k) from the CFL reduction (step.rs:434-479),
+//                     loop bookkeeping, CUDA-graph loop condition.
+//   k_grid_update     per active 8x8 tile: momentum = A + dt*S, normalise, gravity,
+//                     slip walls, speed clamp (grid/mod.rs:264-291, step.rs:150-165),
+//                     then zero the accumulators for the next scatter.
+//   k_particle        per particle, fused: projection recompute, G2P gather
+//                     (transfer/g2p.rs:151-328), constitutive update (:333-340),
+//                     CFL contribution for substep k+1 (step.rs:447-466), projection
+//                     for k+1 (step.rs:347-429), P2G scatter for k+1
+//                     (transfer/p2g.rs:24-72) through a shared-memory window.
+//   k_density         only when a material needs it (step.rs:80-87): density gather
+//                     (solver/density.rs:41-72) + the fluid stress scatter, which
+//                     depends on that density (fluid.rs:157-162, 193-195).
+// Particle state is read once and written once per substep by k_particle.
+// The pass before the first substep of a step sequence (k_particle in prime
+// mode) only projects and scatters.
+#include <cfloat>
+#include <cstdio>
+
+#include "device_state.cuh"
+#include "kernels.h"
+
+namespace emerge {
+
+// ---------------------------------------------------------------- reductions
+__device__ __forceinline__ void red_add_v4(float4 *p, float a, float b, float c, float d) {
+    asm volatile("red.global.add.v4.f32 [%0], {%1, %2, %3, %4};" ::"l"(p), "f"(a), "f"(b), "f"(c),
+                 "f"(d)
+                 : "memory");
+}
+__device__ __forceinline__ void red_add_v2(float2 *p, float a, float b) {
+    asm volatile("red.global.add.v2.f32 [%0], {%1, %2};" ::"l"(p), "f"(a), "f"(b) : "memory");
+}
+
+__device__ __forceinline__ float warp_max(float v) {
+    for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
+__device__ __forceinline__ float warp_min(float v) {
+    for (int o = 16; o > 0; o >>= 1) v = fminf(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
+__device__ __forceinline__ int warp_imin(int v) {
+    for (int o = 16; o > 0; o >>= 1) v = min(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
+__device__ __forceinline__ int warp_imax(int v) {
+    for (int o = 16; o > 0; o >>= 1) v = max(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
+
+__device__ __forceinline__ void count_warp(unsigned long long *ctr, bool pred) {
+    unsigned ballot = __ballot_sync(0xffffffffu, pred);
+    if ((threadIdx.x & 31) == 0 && ballot) atomicAdd(ctr, (unsigned long long)__popc(ballot));
+}
+
+// ---------------------------------------------------------------- particle I/O
+struct LoadFlags {
+    int temperature;  // some material reads particle temperature
+    int activation;   // some material has a non-zero activation scale
+    int pinned;       // some particle is pinned
+};
+
+__device__ __forceinline__ PState load_state(const DevParticles &P, int i, const LoadFlags &lf) {
+    PState p;
+    p.x = P.x[i];
+    p.v = P.v[i];
+    p.c = m_from4(P.c[i]);
+    p.f = m_from4(P.f[i]);
+    p.mass = P.mass[i];
+    p.v0 = P.v0[i];
+    p.vol = P.vol[i];
+    p.rho = P.rho[i];
+    p.mat = P.mat[i];
+    p.jp = P.jp[i];
+    p.h = P.h[i];
+    p.q = P.q[i];
+    p.lvs = P.lvs[i];
+    p.temperature = lf.temperature ? P.temperature[i] : 0.0f;
+    p.activation = lf.activation ? P.activation[i] : 0.0f;
+    p.act_dir = lf.activation ? P.act_dir[i] : v2(0.0f, 0.0f);
+    p.pinned = lf.pinned ? P.pinned[i] : 0u;
+    return p;
+}
+
+__device__ __forceinline__ bool neq(float a, float b) { return __float_as_uint(a) != __float_as_uint(b); }
+__device__ __forceinline__ bool neq2(float2 a, float2 b) { return neq(a.x, b.x) || neq(a.y, b.y); }
+__device__ __forceinline__ bool neqm(M2 a, M2 b) { return neq2(a.xa, b.xa) || neq2(a.ya, b.ya); }
+
+// Writes back the fields that differ (bitwise) from what was loaded.
+__device__ __forceinline__ void store_changed(const DevParticles &P, int i, const PState &o,
+                                              const PState &p) {
+    if (neq2(p.x, o.x)) P.x[i] = p.x;
+    if (neq2(p.v, o.v)) P.v[i] = p.v;
+    if (neqm(p.c, o.c)) P.c[i] = m_to4(p.c);
+    if (neqm(p.f, o.f)) P.f[i] = m_to4(p.f);
+    if (neq(p.mass, o.mass)) P.mass[i] = p.mass;
+    if (neq(p.v0, o.v0)) P.v0[i] = p.v0;
+    if (neq(p.vol, o.vol)) P.vol[i] = p.vol;
+    if (neq(p.rho, o.rho)) P.rho[i] = p.rho;
+    if (neq(p.jp, o.jp)) P.jp[i] = p.jp;
+    if (neq(p.h, o.h)) P.h[i] = p.h;
+    if (neq(p.q, o.q)) P.q[i] = p.q;
+    if (neq(p.lvs, o.lvs)) P.lvs[i] = p.lvs;
+}
+
+// G2P phase 1 for one particle (transfer/g2p.rs:217-326 with ASFLIP, contact and
+// mixture gated off).  Returns 1 if the speed clamp fired.
+__device__ __forceinline__ int g2p_particle(const GridView &g, const DevConfig &cfg, float dt,
+                                            PState &p) {
+    QW w = quadratic_weights(p.x);
+    float2 new_v = v2(0.0f, 0.0f);
+    M2 b = mzero();
+#pragma unroll
+    for (int gx = 0; gx < 3; ++gx) {
+#pragma unroll
+        for (int gy = 0; gy < 3; ++gy) {
+            float weight = w.wx[gx] * w.wy[gy];
+            int cx = w.bx + gx - 1, cy = w.by + gy - 1;
+            float2 dist = vadd(vsub(v2(static_cast<float>(cx), static_cast<float>(cy)), p.x),
+                               splat(0.5f));
+            float2 node_v = in_domain(cx, cy, g.res) ? g.grid_v[cell_index(cx, cy, g.tpd)]
+                                                     : v2(0.0f, 0.0f);
+            float2 wv = vmuls(node_v, weight);
+            M2 term = m2(vmuls(wv, dist.x), vmuls(wv, dist.y));
+            b = madd(b, term);
+            new_v = vadd(new_v, wv);
+        }
+    }
+    if (p.pinned != 0) {
+        p.v = v2(0.0f, 0.0f);
+        p.c = mzero();
+        return 0;
+    }
+    const float vel_limit = cfg.cell / dt;
+    int clamped = 0;
+    float spd = vlen(new_v);
+    if (spd > vel_limit) {
+        float scale = vel_limit / spd;
+        new_v = vmuls(new_v, scale);
+        clamped = 1;
+    }
+    float2 new_pos = vadd(p.x, vmuls(new_v, dt));
+    for (int k = 0; k < cfg.n_bound; ++k) new_pos = clamp_position(cfg.bound_t[k], new_pos, g.res);
+    p.v = new_v;
+    p.c = mscale(mscale(b, KERNEL_D_INVERSE), cfg.apic_blend);
+    p.x = new_pos;
+    return clamped;
+}
+
+// ---------------------------------------------------------------- scatter engine
+// A CTA scatters the 3x3 stencils of up to PPT*THREADS particles.  When the union
+// of their stencils fits in WINDOW_CELLS cells, contributions accumulate in
+// shared memory (red.shared) and each touched cell is flushed once with a vector
+// red.global; otherwise every contribution goes straight to global memory.
+constexpr int THREADS = 256;
+constexpr int PPT = 2;
+constexpr int WINDOW_CELLS = 1024;
+
+struct Payload {
+    float2 x;
+    float m;      // mass channel weight (0 if not scattered)
+    float2 v;
+    M2 c;
+    M2 tau;
+    float s;      // -4 * stress_volume (dt-free stress coefficient); 0 = no stress channel
+    int bx, by;
+    bool valid;
+    bool do_ma;   // scatter mass + affine momentum
+    bool do_s;    // scatter stress impulse
+};
+
+struct ScatterShared {
+    float m[WINDOW_CELLS], ax[WINDOW_CELLS], ay[WINDOW_CELLS], sx[WINDOW_CELLS], sy[WINDOW_CELLS];
+    int red_i[4][THREADS / 32];
+    int box[4];
+    int use_window;
+};
+
+__device__ __forceinline__ void cell_contrib(const Payload &pl, int gx, int gy, const QW &w,
+                                             float &mc, float2 &a, float2 &s, int &cx, int &cy) {
+    float weight = w.wx[gx] * w.wy[gy];
+    cx = w.bx + gx - 1;
+    cy = w.by + gy - 1;
+    float2 cell_dist = vadd(vsub(v2(static_cast<float>(cx), static_cast<float>(cy)), pl.x),
+                            splat(0.5f));
+    mc = weight * pl.m;
+    a = svmul(weight, svmul(pl.m, vadd(pl.v, mv(pl.c, cell_dist))));
+    s = svmul(weight, svmul(pl.s, mv(pl.tau, cell_dist)));
+}
+
+__device__ __forceinline__ void mark_tile(const GridView &g, int cx, int cy) {
+    int t = (cx >> 3) * g.tpd + (cy >> 3);
+    if (g.tile_flag[t] == 0) g.tile_flag[t] = 1;
+}
+
+__device__ void scatter_block(ScatterShared &sh, const GridView &g, Payload (&pl)[PPT],
+                              int use_window, unsigned long long *fallback_ctr,
+                              unsigned long long *blocks_ctr) {
+    const int tid = threadIdx.x;
+    // 1. bounding box of base cells
+    int mnx = INT_MAX, mny = INT_MAX, mxx = INT_MIN, mxy = INT_MIN;
+    bool any = false;
+#pragma unroll
+    for (int k = 0; k < PPT; ++k) {
+        if (pl[k].valid && (pl[k].do_ma || pl[k].do_s)) {
+            any = true;
+            mnx = min(mnx, pl[k].bx);
+            mny = min(mny, pl[k].by);
+            mxx = max(mxx, pl[k].bx);
+            mxy = max(mxy, pl[k].by);
+        }
+    }
+    mnx = warp_imin(mnx);
+    mny = warp_imin(mny);
+    mxx = warp_imax(mxx);
+    mxy = warp_imax(mxy);
+    int warp = tid >> 5, lane = tid & 31;
+    if (lane == 0) {
+        sh.red_i[0][warp] = mnx;
+        sh.red_i[1][warp] = mny;
+        sh.red_i[2][warp] = mxx;
+        sh.red_i[3][warp] = mxy;
+    }
+    int any_block = __syncthreads_or(any ? 1 : 0);
+    if (!any_block) return;
+    if (tid == 0) {
+        int a = INT_MAX, b = INT_MAX, c = INT_MIN, d = INT_MIN;
+        for (int w = 0; w < THREADS / 32; ++w) {
+            a = min(a, sh.red_i[0][w]);
+            b = min(b, sh.red_i[1][w]);
+            c = max(c, sh.red_i[2][w]);
+            d = max(d, sh.red_i[3][w]);
+        }
+        // window: cells [a-1, c+1] x [b-1, d+1]
+        long long ex = (long long)c - a + 3, ey = (long long)d - b + 3;
+        int fits = use_window && ex > 0 && ey > 0 && ex * ey <= WINDOW_CELLS;
+        sh.box[0] = a - 1;
+        sh.box[1] = b - 1;
+        sh.box[2] = static_cast<int>(fits ? ex : 0);
+        sh.box[3] = static_cast<int>(fits ? ey : 0);
+        sh.use_window = fits;
+        atomicAdd(blocks_ctr, 1ull);
+        if (!fits) atomicAdd(fallback_ctr, 1ull);
+    }
+    __syncthreads();
+    const int ox = sh.box[0], oy = sh.box[1], ex = sh.box[2], ey = sh.box[3];
+    if (sh.use_window) {
+        const int ncell = ex * ey;
+        for (int k = tid; k < ncell; k += THREADS) {
+            sh.m[k] = 0.0f;
+            sh.ax[k] = 0.0f;
+            sh.ay[k] = 0.0f;
+            sh.sx[k] = 0.0f;
+            sh.sy[k] = 0.0f;
+        }
+        __syncthreads();
+#pragma unroll
+        for (int k = 0; k < PPT; ++k) {
+            const Payload &p = pl[k];
+            if (!p.valid || !(p.do_ma || p.do_s)) continue;
+            QW w = quadratic_weights(p.x);
+#pragma unroll
+            for (int gx = 0; gx < 3; ++gx)
+#pragma unroll
+                for (int gy = 0; gy < 3; ++gy) {
+                    float mc;
+                    float2 a, s;
+                    int cx, cy;
+                    cell_contrib(p, gx, gy, w, mc, a, s, cx, cy);
+                    int li = (cx - ox) * ey + (cy - oy);
+                    if (p.do_ma) {
+                        atomicAdd(&sh.m[li], mc);
+                        atomicAdd(&sh.ax[li], a.x);
+                        atomicAdd(&sh.ay[li], a.y);
+                    }
+                    if (p.do_s) {
+                        atomicAdd(&sh.sx[li], s.x);
+                        atomicAdd(&sh.sy[li], s.y);
+                    }
+                }
+        }
+        __syncthreads();
+        for (int k = tid; k < ncell; k += THREADS) {
+            float m = sh.m[k], ax = sh.ax[k], ay = sh.ay[k], sx = sh.sx[k], sy = sh.sy[k];
+            int cx = ox + k / ey, cy = oy + k % ey;
+            if (!in_domain(cx, cy, g.res)) continue;
+            bool nz_a = (m != 0.0f) || (ax != 0.0f) || (ay != 0.0f);
+            bool nz_s = (sx != 0.0f) || (sy != 0.0f);
+            if (!nz_a && !nz_s) continue;
+            int ci = cell_index(cx, cy, g.tpd);
+            if (nz_a) red_add_v4(&g.acc_a[ci], m, ax, ay, 0.0f);
+            if (nz_s) red_add_v2(&g.acc_s[ci], sx, sy);
+            mark_tile(g, cx, cy);
+        }
+    } else {
+#pragma unroll
+        for (int k = 0; k < PPT; ++k) {
+            const Payload &p = pl[k];
+            if (!p.valid || !(p.do_ma || p.do_s)) continue;
+            QW w = quadratic_weights(p.x);
+#pragma unroll
+            for (int gx = 0; gx < 3; ++gx)
+#pragma unroll
+                for (int gy = 0; gy < 3; ++gy) {
+                    float mc;
+                    float2 a, s;
+                    int cx, cy;
+                    cell_contrib(p, gx, gy, w, mc, a, s, cx, cy);
+                    if (!in_domain(cx, cy, g.res)) continue;
+                    int ci = cell_index(cx, cy, g.tpd);
+                    if (p.do_ma) red_add_v4(&g.acc_a[ci], mc, a.x, a.y, 0.0f);
+                    if (p.do_s) red_add_v2(&g.acc_s[ci], s.x, s.y);
+                    mark_tile(g, cx, cy);
+                }
+        }
+    }
+}
+
+// ---------------------------------------------------------------- k_particle
+struct ParticleKernelArgs {
+    DevParticles P;
+    int n;
+    const MatP *mats;
+    int n_mats;
+    DevConfig cfg;
+    StepState *st;
+    GridView g;
+    LoadFlags lf;
+    int mode_g2p;       // 0: prime pass (no G2P), 1: G2P(k) + P2G(k+1)
+    int density_mode;   // fluid stress deferred to k_density; G2P reads rho_dp
+    int use_window;
+};
+
+__global__ void __launch_bounds__(THREADS) k_particle(ParticleKernelArgs a) {
+    __shared__ ScatterShared sh;
+    __shared__ MatP s_mats[MAX_MATERIALS];
+    __shared__ float s_red[2][THREADS / 32];
+    for (int k = threadIdx.x; k < a.n_mats; k += THREADS) s_mats[k] = a.mats[k];
+    __syncthreads();
+
+    const DevConfig &cfg = a.cfg;
+    StepState *st = a.st;
+    const int acc_slot = st->acc_slot;
+    const float dt = st->sub_dt;
+    const int base = blockIdx.x * (THREADS * PPT);
+
+    Payload pl[PPT];
+    float max_speed = 0.0f;
+    float min_mdt = INFINITY;
+    int clamped_any = 0, projected_any = 0;
+
+#pragma unroll
+    for (int k = 0; k < PPT; ++k) {
+        const int i = base + k * THREADS + threadIdx.x;
+        pl[k].valid = i < a.n;
+        pl[k].do_ma = false;
+        pl[k].do_s = false;
+        int clamped = 0, projected = 0;
+        if (pl[k].valid) {
+            PState p = load_state(a.P, i, a.lf);
+            const MatP &m = s_mats[p.mat < static_cast<uint32_t>(a.n_mats) ? p.mat : 0u];
+            if (a.mode_g2p) {
+                const PState o = p;
+                if (cfg.project) project_state(cfg, p);  // recompute S'(k); counted earlier
+                if (a.density_mode) {
+                    float d = a.P.rho_dp[i];
+                    if (d > F32_EPS) {
+                        p.rho = d;
+                        p.vol = p.mass / d;
+                    }
+                }
+                clamped = g2p_particle(a.g, cfg, dt, p);
+                update_particle(m, p, dt);
+                store_changed(a.P, i, o, p);
+            }
+            // CFL contribution for the next substep (step.rs:447-466)
+            float sp = vlen(p.v);
+            if (cfg.affine_cfl) sp += affine_cfl(p.c, cfg.cell);
+            max_speed = fmaxf(max_speed, sp);
+            float mdt = timestep_bound(m, p.rho, p.h, cfg.cell, cfg.mat_cfl, cfg.visc_cfl);
+            if (isfinite(mdt) && mdt > 0.0f) min_mdt = fminf(min_mdt, mdt);
+            // projection of the next substep (step.rs:67-73)
+            if (cfg.project) projected = project_state(cfg, p) ? 1 : 0;
+            // P2G payload (transfer/p2g.rs:192-213)
+            pl[k].x = p.x;
+            pl[k].m = p.mass;
+            pl[k].v = p.v;
+            pl[k].c = p.c;
+            pl[k].do_ma = true;
+            bool fluid = m.model == M_FLUID;
+            if (!(a.density_mode && fluid)) {
+                pl[k].tau = combined_kirchhoff_stress(m, p);
+                pl[k].s = -stress_volume(m, p) * KERNEL_D_INVERSE;
+                pl[k].do_s = true;
+            } else {
+                pl[k].tau = mzero();
+                pl[k].s = 0.0f;
+            }
+            QW w = quadratic_weights(p.x);
+            pl[k].bx = w.bx;
+            pl[k].by = w.by;
+        }
+        clamped_any |= clamped;
+        projected_any |= projected;
+        count_warp(&st->vel_clamp, clamped != 0);
+        count_warp(&st->jproj_pending[acc_slot], projected != 0);
+    }
+    (void)clamped_any;
+    (void)projected_any;
+
+    // CFL block reduction -> one atomic per block
+    max_speed = warp_max(max_speed);
+    min_mdt = warp_min(min_mdt);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (lane == 0) {
+        s_red[0][warp] = max_speed;
+        s_red[1][warp] = min_mdt;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        float ms = 0.0f, md = INFINITY;
+        for (int w = 0; w < THREADS / 32; ++w) {
+            ms = fmaxf(ms, s_red[0][w]);
+            md = fminf(md, s_red[1][w]);
+        }
+        atomicMax(&st->max_speed_bits[acc_slot], __float_as_uint(ms));
+        atomicMin(&st->min_mdt_bits[acc_slot], __float_as_uint(md));
+    }
+
+    scatter_block(sh, a.g, pl, a.use_window, &st->window_fallback, &st->window_blocks);
+}
+
+// ---------------------------------------------------------------- k_density
+struct DensityKernelArgs {
+    DevParticles P;
+    int n;
+    const MatP *mats;
+    int n_mats;
+    DevConfig cfg;
+    StepState *st;
+    GridView g;
+    LoadFlags lf;
+    int use_window;
+};
+
+// estimate_particle_volumes gather (solver/density.rs:50-71) at the projected
+// positions, stored as rho_dp, plus the stress scatter of fluid particles.
+__global__ void __launch_bounds__(THREADS) k_density(DensityKernelArgs a) {
+    __shared__ ScatterShared sh;
+    __shared__ MatP s_mats[MAX_MATERIALS];
+    for (int k = threadIdx.x; k < a.n_mats; k += THREADS) s_mats[k] = a.mats[k];
+    __syncthreads();
+    const DevConfig &cfg = a.cfg;
+    const int base = blockIdx.x * (THREADS * PPT);
+    Payload pl[PPT];
+#pragma unroll
+    for (int k = 0; k < PPT; ++k) {
+        const int i = base + k * THREADS + threadIdx.x;
+        pl[k].valid = i < a.n;
+        pl[k].do_ma = false;
+        pl[k].do_s = false;
+        if (!pl[k].valid) continue;
+        PState p = load_state(a.P, i, a.lf);
+        if (cfg.project) project_state(cfg, p);
+        QW w = quadratic_weights(p.x);
+        float density = 0.0f;
+#pragma unroll
+        for (int gx = 0; gx < 3; ++gx)
+#pragma unroll
+            for (int gy = 0; gy < 3; ++gy) {
+                float weight = w.wx[gx] * w.wy[gy];
+                int cx = w.bx + gx - 1, cy = w.by + gy - 1;
+                float mc = in_domain(cx, cy, a.g.res) ? a.g.acc_a[cell_index(cx, cy, a.g.tpd)].x
+                                                      : 0.0f;
+                density += mc * weight;
+            }
+        a.P.rho_dp[i] = density;
+        const MatP &m = s_mats[p.mat < static_cast<uint32_t>(a.n_mats) ? p.mat : 0u];
+        if (m.model == M_FLUID) {
+            if (density > F32_EPS) {
+                p.rho = density;
+                p.vol = p.mass / density;
+            }
+            pl[k].x = p.x;
+            pl[k].m = 0.0f;
+            pl[k].v = v2(0.0f, 0.0f);
+            pl[k].c = mzero();
+            pl[k].tau = combined_kirchhoff_stress(m, p);
+            pl[k].s = -stress_volume(m, p) * KERNEL_D_INVERSE;
+            pl[k].do_s = true;
+            pl[k].bx = w.bx;
+            pl[k].by = w.by;
+        }
+    }
+    scatter_block(sh, a.g, pl, a.use_window, &a.st->window_fallback, &a.st->window_blocks);
+}
+
+// ---------------------------------------------------------------- grid update
+struct GridKernelArgs {
+    GridView g;
+    DevConfig cfg;
+    StepState *st;
+    int n_tiles;
+};
+
+// Grid::update_velocities (grid/mod.rs:264-291), boundaries (step.rs:150-152,
+// 334-344; forces/boundary/mod.rs:78-101), speed clamp (step.rs:155-165).
+__global__ void __launch_bounds__(256) k_grid_update(GridKernelArgs a) {
+    const int tile = blockIdx.x * 4 + (threadIdx.x >> 6);
+    const int local = threadIdx.x & 63;
+    uint8_t flag = 0;
+    if (tile < a.n_tiles) flag = a.g.tile_flag[tile];
+    __syncthreads();
+    if (tile >= a.n_tiles || !flag) return;
+    if (local == 0) a.g.tile_flag[tile] = 0;
+    const int ci = tile * TILE_CELLS + local;
+    const int x = (tile / a.g.tpd) * TILE + (local >> 3);
+    const int y = (tile % a.g.tpd) * TILE + (local & 7);
+    const float dt = a.st->sub_dt;
+    float4 acc = a.g.acc_a[ci];
+    float2 s = a.g.acc_s[ci];
+    float m = acc.x;
+    float2 mom = v2(acc.y + dt * s.x, acc.z + dt * s.y);
+    if (m > 0.0f) {
+        mom = vdivs(mom, m);
+        mom = vadd(mom, vmuls(a.cfg.gravity, dt));
+        for (int k = 0; k < a.cfg.n_bound; ++k) slip_velocity(a.cfg.bound_t[k], x, y, a.g.res, mom);
+        float vel_limit = a.cfg.cell / dt;
+        float spd = vlen(mom);
+        if (spd > vel_limit) mom = vmuls(mom, vel_limit / spd);
+    }
+    a.g.grid_v[ci] = mom;
+    a.g.acc_a[ci] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    a.g.acc_s[ci] = v2(0.0f, 0.0f);
+}
+
+// ---------------------------------------------------------------- controller
+// Step start (step.rs:29-33).
+__global__ void k_step_begin(StepState *st, DevConfig cfg) {
+    st->remaining = cfg.dt;
+    st->substeps = 0;
+    st->vel_clamp = 0;
+    st->jproj = 0;
+    st->dropped = fmaxf(cfg.dt, 0.0f);
+    st->cont = (cfg.dt > F32_EPS && cfg.max_substeps > 0) ? 1u : 0u;
+    st->total_steps += 1;
+}
+
+// Substep start: choose_substep_dt (step.rs:434-468) from the reduction of slot
+// (parity), loop bookkeeping (step.rs:46-48), and the loop condition
+// (step.rs:34) for the graph's while node.
+__global__ void k_substep_begin(StepState *st, DevConfig cfg, int use_cond,
+                                cudaGraphConditionalHandle handle, int kernels_per_substep) {
+    StepState &s = *st;
+    const uint32_t k = s.parity;
+    const float rem = s.remaining;
+    float dt;
+    if (!cfg.adaptive) {
+        dt = fminf(rem, cfg.dt);
+    } else {
+        float max_speed = __uint_as_float(s.max_speed_bits[k]);
+        float min_mdt = __uint_as_float(s.min_mdt_bits[k]);
+        dt = cfl_bound(cfg, max_speed, fminf(rem, min_mdt), rem);
+    }
+    s.sub_dt = dt;
+    s.last_step_dt = dt;
+    s.jproj += s.jproj_pending[k];
+    const uint32_t k1 = k ^ 1u;
+    s.max_speed_bits[k1] = 0u;
+    s.min_mdt_bits[k1] = __float_as_uint(INFINITY);
+    s.jproj_pending[k1] = 0ull;
+    s.acc_slot = k1;
+    s.parity = k1;
+    const float rem_after = rem - dt;
+    s.remaining = rem_after;
+    s.substeps += 1;
+    s.total_substeps += 1;
+    s.dropped = fmaxf(rem_after, 0.0f);
+    s.cont = (rem_after > F32_EPS && s.substeps < static_cast<uint32_t>(cfg.max_substeps)) ? 1u : 0u;
+    if (use_cond) {
+        s.graph_kernels += static_cast<unsigned long long>(kernels_per_substep);
+        cudaGraphSetConditional(handle, s.cont);
+    }
+}
+
+// Before a prime pass: the next k_substep_begin reads slot (parity).
+__global__ void k_prime_setup(StepState *st) {
+    const uint32_t k = st->parity;
+    st->max_speed_bits[k] = 0u;
+    st->min_mdt_bits[k] = __float_as_uint(INFINITY);
+    st->jproj_pending[k] = 0ull;
+    st->acc_slot = k;
+}
+
+// ---------------------------------------------------------------- queries
+struct RegionAcc {
+    unsigned long long count;
+    double sx, sy, speed, jp, det, rho;
+    unsigned int max_jp_bits;  // ordered-int encoding of a float
+    unsigned int pad;
+};
+
+__device__ __forceinline__ unsigned int float_to_ordered(float f) {
+    unsigned int u = __float_as_uint(f);
+    return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+}
+
+// region_state (queries.rs:125-141) as a device reduction (f64 partial sums).
+__global__ void k_region_state(DevParticles P, int n, float cx, float cy, float r2,
+                               RegionAcc *out) {
+    __shared__ double sh[6][256 / 32];
+    __shared__ unsigned long long shc[256 / 32];
+    __shared__ unsigned int shm[256 / 32];
+    double sx = 0, sy = 0, sp = 0, sjp = 0, sdet = 0, srho = 0;
+    unsigned long long cnt = 0;
+    unsigned int mjp = float_to_ordered(0.0f);  // BodyState::default max_volume_ratio = 0
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        float2 x = P.x[i];
+        float2 d = vsub(x, v2(cx, cy));
+        if (vlen2(d) <= r2) {
+            cnt += 1;
+            sx += x.x;
+            sy += x.y;
+            sp += vlen(P.v[i]);
+            float jp = P.jp[i];
+            sjp += jp;
+            unsigned int o = float_to_ordered(jp);
+            if (!isnan(jp) && o > mjp) mjp = o;
+            sdet += mdet(m_from4(P.f[i]));
+            srho += P.rho[i];
+        }
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        sx += __shfl_xor_sync(0xffffffffu, sx, o);
+        sy += __shfl_xor_sync(0xffffffffu, sy, o);
+        sp += __shfl_xor_sync(0xffffffffu, sp, o);
+        sjp += __shfl_xor_sync(0xffffffffu, sjp, o);
+        sdet += __shfl_xor_sync(0xffffffffu, sdet, o);
+        srho += __shfl_xor_sync(0xffffffffu, srho, o);
+        cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
+        mjp = max(mjp, __shfl_xor_sync(0xffffffffu, mjp, o));
+    }
+    int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+    if (l == 0) {
+        sh[0][w] = sx; sh[1][w] = sy; sh[2][w] = sp; sh[3][w] = sjp; sh[4][w] = sdet; sh[5][w] = srho;
+        shc[w] = cnt;
+        shm[w] = mjp;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int k = 1; k < 256 / 32; ++k) {
+            sh[0][0] += sh[0][k]; sh[1][0] += sh[1][k]; sh[2][0] += sh[2][k];
+            sh[3][0] += sh[3][k]; sh[4][0] += sh[4][k]; sh[5][0] += sh[5][k];
+            shc[0] += shc[k];
+            shm[0] = max(shm[0], shm[k]);
+        }
+        if (shc[0]) {
+            atomicAdd(&out->count, shc[0]);
+            atomicAdd(&out->sx, sh[0][0]);
+            atomicAdd(&out->sy, sh[1][0]);
+            atomicAdd(&out->speed, sh[2][0]);
+            atomicAdd(&out->jp, sh[3][0]);
+            atomicAdd(&out->det, sh[4][0]);
+            atomicAdd(&out->rho, sh[5][0]);
+            atomicMax(&out->max_jp_bits, shm[0]);
+        }
+    }
+}
+
+// ---------------------------------------------------------------- particle I/O
+__global__ void k_gather_aos(DevParticles P, int n, emerge_particle *out) {
+    int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= n) return;
+    emerge_particle q;
+    float2 x = P.x[s], v = P.v[s];
+    float4 c = P.c[s], f = P.f[s];
+    q.x[0] = x.x; q.x[1] = x.y;
+    q.v[0] = v.x; q.v[1] = v.y;
+    q.c[0] = c.x; q.c[1] = c.y; q.c[2] = c.z; q.c[3] = c.w;
+    q.f[0] = f.x; q.f[1] = f.y; q.f[2] = f.z; q.f[3] = f.w;
+    q.mass = P.mass[s];
+    q.initial_volume = P.v0[s];
+    q.volume = P.vol[s];
+    q.density = P.rho[s];
+    q.material_id = P.mat[s];
+    q.plastic_volume_ratio = P.jp[s];
+    q.hardening_scale = P.h[s];
+    q.friction_hardening = P.q[s];
+    q.log_volume_strain = P.lvs[s];
+    q.temperature = P.temperature[s];
+    q.user_tag = P.user_tag[s];
+    q.activation = P.activation[s];
+    float2 ad = P.act_dir[s];
+    q.activation_dir[0] = ad.x; q.activation_dir[1] = ad.y;
+    q.muscle_group_id = P.muscle[s];
+    q.contact_group = P.contact[s];
+    q.sleeping = P.sleeping[s];
+    q.pinned = P.pinned[s];
+    q.scalar_field = P.scalar[s];
+    q.pad_ = 0;
+    out[P.slot_to_index[s]] = q;
+}
+
+__device__ __forceinline__ void put_slot(const DevParticles &P, int s, const emerge_particle &q) {
+    P.x[s] = v2(q.x[0], q.x[1]);
+    P.v[s] = v2(q.v[0], q.v[1]);
+    P.c[s] = make_float4(q.c[0], q.c[1], q.c[2], q.c[3]);
+    P.f[s] = make_float4(q.f[0], q.f[1], q.f[2], q.f[3]);
+    P.mass[s] = q.mass;
+    P.v0[s] = q.initial_volume;
+    P.vol[s] = q.volume;
+    P.rho[s] = q.density;
+    P.mat[s] = q.material_id;
+    P.jp[s] = q.plastic_volume_ratio;
+    P.h[s] = q.hardening_scale;
+    P.q[s] = q.friction_hardening;
+    P.lvs[s] = q.log_volume_strain;
+    P.temperature[s] = q.temperature;
+    P.user_tag[s] = q.user_tag;
+    P.activation[s] = q.activation;
+    P.act_dir[s] = v2(q.activation_dir[0], q.activation_dir[1]);
+    P.muscle[s] = q.muscle_group_id;
+    P.contact[s] = q.contact_group;
+    P.sleeping[s] = q.sleeping;
+    P.pinned[s] = q.pinned;
+    P.scalar[s] = q.scalar_field;
+    P.rho_dp[s] = 0.0f;
+}
+
+__global__ void k_scatter_aos(DevParticles P, int n, const emerge_particle *in) {
+    int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= n) return;
+    put_slot(P, s, in[P.slot_to_index[s]]);
+}
+
+__global__ void k_append_aos(DevParticles P, int n_old, int n_new, const emerge_particle *in) {
+    int k = blockIdx.x * blockDim.x + threadIdx.x;
+    int s = n_old + k;
+    if (s >= n_new) return;
+    put_slot(P, s, in[k]);
+    P.slot_to_index[s] = static_cast<uint32_t>(s);
+}
+
+// init_particle for every particle (reinit_all_particle_state, lifecycle.rs:328-334)
+__global__ void k_reinit(DevParticles P, int n, const MatP *mats, int n_mats) {
+    int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= n) return;
+    uint32_t id = P.mat[s];
+    const MatP &m = mats[id < static_cast<uint32_t>(n_mats) ? id : 0u];
+    emerge_particle q;
+    q.friction_hardening = P.q[s];
+    q.plastic_volume_ratio = P.jp[s];
+    q.hardening_scale = P.h[s];
+    q.log_volume_strain = P.lvs[s];
+    init_particle(m, q);
+    P.q[s] = q.friction_hardening;
+    P.jp[s] = q.plastic_volume_ratio;
+    P.h[s] = q.hardening_scale;
+    P.lvs[s] = q.log_volume_strain;
+}
+
+// Mass scatter of estimate_particle_volumes(_local) (density.rs:47-48, 105-120).
+__global__ void k_mass_scatter(DevParticles P, int n, GridView g, int filter, float lox, float loy,
+                               float hix, float hiy) {
+    int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= n) return;
+    float2 x = P.x[s];
+    if (filter && (x.x < lox || x.y < loy || x.x > hix || x.y > hiy)) return;
+    float mass = P.mass[s];
+    QW w = quadratic_weights(x);
+    for (int gx = 0; gx < 3; ++gx)
+        for (int gy = 0; gy < 3; ++gy) {
+            float weight = w.wx[gx] * w.wy[gy];
+            int cx = w.bx + gx - 1, cy = w.by + gy - 1;
+            if (!in_domain(cx, cy, g.res)) continue;
+            atomicAdd(&g.acc_a[cell_index(cx, cy, g.tpd)].x, weight * mass);
+        }
+}
+
+// Density gather of estimate_particle_volumes(_local) (density.rs:50-71, 122-143)
+// for slots [lo, hi).
+__global__ void k_mass_gather(DevParticles P, int lo, int hi, GridView g, int write_initial) {
+    int s = lo + blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= hi) return;
+    float2 x = P.x[s];
+    float mass = P.mass[s];
+    QW w = quadratic_weights(x);
+    float density = 0.0f;
+    for (int gx = 0; gx < 3; ++gx)
+        for (int gy = 0; gy < 3; ++gy) {
+            float weight = w.wx[gx] * w.wy[gy];
+            int cx = w.bx + gx - 1, cy = w.by + gy - 1;
+            float mc = in_domain(cx, cy, g.res) ? g.acc_a[cell_index(cx, cy, g.tpd)].x : 0.0f;
+            density += mc * weight;
+        }
+    if (density > F32_EPS) {
+        P.rho[s] = density;
+        float vol = mass / density;
+        P.vol[s] = vol;
+        if (write_initial) P.v0[s] = vol;
+    }
+}
+
+// ---------------------------------------------------------------- launchers
+static inline int blocks_for(int n, int per) { return (n + per - 1) / per; }
+
+void launch_particle_pass(const StepLaunch &L, const LoadFlagsHost &lfh, int mode_g2p) {
+    if (L.n == 0) return;
+    ParticleKernelArgs a;
+    a.P = L.P;
+    a.n = L.n;
+    a.mats = L.mats;
+    a.n_mats = L.n_mats;
+    a.cfg = L.cfg;
+    a.st = L.st;
+    a.g = L.g;
+    a.lf.temperature = lfh.temperature;
+    a.lf.activation = lfh.activation;
+    a.lf.pinned = lfh.pinned;
+    a.mode_g2p = mode_g2p;
+    a.density_mode = L.density_mode;
+    a.use_window = L.use_window;
+    k_particle<<<blocks_for(L.n, THREADS * PPT), THREADS, 0, L.stream>>>(a);
+}
+
+void launch_density_pass(const StepLaunch &L, const LoadFlagsHost &lfh) {
+    if (L.n == 0) return;
+    DensityKernelArgs a;
+    a.P = L.P;
+    a.n = L.n;
+    a.mats = L.mats;
+    a.n_mats = L.n_mats;
+    a.cfg = L.cfg;
+    a.st = L.st;
+    a.g = L.g;
+    a.lf.temperature = lfh.temperature;
+    a.lf.activation = lfh.activation;
+    a.lf.pinned = lfh.pinned;
+    a.use_window = L.use_window;
+    k_density<<<blocks_for(L.n, THREADS * PPT), THREADS, 0, L.stream>>>(a);
+}
+
+void launch_grid_update(const StepLaunch &L) {
+    GridKernelArgs a;
+    a.g = L.g;
+    a.cfg = L.cfg;
+    a.st = L.st;
+    a.n_tiles = L.g.tpd * L.g.tpd;
+    k_grid_update<<<blocks_for(a.n_tiles, 4), 256, 0, L.stream>>>(a);
+}
+
+void launch_step_begin(const StepLaunch &L) { k_step_begin<<<1, 1, 0, L.stream>>>(L.st, L.cfg); }
+
+void launch_substep_begin(const StepLaunch &L, int use_cond, unsigned long long handle,
+                          int kernels_per_substep) {
+    k_substep_begin<<<1, 1, 0, L.stream>>>(L.st, L.cfg, use_cond,
+                                           static_cast<cudaGraphConditionalHandle>(handle),
+                                           kernels_per_substep);
+}
+
+void launch_prime_setup(const StepLaunch &L) { k_prime_setup<<<1, 1, 0, L.stream>>>(L.st); }
+
+void launch_region_state(const DevParticles &P, int n, float cx, float cy, float r2, void *acc,
+                         cudaStream_t stream) {
+    int blocks = blocks_for(n, 256);
+    if (blocks > 148 * 8) blocks = 148 * 8;
+    if (blocks < 1) blocks = 1;
+    k_region_state<<<blocks, 256, 0, stream>>>(P, n, cx, cy, r2, static_cast<RegionAcc *>(acc));
+}
+
+size_t region_acc_bytes() { return sizeof(RegionAcc); }
+
+void region_acc_finalize(const void *acc, emerge_body_state *out) {
+    const RegionAcc &a = *static_cast<const RegionAcc *>(acc);
+    out->count = a.count;
+    float sx = static_cast<float>(a.sx), sy = static_cast<float>(a.sy);
+    float sp = static_cast<float>(a.speed), sjp = static_cast<float>(a.jp);
+    float sdet = static_cast<float>(a.det), srho = static_cast<float>(a.rho);
+    unsigned int o = a.max_jp_bits;
+    unsigned int u = (o & 0x80000000u) ? (o & 0x7fffffffu) : ~o;
+    float mjp;
+    std::memcpy(&mjp, &u, sizeof(float));
+    if (a.count > 0) {
+        float n = static_cast<float>(a.count);
+        sx /= n; sy /= n; sp /= n; sjp /= n; sdet /= n; srho /= n;
+    }
+    out->avg_volume_ratio = sjp;
+    out->max_volume_ratio = mjp;
+    out->avg_speed = sp;
+    out->avg_det_f = sdet;
+    out->avg_density = srho;
+    out->centroid[0] = sx;
+    out->centroid[1] = sy;
+    out->pad_ = 0;
+}
+
+void launch_gather_aos(const DevParticles &P, int n, emerge_particle *out, cudaStream_t stream) {
+    if (n) k_gather_aos<<<blocks_for(n, 256), 256, 0, stream>>>(P, n, out);
+}
+void launch_scatter_aos(const DevParticles &P, int n, const emerge_particle *in, cudaStream_t stream) {
+    if (n) k_scatter_aos<<<blocks_for(n, 256), 256, 0, stream>>>(P, n, in);
+}
+void launch_append_aos(const DevParticles &P, int n_old, int n_new, const emerge_particle *in,
+                       cudaStream_t stream) {
+    if (n_new > n_old)
+        k_append_aos<<<blocks_for(n_new - n_old, 256), 256, 0, stream>>>(P, n_old, n_new, in);
+}
+void launch_reinit(const DevParticles &P, int n, const MatP *mats, int n_mats, cudaStream_t stream) {
+    if (n) k_reinit<<<blocks_for(n, 256), 256, 0, stream>>>(P, n, mats, n_mats);
+}
+void launch_mass_scatter(const DevParticles &P, int n, const GridView &g, int filter, float lox,
+                         float loy, float hix, float hiy, cudaStream_t stream) {
+    if (n) k_mass_scatter<<<blocks_for(n, 256), 256, 0, stream>>>(P, n, g, filter, lox, loy, hix, hiy);
+}
+void launch_mass_gather(const DevParticles &P, int lo, int hi, const GridView &g, int write_initial,
+                        cudaStream_t stream) {
+    if (hi > lo) k_mass_gather<<<blocks_for(hi - lo, 256), 256, 0, stream>>>(P, lo, hi, g, write_initial);
+}
+
+}  // namespace emerge

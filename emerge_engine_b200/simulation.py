@@ -1,0 +1,247 @@
+"""`Simulation` on the CUDA backend, with the reference's method names.
+
+Mirrors the public surface of the reference `Simulation` that the MLS-MPM step needs:
+construction and builders (spacetime/solver/lifecycle.rs:26-214), `add_body`
+(solver/particles.rs:355-423), `step` / `step_n` (solver/step.rs:23-60, 327-331),
+`region_state` (solver/queries.rs:125-141), `particles()` and the last-step accessors.
+Every call goes through the C ABI of libemerge_cuda.so; nothing is computed on the host
+except scene bookkeeping (material registry, boundary list).
+"""
+from __future__ import annotations
+
+import ctypes
+from ctypes import byref, c_float, c_uint32, c_uint64, c_void_p
+
+import numpy as np
+
+from . import abi
+from .abi import (PARTICLE_DTYPE, BodyStateC, MaterialParamsC, StepTimingC, check,
+                  load_library)
+from .config import BodyState, SimConfig, SlipBoundary, SpawnRegion
+from .materials import DEVICE_MODELS, FallbackMaterial, Material
+
+MAX_MATERIAL_SLOTS = 64  # materials/registry.rs:6
+
+
+class MaterialRegistry:
+    """`MaterialRegistry` semantics (materials/registry.rs:12-112): contiguous ids from 0,
+    at most 64 slots, slot 0 is the default."""
+
+    def __init__(self, default: Material):
+        self.materials = [default]
+
+    def insert(self, material_id: int, material: Material) -> None:
+        if material_id >= MAX_MATERIAL_SLOTS:
+            raise ValueError(f"material_id {material_id} exceeds GPU limit of 64")
+        if material_id < len(self.materials):
+            self.materials[material_id] = material
+        elif material_id == len(self.materials):
+            self.materials.append(material)
+        else:
+            raise ValueError("material IDs must be registered contiguously starting at 0; "
+                             f"expected id {len(self.materials)}, got {material_id}")
+
+    def next_id(self) -> int:
+        return len(self.materials)
+
+    def set_default(self, material: Material) -> None:
+        self.materials[0] = material
+
+    def get(self, material_id: int) -> Material:
+        if material_id < len(self.materials):
+            return self.materials[material_id]
+        return self.materials[0]
+
+    def __len__(self):
+        return len(self.materials)
+
+
+class Simulation:
+    """The reference `Simulation` API, stepped by the B200 kernels."""
+
+    def __init__(self, config: SimConfig, device: int = 0, lib_path: str | None = None):
+        config.validate()
+        self._lib = load_library(lib_path)
+        self.config = config.copy()
+        cfg = config.to_c()
+        ptr = c_void_p()
+        check(self._lib, self._lib.emerge_cuda_create(byref(cfg), int(device), byref(ptr)))
+        self._sim = ptr
+        self.registry = MaterialRegistry(FallbackMaterial())
+        self.boundaries = [SlipBoundary(config.boundary_thickness)]  # lifecycle.rs:29-30
+        self.last_timing: dict | None = None
+
+    # ---------------------------------------------------------------- lifecycle
+    @classmethod
+    def empty(cls, config: SimConfig, device: int = 0) -> "Simulation":
+        return cls(config, device)
+
+    @classmethod
+    def new(cls, config: SimConfig, spawn: SpawnRegion, device: int = 0) -> "Simulation":
+        """`Simulation::new` (lifecycle.rs:57-99)."""
+        s = cls(config, device)
+        if not spawn.fits_in_sim(config):
+            raise ValueError("spawn region must stay inside the simulation domain")
+        sp = spawn.to_c()
+        s._check(s._lib.emerge_cuda_init_with_spawn(s._sim, byref(sp)))
+        return s
+
+    def close(self) -> None:
+        if getattr(self, "_sim", None):
+            self._lib.emerge_cuda_destroy(self._sim)
+            self._sim = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def _check(self, status: int) -> None:
+        check(self._lib, status, self._sim)
+
+    # ---------------------------------------------------------------- materials
+    def _upload_materials(self) -> None:
+        for k, m in enumerate(self.registry.materials):
+            if m.constitutive_model() not in DEVICE_MODELS:
+                raise abi.EmergeError(abi.ERR_UNSUPPORTED,
+                                      f"material {k}: model {m.constitutive_model()} has no "
+                                      "device implementation")
+        arr = (MaterialParamsC * len(self.registry))(
+            *[m.abi_params() for m in self.registry.materials])
+        self._check(self._lib.emerge_cuda_set_materials(self._sim, arr, len(self.registry)))
+
+    def with_default_material(self, material: Material) -> "Simulation":
+        """lifecycle.rs:107-111 (also re-runs init_particle on every particle)."""
+        self.registry.set_default(material)
+        self._upload_materials()
+        return self
+
+    def set_material(self, material_id: int, material: Material) -> None:
+        self.registry.insert(material_id, material)
+        self._upload_materials()
+
+    def with_material(self, material_id: int, material: Material) -> "Simulation":
+        self.set_material(material_id, material)
+        return self
+
+    def register_material(self, material: Material) -> int:
+        mid = self.registry.next_id()
+        self.set_material(mid, material)
+        return mid
+
+    # ---------------------------------------------------------------- boundaries
+    def _upload_boundaries(self) -> None:
+        arr = (c_uint64 * max(len(self.boundaries), 1))(*[b.thickness for b in self.boundaries])
+        self._check(self._lib.emerge_cuda_set_slip_boundaries(self._sim, arr, len(self.boundaries)))
+
+    def add_boundary_condition(self, boundary: SlipBoundary) -> None:
+        if not isinstance(boundary, SlipBoundary):
+            raise abi.EmergeError(abi.ERR_UNSUPPORTED, "only SlipBoundary is on the device path")
+        self.boundaries.append(boundary)
+        self._upload_boundaries()
+
+    def with_boundary(self, boundary: SlipBoundary) -> "Simulation":
+        self.add_boundary_condition(boundary)
+        return self
+
+    def set_boundary_condition(self, boundary: SlipBoundary) -> None:
+        self.boundaries = []
+        self.add_boundary_condition(boundary)
+
+    def clear_boundaries(self) -> None:
+        self.boundaries = []
+        self._upload_boundaries()
+
+    # ---------------------------------------------------------------- particles
+    def add_body(self, spawn: SpawnRegion) -> int:
+        """`add_body` (particles.rs:355-423); returns the group tag."""
+        if not spawn.fits_in_sim(self.config):
+            raise ValueError("spawn region must stay inside the simulation domain")
+        sp = spawn.to_c()
+        tag = c_uint32()
+        self._check(self._lib.emerge_cuda_add_body(self._sim, byref(sp), byref(tag)))
+        return int(tag.value)
+
+    def add_particles(self, particles: np.ndarray, estimate_volumes: bool = False) -> None:
+        arr = np.ascontiguousarray(particles, dtype=PARTICLE_DTYPE)
+        self._check(self._lib.emerge_cuda_add_particles(
+            self._sim, arr.ctypes.data_as(c_void_p), len(arr), 1 if estimate_volumes else 0))
+
+    def particle_count(self) -> int:
+        n = c_uint64()
+        self._check(self._lib.emerge_cuda_particle_count(self._sim, byref(n)))
+        return int(n.value)
+
+    def particles(self) -> np.ndarray:
+        """Copy of every particle in reference index order (structured array)."""
+        n = self.particle_count()
+        out = np.zeros(n, dtype=PARTICLE_DTYPE)
+        if n:
+            self._check(self._lib.emerge_cuda_read_particles(
+                self._sim, out.ctypes.data_as(c_void_p), n))
+        return out
+
+    def set_particles(self, particles: np.ndarray) -> None:
+        """Write-back of `particles_mut()` edits (lifecycle.rs:233)."""
+        arr = np.ascontiguousarray(particles, dtype=PARTICLE_DTYPE)
+        self._check(self._lib.emerge_cuda_write_particles(
+            self._sim, arr.ctypes.data_as(c_void_p), len(arr)))
+
+    # ---------------------------------------------------------------- stepping
+    def step(self) -> None:
+        self.step_n(1)
+
+    def step_n(self, steps: int, timing: bool = False) -> None:
+        if timing:
+            t = StepTimingC()
+            self._check(self._lib.emerge_cuda_step(self._sim, int(steps), byref(t)))
+            self.last_timing = {name: int(getattr(t, name)) for name, _ in StepTimingC._fields_}
+        else:
+            self._check(self._lib.emerge_cuda_step(self._sim, int(steps), None))
+
+    def synchronize(self) -> None:
+        self._check(self._lib.emerge_cuda_synchronize(self._sim))
+
+    def last_substeps(self) -> int:
+        v = c_uint64()
+        self._check(self._lib.emerge_cuda_last_substeps(self._sim, byref(v)))
+        return int(v.value)
+
+    def effective_dt(self) -> float:
+        v = c_float()
+        self._check(self._lib.emerge_cuda_effective_dt(self._sim, byref(v)))
+        return float(v.value)
+
+    def last_counters(self) -> tuple[int, int, float]:
+        a, b, d = c_uint64(), c_uint64(), c_float()
+        self._check(self._lib.emerge_cuda_last_counters(self._sim, byref(a), byref(b), byref(d)))
+        return int(a.value), int(b.value), float(d.value)
+
+    # ---------------------------------------------------------------- queries
+    def region_state(self, center, radius: float) -> BodyState:
+        out = BodyStateC()
+        self._check(self._lib.emerge_cuda_region_state(
+            self._sim, float(center[0]), float(center[1]), float(radius), byref(out)))
+        return BodyState.from_c(out)
+
+    # ---------------------------------------------------------------- tuning
+    def set_option(self, option: int, value: int) -> None:
+        self._check(self._lib.emerge_cuda_set_option(self._sim, int(option), int(value)))
+
+    def sort_now(self, key_mode: int = 0) -> None:
+        self._check(self._lib.emerge_cuda_sort_now(self._sim, int(key_mode)))
+
+    def kernel_launches(self) -> int:
+        v = c_uint64()
+        self._check(self._lib.emerge_cuda_kernel_launches(self._sim, byref(v)))
+        return int(v.value)
+
+    def stream_handle(self) -> int:
+        return int(self._lib.emerge_cuda_stream(self._sim) or 0)

@@ -1,0 +1,303 @@
+/*
+ * emerge_cuda.h -- C ABI of the B200 (sm_100a) MLS-MPM backend for emerge-engine.
+ *
+ * This library is a drop-in `cuda` backend for the reference crate's CPU step
+ * (M1thieu/emerge-engine 0.1.0, Rust).  Every entry point below names the
+ * reference item it stands in for (path:line inside the reference crate).
+ * Signatures use plain pointers, sizes and POD structs only.
+ *
+ * Conventions
+ *  - Every function returns an emerge_status (0 = EMERGE_OK).  On failure the
+ *    message is available from emerge_cuda_last_error(sim) (or, for create,
+ *    emerge_cuda_last_global_error()).  The reference panics in the same
+ *    situations (invalid config, spawn out of bounds, non-contiguous material
+ *    ids); a Rust shim turns the codes back into those panics.
+ *  - The library owns all device memory of a simulation.  Reads copy into
+ *    caller memory; no caller pointer is retained after a call returns.
+ *  - One CUDA stream per simulation.  Calls on one simulation must be
+ *    serialised by the caller (the reference Simulation is `&mut self`);
+ *    different simulations are independent.
+ *  - There is no CPU fallback: a missing or unusable GPU is an error.
+ */
+#ifndef EMERGE_CUDA_H
+#define EMERGE_CUDA_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum emerge_status {
+    EMERGE_OK = 0,
+    EMERGE_ERR_INVALID_ARG = 1,  /* config.rs:247-299 / :485-505, registry.rs:31-46 asserts */
+    EMERGE_ERR_UNSUPPORTED = 2,  /* model / feature with no device implementation */
+    EMERGE_ERR_CUDA = 3,         /* CUDA runtime error (message has the CUDA error string) */
+    EMERGE_ERR_TIMEOUT = 4,      /* a bounded device wait gave up */
+    EMERGE_ERR_NONFINITE = 5,    /* non-finite state where the reference would NaN-cascade */
+    EMERGE_ERR_OOM = 6           /* device allocation failed */
+} emerge_status;
+
+/* Particle, byte-identical to the reference `Particle` (matter/particle.rs:13-138,
+ * size asserted 128 at :144).  Matrices are column-major (glam Mat2 x_axis, y_axis). */
+typedef struct emerge_particle {
+    float x[2];
+    float v[2];
+    float c[4];               /* velocity_gradient (APIC C) */
+    float f[4];               /* deformation_gradient */
+    float mass;
+    float initial_volume;
+    float volume;
+    float density;
+    uint32_t material_id;
+    float plastic_volume_ratio;
+    float hardening_scale;
+    float friction_hardening;
+    float log_volume_strain;
+    float temperature;
+    uint32_t user_tag;
+    float activation;
+    float activation_dir[2];
+    uint32_t muscle_group_id;
+    uint32_t contact_group;   /* must be 0: multi-field contact is not on the device path */
+    uint32_t sleeping;
+    uint32_t pinned;
+    float scalar_field;
+    uint32_t pad_;
+} emerge_particle;
+
+/* SimConfig, field for field (spacetime/solver/config.rs:26-121); usize -> uint64,
+ * bool -> uint32, Vec2 -> float[2].  Explicit padding keeps the layout fixed. */
+typedef struct emerge_sim_config {
+    uint64_t grid_res;
+    float grid_cell_size;
+    float dt;
+    uint32_t adaptive_timestep;
+    uint32_t cfl_include_affine_speed;
+    float cfl_coefficient;
+    float material_cfl_coefficient;
+    float viscous_timestep_coefficient;
+    float min_dt;
+    uint32_t project_invalid_state;
+    float projection_min_density;
+    float projection_min_volume;
+    float projection_min_deformation_j;
+    float gravity[2];
+    uint64_t boundary_thickness;
+    float default_initial_volume;
+    uint32_t recompute_density_each_step;
+    float particle_mass;
+    uint32_t pad0_;
+    uint64_t max_substeps_per_step;
+    float apic_blend;
+    float j_max;
+    float sleep_threshold;          /* must be 0: the sleep partition is not on the device path */
+    float contact_friction;
+    float asflip_blend;             /* must be 0: ASFLIP is not on the device path */
+    float mixture_drag_coefficient;
+    uint32_t mixture_pressure_iterations;
+    float dx_meters;
+    float dt_seconds;
+    uint32_t pad1_;
+} emerge_sim_config;
+
+/* MaterialParams (matter/materials/params.rs:10-101, 96 bytes).  `model` carries
+ * MaterialModel::constitutive_model() (materials/mod.rs:53-66), NOT params().model:
+ * NaccMaterial::params() reports NeoHookean (nacc.rs:300-314).  Supported models:
+ * 0 Fallback, 1 Fluid, 2 NeoHookean, 4 Snow, 5 DruckerPrager, 10 Nacc. */
+typedef struct emerge_material_params {
+    uint32_t model;
+    float lambda;
+    float mu;
+    float hardening_exponent;
+    float compression_limit;
+    float stretch_limit;
+    float rest_density;
+    float eos_stiffness;
+    float eos_power;
+    float dynamic_viscosity;
+    float volume_ratio_min;
+    float volume_ratio_max;
+    float dp_h0;
+    float dp_h1;
+    float dp_h2;
+    float dp_h3;
+    float active_stress_coeff;
+    float hardening_modulus;
+    float thermal_viscosity_coeff;
+    float thermal_expansion;
+    float pressure_floor;
+    float bulk_viscosity;
+    float surface_tension_coeff;
+    float cohesion_coeff;
+} emerge_material_params;
+
+/* SpawnRegion (spacetime/solver/config.rs:317-346). shape: 0 = Box, 1 = Disk. */
+typedef struct emerge_spawn_region {
+    float spacing;
+    int32_t box_size[2];
+    float box_center[2];
+    uint32_t shape;
+    float disk_radius;
+    float initial_deformation_gradient[4];
+    uint32_t precompute_initial_volumes;
+    float initial_velocity_scale;
+    float position_jitter;
+    uint32_t rng_seed;
+    uint32_t material_id;
+    uint32_t has_mass_override;
+    float mass_override;
+} emerge_spawn_region;
+
+/* BodyState (spacetime/solver/query.rs:17-32). */
+typedef struct emerge_body_state {
+    uint64_t count;
+    float avg_volume_ratio;
+    float max_volume_ratio;
+    float avg_speed;
+    float avg_det_f;
+    float avg_density;
+    float centroid[2];
+    uint32_t pad_;
+} emerge_body_state;
+
+/* StepTiming (systems/diagnostics/snapshot.rs:82-105), microseconds of GPU time
+ * measured with CUDA events on the simulation's stream.  Filled per phase only
+ * when the simulation runs in the instrumented (non-graph) mode; in graph mode
+ * only total_us is filled.  fields/thermal/spatial_hash/phase_sleep are 0. */
+typedef struct emerge_step_timing {
+    uint64_t p2g_us;
+    uint64_t grid_update_us;
+    uint64_t g2p_us;
+    uint64_t fields_us;
+    uint64_t thermal_us;
+    uint64_t cfl_us;
+    uint64_t spatial_hash_us;
+    uint64_t phase_sleep_us;
+    uint64_t project_us;
+    uint64_t density_us;
+    uint64_t total_us;
+} emerge_step_timing;
+
+typedef struct emerge_sim emerge_sim;
+
+/* ---- lifecycle -------------------------------------------------------------- */
+
+/* Simulation::empty(config) (spacetime/solver/lifecycle.rs:26-54): validates the
+ * config (SimConfig::validate, config.rs:247-299), registers the fallback material
+ * at id 0 and one SlipBoundary(config.boundary_thickness) (lifecycle.rs:29-30). */
+emerge_status emerge_cuda_create(const emerge_sim_config *config, int device, emerge_sim **out);
+/* Drop for Simulation. */
+emerge_status emerge_cuda_destroy(emerge_sim *sim);
+/* Message for the last failed call on `sim` (never NULL). */
+const char *emerge_cuda_last_error(const emerge_sim *sim);
+/* Message for the last failed emerge_cuda_create on this thread. */
+const char *emerge_cuda_last_global_error(void);
+
+/* MaterialRegistry contents (materials/registry.rs:12-112; all_params :110).
+ * Replaces the whole registry with `count` entries, ids 0..count-1 (count <= 64,
+ * MAX_MATERIAL_SLOTS registry.rs:6).  Entry 0 replaces the default material and,
+ * like with_default_material (lifecycle.rs:107-111), re-runs init_particle on
+ * every particle whose material changed. */
+emerge_status emerge_cuda_set_materials(emerge_sim *sim, const emerge_material_params *params,
+                                        uint32_t count);
+/* Boundary list (Simulation::boundaries, solver/mod.rs:50): `n` SlipBoundary
+ * thicknesses applied in order (with_boundary lifecycle.rs:114 appends;
+ * set_boundary_condition :353 replaces). */
+emerge_status emerge_cuda_set_slip_boundaries(emerge_sim *sim, const uint64_t *thickness,
+                                              uint32_t n);
+
+/* ---- particles ---------------------------------------------------------------- */
+
+/* Simulation::add_body (spacetime/solver/particles.rs:355-423): lattice spawn with
+ * the LCG (solver/mod.rs:88-175), tag stamping, init_particle, and the local
+ * initial-volume estimate (density.rs:81-144) on the device. */
+emerge_status emerge_cuda_add_body(emerge_sim *sim, const emerge_spawn_region *spawn,
+                                   uint32_t *tag_out);
+/* Simulation::new (lifecycle.rs:57-99) particle set-up for an empty simulation:
+ * spawns the region with tag 0 and, if spawn->precompute_initial_volumes, runs the
+ * full estimate_particle_volumes (density.rs:41-72) on the device. */
+emerge_status emerge_cuda_init_with_spawn(emerge_sim *sim, const emerge_spawn_region *spawn);
+/* GpuSimulation::new(config, Vec<Particle>, registry) particle upload
+ * (systems/gpu/solver/mod.rs:246): appends `n` particles as-is.  When
+ * estimate_volumes != 0 the appended group gets add_body's local volume estimate. */
+emerge_status emerge_cuda_add_particles(emerge_sim *sim, const emerge_particle *particles,
+                                        uint64_t n, int estimate_volumes);
+/* Particles::len (matter/particle.rs:300). */
+emerge_status emerge_cuda_particle_count(const emerge_sim *sim, uint64_t *n_out);
+/* Simulation::particles() (lifecycle.rs:214): copies all particles, in the
+ * reference's index order, into `out` (n must equal the particle count). */
+emerge_status emerge_cuda_read_particles(emerge_sim *sim, emerge_particle *out, uint64_t n);
+/* Simulation::particles_mut() (lifecycle.rs:233) write-back: replaces every
+ * particle's state from `in` (reference index order). */
+emerge_status emerge_cuda_write_particles(emerge_sim *sim, const emerge_particle *in, uint64_t n);
+
+/* ---- stepping ------------------------------------------------------------------ */
+
+/* Simulation::step_n(n) (spacetime/solver/step.rs:327-331); each step is
+ * Simulation::step (step.rs:23-60): adaptive substeps with CFL (step.rs:434-488),
+ * state projection (:347-429), density recompute (density.rs:41-72), P2G
+ * (transfer/p2g.rs:24-72), grid update (grid/mod.rs:264-291, step.rs:150-165),
+ * G2P + constitutive update (transfer/g2p.rs:151-343).  Asynchronous: returns
+ * once the work is queued.  `timing` (nullable) receives the last step's timing
+ * and forces a synchronisation. */
+emerge_status emerge_cuda_step(emerge_sim *sim, uint32_t n_steps, emerge_step_timing *timing);
+/* Simulation::last_substeps (step.rs:323). Synchronises. */
+emerge_status emerge_cuda_last_substeps(emerge_sim *sim, uint64_t *out);
+/* Simulation::effective_dt (step.rs:319). Synchronises. */
+emerge_status emerge_cuda_effective_dt(emerge_sim *sim, float *out);
+/* last_vel_clamp_count / last_j_projection_count (solver/mod.rs:63-64) and
+ * last_sim_time_dropped (:65) of the last step. Synchronises. */
+emerge_status emerge_cuda_last_counters(emerge_sim *sim, uint64_t *vel_clamp_count,
+                                        uint64_t *j_projection_count, float *sim_time_dropped);
+/* Blocks until all queued work of `sim` is done. */
+emerge_status emerge_cuda_synchronize(emerge_sim *sim);
+
+/* ---- queries --------------------------------------------------------------------- */
+
+/* Simulation::region_state(center, radius) (spacetime/solver/queries.rs:125-141):
+ * device reduction (f64 accumulators) over active particles with |x-c|^2 <= r^2. */
+emerge_status emerge_cuda_region_state(emerge_sim *sim, float cx, float cy, float radius,
+                                       emerge_body_state *out);
+
+/* ---- options and diagnostics ------------------------------------------------------- */
+
+/* Tuning knobs that change no result beyond float summation order:
+ *   EMERGE_OPT_USE_GRAPH       1 = capture each step in a CUDA graph with a device-side
+ *                              substep loop (default), 0 = host-driven substep loop with
+ *                              per-phase event timing.
+ *   EMERGE_OPT_SORT_INTERVAL   re-sort particles by tile every N steps (0 = adaptive,
+ *                              default; see emerge_cuda_sort_now).
+ *   EMERGE_OPT_P2G_WINDOW      1 = shared-memory window scatter (default), 0 = direct
+ *                              global reductions. */
+enum {
+    EMERGE_OPT_USE_GRAPH = 1,
+    EMERGE_OPT_SORT_INTERVAL = 2,
+    EMERGE_OPT_P2G_WINDOW = 3
+};
+emerge_status emerge_cuda_set_option(emerge_sim *sim, int option, int64_t value);
+
+/* Particle sort (reference GPU path: systems/gpu/shaders/particle_sort.wgsl:124-245,
+ * counting sort by block_index, non-deterministic within a block).  Here: stable
+ * device LSD radix sort of the current particles by key, applied as a permutation
+ * of the device particle storage.  key_mode 0 = tile key (8x8-cell tiles in Morton
+ * order, cell within tile), 1 = the reference's block_index key
+ * (particle_sort.wgsl:94-102).  Host-visible particle order is unchanged. */
+emerge_status emerge_cuda_sort_now(emerge_sim *sim, int key_mode);
+/* Test hook for the sort: computes keys for `n` positions (key_mode as above, for a
+ * grid of `grid_res` cells) and the stable sort permutation, on the device.
+ * keys_out[i] = key of xy[i]; perm_out = stable argsort of the keys. */
+emerge_status emerge_cuda_sort_keys(const float *xy, uint64_t n, uint32_t grid_res, int key_mode,
+                                    uint32_t *keys_out, uint32_t *perm_out);
+
+/* The CUDA stream the simulation's work runs on (cudaStream_t as void*). */
+void *emerge_cuda_stream(emerge_sim *sim);
+/* Number of kernels this library launched on `sim` since creation (graph launches
+ * count every kernel node executed, substep loops included). Synchronises. */
+emerge_status emerge_cuda_kernel_launches(emerge_sim *sim, uint64_t *out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* EMERGE_CUDA_H */

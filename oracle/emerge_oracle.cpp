@@ -1,0 +1,1381 @@
+// emerge_oracle.cpp -- CPU oracle: a C++17 restatement of the reference
+// emerge-engine MLS-MPM step (Rust crate M1thieu/emerge-engine 0.1.0).
+//
+// TEST INFRASTRUCTURE.  Used only by tests/, the smoke check and bench.py's
+// CPU-baseline leg, as the parity checker and the timed CPU baseline.  The
+// product CUDA library never links this file.
+//
+// Every function cites the reference file:line it restates.  Arithmetic is
+// f32 throughout, evaluated in the reference's expression order, compiled
+// with -ffp-contract=off (Rust does not contract a*b+c into FMA).  glam's
+// Mat2/Vec2 operations are restated from their definitions (column-major
+// Mat2; determinant = x_axis.x*y_axis.y - y_axis.x*x_axis.y; length =
+// sqrt(dot)); glam 0.30's source is not present here, so bit-level identity
+// with the Rust build is not claimed.  Transcendentals (expf, logf, sinf,
+// sinhf, powf, sqrtf) call glibc's libm, which is what Rust's f32 methods
+// call on Linux.
+//
+// The sparse FxHash grid of the reference (grid/mod.rs:112-139) is restated
+// as a dense column-major array (index x*res+y) plus a dirty list in
+// first-touch order: per-cell summation order (particle index order) is the
+// same, and every per-cell grid operation is order-independent, so results
+// are unchanged; only the constant factor of the baseline differs (a dense
+// array is faster than a hash map, so the CPU baseline timed from this file
+// is an upper bound on the reference's own CPU throughput).
+
+#include "emerge_oracle.h"
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <limits>
+#include <map>
+#include <numeric>
+#include <utility>
+#include <vector>
+
+#include <thread>
+
+namespace {
+
+int g_threads = 0;  // 0 = std::thread::hardware_concurrency()
+
+// Static-partition parallel for over [0, n): stands in for rayon's par_iter in
+// G2P phase 1 (per-particle work with no cross-particle dependency).
+template <class Fn>
+void parallel_for(long n, Fn fn) {
+    int t = g_threads > 0 ? g_threads : static_cast<int>(std::thread::hardware_concurrency());
+    if (t < 1) t = 1;
+    if (n < 4096 || t == 1) {
+        fn(0L, n);
+        return;
+    }
+    std::vector<std::thread> pool;
+    long chunk = (n + t - 1) / t;
+    for (int k = 0; k < t; ++k) {
+        long lo = k * chunk, hi = std::min(n, lo + chunk);
+        if (lo >= hi) break;
+        pool.emplace_back([=] { fn(lo, hi); });
+    }
+    for (auto &th : pool) th.join();
+}
+
+constexpr float F32_EPS = 1.1920929e-7f;         // f32::EPSILON
+constexpr float KERNEL_D_INVERSE = 4.0f;         // config.rs:22
+constexpr float MIN_J = 1e-6f;                   // materials/utils.rs:11
+constexpr float LOG_CLAMP = 1e-10f;              // materials/utils.rs:6
+constexpr size_t MAX_MATERIAL_SLOTS = 64;        // registry.rs:6
+
+// ---------------------------------------------------------------- glam restated
+struct V2 { float x, y; };
+struct M2 { V2 xa, ya; };  // x_axis, y_axis (columns)
+
+inline V2 v2(float x, float y) { return V2{x, y}; }
+inline V2 add(V2 a, V2 b) { return v2(a.x + b.x, a.y + b.y); }
+inline V2 sub(V2 a, V2 b) { return v2(a.x - b.x, a.y - b.y); }
+inline V2 mul(V2 a, V2 b) { return v2(a.x * b.x, a.y * b.y); }
+inline V2 muls(V2 a, float s) { return v2(a.x * s, a.y * s); }
+inline V2 smul(float s, V2 a) { return v2(s * a.x, s * a.y); }
+inline V2 divs(V2 a, float s) { return v2(a.x / s, a.y / s); }
+inline V2 splat(float s) { return v2(s, s); }
+inline float dot(V2 a, V2 b) { return a.x * b.x + a.y * b.y; }
+inline float length(V2 a) { return std::sqrt(dot(a, a)); }
+inline float length_sq(V2 a) { return dot(a, a); }
+inline bool finite2(V2 a) { return std::isfinite(a.x) && std::isfinite(a.y); }
+inline V2 vabs(V2 a) { return v2(std::fabs(a.x), std::fabs(a.y)); }
+// f32::max / f32::min semantics (a NaN operand yields the other operand).
+inline float fmax_(float a, float b) { return std::fmax(a, b); }
+inline float fmin_(float a, float b) { return std::fmin(a, b); }
+inline V2 vmax(V2 a, V2 b) { return v2(fmax_(a.x, b.x), fmax_(a.y, b.y)); }
+inline V2 vmin(V2 a, V2 b) { return v2(fmin_(a.x, b.x), fmin_(a.y, b.y)); }
+// glam Vec2::clamp = self.max(min).min(max)
+inline V2 vclamp(V2 a, V2 lo, V2 hi) { return vmin(vmax(a, lo), hi); }
+// f32::clamp: NaN stays NaN
+inline float fclamp(float x, float lo, float hi) {
+    if (x < lo) x = lo;
+    if (x > hi) x = hi;
+    return x;
+}
+// glam normalize_or_zero: self * (1 / length) when finite and > 0
+inline V2 normalize_or_zero(V2 a) {
+    float rcp = 1.0f / length(a);
+    if (std::isfinite(rcp) && rcp > 0.0f) return muls(a, rcp);
+    return v2(0.0f, 0.0f);
+}
+
+inline M2 m2(V2 a, V2 b) { return M2{a, b}; }
+inline M2 ident() { return m2(v2(1, 0), v2(0, 1)); }
+inline M2 zero2() { return m2(v2(0, 0), v2(0, 0)); }
+inline M2 diag(V2 d) { return m2(v2(d.x, 0.0f), v2(0.0f, d.y)); }
+inline M2 madd(M2 a, M2 b) { return m2(add(a.xa, b.xa), add(a.ya, b.ya)); }
+inline M2 msub(M2 a, M2 b) { return m2(sub(a.xa, b.xa), sub(a.ya, b.ya)); }
+inline M2 mscale(M2 a, float s) { return m2(muls(a.xa, s), muls(a.ya, s)); }
+inline M2 smscale(float s, M2 a) { return m2(smul(s, a.xa), smul(s, a.ya)); }
+inline V2 mv(M2 a, V2 v) { return add(muls(a.xa, v.x), muls(a.ya, v.y)); }
+inline M2 mm(M2 a, M2 b) { return m2(mv(a, b.xa), mv(a, b.ya)); }
+inline M2 transpose(M2 a) { return m2(v2(a.xa.x, a.ya.x), v2(a.xa.y, a.ya.y)); }
+inline float det(M2 a) { return a.xa.x * a.ya.y - a.ya.x * a.xa.y; }
+inline bool finite_m(M2 a) { return finite2(a.xa) && finite2(a.ya); }
+
+inline M2 load_m(const float *f) { return m2(v2(f[0], f[1]), v2(f[2], f[3])); }
+inline void store_m(float *f, M2 a) { f[0] = a.xa.x; f[1] = a.xa.y; f[2] = a.ya.x; f[3] = a.ya.y; }
+inline V2 load_v(const float *f) { return v2(f[0], f[1]); }
+inline void store_v(float *f, V2 a) { f[0] = a.x; f[1] = a.y; }
+
+struct IV2 { int32_t x, y; };
+
+// Rust `f32 as i32`: saturating, NaN -> 0.
+inline int32_t f2i_sat(float f) {
+    if (std::isnan(f)) return 0;
+    if (f >= 2147483647.0f) return std::numeric_limits<int32_t>::max();
+    if (f <= -2147483648.0f) return std::numeric_limits<int32_t>::min();
+    return static_cast<int32_t>(f);
+}
+
+// ---------------------------------------------------------------- grid/kernel.rs
+// axis_weights (grid/kernel.rs:20-25); powi(2) lowers to x*x.
+inline void axis_weights(float d, float w[3]) {
+    float a = 0.5f - d;
+    float b = 0.5f + d;
+    w[0] = 0.5f * (a * a);
+    w[1] = 0.75f - d * d;
+    w[2] = 0.5f * (b * b);
+}
+
+struct QW { IV2 base; float wx[3], wy[3]; };
+// quadratic_weights (grid/kernel.rs:10-18)
+inline QW quadratic_weights(V2 p) {
+    QW q;
+    q.base.x = f2i_sat(std::floor(p.x));
+    q.base.y = f2i_sat(std::floor(p.y));
+    float dx = (p.x - static_cast<float>(q.base.x)) - 0.5f;
+    float dy = (p.y - static_cast<float>(q.base.y)) - 0.5f;
+    axis_weights(dx, q.wx);
+    axis_weights(dy, q.wy);
+    return q;
+}
+
+// ---------------------------------------------------------------- materials
+// svd2 (materials/svd.rs:14-76) + orthogonal_complement (:81-85)
+inline V2 orthogonal_complement(V2 v) {
+    V2 perp = v2(-v.y, v.x);
+    float len = length(perp);
+    if (len > 1e-10f) return divs(perp, len);
+    return v2(1.0f, 0.0f);
+}
+
+void svd2(M2 f, M2 &u_out, V2 &sigma_out, M2 &vt_out) {
+    float f00 = f.xa.x, f10 = f.xa.y, f01 = f.ya.x, f11 = f.ya.y;
+    float c00 = f00 * f00 + f10 * f10;
+    float c01 = f00 * f01 + f10 * f11;
+    float c11 = f01 * f01 + f11 * f11;
+    float mean = (c00 + c11) * 0.5f;
+    float half_diff = (c00 - c11) * 0.5f;
+    float disc = std::sqrt(half_diff * half_diff + c01 * c01);
+    float lambda1 = mean + disc;
+    float lambda2 = mean - disc;
+    V2 v1;
+    if (std::fabs(c01) > 1e-10f * fmax_(c00 + c11, 1e-30f)) {
+        V2 raw = v2(c01, lambda1 - c00);
+        v1 = divs(raw, length(raw));
+    } else {
+        v1 = (c00 >= c11) ? v2(1.0f, 0.0f) : v2(0.0f, 1.0f);
+    }
+    V2 vv2 = v2(-v1.y, v1.x);
+    M2 v_sorted = m2(v1, vv2);
+    M2 vt = transpose(v_sorted);
+    V2 sigma = v2(std::sqrt(fmax_(lambda1, 0.0f)), std::sqrt(fmax_(lambda2, 0.0f)));
+    V2 fv1 = mv(f, v1);
+    V2 fv2 = mv(f, vv2);
+    V2 u1 = (sigma.x > 1e-10f) ? divs(fv1, sigma.x) : orthogonal_complement(fv2);
+    V2 u2 = (sigma.y > 1e-10f) ? divs(fv2, sigma.y) : orthogonal_complement(u1);
+    M2 u = m2(u1, u2);
+    if (det(u) < 0.0f) {
+        u.ya = v2(-u.ya.x, -u.ya.y);
+        sigma.y = -sigma.y;
+    }
+    u_out = u;
+    sigma_out = sigma;
+    vt_out = vt;
+}
+
+// polar_decomposition_2d (materials/utils.rs:129-138)
+M2 polar(M2 f) {
+    float x = f.xa.x + f.ya.y;
+    float y = f.xa.y - f.ya.x;
+    float norm = std::sqrt(x * x + y * y);
+    if (norm > F32_EPS) return m2(divs(v2(x, y), norm), divs(v2(-y, x), norm));
+    return ident();
+}
+
+// elastic_wave_dt (materials/utils.rs:145-163)
+float elastic_wave_dt(float lambda, float mu, float hardening, float density,
+                      float min_density, float cell_width, float material_cfl) {
+    float rho = fmax_(density, min_density);
+    float modulus = fmax_((lambda + 2.0f * mu) * hardening, 0.0f);
+    if (modulus <= F32_EPS) return INFINITY;
+    float c = std::sqrt(modulus / rho);
+    if (c <= F32_EPS) return INFINITY;
+    return material_cfl * cell_width / c;
+}
+
+enum Model : uint32_t {
+    FALLBACK = 0, FLUID = 1, NEOHOOKEAN = 2, COROTATED = 3, SNOW = 4,
+    DRUCKER_PRAGER = 5, VON_MISES = 6, RANKINE = 7, DP_MUI = 8,
+    VISCOELASTIC = 9, NACC = 10, GRANULAR_FLUID = 11
+};
+
+using Mat = oracle_material;
+using P = oracle_particle;
+
+// DruckerPragerMaterial::alpha (sand.rs:135-141)
+float dp_alpha(const Mat &m, float q) {
+    float phi = m.friction_angle +
+                (m.hardening_peak * q - m.friction_residual) * std::exp(-m.hardening_decay * q);
+    float s = std::sin(phi);
+    return std::sqrt(2.0f / 3.0f) * (2.0f * s) / (3.0f - s);
+}
+
+// DruckerPragerMaterial::project (sand.rs:156-194)
+bool dp_project(const Mat &m, V2 sigma_in, float lvs, float q, V2 &out, float &dq) {
+    V2 sigma = vmax(vabs(sigma_in), splat(LOG_CLAMP));
+    V2 eps = v2(std::log(sigma.x) + lvs * 0.5f, std::log(sigma.y) + lvs * 0.5f);
+    float trace = eps.x + eps.y;
+    V2 dev = sub(eps, splat(trace * 0.5f));
+    float dev_norm = length(dev);
+    if (dev_norm == 0.0f || trace > 0.0f) {
+        out = v2(1.0f, 1.0f);
+        dq = dev_norm;
+        return true;
+    }
+    float ratio = (m.lambda + m.mu) / m.mu;
+    float alpha = dp_alpha(m, q);
+    float cohesion_term = m.cohesion / (2.0f * m.mu);
+    float gamma = dev_norm + ratio * trace * alpha - cohesion_term;
+    if (gamma <= 0.0f) return false;
+    V2 h = sub(eps, smul(gamma, divs(dev, dev_norm)));
+    out = v2(std::exp(h.x), std::exp(h.y));
+    dq = gamma;
+    return true;
+}
+
+inline M2 reconstruct(M2 u, V2 s, M2 vt) { return mm(mm(u, diag(s)), vt); }
+
+// NaccMaterial::project (nacc.rs:129-223)
+void nacc_project(const Mat &m, M2 f, float alpha, M2 &f_out, float &alpha_out) {
+    float xi = m.hardening_factor;
+    float beta = m.nacc_cohesion;
+    float mm_ = m.friction;
+    M2 u, vt;
+    V2 sigma;
+    svd2(f, u, sigma, vt);
+    V2 sv = sigma;
+    V2 sv_sq = mul(sv, sv);
+    float sv_sq_trace = sv_sq.x + sv_sq.y;
+    float p0 = m.kappa * (1.0e-5f + std::sinh(xi * fmax_(-alpha, 0.0f)));
+    float j_e_tr = fmax_(sv.x * sv.y, 1.0e-6f);
+    V2 s_tr = smul(m.mu * (1.0f / j_e_tr), sub(sv_sq, splat(sv_sq_trace * 0.5f)));
+    float psi_kappa = m.kappa * 0.5f * (j_e_tr - 1.0f / j_e_tr);
+    float p_tr = -psi_kappa * j_e_tr;
+    bool hard = m.hardening_enabled != 0;
+    if (p_tr > p0) {
+        float j_n1 = std::sqrt(fmax_(-2.0f * p0 / m.kappa + 1.0f, 1.0e-8f));
+        float sv_new = std::pow(j_n1, 0.5f);
+        if (hard) alpha += std::log(j_e_tr / j_n1);
+        f_out = reconstruct(u, splat(sv_new), vt);
+        alpha_out = alpha;
+        return;
+    }
+    if (p_tr < -beta * p0) {
+        float j_n1 = std::sqrt(fmax_(2.0f * beta * p0 / m.kappa + 1.0f, 1.0e-8f));
+        float sv_new = std::pow(j_n1, 0.5f);
+        if (hard) alpha += std::log(j_e_tr / j_n1);
+        f_out = reconstruct(u, splat(sv_new), vt);
+        alpha_out = alpha;
+        return;
+    }
+    float y0 = (1.0f + 2.0f * beta) * 2.0f;
+    float y1 = mm_ * mm_ * (p_tr + beta * p0) * (p_tr - p0);
+    float s_norm_sq = s_tr.x * s_tr.x + s_tr.y * s_tr.y;
+    float y = y0 * s_norm_sq + y1;
+    if (y < 1.0e-4f) {
+        f_out = f;
+        alpha_out = alpha;
+        return;
+    }
+    if (hard && p0 > 1.0e-4f && p_tr < p0 - 1.0e-4f && p_tr > -beta * p0 + 1.0e-4f) {
+        float p_c = (1.0f - beta) * p0 * 0.5f;
+        float q_tr = std::sqrt(2.0f) * length(s_tr);
+        V2 dir = normalize_or_zero(v2(p_c - p_tr, -q_tr));
+        float c = mm_ * mm_ * (p_c + beta * p0) * (p_c - p0);
+        float b = mm_ * mm_ * dir.x * (2.0f * p_c - p0 + beta * p0);
+        float a = mm_ * mm_ * dir.x * dir.x + (1.0f + 2.0f * beta) * dir.y * dir.y;
+        float discr = std::sqrt(fmax_(b * b - 4.0f * a * c, 0.0f));
+        float l1 = (-b + discr) / (2.0f * a);
+        float l2 = (-b - discr) / (2.0f * a);
+        float p1 = p_c + l1 * dir.x;
+        float p2 = p_c + l2 * dir.x;
+        float p_x = ((p_tr - p_c) * (p1 - p_c) > 0.0f) ? p1 : p2;
+        float j_e_x = std::sqrt(fmax_(std::fabs(-2.0f * p_x / m.kappa + 1.0f), 1.0e-8f));
+        if (j_e_x > 1.0e-4f) alpha += std::log(j_e_tr / j_e_x);
+    }
+    float scale = std::sqrt(fmax_(-y1 / fmax_(y0, 1.0e-10f), 0.0f)) * (j_e_tr / m.mu);
+    V2 b_n1 = add(smul(scale, normalize_or_zero(s_tr)), splat(sv_sq_trace / 2.0f));
+    V2 sv_new = v2(std::sqrt(fmax_(b_n1.x, 1.0e-8f)), std::sqrt(fmax_(b_n1.y, 1.0e-8f)));
+    f_out = reconstruct(u, sv_new, vt);
+    alpha_out = alpha;
+}
+
+// MaterialModel::kirchhoff_stress per model.
+M2 kirchhoff_stress(const Mat &m, const P &p) {
+    M2 f = load_m(p.f);
+    switch (m.model) {
+    case NEOHOOKEAN: {  // elastic.rs:180-255
+        float j = det(f);
+        if (j <= MIN_J) return zero2();
+        float t_scale = 1.0f + m.thermal_expansion * p.temperature;
+        float damage_scale = std::exp(-m.damage_softening_rate * p.friction_hardening);
+        float mu = m.mu * t_scale * damage_scale;
+        float lambda = m.lambda * t_scale * damage_scale;
+        M2 b = mm(f, transpose(f));
+        float tr_b = b.xa.x + b.ya.y;
+        M2 dev_b = msub(b, diag(splat(tr_b * 0.5f)));
+        float k = lambda + mu;
+        M2 dev_stress = smscale(mu / j, dev_b);
+        M2 vol_stress = smscale(k * std::log(j), ident());
+        M2 viscous = zero2();
+        if (m.viscosity > 0.0f) {
+            M2 c = load_m(p.c);
+            M2 sym = madd(c, transpose(c));
+            M2 d = mscale(sym, 0.5f);
+            float d_trace = d.xa.x + d.ya.y;
+            M2 d_dev = msub(d, diag(splat(d_trace * 0.5f)));
+            viscous = smscale(m.viscosity, d_dev);
+        }
+        return madd(madd(dev_stress, vol_stress), viscous);
+    }
+    case FLUID: {  // fluid.rs:135-191
+        float density = fmin_(fmax_(p.density, m.fluid_min_density), m.rest_density * 2.0f);
+        float pressure = fmax_(
+            m.eos_stiffness * (std::pow(density / m.rest_density, m.eos_power) - 1.0f),
+            m.pressure_floor);
+        M2 stress = diag(splat(-pressure));
+        float eff_visc = m.dynamic_viscosity;
+        if (m.thermal_viscosity_coeff > 0.0f)
+            eff_visc = m.dynamic_viscosity * std::exp(-m.thermal_viscosity_coeff * p.temperature);
+        M2 c = load_m(p.c);
+        M2 sym = madd(c, transpose(c));
+        float div_v = sym.xa.x + sym.ya.y;
+        M2 strain_dev = msub(sym, diag(splat(div_v * 0.5f)));
+        stress = madd(stress, smscale(eff_visc, strain_dev));
+        if (m.bulk_viscosity > 0.0f)
+            stress = madd(stress, diag(splat(m.bulk_viscosity * div_v * 0.5f)));
+        if (m.surface_tension_coeff != 0.0f) {
+            float j = f.xa.x * f.ya.y - f.xa.y * f.ya.x;
+            stress = madd(stress, diag(splat(m.surface_tension_coeff * j)));
+        }
+        return stress;
+    }
+    case DRUCKER_PRAGER: {  // sand.rs:220-231
+        float j = det(f);
+        if (j <= MIN_J) return zero2();
+        M2 r = polar(f);
+        M2 f_t = transpose(f);
+        M2 a = mm(smscale(2.0f * m.mu, msub(f, r)), f_t);
+        M2 b = smscale(m.lambda * (j - 1.0f) * j, ident());
+        return madd(a, b);
+    }
+    case SNOW: {  // snow.rs:109-136
+        float j = det(f);
+        if (j <= MIN_J) return zero2();
+        M2 r = polar(f);
+        float h = p.hardening_scale;
+        float mu_eff = m.mu * h;
+        float lambda_eff = m.lambda * h;
+        M2 f_t = transpose(f);
+        M2 tau = madd(mm(smscale(2.0f * mu_eff, msub(f, r)), f_t),
+                      smscale(lambda_eff * (j - 1.0f) * j, ident()));
+        if (m.cohesion_coeff > 0.0f && p.plastic_volume_ratio < 1.0f && j > 1.0f)
+            tau = madd(tau, smscale(m.cohesion_coeff * p.plastic_volume_ratio * (j - 1.0f) * j,
+                                    ident()));
+        return tau;
+    }
+    case NACC: {  // nacc.rs:236-249
+        float j = fmax_(det(f), MIN_J);
+        M2 b = mm(f, transpose(f));
+        float tr_b = b.xa.x + b.ya.y;
+        M2 dev_b = msub(b, diag(splat(tr_b * 0.5f)));
+        M2 dev_stress = smscale(m.mu / j, dev_b);
+        M2 vol_stress = smscale(m.kappa * 0.5f * (j * j - 1.0f), ident());
+        return madd(dev_stress, vol_stress);
+    }
+    default:  // FallbackMaterial (materials/mod.rs:362-366): zero stress
+        return zero2();
+    }
+}
+
+// MaterialModel::activation_scale (mod.rs:181-183): NeoHookean overrides it.
+inline float activation_scale(const Mat &m) {
+    return m.model == NEOHOOKEAN ? m.active_stress_coeff : 0.0f;
+}
+
+// combined_kirchhoff_stress (spacetime/transfer.rs:77-104)
+M2 combined_kirchhoff_stress(const Mat &m, const P &p) {
+    M2 tau = kirchhoff_stress(m, p);
+    float coeff = activation_scale(m);
+    if (p.activation <= 0.0f || coeff <= 0.0f) return tau;
+    bool isotropic = m.model == VISCOELASTIC;
+    M2 tau_active;
+    if (isotropic) {
+        tau_active = diag(splat(p.activation * coeff));
+    } else {
+        V2 n = load_v(p.activation_dir);
+        float len_sq = dot(n, n);
+        if (len_sq > F32_EPS) {
+            V2 n0 = divs(n, std::sqrt(len_sq));
+            M2 n_outer = m2(muls(n0, n0.x), muls(n0, n0.y));
+            M2 a_mat = mscale(n_outer, p.activation * coeff);
+            M2 f = load_m(p.f);
+            tau_active = mm(mm(f, a_mat), transpose(f));
+        } else {
+            tau_active = diag(splat(p.activation * coeff));
+        }
+    }
+    return madd(tau, tau_active);
+}
+
+// MaterialModel::stress_volume
+inline float stress_volume(const Mat &m, const P &p) {
+    if (m.model == FLUID) return fmax_(p.volume, m.fluid_min_volume);  // fluid.rs:193-195
+    return p.initial_volume;  // mod.rs:114 default and every other in-scope model
+}
+
+// MaterialModel::timestep_bound
+float timestep_bound(const Mat &m, float density, float h, float cell, float mat_cfl,
+                     float visc_cfl) {
+    switch (m.model) {
+    case NEOHOOKEAN: {  // elastic.rs:290-327
+        float elastic_dt = elastic_wave_dt(m.lambda, m.mu, 1.0f, density, m.min_density, cell,
+                                           mat_cfl);
+        float viscous_dt = INFINITY;
+        if (m.viscosity > 0.0f) {
+            float d = fmax_(density, 1.0e-6f);
+            float kinematic = m.viscosity / d;
+            if (kinematic > F32_EPS) viscous_dt = visc_cfl * cell * cell / kinematic;
+        }
+        return fmin_(elastic_dt, viscous_dt);
+    }
+    case FLUID: {  // fluid.rs:228-259
+        const float MIN_DENSITY_RATIO = 1.0e-6f;
+        float d = fmax_(density, m.fluid_min_density);
+        float ratio = fmax_(d / fmax_(m.rest_density, m.fluid_min_density), MIN_DENSITY_RATIO);
+        float dt_bound = INFINITY;
+        float c2 = m.eos_stiffness * m.eos_power * std::pow(ratio, m.eos_power - 1.0f) /
+                   fmax_(m.rest_density, m.fluid_min_density);
+        if (std::isfinite(c2) && c2 > F32_EPS)
+            dt_bound = fmin_(dt_bound, mat_cfl * cell / std::sqrt(c2));
+        if (m.dynamic_viscosity > 0.0f) {
+            float kin = m.dynamic_viscosity / d;
+            if (kin > F32_EPS) dt_bound = fmin_(dt_bound, visc_cfl * cell * cell / kin);
+        }
+        return dt_bound;
+    }
+    case DRUCKER_PRAGER:  // sand.rs:345-362
+        return elastic_wave_dt(m.lambda, m.mu, 1.0f, density, MIN_J, cell, mat_cfl);
+    case SNOW:  // snow.rs:193-211
+        return elastic_wave_dt(m.lambda, m.mu, h, density, MIN_J, cell, mat_cfl);
+    case NACC: {  // nacc.rs:279-298
+        float lambda = m.kappa - m.mu;
+        return elastic_wave_dt(lambda, m.mu, h, density, m.nacc_min_density, cell, mat_cfl);
+    }
+    default:
+        return INFINITY;
+    }
+}
+
+// MaterialModel::init_particle
+void init_particle(const Mat &m, P &p) {
+    switch (m.model) {
+    case DRUCKER_PRAGER:  // sand.rs:237-246
+        p.friction_hardening = m.hardening_peak > 0.0f ? m.friction_residual / m.hardening_peak
+                                                       : 0.0f;
+        break;
+    case SNOW:  // snow.rs:104-107
+        p.plastic_volume_ratio = 1.0f;
+        p.hardening_scale = 1.0f;
+        break;
+    case NACC:  // nacc.rs:271-273
+        p.log_volume_strain = 0.0f;
+        break;
+    default:
+        break;
+    }
+}
+
+// Shared tail of the elastoplastic updates: volume/density from J.
+inline void sync_volume_density(P &p, M2 f) {
+    float j = fmax_(det(f), MIN_J);
+    float v = fmax_(p.initial_volume * j, 1.0e-6f);
+    p.volume = v;
+    p.density = p.mass / v;
+}
+
+// MaterialModel::update_particle
+void update_particle(const Mat &m, P &p, float dt) {
+    switch (m.model) {
+    case NEOHOOKEAN: {  // elastic.rs:262-269
+        M2 fp_new = madd(ident(), smscale(dt, load_m(p.c)));
+        M2 f = mm(fp_new, load_m(p.f));
+        store_m(p.f, f);
+        sync_volume_density(p, f);
+        break;
+    }
+    case FLUID: {  // fluid.rs:197-207
+        float j = fclamp(det(load_m(p.f)), 0.5f, 2.0f);
+        float s = std::sqrt(j);
+        store_m(p.f, m2(v2(s, 0.0f), v2(0.0f, s)));
+        if (m.settling_damping > 0.0f) {
+            float k = 1.0f - fmin_(m.settling_damping * dt, 0.5f);
+            p.v[0] *= k;
+            p.v[1] *= k;
+        }
+        break;
+    }
+    case DRUCKER_PRAGER: {  // sand.rs:248-319
+        M2 f_trial = mm(madd(ident(), smscale(dt, load_m(p.c))), load_m(p.f));
+        M2 u, vt;
+        V2 sigma;
+        svd2(f_trial, u, sigma, vt);
+        V2 new_sigma = sigma;
+        V2 proj;
+        float dq;
+        if (dp_project(m, sigma, p.log_volume_strain, p.friction_hardening, proj, dq)) {
+            V2 sigma_abs = vmax(vabs(sigma), splat(LOG_CLAMP));
+            float prev_det = sigma_abs.x * sigma_abs.y;
+            float new_det = proj.x * proj.y;
+            float diff = new_det - prev_det;
+            float corrected = diff > 0.0f ? new_det : prev_det + diff * m.volume_correction;
+            p.log_volume_strain += std::log(prev_det) - std::log(corrected);
+            float q_max = 5.0f / fmax_(m.hardening_decay, 1e-6f);
+            p.friction_hardening = fmin_(p.friction_hardening + dq, q_max);
+            if (m.dilatancy_angle > 0.0f) p.log_volume_strain += std::sin(m.dilatancy_angle) * dq;
+            new_sigma = proj;
+        }
+        new_sigma = vabs(new_sigma);
+        float j_new = new_sigma.x * new_sigma.y;
+        if (j_new < m.min_volume_jacobian)
+            new_sigma = muls(new_sigma, std::sqrt(m.min_volume_jacobian / fmax_(j_new, 1e-6f)));
+        M2 f = mm(mm(u, diag(new_sigma)), vt);
+        store_m(p.f, f);
+        sync_volume_density(p, f);
+        break;
+    }
+    case SNOW: {  // snow.rs:142-176
+        M2 f_trial = mm(madd(ident(), smscale(dt, load_m(p.c))), load_m(p.f));
+        M2 u, vt;
+        V2 sigma;
+        svd2(f_trial, u, sigma, vt);
+        float lo = 1.0f - m.compression_limit, hi = 1.0f + m.stretch_limit;
+        V2 sigma_c = v2(fclamp(sigma.x, lo, hi), fclamp(sigma.y, lo, hi));
+        float jp_new = p.plastic_volume_ratio * (sigma.x * sigma.y) / (sigma_c.x * sigma_c.y);
+        p.plastic_volume_ratio = fclamp(jp_new, m.min_plastic_jacobian, m.max_plastic_jacobian);
+        p.hardening_scale =
+            fclamp(std::exp(m.hardening_exponent * (1.0f - p.plastic_volume_ratio)), 0.1f, 7.0f);
+        M2 f = mm(mm(u, diag(sigma_c)), vt);
+        store_m(p.f, f);
+        sync_volume_density(p, f);
+        break;
+    }
+    case NACC: {  // nacc.rs:255-269
+        M2 nf;
+        float na;
+        nacc_project(m, load_m(p.f), p.log_volume_strain, nf, na);
+        store_m(p.f, nf);
+        p.log_volume_strain = na;
+        float j = fmax_(det(nf), MIN_J);
+        float vol = p.initial_volume * j;
+        p.volume = vol;
+        p.density = vol > MIN_J ? p.mass / vol : p.density;
+        break;
+    }
+    default:
+        break;
+    }
+}
+
+inline bool needs_density_recompute(const Mat &m) { return m.model == FLUID; }
+
+// ---------------------------------------------------------------- boundary
+// apply_slip_wall_velocity (forces/boundary/mod.rs:78-101)
+inline void slip_velocity(size_t thickness, size_t cell_index, size_t res, V2 &v) {
+    size_t hi = res - (thickness + 1);
+    size_t x = cell_index / res;
+    size_t y = cell_index % res;
+    if (x < thickness) v.x = fmax_(v.x, 0.0f);
+    if (x > hi) v.x = fmin_(v.x, 0.0f);
+    if (y < thickness) v.y = fmax_(v.y, 0.0f);
+    if (y > hi) v.y = fmin_(v.y, 0.0f);
+}
+
+inline size_t sat_sub(size_t a, size_t b) { return a > b ? a - b : 0; }
+
+// clamp_position_inside_grid (forces/boundary/mod.rs:103-111)
+inline V2 clamp_position(size_t thickness, V2 pos, size_t res) {
+    float mn = static_cast<float>(sat_sub(thickness, 1));
+    float mx = static_cast<float>(sat_sub(res, thickness));
+    return vclamp(pos, splat(mn), splat(mx));
+}
+
+// ---------------------------------------------------------------- grid/mod.rs
+struct Grid {
+    size_t res = 0;
+    std::vector<float> mass;
+    std::vector<V2> mom;
+    std::vector<uint8_t> touched;
+    std::vector<uint32_t> dirty;  // first-touch order (mod.rs:127)
+
+    void init(size_t r) {
+        res = r;
+        mass.assign(r * r, 0.0f);
+        mom.assign(r * r, v2(0, 0));
+        touched.assign(r * r, 0);
+        dirty.clear();
+    }
+    // Grid::clear (mod.rs:167-180)
+    void clear() {
+        for (uint32_t idx : dirty) {
+            mass[idx] = 0.0f;
+            mom[idx] = v2(0, 0);
+            touched[idx] = 0;
+        }
+        dirty.clear();
+    }
+    // flat_index (mod.rs:89-99)
+    bool flat_index(IV2 c, uint32_t &idx) const {
+        if (c.x < 0 || c.y < 0) return false;
+        size_t x = static_cast<size_t>(c.x), y = static_cast<size_t>(c.y);
+        if (x >= res || y >= res) return false;
+        idx = static_cast<uint32_t>(x * res + y);
+        return true;
+    }
+    // add_mass_momentum / accumulate (mod.rs:190-212)
+    void add(IV2 c, float m, V2 p) {
+        uint32_t idx;
+        if (!flat_index(c, idx)) return;
+        if (touched[idx]) {
+            mass[idx] += m;
+            mom[idx] = add2(mom[idx], p);
+        } else {
+            touched[idx] = 1;
+            dirty.push_back(idx);
+            mass[idx] = m;
+            mom[idx] = p;
+        }
+    }
+    static V2 add2(V2 a, V2 b) { return ::add(a, b); }
+    // velocity_at (mod.rs:215-227): zero for out-of-domain and untouched cells.
+    V2 velocity_at(IV2 c) const {
+        uint32_t idx;
+        if (!flat_index(c, idx)) return v2(0, 0);
+        return touched[idx] ? mom[idx] : v2(0, 0);
+    }
+    float mass_at(IV2 c) const {
+        uint32_t idx;
+        if (!flat_index(c, idx)) return 0.0f;
+        return touched[idx] ? mass[idx] : 0.0f;
+    }
+};
+
+}  // namespace
+
+// ---------------------------------------------------------------- Simulation
+struct oracle_sim {
+    oracle_config cfg{};
+    std::vector<P> p;
+    size_t active_count = 0;
+    uint32_t next_tag = 1;
+    std::vector<Mat> materials;
+    std::vector<size_t> boundaries;  // slip thicknesses, in application order
+    Grid grid;
+    float last_step_dt = 0.0f;
+    size_t last_substeps = 0;
+    size_t last_vel_clamp_count = 0;
+    size_t last_j_projection_count = 0;
+    float last_sim_time_dropped = 0.0f;
+    double timing[7] = {0, 0, 0, 0, 0, 0, 0};
+
+    // MaterialRegistry::get (registry.rs:66-76): unknown ids fall back to slot 0.
+    const Mat &mat(uint32_t id) const {
+        return id < materials.size() ? materials[id] : materials[0];
+    }
+    bool any_needs_density() const {
+        for (const Mat &m : materials)
+            if (needs_density_recompute(m)) return true;
+        return false;
+    }
+};
+
+namespace {
+
+using clk = std::chrono::steady_clock;
+inline double us_since(clk::time_point t) {
+    return std::chrono::duration<double, std::micro>(clk::now() - t).count();
+}
+
+// SimConfig::validate (config.rs:247-299)
+bool validate_config(const oracle_config &c) {
+    if (c.grid_res < 4) return false;
+    if (!(c.grid_cell_size > 0.0f)) return false;
+    if (!(c.dt > 0.0f)) return false;
+    if (!(c.cfl_coefficient > 0.0f)) return false;
+    if (!(c.material_cfl_coefficient > 0.0f)) return false;
+    if (!(c.viscous_timestep_coefficient > 0.0f)) return false;
+    if (!(c.min_dt > 0.0f)) return false;
+    if (!(c.min_dt <= c.dt)) return false;
+    if (!(c.projection_min_density > 0.0f)) return false;
+    if (!(c.projection_min_volume > 0.0f)) return false;
+    if (!(c.projection_min_deformation_j > 0.0f)) return false;
+    if (!(c.particle_mass > 0.0f)) return false;
+    if (!(c.contact_friction >= 0.0f)) return false;
+    if (c.max_substeps_per_step == 0) return false;
+    if (!(c.default_initial_volume > 0.0f)) return false;
+    if (!(c.j_max > 1.0f)) return false;
+    if (!(c.apic_blend >= 0.0f && c.apic_blend <= 1.0f)) return false;
+    if (!(c.boundary_thickness > 0 && c.boundary_thickness < c.grid_res - 1)) return false;
+    return true;
+}
+
+// SpawnRegion::fits_in_sim (config.rs:472-482) + validate_for_sim (:485-505)
+bool spawn_fits(const oracle_spawn &s, const oracle_config &c) {
+    if (!(s.spacing > 0.0f) || s.box_size[0] <= 0 || s.box_size[1] <= 0) return false;
+    V2 half = muls(v2(static_cast<float>(s.box_size[0]), static_cast<float>(s.box_size[1])), 0.5f);
+    V2 mn = sub(v2(s.box_center[0], s.box_center[1]), half);
+    V2 mx = add(v2(s.box_center[0], s.box_center[1]), half);
+    float dmin = static_cast<float>(c.boundary_thickness);
+    float dmax = static_cast<float>(sat_sub(c.grid_res, c.boundary_thickness));
+    return mn.x >= dmin && mn.y >= dmin && mx.x <= dmax && mx.y <= dmax;
+}
+
+// LcgRng (spacetime/solver/mod.rs:154-175)
+struct Lcg {
+    uint32_t state;
+    uint32_t next_u32() {
+        state = state * 1664525u + 1013904223u;
+        return state;
+    }
+    float next_f32() { return static_cast<float>(next_u32()) / 4294967296.0f; }
+};
+
+// initialize_particles (spacetime/solver/mod.rs:88-151)
+std::vector<P> initialize_particles(const oracle_config &c, const oracle_spawn &s, Lcg &rng) {
+    float mass = s.has_mass_override ? s.mass_override : c.particle_mass;
+    std::vector<P> out;
+    V2 half = muls(v2(static_cast<float>(s.box_size[0]), static_cast<float>(s.box_size[1])), 0.5f);
+    V2 center = v2(s.box_center[0], s.box_center[1]);
+    V2 mn = sub(center, half);
+    V2 mx = add(center, half);
+    float i = mn.x;
+    while (i < mx.x) {
+        float j = mn.y;
+        while (j < mx.y) {
+            V2 pos = v2(i, j);
+            bool inside = true;
+            if (s.shape == 1) inside = length(sub(pos, center)) <= s.disk_radius;
+            if (inside) {
+                float jitter_mag = s.position_jitter * s.spacing;
+                float jx = (rng.next_f32() - 0.5f) * 2.0f * jitter_mag;
+                float jy = (rng.next_f32() - 0.5f) * 2.0f * jitter_mag;
+                V2 jittered = add(pos, v2(jx, jy));
+                float rx = rng.next_f32();
+                float ry = rng.next_f32();
+                V2 vel = muls(sub(v2(rx, ry), splat(0.5f)), s.initial_velocity_scale);
+                P q;
+                std::memset(&q, 0, sizeof(q));
+                store_v(q.x, jittered);
+                store_v(q.v, vel);
+                std::memcpy(q.f, s.initial_deformation_gradient, sizeof(q.f));
+                q.mass = mass;
+                q.initial_volume = c.default_initial_volume;
+                q.volume = c.default_initial_volume;
+                q.density = mass / c.default_initial_volume;
+                q.material_id = s.material_id;
+                q.plastic_volume_ratio = 1.0f;
+                q.hardening_scale = 1.0f;
+                out.push_back(q);
+            }
+            j += s.spacing;
+        }
+        i += s.spacing;
+    }
+    return out;
+}
+
+// scatter_particle_mass (transfer/p2g.rs:230-243) over [0, count)
+void scatter_particle_mass(oracle_sim &s, size_t count) {
+    for (size_t i = 0; i < count; ++i) {
+        V2 x = load_v(s.p[i].x);
+        float mass = s.p[i].mass;
+        QW w = quadratic_weights(x);
+        for (int gx = 0; gx < 3; ++gx)
+            for (int gy = 0; gy < 3; ++gy) {
+                float weight = w.wx[gx] * w.wy[gy];
+                IV2 cell{w.base.x + gx - 1, w.base.y + gy - 1};
+                s.grid.add(cell, weight * mass, v2(0, 0));
+            }
+    }
+}
+
+// Density gather shared by estimate_particle_volumes / _local (density.rs:50-71,122-143)
+void gather_density(oracle_sim &s, size_t lo, size_t hi, bool write_initial) {
+    for (size_t i = lo; i < hi; ++i) {
+        P &q = s.p[i];
+        V2 x = load_v(q.x);
+        float mass = q.mass;
+        QW w = quadratic_weights(x);
+        float density = 0.0f;
+        for (int gx = 0; gx < 3; ++gx)
+            for (int gy = 0; gy < 3; ++gy) {
+                float weight = w.wx[gx] * w.wy[gy];
+                IV2 cell{w.base.x + gx - 1, w.base.y + gy - 1};
+                density += s.grid.mass_at(cell) * weight;
+            }
+        if (density > F32_EPS) {
+            q.density = density;
+            q.volume = mass / density;
+            if (write_initial) q.initial_volume = q.volume;
+        }
+    }
+}
+
+// estimate_particle_volumes (density.rs:41-72)
+void estimate_particle_volumes(oracle_sim &s, size_t count, bool write_initial) {
+    s.grid.clear();
+    scatter_particle_mass(s, count);
+    gather_density(s, 0, count, write_initial);
+}
+
+// estimate_particle_volumes_local (density.rs:81-144)
+void estimate_particle_volumes_local(oracle_sim &s, size_t active, size_t new_start,
+                                     bool write_initial) {
+    if (new_start >= active) return;
+    V2 lo = splat(std::numeric_limits<float>::max());
+    V2 hi = splat(std::numeric_limits<float>::lowest());
+    for (size_t i = new_start; i < active; ++i) {
+        lo = vmin(lo, load_v(s.p[i].x));
+        hi = vmax(hi, load_v(s.p[i].x));
+    }
+    const float MARGIN = 3.0f;
+    lo = sub(lo, splat(MARGIN));
+    hi = add(hi, splat(MARGIN));
+    s.grid.clear();
+    for (size_t i = 0; i < active; ++i) {
+        V2 x = load_v(s.p[i].x);
+        if (x.x < lo.x || x.y < lo.y || x.x > hi.x || x.y > hi.y) continue;
+        float mass = s.p[i].mass;
+        QW w = quadratic_weights(x);
+        for (int gx = 0; gx < 3; ++gx)
+            for (int gy = 0; gy < 3; ++gy) {
+                float weight = w.wx[gx] * w.wy[gy];
+                IV2 cell{w.base.x + gx - 1, w.base.y + gy - 1};
+                s.grid.add(cell, weight * mass, v2(0, 0));
+            }
+    }
+    gather_density(s, new_start, active, write_initial);
+}
+
+// affine_cfl_speed_contribution (step.rs:481-488)
+inline float affine_cfl(M2 c, float cell) {
+    const float STENCIL_CORNER_DISTANCE = 1.5f * 1.41421356f;
+    float grad_norm = std::sqrt(length_sq(c.xa) + length_sq(c.ya));
+    return grad_norm * STENCIL_CORNER_DISTANCE * cell;
+}
+
+// cfl_bound (step.rs:472-479)
+float cfl_bound(const oracle_config &c, float max_speed, float min_mat_dt, float max_dt) {
+    float dt = max_dt;
+    if (max_speed > F32_EPS) dt = fmin_(dt, c.cfl_coefficient * c.grid_cell_size / max_speed);
+    dt = fmin_(dt, min_mat_dt);
+    return fclamp(dt, fmin_(c.min_dt, max_dt), max_dt);
+}
+
+// choose_substep_dt (step.rs:434-468)
+float choose_substep_dt(const oracle_sim &s, float max_dt) {
+    const oracle_config &c = s.cfg;
+    if (!c.adaptive_timestep) return fmin_(max_dt, c.dt);
+    float max_speed = 0.0f;
+    float min_mat_dt = max_dt;
+    for (size_t i = 0; i < s.active_count; ++i) {
+        const P &q = s.p[i];
+        float sp = length(load_v(q.v));
+        if (c.cfl_include_affine_speed) sp += affine_cfl(load_m(q.c), c.grid_cell_size);
+        max_speed = fmax_(max_speed, sp);
+        float mdt = timestep_bound(s.mat(q.material_id), q.density, q.hardening_scale,
+                                   c.grid_cell_size, c.material_cfl_coefficient,
+                                   c.viscous_timestep_coefficient);
+        if (std::isfinite(mdt) && mdt > 0.0f) min_mat_dt = fmin_(min_mat_dt, mdt);
+    }
+    return cfl_bound(c, max_speed, min_mat_dt, max_dt);
+}
+
+// project_particle_state_to_admissible (step.rs:347-429)
+bool project_particle(const oracle_config &c, P &q) {
+    bool projected = false;
+    float mn = static_cast<float>(sat_sub(c.boundary_thickness, 1));
+    float mx = static_cast<float>(sat_sub(c.grid_res, c.boundary_thickness));
+    V2 center = splat((mn + mx) * 0.5f);
+    V2 x = load_v(q.x);
+    if (!finite2(x)) {
+        store_v(q.x, center);
+        projected = true;
+    } else {
+        store_v(q.x, vclamp(x, splat(mn), splat(mx)));
+    }
+    if (!finite2(load_v(q.v))) {
+        store_v(q.v, v2(0, 0));
+        projected = true;
+    }
+    if (!finite_m(load_m(q.c))) {
+        store_m(q.c, zero2());
+        projected = true;
+    }
+    M2 f = load_m(q.f);
+    if (!finite_m(f) || det(f) <= c.projection_min_deformation_j) {
+        store_m(q.f, ident());
+        projected = true;
+    } else {
+        float j = det(f);
+        if (j > c.j_max) {
+            store_m(q.f, mscale(f, std::sqrt(c.j_max / j)));
+            projected = true;
+        }
+    }
+    if (!std::isfinite(q.plastic_volume_ratio) || q.plastic_volume_ratio <= 0.0f) {
+        q.plastic_volume_ratio = 1.0f;
+        projected = true;
+    }
+    if (!std::isfinite(q.hardening_scale) || q.hardening_scale <= 0.0f) {
+        q.hardening_scale = 1.0f;
+        projected = true;
+    }
+    if (!std::isfinite(q.friction_hardening)) {
+        q.friction_hardening = 0.0f;
+        projected = true;
+    }
+    if (!std::isfinite(q.log_volume_strain)) {
+        q.log_volume_strain = 0.0f;
+        projected = true;
+    }
+    if (!std::isfinite(q.mass) || q.mass <= 0.0f) {
+        q.mass = c.particle_mass;
+        projected = true;
+    }
+    if (!std::isfinite(q.initial_volume) || q.initial_volume <= 0.0f) {
+        q.initial_volume = fmax_(c.default_initial_volume, c.projection_min_volume);
+        projected = true;
+    }
+    if (!std::isfinite(q.volume) || q.volume <= 0.0f) {
+        q.volume = fmax_(q.initial_volume, c.projection_min_volume);
+        projected = true;
+    }
+    if (!std::isfinite(q.density) || q.density <= 0.0f) {
+        q.density = fmax_(q.mass / q.volume, c.projection_min_density);
+        projected = true;
+    } else {
+        q.density = fmax_(q.density, c.projection_min_density);
+    }
+    return projected;
+}
+
+// scatter_particles_to_grid (transfer/p2g.rs:24-72); contact and mixture scatters are
+// gated off (contact_group == 0, no mixture phase) for every supported scene.
+void p2g(oracle_sim &s, float dt) {
+    for (size_t i = 0; i < s.active_count; ++i) {
+        const P &q = s.p[i];
+        const Mat &m = s.mat(q.material_id);
+        V2 x = load_v(q.x);
+        float mass_i = q.mass;
+        V2 v_i = load_v(q.v);
+        M2 c_i = load_m(q.c);
+        M2 stress = combined_kirchhoff_stress(m, q);
+        float stress_coeff = -stress_volume(m, q) * KERNEL_D_INVERSE * dt;
+        QW w = quadratic_weights(x);
+        for (int gx = 0; gx < 3; ++gx)
+            for (int gy = 0; gy < 3; ++gy) {
+                float weight = w.wx[gx] * w.wy[gy];
+                IV2 cell{w.base.x + gx - 1, w.base.y + gy - 1};
+                V2 cell_dist = add(sub(v2(static_cast<float>(cell.x), static_cast<float>(cell.y)), x),
+                                   splat(0.5f));
+                V2 momentum = smul(weight, add(smul(mass_i, add(v_i, mv(c_i, cell_dist))),
+                                               smul(stress_coeff, mv(stress, cell_dist))));
+                s.grid.add(cell, weight * mass_i, momentum);
+            }
+    }
+}
+
+// Grid::update_velocities (grid/mod.rs:264-291) + boundaries (step.rs:150-152, 334-344)
+// + grid speed clamp (step.rs:155-165)
+void grid_update(oracle_sim &s, float dt) {
+    Grid &g = s.grid;
+    V2 grav = v2(s.cfg.gravity[0], s.cfg.gravity[1]);
+    for (uint32_t idx : g.dirty)
+        if (g.mass[idx] > 0.0f) g.mom[idx] = divs(g.mom[idx], g.mass[idx]);
+    for (uint32_t idx : g.dirty)
+        if (g.mass[idx] > 0.0f) g.mom[idx] = add(g.mom[idx], muls(grav, dt));
+    size_t res = g.res;
+    for (size_t t : s.boundaries)
+        for (uint32_t idx : g.dirty)
+            if (g.mass[idx] > 0.0f) slip_velocity(t, idx, res, g.mom[idx]);
+    float vel_limit = s.cfg.grid_cell_size / dt;
+    for (uint32_t idx : g.dirty) {
+        if (g.mass[idx] > 0.0f) {
+            float spd = length(g.mom[idx]);
+            if (spd > vel_limit) g.mom[idx] = muls(g.mom[idx], vel_limit / spd);
+        }
+    }
+}
+
+// gather_grid_to_particles (transfer/g2p.rs:151-343) with ASFLIP, contact and mixture
+// gated off (asflip_blend = 0, no grip or mixture particles).
+size_t g2p(oracle_sim &s, float dt) {
+    const float vel_limit = s.cfg.grid_cell_size / dt;
+    const float apic_blend = s.cfg.apic_blend;
+    const size_t res = s.grid.res;
+    const long n = static_cast<long>(s.active_count);
+    std::vector<size_t> clamp_counts(static_cast<size_t>(n > 0 ? n : 0), 0);
+    // Phase 1 (g2p.rs:189-328): independent per particle -> parallel, as rayon does.
+    parallel_for(n, [&](long lo, long hi) {
+        for (long ii = lo; ii < hi; ++ii) {
+            P &q = s.p[static_cast<size_t>(ii)];
+            V2 x = load_v(q.x);
+            QW w = quadratic_weights(x);
+            V2 new_v = v2(0, 0);
+            M2 b = zero2();
+            for (int gx = 0; gx < 3; ++gx)
+                for (int gy = 0; gy < 3; ++gy) {
+                    float weight = w.wx[gx] * w.wy[gy];
+                    IV2 cell{w.base.x + gx - 1, w.base.y + gy - 1};
+                    V2 dist = add(sub(v2(static_cast<float>(cell.x), static_cast<float>(cell.y)), x),
+                                  splat(0.5f));
+                    V2 node_v = s.grid.velocity_at(cell);
+                    V2 wv = muls(node_v, weight);
+                    M2 term = m2(muls(wv, dist.x), muls(wv, dist.y));
+                    b = madd(b, term);
+                    new_v = add(new_v, wv);
+                }
+            if (q.pinned != 0) {
+                store_v(q.v, v2(0, 0));
+                store_m(q.c, zero2());
+                continue;
+            }
+            V2 v_store = new_v, v_pos = new_v;
+            float spd = length(v_store);
+            if (spd > vel_limit) {
+                float scale = vel_limit / spd;
+                v_store = muls(v_store, scale);
+                v_pos = muls(v_pos, scale);
+                clamp_counts[static_cast<size_t>(ii)] = 1;
+            }
+            V2 new_pos = add(x, muls(v_pos, dt));
+            for (size_t t : s.boundaries) new_pos = clamp_position(t, new_pos, res);
+            store_v(q.v, v_store);
+            store_m(q.c, mscale(mscale(b, KERNEL_D_INVERSE), apic_blend));
+            store_v(q.x, new_pos);
+        }
+    });
+    size_t clamp_count = 0;
+    for (size_t c : clamp_counts) clamp_count += c;
+    // Phase 2 (g2p.rs:333-340): sequential constitutive update.
+    for (size_t i = 0; i < s.active_count; ++i) update_particle(s.mat(s.p[i].material_id), s.p[i], dt);
+    return clamp_count;
+}
+
+// Simulation::do_substep (step.rs:62-317) restricted to the gated-on phases.
+void do_substep(oracle_sim &s, float sub_dt) {
+    auto t0 = clk::now();
+    if (s.cfg.project_invalid_state)
+        for (size_t i = 0; i < s.active_count; ++i)
+            if (project_particle(s.cfg, s.p[i])) s.last_j_projection_count += 1;
+    s.timing[1] += us_since(t0);
+    t0 = clk::now();
+    if (s.cfg.recompute_density_each_step || s.any_needs_density())
+        estimate_particle_volumes(s, s.active_count, false);
+    s.timing[2] += us_since(t0);
+    t0 = clk::now();
+    s.grid.clear();
+    p2g(s, sub_dt);
+    s.timing[3] += us_since(t0);
+    t0 = clk::now();
+    grid_update(s, sub_dt);
+    s.timing[4] += us_since(t0);
+    t0 = clk::now();
+    s.last_vel_clamp_count += g2p(s, sub_dt);
+    s.timing[5] += us_since(t0);
+}
+
+// Simulation::step (step.rs:23-60)
+void step_once(oracle_sim &s) {
+    auto t_start = clk::now();
+    for (double &t : s.timing) t = 0.0;
+    float remaining = s.cfg.dt;
+    size_t substeps = 0;
+    s.last_vel_clamp_count = 0;
+    s.last_j_projection_count = 0;
+    while (remaining > F32_EPS && substeps < s.cfg.max_substeps_per_step) {
+        auto t_cfl = clk::now();
+        float sub_dt = choose_substep_dt(s, remaining);
+        s.timing[0] += us_since(t_cfl);
+        do_substep(s, sub_dt);
+        remaining -= sub_dt;
+        s.last_step_dt = sub_dt;
+        substeps += 1;
+    }
+    s.last_substeps = substeps;
+    s.last_sim_time_dropped = fmax_(remaining, 0.0f);
+    s.timing[6] = us_since(t_start);
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------- C API
+extern "C" {
+
+oracle_sim *oracle_create(const oracle_config *cfg) {
+    if (!cfg || !validate_config(*cfg)) return nullptr;
+    oracle_sim *s = new oracle_sim();
+    s->cfg = *cfg;
+    Mat fallback;
+    std::memset(&fallback, 0, sizeof(fallback));
+    fallback.model = FALLBACK;
+    s->materials.push_back(fallback);
+    s->boundaries.push_back(static_cast<size_t>(cfg->boundary_thickness));
+    s->grid.init(static_cast<size_t>(cfg->grid_res));
+    s->last_step_dt = cfg->dt;
+    return s;
+}
+
+void oracle_destroy(oracle_sim *s) { delete s; }
+
+int oracle_set_material(oracle_sim *s, uint32_t id, const oracle_material *m) {
+    if (id >= MAX_MATERIAL_SLOTS) return -1;
+    if (id < s->materials.size()) {
+        s->materials[id] = *m;
+    } else if (id == s->materials.size()) {
+        s->materials.push_back(*m);
+    } else {
+        return -1;
+    }
+    if (id == 0)  // with_default_material -> reinit_all_particle_state (lifecycle.rs:328-334)
+        for (P &q : s->p) init_particle(s->mat(q.material_id), q);
+    return 0;
+}
+
+int oracle_add_slip_boundary(oracle_sim *s, uint64_t thickness, int clear_first) {
+    if (clear_first) s->boundaries.clear();
+    s->boundaries.push_back(static_cast<size_t>(thickness));
+    return 0;
+}
+
+int oracle_add_body(oracle_sim *s, const oracle_spawn *spawn, uint32_t *tag_out) {
+    if (!spawn_fits(*spawn, s->cfg)) return -1;
+    uint32_t tag = s->next_tag++;
+    size_t old_active = s->active_count;
+    Lcg rng{spawn->rng_seed};
+    std::vector<P> np = initialize_particles(s->cfg, *spawn, rng);
+    bool registered = spawn->material_id < s->materials.size();
+    for (P &q : np) {
+        q.user_tag = tag;
+        if (registered) init_particle(s->materials[spawn->material_id], q);
+    }
+    // No sleeping partition (sleep_threshold = 0): new particles append at the end.
+    s->p.insert(s->p.end(), np.begin(), np.end());
+    s->active_count = s->p.size();
+    estimate_particle_volumes_local(*s, s->active_count, old_active, true);
+    if (tag_out) *tag_out = tag;
+    return 0;
+}
+
+int oracle_init_with_spawn(oracle_sim *s, const oracle_spawn *spawn) {
+    if (!spawn_fits(*spawn, s->cfg) || !s->p.empty()) return -1;
+    Lcg rng{spawn->rng_seed};
+    s->p = initialize_particles(s->cfg, *spawn, rng);
+    s->active_count = s->p.size();
+    if (spawn->precompute_initial_volumes) estimate_particle_volumes(*s, s->p.size(), true);
+    return 0;
+}
+
+int oracle_push_particles(oracle_sim *s, const oracle_particle *p, uint64_t n) {
+    s->p.insert(s->p.end(), p, p + n);
+    s->active_count = s->p.size();
+    return 0;
+}
+
+void oracle_step(oracle_sim *s, uint32_t n_steps) {
+    for (uint32_t k = 0; k < n_steps; ++k) step_once(*s);
+}
+
+uint64_t oracle_particle_count(const oracle_sim *s) { return s->p.size(); }
+
+void oracle_read_particles(const oracle_sim *s, oracle_particle *out) {
+    std::memcpy(out, s->p.data(), s->p.size() * sizeof(P));
+}
+
+void oracle_write_particles(oracle_sim *s, const oracle_particle *in) {
+    std::memcpy(s->p.data(), in, s->p.size() * sizeof(P));
+}
+
+// region_state (spacetime/solver/queries.rs:125-141): candidates in SpatialHash
+// iteration order (spatial_hash.rs:47-105: cells gx outer, gy inner, each bucket in
+// particle index order), exact |x-c|^2 <= r^2 filter, BodyState::accumulate/finalize
+// (query.rs:123-142).
+void oracle_region_state(const oracle_sim *s, float cx, float cy, float r,
+                         oracle_body_state *out) {
+    float inv_cell = 1.0f / s->cfg.grid_cell_size;
+    auto cell_of = [&](V2 pp) {
+        return std::make_pair(f2i_sat(std::floor(pp.x * inv_cell)),
+                              f2i_sat(std::floor(pp.y * inv_cell)));
+    };
+    std::map<std::pair<int32_t, int32_t>, std::vector<size_t>> table;
+    for (size_t i = 0; i < s->active_count; ++i) table[cell_of(load_v(s->p[i].x))].push_back(i);
+    V2 center = v2(cx, cy);
+    int32_t r_cells = f2i_sat(std::ceil(r * inv_cell));
+    auto cc = cell_of(center);
+    float r2 = r * r;
+    uint64_t count = 0;
+    V2 centroid = v2(0, 0);
+    float avg_speed = 0, avg_vr = 0, max_vr = 0, avg_det = 0, avg_den = 0;
+    for (int32_t gx = -r_cells; gx <= r_cells; ++gx)
+        for (int32_t gy = -r_cells; gy <= r_cells; ++gy) {
+            auto it = table.find(std::make_pair(cc.first + gx, cc.second + gy));
+            if (it == table.end()) continue;
+            for (size_t i : it->second) {
+                const P &q = s->p[i];
+                V2 x = load_v(q.x);
+                if (length_sq(sub(x, center)) <= r2) {
+                    count += 1;
+                    centroid = add(centroid, x);
+                    avg_speed += length(load_v(q.v));
+                    avg_vr += q.plastic_volume_ratio;
+                    max_vr = fmax_(max_vr, q.plastic_volume_ratio);
+                    avg_det += det(load_m(q.f));
+                    avg_den += q.density;
+                }
+            }
+        }
+    if (count > 0) {
+        float n = static_cast<float>(count);
+        centroid = divs(centroid, n);
+        avg_speed /= n;
+        avg_vr /= n;
+        avg_det /= n;
+        avg_den /= n;
+    }
+    std::memset(out, 0, sizeof(*out));
+    out->count = count;
+    out->avg_volume_ratio = avg_vr;
+    out->max_volume_ratio = max_vr;
+    out->avg_speed = avg_speed;
+    out->avg_det_f = avg_det;
+    out->avg_density = avg_den;
+    out->centroid[0] = centroid.x;
+    out->centroid[1] = centroid.y;
+}
+
+float oracle_effective_dt(const oracle_sim *s) { return s->last_step_dt; }
+uint64_t oracle_last_substeps(const oracle_sim *s) { return s->last_substeps; }
+uint64_t oracle_last_vel_clamp_count(const oracle_sim *s) { return s->last_vel_clamp_count; }
+uint64_t oracle_last_j_projection_count(const oracle_sim *s) { return s->last_j_projection_count; }
+void oracle_last_timing_us(const oracle_sim *s, double out[7]) {
+    for (int i = 0; i < 7; ++i) out[i] = s->timing[i];
+}
+
+int oracle_set_threads(int n) {
+    if (n >= 0) g_threads = n;
+    return g_threads > 0 ? g_threads : static_cast<int>(std::thread::hardware_concurrency());
+}
+
+void oracle_svd2(const float f[4], float u[4], float sigma[2], float vt[4]) {
+    M2 uu, vv;
+    V2 ss;
+    svd2(load_m(f), uu, ss, vv);
+    store_m(u, uu);
+    store_v(sigma, ss);
+    store_m(vt, vv);
+}
+
+void oracle_polar(const float f[4], float r[4]) { store_m(r, polar(load_m(f))); }
+
+void oracle_axis_weights(float d, float w[3]) { axis_weights(d, w); }
+
+void oracle_kirchhoff(const oracle_material *m, const oracle_particle *p, float tau[4]) {
+    store_m(tau, combined_kirchhoff_stress(*m, *p));
+}
+
+void oracle_update_particle(const oracle_material *m, oracle_particle *p, float dt) {
+    update_particle(*m, *p, dt);
+}
+
+void oracle_init_particle(const oracle_material *m, oracle_particle *p) { init_particle(*m, *p); }
+
+float oracle_timestep_bound(const oracle_material *m, float density, float h, float cell,
+                            float mat_cfl, float visc_cfl) {
+    return timestep_bound(*m, density, h, cell, mat_cfl, visc_cfl);
+}
+
+void oracle_nacc_project(const oracle_material *m, const float f[4], float alpha, float f_out[4],
+                         float *alpha_out) {
+    M2 nf;
+    nacc_project(*m, load_m(f), alpha, nf, *alpha_out);
+    store_m(f_out, nf);
+}
+
+int oracle_dp_project(const oracle_material *m, const float sigma[2], float lvs, float q,
+                      float sigma_out[2], float *dq_out) {
+    V2 o;
+    float dq = 0.0f;
+    bool r = dp_project(*m, load_v(sigma), lvs, q, o, dq);
+    if (r) {
+        store_v(sigma_out, o);
+        *dq_out = dq;
+    }
+    return r ? 1 : 0;
+}
+
+void oracle_slip_velocity(uint64_t thickness, uint64_t cell_index, uint64_t res, float v[2]) {
+    V2 vv = load_v(v);
+    slip_velocity(static_cast<size_t>(thickness), static_cast<size_t>(cell_index),
+                  static_cast<size_t>(res), vv);
+    store_v(v, vv);
+}
+
+// block_index (systems/gpu/shaders/particle_sort.wgsl:94-102), NUM_BLOCKS_PER_DIM = 16.
+uint32_t oracle_block_index(float px, float py, uint32_t grid_res) {
+    const uint32_t NB = 16;
+    uint32_t max_cell = grid_res - 1u;
+    float fx = fmin_(fmax_(px, 0.0f), static_cast<float>(max_cell));
+    float fy = fmin_(fmax_(py, 0.0f), static_cast<float>(max_cell));
+    uint32_t cell_x = static_cast<uint32_t>(fx);
+    uint32_t cell_y = static_cast<uint32_t>(fy);
+    uint32_t block_size = (grid_res + NB - 1u) / NB;
+    uint32_t bx = std::min(cell_x / block_size, NB - 1u);
+    uint32_t by = std::min(cell_y / block_size, NB - 1u);
+    return by * NB + bx;
+}
+
+void oracle_stable_argsort_u32(const uint32_t *keys, uint64_t n, uint32_t *perm_out) {
+    std::vector<uint32_t> idx(n);
+    std::iota(idx.begin(), idx.end(), 0u);
+    std::stable_sort(idx.begin(), idx.end(),
+                     [&](uint32_t a, uint32_t b) { return keys[a] < keys[b]; });
+    std::memcpy(perm_out, idx.data(), n * sizeof(uint32_t));
+}
+
+int oracle_project_particle(const oracle_config *cfg, oracle_particle *p) {
+    return project_particle(*cfg, *p) ? 1 : 0;
+}
+
+float oracle_choose_substep_dt(const oracle_sim *s, float max_dt) {
+    return choose_substep_dt(*s, max_dt);
+}
+
+}  // extern "C"
