@@ -31,6 +31,7 @@ STATUS_NAMES = {0: "OK", 1: "INVALID_ARG", 2: "UNSUPPORTED", 3: "CUDA", 4: "TIME
 OPT_USE_GRAPH = 1
 OPT_SORT_INTERVAL = 2
 OPT_P2G_WINDOW = 3
+OPT_DETERMINISTIC = 4
 
 
 class Particle(Structure):

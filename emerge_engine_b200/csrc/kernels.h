@@ -17,7 +17,8 @@ struct LoadFlagsHost {
 };
 
 // step_kernels.cu
-void launch_particle_pass(const StepLaunch &L, const LoadFlagsHost &lf, int mode_g2p);
+void launch_particle_pass(const StepLaunch &L, const LoadFlagsHost &lf, int mode_g2p,
+                          int project_in, int emit_p2g);
 void launch_density_pass(const StepLaunch &L, const LoadFlagsHost &lf);
 void launch_grid_update(const StepLaunch &L);
 void launch_step_begin(const StepLaunch &L);
@@ -37,6 +38,14 @@ void launch_mass_scatter(const DevParticles &P, int n, const GridView &g, int fi
                          float loy, float hix, float hiy, cudaStream_t stream);
 void launch_mass_gather(const DevParticles &P, int lo, int hi, const GridView &g, int write_initial,
                         cudaStream_t stream);
+
+// det_kernels.cu (reference-order mode)
+void launch_project(const StepLaunch &L);
+void launch_det_records(const StepLaunch &L, int mode, uint32_t invalid_key, uint32_t *keys,
+                        uint32_t *vals, float4 *payload, int filter = 0, float lox = 0.f,
+                        float loy = 0.f, float hix = 0.f, float hiy = 0.f);
+void launch_segsum(const uint32_t *keys, const uint32_t *vals, const float4 *payload, int n_rec,
+                   uint32_t invalid_key, const GridView &g, int mass_only, cudaStream_t stream);
 
 // sort.cu
 // Scratch for a stable LSD radix sort of up to `capacity` (key, value) pairs.

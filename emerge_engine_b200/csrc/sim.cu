@@ -22,8 +22,6 @@ namespace {
 
 thread_local std::string g_global_error;
 
-constexpr float F32_EPSILON = 1.1920929e-7f;
-
 struct Buffer {
     void *ptr = nullptr;
     size_t bytes = 0;
@@ -142,6 +140,13 @@ struct emerge_sim {
     uint64_t steps_since_sort = 0;
     bool sorted_once = false;
     unsigned long long fallback_at_sort = 0, blocks_at_sort = 0;
+
+    // reference-order (deterministic) mode
+    int deterministic = 0;
+    Buffer detbuf;
+    SortScratch det_sort;
+    float4 *det_payload = nullptr;
+    size_t det_cap = 0;
 
     // step pipeline
     bool pending_valid = false;  // the next substep's P2G (+density) is already on the grid
@@ -369,7 +374,7 @@ emerge_status build_graph(emerge_sim *s) {
                                      cudaStreamCaptureModeThreadLocal));
     launch_substep_begin(L, 1, static_cast<unsigned long long>(handle), kps);
     launch_grid_update(L);
-    launch_particle_pass(L, s->lf, 1);
+    launch_particle_pass(L, s->lf, 1, L.cfg.project, 1);
     if (L.density_mode) launch_density_pass(L, s->lf);
     CK(cudaStreamEndCapture(s->stream, &body));
     CK(cudaGraphInstantiate(&s->graph_exec, graph, 0));
@@ -380,7 +385,14 @@ emerge_status build_graph(emerge_sim *s) {
 emerge_status prime(emerge_sim *s) {
     StepLaunch L = make_launch(s);
     launch_prime_setup(L);
-    launch_particle_pass(L, s->lf, 0);
+    if (s->deterministic) {  // CFL reduction only; the substep scatters after dt is known
+        launch_particle_pass(L, s->lf, 0, 0, 0);
+        s->host_launches += 2;
+        CK(cudaGetLastError());
+        s->pending_valid = true;
+        return EMERGE_OK;
+    }
+    launch_particle_pass(L, s->lf, 0, 0, 1);
     s->host_launches += 2;
     if (L.density_mode) {
         launch_density_pass(L, s->lf);
@@ -441,7 +453,7 @@ emerge_status run_host_loop_step(emerge_sim *s, bool timed) {
         CK(cudaEventRecord(s->ev[2], s->stream));
         launch_grid_update(L);
         CK(cudaEventRecord(s->ev[3], s->stream));
-        launch_particle_pass(L, s->lf, 1);
+        launch_particle_pass(L, s->lf, 1, L.cfg.project, 1);
         CK(cudaEventRecord(s->ev[4], s->stream));
         s->host_launches += 3;
         if (L.density_mode) {
@@ -474,6 +486,128 @@ emerge_status run_host_loop_step(emerge_sim *s, bool timed) {
         t.grid_update_us = static_cast<uint64_t>(t_grid * 1000.0f);
         t.g2p_us = static_cast<uint64_t>(t_part * 1000.0f);  // fused G2P+update+projection+P2G pass
         t.density_us = static_cast<uint64_t>(t_dens * 1000.0f);
+        t.total_us = static_cast<uint64_t>(tot * 1000.0f);
+    }
+    return EMERGE_OK;
+}
+
+emerge_status ensure_det_scratch(emerge_sim *s) {
+    size_t need = 9 * (s->cap > 0 ? s->cap : 1);
+    if (s->det_cap >= need) return EMERGE_OK;
+    s->detbuf.reset();
+    size_t bytes = sort_scratch_bytes(need) + need * sizeof(float4) + 512;
+    CK(cudaMalloc(&s->detbuf.ptr, bytes));
+    s->detbuf.bytes = bytes;
+    sort_scratch_bind(s->det_sort, s->detbuf.ptr, need);
+    uintptr_t p = reinterpret_cast<uintptr_t>(s->detbuf.ptr) + sort_scratch_bytes(need);
+    p = (p + 255) & ~static_cast<uintptr_t>(255);
+    s->det_payload = reinterpret_cast<float4 *>(p);
+    s->det_cap = need;
+    return EMERGE_OK;
+}
+
+uint32_t det_invalid_key(const emerge_sim *s) {
+    return static_cast<uint32_t>(s->res) * static_cast<uint32_t>(s->res);
+}
+
+int det_key_bits(const emerge_sim *s) {
+    uint64_t top = static_cast<uint64_t>(det_invalid_key(s));
+    int b = 0;
+    while ((1ull << b) <= top) ++b;
+    return b;
+}
+
+// Records -> stable sort by cell -> sequential per-cell sums (see det_kernels.cu).
+emerge_status det_scatter(emerge_sim *s, const StepLaunch &L, int mode, int filter, float lox,
+                          float loy, float hix, float hiy) {
+    emerge_status st = ensure_det_scratch(s);
+    if (st != EMERGE_OK) return st;
+    const uint32_t inv = det_invalid_key(s);
+    const int n_rec = 9 * L.n;
+    launch_det_records(L, mode, inv, s->det_sort.keys[0], s->det_sort.vals[0], s->det_payload, filter,
+                       lox, loy, hix, hiy);
+    int bits = det_key_bits(s);
+    int r = radix_sort_pairs(s->det_sort, n_rec, bits, s->stream);
+    launch_segsum(s->det_sort.keys[r], s->det_sort.vals[r], s->det_payload, n_rec, inv, s->g,
+                  mode == 0 ? 1 : 0, s->stream);
+    s->host_launches += 2 + 5 * ((bits + 7) / 8);
+    CK(cudaGetLastError());
+    return EMERGE_OK;
+}
+
+emerge_status clear_grid(emerge_sim *s) {
+    size_t cells = static_cast<size_t>(s->tpd) * s->tpd * TILE_CELLS;
+    CK(cudaMemsetAsync(s->g.acc_a, 0, cells * sizeof(float4), s->stream));
+    CK(cudaMemsetAsync(s->g.acc_s, 0, cells * sizeof(float2), s->stream));
+    CK(cudaMemsetAsync(s->g.tile_flag, 0, static_cast<size_t>(s->tpd) * s->tpd, s->stream));
+    return EMERGE_OK;
+}
+
+// One Simulation::step in reference order (step.rs:23-60, 62-210), host-driven.
+emerge_status run_det_step(emerge_sim *s, bool timed) {
+    StepLaunch L = make_launch(s);
+    float t_cfl = 0, t_grid = 0, t_part = 0, t_dens = 0, t_p2g = 0, t_proj = 0;
+    if (timed) CK(cudaEventRecord(s->ev[0], s->stream));
+    launch_step_begin(L);
+    s->host_launches += 1;
+    CK(cudaMemcpyAsync(s->h_state, s->d_state, sizeof(StepState), cudaMemcpyDeviceToHost, s->stream));
+    CK(cudaStreamSynchronize(s->stream));
+    emerge_status st = EMERGE_OK;
+    while (s->h_state->cont) {
+        CK(cudaEventRecord(s->ev[1], s->stream));
+        launch_substep_begin(L, 0, 0ull, 0);
+        CK(cudaEventRecord(s->ev[2], s->stream));
+        if (L.cfg.project) launch_project(L);
+        CK(cudaEventRecord(s->ev[3], s->stream));
+        s->host_launches += 2;
+        if (L.density_mode) {  // estimate_particle_volumes(.., false) (density.rs:41-72)
+            st = det_scatter(s, L, 0, 0, 0, 0, 0, 0);
+            if (st != EMERGE_OK) return st;
+            launch_mass_gather(L.P, 0, L.n, L.g, 0, s->stream);
+            s->host_launches += 1;
+            st = clear_grid(s);
+            if (st != EMERGE_OK) return st;
+        }
+        CK(cudaEventRecord(s->ev[4], s->stream));
+        st = det_scatter(s, L, 1, 0, 0, 0, 0, 0);
+        if (st != EMERGE_OK) return st;
+        CK(cudaEventRecord(s->ev[5], s->stream));
+        launch_grid_update(L);
+        CK(cudaEventRecord(s->ev[6], s->stream));
+        launch_particle_pass(L, s->lf, 1, 0, 0);
+        CK(cudaEventRecord(s->ev[7], s->stream));
+        s->host_launches += 2;
+        CK(cudaMemcpyAsync(s->h_state, s->d_state, sizeof(StepState), cudaMemcpyDeviceToHost,
+                           s->stream));
+        CK(cudaStreamSynchronize(s->stream));
+        CK(cudaGetLastError());
+        float a, b, c, d, e, f;
+        cudaEventElapsedTime(&a, s->ev[1], s->ev[2]);
+        cudaEventElapsedTime(&b, s->ev[2], s->ev[3]);
+        cudaEventElapsedTime(&c, s->ev[3], s->ev[4]);
+        cudaEventElapsedTime(&d, s->ev[4], s->ev[5]);
+        cudaEventElapsedTime(&e, s->ev[5], s->ev[6]);
+        cudaEventElapsedTime(&f, s->ev[6], s->ev[7]);
+        t_cfl += a;
+        t_proj += b;
+        t_dens += c;
+        t_p2g += d;
+        t_grid += e;
+        t_part += f;
+    }
+    if (timed) {
+        CK(cudaEventRecord(s->ev[7], s->stream));
+        CK(cudaEventSynchronize(s->ev[7]));
+        float tot;
+        cudaEventElapsedTime(&tot, s->ev[0], s->ev[7]);
+        emerge_step_timing &t = s->last_timing;
+        std::memset(&t, 0, sizeof(t));
+        t.cfl_us = static_cast<uint64_t>(t_cfl * 1000.0f);
+        t.project_us = static_cast<uint64_t>(t_proj * 1000.0f);
+        t.density_us = static_cast<uint64_t>(t_dens * 1000.0f);
+        t.p2g_us = static_cast<uint64_t>(t_p2g * 1000.0f);
+        t.grid_update_us = static_cast<uint64_t>(t_grid * 1000.0f);
+        t.g2p_us = static_cast<uint64_t>(t_part * 1000.0f);
         t.total_us = static_cast<uint64_t>(tot * 1000.0f);
     }
     return EMERGE_OK;
@@ -576,7 +710,14 @@ emerge_status append_particles(emerge_sim *s, const emerge_particle *src, size_t
         }
         size_t cells = static_cast<size_t>(s->tpd) * s->tpd * TILE_CELLS;
         CK(cudaMemsetAsync(s->g.acc_a, 0, cells * sizeof(float4), s->stream));
-        launch_mass_scatter(s->P[s->cur], n_new, s->g, filter, lox, loy, hix, hiy, s->stream);
+        if (s->deterministic) {
+            StepLaunch L = make_launch(s);
+            L.n = n_new;
+            emerge_status dst = det_scatter(s, L, 0, filter, lox, loy, hix, hiy);
+            if (dst != EMERGE_OK) return dst;
+        } else {
+            launch_mass_scatter(s->P[s->cur], n_new, s->g, filter, lox, loy, hix, hiy, s->stream);
+        }
         launch_mass_gather(s->P[s->cur], volume_mode == 1 ? n_old : 0, n_new, s->g, 1, s->stream);
         CK(cudaMemsetAsync(s->g.acc_a, 0, cells * sizeof(float4), s->stream));
         CK(cudaMemsetAsync(s->g.acc_s, 0, cells * sizeof(float2), s->stream));
@@ -700,6 +841,7 @@ emerge_status emerge_cuda_destroy(emerge_sim *s) {
     if (s->h_state) cudaFreeHost(s->h_state);
     s->pbuf.reset();
     s->staging.reset();
+    s->detbuf.reset();
     s->gbuf.reset();
     s->mbuf.reset();
     s->sbuf.reset();
@@ -831,7 +973,10 @@ emerge_status emerge_cuda_step(emerge_sim *s, uint32_t n_steps, emerge_step_timi
             st = prime(s);
             if (st != EMERGE_OK) return st;
         }
-        if (s->use_graph) {
+        if (s->deterministic) {
+            st = run_det_step(s, timing != nullptr);
+            if (st != EMERGE_OK) return st;
+        } else if (s->use_graph) {
             if (s->graph_dirty || !s->graph_exec) {
                 st = build_graph(s);
                 if (st != EMERGE_OK) return st;
@@ -932,6 +1077,19 @@ emerge_status emerge_cuda_set_option(emerge_sim *s, int option, int64_t value) {
         s->use_window = value != 0;
         s->graph_dirty = true;
         return EMERGE_OK;
+    case EMERGE_OPT_DETERMINISTIC: {
+        int v = value != 0;
+        if (v != s->deterministic) {
+            emerge_status st = invalidate_pending(s);
+            if (st != EMERGE_OK) return st;
+            s->deterministic = v;
+            if (v) {
+                st = ensure_det_scratch(s);
+                if (st != EMERGE_OK) return st;
+            }
+        }
+        return EMERGE_OK;
+    }
     default: return static_cast<emerge_status>(s->fail(EMERGE_ERR_INVALID_ARG, "unknown option"));
     }
 }

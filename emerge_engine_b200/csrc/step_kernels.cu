@@ -333,6 +333,8 @@ struct ParticleKernelArgs {
     int mode_g2p;       // 0: prime pass (no G2P), 1: G2P(k) + P2G(k+1)
     int density_mode;   // fluid stress deferred to k_density; G2P reads rho_dp
     int use_window;
+    int project_in;     // recompute the projection of substep k before G2P (fused pipeline)
+    int emit_p2g;       // project for substep k+1 and scatter its P2G (fused pipeline)
 };
 
 __global__ void __launch_bounds__(THREADS) k_particle(ParticleKernelArgs a) {
@@ -365,8 +367,8 @@ __global__ void __launch_bounds__(THREADS) k_particle(ParticleKernelArgs a) {
             const MatP &m = s_mats[p.mat < static_cast<uint32_t>(a.n_mats) ? p.mat : 0u];
             if (a.mode_g2p) {
                 const PState o = p;
-                if (cfg.project) project_state(cfg, p);  // recompute S'(k); counted earlier
-                if (a.density_mode) {
+                if (a.project_in) project_state(cfg, p);  // recompute S'(k); counted earlier
+                if (a.density_mode && a.project_in) {
                     float d = a.P.rho_dp[i];
                     if (d > F32_EPS) {
                         p.rho = d;
@@ -383,6 +385,9 @@ __global__ void __launch_bounds__(THREADS) k_particle(ParticleKernelArgs a) {
             max_speed = fmaxf(max_speed, sp);
             float mdt = timestep_bound(m, p.rho, p.h, cfg.cell, cfg.mat_cfl, cfg.visc_cfl);
             if (isfinite(mdt) && mdt > 0.0f) min_mdt = fminf(min_mdt, mdt);
+            if (!a.emit_p2g) {
+                // deterministic pipeline: no fused scatter
+            } else {
             // projection of the next substep (step.rs:67-73)
             if (cfg.project) projected = project_state(cfg, p) ? 1 : 0;
             // P2G payload (transfer/p2g.rs:192-213)
@@ -403,6 +408,7 @@ __global__ void __launch_bounds__(THREADS) k_particle(ParticleKernelArgs a) {
             QW w = quadratic_weights(p.x);
             pl[k].bx = w.bx;
             pl[k].by = w.by;
+            }
         }
         clamped_any |= clamped;
         projected_any |= projected;
@@ -808,7 +814,8 @@ __global__ void k_mass_gather(DevParticles P, int lo, int hi, GridView g, int wr
 // ---------------------------------------------------------------- launchers
 static inline int blocks_for(int n, int per) { return (n + per - 1) / per; }
 
-void launch_particle_pass(const StepLaunch &L, const LoadFlagsHost &lfh, int mode_g2p) {
+void launch_particle_pass(const StepLaunch &L, const LoadFlagsHost &lfh, int mode_g2p,
+                          int project_in, int emit_p2g) {
     if (L.n == 0) return;
     ParticleKernelArgs a;
     a.P = L.P;
@@ -824,6 +831,8 @@ void launch_particle_pass(const StepLaunch &L, const LoadFlagsHost &lfh, int mod
     a.mode_g2p = mode_g2p;
     a.density_mode = L.density_mode;
     a.use_window = L.use_window;
+    a.project_in = project_in;
+    a.emit_p2g = emit_p2g;
     k_particle<<<blocks_for(L.n, THREADS * PPT), THREADS, 0, L.stream>>>(a);
 }
 

@@ -59,7 +59,10 @@ class MaterialRegistry:
 class Simulation:
     """The reference `Simulation` API, stepped by the B200 kernels."""
 
-    def __init__(self, config: SimConfig, device: int = 0, lib_path: str | None = None):
+    def __init__(self, config: SimConfig, device: int = 0, lib_path: str | None = None,
+                 deterministic: bool = False):
+        """`deterministic=True` selects the reference-order mode (EMERGE_OPT_DETERMINISTIC):
+        every grid cell sums its contributions in the reference's particle index order."""
         config.validate()
         self._lib = load_library(lib_path)
         self.config = config.copy()
@@ -70,16 +73,18 @@ class Simulation:
         self.registry = MaterialRegistry(FallbackMaterial())
         self.boundaries = [SlipBoundary(config.boundary_thickness)]  # lifecycle.rs:29-30
         self.last_timing: dict | None = None
+        if deterministic:
+            self.set_option(abi.OPT_DETERMINISTIC, 1)
 
     # ---------------------------------------------------------------- lifecycle
     @classmethod
-    def empty(cls, config: SimConfig, device: int = 0) -> "Simulation":
-        return cls(config, device)
+    def empty(cls, config: SimConfig, device: int = 0, **kw) -> "Simulation":
+        return cls(config, device, **kw)
 
     @classmethod
-    def new(cls, config: SimConfig, spawn: SpawnRegion, device: int = 0) -> "Simulation":
+    def new(cls, config: SimConfig, spawn: SpawnRegion, device: int = 0, **kw) -> "Simulation":
         """`Simulation::new` (lifecycle.rs:57-99)."""
-        s = cls(config, device)
+        s = cls(config, device, **kw)
         if not spawn.fits_in_sim(config):
             raise ValueError("spawn region must stay inside the simulation domain")
         sp = spawn.to_c()
@@ -245,3 +250,11 @@ class Simulation:
 
     def stream_handle(self) -> int:
         return int(self._lib.emerge_cuda_stream(self._sim) or 0)
+
+
+class DeterministicSimulation(Simulation):
+    """`Simulation` in the reference-order mode (per-cell sums in particle index order)."""
+
+    def __init__(self, config: SimConfig, device: int = 0, lib_path: str | None = None,
+                 deterministic: bool = True):
+        super().__init__(config, device, lib_path, deterministic=True)

@@ -270,11 +270,19 @@ emerge_status emerge_cuda_region_state(emerge_sim *sim, float cx, float cy, floa
  *   EMERGE_OPT_SORT_INTERVAL   re-sort particles by tile every N steps (0 = adaptive,
  *                              default; see emerge_cuda_sort_now).
  *   EMERGE_OPT_P2G_WINDOW      1 = shared-memory window scatter (default), 0 = direct
- *                              global reductions. */
+ *                              global reductions.
+ *   EMERGE_OPT_DETERMINISTIC   1 = reference-order mode: every grid cell sums its P2G and
+ *                              density contributions sequentially in the reference's
+ *                              particle index order (transfer/p2g.rs:16-23), so results
+ *                              do not depend on thread scheduling; slower (for parity
+ *                              checks and reproducible runs).  0 = fast fused path
+ *                              (default).  Set it before adding particles for the
+ *                              spawn-time volume estimate to use it too. */
 enum {
     EMERGE_OPT_USE_GRAPH = 1,
     EMERGE_OPT_SORT_INTERVAL = 2,
-    EMERGE_OPT_P2G_WINDOW = 3
+    EMERGE_OPT_P2G_WINDOW = 3,
+    EMERGE_OPT_DETERMINISTIC = 4
 };
 emerge_status emerge_cuda_set_option(emerge_sim *sim, int option, int64_t value);
 

@@ -1,28 +1,35 @@
 """CUDA step vs the CPU oracle on the same seeded scenes (through the C ABI).
 
-Tolerances (f32; the device sums P2G contributions with float atomics, so the
-per-cell summation order differs from the reference's particle-index order):
-  * positions: |dx| <= 1e-5 * max(|x_ref|, 1) per particle after one step,
-  * velocities: |dv| <= 1e-5 * max(|v_ref|, V_FLOOR) with V_FLOOR = 1e-2 * max|v_ref|
-    (the relative bound is taken against a floor so particles at rest, whose v is
-    a cancellation of large stress terms, are judged on the scene's velocity scale),
-  * total mass: exact (masses are never changed by the step),
-  * region_state statistics after many steps: 1e-3 relative.
+Two device modes are checked:
+  * reference order (`DeterministicSimulation`): every grid cell sums its contributions in
+    the reference's particle index order, so device and oracle differ only by the last-ulp
+    behaviour of expf/logf/sinf/powf.  Bar: per-particle relative error <= 1e-5 on x and v
+    after one step (v judged against max(|v_ref|, 1e-2 * max|v_ref|) so particles at rest
+    are measured on the scene's velocity scale).
+  * fast (`Simulation`): P2G reduces with float atomics in shared and global memory, so the
+    per-cell summation order changes from run to run.  Where stress impulses cancel, the
+    resulting velocity is ill-conditioned; the bar is x <= 1e-5 per particle, v <= 1e-4 at
+    the 99th percentile and <= 5e-3 at the maximum (same floor), total momentum within
+    1e-6 of the total absolute momentum, total mass exact.
+region_state statistics after many steps: 1e-3 relative in both modes.
 """
 import numpy as np
 import pytest
 
-from emerge_engine_b200 import Simulation, SimConfig, SpawnRegion, NeoHookeanMaterial
+from emerge_engine_b200 import (DeterministicSimulation, NeoHookeanMaterial, SimConfig,
+                                Simulation, SpawnRegion)
 from oracle.oracle import OracleSimulation
 from tests import scenes
 
 pytestmark = pytest.mark.gpu
 
-X_TOL = 1e-5
-V_TOL = 1e-5
+MODES = {
+    "reference_order": dict(cls=DeterministicSimulation, x_tol=1e-5, v_tol=1e-5, v_p99=1e-5),
+    "fast": dict(cls=Simulation, x_tol=1e-5, v_tol=5e-3, v_p99=1e-4),
+}
 
 
-def compare_particles(pg, pc, x_tol=X_TOL, v_tol=V_TOL):
+def compare_particles(pg, pc, x_tol, v_tol, v_p99):
     assert len(pg) == len(pc)
     dx = np.linalg.norm(pg["x"].astype(np.float64) - pc["x"], axis=1)
     x_rel = dx / np.maximum(np.linalg.norm(pc["x"], axis=1), 1.0)
@@ -30,41 +37,57 @@ def compare_particles(pg, pc, x_tol=X_TOL, v_tol=V_TOL):
     floor = max(1e-2 * vn.max(), 1e-12)
     dv = np.linalg.norm(pg["v"].astype(np.float64) - pc["v"], axis=1)
     v_rel = dv / np.maximum(vn, floor)
+    m = pc["mass"].astype(np.float64)
+    p_g = (m[:, None] * pg["v"]).sum(0)
+    p_c = (m[:, None] * pc["v"]).sum(0)
+    p_abs = (m * vn).sum()
     stats = dict(x_rel_max=float(x_rel.max()), v_rel_max=float(v_rel.max()),
-                 v_rel_p99=float(np.quantile(v_rel, 0.99)))
+                 v_rel_p99=float(np.quantile(v_rel, 0.99)),
+                 momentum_rel=float(np.linalg.norm(p_g - p_c) / max(p_abs, 1e-30)))
+    assert pg["mass"].sum(dtype=np.float64) == pc["mass"].sum(dtype=np.float64)
     assert x_rel.max() <= x_tol, stats
+    assert np.quantile(v_rel, 0.99) <= v_p99, stats
     assert v_rel.max() <= v_tol, stats
+    assert stats["momentum_rel"] <= 1e-6, stats
     return stats
 
 
-def both(builder, *args, **kw):
-    return builder(Simulation, *args, **kw), builder(OracleSimulation, *args, **kw)
+def both(mode, builder, *args, **kw):
+    return builder(MODES[mode]["cls"], *args, **kw), builder(OracleSimulation, *args, **kw)
 
 
-def test_spawn_state_matches(cuda_lib):
-    g, c = both(scenes.quickstart)
+def tol(mode):
+    t = MODES[mode]
+    return dict(x_tol=t["x_tol"], v_tol=t["v_tol"], v_p99=t["v_p99"])
+
+
+@pytest.mark.parametrize("mode", sorted(MODES))
+def test_spawn_state_matches(cuda_lib, mode):
+    g, c = both(mode, scenes.quickstart)
     pg, pc = g.particles(), c.particles()
-    # spawn lattice, tags and init are integer/exact work on the host side
+    # spawn lattice, tags and init_particle are exact host-side work
     np.testing.assert_array_equal(pg["x"], pc["x"])
     np.testing.assert_array_equal(pg["user_tag"], pc["user_tag"])
     np.testing.assert_array_equal(pg["material_id"], pc["material_id"])
-    # add_body's local volume estimate ran on the device (float atomics)
+    # add_body's local volume estimate ran on the device
+    rtol = 0 if mode == "reference_order" else 1e-6
     for k in ("initial_volume", "volume", "density"):
-        np.testing.assert_allclose(pg[k], pc[k], rtol=1e-6, atol=0)
+        np.testing.assert_allclose(pg[k], pc[k], rtol=rtol, atol=0, err_msg=k)
 
 
-def test_quickstart_one_step(cuda_lib):
-    g, c = both(scenes.quickstart)
+@pytest.mark.parametrize("mode", sorted(MODES))
+def test_quickstart_one_step(cuda_lib, mode):
+    g, c = both(mode, scenes.quickstart)
     g.step()
     c.step()
     assert g.last_substeps() == c.last_substeps()
     assert g.effective_dt() == pytest.approx(c.effective_dt(), rel=1e-6)
-    stats = compare_particles(g.particles(), c.particles())
-    print("quickstart 1 step", stats)
+    print(mode, "quickstart 1 step", compare_particles(g.particles(), c.particles(), **tol(mode)))
 
 
-def test_quickstart_region_state_60_steps(cuda_lib):
-    g, c = both(scenes.quickstart)
+@pytest.mark.parametrize("mode", sorted(MODES))
+def test_quickstart_region_state_60_steps(cuda_lib, mode):
+    g, c = both(mode, scenes.quickstart)
     g.step_n(60)
     c.step_n(60)
     pg, pc = g.particles(), c.particles()
@@ -78,29 +101,31 @@ def test_quickstart_region_state_60_steps(cuda_lib):
         assert sg.centroid == pytest.approx(sc.centroid, rel=1e-3)
 
 
-def test_dam_break_small_one_step(cuda_lib):
-    g, c = both(scenes.dam_break, grid_res=128, column=64)
+@pytest.mark.parametrize("mode", sorted(MODES))
+def test_dam_break_small_one_step(cuda_lib, mode):
+    g, c = both(mode, scenes.dam_break, grid_res=128, column=64)
     g.step()
     c.step()
     assert g.last_substeps() == c.last_substeps()
-    stats = compare_particles(g.particles(), c.particles())
-    print("dam break 1 step", stats)
+    print(mode, "dam break 1 step", compare_particles(g.particles(), c.particles(), **tol(mode)))
 
 
-def test_granular_small_one_step(cuda_lib):
-    g, c = both(scenes.mixed_granular, grid_res=256, target_particles=120_000)
+@pytest.mark.parametrize("mode", sorted(MODES))
+def test_granular_small_one_step(cuda_lib, mode):
+    g, c = both(mode, scenes.mixed_granular, grid_res=256, target_particles=120_000)
     g.step()
     c.step()
     assert g.last_substeps() == c.last_substeps()
     pg, pc = g.particles(), c.particles()
-    stats = compare_particles(pg, pc)
+    stats = compare_particles(pg, pc, **tol(mode))
     # plastic state (Drucker-Prager q, NACC alpha, snow Jp/h)
     for k in ("friction_hardening", "log_volume_strain", "plastic_volume_ratio", "hardening_scale"):
         np.testing.assert_allclose(pg[k], pc[k], rtol=1e-4, atol=1e-5, err_msg=k)
-    print("granular 1 step", stats)
+    print(mode, "granular 1 step", stats)
 
 
-def test_projection_recovers_guarded_fields(cuda_lib):
+@pytest.mark.parametrize("mode", sorted(MODES))
+def test_projection_recovers_guarded_fields(cuda_lib, mode):
     """physics_correctness.rs:2237 NaN-injection recovery, GPU vs oracle."""
     def build(cls):
         cfg = SimConfig.standard(32, 0.02, (0.0, 0.0))
@@ -126,21 +151,22 @@ def test_projection_recovers_guarded_fields(cuda_lib):
         p["density"][13] = -1.0
         sim.set_particles(p)
         return sim
-    g, c = build(Simulation), build(OracleSimulation)
+    g, c = build(MODES[mode]["cls"]), build(OracleSimulation)
     g.step()
     c.step()
     pg, pc = g.particles(), c.particles()
     for k in ("x", "v", "c", "f", "mass", "initial_volume", "volume", "density",
               "plastic_volume_ratio", "hardening_scale", "friction_hardening", "log_volume_strain"):
         assert np.isfinite(pg[k]).all(), k
-    compare_particles(pg, pc)
+        np.testing.assert_allclose(pg[k], pc[k], rtol=1e-5, atol=1e-6, err_msg=k)
+    compare_particles(pg, pc, **tol(mode))
     assert g.last_counters()[1] == c.last_counters()[1]
 
 
 def test_sort_preserves_results(cuda_lib):
     """Sorting permutes device storage only: reference-order readback is unchanged and a
     step after a sort agrees with the oracle."""
-    g, c = both(scenes.quickstart)
+    g, c = both("reference_order", scenes.quickstart)
     before = g.particles()
     g.sort_now(0)
     np.testing.assert_array_equal(before, g.particles())
@@ -148,4 +174,26 @@ def test_sort_preserves_results(cuda_lib):
     np.testing.assert_array_equal(before, g.particles())
     g.step()
     c.step()
-    compare_particles(g.particles(), c.particles())
+    compare_particles(g.particles(), c.particles(), **tol("reference_order"))
+
+
+def test_reference_order_is_run_to_run_deterministic(cuda_lib):
+    a = scenes.dam_break(DeterministicSimulation, grid_res=128, column=64)
+    b = scenes.dam_break(DeterministicSimulation, grid_res=128, column=64)
+    a.step_n(3)
+    b.step_n(3)
+    np.testing.assert_array_equal(a.particles(), b.particles())
+
+
+def test_graph_and_host_loop_agree(cuda_lib):
+    """The device-side substep loop (CUDA graph while node) and the host-driven loop run
+    the same kernels; results agree to float-reduction order."""
+    from emerge_engine_b200.abi import OPT_USE_GRAPH
+    a = scenes.dam_break(Simulation, grid_res=128, column=64)
+    b = scenes.dam_break(Simulation, grid_res=128, column=64)
+    b.set_option(OPT_USE_GRAPH, 0)
+    a.step_n(3)
+    b.step_n(3, timing=True)
+    assert a.last_substeps() == b.last_substeps()
+    compare_particles(a.particles(), b.particles(), **tol("fast"))
+    assert b.last_timing["total_us"] > 0 and b.last_timing["g2p_us"] > 0
