@@ -32,6 +32,7 @@ OPT_USE_GRAPH = 1
 OPT_SORT_INTERVAL = 2
 OPT_P2G_WINDOW = 3
 OPT_DETERMINISTIC = 4
+OPT_PRECISE_MATH = 5
 
 
 class Particle(Structure):

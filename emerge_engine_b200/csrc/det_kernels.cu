@@ -95,7 +95,7 @@ __global__ void k_det_records(DevParticles P, int n, const MatP *mats, int n_mat
         const MatP &m = mats[p.mat < static_cast<uint32_t>(n_mats) ? p.mat : 0u];
         v = p.v;
         c = p.c;
-        stress = combined_kirchhoff_stress(m, p);
+        stress = combined_kirchhoff_stress(m, p, cfg.precise_math != 0);
         stress_coeff = -stress_volume(m, p) * KERNEL_D_INVERSE * st->sub_dt;
     }
     QW w = quadratic_weights(p.x);

@@ -4,10 +4,10 @@
 // crate M1thieu/emerge-engine) in f32, in the reference's expression order.
 // Translation units including this header are compiled with -fmad=false so
 // a*b+c is never contracted into an FMA (the Rust reference never contracts),
-// and with IEEE division/sqrt (nvcc defaults).  expf/logf/sinf/sinhf/powf are
-// CUDA's libdevice-free intrinsics-by-default implementations, whose last-ulp
-// behaviour differs from glibc: results agree with the CPU reference to
-// tolerance, not bit for bit.
+// and with IEEE division/sqrt (nvcc defaults).  exp/log/sin/sinh/pow go through
+// em_* below: either CUDA's single-precision functions (fast path) or a double
+// evaluation rounded once to f32 (precise path, on in the reference-order mode),
+// which agrees with glibc's f32 results in nearly all cases.
 #pragma once
 
 #include <cstdint>
@@ -80,6 +80,18 @@ EM_HD float4 m_to4(M2 a) { return make_float4(a.xa.x, a.xa.y, a.ya.x, a.ya.y); }
 
 // Rust `f32 as i32` (saturating, NaN -> 0); cvt.rzi.s32.f32 has the same semantics.
 EM_HD int f2i(float f) { return static_cast<int>(f); }
+
+// Transcendentals.  `pr` (precise) evaluates in double and rounds once to f32: the
+// correctly rounded result in all but vanishingly rare cases, which is what glibc's
+// f32 functions (called by the Rust reference) return in nearly all cases.  With
+// `pr` false the single-precision CUDA functions are used.
+EM_HD float em_exp(float x, bool pr) { return pr ? static_cast<float>(exp(static_cast<double>(x))) : expf(x); }
+EM_HD float em_log(float x, bool pr) { return pr ? static_cast<float>(log(static_cast<double>(x))) : logf(x); }
+EM_HD float em_sin(float x, bool pr) { return pr ? static_cast<float>(sin(static_cast<double>(x))) : sinf(x); }
+EM_HD float em_sinh(float x, bool pr) { return pr ? static_cast<float>(sinh(static_cast<double>(x))) : sinhf(x); }
+EM_HD float em_pow(float x, float y, bool pr) {
+    return pr ? static_cast<float>(pow(static_cast<double>(x), static_cast<double>(y))) : powf(x, y);
+}
 
 // axis_weights (spacetime/grid/kernel.rs:20-25)
 EM_HD void axis_weights(float d, float w[3]) {
@@ -180,17 +192,17 @@ typedef emerge_material_params MatP;
 EM_HD float nacc_kappa(const MatP &m) { return m.lambda + m.mu; }  // inverse of nacc.rs:304
 
 // DruckerPragerMaterial::alpha (sand.rs:135-141); dp_h0..3 = phi0, h1, h2, phi_r
-EM_HD float dp_alpha(const MatP &m, float q) {
-    float phi = m.dp_h0 + (m.dp_h1 * q - m.dp_h3) * expf(-m.dp_h2 * q);
-    float s = sinf(phi);
+EM_HD float dp_alpha(const MatP &m, float q, bool pr) {
+    float phi = m.dp_h0 + (m.dp_h1 * q - m.dp_h3) * em_exp(-m.dp_h2 * q, pr);
+    float s = em_sin(phi, pr);
     return sqrtf(2.0f / 3.0f) * (2.0f * s) / (3.0f - s);
 }
 
 // DruckerPragerMaterial::project (sand.rs:156-194); cohesion in stretch_limit (sand.rs:335)
 EM_HD bool dp_project(const MatP &m, float2 sigma_in, float lvs, float q, float2 &out,
-                      float &dq) {
+                      float &dq, bool pr) {
     float2 sigma = vmax2(vabs2(sigma_in), splat(LOG_CLAMP));
-    float2 eps = v2(logf(sigma.x) + lvs * 0.5f, logf(sigma.y) + lvs * 0.5f);
+    float2 eps = v2(em_log(sigma.x, pr) + lvs * 0.5f, em_log(sigma.y, pr) + lvs * 0.5f);
     float trace = eps.x + eps.y;
     float2 dev = vsub(eps, splat(trace * 0.5f));
     float dev_norm = vlen(dev);
@@ -200,12 +212,12 @@ EM_HD bool dp_project(const MatP &m, float2 sigma_in, float lvs, float q, float2
         return true;
     }
     float ratio = (m.lambda + m.mu) / m.mu;
-    float alpha = dp_alpha(m, q);
+    float alpha = dp_alpha(m, q, pr);
     float cohesion_term = m.stretch_limit / (2.0f * m.mu);
     float gamma = dev_norm + ratio * trace * alpha - cohesion_term;
     if (gamma <= 0.0f) return false;
     float2 h = vsub(eps, svmul(gamma, vdivs(dev, dev_norm)));
-    out = v2(expf(h.x), expf(h.y));
+    out = v2(em_exp(h.x, pr), em_exp(h.y, pr));
     dq = gamma;
     return true;
 }
@@ -214,7 +226,7 @@ EM_HD M2 reconstruct(M2 u, float2 s, M2 vt) { return mm(mm(u, mdiag(s)), vt); }
 
 // NaccMaterial::project (nacc.rs:129-223).  params(): hardening_exponent = xi,
 // compression_limit = beta, stretch_limit = M (nacc.rs:309-311).
-EM_HD void nacc_project(const MatP &m, M2 f, float alpha, M2 &f_out, float &alpha_out) {
+EM_HD void nacc_project(const MatP &m, M2 f, float alpha, M2 &f_out, float &alpha_out, bool pr) {
     const float kappa = nacc_kappa(m);
     float xi = m.hardening_exponent;
     float beta = m.compression_limit;
@@ -225,23 +237,23 @@ EM_HD void nacc_project(const MatP &m, M2 f, float alpha, M2 &f_out, float &alph
     svd2(f, u, sv, vt);
     float2 sv_sq = vmulv(sv, sv);
     float sv_sq_trace = sv_sq.x + sv_sq.y;
-    float p0 = kappa * (1.0e-5f + sinhf(xi * fmaxf(-alpha, 0.0f)));
+    float p0 = kappa * (1.0e-5f + em_sinh(xi * fmaxf(-alpha, 0.0f), pr));
     float j_e_tr = fmaxf(sv.x * sv.y, 1.0e-6f);
     float2 s_tr = svmul(m.mu * (1.0f / j_e_tr), vsub(sv_sq, splat(sv_sq_trace * 0.5f)));
     float psi_kappa = kappa * 0.5f * (j_e_tr - 1.0f / j_e_tr);
     float p_tr = -psi_kappa * j_e_tr;
     if (p_tr > p0) {
         float j_n1 = sqrtf(fmaxf(-2.0f * p0 / kappa + 1.0f, 1.0e-8f));
-        float sv_new = powf(j_n1, 0.5f);
-        if (hard) alpha += logf(j_e_tr / j_n1);
+        float sv_new = em_pow(j_n1, 0.5f, pr);
+        if (hard) alpha += em_log(j_e_tr / j_n1, pr);
         f_out = reconstruct(u, splat(sv_new), vt);
         alpha_out = alpha;
         return;
     }
     if (p_tr < -beta * p0) {
         float j_n1 = sqrtf(fmaxf(2.0f * beta * p0 / kappa + 1.0f, 1.0e-8f));
-        float sv_new = powf(j_n1, 0.5f);
-        if (hard) alpha += logf(j_e_tr / j_n1);
+        float sv_new = em_pow(j_n1, 0.5f, pr);
+        if (hard) alpha += em_log(j_e_tr / j_n1, pr);
         f_out = reconstruct(u, splat(sv_new), vt);
         alpha_out = alpha;
         return;
@@ -269,7 +281,7 @@ EM_HD void nacc_project(const MatP &m, M2 f, float alpha, M2 &f_out, float &alph
         float p2 = p_c + l2 * dir.x;
         float p_x = ((p_tr - p_c) * (p1 - p_c) > 0.0f) ? p1 : p2;
         float j_e_x = sqrtf(fmaxf(fabsf(-2.0f * p_x / kappa + 1.0f), 1.0e-8f));
-        if (j_e_x > 1.0e-4f) alpha += logf(j_e_tr / j_e_x);
+        if (j_e_x > 1.0e-4f) alpha += em_log(j_e_tr / j_e_x, pr);
     }
     float scale = sqrtf(fmaxf(-y1 / fmaxf(y0, 1.0e-10f), 0.0f)) * (j_e_tr / m.mu);
     float2 b_n1 = vadd(svmul(scale, normalize_or_zero(s_tr)), splat(sv_sq_trace / 2.0f));
@@ -292,14 +304,14 @@ struct PState {
 };
 
 // MaterialModel::kirchhoff_stress per model.
-EM_HD M2 kirchhoff_stress(const MatP &m, const PState &p) {
+EM_HD M2 kirchhoff_stress(const MatP &m, const PState &p, bool pr) {
     const M2 f = p.f;
     switch (m.model) {
     case M_NEOHOOKEAN: {  // elastic.rs:180-255; damage rate in cohesion_coeff (elastic.rs:284)
         float j = mdet(f);
         if (j <= MIN_J) return mzero();
         float t_scale = 1.0f + m.thermal_expansion * p.temperature;
-        float damage_scale = expf(-m.cohesion_coeff * p.q);
+        float damage_scale = em_exp(-m.cohesion_coeff * p.q, pr);
         float mu = m.mu * t_scale * damage_scale;
         float lambda = m.lambda * t_scale * damage_scale;
         M2 b = mm(f, mtrans(f));
@@ -307,7 +319,7 @@ EM_HD M2 kirchhoff_stress(const MatP &m, const PState &p) {
         M2 dev_b = msub(b, mdiag(splat(tr_b * 0.5f)));
         float k = lambda + mu;
         M2 dev_stress = smscale(mu / j, dev_b);
-        M2 vol_stress = smscale(k * logf(j), mident());
+        M2 vol_stress = smscale(k * em_log(j, pr), mident());
         M2 viscous = mzero();
         if (m.dynamic_viscosity > 0.0f) {  // viscosity in dynamic_viscosity (elastic.rs:285)
             M2 sym = madd(p.c, mtrans(p.c));
@@ -321,12 +333,12 @@ EM_HD M2 kirchhoff_stress(const MatP &m, const PState &p) {
     case M_FLUID: {  // fluid.rs:135-191 (min_density 1e-6, fluid.rs:60)
         float density = fminf(fmaxf(p.rho, 1.0e-6f), m.rest_density * 2.0f);
         float pressure = fmaxf(
-            m.eos_stiffness * (powf(density / m.rest_density, m.eos_power) - 1.0f),
+            m.eos_stiffness * (em_pow(density / m.rest_density, m.eos_power, pr) - 1.0f),
             m.pressure_floor);
         M2 stress = mdiag(splat(-pressure));
         float eff_visc = m.dynamic_viscosity;
         if (m.thermal_viscosity_coeff > 0.0f)
-            eff_visc = m.dynamic_viscosity * expf(-m.thermal_viscosity_coeff * p.temperature);
+            eff_visc = m.dynamic_viscosity * em_exp(-m.thermal_viscosity_coeff * p.temperature, pr);
         M2 sym = madd(p.c, mtrans(p.c));
         float div_v = sym.xa.x + sym.ya.y;
         M2 strain_dev = msub(sym, mdiag(splat(div_v * 0.5f)));
@@ -375,8 +387,8 @@ EM_HD M2 kirchhoff_stress(const MatP &m, const PState &p) {
 
 // combined_kirchhoff_stress (spacetime/transfer.rs:77-104).  Only NeoHookean has a
 // non-zero activation_scale among the supported models (elastic.rs:271-273).
-EM_HD M2 combined_kirchhoff_stress(const MatP &m, const PState &p) {
-    M2 tau = kirchhoff_stress(m, p);
+EM_HD M2 combined_kirchhoff_stress(const MatP &m, const PState &p, bool pr) {
+    M2 tau = kirchhoff_stress(m, p, pr);
     float coeff = (m.model == M_NEOHOOKEAN) ? m.active_stress_coeff : 0.0f;
     if (p.activation <= 0.0f || coeff <= 0.0f) return tau;
     M2 tau_active;
@@ -402,7 +414,7 @@ EM_HD float stress_volume(const MatP &m, const PState &p) {
 
 // MaterialModel::timestep_bound
 EM_HD float timestep_bound(const MatP &m, float density, float h, float cell, float mat_cfl,
-                           float visc_cfl) {
+                           float visc_cfl, bool pr) {
     switch (m.model) {
     case M_NEOHOOKEAN: {  // elastic.rs:290-327
         float elastic_dt = elastic_wave_dt(m.lambda, m.mu, 1.0f, density, 1.0e-6f, cell, mat_cfl);
@@ -419,7 +431,7 @@ EM_HD float timestep_bound(const MatP &m, float density, float h, float cell, fl
         float d = fmaxf(density, 1.0e-6f);
         float ratio = fmaxf(d / fmaxf(m.rest_density, 1.0e-6f), MIN_DENSITY_RATIO);
         float dt_bound = INFINITY;
-        float c2 = m.eos_stiffness * m.eos_power * powf(ratio, m.eos_power - 1.0f) /
+        float c2 = m.eos_stiffness * m.eos_power * em_pow(ratio, m.eos_power - 1.0f, pr) /
                    fmaxf(m.rest_density, 1.0e-6f);
         if (isfinite(c2) && c2 > F32_EPS) dt_bound = fminf(dt_bound, mat_cfl * cell / sqrtf(c2));
         if (m.dynamic_viscosity > 0.0f) {
@@ -449,7 +461,7 @@ EM_HD void sync_volume_density(PState &p) {
 
 // DP update after the return map decision (sand.rs:258-318).
 EM_HD void dp_finish(const MatP &m, PState &p, M2 u, float2 sigma, M2 vt, bool projected,
-                     float2 proj, float dq) {
+                     float2 proj, float dq, bool pr) {
     float2 new_sigma = sigma;
     if (projected) {
         float2 sigma_abs = vmax2(vabs2(sigma), splat(LOG_CLAMP));
@@ -457,10 +469,10 @@ EM_HD void dp_finish(const MatP &m, PState &p, M2 u, float2 sigma, M2 vt, bool p
         float new_det = proj.x * proj.y;
         float diff = new_det - prev_det;
         float corrected = diff > 0.0f ? new_det : prev_det + diff * 1.0f;  // volume_correction 1.0
-        p.lvs += logf(prev_det) - logf(corrected);
+        p.lvs += em_log(prev_det, pr) - em_log(corrected, pr);
         float q_max = 5.0f / fmaxf(m.dp_h2, 1e-6f);
         p.q = fminf(p.q + dq, q_max);
-        if (m.compression_limit > 0.0f) p.lvs += sinf(m.compression_limit) * dq;  // dilatancy
+        if (m.compression_limit > 0.0f) p.lvs += em_sin(m.compression_limit, pr) * dq;  // dilatancy
         new_sigma = proj;
     }
     new_sigma = vabs2(new_sigma);
@@ -472,7 +484,7 @@ EM_HD void dp_finish(const MatP &m, PState &p, M2 u, float2 sigma, M2 vt, bool p
 }
 
 // MaterialModel::update_particle
-EM_HD void update_particle(const MatP &m, PState &p, float dt) {
+EM_HD void update_particle(const MatP &m, PState &p, float dt, bool pr) {
     switch (m.model) {
     case M_NEOHOOKEAN: {  // elastic.rs:262-269
         M2 fp_new = madd(mident(), smscale(dt, p.c));
@@ -498,8 +510,8 @@ EM_HD void update_particle(const MatP &m, PState &p, float dt) {
         svd2(f_trial, u, sigma, vt);
         float2 proj;
         float dq = 0.0f;
-        bool projected = dp_project(m, sigma, p.lvs, p.q, proj, dq);
-        dp_finish(m, p, u, sigma, vt, projected, proj, dq);
+        bool projected = dp_project(m, sigma, p.lvs, p.q, proj, dq, pr);
+        dp_finish(m, p, u, sigma, vt, projected, proj, dq, pr);
         break;
     }
     case M_SNOW: {  // snow.rs:142-176
@@ -511,7 +523,7 @@ EM_HD void update_particle(const MatP &m, PState &p, float dt) {
         float2 sigma_c = v2(fclampf(sigma.x, lo, hi), fclampf(sigma.y, lo, hi));
         float jp_new = p.jp * (sigma.x * sigma.y) / (sigma_c.x * sigma_c.y);
         p.jp = fclampf(jp_new, m.volume_ratio_min, m.volume_ratio_max);
-        p.h = fclampf(expf(m.hardening_exponent * (1.0f - p.jp)), 0.1f, 7.0f);
+        p.h = fclampf(em_exp(m.hardening_exponent * (1.0f - p.jp), pr), 0.1f, 7.0f);
         p.f = mm(mm(u, mdiag(sigma_c)), vt);
         sync_volume_density(p);
         break;
@@ -519,7 +531,7 @@ EM_HD void update_particle(const MatP &m, PState &p, float dt) {
     case M_NACC: {  // nacc.rs:255-269 (no F advance on the CPU path)
         M2 nf;
         float na;
-        nacc_project(m, p.f, p.lvs, nf, na);
+        nacc_project(m, p.f, p.lvs, nf, na, pr);
         p.f = nf;
         p.lvs = na;
         float j = fmaxf(mdet(nf), MIN_J);
@@ -567,6 +579,7 @@ struct DevConfig {
     float particle_mass;
     int max_substeps;
     float apic_blend, j_max;
+    int precise_math;        // evaluate exp/log/sin/sinh/pow in double, round once
     int n_bound;             // slip boundaries in order
     int bound_t[8];
 };

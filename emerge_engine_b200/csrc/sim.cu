@@ -143,6 +143,7 @@ struct emerge_sim {
 
     // reference-order (deterministic) mode
     int deterministic = 0;
+    int precise_opt = -1;  // -1: precise math follows `deterministic`
     Buffer detbuf;
     SortScratch det_sort;
     float4 *det_payload = nullptr;
@@ -228,8 +229,10 @@ emerge_status validate_config(const emerge_sim_config &c, std::string &msg) {
     return EMERGE_OK;
 }
 
-DevConfig make_dev_config(const emerge_sim_config &c, const std::vector<uint64_t> &bounds) {
+DevConfig make_dev_config(const emerge_sim_config &c, const std::vector<uint64_t> &bounds,
+                          int precise) {
     DevConfig d{};
+    d.precise_math = precise;
     d.res = static_cast<int>(c.grid_res);
     d.cell = c.grid_cell_size;
     d.dt = c.dt;
@@ -783,7 +786,7 @@ emerge_status emerge_cuda_create(const emerge_sim_config *config, int device, em
     s->cfg = *config;
     s->device = device;
     s->bounds.push_back(config->boundary_thickness);  // default SlipBoundary (lifecycle.rs:29-30)
-    s->dcfg = make_dev_config(s->cfg, s->bounds);
+    s->dcfg = make_dev_config(s->cfg, s->bounds, 0);
     emerge_material_params fallback;
     std::memset(&fallback, 0, sizeof(fallback));
     s->mats.push_back(fallback);
@@ -884,7 +887,7 @@ emerge_status emerge_cuda_set_slip_boundaries(emerge_sim *s, const uint64_t *thi
         if (thickness[k] + 1 > s->cfg.grid_res)
             return static_cast<emerge_status>(s->fail(EMERGE_ERR_INVALID_ARG, "boundary thickness exceeds grid"));
     s->bounds.assign(thickness, thickness + n);
-    s->dcfg = make_dev_config(s->cfg, s->bounds);
+    s->dcfg = make_dev_config(s->cfg, s->bounds, s->dcfg.precise_math);
     s->graph_dirty = true;
     return EMERGE_OK;
 }
@@ -1088,8 +1091,15 @@ emerge_status emerge_cuda_set_option(emerge_sim *s, int option, int64_t value) {
                 if (st != EMERGE_OK) return st;
             }
         }
+        s->dcfg.precise_math = s->precise_opt >= 0 ? s->precise_opt : s->deterministic;
+        s->graph_dirty = true;
         return EMERGE_OK;
     }
+    case EMERGE_OPT_PRECISE_MATH:
+        s->precise_opt = value < 0 ? -1 : (value != 0);
+        s->dcfg.precise_math = s->precise_opt >= 0 ? s->precise_opt : s->deterministic;
+        s->graph_dirty = true;
+        return invalidate_pending(s);
     default: return static_cast<emerge_status>(s->fail(EMERGE_ERR_INVALID_ARG, "unknown option"));
     }
 }

@@ -376,14 +376,15 @@ __global__ void __launch_bounds__(THREADS) k_particle(ParticleKernelArgs a) {
                     }
                 }
                 clamped = g2p_particle(a.g, cfg, dt, p);
-                update_particle(m, p, dt);
+                update_particle(m, p, dt, cfg.precise_math != 0);
                 store_changed(a.P, i, o, p);
             }
             // CFL contribution for the next substep (step.rs:447-466)
             float sp = vlen(p.v);
             if (cfg.affine_cfl) sp += affine_cfl(p.c, cfg.cell);
             max_speed = fmaxf(max_speed, sp);
-            float mdt = timestep_bound(m, p.rho, p.h, cfg.cell, cfg.mat_cfl, cfg.visc_cfl);
+            float mdt = timestep_bound(m, p.rho, p.h, cfg.cell, cfg.mat_cfl, cfg.visc_cfl,
+                                       cfg.precise_math != 0);
             if (isfinite(mdt) && mdt > 0.0f) min_mdt = fminf(min_mdt, mdt);
             if (!a.emit_p2g) {
                 // deterministic pipeline: no fused scatter
@@ -398,7 +399,7 @@ __global__ void __launch_bounds__(THREADS) k_particle(ParticleKernelArgs a) {
             pl[k].do_ma = true;
             bool fluid = m.model == M_FLUID;
             if (!(a.density_mode && fluid)) {
-                pl[k].tau = combined_kirchhoff_stress(m, p);
+                pl[k].tau = combined_kirchhoff_stress(m, p, cfg.precise_math != 0);
                 pl[k].s = -stress_volume(m, p) * KERNEL_D_INVERSE;
                 pl[k].do_s = true;
             } else {
@@ -495,7 +496,7 @@ __global__ void __launch_bounds__(THREADS) k_density(DensityKernelArgs a) {
             pl[k].m = 0.0f;
             pl[k].v = v2(0.0f, 0.0f);
             pl[k].c = mzero();
-            pl[k].tau = combined_kirchhoff_stress(m, p);
+            pl[k].tau = combined_kirchhoff_stress(m, p, cfg.precise_math != 0);
             pl[k].s = -stress_volume(m, p) * KERNEL_D_INVERSE;
             pl[k].do_s = true;
             pl[k].bx = w.bx;

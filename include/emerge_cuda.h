@@ -277,12 +277,17 @@ emerge_status emerge_cuda_region_state(emerge_sim *sim, float cx, float cy, floa
  *                              do not depend on thread scheduling; slower (for parity
  *                              checks and reproducible runs).  0 = fast fused path
  *                              (default).  Set it before adding particles for the
- *                              spawn-time volume estimate to use it too. */
+ *                              spawn-time volume estimate to use it too.
+ *   EMERGE_OPT_PRECISE_MATH    1 = evaluate exp/log/sin/sinh/pow in double and round once
+ *                              to f32 (agrees with the reference's glibc f32 results in
+ *                              nearly all cases), 0 = CUDA single-precision functions,
+ *                              -1 = follow EMERGE_OPT_DETERMINISTIC (default). */
 enum {
     EMERGE_OPT_USE_GRAPH = 1,
     EMERGE_OPT_SORT_INTERVAL = 2,
     EMERGE_OPT_P2G_WINDOW = 3,
-    EMERGE_OPT_DETERMINISTIC = 4
+    EMERGE_OPT_DETERMINISTIC = 4,
+    EMERGE_OPT_PRECISE_MATH = 5
 };
 emerge_status emerge_cuda_set_option(emerge_sim *sim, int option, int64_t value);
 
