@@ -1,0 +1,363 @@
+#!/usr/bin/env python
+"""Benchmark of the MLS-MPM step on B200: particle-steps/s.
+
+One unit of the metric is one particle advanced through one substep (P2G, grid update,
+G2P + constitutive update); a benchmark "step" is one `Simulation::step()` call (one frame
+of config.dt = 0.05, with as many CFL-limited substeps as the reference loop takes).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--workload NAME] [--impl ours|reference]
+
+Default workload: the dam break at ~1M particles (512 x 512-cell water column at 4 particles
+per cell on a 1024^2 grid).  Inputs are resident in HBM when the timed region starts; L2 is
+flushed (512 MiB device write) before every timed step.  `e2e` repeats the measurement
+through the C ABI with the particle state uploaded from pinned host memory before and read
+back after every step.  `--impl reference` times the CPU oracle (the reference step restated
+in C++) on the host cores instead.  Under torchrun each rank runs an independent replica
+(replicas only: the single-scene step does not shard), timed on the device, max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import re
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+METRIC = "particle-steps/s on 1 B200 (plain CUDA vs learned closure at stated error) vs CPU"
+UNIT = "particle-steps/s"
+
+WORKLOADS = {
+    "dam_break_1m": dict(builder="dam_break", kwargs=dict(grid_res=1024, column=512),
+                         desc="dam break: 512x512-cell water column, 4 ppc, 1024^2 grid, "
+                              "NewtonianFluid Tait rho0=1000 k=1e4 gamma=7, SlipBoundary(2), "
+                              "dt=0.05, adaptive CFL substeps",
+                         material="NewtonianFluid", grid_res=1024),
+    "dam_break_262k": dict(builder="dam_break", kwargs=dict(grid_res=512, column=256),
+                           desc="dam break: 256x256-cell water column, 4 ppc, 512^2 grid",
+                           material="NewtonianFluid", grid_res=512),
+    "mixed_granular_4m": dict(builder="mixed_granular",
+                              kwargs=dict(grid_res=1024, target_particles=4_000_000),
+                              desc="mixed granular: seeded blocks 16-128 cells, DruckerPrager / "
+                                   "Stomakhin snow / NACC, 4 ppc, 1024^2 grid",
+                              material="DP+Snow+NACC", grid_res=1024),
+}
+DEFAULT_WORKLOAD = "dam_break_1m"
+
+# Algorithmic bytes per particle of one launch of the fused particle pass (k_particle):
+# the hot state it must read and write once per substep, plus its share of grid traffic
+# (grid velocity gather 8 B/cell, mass+momentum+stress reductions 24 B/cell, 4 ppc).
+#   fluid:    read x8 v8 C16 F16 m4 V0 4 V4 rho4 mat4 plastic16 rho_dp4 = 88,
+#             write x8 v8 C16 V4 rho4 = 40, grid 32/4 = 8              -> 136 B
+#   granular: read 84, write x8 v8 C16 F16 V4 rho4 plastic16 = 72, grid 8 -> 164 B
+K_PARTICLE_BYTES = {"NewtonianFluid": 136, "DP+Snow+NACC": 164}
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+def load_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def profile_traffic(workload: str):
+    """DRAM bytes per k_particle launch from the committed ncu summary, if present."""
+    path = os.path.join(ROOT, "profiles", f"k_particle_{workload}.md")
+    if not os.path.exists(path):
+        return None
+    with open(path) as f:
+        m = re.search(r"dram_bytes_per_launch:\s*([0-9.eE+]+)", f.read())
+    return float(m.group(1)) if m else None
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms while running."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+        self.thread = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits",
+                 "-i", str(self.gpu), "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except (OSError, ValueError):
+            self.proc = None
+            return
+        self.thread = threading.Thread(target=self._read, daemon=True)
+        self.thread.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self) -> dict | None:
+        if not self.proc:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        if self.thread:
+            self.thread.join(timeout=2)
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for name, val in zip(names, parts[5:9]):
+                if val.lower() == "active":
+                    reasons.add(name)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def build_scene(sim_cls, workload: str, **kw):
+    from tests import scenes
+    spec = WORKLOADS[workload]
+    return getattr(scenes, spec["builder"])(sim_cls, **spec["kwargs"], **kw)
+
+
+def cpu_baseline(workload: str, budget_s: float = 15.0) -> dict:
+    """The CPU oracle (reference step restated in C++) on this host, bounded sample."""
+    from oracle.oracle import OracleSimulation, set_threads
+    threads = set_threads(0)
+    sim = build_scene(OracleSimulation, workload)
+    n = sim.particle_count()
+    sim.step()  # warm-up
+    steps = subs = 0
+    t0 = time.perf_counter()
+    while True:
+        sim.step()
+        steps += 1
+        subs += sim.last_substeps()
+        if time.perf_counter() - t0 >= budget_s:
+            break
+    dt = time.perf_counter() - t0
+    return {"value": n * subs / dt, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"{workload}: {steps} full step(s) = {subs} substeps of {n} particles "
+                      f"after 1 warm-up step, {dt:.1f} s (P2G, density and constitutive "
+                      "update sequential as in the reference; G2P gather on all threads)",
+            "seconds": dt}
+
+
+def run_reference(args):
+    """--impl reference: the oracle on the host cores, same workload and metric."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    from oracle.oracle import OracleSimulation, set_threads
+    threads = set_threads(0)
+    sim = build_scene(OracleSimulation, args.workload)
+    n = sim.particle_count()
+    for _ in range(args.warmup):
+        sim.step()
+    subs = 0
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        sim.step()
+        subs += sim.last_substeps()
+    dt = time.perf_counter() - t0
+    value = n * subs / dt
+    spec = WORKLOADS[args.workload]
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT,
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": dt * 1000.0 / max(args.steps, 1), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded scene generator, tests/scenes.py)",
+        "config": {"workload": args.workload, "description": spec["desc"], "particles": n,
+                   "grid": spec["grid_res"], "substeps": subs},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
+                         "sample": f"{args.steps} full steps ({subs} substeps) of {n} particles"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--workload", default=DEFAULT_WORKLOAD, choices=sorted(WORKLOADS))
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-extras", action="store_true",
+                    help="skip e2e, roofline instrumentation and CPU baseline (profiling runs)")
+    ap.add_argument("--cpu-budget", type=float, default=15.0)
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3) if args.impl == "ours" else args.warmup
+
+    if args.impl == "reference":
+        run_reference(args)
+        return
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist_mod
+        torch.cuda.set_device(local_rank)
+        dist_mod.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+        dist = dist_mod
+
+    from emerge_engine_b200 import Simulation
+    from emerge_engine_b200.abi import OPT_USE_GRAPH
+    from emerge_engine_b200.build import build
+    build()
+
+    spec = WORKLOADS[args.workload]
+    sim = build_scene(Simulation, args.workload, device=local_rank)
+    n = sim.particle_count()
+    for _ in range(args.warmup):
+        sim.step()
+    sim.synchronize()
+
+    def barrier():
+        if dist is not None:
+            import torch
+            dist.barrier(device_ids=[local_rank])
+            torch.cuda.synchronize()
+        sim.synchronize()
+
+    clocks = ClockSampler(local_rank)
+    st0 = sim.stats()
+    barrier()
+    clocks.start()
+    total_ms = 0.0
+    for _ in range(args.steps):
+        sim.flush_l2()
+        sim.event_record(0)
+        sim.step()
+        sim.event_record(1)
+        total_ms += sim.event_elapsed_ms(0, 1)
+    sim.synchronize()
+    clock_info = clocks.stop()
+    st1 = sim.stats()
+    barrier()
+    substeps = st1["substeps"] - st0["substeps"]
+    launches = st1["kernel_launches"] - st0["kernel_launches"]
+    units = float(n * substeps)
+    if dist is not None:
+        import torch
+        t = torch.tensor([total_ms], dtype=torch.float64, device=f"cuda:{local_rank}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+        u = torch.tensor([units, float(launches)], dtype=torch.float64, device=f"cuda:{local_rank}")
+        dist.all_reduce(u, op=dist.ReduceOp.SUM)
+        units, launches = float(u[0].item()), int(u[1].item())
+    value = units / (total_ms / 1000.0)
+    ms_per_step = total_ms / args.steps
+
+    extras = {}
+    if not args.no_extras:
+        # Roofline of the dominant kernel: the fused particle pass, timed per launch with
+        # CUDA events on the simulation's stream (host-driven substep loop, same kernels).
+        sim.set_option(OPT_USE_GRAPH, 0)
+        part_us, subs_i = 0.0, 0
+        for _ in range(3):
+            sim.flush_l2()
+            sim.step_n(1, timing=True)
+            part_us += sim.last_timing["g2p_us"]
+            subs_i += sim.last_substeps()
+        sim.set_option(OPT_USE_GRAPH, 1)
+        peak, peak_kind = load_peaks()
+        per_launch_s = part_us * 1e-6 / max(subs_i, 1)
+        alg_bytes = K_PARTICLE_BYTES[spec["material"]] * n
+        achieved = alg_bytes / per_launch_s / 1e9
+        traffic = profile_traffic(args.workload)
+        extras["roofline"] = {
+            "kernel": "k_particle (fused G2P + update + CFL + projection + P2G)",
+            "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+            "frac": achieved / peak, "traffic": traffic,
+            "algorithmic_bytes_per_launch": alg_bytes, "launch_us": per_launch_s * 1e6,
+            "peak_source": f"{peak_kind} hbm_gbs (MEASURED_PEAKS.json)" if peak_kind == "measured"
+            else "fallback 6.65 TB/s"}
+
+        # End to end through the C ABI with host buffers: upload the particle state from
+        # pinned memory, step, read it back, every step.
+        from emerge_engine_b200.simulation import PinnedBuffer
+        host = PinnedBuffer(n * 128)
+        sim.read_particles_raw(host.ptr, n)
+        e2e_steps = max(3, min(args.steps, 10))
+        sub0 = sim.stats()["substeps"]
+        sim.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(e2e_steps):
+            sim.write_particles_raw(host.ptr, n)
+            sim.step()
+            sim.read_particles_raw(host.ptr, n)
+        e2e_s = time.perf_counter() - t0
+        e2e_subs = sim.stats()["substeps"] - sub0
+        e2e_units = float(n * e2e_subs)
+        if dist is not None:
+            import torch
+            t = torch.tensor([e2e_s], dtype=torch.float64, device=f"cuda:{local_rank}")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            e2e_s = float(t.item())
+            u = torch.tensor([e2e_units], dtype=torch.float64, device=f"cuda:{local_rank}")
+            dist.all_reduce(u, op=dist.ReduceOp.SUM)
+            e2e_units = float(u.item())
+        host.free()
+        extras["e2e"] = {"value": e2e_units / e2e_s, "unit": UNIT,
+                         "h2d_bytes_per_step": n * 128, "d2h_bytes_per_step": n * 128,
+                         "steps": e2e_steps, "timing": "host wall clock around the C-ABI calls"}
+        if world == 1 and rank == 0:
+            extras["cpu_baseline"] = cpu_baseline(args.workload, args.cpu_budget)
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded scene generator, tests/scenes.py)",
+            "config": {"workload": args.workload, "description": spec["desc"],
+                       "particles_per_gpu": n, "grid": spec["grid_res"],
+                       "substeps_per_step": substeps / args.steps,
+                       "l2": "flushed (512 MiB write) before every timed step",
+                       "parallelism": f"replicas x{world}"},
+            "gpu_launches": launches,
+            "clocks": clock_info,
+        }
+        line.update(extras)
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -134,6 +134,12 @@ class StepTimingC(Structure):
         "spatial_hash_us", "phase_sleep_us", "project_us", "density_us", "total_us")]
 
 
+class StatsC(Structure):
+    """`emerge_stats` (include/emerge_cuda.h)."""
+    _fields_ = [(name, c_uint64) for name in (
+        "steps", "substeps", "kernel_launches", "p2g_blocks", "p2g_fallback_blocks", "sorts")]
+
+
 # Entry points declared in include/emerge_cuda.h: (name, restype, argtypes)
 SIM = c_void_p
 ABI_FUNCTIONS = [
@@ -161,6 +167,12 @@ ABI_FUNCTIONS = [
     ("emerge_cuda_sort_keys", c_int, [c_void_p, c_uint64, c_uint32, c_int, c_void_p, c_void_p]),
     ("emerge_cuda_stream", c_void_p, [SIM]),
     ("emerge_cuda_kernel_launches", c_int, [SIM, POINTER(c_uint64)]),
+    ("emerge_cuda_event_record", c_int, [SIM, c_int]),
+    ("emerge_cuda_event_elapsed", c_int, [SIM, c_int, c_int, POINTER(c_float)]),
+    ("emerge_cuda_flush_l2", c_int, [SIM]),
+    ("emerge_cuda_host_alloc", c_int, [ctypes.c_size_t, POINTER(c_void_p)]),
+    ("emerge_cuda_host_free", c_int, [c_void_p]),
+    ("emerge_cuda_stats", c_int, [SIM, POINTER(StatsC)]),
 ]
 
 _lib = None

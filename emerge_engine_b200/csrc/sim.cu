@@ -159,7 +159,10 @@ struct emerge_sim {
     bool graph_dirty = true;
     unsigned long long host_launches = 0;
     unsigned long long graph_launches = 0;
+    unsigned long long sorts = 0;
     cudaEvent_t ev[8] = {};
+    cudaEvent_t user_ev[16] = {};
+    Buffer flushbuf;
     emerge_step_timing last_timing{};
 
     int fail(emerge_status st, const std::string &msg) {
@@ -416,6 +419,7 @@ emerge_status sort_particles(emerge_sim *s, int key_mode) {
     launch_permute(s->P[s->cur], s->P[s->cur ^ 1], s->sort.vals[r], n, s->stream);
     s->host_launches += 2 + 5 * ((bits + 7) / 8);
     s->cur ^= 1;
+    s->sorts += 1;
     s->graph_dirty = true;
     s->sorted_once = true;
     s->steps_since_sort = 0;
@@ -841,6 +845,9 @@ emerge_status emerge_cuda_destroy(emerge_sim *s) {
     destroy_graph(s);
     for (auto &ev : s->ev)
         if (ev) cudaEventDestroy(ev);
+    for (auto &ev : s->user_ev)
+        if (ev) cudaEventDestroy(ev);
+    s->flushbuf.reset();
     if (s->h_state) cudaFreeHost(s->h_state);
     s->pbuf.reset();
     s->staging.reset();
@@ -1151,6 +1158,61 @@ done:
 }
 
 void *emerge_cuda_stream(emerge_sim *s) { return s ? static_cast<void *>(s->stream) : nullptr; }
+
+emerge_status emerge_cuda_event_record(emerge_sim *s, int slot) {
+    if (!s || slot < 0 || slot >= 16) return EMERGE_ERR_INVALID_ARG;
+    if (!s->user_ev[slot]) CK(cudaEventCreate(&s->user_ev[slot]));
+    CK(cudaEventRecord(s->user_ev[slot], s->stream));
+    return EMERGE_OK;
+}
+
+emerge_status emerge_cuda_event_elapsed(emerge_sim *s, int from, int to, float *ms) {
+    if (!s || !ms || from < 0 || from >= 16 || to < 0 || to >= 16 || !s->user_ev[from] ||
+        !s->user_ev[to])
+        return EMERGE_ERR_INVALID_ARG;
+    CK(cudaEventSynchronize(s->user_ev[to]));
+    CK(cudaEventElapsedTime(ms, s->user_ev[from], s->user_ev[to]));
+    return EMERGE_OK;
+}
+
+emerge_status emerge_cuda_flush_l2(emerge_sim *s) {
+    if (!s) return EMERGE_ERR_INVALID_ARG;
+    const size_t bytes = size_t(512) << 20;  // 512 MiB > 126 MB L2
+    if (!s->flushbuf.ptr) {
+        CK(cudaMalloc(&s->flushbuf.ptr, bytes));
+        s->flushbuf.bytes = bytes;
+    }
+    CK(cudaMemsetAsync(s->flushbuf.ptr, static_cast<int>(s->host_launches & 0xff), bytes, s->stream));
+    return EMERGE_OK;
+}
+
+emerge_status emerge_cuda_host_alloc(size_t bytes, void **out) {
+    if (!out) return EMERGE_ERR_INVALID_ARG;
+    cudaError_t e = cudaMallocHost(out, bytes);
+    if (e != cudaSuccess) {
+        g_global_error = cudaGetErrorString(e);
+        return EMERGE_ERR_OOM;
+    }
+    return EMERGE_OK;
+}
+
+emerge_status emerge_cuda_host_free(void *ptr) {
+    if (ptr) cudaFreeHost(ptr);
+    return EMERGE_OK;
+}
+
+emerge_status emerge_cuda_stats(emerge_sim *s, emerge_stats *out) {
+    if (!s || !out) return EMERGE_ERR_INVALID_ARG;
+    emerge_status st = sync_state(s);
+    if (st != EMERGE_OK) return st;
+    out->steps = s->h_state->total_steps;
+    out->substeps = s->h_state->total_substeps;
+    out->kernel_launches = s->host_launches + s->graph_launches + s->h_state->graph_kernels;
+    out->p2g_blocks = s->h_state->window_blocks;
+    out->p2g_fallback_blocks = s->h_state->window_fallback;
+    out->sorts = s->sorts;
+    return EMERGE_OK;
+}
 
 emerge_status emerge_cuda_kernel_launches(emerge_sim *s, uint64_t *out) {
     if (!s || !out) return EMERGE_ERR_INVALID_ARG;

@@ -251,6 +251,57 @@ class Simulation:
     def stream_handle(self) -> int:
         return int(self._lib.emerge_cuda_stream(self._sim) or 0)
 
+    # ---------------------------------------------------------------- measurement
+    def event_record(self, slot: int) -> None:
+        self._check(self._lib.emerge_cuda_event_record(self._sim, int(slot)))
+
+    def event_elapsed_ms(self, a: int, b: int) -> float:
+        v = c_float()
+        self._check(self._lib.emerge_cuda_event_elapsed(self._sim, int(a), int(b), byref(v)))
+        return float(v.value)
+
+    def flush_l2(self) -> None:
+        self._check(self._lib.emerge_cuda_flush_l2(self._sim))
+
+    def stats(self) -> dict:
+        st = abi.StatsC()
+        self._check(self._lib.emerge_cuda_stats(self._sim, byref(st)))
+        return {name: int(getattr(st, name)) for name, _ in abi.StatsC._fields_}
+
+    def write_particles_raw(self, ptr: int, n: int) -> None:
+        """Upload `n` particles from host memory at address `ptr` (AoS, 128 B each)."""
+        self._check(self._lib.emerge_cuda_write_particles(self._sim, c_void_p(ptr), int(n)))
+
+    def read_particles_raw(self, ptr: int, n: int) -> None:
+        """Read back `n` particles into host memory at address `ptr` (AoS, 128 B each)."""
+        self._check(self._lib.emerge_cuda_read_particles(self._sim, c_void_p(ptr), int(n)))
+
+
+class PinnedBuffer:
+    """Page-locked host buffer from the CUDA library (cudaMallocHost)."""
+
+    def __init__(self, nbytes: int):
+        self._lib = load_library()
+        ptr = c_void_p()
+        check(self._lib, self._lib.emerge_cuda_host_alloc(int(nbytes), byref(ptr)))
+        self.ptr = int(ptr.value)
+        self.nbytes = int(nbytes)
+
+    def as_particles(self, n: int) -> np.ndarray:
+        buf = (ctypes.c_char * (n * PARTICLE_DTYPE.itemsize)).from_address(self.ptr)
+        return np.frombuffer(buf, dtype=PARTICLE_DTYPE, count=n)
+
+    def free(self) -> None:
+        if self.ptr:
+            self._lib.emerge_cuda_host_free(c_void_p(self.ptr))
+            self.ptr = 0
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
 
 class DeterministicSimulation(Simulation):
     """`Simulation` in the reference-order mode (per-cell sums in particle index order)."""

@@ -306,6 +306,29 @@ emerge_status emerge_cuda_sort_keys(const float *xy, uint64_t n, uint32_t grid_r
 
 /* The CUDA stream the simulation's work runs on (cudaStream_t as void*). */
 void *emerge_cuda_stream(emerge_sim *sim);
+
+/* ---- measurement helpers (no reference counterpart) --------------------------------- */
+
+/* Records CUDA event `slot` (0..15) on the simulation's stream. */
+emerge_status emerge_cuda_event_record(emerge_sim *sim, int slot);
+/* Milliseconds between two recorded events (synchronises on `to`). */
+emerge_status emerge_cuda_event_elapsed(emerge_sim *sim, int from, int to, float *ms);
+/* Evicts the L2 cache: writes a device buffer larger than L2 on the simulation's stream. */
+emerge_status emerge_cuda_flush_l2(emerge_sim *sim);
+/* Page-locked host memory for fast uploads/readbacks (cudaMallocHost). */
+emerge_status emerge_cuda_host_alloc(size_t bytes, void **out);
+emerge_status emerge_cuda_host_free(void *ptr);
+
+/* Lifetime counters of a simulation. Synchronises. */
+typedef struct emerge_stats {
+    uint64_t steps;              /* Simulation::step calls executed */
+    uint64_t substeps;           /* substeps executed */
+    uint64_t kernel_launches;    /* kernels of this library executed (see emerge_cuda_kernel_launches) */
+    uint64_t p2g_blocks;         /* CTAs of the particle/density passes */
+    uint64_t p2g_fallback_blocks;/* of which scattered with global reductions (window did not fit) */
+    uint64_t sorts;              /* particle re-sorts */
+} emerge_stats;
+emerge_status emerge_cuda_stats(emerge_sim *sim, emerge_stats *out);
 /* Number of kernels this library launched on `sim` since creation (graph launches
  * count every kernel node executed, substep loops included). Synchronises. */
 emerge_status emerge_cuda_kernel_launches(emerge_sim *sim, uint64_t *out);
