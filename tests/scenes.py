@@ -12,10 +12,10 @@ from emerge_engine_b200 import (DruckerPragerMaterial, NaccMaterial, NeoHookeanM
                                 StomakhinMaterial)
 
 
-def quickstart(sim_cls):
+def quickstart(sim_cls, **sim_kw):
     """README quick start (README.md:20-49): NeoHookean 12x12 block + fluid 12x8 block."""
     cfg = SimConfig.standard(64, 0.05, (0.0, -1.0))
-    sim = (sim_cls.empty(cfg)
+    sim = (sim_cls.empty(cfg, **sim_kw)
            .with_default_material(NeoHookeanMaterial.new(400.0, 200.0))
            .with_material(1, NewtonianFluidMaterial.low_viscosity(1000.0, 1e4))
            .with_boundary(SlipBoundary(2)))
@@ -28,13 +28,13 @@ def quickstart(sim_cls):
     return sim
 
 
-def dam_break(sim_cls, grid_res=512, column=256, seed=1, gravity=-1.0):
+def dam_break(sim_cls, grid_res=512, column=256, seed=1, gravity=-1.0, **sim_kw):
     """Dam break: a `column` x `column` water column at 4 particles per cell (spacing 0.5,
     seeded jitter of +-0.25 cell) in the lower-left corner of a grid_res^2 grid.
     NewtonianFluid Tait EOS rho0 = 1000, stiffness 1e4, gamma 7; particle mass
     rho0 * spacing^2 = 250 so the rest density matches rho0."""
     cfg = SimConfig.standard(grid_res, 0.05, (0.0, gravity))
-    sim = sim_cls.empty(cfg).with_default_material(
+    sim = sim_cls.empty(cfg, **sim_kw).with_default_material(
         NewtonianFluidMaterial.low_viscosity(1000.0, 1e4))
     s = SpawnRegion.for_sim(cfg)
     t = cfg.boundary_thickness
@@ -49,33 +49,52 @@ def dam_break(sim_cls, grid_res=512, column=256, seed=1, gravity=-1.0):
 
 
 def granular_blocks(grid_res, target_particles, seed=42, side_range=(16, 128), spacing=0.5):
-    """Seeded non-overlapping axis-aligned blocks (side uniform in side_range cells) inside
-    [t, grid_res - t), until the particle target is reached.  Returns (x, y, w, h, mat)."""
+    """Seeded axis-aligned blocks with sides in side_range cells: a guillotine partition of
+    [t, grid_res - t)^2 (split each rectangle at a random position until both sides are at
+    most side_range[1], never below side_range[0]), then blocks are kept in seeded random
+    order until the particle target is reached; the dropped blocks leave voids.  Each block
+    gets a material index uniform over {0, 1, 2}.  Returns [(x0, y0, w, h, mat)]."""
     rng = np.random.default_rng(seed)
     t = 2
-    occ = np.zeros((grid_res, grid_res), dtype=bool)
-    blocks, count, tries = [], 0, 0
-    per_cell = int(round(1.0 / spacing)) ** 2
-    while count < target_particles and tries < 20000:
-        tries += 1
-        w, h = (int(v) for v in rng.integers(side_range[0], side_range[1] + 1, size=2))
-        x0 = int(rng.integers(t, grid_res - t - w))
-        y0 = int(rng.integers(t, grid_res - t - h))
-        if occ[x0:x0 + w, y0:y0 + h].any():
+    lo, hi = side_range
+    stack = [(t, t, grid_res - 2 * t, grid_res - 2 * t)]
+    leaves = []
+    while stack:
+        x0, y0, w, h = stack.pop()
+        axis = None
+        if w > hi and (h <= hi or w >= h):
+            axis = 0
+        elif h > hi:
+            axis = 1
+        if axis is None:
+            leaves.append((x0, y0, w, h))
             continue
-        occ[max(x0 - 1, 0):x0 + w + 1, max(y0 - 1, 0):y0 + h + 1] = True
-        mat = int(rng.integers(0, 3))
-        blocks.append((x0, y0, w, h, mat))
+        side = w if axis == 0 else h
+        cut = int(rng.integers(lo, side - lo + 1))
+        if axis == 0:
+            stack += [(x0, y0, cut, h), (x0 + cut, y0, w - cut, h)]
+        else:
+            stack += [(x0, y0, w, cut), (x0, y0 + cut, w, h - cut)]
+    per_cell = int(round(1.0 / spacing)) ** 2
+    order = rng.permutation(len(leaves))
+    blocks, count = [], 0
+    for k in order:
+        if count >= target_particles:
+            break
+        x0, y0, w, h = leaves[k]
+        blocks.append((x0, y0, w, h, int(rng.integers(0, 3))))
         count += w * h * per_cell
+    blocks.sort()
     return blocks
 
 
-def mixed_granular(sim_cls, grid_res=1024, target_particles=4_000_000, seed=42, gravity=-1.0):
+def mixed_granular(sim_cls, grid_res=1024, target_particles=4_000_000, seed=42, gravity=-1.0,
+                   **sim_kw):
     """Mixed granular: seeded random blocks (16-128 cells a side), each block uniformly
     DruckerPrager sand, Stomakhin snow or NACC soil with the reference's canonical
     constructors (sand.rs:106, snow.rs:68, nacc.rs:93), 4 particles per cell."""
     cfg = SimConfig.standard(grid_res, 0.05, (0.0, gravity))
-    sim = (sim_cls.empty(cfg)
+    sim = (sim_cls.empty(cfg, **sim_kw)
            .with_default_material(DruckerPragerMaterial.cohesionless(1e5, 0.2))
            .with_material(1, StomakhinMaterial.from_young_modulus(1.4e5, 0.2))
            .with_material(2, NaccMaterial.soft_clay(5e4, 0.3)))
