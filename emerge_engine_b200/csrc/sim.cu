@@ -46,11 +46,6 @@ struct Carver {
     }
 };
 
-size_t particle_set_bytes(size_t cap) {
-    // 2 float2 + 2 float4 + 12 four-byte scalars + float2 + slot index + rho_dp, + alignment
-    return cap * (8 * 2 + 16 * 2 + 4 * 16 + 8 + 4 + 4) + 32 * 256;
-}
-
 DevParticles carve_particles(Carver &c, size_t cap) {
     DevParticles P;
     P.x = c.take<float2>(cap);
@@ -78,6 +73,14 @@ DevParticles carve_particles(Carver &c, size_t cap) {
     P.slot_to_index = c.take<uint32_t>(cap);
     P.rho_dp = c.take<float>(cap);
     return P;
+}
+
+// Exact size of one particle set: a dry-run carve from address 0, so the allocation
+// and carve_particles can never disagree.
+size_t particle_set_bytes(size_t cap) {
+    Carver c(nullptr);
+    carve_particles(c, cap);
+    return static_cast<size_t>(c.p) + 256;
 }
 
 bool model_supported(uint32_t m) {
@@ -294,13 +297,19 @@ emerge_status ensure_capacity(emerge_sim *s, size_t need) {
     if (need <= s->cap) return EMERGE_OK;
     size_t cap = s->cap ? s->cap : 1024;
     while (cap < need) cap *= 2;
-    size_t bytes = 2 * particle_set_bytes(cap);
+    const size_t set_bytes = particle_set_bytes(cap);
+    size_t bytes = 2 * set_bytes;
     void *ptr = nullptr;
     CK(cudaMalloc(&ptr, bytes));
     Carver c(ptr);
     DevParticles np[2];
     np[0] = carve_particles(c, cap);
+    c.p = reinterpret_cast<uintptr_t>(ptr) + set_bytes;
     np[1] = carve_particles(c, cap);
+    if (c.p > reinterpret_cast<uintptr_t>(ptr) + bytes) {
+        cudaFree(ptr);
+        return static_cast<emerge_status>(s->fail(EMERGE_ERR_OOM, "particle carve exceeds allocation"));
+    }
     if (s->n > 0) {
         // move the live set into np[0] (same slot order)
         std::vector<uint32_t> ident;  // identity permutation via a device copy of slots
