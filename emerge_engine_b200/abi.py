@@ -30,7 +30,7 @@ STATUS_NAMES = {0: "OK", 1: "INVALID_ARG", 2: "UNSUPPORTED", 3: "CUDA", 4: "TIME
 
 OPT_USE_GRAPH = 1
 OPT_SORT_INTERVAL = 2
-OPT_P2G_WINDOW = 3
+OPT_P2G_AGGREGATE = 3
 OPT_DETERMINISTIC = 4
 OPT_PRECISE_MATH = 5
 
@@ -191,7 +191,7 @@ def load_library(path: str | None = None) -> ctypes.CDLL:
     global _lib
     if _lib is not None and path is None:
         return _lib
-    p = path or LIB_PATH
+    p = path or os.environ.get("EMERGE_CUDA_LIB") or LIB_PATH
     if not os.path.exists(p):
         raise RuntimeError(
             f"CUDA backend library not found at {p}; build it with "

@@ -156,7 +156,7 @@ struct emerge_sim {
     bool pending_valid = false;  // the next substep's P2G (+density) is already on the grid
     int use_graph = 1;
     int use_window = 1;
-    int64_t sort_interval = 0;   // 0 = adaptive
+    int64_t sort_interval = 8;   // re-sort every N steps; 0 = keep the first sort
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t graph_exec = nullptr;
     bool graph_dirty = true;
@@ -436,23 +436,16 @@ emerge_status sort_particles(emerge_sim *s, int key_mode) {
     return EMERGE_OK;
 }
 
-// Particle order policy: sort when never sorted, every sort_interval steps when
-// set, else when more than 5% of the particle-pass CTAs since the last sort had
-// to fall back to global reductions (their stencils no longer fit one window).
+// Particle order policy: sort by tile before the first step after particles are
+// added, then every sort_interval steps (0: never again).  Sorting changes no result
+// beyond float summation order; it keeps each warp's particles in few cells so the
+// warp-aggregated P2G issues few reductions and the G2P gather stays cache-local.
 emerge_status maybe_sort(emerge_sim *s) {
     bool need = !s->sorted_once;
-    if (!need && s->sort_interval > 0) need = s->steps_since_sort >= static_cast<uint64_t>(s->sort_interval);
-    if (!need && s->sort_interval == 0 && s->use_window) {
-        // the pinned mirror is refreshed after every step launch (async); use what is there
-        unsigned long long fb = s->h_state->window_fallback - s->fallback_at_sort;
-        unsigned long long bl = s->h_state->window_blocks - s->blocks_at_sort;
-        if (bl > 0 && fb * 20 > bl) need = true;
-    }
+    if (!need && s->sort_interval > 0)
+        need = s->steps_since_sort >= static_cast<uint64_t>(s->sort_interval);
     if (!need) return EMERGE_OK;
-    emerge_status st = sort_particles(s, 0);
-    s->fallback_at_sort = s->h_state->window_fallback;
-    s->blocks_at_sort = s->h_state->window_blocks;
-    return st;
+    return sort_particles(s, 0);
 }
 
 emerge_status run_host_loop_step(emerge_sim *s, bool timed) {
@@ -1092,7 +1085,7 @@ emerge_status emerge_cuda_set_option(emerge_sim *s, int option, int64_t value) {
         if (value < 0) return static_cast<emerge_status>(s->fail(EMERGE_ERR_INVALID_ARG, "sort interval < 0"));
         s->sort_interval = value;
         return EMERGE_OK;
-    case EMERGE_OPT_P2G_WINDOW:
+    case EMERGE_OPT_P2G_AGGREGATE:
         s->use_window = value != 0;
         s->graph_dirty = true;
         return EMERGE_OK;

@@ -107,6 +107,41 @@ __device__ __forceinline__ void store_changed(const DevParticles &P, int i, cons
     if (neq(p.lvs, o.lvs)) P.lvs[i] = p.lvs;
 }
 
+// Fields the particle pass may leave unchanged (x, v and C always change in G2P):
+// kept to skip stores of bitwise-equal values.
+struct Saved {
+    M2 f;
+    float mass, v0, vol, rho, jp, h, q, lvs;
+};
+__device__ __forceinline__ Saved save_fields(const PState &p) {
+    Saved o;
+    o.f = p.f;
+    o.mass = p.mass;
+    o.v0 = p.v0;
+    o.vol = p.vol;
+    o.rho = p.rho;
+    o.jp = p.jp;
+    o.h = p.h;
+    o.q = p.q;
+    o.lvs = p.lvs;
+    return o;
+}
+__device__ __forceinline__ void store_fields(const DevParticles &P, int i, const Saved &o,
+                                             const PState &p) {
+    P.x[i] = p.x;
+    P.v[i] = p.v;
+    P.c[i] = m_to4(p.c);
+    if (neqm(p.f, o.f)) P.f[i] = m_to4(p.f);
+    if (neq(p.mass, o.mass)) P.mass[i] = p.mass;
+    if (neq(p.v0, o.v0)) P.v0[i] = p.v0;
+    if (neq(p.vol, o.vol)) P.vol[i] = p.vol;
+    if (neq(p.rho, o.rho)) P.rho[i] = p.rho;
+    if (neq(p.jp, o.jp)) P.jp[i] = p.jp;
+    if (neq(p.h, o.h)) P.h[i] = p.h;
+    if (neq(p.q, o.q)) P.q[i] = p.q;
+    if (neq(p.lvs, o.lvs)) P.lvs[i] = p.lvs;
+}
+
 // G2P phase 1 for one particle (transfer/g2p.rs:217-326 with ASFLIP, contact and
 // mixture gated off).  Returns 1 if the speed clamp fired.
 __device__ __forceinline__ int g2p_particle(const GridView &g, const DevConfig &cfg, float dt,
@@ -152,13 +187,13 @@ __device__ __forceinline__ int g2p_particle(const GridView &g, const DevConfig &
 }
 
 // ---------------------------------------------------------------- scatter engine
-// A CTA scatters the 3x3 stencils of up to PPT*THREADS particles.  When the union
-// of their stencils fits in WINDOW_CELLS cells, contributions accumulate in
-// shared memory (red.shared) and each touched cell is flushed once with a vector
-// red.global; otherwise every contribution goes straight to global memory.
+// P2G scatter of a CTA's particles with warp-aggregated global reductions.  Within a
+// warp, lanes whose particles share a base cell (contiguous after the tile sort) have
+// the same 9 target cells; for each stencil slot a segmented shuffle reduction sums
+// their contributions into the segment's first lane, which issues one vector
+// red.global.add per target cell.  No float atomics in shared memory.
 constexpr int THREADS = 256;
 constexpr int PPT = 2;
-constexpr int WINDOW_CELLS = 1024;
 
 struct Payload {
     float2 x;
@@ -173,13 +208,7 @@ struct Payload {
     bool do_s;    // scatter stress impulse
 };
 
-struct ScatterShared {
-    float m[WINDOW_CELLS], ax[WINDOW_CELLS], ay[WINDOW_CELLS], sx[WINDOW_CELLS], sy[WINDOW_CELLS];
-    int red_i[4][THREADS / 32];
-    int box[4];
-    int use_window;
-};
-
+// Stencil slot k (0..8, gx = k / 3, gy = k % 3) of one particle.
 __device__ __forceinline__ void cell_contrib(const Payload &pl, int gx, int gy, const QW &w,
                                              float &mc, float2 &a, float2 &s, int &cx, int &cy) {
     float weight = w.wx[gx] * w.wy[gy];
@@ -197,125 +226,67 @@ __device__ __forceinline__ void mark_tile(const GridView &g, int cx, int cy) {
     if (g.tile_flag[t] == 0) g.tile_flag[t] = 1;
 }
 
-__device__ void scatter_block(ScatterShared &sh, const GridView &g, Payload (&pl)[PPT],
-                              int use_window, unsigned long long *fallback_ctr,
-                              unsigned long long *blocks_ctr) {
-    const int tid = threadIdx.x;
-    // 1. bounding box of base cells
-    int mnx = INT_MAX, mny = INT_MAX, mxx = INT_MIN, mxy = INT_MIN;
-    bool any = false;
+// Adds the values of lanes [lane, seg_end) into `lane` (suffix sums within segments).
+__device__ __forceinline__ float seg_sum(float v, int lane, int seg_end) {
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+        float y = __shfl_down_sync(0xffffffffu, v, off);
+        if (lane + off < seg_end) v += y;
+    }
+    return v;
+}
+
+__device__ void scatter_block(const GridView &g, Payload (&pl)[PPT], int aggregate) {
+    const int lane = threadIdx.x & 31;
 #pragma unroll
     for (int k = 0; k < PPT; ++k) {
-        if (pl[k].valid && (pl[k].do_ma || pl[k].do_s)) {
-            any = true;
-            mnx = min(mnx, pl[k].bx);
-            mny = min(mny, pl[k].by);
-            mxx = max(mxx, pl[k].bx);
-            mxy = max(mxy, pl[k].by);
-        }
-    }
-    mnx = warp_imin(mnx);
-    mny = warp_imin(mny);
-    mxx = warp_imax(mxx);
-    mxy = warp_imax(mxy);
-    int warp = tid >> 5, lane = tid & 31;
-    if (lane == 0) {
-        sh.red_i[0][warp] = mnx;
-        sh.red_i[1][warp] = mny;
-        sh.red_i[2][warp] = mxx;
-        sh.red_i[3][warp] = mxy;
-    }
-    int any_block = __syncthreads_or(any ? 1 : 0);
-    if (!any_block) return;
-    if (tid == 0) {
-        int a = INT_MAX, b = INT_MAX, c = INT_MIN, d = INT_MIN;
-        for (int w = 0; w < THREADS / 32; ++w) {
-            a = min(a, sh.red_i[0][w]);
-            b = min(b, sh.red_i[1][w]);
-            c = max(c, sh.red_i[2][w]);
-            d = max(d, sh.red_i[3][w]);
-        }
-        // window: cells [a-1, c+1] x [b-1, d+1]
-        long long ex = (long long)c - a + 3, ey = (long long)d - b + 3;
-        int fits = use_window && ex > 0 && ey > 0 && ex * ey <= WINDOW_CELLS;
-        sh.box[0] = a - 1;
-        sh.box[1] = b - 1;
-        sh.box[2] = static_cast<int>(fits ? ex : 0);
-        sh.box[3] = static_cast<int>(fits ? ey : 0);
-        sh.use_window = fits;
-        atomicAdd(blocks_ctr, 1ull);
-        if (!fits) atomicAdd(fallback_ctr, 1ull);
-    }
-    __syncthreads();
-    const int ox = sh.box[0], oy = sh.box[1], ex = sh.box[2], ey = sh.box[3];
-    if (sh.use_window) {
-        const int ncell = ex * ey;
-        for (int k = tid; k < ncell; k += THREADS) {
-            sh.m[k] = 0.0f;
-            sh.ax[k] = 0.0f;
-            sh.ay[k] = 0.0f;
-            sh.sx[k] = 0.0f;
-            sh.sy[k] = 0.0f;
-        }
-        __syncthreads();
+        const Payload &p = pl[k];
+        const bool active = p.valid && (p.do_ma || p.do_s);
+        const unsigned any_ma = __ballot_sync(0xffffffffu, active && p.do_ma);
+        const unsigned any_s = __ballot_sync(0xffffffffu, active && p.do_s);
+        if (!any_ma && !any_s) continue;
+        // segments: runs of consecutive lanes with the same base cell
+        const int key_x = active ? p.bx : INT_MIN, key_y = active ? p.by : lane;
+        const int px = __shfl_up_sync(0xffffffffu, key_x, 1);
+        const int py = __shfl_up_sync(0xffffffffu, key_y, 1);
+        const bool head = !aggregate || lane == 0 || !active || px != key_x || py != key_y;
+        const unsigned heads = __ballot_sync(0xffffffffu, head);
+        const unsigned after = heads & ~((2u << lane) - 1u);  // heads strictly above lane
+        const int seg_end = after ? __ffs(after) - 1 : 32;
+        QW w = quadratic_weights(p.x);
 #pragma unroll
-        for (int k = 0; k < PPT; ++k) {
-            const Payload &p = pl[k];
-            if (!p.valid || !(p.do_ma || p.do_s)) continue;
-            QW w = quadratic_weights(p.x);
+        for (int gx = 0; gx < 3; ++gx) {
 #pragma unroll
-            for (int gx = 0; gx < 3; ++gx)
-#pragma unroll
-                for (int gy = 0; gy < 3; ++gy) {
-                    float mc;
-                    float2 a, s;
-                    int cx, cy;
+            for (int gy = 0; gy < 3; ++gy) {
+                float mc = 0.0f;
+                float2 a = v2(0.0f, 0.0f), s = v2(0.0f, 0.0f);
+                int cx = 0, cy = 0;
+                if (active) {
                     cell_contrib(p, gx, gy, w, mc, a, s, cx, cy);
-                    int li = (cx - ox) * ey + (cy - oy);
-                    if (p.do_ma) {
-                        atomicAdd(&sh.m[li], mc);
-                        atomicAdd(&sh.ax[li], a.x);
-                        atomicAdd(&sh.ay[li], a.y);
+                    if (!p.do_ma) {
+                        mc = 0.0f;
+                        a = v2(0.0f, 0.0f);
                     }
-                    if (p.do_s) {
-                        atomicAdd(&sh.sx[li], s.x);
-                        atomicAdd(&sh.sy[li], s.y);
+                    if (!p.do_s) s = v2(0.0f, 0.0f);
+                }
+                if (aggregate) {
+                    if (any_ma) {
+                        mc = seg_sum(mc, lane, seg_end);
+                        a.x = seg_sum(a.x, lane, seg_end);
+                        a.y = seg_sum(a.y, lane, seg_end);
+                    }
+                    if (any_s) {
+                        s.x = seg_sum(s.x, lane, seg_end);
+                        s.y = seg_sum(s.y, lane, seg_end);
                     }
                 }
-        }
-        __syncthreads();
-        for (int k = tid; k < ncell; k += THREADS) {
-            float m = sh.m[k], ax = sh.ax[k], ay = sh.ay[k], sx = sh.sx[k], sy = sh.sy[k];
-            int cx = ox + k / ey, cy = oy + k % ey;
-            if (!in_domain(cx, cy, g.res)) continue;
-            bool nz_a = (m != 0.0f) || (ax != 0.0f) || (ay != 0.0f);
-            bool nz_s = (sx != 0.0f) || (sy != 0.0f);
-            if (!nz_a && !nz_s) continue;
-            int ci = cell_index(cx, cy, g.tpd);
-            if (nz_a) red_add_v4(&g.acc_a[ci], m, ax, ay, 0.0f);
-            if (nz_s) red_add_v2(&g.acc_s[ci], sx, sy);
-            mark_tile(g, cx, cy);
-        }
-    } else {
-#pragma unroll
-        for (int k = 0; k < PPT; ++k) {
-            const Payload &p = pl[k];
-            if (!p.valid || !(p.do_ma || p.do_s)) continue;
-            QW w = quadratic_weights(p.x);
-#pragma unroll
-            for (int gx = 0; gx < 3; ++gx)
-#pragma unroll
-                for (int gy = 0; gy < 3; ++gy) {
-                    float mc;
-                    float2 a, s;
-                    int cx, cy;
-                    cell_contrib(p, gx, gy, w, mc, a, s, cx, cy);
-                    if (!in_domain(cx, cy, g.res)) continue;
-                    int ci = cell_index(cx, cy, g.tpd);
-                    if (p.do_ma) red_add_v4(&g.acc_a[ci], mc, a.x, a.y, 0.0f);
-                    if (p.do_s) red_add_v2(&g.acc_s[ci], s.x, s.y);
+                if (head && active && in_domain(cx, cy, g.res)) {
+                    const int ci = cell_index(cx, cy, g.tpd);
+                    if (mc != 0.0f || a.x != 0.0f || a.y != 0.0f) red_add_v4(&g.acc_a[ci], mc, a.x, a.y, 0.0f);
+                    if (s.x != 0.0f || s.y != 0.0f) red_add_v2(&g.acc_s[ci], s.x, s.y);
                     mark_tile(g, cx, cy);
                 }
+            }
         }
     }
 }
@@ -337,8 +308,7 @@ struct ParticleKernelArgs {
     int emit_p2g;       // project for substep k+1 and scatter its P2G (fused pipeline)
 };
 
-__global__ void __launch_bounds__(THREADS) k_particle(ParticleKernelArgs a) {
-    __shared__ ScatterShared sh;
+__global__ void __launch_bounds__(THREADS, 3) k_particle(ParticleKernelArgs a) {
     __shared__ MatP s_mats[MAX_MATERIALS];
     __shared__ float s_red[2][THREADS / 32];
     for (int k = threadIdx.x; k < a.n_mats; k += THREADS) s_mats[k] = a.mats[k];
@@ -366,7 +336,7 @@ __global__ void __launch_bounds__(THREADS) k_particle(ParticleKernelArgs a) {
             PState p = load_state(a.P, i, a.lf);
             const MatP &m = s_mats[p.mat < static_cast<uint32_t>(a.n_mats) ? p.mat : 0u];
             if (a.mode_g2p) {
-                const PState o = p;
+                const Saved o = save_fields(p);
                 if (a.project_in) project_state(cfg, p);  // recompute S'(k); counted earlier
                 if (a.density_mode && a.project_in) {
                     float d = a.P.rho_dp[i];
@@ -377,7 +347,7 @@ __global__ void __launch_bounds__(THREADS) k_particle(ParticleKernelArgs a) {
                 }
                 clamped = g2p_particle(a.g, cfg, dt, p);
                 update_particle(m, p, dt, cfg.precise_math != 0);
-                store_changed(a.P, i, o, p);
+                store_fields(a.P, i, o, p);
             }
             // CFL contribution for the next substep (step.rs:447-466)
             float sp = vlen(p.v);
@@ -438,7 +408,8 @@ __global__ void __launch_bounds__(THREADS) k_particle(ParticleKernelArgs a) {
         atomicMin(&st->min_mdt_bits[acc_slot], __float_as_uint(md));
     }
 
-    scatter_block(sh, a.g, pl, a.use_window, &st->window_fallback, &st->window_blocks);
+    if (threadIdx.x == 0) atomicAdd(&st->window_blocks, 1ull);
+    scatter_block(a.g, pl, a.use_window);
 }
 
 // ---------------------------------------------------------------- k_density
@@ -457,7 +428,6 @@ struct DensityKernelArgs {
 // estimate_particle_volumes gather (solver/density.rs:50-71) at the projected
 // positions, stored as rho_dp, plus the stress scatter of fluid particles.
 __global__ void __launch_bounds__(THREADS) k_density(DensityKernelArgs a) {
-    __shared__ ScatterShared sh;
     __shared__ MatP s_mats[MAX_MATERIALS];
     for (int k = threadIdx.x; k < a.n_mats; k += THREADS) s_mats[k] = a.mats[k];
     __syncthreads();
@@ -503,7 +473,7 @@ __global__ void __launch_bounds__(THREADS) k_density(DensityKernelArgs a) {
             pl[k].by = w.by;
         }
     }
-    scatter_block(sh, a.g, pl, a.use_window, &a.st->window_fallback, &a.st->window_blocks);
+    scatter_block(a.g, pl, a.use_window);
 }
 
 // ---------------------------------------------------------------- grid update

@@ -267,10 +267,12 @@ emerge_status emerge_cuda_region_state(emerge_sim *sim, float cx, float cy, floa
  *   EMERGE_OPT_USE_GRAPH       1 = capture each step in a CUDA graph with a device-side
  *                              substep loop (default), 0 = host-driven substep loop with
  *                              per-phase event timing.
- *   EMERGE_OPT_SORT_INTERVAL   re-sort particles by tile every N steps (0 = adaptive,
- *                              default; see emerge_cuda_sort_now).
- *   EMERGE_OPT_P2G_WINDOW      1 = shared-memory window scatter (default), 0 = direct
- *                              global reductions.
+ *   EMERGE_OPT_SORT_INTERVAL   re-sort particles by tile every N steps (default 8;
+ *                              0 = only before the first step after particles are added;
+ *                              see emerge_cuda_sort_now).
+ *   EMERGE_OPT_P2G_AGGREGATE   1 = P2G contributions of lanes sharing a base cell are
+ *                              summed in the warp before one global reduction per cell
+ *                              (default), 0 = one global reduction per contribution.
  *   EMERGE_OPT_DETERMINISTIC   1 = reference-order mode: every grid cell sums its P2G and
  *                              density contributions sequentially in the reference's
  *                              particle index order (transfer/p2g.rs:16-23), so results
@@ -285,7 +287,7 @@ emerge_status emerge_cuda_region_state(emerge_sim *sim, float cx, float cy, floa
 enum {
     EMERGE_OPT_USE_GRAPH = 1,
     EMERGE_OPT_SORT_INTERVAL = 2,
-    EMERGE_OPT_P2G_WINDOW = 3,
+    EMERGE_OPT_P2G_AGGREGATE = 3,
     EMERGE_OPT_DETERMINISTIC = 4,
     EMERGE_OPT_PRECISE_MATH = 5
 };
