@@ -96,7 +96,8 @@ struct StepLaunch {
     StepState *st;
     GridView g;
     int density_mode;   // any registered material needs the density pass
-    int use_window;
+    int use_window;     // warp-aggregated P2G reductions
+    unsigned model_mask;  // bit m set: ConstitutiveModel m is registered
     cudaStream_t stream;
 };
 

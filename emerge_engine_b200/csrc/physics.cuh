@@ -290,6 +290,12 @@ EM_HD void nacc_project(const MatP &m, M2 f, float alpha, M2 &f_out, float &alph
     alpha_out = alpha;
 }
 
+// Kernels are specialised on the set of models present in a scene: MASK bit m set
+// means ConstitutiveModel m is compiled in; other models' code is left out.
+#define HAS_MODEL(mask, model) ((((mask) >> (model)) & 1u) != 0u)
+constexpr unsigned ALL_MODELS = (1u << M_FALLBACK) | (1u << M_FLUID) | (1u << M_NEOHOOKEAN) |
+                                (1u << M_SNOW) | (1u << M_DRUCKER_PRAGER) | (1u << M_NACC);
+
 // ---------------------------------------------------------------- particle view
 // Registers of one particle while a kernel works on it.
 struct PState {
@@ -304,10 +310,12 @@ struct PState {
 };
 
 // MaterialModel::kirchhoff_stress per model.
+template <unsigned MASK = ALL_MODELS>
 EM_HD M2 kirchhoff_stress(const MatP &m, const PState &p, bool pr) {
     const M2 f = p.f;
     switch (m.model) {
-    case M_NEOHOOKEAN: {  // elastic.rs:180-255; damage rate in cohesion_coeff (elastic.rs:284)
+    case M_NEOHOOKEAN: {
+        if constexpr (HAS_MODEL(MASK, M_NEOHOOKEAN)) {  // elastic.rs:180-255; damage rate in cohesion_coeff (elastic.rs:284)
         float j = mdet(f);
         if (j <= MIN_J) return mzero();
         float t_scale = 1.0f + m.thermal_expansion * p.temperature;
@@ -330,7 +338,10 @@ EM_HD M2 kirchhoff_stress(const MatP &m, const PState &p, bool pr) {
         }
         return madd(madd(dev_stress, vol_stress), viscous);
     }
-    case M_FLUID: {  // fluid.rs:135-191 (min_density 1e-6, fluid.rs:60)
+        return mzero();
+    }
+    case M_FLUID: {
+        if constexpr (HAS_MODEL(MASK, M_FLUID)) {  // fluid.rs:135-191 (min_density 1e-6, fluid.rs:60)
         float density = fminf(fmaxf(p.rho, 1.0e-6f), m.rest_density * 2.0f);
         float pressure = fmaxf(
             m.eos_stiffness * (em_pow(density / m.rest_density, m.eos_power, pr) - 1.0f),
@@ -351,7 +362,10 @@ EM_HD M2 kirchhoff_stress(const MatP &m, const PState &p, bool pr) {
         }
         return stress;
     }
-    case M_DRUCKER_PRAGER: {  // sand.rs:220-231
+        return mzero();
+    }
+    case M_DRUCKER_PRAGER: {
+        if constexpr (HAS_MODEL(MASK, M_DRUCKER_PRAGER)) {  // sand.rs:220-231
         float j = mdet(f);
         if (j <= MIN_J) return mzero();
         M2 r = polar(f);
@@ -359,7 +373,10 @@ EM_HD M2 kirchhoff_stress(const MatP &m, const PState &p, bool pr) {
         M2 b = smscale(m.lambda * (j - 1.0f) * j, mident());
         return madd(a, b);
     }
-    case M_SNOW: {  // snow.rs:109-136
+        return mzero();
+    }
+    case M_SNOW: {
+        if constexpr (HAS_MODEL(MASK, M_SNOW)) {  // snow.rs:109-136
         float j = mdet(f);
         if (j <= MIN_J) return mzero();
         M2 r = polar(f);
@@ -371,7 +388,10 @@ EM_HD M2 kirchhoff_stress(const MatP &m, const PState &p, bool pr) {
             tau = madd(tau, smscale(m.cohesion_coeff * p.jp * (j - 1.0f) * j, mident()));
         return tau;
     }
-    case M_NACC: {  // nacc.rs:236-249
+        return mzero();
+    }
+    case M_NACC: {
+        if constexpr (HAS_MODEL(MASK, M_NACC)) {  // nacc.rs:236-249
         float j = fmaxf(mdet(f), MIN_J);
         M2 b = mm(f, mtrans(f));
         float tr_b = b.xa.x + b.ya.y;
@@ -380,6 +400,8 @@ EM_HD M2 kirchhoff_stress(const MatP &m, const PState &p, bool pr) {
         M2 vol_stress = smscale(nacc_kappa(m) * 0.5f * (j * j - 1.0f), mident());
         return madd(dev_stress, vol_stress);
     }
+        return mzero();
+    }
     default:  // FallbackMaterial: zero stress (materials/mod.rs:362-366)
         return mzero();
     }
@@ -387,8 +409,9 @@ EM_HD M2 kirchhoff_stress(const MatP &m, const PState &p, bool pr) {
 
 // combined_kirchhoff_stress (spacetime/transfer.rs:77-104).  Only NeoHookean has a
 // non-zero activation_scale among the supported models (elastic.rs:271-273).
+template <unsigned MASK = ALL_MODELS>
 EM_HD M2 combined_kirchhoff_stress(const MatP &m, const PState &p, bool pr) {
-    M2 tau = kirchhoff_stress(m, p, pr);
+    M2 tau = kirchhoff_stress<MASK>(m, p, pr);
     float coeff = (m.model == M_NEOHOOKEAN) ? m.active_stress_coeff : 0.0f;
     if (p.activation <= 0.0f || coeff <= 0.0f) return tau;
     M2 tau_active;
@@ -413,10 +436,12 @@ EM_HD float stress_volume(const MatP &m, const PState &p) {
 }
 
 // MaterialModel::timestep_bound
+template <unsigned MASK = ALL_MODELS>
 EM_HD float timestep_bound(const MatP &m, float density, float h, float cell, float mat_cfl,
                            float visc_cfl, bool pr) {
     switch (m.model) {
-    case M_NEOHOOKEAN: {  // elastic.rs:290-327
+    case M_NEOHOOKEAN: {
+        if constexpr (HAS_MODEL(MASK, M_NEOHOOKEAN)) {  // elastic.rs:290-327
         float elastic_dt = elastic_wave_dt(m.lambda, m.mu, 1.0f, density, 1.0e-6f, cell, mat_cfl);
         float viscous_dt = INFINITY;
         if (m.dynamic_viscosity > 0.0f) {
@@ -426,7 +451,10 @@ EM_HD float timestep_bound(const MatP &m, float density, float h, float cell, fl
         }
         return fminf(elastic_dt, viscous_dt);
     }
-    case M_FLUID: {  // fluid.rs:228-259
+        return INFINITY;
+    }
+    case M_FLUID: {
+        if constexpr (HAS_MODEL(MASK, M_FLUID)) {  // fluid.rs:228-259
         const float MIN_DENSITY_RATIO = 1.0e-6f;
         float d = fmaxf(density, 1.0e-6f);
         float ratio = fmaxf(d / fmaxf(m.rest_density, 1.0e-6f), MIN_DENSITY_RATIO);
@@ -440,12 +468,21 @@ EM_HD float timestep_bound(const MatP &m, float density, float h, float cell, fl
         }
         return dt_bound;
     }
+        return INFINITY;
+    }
     case M_DRUCKER_PRAGER:  // sand.rs:345-362
-        return elastic_wave_dt(m.lambda, m.mu, 1.0f, density, MIN_J, cell, mat_cfl);
+        if constexpr (HAS_MODEL(MASK, M_DRUCKER_PRAGER))
+            return elastic_wave_dt(m.lambda, m.mu, 1.0f, density, MIN_J, cell, mat_cfl);
+        return INFINITY;
     case M_SNOW:  // snow.rs:193-211
-        return elastic_wave_dt(m.lambda, m.mu, h, density, MIN_J, cell, mat_cfl);
-    case M_NACC: {  // nacc.rs:279-298: lambda = kappa - mu = params().lambda
+        if constexpr (HAS_MODEL(MASK, M_SNOW))
+            return elastic_wave_dt(m.lambda, m.mu, h, density, MIN_J, cell, mat_cfl);
+        return INFINITY;
+    case M_NACC: {
+        if constexpr (HAS_MODEL(MASK, M_NACC)) {  // nacc.rs:279-298: lambda = kappa - mu = params().lambda
         return elastic_wave_dt(m.lambda, m.mu, h, density, 1.0e-6f, cell, mat_cfl);
+    }
+        return INFINITY;
     }
     default:
         return INFINITY;
@@ -484,15 +521,20 @@ EM_HD void dp_finish(const MatP &m, PState &p, M2 u, float2 sigma, M2 vt, bool p
 }
 
 // MaterialModel::update_particle
+template <unsigned MASK = ALL_MODELS>
 EM_HD void update_particle(const MatP &m, PState &p, float dt, bool pr) {
     switch (m.model) {
-    case M_NEOHOOKEAN: {  // elastic.rs:262-269
+    case M_NEOHOOKEAN: {
+        if constexpr (HAS_MODEL(MASK, M_NEOHOOKEAN)) {  // elastic.rs:262-269
         M2 fp_new = madd(mident(), smscale(dt, p.c));
         p.f = mm(fp_new, p.f);
         sync_volume_density(p);
         break;
     }
-    case M_FLUID: {  // fluid.rs:197-207; settling_damping in dp_h0 (fluid.rs:223)
+        break;
+    }
+    case M_FLUID: {
+        if constexpr (HAS_MODEL(MASK, M_FLUID)) {  // fluid.rs:197-207; settling_damping in dp_h0 (fluid.rs:223)
         float j = fclampf(mdet(p.f), 0.5f, 2.0f);
         float s = sqrtf(j);
         p.f = m2(v2(s, 0.0f), v2(0.0f, s));
@@ -503,7 +545,10 @@ EM_HD void update_particle(const MatP &m, PState &p, float dt, bool pr) {
         }
         break;
     }
-    case M_DRUCKER_PRAGER: {  // sand.rs:248-319
+        break;
+    }
+    case M_DRUCKER_PRAGER: {
+        if constexpr (HAS_MODEL(MASK, M_DRUCKER_PRAGER)) {  // sand.rs:248-319
         M2 f_trial = mm(madd(mident(), smscale(dt, p.c)), p.f);
         M2 u, vt;
         float2 sigma;
@@ -514,7 +559,10 @@ EM_HD void update_particle(const MatP &m, PState &p, float dt, bool pr) {
         dp_finish(m, p, u, sigma, vt, projected, proj, dq, pr);
         break;
     }
-    case M_SNOW: {  // snow.rs:142-176
+        break;
+    }
+    case M_SNOW: {
+        if constexpr (HAS_MODEL(MASK, M_SNOW)) {  // snow.rs:142-176
         M2 f_trial = mm(madd(mident(), smscale(dt, p.c)), p.f);
         M2 u, vt;
         float2 sigma;
@@ -528,7 +576,10 @@ EM_HD void update_particle(const MatP &m, PState &p, float dt, bool pr) {
         sync_volume_density(p);
         break;
     }
-    case M_NACC: {  // nacc.rs:255-269 (no F advance on the CPU path)
+        break;
+    }
+    case M_NACC: {
+        if constexpr (HAS_MODEL(MASK, M_NACC)) {  // nacc.rs:255-269 (no F advance on the CPU path)
         M2 nf;
         float na;
         nacc_project(m, p.f, p.lvs, nf, na, pr);
@@ -538,6 +589,8 @@ EM_HD void update_particle(const MatP &m, PState &p, float dt, bool pr) {
         float vol = p.v0 * j;
         p.vol = vol;
         p.rho = vol > MIN_J ? p.mass / vol : p.rho;
+        break;
+    }
         break;
     }
     default:

@@ -155,7 +155,7 @@ struct emerge_sim {
     // step pipeline
     bool pending_valid = false;  // the next substep's P2G (+density) is already on the grid
     int use_graph = 1;
-    int use_window = 1;
+    int use_window = 0;
     int64_t sort_interval = 8;   // re-sort every N steps; 0 = keep the first sort
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t graph_exec = nullptr;
@@ -279,6 +279,8 @@ StepLaunch make_launch(emerge_sim *s) {
         if (m.model == M_FLUID) density = 1;  // needs_density_recompute (fluid.rs:261-263)
     L.density_mode = density;
     L.use_window = s->use_window;
+    L.model_mask = 1u << M_FALLBACK;
+    for (const auto &m : s->mats) L.model_mask |= 1u << m.model;
     L.stream = s->stream;
     return L;
 }

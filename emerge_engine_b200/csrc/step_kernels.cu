@@ -142,11 +142,22 @@ __device__ __forceinline__ void store_fields(const DevParticles &P, int i, const
     if (neq(p.lvs, o.lvs)) P.lvs[i] = p.lvs;
 }
 
+// Tiled cell index split into an x part and a y part (cell_index = X(x) + Y(y)).
+__device__ __forceinline__ int cell_x_part(int x, int tpd) { return (((x >> 3) * tpd) << 6) + ((x & 7) << 3); }
+__device__ __forceinline__ int cell_y_part(int y) { return ((y >> 3) << 6) + (y & 7); }
+
 // G2P phase 1 for one particle (transfer/g2p.rs:217-326 with ASFLIP, contact and
 // mixture gated off).  Returns 1 if the speed clamp fired.
 __device__ __forceinline__ int g2p_particle(const GridView &g, const DevConfig &cfg, float dt,
                                             PState &p) {
     QW w = quadratic_weights(p.x);
+    const bool inside = w.bx >= 1 && w.by >= 1 && w.bx + 1 < g.res && w.by + 1 < g.res;
+    int xp[3], yp[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        xp[k] = cell_x_part(w.bx + k - 1, g.tpd);
+        yp[k] = cell_y_part(w.by + k - 1);
+    }
     float2 new_v = v2(0.0f, 0.0f);
     M2 b = mzero();
 #pragma unroll
@@ -157,8 +168,8 @@ __device__ __forceinline__ int g2p_particle(const GridView &g, const DevConfig &
             int cx = w.bx + gx - 1, cy = w.by + gy - 1;
             float2 dist = vadd(vsub(v2(static_cast<float>(cx), static_cast<float>(cy)), p.x),
                                splat(0.5f));
-            float2 node_v = in_domain(cx, cy, g.res) ? g.grid_v[cell_index(cx, cy, g.tpd)]
-                                                     : v2(0.0f, 0.0f);
+            float2 node_v = (inside || in_domain(cx, cy, g.res)) ? g.grid_v[xp[gx] + yp[gy]]
+                                                                  : v2(0.0f, 0.0f);
             float2 wv = vmuls(node_v, weight);
             M2 term = m2(vmuls(wv, dist.x), vmuls(wv, dist.y));
             b = madd(b, term);
@@ -186,45 +197,27 @@ __device__ __forceinline__ int g2p_particle(const GridView &g, const DevConfig &
     return clamped;
 }
 
+static inline int blocks_for(int n, int per) { return (n + per - 1) / per; }
+
 // ---------------------------------------------------------------- scatter engine
-// P2G scatter of a CTA's particles with warp-aggregated global reductions.  Within a
-// warp, lanes whose particles share a base cell (contiguous after the tile sort) have
-// the same 9 target cells; for each stencil slot a segmented shuffle reduction sums
-// their contributions into the segment's first lane, which issues one vector
-// red.global.add per target cell.  No float atomics in shared memory.
+// P2G scatter of one particle per thread with vector red.global reductions (native
+// in L2 on sm_100).  Optional warp aggregation: lanes whose particles share a base
+// cell (contiguous after the tile sort) sum their contributions with a segmented
+// shuffle reduction and the segment's first lane issues one reduction per cell.
+// Tile flags for the grid update are set once per particle (its stencil spans at
+// most 2 x 2 tiles).
 constexpr int THREADS = 256;
-constexpr int PPT = 2;
 
 struct Payload {
     float2 x;
-    float m;      // mass channel weight (0 if not scattered)
+    float m;      // mass channel weight
     float2 v;
     M2 c;
     M2 tau;
-    float s;      // -4 * stress_volume (dt-free stress coefficient); 0 = no stress channel
-    int bx, by;
-    bool valid;
+    float s;      // -4 * stress_volume (dt-free stress coefficient)
     bool do_ma;   // scatter mass + affine momentum
     bool do_s;    // scatter stress impulse
 };
-
-// Stencil slot k (0..8, gx = k / 3, gy = k % 3) of one particle.
-__device__ __forceinline__ void cell_contrib(const Payload &pl, int gx, int gy, const QW &w,
-                                             float &mc, float2 &a, float2 &s, int &cx, int &cy) {
-    float weight = w.wx[gx] * w.wy[gy];
-    cx = w.bx + gx - 1;
-    cy = w.by + gy - 1;
-    float2 cell_dist = vadd(vsub(v2(static_cast<float>(cx), static_cast<float>(cy)), pl.x),
-                            splat(0.5f));
-    mc = weight * pl.m;
-    a = svmul(weight, svmul(pl.m, vadd(pl.v, mv(pl.c, cell_dist))));
-    s = svmul(weight, svmul(pl.s, mv(pl.tau, cell_dist)));
-}
-
-__device__ __forceinline__ void mark_tile(const GridView &g, int cx, int cy) {
-    int t = (cx >> 3) * g.tpd + (cy >> 3);
-    if (g.tile_flag[t] == 0) g.tile_flag[t] = 1;
-}
 
 // Adds the values of lanes [lane, seg_end) into `lane` (suffix sums within segments).
 __device__ __forceinline__ float seg_sum(float v, int lane, int seg_end) {
@@ -236,59 +229,86 @@ __device__ __forceinline__ float seg_sum(float v, int lane, int seg_end) {
     return v;
 }
 
-__device__ void scatter_block(const GridView &g, Payload (&pl)[PPT], int aggregate) {
+__device__ __forceinline__ void mark_tiles(const GridView &g, int bx, int by) {
+    const int tx0 = max(bx - 1, 0) >> 3, tx1 = min(bx + 1, g.res - 1) >> 3;
+    const int ty0 = max(by - 1, 0) >> 3, ty1 = min(by + 1, g.res - 1) >> 3;
+    if (bx + 1 < 0 || by + 1 < 0 || bx - 1 >= g.res || by - 1 >= g.res) return;
+    g.tile_flag[tx0 * g.tpd + ty0] = 1;
+    if (tx1 != tx0) g.tile_flag[tx1 * g.tpd + ty0] = 1;
+    if (ty1 != ty0) {
+        g.tile_flag[tx0 * g.tpd + ty1] = 1;
+        if (tx1 != tx0) g.tile_flag[tx1 * g.tpd + ty1] = 1;
+    }
+}
+
+__device__ __forceinline__ void scatter_particle(const GridView &g, const Payload &p, bool valid,
+                                                 int aggregate) {
     const int lane = threadIdx.x & 31;
+    const bool active = valid && (p.do_ma || p.do_s);
+    QW w;
+    if (active) w = quadratic_weights(p.x);
+    int head = 1, seg_end = 32;
+    bool any_ma = true, any_s = true;
+    if (aggregate) {
+        any_ma = __ballot_sync(0xffffffffu, active && p.do_ma) != 0u;
+        any_s = __ballot_sync(0xffffffffu, active && p.do_s) != 0u;
+        const int kx = active ? w.bx : INT_MIN, ky = active ? w.by : lane;
+        const int px = __shfl_up_sync(0xffffffffu, kx, 1);
+        const int py = __shfl_up_sync(0xffffffffu, ky, 1);
+        head = (lane == 0 || !active || px != kx || py != ky) ? 1 : 0;
+        const unsigned heads = __ballot_sync(0xffffffffu, head != 0);
+        const unsigned after = heads & ~((2u << lane) - 1u);
+        seg_end = after ? __ffs(after) - 1 : 32;
+    } else if (!active) {
+        return;
+    }
+    const bool inside = active && w.bx >= 1 && w.by >= 1 && w.bx + 1 < g.res && w.by + 1 < g.res;
+    int xp[3] = {0, 0, 0}, yp[3] = {0, 0, 0};
+    if (active) {
 #pragma unroll
-    for (int k = 0; k < PPT; ++k) {
-        const Payload &p = pl[k];
-        const bool active = p.valid && (p.do_ma || p.do_s);
-        const unsigned any_ma = __ballot_sync(0xffffffffu, active && p.do_ma);
-        const unsigned any_s = __ballot_sync(0xffffffffu, active && p.do_s);
-        if (!any_ma && !any_s) continue;
-        // segments: runs of consecutive lanes with the same base cell
-        const int key_x = active ? p.bx : INT_MIN, key_y = active ? p.by : lane;
-        const int px = __shfl_up_sync(0xffffffffu, key_x, 1);
-        const int py = __shfl_up_sync(0xffffffffu, key_y, 1);
-        const bool head = !aggregate || lane == 0 || !active || px != key_x || py != key_y;
-        const unsigned heads = __ballot_sync(0xffffffffu, head);
-        const unsigned after = heads & ~((2u << lane) - 1u);  // heads strictly above lane
-        const int seg_end = after ? __ffs(after) - 1 : 32;
-        QW w = quadratic_weights(p.x);
+        for (int k = 0; k < 3; ++k) {
+            xp[k] = cell_x_part(w.bx + k - 1, g.tpd);
+            yp[k] = cell_y_part(w.by + k - 1);
+        }
+    }
 #pragma unroll
-        for (int gx = 0; gx < 3; ++gx) {
+    for (int gx = 0; gx < 3; ++gx) {
 #pragma unroll
-            for (int gy = 0; gy < 3; ++gy) {
-                float mc = 0.0f;
-                float2 a = v2(0.0f, 0.0f), s = v2(0.0f, 0.0f);
-                int cx = 0, cy = 0;
-                if (active) {
-                    cell_contrib(p, gx, gy, w, mc, a, s, cx, cy);
-                    if (!p.do_ma) {
-                        mc = 0.0f;
-                        a = v2(0.0f, 0.0f);
-                    }
-                    if (!p.do_s) s = v2(0.0f, 0.0f);
+        for (int gy = 0; gy < 3; ++gy) {
+            float mc = 0.0f;
+            float2 a = v2(0.0f, 0.0f), s = v2(0.0f, 0.0f);
+            int cx = 0, cy = 0;
+            if (active) {
+                float weight = w.wx[gx] * w.wy[gy];
+                cx = w.bx + gx - 1;
+                cy = w.by + gy - 1;
+                float2 cell_dist = vadd(vsub(v2(static_cast<float>(cx), static_cast<float>(cy)), p.x),
+                                        splat(0.5f));
+                if (p.do_ma) {
+                    mc = weight * p.m;
+                    a = svmul(weight, svmul(p.m, vadd(p.v, mv(p.c, cell_dist))));
                 }
-                if (aggregate) {
-                    if (any_ma) {
-                        mc = seg_sum(mc, lane, seg_end);
-                        a.x = seg_sum(a.x, lane, seg_end);
-                        a.y = seg_sum(a.y, lane, seg_end);
-                    }
-                    if (any_s) {
-                        s.x = seg_sum(s.x, lane, seg_end);
-                        s.y = seg_sum(s.y, lane, seg_end);
-                    }
+                if (p.do_s) s = svmul(weight, svmul(p.s, mv(p.tau, cell_dist)));
+            }
+            if (aggregate) {
+                if (any_ma) {
+                    mc = seg_sum(mc, lane, seg_end);
+                    a.x = seg_sum(a.x, lane, seg_end);
+                    a.y = seg_sum(a.y, lane, seg_end);
                 }
-                if (head && active && in_domain(cx, cy, g.res)) {
-                    const int ci = cell_index(cx, cy, g.tpd);
-                    if (mc != 0.0f || a.x != 0.0f || a.y != 0.0f) red_add_v4(&g.acc_a[ci], mc, a.x, a.y, 0.0f);
-                    if (s.x != 0.0f || s.y != 0.0f) red_add_v2(&g.acc_s[ci], s.x, s.y);
-                    mark_tile(g, cx, cy);
+                if (any_s) {
+                    s.x = seg_sum(s.x, lane, seg_end);
+                    s.y = seg_sum(s.y, lane, seg_end);
                 }
+            }
+            if (head && active && (inside || in_domain(cx, cy, g.res))) {
+                const int ci = xp[gx] + yp[gy];
+                if (p.do_ma || (aggregate && any_ma)) red_add_v4(&g.acc_a[ci], mc, a.x, a.y, 0.0f);
+                if (p.do_s || (aggregate && any_s)) red_add_v2(&g.acc_s[ci], s.x, s.y);
             }
         }
     }
+    if (active) mark_tiles(g, w.bx, w.by);
 }
 
 // ---------------------------------------------------------------- k_particle
@@ -303,91 +323,72 @@ struct ParticleKernelArgs {
     LoadFlags lf;
     int mode_g2p;       // 0: prime pass (no G2P), 1: G2P(k) + P2G(k+1)
     int density_mode;   // fluid stress deferred to k_density; G2P reads rho_dp
-    int use_window;
+    int aggregate;      // warp-aggregated P2G reductions
     int project_in;     // recompute the projection of substep k before G2P (fused pipeline)
     int emit_p2g;       // project for substep k+1 and scatter its P2G (fused pipeline)
 };
 
-__global__ void __launch_bounds__(THREADS, 3) k_particle(ParticleKernelArgs a) {
+template <unsigned MASK>
+__global__ void __launch_bounds__(THREADS) k_particle(ParticleKernelArgs a) {
     __shared__ MatP s_mats[MAX_MATERIALS];
     __shared__ float s_red[2][THREADS / 32];
     for (int k = threadIdx.x; k < a.n_mats; k += THREADS) s_mats[k] = a.mats[k];
     __syncthreads();
 
     const DevConfig &cfg = a.cfg;
+    const bool pr = cfg.precise_math != 0;
     StepState *st = a.st;
     const int acc_slot = st->acc_slot;
     const float dt = st->sub_dt;
-    const int base = blockIdx.x * (THREADS * PPT);
+    const int i = blockIdx.x * THREADS + threadIdx.x;
+    const bool valid = i < a.n;
 
-    Payload pl[PPT];
+    Payload pl;
+    pl.do_ma = false;
+    pl.do_s = false;
     float max_speed = 0.0f;
     float min_mdt = INFINITY;
-    int clamped_any = 0, projected_any = 0;
-
-#pragma unroll
-    for (int k = 0; k < PPT; ++k) {
-        const int i = base + k * THREADS + threadIdx.x;
-        pl[k].valid = i < a.n;
-        pl[k].do_ma = false;
-        pl[k].do_s = false;
-        int clamped = 0, projected = 0;
-        if (pl[k].valid) {
-            PState p = load_state(a.P, i, a.lf);
-            const MatP &m = s_mats[p.mat < static_cast<uint32_t>(a.n_mats) ? p.mat : 0u];
-            if (a.mode_g2p) {
-                const Saved o = save_fields(p);
-                if (a.project_in) project_state(cfg, p);  // recompute S'(k); counted earlier
-                if (a.density_mode && a.project_in) {
-                    float d = a.P.rho_dp[i];
-                    if (d > F32_EPS) {
-                        p.rho = d;
-                        p.vol = p.mass / d;
-                    }
+    int clamped = 0, projected = 0;
+    if (valid) {
+        PState p = load_state(a.P, i, a.lf);
+        const MatP &m = s_mats[p.mat < static_cast<uint32_t>(a.n_mats) ? p.mat : 0u];
+        if (a.mode_g2p) {
+            const Saved o = save_fields(p);
+            if (a.project_in) project_state(cfg, p);  // recompute S'(k); counted earlier
+            if (a.density_mode && a.project_in) {
+                float d = a.P.rho_dp[i];
+                if (d > F32_EPS) {
+                    p.rho = d;
+                    p.vol = p.mass / d;
                 }
-                clamped = g2p_particle(a.g, cfg, dt, p);
-                update_particle(m, p, dt, cfg.precise_math != 0);
-                store_fields(a.P, i, o, p);
             }
-            // CFL contribution for the next substep (step.rs:447-466)
-            float sp = vlen(p.v);
-            if (cfg.affine_cfl) sp += affine_cfl(p.c, cfg.cell);
-            max_speed = fmaxf(max_speed, sp);
-            float mdt = timestep_bound(m, p.rho, p.h, cfg.cell, cfg.mat_cfl, cfg.visc_cfl,
-                                       cfg.precise_math != 0);
-            if (isfinite(mdt) && mdt > 0.0f) min_mdt = fminf(min_mdt, mdt);
-            if (!a.emit_p2g) {
-                // deterministic pipeline: no fused scatter
-            } else {
-            // projection of the next substep (step.rs:67-73)
+            clamped = g2p_particle(a.g, cfg, dt, p);
+            update_particle<MASK>(m, p, dt, pr);
+            store_fields(a.P, i, o, p);
+        }
+        // CFL contribution for the next substep (step.rs:447-466)
+        float sp = vlen(p.v);
+        if (cfg.affine_cfl) sp += affine_cfl(p.c, cfg.cell);
+        max_speed = sp;
+        float mdt = timestep_bound<MASK>(m, p.rho, p.h, cfg.cell, cfg.mat_cfl, cfg.visc_cfl, pr);
+        if (isfinite(mdt) && mdt > 0.0f) min_mdt = mdt;
+        if (a.emit_p2g) {
+            // projection of the next substep (step.rs:67-73) and its P2G payload
             if (cfg.project) projected = project_state(cfg, p) ? 1 : 0;
-            // P2G payload (transfer/p2g.rs:192-213)
-            pl[k].x = p.x;
-            pl[k].m = p.mass;
-            pl[k].v = p.v;
-            pl[k].c = p.c;
-            pl[k].do_ma = true;
-            bool fluid = m.model == M_FLUID;
-            if (!(a.density_mode && fluid)) {
-                pl[k].tau = combined_kirchhoff_stress(m, p, cfg.precise_math != 0);
-                pl[k].s = -stress_volume(m, p) * KERNEL_D_INVERSE;
-                pl[k].do_s = true;
-            } else {
-                pl[k].tau = mzero();
-                pl[k].s = 0.0f;
-            }
-            QW w = quadratic_weights(p.x);
-            pl[k].bx = w.bx;
-            pl[k].by = w.by;
+            pl.x = p.x;
+            pl.m = p.mass;
+            pl.v = p.v;
+            pl.c = p.c;
+            pl.do_ma = true;
+            if (!(a.density_mode && m.model == M_FLUID)) {
+                pl.tau = combined_kirchhoff_stress<MASK>(m, p, pr);
+                pl.s = -stress_volume(m, p) * KERNEL_D_INVERSE;
+                pl.do_s = true;
             }
         }
-        clamped_any |= clamped;
-        projected_any |= projected;
-        count_warp(&st->vel_clamp, clamped != 0);
-        count_warp(&st->jproj_pending[acc_slot], projected != 0);
     }
-    (void)clamped_any;
-    (void)projected_any;
+    count_warp(&st->vel_clamp, clamped != 0);
+    count_warp(&st->jproj_pending[acc_slot], projected != 0);
 
     // CFL block reduction -> one atomic per block
     max_speed = warp_max(max_speed);
@@ -406,10 +407,9 @@ __global__ void __launch_bounds__(THREADS, 3) k_particle(ParticleKernelArgs a) {
         }
         atomicMax(&st->max_speed_bits[acc_slot], __float_as_uint(ms));
         atomicMin(&st->min_mdt_bits[acc_slot], __float_as_uint(md));
+        atomicAdd(&st->window_blocks, 1ull);
     }
-
-    if (threadIdx.x == 0) atomicAdd(&st->window_blocks, 1ull);
-    scatter_block(a.g, pl, a.use_window);
+    scatter_particle(a.g, pl, valid, a.aggregate);
 }
 
 // ---------------------------------------------------------------- k_density
@@ -422,39 +422,41 @@ struct DensityKernelArgs {
     StepState *st;
     GridView g;
     LoadFlags lf;
-    int use_window;
+    int aggregate;
 };
 
 // estimate_particle_volumes gather (solver/density.rs:50-71) at the projected
 // positions, stored as rho_dp, plus the stress scatter of fluid particles.
+template <unsigned MASK>
 __global__ void __launch_bounds__(THREADS) k_density(DensityKernelArgs a) {
     __shared__ MatP s_mats[MAX_MATERIALS];
     for (int k = threadIdx.x; k < a.n_mats; k += THREADS) s_mats[k] = a.mats[k];
     __syncthreads();
     const DevConfig &cfg = a.cfg;
-    const int base = blockIdx.x * (THREADS * PPT);
-    Payload pl[PPT];
-#pragma unroll
-    for (int k = 0; k < PPT; ++k) {
-        const int i = base + k * THREADS + threadIdx.x;
-        pl[k].valid = i < a.n;
-        pl[k].do_ma = false;
-        pl[k].do_s = false;
-        if (!pl[k].valid) continue;
+    const bool pr = cfg.precise_math != 0;
+    const int i = blockIdx.x * THREADS + threadIdx.x;
+    const bool valid = i < a.n;
+    Payload pl;
+    pl.do_ma = false;
+    pl.do_s = false;
+    if (valid) {
         PState p = load_state(a.P, i, a.lf);
         if (cfg.project) project_state(cfg, p);
         QW w = quadratic_weights(p.x);
+        const bool inside = w.bx >= 1 && w.by >= 1 && w.bx + 1 < a.g.res && w.by + 1 < a.g.res;
         float density = 0.0f;
 #pragma unroll
-        for (int gx = 0; gx < 3; ++gx)
+        for (int gx = 0; gx < 3; ++gx) {
+            const int xp = cell_x_part(w.bx + gx - 1, a.g.tpd);
 #pragma unroll
             for (int gy = 0; gy < 3; ++gy) {
                 float weight = w.wx[gx] * w.wy[gy];
                 int cx = w.bx + gx - 1, cy = w.by + gy - 1;
-                float mc = in_domain(cx, cy, a.g.res) ? a.g.acc_a[cell_index(cx, cy, a.g.tpd)].x
-                                                      : 0.0f;
+                float mc = (inside || in_domain(cx, cy, a.g.res))
+                               ? a.g.acc_a[xp + cell_y_part(cy)].x : 0.0f;
                 density += mc * weight;
             }
+        }
         a.P.rho_dp[i] = density;
         const MatP &m = s_mats[p.mat < static_cast<uint32_t>(a.n_mats) ? p.mat : 0u];
         if (m.model == M_FLUID) {
@@ -462,18 +464,14 @@ __global__ void __launch_bounds__(THREADS) k_density(DensityKernelArgs a) {
                 p.rho = density;
                 p.vol = p.mass / density;
             }
-            pl[k].x = p.x;
-            pl[k].m = 0.0f;
-            pl[k].v = v2(0.0f, 0.0f);
-            pl[k].c = mzero();
-            pl[k].tau = combined_kirchhoff_stress(m, p, cfg.precise_math != 0);
-            pl[k].s = -stress_volume(m, p) * KERNEL_D_INVERSE;
-            pl[k].do_s = true;
-            pl[k].bx = w.bx;
-            pl[k].by = w.by;
+            pl.x = p.x;
+            pl.m = 0.0f;
+            pl.tau = combined_kirchhoff_stress<MASK>(m, p, pr);
+            pl.s = -stress_volume(m, p) * KERNEL_D_INVERSE;
+            pl.do_s = true;
         }
     }
-    scatter_block(a.g, pl, a.use_window);
+    scatter_particle(a.g, pl, valid, a.aggregate);
 }
 
 // ---------------------------------------------------------------- grid update
@@ -783,45 +781,66 @@ __global__ void k_mass_gather(DevParticles P, int lo, int hi, GridView g, int wr
 }
 
 // ---------------------------------------------------------------- launchers
-static inline int blocks_for(int n, int per) { return (n + per - 1) / per; }
+
+// Instantiated model sets; a scene uses the smallest one covering its materials.
+constexpr unsigned MASK_FLUID = (1u << M_FALLBACK) | (1u << M_FLUID);
+constexpr unsigned MASK_SOLID = (1u << M_FALLBACK) | (1u << M_NEOHOOKEAN);
+constexpr unsigned MASK_SOLID_FLUID = MASK_FLUID | MASK_SOLID;
+constexpr unsigned MASK_GRANULAR =
+    (1u << M_FALLBACK) | (1u << M_DRUCKER_PRAGER) | (1u << M_SNOW) | (1u << M_NACC);
+
+unsigned covering_mask(unsigned m) {
+    const unsigned masks[4] = {MASK_FLUID, MASK_SOLID, MASK_SOLID_FLUID, MASK_GRANULAR};
+    for (unsigned c : masks)
+        if ((m & ~c) == 0u) return c;
+    return ALL_MODELS;
+}
+
+template <class Args>
+static void fill_common(Args &a, const StepLaunch &L, const LoadFlagsHost &lfh) {
+    a.P = L.P;
+    a.n = L.n;
+    a.mats = L.mats;
+    a.n_mats = L.n_mats;
+    a.cfg = L.cfg;
+    a.st = L.st;
+    a.g = L.g;
+    a.lf.temperature = lfh.temperature;
+    a.lf.activation = lfh.activation;
+    a.lf.pinned = lfh.pinned;
+    a.aggregate = L.use_window;
+}
+
+#define EMERGE_DISPATCH_MASK(kernel, mask, grid, args)                                 \
+    switch (covering_mask(mask)) {                                                     \
+    case MASK_FLUID: kernel<MASK_FLUID><<<grid, THREADS, 0, L.stream>>>(args); break;   \
+    case MASK_SOLID: kernel<MASK_SOLID><<<grid, THREADS, 0, L.stream>>>(args); break;   \
+    case MASK_SOLID_FLUID:                                                             \
+        kernel<MASK_SOLID_FLUID><<<grid, THREADS, 0, L.stream>>>(args);                \
+        break;                                                                         \
+    case MASK_GRANULAR: kernel<MASK_GRANULAR><<<grid, THREADS, 0, L.stream>>>(args); break; \
+    default: kernel<ALL_MODELS><<<grid, THREADS, 0, L.stream>>>(args); break;           \
+    }
 
 void launch_particle_pass(const StepLaunch &L, const LoadFlagsHost &lfh, int mode_g2p,
                           int project_in, int emit_p2g) {
     if (L.n == 0) return;
     ParticleKernelArgs a;
-    a.P = L.P;
-    a.n = L.n;
-    a.mats = L.mats;
-    a.n_mats = L.n_mats;
-    a.cfg = L.cfg;
-    a.st = L.st;
-    a.g = L.g;
-    a.lf.temperature = lfh.temperature;
-    a.lf.activation = lfh.activation;
-    a.lf.pinned = lfh.pinned;
+    fill_common(a, L, lfh);
     a.mode_g2p = mode_g2p;
     a.density_mode = L.density_mode;
-    a.use_window = L.use_window;
     a.project_in = project_in;
     a.emit_p2g = emit_p2g;
-    k_particle<<<blocks_for(L.n, THREADS * PPT), THREADS, 0, L.stream>>>(a);
+    const int grid = blocks_for(L.n, THREADS);
+    EMERGE_DISPATCH_MASK(k_particle, L.model_mask, grid, a)
 }
 
 void launch_density_pass(const StepLaunch &L, const LoadFlagsHost &lfh) {
     if (L.n == 0) return;
     DensityKernelArgs a;
-    a.P = L.P;
-    a.n = L.n;
-    a.mats = L.mats;
-    a.n_mats = L.n_mats;
-    a.cfg = L.cfg;
-    a.st = L.st;
-    a.g = L.g;
-    a.lf.temperature = lfh.temperature;
-    a.lf.activation = lfh.activation;
-    a.lf.pinned = lfh.pinned;
-    a.use_window = L.use_window;
-    k_density<<<blocks_for(L.n, THREADS * PPT), THREADS, 0, L.stream>>>(a);
+    fill_common(a, L, lfh);
+    const int grid = blocks_for(L.n, THREADS);
+    EMERGE_DISPATCH_MASK(k_density, L.model_mask, grid, a)
 }
 
 void launch_grid_update(const StepLaunch &L) {
