@@ -89,11 +89,11 @@ def granular_blocks(grid_res, target_particles, seed=42, side_range=(16, 128), s
 
 
 def mixed_granular(sim_cls, grid_res=1024, target_particles=4_000_000, seed=42, gravity=-1.0,
-                   **sim_kw):
+                   dt=0.05, **sim_kw):
     """Mixed granular: seeded random blocks (16-128 cells a side), each block uniformly
     DruckerPrager sand, Stomakhin snow or NACC soil with the reference's canonical
     constructors (sand.rs:106, snow.rs:68, nacc.rs:93), 4 particles per cell."""
-    cfg = SimConfig.standard(grid_res, 0.05, (0.0, gravity))
+    cfg = SimConfig.standard(grid_res, dt, (0.0, gravity))
     sim = (sim_cls.empty(cfg, **sim_kw)
            .with_default_material(DruckerPragerMaterial.cohesionless(1e5, 0.2))
            .with_material(1, StomakhinMaterial.from_young_modulus(1.4e5, 0.2))
