@@ -142,6 +142,17 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
+def reduce_over_ranks(dist, device, total_ms: float, units: float, launches: int):
+    """Replica aggregation: device time is the max over ranks (the job ends with the slowest
+    replica); particle-substeps and kernel launches add up."""
+    import torch
+    t = torch.tensor([total_ms], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    u = torch.tensor([units, float(launches)], dtype=torch.float64, device=device)
+    dist.all_reduce(u, op=dist.ReduceOp.SUM)
+    return float(t.item()), float(u[0].item()), int(u[1].item())
+
+
 def build_scene(sim_cls, workload: str, **kw):
     from tests import scenes
     spec = WORKLOADS[workload]
@@ -273,13 +284,8 @@ def main():
     launches = st1["kernel_launches"] - st0["kernel_launches"]
     units = float(n * substeps)
     if dist is not None:
-        import torch
-        t = torch.tensor([total_ms], dtype=torch.float64, device=f"cuda:{local_rank}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms = float(t.item())
-        u = torch.tensor([units, float(launches)], dtype=torch.float64, device=f"cuda:{local_rank}")
-        dist.all_reduce(u, op=dist.ReduceOp.SUM)
-        units, launches = float(u[0].item()), int(u[1].item())
+        total_ms, units, launches = reduce_over_ranks(dist, f"cuda:{local_rank}", total_ms, units,
+                                                      launches)
     value = units / (total_ms / 1000.0)
     ms_per_step = total_ms / args.steps
 
@@ -325,13 +331,9 @@ def main():
         e2e_subs = sim.stats()["substeps"] - sub0
         e2e_units = float(n * e2e_subs)
         if dist is not None:
-            import torch
-            t = torch.tensor([e2e_s], dtype=torch.float64, device=f"cuda:{local_rank}")
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            e2e_s = float(t.item())
-            u = torch.tensor([e2e_units], dtype=torch.float64, device=f"cuda:{local_rank}")
-            dist.all_reduce(u, op=dist.ReduceOp.SUM)
-            e2e_units = float(u.item())
+            e2e_ms, e2e_units, _ = reduce_over_ranks(dist, f"cuda:{local_rank}", e2e_s * 1e3,
+                                                     e2e_units, 0)
+            e2e_s = e2e_ms / 1e3
         host.free()
         extras["e2e"] = {"value": e2e_units / e2e_s, "unit": UNIT,
                          "h2d_bytes_per_step": n * 128, "d2h_bytes_per_step": n * 128,
