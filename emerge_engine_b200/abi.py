@@ -165,6 +165,8 @@ ABI_FUNCTIONS = [
     ("emerge_cuda_set_option", c_int, [SIM, c_int, c_int64]),
     ("emerge_cuda_sort_now", c_int, [SIM, c_int]),
     ("emerge_cuda_sort_keys", c_int, [c_void_p, c_uint64, c_uint32, c_int, c_void_p, c_void_p]),
+    ("emerge_cuda_sort_keys_noalloc", c_int, [c_void_p, c_uint32, c_uint32, c_int, c_void_p,
+                                              c_void_p, c_void_p]),
     ("emerge_cuda_stream", c_void_p, [SIM]),
     ("emerge_cuda_kernel_launches", c_int, [SIM, POINTER(c_uint64)]),
     ("emerge_cuda_event_record", c_int, [SIM, c_int]),

@@ -14,7 +14,7 @@ import sys
 PKG = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(PKG, "csrc")
 OUT = os.path.join(PKG, "libemerge_cuda.so")
-SOURCES = ["step_kernels.cu", "det_kernels.cu", "sort.cu", "sim.cu"]
+SOURCES = ["step_kernels.cu", "det_kernels.cu", "sort.cu", "sort_noalloc.cu", "sim.cu"]
 HEADERS = ["physics.cuh", "device_state.cuh", "kernels.h"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC = os.environ.get("NVCC", "nvcc")

@@ -755,6 +755,11 @@ emerge_status invalidate_pending(emerge_sim *s) {
 }  // namespace
 
 // =============================================================== C ABI
+namespace emerge {
+// Message returned by emerge_cuda_last_global_error for entry points in other files.
+void set_global_error(const char *msg) { g_global_error = msg; }
+}  // namespace emerge
+
 extern "C" {
 
 const char *emerge_cuda_last_error(const emerge_sim *sim) {

@@ -306,6 +306,30 @@ emerge_status emerge_cuda_sort_now(emerge_sim *sim, int key_mode);
 emerge_status emerge_cuda_sort_keys(const float *xy, uint64_t n, uint32_t grid_res, int key_mode,
                                     uint32_t *keys_out, uint32_t *perm_out);
 
+/* Allocation-free variant of emerge_cuda_sort_keys (no counterpart in the reference).
+ * For callers that must not let a library allocate: cudaMalloc/cudaFree synchronise the
+ * whole device, stalling the caller's other streams, and fail outright when the caller's
+ * memory pool has reserved the device's memory.  Same keys and the same stable
+ * permutation as emerge_cuda_sort_keys, but every buffer is the caller's DEVICE memory
+ * (current device, or managed) and the work is enqueued on the caller's stream:
+ *   xy_dev    n (x, y) float pairs, 8-byte aligned
+ *   keys_dev  n uint32: key of xy[i];  perm_dev  n uint32: stable argsort of the keys
+ *   stream    cudaStream_t as void* (NULL = the legacy default stream)
+ * The library allocates nothing; it works in one fixed array of about 1 MiB inside its
+ * device image, so n is limited to EMERGE_SORT_NOALLOC_MAX and a larger n returns
+ * EMERGE_ERR_INVALID_ARG before any device work.  Nothing needs to start at zero (the
+ * outputs need no initial contents; the working array is written before it is read).
+ * Returns once the work is enqueued; results are ready when the stream reaches it.
+ * The first call on each device looks up the working array's address
+ * (cudaGetSymbolAddress): make that first call before any stream capture begins.
+ * All calls on one device share the one working array, so calls whose work may overlap
+ * in time (unordered streams, several host threads) race and corrupt each other's
+ * results: order them on one stream or with events. */
+#define EMERGE_SORT_NOALLOC_MAX 65536u
+emerge_status emerge_cuda_sort_keys_noalloc(const float *xy_dev, uint32_t n, uint32_t grid_res,
+                                            int key_mode, uint32_t *keys_dev, uint32_t *perm_dev,
+                                            void *stream);
+
 /* The CUDA stream the simulation's work runs on (cudaStream_t as void*). */
 void *emerge_cuda_stream(emerge_sim *sim);
 

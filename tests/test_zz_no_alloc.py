@@ -1,0 +1,78 @@
+"""Allocation-free sort entry point (emerge_cuda_sort_keys_noalloc): with caller-owned
+device buffers and the caller's stream it returns the same keys and stable permutation as
+the allocating emerge_cuda_sort_keys.  Named to be collected last, so it runs both alone
+and after every other test in the same process."""
+import ctypes
+
+import numpy as np
+import pytest
+
+from emerge_engine_b200 import abi
+
+MAX = 65536  # EMERGE_SORT_NOALLOC_MAX
+
+
+def allocating_sort(cuda_lib, xy, res, mode):
+    n = len(xy)
+    keys = np.zeros(n, dtype=np.uint32)
+    perm = np.zeros(n, dtype=np.uint32)
+    st = cuda_lib.emerge_cuda_sort_keys(xy.ctypes.data_as(ctypes.c_void_p), n, res, mode,
+                                        keys.ctypes.data_as(ctypes.c_void_p),
+                                        perm.ctypes.data_as(ctypes.c_void_p))
+    assert st == 0, cuda_lib.emerge_cuda_last_global_error()
+    return keys, perm
+
+
+def test_rejects_more_than_the_maximum_before_device_work(cuda_lib):
+    """Runs without a GPU too: the size check precedes every CUDA call."""
+    p = ctypes.c_void_p(256)
+    st = cuda_lib.emerge_cuda_sort_keys_noalloc(p, MAX + 1, 64, 0, p, p, None)
+    assert st == abi.ERR_INVALID_ARG
+    assert b"EMERGE_SORT_NOALLOC_MAX" in cuda_lib.emerge_cuda_last_global_error()
+    assert cuda_lib.emerge_cuda_sort_keys_noalloc(p, 16, 64, 2, p, p, None) == abi.ERR_INVALID_ARG
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("mode,res", [(0, 1024), (1, 256)])
+def test_matches_the_allocating_sort_two_calls_in_a_row(cuda_lib, mode, res):
+    import torch
+
+    dev = torch.device("cuda:0")
+    rng = np.random.default_rng(1234 + mode)
+    cases = []
+    for n in (MAX, 40_001):  # the second call is smaller: nothing of the first may leak
+        xy = rng.uniform(-2.0, res + 2.0, size=(n, 2)).astype(np.float32)
+        xy[::5] = xy[3]  # many equal keys: the permutation must keep input order
+        xy[: n // 8] = np.floor(xy[: n // 8])  # exact cell boundaries
+        keys, perm = allocating_sort(cuda_lib, xy, res, mode)
+        d_xy = torch.from_numpy(xy).to(dev)
+        d_keys = torch.full((n,), -1, dtype=torch.int32, device=dev)
+        d_perm = torch.full((n,), -1, dtype=torch.int32, device=dev)
+        cases.append((n, keys, perm, d_xy, d_keys, d_perm))
+    torch.cuda.synchronize(dev)
+
+    side = torch.cuda.Stream(dev)
+    for n, _, _, d_xy, d_keys, d_perm in cases:  # both calls queued back to back
+        st = cuda_lib.emerge_cuda_sort_keys_noalloc(
+            ctypes.c_void_p(d_xy.data_ptr()), n, res, mode, ctypes.c_void_p(d_keys.data_ptr()),
+            ctypes.c_void_p(d_perm.data_ptr()), ctypes.c_void_p(side.cuda_stream))
+        assert st == 0, cuda_lib.emerge_cuda_last_global_error()
+    side.synchronize()
+
+    for n, keys, perm, _, d_keys, d_perm in cases:
+        np.testing.assert_array_equal(d_keys.cpu().numpy().view(np.uint32), keys)
+        np.testing.assert_array_equal(d_perm.cpu().numpy().view(np.uint32), perm)
+        np.testing.assert_array_equal(perm, np.argsort(keys, kind="stable").astype(np.uint32))
+
+
+@pytest.mark.gpu
+def test_rejects_host_memory(cuda_lib):
+    import torch
+
+    torch.cuda.init()
+    xy = np.zeros((8, 2), dtype=np.float32)
+    out = np.zeros(8, dtype=np.uint32)
+    st = cuda_lib.emerge_cuda_sort_keys_noalloc(
+        xy.ctypes.data_as(ctypes.c_void_p), 8, 64, 0, out.ctypes.data_as(ctypes.c_void_p),
+        out.ctypes.data_as(ctypes.c_void_p), None)
+    assert st == abi.ERR_INVALID_ARG
