@@ -84,62 +84,113 @@ def profile_traffic(workload: str):
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled every 200 ms while running."""
+    """SM clocks and clock-event (throttle) reasons, read through NVML (the library behind
+    nvidia-smi) every 5 ms on a background thread while the benchmark runs.  Reading only;
+    nothing is set.  Falls back to `nvidia-smi -lms 200` where NVML is unavailable."""
 
+    REASONS = {"hw_slowdown": 0x8, "sw_thermal_slowdown": 0x20, "hw_thermal_slowdown": 0x40,
+               "sw_power_cap": 0x4}
     QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
-    def __init__(self, gpu_index: int):
-        self.gpu = gpu_index
-        self.proc = None
-        self.lines = []
+    def __init__(self, local_rank: int):
+        self.local_rank = local_rank
+        self.samples = []  # (time, sm MHz, set of reason names)
+        self.max_mhz = None
+        self.source = None
+        self._stop = threading.Event()
         self.thread = None
+        self.proc = None
+
+    def _nvml_handle(self, nv):
+        ident = str(self.local_rank)
+        vis = os.environ.get("CUDA_VISIBLE_DEVICES")
+        if vis:
+            items = [v.strip() for v in vis.split(",") if v.strip()]
+            if self.local_rank < len(items):
+                ident = items[self.local_rank]
+        if ident.startswith("GPU-") or ident.startswith("MIG-"):
+            return nv.nvmlDeviceGetHandleByUUID(ident)
+        return nv.nvmlDeviceGetHandleByIndex(int(ident))
 
     def start(self):
         try:
+            import pynvml as nv
+            nv.nvmlInit()
+            h = self._nvml_handle(nv)
+            self.max_mhz = float(nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM))
+            get_reasons = getattr(nv, "nvmlDeviceGetCurrentClocksEventReasons", None) or \
+                nv.nvmlDeviceGetCurrentClocksThrottleReasons
+        except Exception:
+            self._start_smi()
+            return
+        self.source = "nvml (5 ms)"
+
+        def run():
+            while not self._stop.is_set():
+                try:
+                    mhz = float(nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM))
+                    bits = int(get_reasons(h))
+                except Exception:
+                    break
+                names = {k for k, b in self.REASONS.items() if bits & b}
+                self.samples.append((time.perf_counter(), mhz, names))
+                self._stop.wait(0.005)
+
+        self.thread = threading.Thread(target=run, daemon=True)
+        self.thread.start()
+
+    def _start_smi(self):
+        try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits",
-                 "-i", str(self.gpu), "-lms", "200"],
+                 "-i", str(self.local_rank), "-lms", "200"],
                 stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
         except (OSError, ValueError):
             self.proc = None
             return
-        self.thread = threading.Thread(target=self._read, daemon=True)
+        self.source = "nvidia-smi (200 ms)"
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+
+        def run():
+            for line in self.proc.stdout:
+                parts = [p.strip() for p in line.split(",")]
+                if len(parts) < 9:
+                    continue
+                try:
+                    mhz, self.max_mhz = float(parts[1]), float(parts[2])
+                except ValueError:
+                    continue
+                self.samples.append((time.perf_counter(), mhz,
+                                     {n for n, v in zip(names, parts[5:9]) if v.lower() == "active"}))
+
+        self.thread = threading.Thread(target=run, daemon=True)
         self.thread.start()
 
-    def _read(self):
-        for line in self.proc.stdout:
-            self.lines.append(line.strip())
-
-    def stop(self) -> dict | None:
-        if not self.proc:
-            return None
-        self.proc.terminate()
-        try:
-            self.proc.wait(timeout=5)
-        except subprocess.TimeoutExpired:
-            self.proc.kill()
+    def stop(self, t_begin: float, t_end: float, t_load: float) -> dict | None:
+        """Summary of the samples taken in [t_begin, t_end] (the timed region); when that
+        window holds fewer than 3 samples, of [t_load, t_end] (warm-up included)."""
+        self._stop.set()
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
         if self.thread:
             self.thread.join(timeout=2)
-        sm, mx, reasons = [], None, set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for line in self.lines:
-            parts = [p.strip() for p in line.split(",")]
-            if len(parts) < 9:
-                continue
-            try:
-                sm.append(float(parts[1]))
-                mx = float(parts[2])
-            except ValueError:
-                continue
-            for name, val in zip(names, parts[5:9]):
-                if val.lower() == "active":
-                    reasons.add(name)
-        if not sm:
+        window = "timed region"
+        sel = [s for s in self.samples if t_begin <= s[0] <= t_end]
+        if len(sel) < 3:
+            sel = [s for s in self.samples if t_load <= s[0] <= t_end]
+            window = "warm-up + timed region"
+        if not sel:
             return None
-        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons),
-                "samples": len(sm)}
+        reasons = sorted(set().union(*(s[2] for s in sel)))
+        return {"sm_mhz": statistics.median(s[1] for s in sel), "sm_max_mhz": self.max_mhz,
+                "reasons": reasons, "samples": len(sel), "window": window,
+                "source": self.source}
 
 
 def reduce_over_ranks(dist, device, total_ms: float, units: float, launches: int):
@@ -191,26 +242,35 @@ def run_reference(args):
     threads = set_threads(0)
     sim = build_scene(OracleSimulation, args.workload)
     n = sim.particle_count()
+    # Bounded sample: warm-up and timed steps each stop early once their time budget is
+    # spent, so the run ends within a few minutes whatever the workload.
+    t0 = time.perf_counter()
     for _ in range(args.warmup):
         sim.step()
-    subs = 0
+        if time.perf_counter() - t0 >= args.ref_warmup_budget:
+            break
+    subs = steps = 0
     t0 = time.perf_counter()
     for _ in range(args.steps):
         sim.step()
+        steps += 1
         subs += sim.last_substeps()
+        if time.perf_counter() - t0 >= args.ref_budget:
+            break
     dt = time.perf_counter() - t0
     value = n * subs / dt
     spec = WORKLOADS[args.workload]
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT,
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": dt * 1000.0 / max(args.steps, 1), "higher_is_better": True,
+        "ms_per_step": dt * 1000.0 / max(steps, 1), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic (seeded scene generator, tests/scenes.py)",
         "config": {"workload": args.workload, "description": spec["desc"], "particles": n,
                    "grid": spec["grid_res"], "substeps": subs},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
-                         "sample": f"{args.steps} full steps ({subs} substeps) of {n} particles"},
+                         "sample": f"{steps} of {args.steps} full steps ({subs} substeps) of {n} "
+                                   f"particles, {dt:.1f} s (time budget {args.ref_budget:.0f} s)"},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -219,13 +279,16 @@ def run_reference(args):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=100)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--workload", default=DEFAULT_WORKLOAD, choices=sorted(WORKLOADS))
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-extras", action="store_true",
                     help="skip e2e, roofline instrumentation and CPU baseline (profiling runs)")
     ap.add_argument("--cpu-budget", type=float, default=15.0)
+    ap.add_argument("--ref-budget", type=float, default=90.0,
+                    help="--impl reference: seconds of timed CPU steps at most")
+    ap.add_argument("--ref-warmup-budget", type=float, default=20.0)
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3) if args.impl == "ours" else args.warmup
 
@@ -254,6 +317,9 @@ def main():
     spec = WORKLOADS[args.workload]
     sim = build_scene(Simulation, args.workload, device=local_rank)
     n = sim.particle_count()
+    clocks = ClockSampler(local_rank)
+    clocks.start()
+    t_load = time.perf_counter()
     for _ in range(args.warmup):
         sim.step()
     sim.synchronize()
@@ -265,10 +331,9 @@ def main():
             torch.cuda.synchronize()
         sim.synchronize()
 
-    clocks = ClockSampler(local_rank)
     st0 = sim.stats()
     barrier()
-    clocks.start()
+    t_begin = time.perf_counter()
     total_ms = 0.0
     for _ in range(args.steps):
         sim.flush_l2()
@@ -277,7 +342,7 @@ def main():
         sim.event_record(1)
         total_ms += sim.event_elapsed_ms(0, 1)
     sim.synchronize()
-    clock_info = clocks.stop()
+    clock_info = clocks.stop(t_begin, time.perf_counter(), t_load)
     st1 = sim.stats()
     barrier()
     substeps = st1["substeps"] - st0["substeps"]

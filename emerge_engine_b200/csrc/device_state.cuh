@@ -67,7 +67,7 @@ struct StepState {
     unsigned long long window_blocks;      // particle-pass blocks in total
     unsigned long long graph_kernels;      // kernels executed inside step graphs
     uint32_t error_flags;
-    uint32_t pad_;
+    uint32_t upload_flags;      // k_check_aos: bit 0 contact_group != 0, bit 1 pinned
 };
 
 struct GridView {
@@ -98,6 +98,7 @@ struct StepLaunch {
     int density_mode;   // any registered material needs the density pass
     int use_window;     // warp-aggregated P2G reductions
     unsigned model_mask;  // bit m set: ConstitutiveModel m is registered
+    int fast;           // fast path (stencil-offset sums with FMA); 0 in the reference-order mode
     cudaStream_t stream;
 };
 

@@ -31,6 +31,7 @@ size_t region_acc_bytes();
 void region_acc_finalize(const void *acc, emerge_body_state *out);
 void launch_gather_aos(const DevParticles &P, int n, emerge_particle *out, cudaStream_t stream);
 void launch_scatter_aos(const DevParticles &P, int n, const emerge_particle *in, cudaStream_t stream);
+void launch_check_aos(const emerge_particle *in, int n, uint32_t *flags, cudaStream_t stream);
 void launch_append_aos(const DevParticles &P, int n_old, int n_new, const emerge_particle *in,
                        cudaStream_t stream);
 void launch_reinit(const DevParticles &P, int n, const MatP *mats, int n_mats, cudaStream_t stream);

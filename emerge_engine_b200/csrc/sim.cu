@@ -281,6 +281,7 @@ StepLaunch make_launch(emerge_sim *s) {
     L.use_window = s->use_window;
     L.model_mask = 1u << M_FALLBACK;
     for (const auto &m : s->mats) L.model_mask |= 1u << m.model;
+    L.fast = s->deterministic ? 0 : 1;
     L.stream = s->stream;
     return L;
 }
@@ -964,18 +965,29 @@ emerge_status emerge_cuda_read_particles(emerge_sim *s, emerge_particle *out, ui
 emerge_status emerge_cuda_write_particles(emerge_sim *s, const emerge_particle *in, uint64_t n) {
     if (!s || (!in && n)) return EMERGE_ERR_INVALID_ARG;
     if (n != s->n) return static_cast<emerge_status>(s->fail(EMERGE_ERR_INVALID_ARG, "n must equal the particle count"));
-    for (uint64_t k = 0; k < n; ++k) {
-        if (in[k].contact_group != 0)
-            return static_cast<emerge_status>(s->fail(
-                EMERGE_ERR_UNSUPPORTED, "contact_group != 0 (multi-field contact) is not on the device path"));
-        if (in[k].pinned) s->lf.pinned = 1;
-    }
     if (n == 0) return EMERGE_OK;
+    // Upload into the staging buffer and check it there (contact groups are not on the
+    // device path; pinned particles switch the pinned load on), so a rejected upload
+    // leaves the simulation's particles untouched.
     CK(cudaMemcpyAsync(s->d_aos, in, n * sizeof(emerge_particle), cudaMemcpyHostToDevice, s->stream));
+    CK(cudaMemsetAsync(&s->d_state->upload_flags, 0, sizeof(uint32_t), s->stream));
+    launch_check_aos(s->d_aos, static_cast<int>(n), &s->d_state->upload_flags, s->stream);
+    CK(cudaMemcpyAsync(&s->h_state->upload_flags, &s->d_state->upload_flags, sizeof(uint32_t),
+                       cudaMemcpyDeviceToHost, s->stream));
+    CK(cudaStreamSynchronize(s->stream));
+    s->host_launches += 1;
+    const uint32_t flags = s->h_state->upload_flags;
+    if (flags & 1u)
+        return static_cast<emerge_status>(s->fail(
+            EMERGE_ERR_UNSUPPORTED, "contact_group != 0 (multi-field contact) is not on the device path"));
+    const int pinned = (flags & 2u) ? 1 : 0;  // the upload replaces every particle
+    if (pinned != s->lf.pinned) {
+        s->lf.pinned = pinned;
+        s->graph_dirty = true;  // the particle kernels' load flags are baked into the graph
+    }
     launch_scatter_aos(s->P[s->cur], static_cast<int>(n), s->d_aos, s->stream);
     s->host_launches += 1;
     CK(cudaGetLastError());
-    s->graph_dirty = true;  // load flags may have changed
     return invalidate_pending(s);
 }
 

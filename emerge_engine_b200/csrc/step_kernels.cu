@@ -10,7 +10,7 @@
 //                     (transfer/g2p.rs:151-328), constitutive update (:333-340),
 //                     CFL contribution for substep k+1 (step.rs:447-466), projection
 //                     for k+1 (step.rs:347-429), P2G scatter for k+1
-//                     (transfer/p2g.rs:24-72) through a shared-memory window.
+//                     (transfer/p2g.rs:24-72) as vector reductions into L2.
 //   k_density         only when a material needs it (step.rs:80-87): density gather
 //                     (solver/density.rs:41-72) + the fluid stress scatter, which
 //                     depends on that density (fluid.rs:157-162, 193-195).
@@ -146,34 +146,104 @@ __device__ __forceinline__ void store_fields(const DevParticles &P, int i, const
 __device__ __forceinline__ int cell_x_part(int x, int tpd) { return (((x >> 3) * tpd) << 6) + ((x & 7) << 3); }
 __device__ __forceinline__ int cell_y_part(int y) { return ((y >> 3) << 6) + (y & 7); }
 
+// True when the whole 3 x 3 stencil around base cell (bx, by) lies in the domain
+// (bx and by in [1, res - 2]); unsigned arithmetic keeps saturated bases false.
+__device__ __forceinline__ bool stencil_inside(int bx, int by, int res) {
+    return static_cast<unsigned>(bx) - 1u < static_cast<unsigned>(res - 2) &&
+           static_cast<unsigned>(by) - 1u < static_cast<unsigned>(res - 2);
+}
+
+// Stencil-offset form used by the fast path.  With e = (bx - x) + 0.5, the offset of
+// the centre cell, the offset of cell (bx + gx - 1, by + gy - 1) is
+// d = e + (gx - 1, gy - 1), so sums over the 3 x 3 stencil factor into per-row sums.
+__device__ __forceinline__ float2 centre_offset(const QW &w, float2 x) {
+    return v2((static_cast<float>(w.bx) - x.x) + 0.5f, (static_cast<float>(w.by) - x.y) + 0.5f);
+}
+
+// Grid velocities of the 3 x 3 stencil; cells outside the domain read as zero.
+template <bool CHECK>
+__device__ __forceinline__ void load_stencil_v(const GridView &g, const QW &w, float2 (&nv)[3][3]) {
+    int yp[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) yp[k] = cell_y_part(w.by + k - 1);
+#pragma unroll
+    for (int gx = 0; gx < 3; ++gx) {
+        const float2 *row = g.grid_v + cell_x_part(w.bx + gx - 1, g.tpd);
+#pragma unroll
+        for (int gy = 0; gy < 3; ++gy) {
+            if (CHECK && !in_domain(w.bx + gx - 1, w.by + gy - 1, g.res))
+                nv[gx][gy] = v2(0.0f, 0.0f);
+            else
+                nv[gx][gy] = row[yp[gy]];
+        }
+    }
+}
+
 // G2P phase 1 for one particle (transfer/g2p.rs:217-326 with ASFLIP, contact and
 // mixture gated off).  Returns 1 if the speed clamp fired.
+// FAST = false: the reference's cell-by-cell expression order (bit-level parity).
+// FAST = true: the same sums in stencil-offset form with fused multiply-adds:
+//   v' = sum w v_i,  B = v' (x) e + [sum (gx-1) w v_i, sum (gy-1) w v_i].
+template <bool FAST>
 __device__ __forceinline__ int g2p_particle(const GridView &g, const DevConfig &cfg, float dt,
                                             PState &p) {
     QW w = quadratic_weights(p.x);
-    const bool inside = w.bx >= 1 && w.by >= 1 && w.bx + 1 < g.res && w.by + 1 < g.res;
-    int xp[3], yp[3];
-#pragma unroll
-    for (int k = 0; k < 3; ++k) {
-        xp[k] = cell_x_part(w.bx + k - 1, g.tpd);
-        yp[k] = cell_y_part(w.by + k - 1);
-    }
+    const bool inside = stencil_inside(w.bx, w.by, g.res);
     float2 new_v = v2(0.0f, 0.0f);
     M2 b = mzero();
+    if constexpr (FAST) {
+        float2 nv[3][3];
+        if (inside)
+            load_stencil_v<false>(g, w, nv);
+        else
+            load_stencil_v<true>(g, w, nv);
+        float2 sx = v2(0.0f, 0.0f), sy = v2(0.0f, 0.0f);
 #pragma unroll
-    for (int gx = 0; gx < 3; ++gx) {
+        for (int gx = 0; gx < 3; ++gx) {
+            // row sums over gy: R = sum wy v, Ry = sum (gy-1) wy v
+            float2 r, ry;
+            r.x = __fmaf_rn(w.wy[0], nv[gx][0].x, __fmaf_rn(w.wy[1], nv[gx][1].x, w.wy[2] * nv[gx][2].x));
+            r.y = __fmaf_rn(w.wy[0], nv[gx][0].y, __fmaf_rn(w.wy[1], nv[gx][1].y, w.wy[2] * nv[gx][2].y));
+            ry.x = __fmaf_rn(w.wy[2], nv[gx][2].x, -(w.wy[0] * nv[gx][0].x));
+            ry.y = __fmaf_rn(w.wy[2], nv[gx][2].y, -(w.wy[0] * nv[gx][0].y));
+            const float wx = w.wx[gx];
+            new_v.x = __fmaf_rn(wx, r.x, new_v.x);
+            new_v.y = __fmaf_rn(wx, r.y, new_v.y);
+            sy.x = __fmaf_rn(wx, ry.x, sy.x);
+            sy.y = __fmaf_rn(wx, ry.y, sy.y);
+            if (gx == 0) {
+                sx.x = __fmaf_rn(-wx, r.x, sx.x);
+                sx.y = __fmaf_rn(-wx, r.y, sx.y);
+            } else if (gx == 2) {
+                sx.x = __fmaf_rn(wx, r.x, sx.x);
+                sx.y = __fmaf_rn(wx, r.y, sx.y);
+            }
+        }
+        const float2 e = centre_offset(w, p.x);
+        b.xa = v2(__fmaf_rn(new_v.x, e.x, sx.x), __fmaf_rn(new_v.y, e.x, sx.y));
+        b.ya = v2(__fmaf_rn(new_v.x, e.y, sy.x), __fmaf_rn(new_v.y, e.y, sy.y));
+    } else {
+        int xp[3], yp[3];
 #pragma unroll
-        for (int gy = 0; gy < 3; ++gy) {
-            float weight = w.wx[gx] * w.wy[gy];
-            int cx = w.bx + gx - 1, cy = w.by + gy - 1;
-            float2 dist = vadd(vsub(v2(static_cast<float>(cx), static_cast<float>(cy)), p.x),
-                               splat(0.5f));
-            float2 node_v = (inside || in_domain(cx, cy, g.res)) ? g.grid_v[xp[gx] + yp[gy]]
-                                                                  : v2(0.0f, 0.0f);
-            float2 wv = vmuls(node_v, weight);
-            M2 term = m2(vmuls(wv, dist.x), vmuls(wv, dist.y));
-            b = madd(b, term);
-            new_v = vadd(new_v, wv);
+        for (int k = 0; k < 3; ++k) {
+            xp[k] = cell_x_part(w.bx + k - 1, g.tpd);
+            yp[k] = cell_y_part(w.by + k - 1);
+        }
+#pragma unroll
+        for (int gx = 0; gx < 3; ++gx) {
+#pragma unroll
+            for (int gy = 0; gy < 3; ++gy) {
+                float weight = w.wx[gx] * w.wy[gy];
+                int cx = w.bx + gx - 1, cy = w.by + gy - 1;
+                float2 dist = vadd(vsub(v2(static_cast<float>(cx), static_cast<float>(cy)), p.x),
+                                   splat(0.5f));
+                float2 node_v = (inside || in_domain(cx, cy, g.res)) ? g.grid_v[xp[gx] + yp[gy]]
+                                                                      : v2(0.0f, 0.0f);
+                float2 wv = vmuls(node_v, weight);
+                M2 term = m2(vmuls(wv, dist.x), vmuls(wv, dist.y));
+                b = madd(b, term);
+                new_v = vadd(new_v, wv);
+            }
         }
     }
     if (p.pinned != 0) {
@@ -199,13 +269,25 @@ __device__ __forceinline__ int g2p_particle(const GridView &g, const DevConfig &
 
 static inline int blocks_for(int n, int per) { return (n + per - 1) / per; }
 
+// Instantiated model sets; a scene uses the smallest one covering its materials.
+constexpr unsigned MASK_FLUID = (1u << M_FALLBACK) | (1u << M_FLUID);
+constexpr unsigned MASK_SOLID = (1u << M_FALLBACK) | (1u << M_NEOHOOKEAN);
+constexpr unsigned MASK_SOLID_FLUID = MASK_FLUID | MASK_SOLID;
+constexpr unsigned MASK_GRANULAR =
+    (1u << M_FALLBACK) | (1u << M_DRUCKER_PRAGER) | (1u << M_SNOW) | (1u << M_NACC);
+
 // ---------------------------------------------------------------- scatter engine
 // P2G scatter of one particle per thread with vector red.global reductions (native
-// in L2 on sm_100).  Optional warp aggregation: lanes whose particles share a base
-// cell (contiguous after the tile sort) sum their contributions with a segmented
-// shuffle reduction and the segment's first lane issues one reduction per cell.
-// Tile flags for the grid update are set once per particle (its stencil spans at
-// most 2 x 2 tiles).
+// in L2 on sm_100).  The contribution to cell (bx + gx - 1, by + gy - 1) is
+//   mass      w m
+//   momentum  w m (v + C d)        = w (qa + (gx-1) m C.x_axis + (gy-1) m C.y_axis)
+//   stress    w s tau d            = w (qs + (gx-1) s tau.x_axis + (gy-1) s tau.y_axis)
+// with d = e + (gx - 1, gy - 1), qa = m (v + C e), qs = s tau e (stencil-offset form),
+// so a cell costs one weight product and a scale of a per-row vector.
+// Optional warp aggregation: lanes whose particles share a base cell (contiguous
+// after the tile sort) sum their contributions with a segmented shuffle reduction
+// and the segment's first lane issues one reduction per cell.  Tile flags for the
+// grid update are set once per particle (its stencil spans at most 2 x 2 tiles).
 constexpr int THREADS = 256;
 
 struct Payload {
@@ -218,6 +300,53 @@ struct Payload {
     bool do_ma;   // scatter mass + affine momentum
     bool do_s;    // scatter stress impulse
 };
+
+// Which channels a scatter call carries: mass + momentum, stress, or per-particle flags.
+enum ScatterChannels { SC_MA = 0, SC_S = 1, SC_BOTH = 2 };
+
+// Per-particle scatter plan: weights, mass, and (momentum.xy, stress.xy) as a row base
+// plus x/y steps.
+struct ScatterPlan {
+    QW w;
+    float m;
+    float4 q, sx, sy;
+};
+
+template <int SC>
+__device__ __forceinline__ ScatterPlan make_plan(const Payload &p) {
+    ScatterPlan r;
+    r.w = quadratic_weights(p.x);
+    const float2 e = centre_offset(r.w, p.x);
+    r.m = 0.0f;
+    r.q = r.sx = r.sy = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    if (SC != SC_S && (SC == SC_MA || p.do_ma)) {
+        r.m = p.m;
+        const float2 mx = svmul(p.m, p.c.xa), my = svmul(p.m, p.c.ya);
+        r.q.x = __fmaf_rn(mx.x, e.x, __fmaf_rn(my.x, e.y, p.m * p.v.x));
+        r.q.y = __fmaf_rn(mx.y, e.x, __fmaf_rn(my.y, e.y, p.m * p.v.y));
+        r.sx.x = mx.x; r.sx.y = mx.y;
+        r.sy.x = my.x; r.sy.y = my.y;
+    }
+    if (SC != SC_MA && (SC == SC_S || p.do_s)) {
+        const float2 tx = svmul(p.s, p.tau.xa), ty = svmul(p.s, p.tau.ya);
+        r.q.z = __fmaf_rn(tx.x, e.x, ty.x * e.y);
+        r.q.w = __fmaf_rn(tx.y, e.x, ty.y * e.y);
+        r.sx.z = tx.x; r.sx.w = tx.y;
+        r.sy.z = ty.x; r.sy.w = ty.y;
+    }
+    return r;
+}
+
+__device__ __forceinline__ float4 f4add(float4 a, float4 b) {
+    return make_float4(a.x + b.x, a.y + b.y, a.z + b.z, a.w + b.w);
+}
+__device__ __forceinline__ float4 f4sub(float4 a, float4 b) {
+    return make_float4(a.x - b.x, a.y - b.y, a.z - b.z, a.w - b.w);
+}
+// value of the plan's vector at stencil step k - 1 (k = 0, 1, 2)
+__device__ __forceinline__ float4 f4step(float4 base, float4 step, int k) {
+    return k == 0 ? f4sub(base, step) : (k == 2 ? f4add(base, step) : base);
+}
 
 // Adds the values of lanes [lane, seg_end) into `lane` (suffix sums within segments);
 // `span` (warp-uniform) bounds the segment lengths.
@@ -232,7 +361,7 @@ __device__ __forceinline__ float seg_sum(float v, int lane, int seg_end, int spa
 __device__ __forceinline__ void mark_tiles(const GridView &g, int bx, int by) {
     const int tx0 = max(bx - 1, 0) >> 3, tx1 = min(bx + 1, g.res - 1) >> 3;
     const int ty0 = max(by - 1, 0) >> 3, ty1 = min(by + 1, g.res - 1) >> 3;
-    if (bx + 1 < 0 || by + 1 < 0 || bx - 1 >= g.res || by - 1 >= g.res) return;
+    if (bx < -1 || by < -1 || bx > g.res || by > g.res) return;  // stencil misses the grid
     g.tile_flag[tx0 * g.tpd + ty0] = 1;
     if (tx1 != tx0) g.tile_flag[tx1 * g.tpd + ty0] = 1;
     if (ty1 != ty0) {
@@ -241,80 +370,105 @@ __device__ __forceinline__ void mark_tiles(const GridView &g, int bx, int by) {
     }
 }
 
-__device__ __forceinline__ void scatter_particle(const GridView &g, const Payload &p, bool valid,
-                                                 int aggregate) {
-    const int lane = threadIdx.x & 31;
-    const bool active = valid && (p.do_ma || p.do_s);
-    QW w;
-    if (active) w = quadratic_weights(p.x);
-    int head = 1, seg_end = 32, span = 1;
-    bool any_ma = true, any_s = true;
-    if (aggregate) {
-        any_ma = __ballot_sync(0xffffffffu, active && p.do_ma) != 0u;
-        any_s = __ballot_sync(0xffffffffu, active && p.do_s) != 0u;
-        const int kx = active ? w.bx : INT_MIN, ky = active ? w.by : lane;
-        const int px = __shfl_up_sync(0xffffffffu, kx, 1);
-        const int py = __shfl_up_sync(0xffffffffu, ky, 1);
-        head = (lane == 0 || !active || px != kx || py != ky) ? 1 : 0;
-        const unsigned heads = __ballot_sync(0xffffffffu, head != 0);
-        const unsigned after = heads & ~((2u << lane) - 1u);
-        seg_end = after ? __ffs(after) - 1 : 32;
-        // longest run of lanes sharing a base cell; 1 means nothing to combine
-        span = static_cast<int>(__reduce_max_sync(0xffffffffu, head ? static_cast<unsigned>(seg_end - lane) : 0u));
-        if (span <= 1) {
-            if (!active) return;
-            span = 1;
-        }
-    } else if (!active) {
-        return;
-    }
-    const bool inside = active && w.bx >= 1 && w.by >= 1 && w.bx + 1 < g.res && w.by + 1 < g.res;
-    int xp[3] = {0, 0, 0}, yp[3] = {0, 0, 0};
-    if (active) {
+// One lane's 3 x 3 reductions (no aggregation).  CHECK skips cells outside the domain.
+template <int SC, bool CHECK>
+__device__ __forceinline__ void scatter_cells(const GridView &g, const ScatterPlan &pl,
+                                              bool do_ma, bool do_s) {
+    const QW &w = pl.w;
+    int yp[3];
 #pragma unroll
-        for (int k = 0; k < 3; ++k) {
-            xp[k] = cell_x_part(w.bx + k - 1, g.tpd);
-            yp[k] = cell_y_part(w.by + k - 1);
-        }
-    }
+    for (int k = 0; k < 3; ++k) yp[k] = cell_y_part(w.by + k - 1);
 #pragma unroll
     for (int gx = 0; gx < 3; ++gx) {
+        const int xp = cell_x_part(w.bx + gx - 1, g.tpd);
+        const float4 r = f4step(pl.q, pl.sx, gx);
+        const float wm = w.wx[gx] * pl.m;
 #pragma unroll
         for (int gy = 0; gy < 3; ++gy) {
-            float mc = 0.0f;
-            float2 a = v2(0.0f, 0.0f), s = v2(0.0f, 0.0f);
-            int cx = 0, cy = 0;
-            if (active) {
-                float weight = w.wx[gx] * w.wy[gy];
-                cx = w.bx + gx - 1;
-                cy = w.by + gy - 1;
-                float2 cell_dist = vadd(vsub(v2(static_cast<float>(cx), static_cast<float>(cy)), p.x),
-                                        splat(0.5f));
-                if (p.do_ma) {
-                    mc = weight * p.m;
-                    a = svmul(weight, svmul(p.m, vadd(p.v, mv(p.c, cell_dist))));
-                }
-                if (p.do_s) s = svmul(weight, svmul(p.s, mv(p.tau, cell_dist)));
+            if (CHECK && !in_domain(w.bx + gx - 1, w.by + gy - 1, g.res)) continue;
+            const float4 t = f4step(r, pl.sy, gy);
+            const float wt = w.wx[gx] * w.wy[gy];
+            const int ci = xp + yp[gy];
+            if (SC == SC_MA || (SC == SC_BOTH && do_ma))
+                red_add_v4(&g.acc_a[ci], wm * w.wy[gy], wt * t.x, wt * t.y, 0.0f);
+            if (SC == SC_S || (SC == SC_BOTH && do_s)) red_add_v2(&g.acc_s[ci], wt * t.z, wt * t.w);
+        }
+    }
+}
+
+// Warp-aggregated variant: every lane of the warp takes part (inactive lanes add zero).
+template <int SC>
+__device__ __forceinline__ void scatter_cells_aggregated(const GridView &g, const ScatterPlan &pl,
+                                                         bool active, bool do_ma, bool do_s) {
+    const int lane = threadIdx.x & 31;
+    const QW &w = pl.w;
+    const bool any_ma = SC != SC_S && __ballot_sync(0xffffffffu, active && do_ma) != 0u;
+    const bool any_s = SC != SC_MA && __ballot_sync(0xffffffffu, active && do_s) != 0u;
+    const int kx = active ? w.bx : INT_MIN, ky = active ? w.by : lane;
+    const int px = __shfl_up_sync(0xffffffffu, kx, 1);
+    const int py = __shfl_up_sync(0xffffffffu, ky, 1);
+    const int head = (lane == 0 || !active || px != kx || py != ky) ? 1 : 0;
+    const unsigned heads = __ballot_sync(0xffffffffu, head != 0);
+    const unsigned after = heads & ~((2u << lane) - 1u);
+    const int seg_end = after ? __ffs(after) - 1 : 32;
+    // longest run of lanes sharing a base cell; 1 means nothing to combine
+    const int span = static_cast<int>(
+        __reduce_max_sync(0xffffffffu, head ? static_cast<unsigned>(seg_end - lane) : 0u));
+    if (span <= 1) {
+        if (!active) return;
+        if (SC == SC_MA) scatter_cells<SC_MA, true>(g, pl, do_ma, do_s);
+        else if (SC == SC_S) scatter_cells<SC_S, true>(g, pl, do_ma, do_s);
+        else scatter_cells<SC_BOTH, true>(g, pl, do_ma, do_s);
+        return;
+    }
+    int yp[3] = {0, 0, 0};
+#pragma unroll
+    for (int k = 0; k < 3; ++k) yp[k] = cell_y_part(w.by + k - 1);
+#pragma unroll
+    for (int gx = 0; gx < 3; ++gx) {
+        const int xp = cell_x_part(w.bx + gx - 1, g.tpd);
+        const float4 r = f4step(pl.q, pl.sx, gx);
+#pragma unroll
+        for (int gy = 0; gy < 3; ++gy) {
+            const float4 t = f4step(r, pl.sy, gy);
+            const float wt = active ? w.wx[gx] * w.wy[gy] : 0.0f;
+            float mc = wt * pl.m, ax = wt * t.x, ay = wt * t.y, sx = wt * t.z, sy = wt * t.w;
+            if (any_ma) {
+                mc = seg_sum(mc, lane, seg_end, span);
+                ax = seg_sum(ax, lane, seg_end, span);
+                ay = seg_sum(ay, lane, seg_end, span);
             }
-            if (span > 1) {
-                if (any_ma) {
-                    mc = seg_sum(mc, lane, seg_end, span);
-                    a.x = seg_sum(a.x, lane, seg_end, span);
-                    a.y = seg_sum(a.y, lane, seg_end, span);
-                }
-                if (any_s) {
-                    s.x = seg_sum(s.x, lane, seg_end, span);
-                    s.y = seg_sum(s.y, lane, seg_end, span);
-                }
+            if (any_s) {
+                sx = seg_sum(sx, lane, seg_end, span);
+                sy = seg_sum(sy, lane, seg_end, span);
             }
-            if (head && active && (inside || in_domain(cx, cy, g.res))) {
-                const int ci = xp[gx] + yp[gy];
-                if (p.do_ma || (span > 1 && any_ma)) red_add_v4(&g.acc_a[ci], mc, a.x, a.y, 0.0f);
-                if (p.do_s || (span > 1 && any_s)) red_add_v2(&g.acc_s[ci], s.x, s.y);
+            const int cx = w.bx + gx - 1, cy = w.by + gy - 1;
+            if (head && active && in_domain(cx, cy, g.res)) {
+                const int ci = xp + yp[gy];
+                if (any_ma) red_add_v4(&g.acc_a[ci], mc, ax, ay, 0.0f);
+                if (any_s) red_add_v2(&g.acc_s[ci], sx, sy);
             }
         }
     }
-    if (active) mark_tiles(g, w.bx, w.by);
+}
+
+template <int SC>
+__device__ __forceinline__ void scatter_particle(const GridView &g, const Payload &p, bool valid,
+                                                 int aggregate) {
+    const bool active = valid && (p.do_ma || p.do_s);
+    ScatterPlan pl{};
+    if (active) pl = make_plan<SC>(p);
+    if (aggregate) {
+        scatter_cells_aggregated<SC>(g, pl, active, p.do_ma, p.do_s);
+    } else {
+        if (!active) return;
+        const QW &w = pl.w;
+        if (stencil_inside(w.bx, w.by, g.res))
+            scatter_cells<SC, false>(g, pl, p.do_ma, p.do_s);
+        else
+            scatter_cells<SC, true>(g, pl, p.do_ma, p.do_s);
+    }
+    if (active) mark_tiles(g, pl.w.bx, pl.w.by);
 }
 
 // ---------------------------------------------------------------- k_particle
@@ -334,7 +488,7 @@ struct ParticleKernelArgs {
     int emit_p2g;       // project for substep k+1 and scatter its P2G (fused pipeline)
 };
 
-template <unsigned MASK>
+template <unsigned MASK, bool FAST>
 __global__ void __launch_bounds__(THREADS, 4) k_particle(ParticleKernelArgs a) {
     __shared__ MatP s_mats[MAX_MATERIALS];
     __shared__ float s_red[2][THREADS / 32];
@@ -368,7 +522,7 @@ __global__ void __launch_bounds__(THREADS, 4) k_particle(ParticleKernelArgs a) {
                     p.vol = p.mass / d;
                 }
             }
-            clamped = g2p_particle(a.g, cfg, dt, p);
+            clamped = g2p_particle<FAST>(a.g, cfg, dt, p);
             update_particle<MASK>(m, p, dt, pr);
             store_fields(a.P, i, o, p);
         }
@@ -415,10 +569,34 @@ __global__ void __launch_bounds__(THREADS, 4) k_particle(ParticleKernelArgs a) {
         atomicMin(&st->min_mdt_bits[acc_slot], __float_as_uint(md));
         atomicAdd(&st->window_blocks, 1ull);
     }
-    scatter_particle(a.g, pl, valid, a.aggregate);
+    if (MASK == MASK_FLUID && a.density_mode)
+        scatter_particle<SC_MA>(a.g, pl, valid, a.aggregate);
+    else
+        scatter_particle<SC_BOTH>(a.g, pl, valid, a.aggregate);
 }
 
 // ---------------------------------------------------------------- k_density
+// Density at a particle: sum of w m over its stencil (solver/density.rs:50-71), as
+// row sums sum_gx wx (sum_gy wy m).  CHECK reads cells outside the domain as zero.
+template <bool CHECK>
+__device__ __forceinline__ float gather_density(const GridView &g, const QW &w) {
+    int yp[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) yp[k] = cell_y_part(w.by + k - 1);
+    float density = 0.0f;
+#pragma unroll
+    for (int gx = 0; gx < 3; ++gx) {
+        const float4 *row = g.acc_a + cell_x_part(w.bx + gx - 1, g.tpd);
+        float mk[3];
+#pragma unroll
+        for (int gy = 0; gy < 3; ++gy)
+            mk[gy] = (CHECK && !in_domain(w.bx + gx - 1, w.by + gy - 1, g.res)) ? 0.0f : row[yp[gy]].x;
+        const float r = __fmaf_rn(w.wy[0], mk[0], __fmaf_rn(w.wy[1], mk[1], w.wy[2] * mk[2]));
+        density = __fmaf_rn(w.wx[gx], r, density);
+    }
+    return density;
+}
+
 struct DensityKernelArgs {
     DevParticles P;
     int n;
@@ -448,21 +626,9 @@ __global__ void __launch_bounds__(THREADS, 4) k_density(DensityKernelArgs a) {
     if (valid) {
         PState p = load_state(a.P, i, a.lf);
         if (cfg.project) project_state(cfg, p);
-        QW w = quadratic_weights(p.x);
-        const bool inside = w.bx >= 1 && w.by >= 1 && w.bx + 1 < a.g.res && w.by + 1 < a.g.res;
-        float density = 0.0f;
-#pragma unroll
-        for (int gx = 0; gx < 3; ++gx) {
-            const int xp = cell_x_part(w.bx + gx - 1, a.g.tpd);
-#pragma unroll
-            for (int gy = 0; gy < 3; ++gy) {
-                float weight = w.wx[gx] * w.wy[gy];
-                int cx = w.bx + gx - 1, cy = w.by + gy - 1;
-                float mc = (inside || in_domain(cx, cy, a.g.res))
-                               ? a.g.acc_a[xp + cell_y_part(cy)].x : 0.0f;
-                density += mc * weight;
-            }
-        }
+        const QW w = quadratic_weights(p.x);
+        const bool inside = stencil_inside(w.bx, w.by, a.g.res);
+        const float density = inside ? gather_density<false>(a.g, w) : gather_density<true>(a.g, w);
         a.P.rho_dp[i] = density;
         const MatP &m = s_mats[p.mat < static_cast<uint32_t>(a.n_mats) ? p.mat : 0u];
         if (m.model == M_FLUID) {
@@ -477,7 +643,7 @@ __global__ void __launch_bounds__(THREADS, 4) k_density(DensityKernelArgs a) {
             pl.do_s = true;
         }
     }
-    scatter_particle(a.g, pl, valid, a.aggregate);
+    scatter_particle<SC_S>(a.g, pl, valid, a.aggregate);
 }
 
 // ---------------------------------------------------------------- grid update
@@ -718,6 +884,18 @@ __global__ void k_scatter_aos(DevParticles P, int n, const emerge_particle *in) 
     put_slot(P, s, in[P.slot_to_index[s]]);
 }
 
+// Flags of an uploaded particle array: bit 0 some contact_group != 0 (not on the device
+// path), bit 1 some particle pinned.
+__global__ void k_check_aos(const emerge_particle *in, int n, uint32_t *flags) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    uint32_t f = 0;
+    if (k < n) f = (in[k].contact_group != 0 ? 1u : 0u) | (in[k].pinned != 0 ? 2u : 0u);
+    const unsigned any_c = __ballot_sync(0xffffffffu, (f & 1u) != 0u);
+    const unsigned any_p = __ballot_sync(0xffffffffu, (f & 2u) != 0u);
+    if ((threadIdx.x & 31) == 0 && (any_c | any_p))
+        atomicOr(flags, (any_c ? 1u : 0u) | (any_p ? 2u : 0u));
+}
+
 __global__ void k_append_aos(DevParticles P, int n_old, int n_new, const emerge_particle *in) {
     int k = blockIdx.x * blockDim.x + threadIdx.x;
     int s = n_old + k;
@@ -788,13 +966,6 @@ __global__ void k_mass_gather(DevParticles P, int lo, int hi, GridView g, int wr
 
 // ---------------------------------------------------------------- launchers
 
-// Instantiated model sets; a scene uses the smallest one covering its materials.
-constexpr unsigned MASK_FLUID = (1u << M_FALLBACK) | (1u << M_FLUID);
-constexpr unsigned MASK_SOLID = (1u << M_FALLBACK) | (1u << M_NEOHOOKEAN);
-constexpr unsigned MASK_SOLID_FLUID = MASK_FLUID | MASK_SOLID;
-constexpr unsigned MASK_GRANULAR =
-    (1u << M_FALLBACK) | (1u << M_DRUCKER_PRAGER) | (1u << M_SNOW) | (1u << M_NACC);
-
 unsigned covering_mask(unsigned m) {
     const unsigned masks[4] = {MASK_FLUID, MASK_SOLID, MASK_SOLID_FLUID, MASK_GRANULAR};
     for (unsigned c : masks)
@@ -828,6 +999,18 @@ static void fill_common(Args &a, const StepLaunch &L, const LoadFlagsHost &lfh) 
     default: kernel<ALL_MODELS><<<grid, THREADS, 0, L.stream>>>(args); break;           \
     }
 
+template <bool FAST>
+static void launch_particle_kernel(unsigned model_mask, int grid, const ParticleKernelArgs &a,
+                                   cudaStream_t stream) {
+    switch (covering_mask(model_mask)) {
+    case MASK_FLUID: k_particle<MASK_FLUID, FAST><<<grid, THREADS, 0, stream>>>(a); break;
+    case MASK_SOLID: k_particle<MASK_SOLID, FAST><<<grid, THREADS, 0, stream>>>(a); break;
+    case MASK_SOLID_FLUID: k_particle<MASK_SOLID_FLUID, FAST><<<grid, THREADS, 0, stream>>>(a); break;
+    case MASK_GRANULAR: k_particle<MASK_GRANULAR, FAST><<<grid, THREADS, 0, stream>>>(a); break;
+    default: k_particle<ALL_MODELS, FAST><<<grid, THREADS, 0, stream>>>(a); break;
+    }
+}
+
 void launch_particle_pass(const StepLaunch &L, const LoadFlagsHost &lfh, int mode_g2p,
                           int project_in, int emit_p2g) {
     if (L.n == 0) return;
@@ -838,7 +1021,10 @@ void launch_particle_pass(const StepLaunch &L, const LoadFlagsHost &lfh, int mod
     a.project_in = project_in;
     a.emit_p2g = emit_p2g;
     const int grid = blocks_for(L.n, THREADS);
-    EMERGE_DISPATCH_MASK(k_particle, L.model_mask, grid, a)
+    if (L.fast)
+        launch_particle_kernel<true>(L.model_mask, grid, a, L.stream);
+    else
+        launch_particle_kernel<false>(L.model_mask, grid, a, L.stream);
 }
 
 void launch_density_pass(const StepLaunch &L, const LoadFlagsHost &lfh) {
@@ -908,6 +1094,9 @@ void launch_gather_aos(const DevParticles &P, int n, emerge_particle *out, cudaS
 }
 void launch_scatter_aos(const DevParticles &P, int n, const emerge_particle *in, cudaStream_t stream) {
     if (n) k_scatter_aos<<<blocks_for(n, 256), 256, 0, stream>>>(P, n, in);
+}
+void launch_check_aos(const emerge_particle *in, int n, uint32_t *flags, cudaStream_t stream) {
+    if (n) k_check_aos<<<blocks_for(n, 256), 256, 0, stream>>>(in, n, flags);
 }
 void launch_append_aos(const DevParticles &P, int n_old, int n_new, const emerge_particle *in,
                        cudaStream_t stream) {

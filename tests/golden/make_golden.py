@@ -8,6 +8,8 @@ pinned by the reference's known-answer tests) on seeded scenes:
   quickstart_step1.npz / quickstart_step60.npz  -- full particle state of the README scene
   dam_break_128_step1.npz                        -- every 16th particle of 16384
   granular_256_region.json                       -- region_state after one frame
+  granular_256_substep1.npz                      -- every 32nd particle after one substep
+                                                    (frame dt = 1e-3, below the CFL bound)
 """
 import json
 import os
@@ -46,6 +48,10 @@ def main():
                         substeps=sim.last_substeps())
     with open(os.path.join(HERE, "granular_256_region.json"), "w") as f:
         json.dump(out, f, indent=1)
+    sim = scenes.mixed_granular(OracleSimulation, grid_res=256, target_particles=120_000, dt=1e-3)
+    sim.step()
+    assert sim.last_substeps() == 1
+    save("granular_256_substep1.npz", sim.particles()[::32].copy())
 
 
 if __name__ == "__main__":
