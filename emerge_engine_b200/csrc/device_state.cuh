@@ -59,6 +59,7 @@ struct StepState {
     unsigned long long vel_clamp;          // last_vel_clamp_count of the current step
     unsigned long long jproj;              // last_j_projection_count of the current step
     unsigned long long jproj_pending[2];   // projections counted for substep slot
+    unsigned long long proj_changed[2];    // particles whose projection changed their state, per slot
     float last_step_dt;
     float dropped;
     unsigned long long total_substeps;     // lifetime

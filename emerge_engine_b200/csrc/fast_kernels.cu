@@ -1,0 +1,54 @@
+// fast_kernels.cu -- the fast path's particle and density passes.
+//
+// Compiled with contraction into FMA and approximate division and square root (see
+// build.py): the fused pipeline's default mode, whose results differ from the reference
+// only in float rounding (summation order of the L2 reductions, FMA, 2-ulp division and
+// square root).  The reference-order mode runs the exact instantiation in step_kernels.cu.
+#define EMERGE_FAST_TU 1  // em_pow: integer exponents by repeated multiplication
+#include "particle_pass.cuh"
+
+// Resident CTAs per SM the register allocation is sized for (256 threads each).
+#ifndef EMERGE_PARTICLE_CTAS_PER_SM
+#define EMERGE_PARTICLE_CTAS_PER_SM 4
+#endif
+#ifndef EMERGE_DENSITY_CTAS_PER_SM
+#define EMERGE_DENSITY_CTAS_PER_SM 6
+#endif
+
+namespace emerge {
+
+template <unsigned MASK>
+__global__ void __launch_bounds__(THREADS, EMERGE_PARTICLE_CTAS_PER_SM) k_particle_fast(ParticleKernelArgs a) {
+    particle_pass<MASK, true>(a);
+}
+
+// estimate_particle_volumes gather (solver/density.rs:50-71) at the projected
+// positions, stored as rho_dp, plus the stress scatter of fluid particles.
+template <unsigned MASK>
+__global__ void __launch_bounds__(THREADS, EMERGE_DENSITY_CTAS_PER_SM) k_density(DensityKernelArgs a) {
+    density_pass<MASK>(a);
+}
+
+void launch_particle_pass_fast(const ParticleKernelArgs &a, unsigned model_mask, cudaStream_t stream) {
+    const int grid = blocks_for(a.n, THREADS);
+    switch (covering_mask(model_mask)) {
+    case MASK_FLUID: k_particle_fast<MASK_FLUID><<<grid, THREADS, 0, stream>>>(a); break;
+    case MASK_SOLID: k_particle_fast<MASK_SOLID><<<grid, THREADS, 0, stream>>>(a); break;
+    case MASK_SOLID_FLUID: k_particle_fast<MASK_SOLID_FLUID><<<grid, THREADS, 0, stream>>>(a); break;
+    case MASK_GRANULAR: k_particle_fast<MASK_GRANULAR><<<grid, THREADS, 0, stream>>>(a); break;
+    default: k_particle_fast<ALL_MODELS><<<grid, THREADS, 0, stream>>>(a); break;
+    }
+}
+
+void launch_density_pass_fast(const DensityKernelArgs &a, unsigned model_mask, cudaStream_t stream) {
+    const int grid = blocks_for(a.n, THREADS);
+    switch (covering_mask(model_mask)) {
+    case MASK_FLUID: k_density<MASK_FLUID><<<grid, THREADS, 0, stream>>>(a); break;
+    case MASK_SOLID: k_density<MASK_SOLID><<<grid, THREADS, 0, stream>>>(a); break;
+    case MASK_SOLID_FLUID: k_density<MASK_SOLID_FLUID><<<grid, THREADS, 0, stream>>>(a); break;
+    case MASK_GRANULAR: k_density<MASK_GRANULAR><<<grid, THREADS, 0, stream>>>(a); break;
+    default: k_density<ALL_MODELS><<<grid, THREADS, 0, stream>>>(a); break;
+    }
+}
+
+}  // namespace emerge

@@ -90,7 +90,22 @@ EM_HD float em_log(float x, bool pr) { return pr ? static_cast<float>(log(static
 EM_HD float em_sin(float x, bool pr) { return pr ? static_cast<float>(sin(static_cast<double>(x))) : sinf(x); }
 EM_HD float em_sinh(float x, bool pr) { return pr ? static_cast<float>(sinh(static_cast<double>(x))) : sinhf(x); }
 EM_HD float em_pow(float x, float y, bool pr) {
-    return pr ? static_cast<float>(pow(static_cast<double>(x), static_cast<double>(y))) : powf(x, y);
+    if (pr) return static_cast<float>(pow(static_cast<double>(x), static_cast<double>(y)));
+#if defined(EMERGE_FAST_TU)
+    // Fast path only: small integer exponents (the Tait equation of state's gamma = 7) by
+    // binary exponentiation, a few multiplies instead of a log/exp evaluation.
+    if (y == floorf(y) && fabsf(y) <= 16.0f) {
+        int e = static_cast<int>(fabsf(y));
+        float r = 1.0f, b = x;
+        while (e) {
+            if (e & 1) r *= b;
+            b *= b;
+            e >>= 1;
+        }
+        return y < 0.0f ? 1.0f / r : r;
+    }
+#endif
+    return powf(x, y);
 }
 
 // axis_weights (spacetime/grid/kernel.rs:20-25)
@@ -655,8 +670,11 @@ EM_HD float cfl_bound(const DevConfig &c, float max_speed, float min_mat_dt, flo
 EM_HD int sat_sub(int a, int b) { return a > b ? a - b : 0; }
 
 // project_particle_state_to_admissible (step.rs:347-429); returns true if corrected.
-EM_HD bool project_state(const DevConfig &c, PState &q) {
+// `changed` (optional) is set when the projection altered any field, the position clamp
+// and the density floor included: a state with changed == false is its own projection.
+EM_HD bool project_state(const DevConfig &c, PState &q, bool *changed = nullptr) {
     bool projected = false;
+    bool clamped = false;
     float mn = static_cast<float>(sat_sub(c.thickness, 1));
     float mx = static_cast<float>(sat_sub(c.res, c.thickness));
     float2 center = splat((mn + mx) * 0.5f);
@@ -664,7 +682,9 @@ EM_HD bool project_state(const DevConfig &c, PState &q) {
         q.x = center;
         projected = true;
     } else {
-        q.x = vclamp2(q.x, splat(mn), splat(mx));
+        const float2 xc = vclamp2(q.x, splat(mn), splat(mx));
+        clamped = xc.x != q.x.x || xc.y != q.x.y;
+        q.x = xc;
     }
     if (!vfinite(q.v)) {
         q.v = v2(0.0f, 0.0f);
@@ -701,8 +721,10 @@ EM_HD bool project_state(const DevConfig &c, PState &q) {
         q.rho = fmaxf(q.mass / q.vol, c.min_density);
         projected = true;
     } else {
+        clamped = clamped || q.rho < c.min_density;
         q.rho = fmaxf(q.rho, c.min_density);
     }
+    if (changed) *changed = projected || clamped;
     return projected;
 }
 

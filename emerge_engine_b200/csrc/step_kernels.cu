@@ -20,630 +20,16 @@
 #include <cfloat>
 #include <cstdio>
 
-#include "device_state.cuh"
-#include "kernels.h"
+#include "particle_pass.cuh"
 
 namespace emerge {
 
-// ---------------------------------------------------------------- reductions
-__device__ __forceinline__ void red_add_v4(float4 *p, float a, float b, float c, float d) {
-    asm volatile("red.global.add.v4.f32 [%0], {%1, %2, %3, %4};" ::"l"(p), "f"(a), "f"(b), "f"(c),
-                 "f"(d)
-                 : "memory");
-}
-__device__ __forceinline__ void red_add_v2(float2 *p, float a, float b) {
-    asm volatile("red.global.add.v2.f32 [%0], {%1, %2};" ::"l"(p), "f"(a), "f"(b) : "memory");
-}
-
-__device__ __forceinline__ float warp_max(float v) {
-    for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, o));
-    return v;
-}
-__device__ __forceinline__ float warp_min(float v) {
-    for (int o = 16; o > 0; o >>= 1) v = fminf(v, __shfl_xor_sync(0xffffffffu, v, o));
-    return v;
-}
-__device__ __forceinline__ int warp_imin(int v) {
-    for (int o = 16; o > 0; o >>= 1) v = min(v, __shfl_xor_sync(0xffffffffu, v, o));
-    return v;
-}
-__device__ __forceinline__ int warp_imax(int v) {
-    for (int o = 16; o > 0; o >>= 1) v = max(v, __shfl_xor_sync(0xffffffffu, v, o));
-    return v;
-}
-
-__device__ __forceinline__ void count_warp(unsigned long long *ctr, bool pred) {
-    unsigned ballot = __ballot_sync(0xffffffffu, pred);
-    if ((threadIdx.x & 31) == 0 && ballot) atomicAdd(ctr, (unsigned long long)__popc(ballot));
-}
-
-// ---------------------------------------------------------------- particle I/O
-struct LoadFlags {
-    int temperature;  // some material reads particle temperature
-    int activation;   // some material has a non-zero activation scale
-    int pinned;       // some particle is pinned
-};
-
-__device__ __forceinline__ PState load_state(const DevParticles &P, int i, const LoadFlags &lf) {
-    PState p;
-    p.x = P.x[i];
-    p.v = P.v[i];
-    p.c = m_from4(P.c[i]);
-    p.f = m_from4(P.f[i]);
-    p.mass = P.mass[i];
-    p.v0 = P.v0[i];
-    p.vol = P.vol[i];
-    p.rho = P.rho[i];
-    p.mat = P.mat[i];
-    p.jp = P.jp[i];
-    p.h = P.h[i];
-    p.q = P.q[i];
-    p.lvs = P.lvs[i];
-    p.temperature = lf.temperature ? P.temperature[i] : 0.0f;
-    p.activation = lf.activation ? P.activation[i] : 0.0f;
-    p.act_dir = lf.activation ? P.act_dir[i] : v2(0.0f, 0.0f);
-    p.pinned = lf.pinned ? P.pinned[i] : 0u;
-    return p;
-}
-
-__device__ __forceinline__ bool neq(float a, float b) { return __float_as_uint(a) != __float_as_uint(b); }
-__device__ __forceinline__ bool neq2(float2 a, float2 b) { return neq(a.x, b.x) || neq(a.y, b.y); }
-__device__ __forceinline__ bool neqm(M2 a, M2 b) { return neq2(a.xa, b.xa) || neq2(a.ya, b.ya); }
-
-// Writes back the fields that differ (bitwise) from what was loaded.
-__device__ __forceinline__ void store_changed(const DevParticles &P, int i, const PState &o,
-                                              const PState &p) {
-    if (neq2(p.x, o.x)) P.x[i] = p.x;
-    if (neq2(p.v, o.v)) P.v[i] = p.v;
-    if (neqm(p.c, o.c)) P.c[i] = m_to4(p.c);
-    if (neqm(p.f, o.f)) P.f[i] = m_to4(p.f);
-    if (neq(p.mass, o.mass)) P.mass[i] = p.mass;
-    if (neq(p.v0, o.v0)) P.v0[i] = p.v0;
-    if (neq(p.vol, o.vol)) P.vol[i] = p.vol;
-    if (neq(p.rho, o.rho)) P.rho[i] = p.rho;
-    if (neq(p.jp, o.jp)) P.jp[i] = p.jp;
-    if (neq(p.h, o.h)) P.h[i] = p.h;
-    if (neq(p.q, o.q)) P.q[i] = p.q;
-    if (neq(p.lvs, o.lvs)) P.lvs[i] = p.lvs;
-}
-
-// Fields the particle pass may leave unchanged (x, v and C always change in G2P):
-// kept to skip stores of bitwise-equal values.
-struct Saved {
-    M2 f;
-    float mass, v0, vol, rho, jp, h, q, lvs;
-};
-__device__ __forceinline__ Saved save_fields(const PState &p) {
-    Saved o;
-    o.f = p.f;
-    o.mass = p.mass;
-    o.v0 = p.v0;
-    o.vol = p.vol;
-    o.rho = p.rho;
-    o.jp = p.jp;
-    o.h = p.h;
-    o.q = p.q;
-    o.lvs = p.lvs;
-    return o;
-}
-__device__ __forceinline__ void store_fields(const DevParticles &P, int i, const Saved &o,
-                                             const PState &p) {
-    P.x[i] = p.x;
-    P.v[i] = p.v;
-    P.c[i] = m_to4(p.c);
-    if (neqm(p.f, o.f)) P.f[i] = m_to4(p.f);
-    if (neq(p.mass, o.mass)) P.mass[i] = p.mass;
-    if (neq(p.v0, o.v0)) P.v0[i] = p.v0;
-    if (neq(p.vol, o.vol)) P.vol[i] = p.vol;
-    if (neq(p.rho, o.rho)) P.rho[i] = p.rho;
-    if (neq(p.jp, o.jp)) P.jp[i] = p.jp;
-    if (neq(p.h, o.h)) P.h[i] = p.h;
-    if (neq(p.q, o.q)) P.q[i] = p.q;
-    if (neq(p.lvs, o.lvs)) P.lvs[i] = p.lvs;
-}
-
-// Tiled cell index split into an x part and a y part (cell_index = X(x) + Y(y)).
-__device__ __forceinline__ int cell_x_part(int x, int tpd) { return (((x >> 3) * tpd) << 6) + ((x & 7) << 3); }
-__device__ __forceinline__ int cell_y_part(int y) { return ((y >> 3) << 6) + (y & 7); }
-
-// True when the whole 3 x 3 stencil around base cell (bx, by) lies in the domain
-// (bx and by in [1, res - 2]); unsigned arithmetic keeps saturated bases false.
-__device__ __forceinline__ bool stencil_inside(int bx, int by, int res) {
-    return static_cast<unsigned>(bx) - 1u < static_cast<unsigned>(res - 2) &&
-           static_cast<unsigned>(by) - 1u < static_cast<unsigned>(res - 2);
-}
-
-// Stencil-offset form used by the fast path.  With e = (bx - x) + 0.5, the offset of
-// the centre cell, the offset of cell (bx + gx - 1, by + gy - 1) is
-// d = e + (gx - 1, gy - 1), so sums over the 3 x 3 stencil factor into per-row sums.
-__device__ __forceinline__ float2 centre_offset(const QW &w, float2 x) {
-    return v2((static_cast<float>(w.bx) - x.x) + 0.5f, (static_cast<float>(w.by) - x.y) + 0.5f);
-}
-
-// Grid velocities of the 3 x 3 stencil; cells outside the domain read as zero.
-template <bool CHECK>
-__device__ __forceinline__ void load_stencil_v(const GridView &g, const QW &w, float2 (&nv)[3][3]) {
-    int yp[3];
-#pragma unroll
-    for (int k = 0; k < 3; ++k) yp[k] = cell_y_part(w.by + k - 1);
-#pragma unroll
-    for (int gx = 0; gx < 3; ++gx) {
-        const float2 *row = g.grid_v + cell_x_part(w.bx + gx - 1, g.tpd);
-#pragma unroll
-        for (int gy = 0; gy < 3; ++gy) {
-            if (CHECK && !in_domain(w.bx + gx - 1, w.by + gy - 1, g.res))
-                nv[gx][gy] = v2(0.0f, 0.0f);
-            else
-                nv[gx][gy] = row[yp[gy]];
-        }
-    }
-}
-
-// G2P phase 1 for one particle (transfer/g2p.rs:217-326 with ASFLIP, contact and
-// mixture gated off).  Returns 1 if the speed clamp fired.
-// FAST = false: the reference's cell-by-cell expression order (bit-level parity).
-// FAST = true: the same sums in stencil-offset form with fused multiply-adds:
-//   v' = sum w v_i,  B = v' (x) e + [sum (gx-1) w v_i, sum (gy-1) w v_i].
-template <bool FAST>
-__device__ __forceinline__ int g2p_particle(const GridView &g, const DevConfig &cfg, float dt,
-                                            PState &p) {
-    QW w = quadratic_weights(p.x);
-    const bool inside = stencil_inside(w.bx, w.by, g.res);
-    float2 new_v = v2(0.0f, 0.0f);
-    M2 b = mzero();
-    if constexpr (FAST) {
-        float2 nv[3][3];
-        if (inside)
-            load_stencil_v<false>(g, w, nv);
-        else
-            load_stencil_v<true>(g, w, nv);
-        float2 sx = v2(0.0f, 0.0f), sy = v2(0.0f, 0.0f);
-#pragma unroll
-        for (int gx = 0; gx < 3; ++gx) {
-            // row sums over gy: R = sum wy v, Ry = sum (gy-1) wy v
-            float2 r, ry;
-            r.x = __fmaf_rn(w.wy[0], nv[gx][0].x, __fmaf_rn(w.wy[1], nv[gx][1].x, w.wy[2] * nv[gx][2].x));
-            r.y = __fmaf_rn(w.wy[0], nv[gx][0].y, __fmaf_rn(w.wy[1], nv[gx][1].y, w.wy[2] * nv[gx][2].y));
-            ry.x = __fmaf_rn(w.wy[2], nv[gx][2].x, -(w.wy[0] * nv[gx][0].x));
-            ry.y = __fmaf_rn(w.wy[2], nv[gx][2].y, -(w.wy[0] * nv[gx][0].y));
-            const float wx = w.wx[gx];
-            new_v.x = __fmaf_rn(wx, r.x, new_v.x);
-            new_v.y = __fmaf_rn(wx, r.y, new_v.y);
-            sy.x = __fmaf_rn(wx, ry.x, sy.x);
-            sy.y = __fmaf_rn(wx, ry.y, sy.y);
-            if (gx == 0) {
-                sx.x = __fmaf_rn(-wx, r.x, sx.x);
-                sx.y = __fmaf_rn(-wx, r.y, sx.y);
-            } else if (gx == 2) {
-                sx.x = __fmaf_rn(wx, r.x, sx.x);
-                sx.y = __fmaf_rn(wx, r.y, sx.y);
-            }
-        }
-        const float2 e = centre_offset(w, p.x);
-        b.xa = v2(__fmaf_rn(new_v.x, e.x, sx.x), __fmaf_rn(new_v.y, e.x, sx.y));
-        b.ya = v2(__fmaf_rn(new_v.x, e.y, sy.x), __fmaf_rn(new_v.y, e.y, sy.y));
-    } else {
-        int xp[3], yp[3];
-#pragma unroll
-        for (int k = 0; k < 3; ++k) {
-            xp[k] = cell_x_part(w.bx + k - 1, g.tpd);
-            yp[k] = cell_y_part(w.by + k - 1);
-        }
-#pragma unroll
-        for (int gx = 0; gx < 3; ++gx) {
-#pragma unroll
-            for (int gy = 0; gy < 3; ++gy) {
-                float weight = w.wx[gx] * w.wy[gy];
-                int cx = w.bx + gx - 1, cy = w.by + gy - 1;
-                float2 dist = vadd(vsub(v2(static_cast<float>(cx), static_cast<float>(cy)), p.x),
-                                   splat(0.5f));
-                float2 node_v = (inside || in_domain(cx, cy, g.res)) ? g.grid_v[xp[gx] + yp[gy]]
-                                                                      : v2(0.0f, 0.0f);
-                float2 wv = vmuls(node_v, weight);
-                M2 term = m2(vmuls(wv, dist.x), vmuls(wv, dist.y));
-                b = madd(b, term);
-                new_v = vadd(new_v, wv);
-            }
-        }
-    }
-    if (p.pinned != 0) {
-        p.v = v2(0.0f, 0.0f);
-        p.c = mzero();
-        return 0;
-    }
-    const float vel_limit = cfg.cell / dt;
-    int clamped = 0;
-    float spd = vlen(new_v);
-    if (spd > vel_limit) {
-        float scale = vel_limit / spd;
-        new_v = vmuls(new_v, scale);
-        clamped = 1;
-    }
-    float2 new_pos = vadd(p.x, vmuls(new_v, dt));
-    for (int k = 0; k < cfg.n_bound; ++k) new_pos = clamp_position(cfg.bound_t[k], new_pos, g.res);
-    p.v = new_v;
-    p.c = mscale(mscale(b, KERNEL_D_INVERSE), cfg.apic_blend);
-    p.x = new_pos;
-    return clamped;
-}
-
-static inline int blocks_for(int n, int per) { return (n + per - 1) / per; }
-
-// Instantiated model sets; a scene uses the smallest one covering its materials.
-constexpr unsigned MASK_FLUID = (1u << M_FALLBACK) | (1u << M_FLUID);
-constexpr unsigned MASK_SOLID = (1u << M_FALLBACK) | (1u << M_NEOHOOKEAN);
-constexpr unsigned MASK_SOLID_FLUID = MASK_FLUID | MASK_SOLID;
-constexpr unsigned MASK_GRANULAR =
-    (1u << M_FALLBACK) | (1u << M_DRUCKER_PRAGER) | (1u << M_SNOW) | (1u << M_NACC);
-
-// ---------------------------------------------------------------- scatter engine
-// P2G scatter of one particle per thread with vector red.global reductions (native
-// in L2 on sm_100).  The contribution to cell (bx + gx - 1, by + gy - 1) is
-//   mass      w m
-//   momentum  w m (v + C d)        = w (qa + (gx-1) m C.x_axis + (gy-1) m C.y_axis)
-//   stress    w s tau d            = w (qs + (gx-1) s tau.x_axis + (gy-1) s tau.y_axis)
-// with d = e + (gx - 1, gy - 1), qa = m (v + C e), qs = s tau e (stencil-offset form),
-// so a cell costs one weight product and a scale of a per-row vector.
-// Optional warp aggregation: lanes whose particles share a base cell (contiguous
-// after the tile sort) sum their contributions with a segmented shuffle reduction
-// and the segment's first lane issues one reduction per cell.  Tile flags for the
-// grid update are set once per particle (its stencil spans at most 2 x 2 tiles).
-constexpr int THREADS = 256;
-
-struct Payload {
-    float2 x;
-    float m;      // mass channel weight
-    float2 v;
-    M2 c;
-    M2 tau;
-    float s;      // -4 * stress_volume (dt-free stress coefficient)
-    bool do_ma;   // scatter mass + affine momentum
-    bool do_s;    // scatter stress impulse
-};
-
-// Which channels a scatter call carries: mass + momentum, stress, or per-particle flags.
-enum ScatterChannels { SC_MA = 0, SC_S = 1, SC_BOTH = 2 };
-
-// Per-particle scatter plan: weights, mass, and (momentum.xy, stress.xy) as a row base
-// plus x/y steps.
-struct ScatterPlan {
-    QW w;
-    float m;
-    float4 q, sx, sy;
-};
-
-template <int SC>
-__device__ __forceinline__ ScatterPlan make_plan(const Payload &p) {
-    ScatterPlan r;
-    r.w = quadratic_weights(p.x);
-    const float2 e = centre_offset(r.w, p.x);
-    r.m = 0.0f;
-    r.q = r.sx = r.sy = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-    if (SC != SC_S && (SC == SC_MA || p.do_ma)) {
-        r.m = p.m;
-        const float2 mx = svmul(p.m, p.c.xa), my = svmul(p.m, p.c.ya);
-        r.q.x = __fmaf_rn(mx.x, e.x, __fmaf_rn(my.x, e.y, p.m * p.v.x));
-        r.q.y = __fmaf_rn(mx.y, e.x, __fmaf_rn(my.y, e.y, p.m * p.v.y));
-        r.sx.x = mx.x; r.sx.y = mx.y;
-        r.sy.x = my.x; r.sy.y = my.y;
-    }
-    if (SC != SC_MA && (SC == SC_S || p.do_s)) {
-        const float2 tx = svmul(p.s, p.tau.xa), ty = svmul(p.s, p.tau.ya);
-        r.q.z = __fmaf_rn(tx.x, e.x, ty.x * e.y);
-        r.q.w = __fmaf_rn(tx.y, e.x, ty.y * e.y);
-        r.sx.z = tx.x; r.sx.w = tx.y;
-        r.sy.z = ty.x; r.sy.w = ty.y;
-    }
-    return r;
-}
-
-__device__ __forceinline__ float4 f4add(float4 a, float4 b) {
-    return make_float4(a.x + b.x, a.y + b.y, a.z + b.z, a.w + b.w);
-}
-__device__ __forceinline__ float4 f4sub(float4 a, float4 b) {
-    return make_float4(a.x - b.x, a.y - b.y, a.z - b.z, a.w - b.w);
-}
-// value of the plan's vector at stencil step k - 1 (k = 0, 1, 2)
-__device__ __forceinline__ float4 f4step(float4 base, float4 step, int k) {
-    return k == 0 ? f4sub(base, step) : (k == 2 ? f4add(base, step) : base);
-}
-
-// Adds the values of lanes [lane, seg_end) into `lane` (suffix sums within segments);
-// `span` (warp-uniform) bounds the segment lengths.
-__device__ __forceinline__ float seg_sum(float v, int lane, int seg_end, int span) {
-    for (int off = 1; off < span; off <<= 1) {
-        float y = __shfl_down_sync(0xffffffffu, v, off);
-        if (lane + off < seg_end) v += y;
-    }
-    return v;
-}
-
-__device__ __forceinline__ void mark_tiles(const GridView &g, int bx, int by) {
-    const int tx0 = max(bx - 1, 0) >> 3, tx1 = min(bx + 1, g.res - 1) >> 3;
-    const int ty0 = max(by - 1, 0) >> 3, ty1 = min(by + 1, g.res - 1) >> 3;
-    if (bx < -1 || by < -1 || bx > g.res || by > g.res) return;  // stencil misses the grid
-    g.tile_flag[tx0 * g.tpd + ty0] = 1;
-    if (tx1 != tx0) g.tile_flag[tx1 * g.tpd + ty0] = 1;
-    if (ty1 != ty0) {
-        g.tile_flag[tx0 * g.tpd + ty1] = 1;
-        if (tx1 != tx0) g.tile_flag[tx1 * g.tpd + ty1] = 1;
-    }
-}
-
-// One lane's 3 x 3 reductions (no aggregation).  CHECK skips cells outside the domain.
-template <int SC, bool CHECK>
-__device__ __forceinline__ void scatter_cells(const GridView &g, const ScatterPlan &pl,
-                                              bool do_ma, bool do_s) {
-    const QW &w = pl.w;
-    int yp[3];
-#pragma unroll
-    for (int k = 0; k < 3; ++k) yp[k] = cell_y_part(w.by + k - 1);
-#pragma unroll
-    for (int gx = 0; gx < 3; ++gx) {
-        const int xp = cell_x_part(w.bx + gx - 1, g.tpd);
-        const float4 r = f4step(pl.q, pl.sx, gx);
-        const float wm = w.wx[gx] * pl.m;
-#pragma unroll
-        for (int gy = 0; gy < 3; ++gy) {
-            if (CHECK && !in_domain(w.bx + gx - 1, w.by + gy - 1, g.res)) continue;
-            const float4 t = f4step(r, pl.sy, gy);
-            const float wt = w.wx[gx] * w.wy[gy];
-            const int ci = xp + yp[gy];
-            if (SC == SC_MA || (SC == SC_BOTH && do_ma))
-                red_add_v4(&g.acc_a[ci], wm * w.wy[gy], wt * t.x, wt * t.y, 0.0f);
-            if (SC == SC_S || (SC == SC_BOTH && do_s)) red_add_v2(&g.acc_s[ci], wt * t.z, wt * t.w);
-        }
-    }
-}
-
-// Warp-aggregated variant: every lane of the warp takes part (inactive lanes add zero).
-template <int SC>
-__device__ __forceinline__ void scatter_cells_aggregated(const GridView &g, const ScatterPlan &pl,
-                                                         bool active, bool do_ma, bool do_s) {
-    const int lane = threadIdx.x & 31;
-    const QW &w = pl.w;
-    const bool any_ma = SC != SC_S && __ballot_sync(0xffffffffu, active && do_ma) != 0u;
-    const bool any_s = SC != SC_MA && __ballot_sync(0xffffffffu, active && do_s) != 0u;
-    const int kx = active ? w.bx : INT_MIN, ky = active ? w.by : lane;
-    const int px = __shfl_up_sync(0xffffffffu, kx, 1);
-    const int py = __shfl_up_sync(0xffffffffu, ky, 1);
-    const int head = (lane == 0 || !active || px != kx || py != ky) ? 1 : 0;
-    const unsigned heads = __ballot_sync(0xffffffffu, head != 0);
-    const unsigned after = heads & ~((2u << lane) - 1u);
-    const int seg_end = after ? __ffs(after) - 1 : 32;
-    // longest run of lanes sharing a base cell; 1 means nothing to combine
-    const int span = static_cast<int>(
-        __reduce_max_sync(0xffffffffu, head ? static_cast<unsigned>(seg_end - lane) : 0u));
-    if (span <= 1) {
-        if (!active) return;
-        if (SC == SC_MA) scatter_cells<SC_MA, true>(g, pl, do_ma, do_s);
-        else if (SC == SC_S) scatter_cells<SC_S, true>(g, pl, do_ma, do_s);
-        else scatter_cells<SC_BOTH, true>(g, pl, do_ma, do_s);
-        return;
-    }
-    int yp[3] = {0, 0, 0};
-#pragma unroll
-    for (int k = 0; k < 3; ++k) yp[k] = cell_y_part(w.by + k - 1);
-#pragma unroll
-    for (int gx = 0; gx < 3; ++gx) {
-        const int xp = cell_x_part(w.bx + gx - 1, g.tpd);
-        const float4 r = f4step(pl.q, pl.sx, gx);
-#pragma unroll
-        for (int gy = 0; gy < 3; ++gy) {
-            const float4 t = f4step(r, pl.sy, gy);
-            const float wt = active ? w.wx[gx] * w.wy[gy] : 0.0f;
-            float mc = wt * pl.m, ax = wt * t.x, ay = wt * t.y, sx = wt * t.z, sy = wt * t.w;
-            if (any_ma) {
-                mc = seg_sum(mc, lane, seg_end, span);
-                ax = seg_sum(ax, lane, seg_end, span);
-                ay = seg_sum(ay, lane, seg_end, span);
-            }
-            if (any_s) {
-                sx = seg_sum(sx, lane, seg_end, span);
-                sy = seg_sum(sy, lane, seg_end, span);
-            }
-            const int cx = w.bx + gx - 1, cy = w.by + gy - 1;
-            if (head && active && in_domain(cx, cy, g.res)) {
-                const int ci = xp + yp[gy];
-                if (any_ma) red_add_v4(&g.acc_a[ci], mc, ax, ay, 0.0f);
-                if (any_s) red_add_v2(&g.acc_s[ci], sx, sy);
-            }
-        }
-    }
-}
-
-template <int SC>
-__device__ __forceinline__ void scatter_particle(const GridView &g, const Payload &p, bool valid,
-                                                 int aggregate) {
-    const bool active = valid && (p.do_ma || p.do_s);
-    ScatterPlan pl{};
-    if (active) pl = make_plan<SC>(p);
-    if (aggregate) {
-        scatter_cells_aggregated<SC>(g, pl, active, p.do_ma, p.do_s);
-    } else {
-        if (!active) return;
-        const QW &w = pl.w;
-        if (stencil_inside(w.bx, w.by, g.res))
-            scatter_cells<SC, false>(g, pl, p.do_ma, p.do_s);
-        else
-            scatter_cells<SC, true>(g, pl, p.do_ma, p.do_s);
-    }
-    if (active) mark_tiles(g, pl.w.bx, pl.w.by);
-}
-
-// ---------------------------------------------------------------- k_particle
-struct ParticleKernelArgs {
-    DevParticles P;
-    int n;
-    const MatP *mats;
-    int n_mats;
-    DevConfig cfg;
-    StepState *st;
-    GridView g;
-    LoadFlags lf;
-    int mode_g2p;       // 0: prime pass (no G2P), 1: G2P(k) + P2G(k+1)
-    int density_mode;   // fluid stress deferred to k_density; G2P reads rho_dp
-    int aggregate;      // warp-aggregated P2G reductions
-    int project_in;     // recompute the projection of substep k before G2P (fused pipeline)
-    int emit_p2g;       // project for substep k+1 and scatter its P2G (fused pipeline)
-};
-
-template <unsigned MASK, bool FAST>
-__global__ void __launch_bounds__(THREADS, 4) k_particle(ParticleKernelArgs a) {
-    __shared__ MatP s_mats[MAX_MATERIALS];
-    __shared__ float s_red[2][THREADS / 32];
-    for (int k = threadIdx.x; k < a.n_mats; k += THREADS) s_mats[k] = a.mats[k];
-    __syncthreads();
-
-    const DevConfig &cfg = a.cfg;
-    const bool pr = cfg.precise_math != 0;
-    StepState *st = a.st;
-    const int acc_slot = st->acc_slot;
-    const float dt = st->sub_dt;
-    const int i = blockIdx.x * THREADS + threadIdx.x;
-    const bool valid = i < a.n;
-
-    Payload pl;
-    pl.do_ma = false;
-    pl.do_s = false;
-    float max_speed = 0.0f;
-    float min_mdt = INFINITY;
-    int clamped = 0, projected = 0;
-    if (valid) {
-        PState p = load_state(a.P, i, a.lf);
-        const MatP &m = s_mats[p.mat < static_cast<uint32_t>(a.n_mats) ? p.mat : 0u];
-        if (a.mode_g2p) {
-            const Saved o = save_fields(p);
-            if (a.project_in) project_state(cfg, p);  // recompute S'(k); counted earlier
-            if (a.density_mode && a.project_in) {
-                float d = a.P.rho_dp[i];
-                if (d > F32_EPS) {
-                    p.rho = d;
-                    p.vol = p.mass / d;
-                }
-            }
-            clamped = g2p_particle<FAST>(a.g, cfg, dt, p);
-            update_particle<MASK>(m, p, dt, pr);
-            store_fields(a.P, i, o, p);
-        }
-        // CFL contribution for the next substep (step.rs:447-466)
-        float sp = vlen(p.v);
-        if (cfg.affine_cfl) sp += affine_cfl(p.c, cfg.cell);
-        max_speed = sp;
-        float mdt = timestep_bound<MASK>(m, p.rho, p.h, cfg.cell, cfg.mat_cfl, cfg.visc_cfl, pr);
-        if (isfinite(mdt) && mdt > 0.0f) min_mdt = mdt;
-        if (a.emit_p2g) {
-            // projection of the next substep (step.rs:67-73) and its P2G payload
-            if (cfg.project) projected = project_state(cfg, p) ? 1 : 0;
-            pl.x = p.x;
-            pl.m = p.mass;
-            pl.v = p.v;
-            pl.c = p.c;
-            pl.do_ma = true;
-            if (!(a.density_mode && m.model == M_FLUID)) {
-                pl.tau = combined_kirchhoff_stress<MASK>(m, p, pr);
-                pl.s = -stress_volume(m, p) * KERNEL_D_INVERSE;
-                pl.do_s = true;
-            }
-        }
-    }
-    count_warp(&st->vel_clamp, clamped != 0);
-    count_warp(&st->jproj_pending[acc_slot], projected != 0);
-
-    // CFL block reduction -> one atomic per block
-    max_speed = warp_max(max_speed);
-    min_mdt = warp_min(min_mdt);
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    if (lane == 0) {
-        s_red[0][warp] = max_speed;
-        s_red[1][warp] = min_mdt;
-    }
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        float ms = 0.0f, md = INFINITY;
-        for (int w = 0; w < THREADS / 32; ++w) {
-            ms = fmaxf(ms, s_red[0][w]);
-            md = fminf(md, s_red[1][w]);
-        }
-        atomicMax(&st->max_speed_bits[acc_slot], __float_as_uint(ms));
-        atomicMin(&st->min_mdt_bits[acc_slot], __float_as_uint(md));
-        atomicAdd(&st->window_blocks, 1ull);
-    }
-    if (MASK == MASK_FLUID && a.density_mode)
-        scatter_particle<SC_MA>(a.g, pl, valid, a.aggregate);
-    else
-        scatter_particle<SC_BOTH>(a.g, pl, valid, a.aggregate);
-}
-
-// ---------------------------------------------------------------- k_density
-// Density at a particle: sum of w m over its stencil (solver/density.rs:50-71), as
-// row sums sum_gx wx (sum_gy wy m).  CHECK reads cells outside the domain as zero.
-template <bool CHECK>
-__device__ __forceinline__ float gather_density(const GridView &g, const QW &w) {
-    int yp[3];
-#pragma unroll
-    for (int k = 0; k < 3; ++k) yp[k] = cell_y_part(w.by + k - 1);
-    float density = 0.0f;
-#pragma unroll
-    for (int gx = 0; gx < 3; ++gx) {
-        const float4 *row = g.acc_a + cell_x_part(w.bx + gx - 1, g.tpd);
-        float mk[3];
-#pragma unroll
-        for (int gy = 0; gy < 3; ++gy)
-            mk[gy] = (CHECK && !in_domain(w.bx + gx - 1, w.by + gy - 1, g.res)) ? 0.0f : row[yp[gy]].x;
-        const float r = __fmaf_rn(w.wy[0], mk[0], __fmaf_rn(w.wy[1], mk[1], w.wy[2] * mk[2]));
-        density = __fmaf_rn(w.wx[gx], r, density);
-    }
-    return density;
-}
-
-struct DensityKernelArgs {
-    DevParticles P;
-    int n;
-    const MatP *mats;
-    int n_mats;
-    DevConfig cfg;
-    StepState *st;
-    GridView g;
-    LoadFlags lf;
-    int aggregate;
-};
-
-// estimate_particle_volumes gather (solver/density.rs:50-71) at the projected
-// positions, stored as rho_dp, plus the stress scatter of fluid particles.
+// ---------------------------------------------------------------- k_particle (exact)
+// Reference-order mode: cell-by-cell stencil sums, IEEE division and square root, no
+// contraction (this file is compiled with -fmad=false).
 template <unsigned MASK>
-__global__ void __launch_bounds__(THREADS, 4) k_density(DensityKernelArgs a) {
-    __shared__ MatP s_mats[MAX_MATERIALS];
-    for (int k = threadIdx.x; k < a.n_mats; k += THREADS) s_mats[k] = a.mats[k];
-    __syncthreads();
-    const DevConfig &cfg = a.cfg;
-    const bool pr = cfg.precise_math != 0;
-    const int i = blockIdx.x * THREADS + threadIdx.x;
-    const bool valid = i < a.n;
-    Payload pl;
-    pl.do_ma = false;
-    pl.do_s = false;
-    if (valid) {
-        PState p = load_state(a.P, i, a.lf);
-        if (cfg.project) project_state(cfg, p);
-        const QW w = quadratic_weights(p.x);
-        const bool inside = stencil_inside(w.bx, w.by, a.g.res);
-        const float density = inside ? gather_density<false>(a.g, w) : gather_density<true>(a.g, w);
-        a.P.rho_dp[i] = density;
-        const MatP &m = s_mats[p.mat < static_cast<uint32_t>(a.n_mats) ? p.mat : 0u];
-        if (m.model == M_FLUID) {
-            if (density > F32_EPS) {
-                p.rho = density;
-                p.vol = p.mass / density;
-            }
-            pl.x = p.x;
-            pl.m = 0.0f;
-            pl.tau = combined_kirchhoff_stress<MASK>(m, p, pr);
-            pl.s = -stress_volume(m, p) * KERNEL_D_INVERSE;
-            pl.do_s = true;
-        }
-    }
-    scatter_particle<SC_S>(a.g, pl, valid, a.aggregate);
+__global__ void __launch_bounds__(THREADS, 4) k_particle(ParticleKernelArgs a) {
+    particle_pass<MASK, false>(a);
 }
 
 // ---------------------------------------------------------------- grid update
@@ -720,6 +106,7 @@ __global__ void k_substep_begin(StepState *st, DevConfig cfg, int use_cond,
     s.max_speed_bits[k1] = 0u;
     s.min_mdt_bits[k1] = __float_as_uint(INFINITY);
     s.jproj_pending[k1] = 0ull;
+    s.proj_changed[k1] = 0ull;
     s.acc_slot = k1;
     s.parity = k1;
     const float rem_after = rem - dt;
@@ -740,6 +127,7 @@ __global__ void k_prime_setup(StepState *st) {
     st->max_speed_bits[k] = 0u;
     st->min_mdt_bits[k] = __float_as_uint(INFINITY);
     st->jproj_pending[k] = 0ull;
+    st->proj_changed[k] = 0ull;
     st->acc_slot = k;
 }
 
@@ -966,51 +354,6 @@ __global__ void k_mass_gather(DevParticles P, int lo, int hi, GridView g, int wr
 
 // ---------------------------------------------------------------- launchers
 
-unsigned covering_mask(unsigned m) {
-    const unsigned masks[4] = {MASK_FLUID, MASK_SOLID, MASK_SOLID_FLUID, MASK_GRANULAR};
-    for (unsigned c : masks)
-        if ((m & ~c) == 0u) return c;
-    return ALL_MODELS;
-}
-
-template <class Args>
-static void fill_common(Args &a, const StepLaunch &L, const LoadFlagsHost &lfh) {
-    a.P = L.P;
-    a.n = L.n;
-    a.mats = L.mats;
-    a.n_mats = L.n_mats;
-    a.cfg = L.cfg;
-    a.st = L.st;
-    a.g = L.g;
-    a.lf.temperature = lfh.temperature;
-    a.lf.activation = lfh.activation;
-    a.lf.pinned = lfh.pinned;
-    a.aggregate = L.use_window;
-}
-
-#define EMERGE_DISPATCH_MASK(kernel, mask, grid, args)                                 \
-    switch (covering_mask(mask)) {                                                     \
-    case MASK_FLUID: kernel<MASK_FLUID><<<grid, THREADS, 0, L.stream>>>(args); break;   \
-    case MASK_SOLID: kernel<MASK_SOLID><<<grid, THREADS, 0, L.stream>>>(args); break;   \
-    case MASK_SOLID_FLUID:                                                             \
-        kernel<MASK_SOLID_FLUID><<<grid, THREADS, 0, L.stream>>>(args);                \
-        break;                                                                         \
-    case MASK_GRANULAR: kernel<MASK_GRANULAR><<<grid, THREADS, 0, L.stream>>>(args); break; \
-    default: kernel<ALL_MODELS><<<grid, THREADS, 0, L.stream>>>(args); break;           \
-    }
-
-template <bool FAST>
-static void launch_particle_kernel(unsigned model_mask, int grid, const ParticleKernelArgs &a,
-                                   cudaStream_t stream) {
-    switch (covering_mask(model_mask)) {
-    case MASK_FLUID: k_particle<MASK_FLUID, FAST><<<grid, THREADS, 0, stream>>>(a); break;
-    case MASK_SOLID: k_particle<MASK_SOLID, FAST><<<grid, THREADS, 0, stream>>>(a); break;
-    case MASK_SOLID_FLUID: k_particle<MASK_SOLID_FLUID, FAST><<<grid, THREADS, 0, stream>>>(a); break;
-    case MASK_GRANULAR: k_particle<MASK_GRANULAR, FAST><<<grid, THREADS, 0, stream>>>(a); break;
-    default: k_particle<ALL_MODELS, FAST><<<grid, THREADS, 0, stream>>>(a); break;
-    }
-}
-
 void launch_particle_pass(const StepLaunch &L, const LoadFlagsHost &lfh, int mode_g2p,
                           int project_in, int emit_p2g) {
     if (L.n == 0) return;
@@ -1020,19 +363,25 @@ void launch_particle_pass(const StepLaunch &L, const LoadFlagsHost &lfh, int mod
     a.density_mode = L.density_mode;
     a.project_in = project_in;
     a.emit_p2g = emit_p2g;
+    if (L.fast) {
+        launch_particle_pass_fast(a, L.model_mask, L.stream);
+        return;
+    }
     const int grid = blocks_for(L.n, THREADS);
-    if (L.fast)
-        launch_particle_kernel<true>(L.model_mask, grid, a, L.stream);
-    else
-        launch_particle_kernel<false>(L.model_mask, grid, a, L.stream);
+    switch (covering_mask(L.model_mask)) {
+    case MASK_FLUID: k_particle<MASK_FLUID><<<grid, THREADS, 0, L.stream>>>(a); break;
+    case MASK_SOLID: k_particle<MASK_SOLID><<<grid, THREADS, 0, L.stream>>>(a); break;
+    case MASK_SOLID_FLUID: k_particle<MASK_SOLID_FLUID><<<grid, THREADS, 0, L.stream>>>(a); break;
+    case MASK_GRANULAR: k_particle<MASK_GRANULAR><<<grid, THREADS, 0, L.stream>>>(a); break;
+    default: k_particle<ALL_MODELS><<<grid, THREADS, 0, L.stream>>>(a); break;
+    }
 }
 
 void launch_density_pass(const StepLaunch &L, const LoadFlagsHost &lfh) {
     if (L.n == 0) return;
     DensityKernelArgs a;
     fill_common(a, L, lfh);
-    const int grid = blocks_for(L.n, THREADS);
-    EMERGE_DISPATCH_MASK(k_density, L.model_mask, grid, a)
+    launch_density_pass_fast(a, L.model_mask, L.stream);
 }
 
 void launch_grid_update(const StepLaunch &L) {
