@@ -193,6 +193,50 @@ class ClockSampler:
                 "source": self.source}
 
 
+def closure_ab(sim, n: int, steps: int, plain_value: float) -> dict:
+    """Learned return-mapping closure on the same scene: log the plain mapping for one step,
+    train the networks with the library's kernels, then time `steps` steps with the closure
+    on (same timing as the main loop) and report its live judged error."""
+    sim.closure_log(2_000_000, 8)
+    sim.step()
+    sim.closure_log(0, 1)
+    logged = sim.closure_stats()["logged"]
+    train = {}
+    for model, name in ((0, "drucker_prager"), (1, "nacc")):
+        if logged[model] < 1024:
+            train[name] = {"samples": int(logged[model]), "trained": False,
+                           "note": "too few samples on the smooth plastic branch"}
+            continue
+        rep = sim.closure_train(model, epochs=20, batch=8192, lr=3e-3, lr_decay=0.9, seed=1)
+        train[name] = {"trained": True, "samples": int(rep["n_train"] + rep["n_val"]),
+                       "epochs": 20, "seconds": rep["seconds"], "val_err_mean": rep["val_err_mean"],
+                       "val_err_p99": rep["val_err_p99"], "val_err_max": rep["val_err_max"],
+                       "val_err_trial_mean": rep["val_err_trial_mean"]}
+    sim.closure_enable(True, judge_stride=64)
+    sim.step()
+    sim.synchronize()
+    sim.closure_stats(reset=True)
+    sub0 = sim.stats()["substeps"]
+    total_ms = 0.0
+    for _ in range(steps):
+        sim.flush_l2()
+        sim.event_record(0)
+        sim.step()
+        sim.event_record(1)
+        total_ms += sim.event_elapsed_ms(0, 1)
+    subs = sim.stats()["substeps"] - sub0
+    st = sim.closure_stats()
+    sim.closure_enable(False)
+    value = n * subs / (total_ms / 1000.0)
+    smooth = max(st["smooth"], 1)
+    return {"value": value, "unit": UNIT, "ms_per_step": total_ms / steps,
+            "vs_plain": value / plain_value, "judge_stride": 64,
+            "err_mean": st["err_mean"], "err_max": st["err_max"], "judged": st["judged"],
+            "net_frac": st["net"] / smooth, "hull_fallback_frac": st["hull_fallback"] / smooth,
+            "error_metric": "relative error of the principal Kirchhoff stress vs the plain mapping",
+            "train": train}
+
+
 def reduce_over_ranks(dist, device, total_ms: float, units: float, launches: int):
     """Replica aggregation: device time is the max over ranks (the job ends with the slowest
     replica); particle-substeps and kernel launches add up."""
@@ -286,6 +330,8 @@ def main():
     ap.add_argument("--no-extras", action="store_true",
                     help="skip e2e, roofline instrumentation and CPU baseline (profiling runs)")
     ap.add_argument("--cpu-budget", type=float, default=15.0)
+    ap.add_argument("--no-closure", action="store_true",
+                    help="skip the learned-closure A/B on scenes with plastic materials")
     ap.add_argument("--ref-budget", type=float, default=90.0,
                     help="--impl reference: seconds of timed CPU steps at most")
     ap.add_argument("--ref-warmup-budget", type=float, default=20.0)
@@ -403,6 +449,8 @@ def main():
         extras["e2e"] = {"value": e2e_units / e2e_s, "unit": UNIT,
                          "h2d_bytes_per_step": n * 128, "d2h_bytes_per_step": n * 128,
                          "steps": e2e_steps, "timing": "host wall clock around the C-ABI calls"}
+        if spec["material"] == "DP+Snow+NACC" and not args.no_closure:
+            extras["learned_closure"] = closure_ab(sim, n, args.steps, value)
         if world == 1 and rank == 0:
             extras["cpu_baseline"] = cpu_baseline(args.workload, args.cpu_budget)
 

@@ -140,6 +140,32 @@ class StatsC(Structure):
         "steps", "substeps", "kernel_launches", "p2g_blocks", "p2g_fallback_blocks", "sorts")]
 
 
+class ClosureStatsC(Structure):
+    """`emerge_closure_stats` (include/emerge_cuda.h)."""
+    _fields_ = [("smooth", c_uint64), ("net", c_uint64), ("hull_fallback", c_uint64),
+                ("judged", c_uint64), ("logged", c_uint64 * 2), ("err_mean", ctypes.c_double),
+                ("err_max", c_float), ("pad_", c_uint32)]
+
+
+class ClosureTrainConfigC(Structure):
+    """`emerge_closure_train_config` (include/emerge_cuda.h)."""
+    _fields_ = [("epochs", c_uint32), ("batch", c_uint32), ("lr", c_float), ("lr_decay", c_float),
+                ("beta1", c_float), ("beta2", c_float), ("eps", c_float), ("val_fraction", c_float),
+                ("seed", c_uint64), ("max_samples", c_uint64)]
+
+
+class ClosureTrainReportC(Structure):
+    """`emerge_closure_train_report` (include/emerge_cuda.h)."""
+    _fields_ = [("n_train", c_uint64), ("n_val", c_uint64), ("train_loss", c_float),
+                ("val_loss", c_float), ("val_err_mean", c_float), ("val_err_p50", c_float),
+                ("val_err_p99", c_float), ("val_err_max", c_float), ("val_err_trial_mean", c_float),
+                ("seconds", c_float),
+                ("steps", c_uint32)]
+
+
+CLOSURE_NPARAMS = 8963  # W1[6][64] b1 W2[64][64] b2 W3[64][64] b3 W4[64][3] b4
+CLOSURE_NNORM = 18      # in_shift[6] in_scale[6] out_shift[3] out_scale[3]
+
 # Entry points declared in include/emerge_cuda.h: (name, restype, argtypes)
 SIM = c_void_p
 ABI_FUNCTIONS = [
@@ -175,6 +201,18 @@ ABI_FUNCTIONS = [
     ("emerge_cuda_host_alloc", c_int, [ctypes.c_size_t, POINTER(c_void_p)]),
     ("emerge_cuda_host_free", c_int, [c_void_p]),
     ("emerge_cuda_stats", c_int, [SIM, POINTER(StatsC)]),
+    ("emerge_cuda_closure_log", c_int, [SIM, c_uint64, c_uint32]),
+    ("emerge_cuda_closure_train", c_int, [SIM, c_int, POINTER(ClosureTrainConfigC),
+                                          POINTER(ClosureTrainReportC)]),
+    ("emerge_cuda_closure_enable", c_int, [SIM, c_int, c_uint32]),
+    ("emerge_cuda_closure_stats", c_int, [SIM, POINTER(ClosureStatsC), c_int]),
+    ("emerge_cuda_closure_get_params", c_int, [SIM, c_int, c_void_p, c_void_p]),
+    ("emerge_cuda_closure_get_log", c_int, [SIM, c_int, c_void_p, c_void_p, c_uint64, POINTER(c_uint64)]),
+    ("emerge_cuda_closure_set_params", c_int, [SIM, c_int, c_void_p, c_void_p, c_void_p]),
+    ("emerge_cuda_mlp_loss_grad", c_int, [c_void_p, c_void_p, c_void_p, c_uint32, c_void_p, c_void_p]),
+    ("emerge_cuda_mlp_adam", c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_uint32, c_uint32,
+                                     c_float, c_float, c_float, c_float]),
+    ("emerge_cuda_mlp_infer_bf16", c_int, [c_void_p, c_void_p, c_uint32, c_void_p]),
 ]
 
 _lib = None

@@ -30,8 +30,9 @@ SOURCES = {
     "sort.cu": EXACT,
     "sort_noalloc.cu": EXACT,
     "sim.cu": EXACT,
+    "closure.cu": FAST,
 }
-HEADERS = ["physics.cuh", "device_state.cuh", "kernels.h", "particle_pass.cuh"]
+HEADERS = ["physics.cuh", "device_state.cuh", "kernels.h", "particle_pass.cuh", "closure.cuh", "closure_host.h"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC,-ffp-contract=off"]
 NVCC = os.environ.get("NVCC", "nvcc")

@@ -20,6 +20,7 @@
 #include <cstdint>
 #include <cuda_runtime.h>
 
+#include "closure.cuh"
 #include "physics.cuh"
 
 namespace emerge {
@@ -100,6 +101,7 @@ struct StepLaunch {
     int use_window;     // warp-aggregated P2G reductions
     unsigned model_mask;  // bit m set: ConstitutiveModel m is registered
     int fast;           // fast path (stencil-offset sums with FMA); 0 in the reference-order mode
+    ClosureArgs cl;     // learned closure switches and buffers (fast path only)
     cudaStream_t stream;
 };
 

@@ -22,6 +22,16 @@ __global__ void __launch_bounds__(THREADS, EMERGE_PARTICLE_CTAS_PER_SM) k_partic
     particle_pass<MASK, true>(a);
 }
 
+// The particle pass with the learned closure (or its data logging) for scenes with
+// Drucker-Prager or NACC particles; 2 CTAs per SM leave registers for the network.
+#ifndef EMERGE_CLOSURE_CTAS_PER_SM
+#define EMERGE_CLOSURE_CTAS_PER_SM 2
+#endif
+template <unsigned MASK>
+__global__ void __launch_bounds__(THREADS, EMERGE_CLOSURE_CTAS_PER_SM) k_particle_closure(ParticleKernelArgs a) {
+    particle_pass<MASK, true, true>(a);
+}
+
 // estimate_particle_volumes gather (solver/density.rs:50-71) at the projected
 // positions, stored as rho_dp, plus the stress scatter of fluid particles.
 template <unsigned MASK>
@@ -31,6 +41,14 @@ __global__ void __launch_bounds__(THREADS, EMERGE_DENSITY_CTAS_PER_SM) k_density
 
 void launch_particle_pass_fast(const ParticleKernelArgs &a, unsigned model_mask, cudaStream_t stream) {
     const int grid = blocks_for(a.n, THREADS);
+    const unsigned plastic = (1u << M_DRUCKER_PRAGER) | (1u << M_NACC);
+    if ((a.cl.infer || a.cl.log) && (model_mask & plastic)) {
+        if (covering_mask(model_mask) == MASK_GRANULAR)
+            k_particle_closure<MASK_GRANULAR><<<grid, THREADS, 0, stream>>>(a);
+        else
+            k_particle_closure<ALL_MODELS><<<grid, THREADS, 0, stream>>>(a);
+        return;
+    }
     switch (covering_mask(model_mask)) {
     case MASK_FLUID: k_particle_fast<MASK_FLUID><<<grid, THREADS, 0, stream>>>(a); break;
     case MASK_SOLID: k_particle_fast<MASK_SOLID><<<grid, THREADS, 0, stream>>>(a); break;

@@ -10,6 +10,7 @@
 #include <cfloat>
 #include <climits>
 
+#include "closure.cuh"
 #include "device_state.cuh"
 #include "kernels.h"
 
@@ -476,11 +477,226 @@ struct ParticleKernelArgs {
     int aggregate;      // warp-aggregated P2G reductions
     int project_in;     // recompute the projection of substep k before G2P (fused pipeline)
     int emit_p2g;       // project for substep k+1 and scatter its P2G (fused pipeline)
+    ClosureArgs cl;     // learned closure (kernels instantiated with CLOSURE only)
 };
+
+// ---------------------------------------------------------------- learned closure
+// Per-lane state carried across the warp-level network evaluation.
+struct ClosureWork {
+    M2 u, vt;
+    float2 sigma;      // Drucker-Prager: trial singular values; NACC: singular values of F
+    float x[CL_IN];    // raw network inputs
+    int kind;          // 0: update complete; 1: Drucker-Prager network; 2: NACC network
+    int judge;         // also run the plain mapping and compare stresses
+    int smooth;        // on a smooth plastic branch (network or plain fallback)
+    float scale;       // Drucker-Prager: trial deviatoric norm (unit of the network's strains)
+};
+
+__device__ __forceinline__ uint32_t closure_hash(int i, const StepState *st) {
+    return (static_cast<uint32_t>(i) * 2654435761u) ^ (static_cast<uint32_t>(st->total_substeps) * 40503u);
+}
+
+__device__ __forceinline__ void closure_log(const ClosureArgs &cl, int model, const float (&x)[CL_IN],
+                                            float t0, float t1, float t2) {
+    const unsigned long long k = atomicAdd(&cl.stats->logged[model], 1ull);
+    if (k >= cl.log_cap) return;
+    float *dx = cl.log_x[model] + k * CL_IN;
+#pragma unroll
+    for (int j = 0; j < CL_IN; ++j) dx[j] = x[j];
+    float *dt = cl.log_t[model] + k * CL_OUT;
+    dt[0] = t0;
+    dt[1] = t1;
+    dt[2] = t2;
+}
+
+__device__ __forceinline__ bool closure_in_hull(const ClosureNet &net, const float (&x)[CL_IN]) {
+    bool in = net.ready != 0;
+#pragma unroll
+    for (int j = 0; j < CL_IN; ++j) {
+        const float xn = (x[j] - net.in_shift[j]) * net.in_scale[j];
+        in = in && xn >= net.hull_lo[j] && xn <= net.hull_hi[j];
+    }
+    return in;
+}
+
+// NACC tail of update_particle (nacc.rs:255-269) after the projection.
+__device__ __forceinline__ void nacc_apply(PState &p, M2 nf, float alpha) {
+    p.f = nf;
+    p.lvs = alpha;
+    float j = fmaxf(mdet(nf), MIN_J);
+    float vol = p.v0 * j;
+    p.vol = vol;
+    p.rho = vol > MIN_J ? p.mass / vol : p.rho;
+}
+
+// Phase 1 of the closure update: trial state, exact branch decisions, logging; particles
+// on a smooth plastic branch inside the training box are left for the network.
+template <unsigned MASK>
+__device__ __forceinline__ void closure_prepare(const MatP &m, PState &p, float dt, bool pr,
+                                                const ClosureArgs &cl, uint32_t hash,
+                                                ClosureWork &w) {
+    w.kind = 0;
+    w.judge = 0;
+    w.smooth = 0;
+    const bool dp = HAS_MODEL(MASK, M_DRUCKER_PRAGER) && m.model == M_DRUCKER_PRAGER;
+    const bool nacc = HAS_MODEL(MASK, M_NACC) && m.model == M_NACC;
+    if (dp) {
+        const M2 f_trial = mm(madd(mident(), smscale(dt, p.c)), p.f);
+        svd2(f_trial, w.u, w.sigma, w.vt);
+        const DpTrial t = dp_trial(m, w.sigma, p.lvs, p.q, pr);
+        if (t.dev_norm == 0.0f || t.trace > 0.0f) {  // tip: exact
+            dp_finish(m, p, w.u, w.sigma, w.vt, true, v2(1.0f, 1.0f), t.dev_norm, pr);
+            return;
+        }
+        if (t.gamma <= 0.0f) {  // elastic: exact
+            dp_finish(m, p, w.u, w.sigma, w.vt, false, v2(0.0f, 0.0f), 0.0f, pr);
+            return;
+        }
+        // scale-invariant form: strains in units of the trial deviatoric norm s, so the
+        // network sees O(1) inputs and its error is relative to the plastic correction
+        w.smooth = 1;
+        const float inv_s = 1.0f / t.dev_norm;
+        w.x[0] = t.eps.x * inv_s;
+        w.x[1] = t.eps.y * inv_s;
+        w.x[2] = t.alpha;
+        w.x[3] = t.ratio;
+        w.x[4] = t.cohesion * inv_s;
+        w.x[5] = em_log(t.dev_norm, pr);
+        w.scale = t.dev_norm;
+        float2 h;
+        float dq;
+        if (cl.log && hash % cl.log_stride == 0u) {
+            dp_smooth(t, h, dq);
+            closure_log(cl, 0, w.x, h.x * inv_s, h.y * inv_s, dq * inv_s);
+        }
+        if (cl.infer && closure_in_hull(cl.nets[0], w.x)) {
+            w.kind = 1;
+            w.judge = (hash >> 7) % cl.judge_stride == 0u;
+            return;
+        }
+        dp_smooth(t, h, dq);
+        dp_finish(m, p, w.u, w.sigma, w.vt, true, v2(em_exp(h.x, pr), em_exp(h.y, pr)), dq, pr);
+        return;
+    }
+    if (nacc) {
+        svd2(p.f, w.u, w.sigma, w.vt);
+        const NaccTrial t = nacc_trial(m, w.sigma, p.lvs, pr);
+        if (t.branch != 3) {  // caps and elastic: exact (nacc.rs:129-170)
+            update_particle<MASK>(m, p, dt, pr);
+            return;
+        }
+        const float kappa = nacc_kappa(m);
+        w.smooth = 1;
+        w.x[0] = em_log(fmaxf(w.sigma.x, LOG_CLAMP), pr);
+        w.x[1] = em_log(fmaxf(w.sigma.y, LOG_CLAMP), pr);
+        w.x[2] = t.p0 / kappa;
+        w.x[3] = m.mu / kappa;
+        w.x[4] = m.compression_limit;
+        w.x[5] = m.stretch_limit;
+        float2 sv_new;
+        float a_new;
+        if (cl.log && hash % cl.log_stride == 0u) {
+            nacc_smooth(m, t, p.lvs, sv_new, a_new, pr);
+            closure_log(cl, 1, w.x, em_log(sv_new.x, pr), em_log(sv_new.y, pr), a_new - p.lvs);
+        }
+        if (cl.infer && closure_in_hull(cl.nets[1], w.x)) {
+            w.kind = 2;
+            w.judge = (hash >> 7) % cl.judge_stride == 0u;
+            return;
+        }
+        nacc_smooth(m, t, p.lvs, sv_new, a_new, pr);
+        nacc_apply(p, reconstruct(w.u, sv_new, w.vt), a_new);
+        return;
+    }
+    update_particle<MASK>(m, p, dt, pr);
+}
+
+// Phase 2 (all 32 lanes): network evaluation for the lanes that asked for it.
+template <unsigned MASK>
+__device__ __forceinline__ void closure_evaluate(const ClosureArgs &cl, const ClosureWork &w,
+                                                 float (&y)[CL_OUT]) {
+#pragma unroll
+    for (int net = 0; net < CL_NMODELS; ++net) {
+        if (net == 0 && !HAS_MODEL(MASK, M_DRUCKER_PRAGER)) continue;
+        if (net == 1 && !HAS_MODEL(MASK, M_NACC)) continue;
+        const bool want = w.kind == net + 1;
+        if (!__any_sync(0xffffffffu, want)) continue;
+        const ClosureNet &nn = cl.nets[net];
+        float xn[CL_IN], yn[CL_OUT];
+#pragma unroll
+        for (int j = 0; j < CL_IN; ++j) xn[j] = want ? (w.x[j] - nn.in_shift[j]) * nn.in_scale[j] : 0.0f;
+        closure_warp_infer(nn, want, xn, yn);
+        if (want) {
+#pragma unroll
+            for (int j = 0; j < CL_OUT; ++j) y[j] = yn[j] * nn.out_scale[j] + nn.out_shift[j];
+        }
+    }
+}
+
+// Phase 3: finish the update from the network's outputs; judge sampled particles against
+// the plain mapping (relative error of the principal Kirchhoff stress).
+template <unsigned MASK>
+__device__ __forceinline__ void closure_finish(const MatP &m, PState &p, bool pr, const ClosureWork &w,
+                                               const float (&y)[CL_OUT], float &err) {
+    err = -1.0f;
+    if (w.kind == 1) {
+        const float2 proj = v2(em_exp(y[0] * w.scale, pr), em_exp(y[1] * w.scale, pr));
+        const float dq = fmaxf(y[2] * w.scale, 0.0f);
+        if (w.judge) {
+            const DpTrial t = dp_trial(m, w.sigma, p.lvs, p.q, pr);
+            float2 h;
+            float dq_ref;
+            dp_smooth(t, h, dq_ref);
+            const float2 s_ref = dp_principal_stress(m, v2(em_exp(h.x, pr), em_exp(h.y, pr)));
+            const float2 s_net = dp_principal_stress(m, proj);
+            err = vlen(vsub(s_net, s_ref)) / fmaxf(vlen(s_ref), 1e-6f * m.mu);
+        }
+        dp_finish(m, p, w.u, w.sigma, w.vt, true, proj, dq, pr);
+    } else if (w.kind == 2) {
+        const float2 sv_new = v2(em_exp(y[0], pr), em_exp(y[1], pr));
+        const float a_new = m.hardening_exponent > 0.0f ? p.lvs + y[2] : p.lvs;
+        if (w.judge) {
+            const NaccTrial t = nacc_trial(m, w.sigma, p.lvs, pr);
+            float2 sv_ref;
+            float a_ref;
+            nacc_smooth(m, t, p.lvs, sv_ref, a_ref, pr);
+            const float2 s_ref = nacc_principal_stress(m, sv_ref);
+            const float2 s_net = nacc_principal_stress(m, sv_new);
+            err = vlen(vsub(s_net, s_ref)) / fmaxf(vlen(s_ref), 1e-6f * m.mu);
+        }
+        nacc_apply(p, reconstruct(w.u, sv_new, w.vt), a_new);
+    }
+}
+
+__device__ __forceinline__ void closure_count(const ClosureArgs &cl, int smooth, int net, int fallback,
+                                              float err) {
+    const unsigned full = 0xffffffffu;
+    const int n_smooth = __reduce_add_sync(full, smooth);
+    const int n_net = __reduce_add_sync(full, net);
+    const int n_fb = __reduce_add_sync(full, fallback);
+    const int n_judged = __reduce_add_sync(full, err >= 0.0f ? 1 : 0);
+    float e = err >= 0.0f ? err : 0.0f;
+    float e_sum = e, e_max = e;
+    for (int o = 16; o > 0; o >>= 1) {
+        e_sum += __shfl_xor_sync(full, e_sum, o);
+        e_max = fmaxf(e_max, __shfl_xor_sync(full, e_max, o));
+    }
+    if ((threadIdx.x & 31) == 0 && n_smooth) {
+        ClosureStats *s = cl.stats;
+        atomicAdd(&s->smooth, static_cast<unsigned long long>(n_smooth));
+        if (n_net) atomicAdd(&s->net, static_cast<unsigned long long>(n_net));
+        if (n_fb) atomicAdd(&s->hull_fallback, static_cast<unsigned long long>(n_fb));
+        if (n_judged) {
+            atomicAdd(&s->judged, static_cast<unsigned long long>(n_judged));
+            atomicAdd(&s->err_sum, static_cast<double>(e_sum));
+            atomicMax(&s->err_max_bits, __float_as_uint(e_max));
+        }
+    }
+}
 
 // Body of the particle pass (one particle per thread); the kernels that run it are
 // instantiated in step_kernels.cu (reference-order arithmetic) and fast_kernels.cu.
-template <unsigned MASK, bool FAST>
+template <unsigned MASK, bool FAST, bool CLOSURE = false>
 __device__ __forceinline__ void particle_pass(const ParticleKernelArgs &a) {
     __shared__ MatP s_mats[MAX_MATERIALS];
     __shared__ uint32_t s_max_speed, s_min_mdt, s_warps_done;
@@ -508,10 +724,18 @@ __device__ __forceinline__ void particle_pass(const ParticleKernelArgs &a) {
     float max_speed = 0.0f;
     float min_mdt = INFINITY;
     int clamped = 0, projected = 0, proj_changed = 0;
+    const MatP *mp = &s_mats[0];
+    Saved o;
+    ClosureWork w;
+    if constexpr (CLOSURE) {
+        w.kind = 0;
+        w.smooth = 0;
+        w.judge = 0;
+    }
     if (valid) {
-        const MatP &m = s_mats[p.mat < static_cast<uint32_t>(a.n_mats) ? p.mat : 0u];
+        mp = &s_mats[p.mat < static_cast<uint32_t>(a.n_mats) ? p.mat : 0u];
         if (a.mode_g2p) {
-            const Saved o = save_fields(p);
+            o = save_fields(p);
             // the stored state is the unprojected post-G2P state S''(k): recompute its
             // projection S'(k) (counted when it was first computed)
             if (a.project_in) project_state(cfg, p);
@@ -523,9 +747,25 @@ __device__ __forceinline__ void particle_pass(const ParticleKernelArgs &a) {
                 }
             }
             clamped = g2p_particle<FAST>(a.g, cfg, dt, p);
-            update_particle<MASK>(m, p, dt, pr);
-            store_fields(a.P, i, o, p);
+            if constexpr (CLOSURE)
+                closure_prepare<MASK>(*mp, p, dt, pr, a.cl, closure_hash(i, st), w);
+            else
+                update_particle<MASK>(*mp, p, dt, pr);
         }
+    }
+    if constexpr (CLOSURE) {
+        // learned closure: the network runs for the whole warp (warp-synchronous MMA)
+        float y[CL_OUT] = {0.0f, 0.0f, 0.0f};
+        float err = -1.0f;
+        if (a.mode_g2p) {
+            closure_evaluate<MASK>(a.cl, w, y);
+            if (valid) closure_finish<MASK>(*mp, p, pr, w, y, err);
+            closure_count(a.cl, w.smooth, w.kind != 0 ? 1 : 0, (w.smooth && w.kind == 0 && a.cl.infer) ? 1 : 0, err);
+        }
+    }
+    if (valid) {
+        const MatP &m = *mp;
+        if (a.mode_g2p) store_fields(a.P, i, o, p);
         // CFL contribution for the next substep (step.rs:447-466)
         float sp = vlen(p.v);
         if (cfg.affine_cfl) sp += affine_cfl(p.c, cfg.cell);

@@ -13,6 +13,7 @@
 #include <string>
 #include <vector>
 
+#include "closure_host.h"
 #include "device_state.cuh"
 #include "kernels.h"
 
@@ -163,6 +164,7 @@ struct emerge_sim {
     unsigned long long host_launches = 0;
     unsigned long long graph_launches = 0;
     unsigned long long sorts = 0;
+    ClosureHost *closure = nullptr;  // learned return-mapping closure (closure.cu)
     cudaEvent_t ev[8] = {};
     cudaEvent_t user_ev[16] = {};
     Buffer flushbuf;
@@ -282,6 +284,7 @@ StepLaunch make_launch(emerge_sim *s) {
     L.model_mask = 1u << M_FALLBACK;
     for (const auto &m : s->mats) L.model_mask |= 1u << m.model;
     L.fast = s->deterministic ? 0 : 1;
+    L.cl = closure_args(s->closure);
     L.stream = s->stream;
     return L;
 }
@@ -759,6 +762,13 @@ emerge_status invalidate_pending(emerge_sim *s) {
 namespace emerge {
 // Message returned by emerge_cuda_last_global_error for entry points in other files.
 void set_global_error(const char *msg) { g_global_error = msg; }
+
+cudaStream_t sim_stream(emerge_sim *s) { return s->stream; }
+ClosureHost *&sim_closure(emerge_sim *s) { return s->closure; }
+void sim_invalidate_graph(emerge_sim *s) { s->graph_dirty = true; }
+emerge_status sim_fail(emerge_sim *s, emerge_status st, const std::string &msg) {
+    return static_cast<emerge_status>(s->fail(st, msg));
+}
 }  // namespace emerge
 
 extern "C" {
@@ -867,6 +877,8 @@ emerge_status emerge_cuda_destroy(emerge_sim *s) {
     s->sbuf.reset();
     s->sortbuf.reset();
     s->region_buf.reset();
+    closure_destroy(s->closure);
+    s->closure = nullptr;
     if (s->stream) cudaStreamDestroy(s->stream);
     delete s;
     return EMERGE_OK;

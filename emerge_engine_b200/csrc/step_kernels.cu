@@ -363,6 +363,7 @@ void launch_particle_pass(const StepLaunch &L, const LoadFlagsHost &lfh, int mod
     a.density_mode = L.density_mode;
     a.project_in = project_in;
     a.emit_p2g = emit_p2g;
+    a.cl = L.cl;
     if (L.fast) {
         launch_particle_pass_fast(a, L.model_mask, L.stream);
         return;

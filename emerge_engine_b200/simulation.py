@@ -276,6 +276,60 @@ class Simulation:
         """Read back `n` particles into host memory at address `ptr` (AoS, 128 B each)."""
         self._check(self._lib.emerge_cuda_read_particles(self._sim, c_void_p(ptr), int(n)))
 
+    # ---------------------------------------------------------------- learned closure
+    # No counterpart in the reference: a network standing in for the smooth plastic branch
+    # of the Drucker-Prager (model 0) and NACC (model 1) return mappings.
+    def closure_log(self, capacity: int, stride: int = 1) -> None:
+        """Log (inputs, targets) of the plain mapping during the following steps."""
+        self._check(self._lib.emerge_cuda_closure_log(self._sim, int(capacity), int(stride)))
+
+    def closure_train(self, model: int, epochs: int = 20, batch: int = 4096, lr: float = 2e-3,
+                      lr_decay: float = 0.9, seed: int = 1, val_fraction: float = 0.1,
+                      max_samples: int = 0, beta1: float = 0.9, beta2: float = 0.999,
+                      eps: float = 1e-8) -> dict:
+        cfg = abi.ClosureTrainConfigC(epochs=epochs, batch=batch, lr=lr, lr_decay=lr_decay,
+                                      beta1=beta1, beta2=beta2, eps=eps, val_fraction=val_fraction,
+                                      seed=seed, max_samples=max_samples)
+        rep = abi.ClosureTrainReportC()
+        self._check(self._lib.emerge_cuda_closure_train(self._sim, int(model), byref(cfg), byref(rep)))
+        return {name: getattr(rep, name) for name, _ in abi.ClosureTrainReportC._fields_}
+
+    def closure_enable(self, on: bool = True, judge_stride: int = 64) -> None:
+        self._check(self._lib.emerge_cuda_closure_enable(self._sim, 1 if on else 0, int(judge_stride)))
+
+    def closure_stats(self, reset: bool = False) -> dict:
+        st = abi.ClosureStatsC()
+        self._check(self._lib.emerge_cuda_closure_stats(self._sim, byref(st), 1 if reset else 0))
+        out = {name: getattr(st, name) for name, _ in abi.ClosureStatsC._fields_ if name != "pad_"}
+        out["logged"] = [int(v) for v in st.logged]
+        return out
+
+    def closure_log_samples(self, model: int, max_samples: int = 1 << 20) -> tuple[np.ndarray, np.ndarray]:
+        x = np.zeros((max_samples, 6), np.float32)
+        t = np.zeros((max_samples, 3), np.float32)
+        n = c_uint64()
+        self._check(self._lib.emerge_cuda_closure_get_log(
+            self._sim, int(model), x.ctypes.data_as(c_void_p), t.ctypes.data_as(c_void_p),
+            int(max_samples), byref(n)))
+        return x[:n.value].copy(), t[:n.value].copy()
+
+    def closure_params(self, model: int) -> tuple[np.ndarray, np.ndarray]:
+        params = np.zeros(abi.CLOSURE_NPARAMS, np.float32)
+        norm = np.zeros(abi.CLOSURE_NNORM, np.float32)
+        self._check(self._lib.emerge_cuda_closure_get_params(
+            self._sim, int(model), params.ctypes.data_as(c_void_p), norm.ctypes.data_as(c_void_p)))
+        return params, norm
+
+    def set_closure_params(self, model: int, params: np.ndarray, norm: np.ndarray,
+                           hull: np.ndarray) -> None:
+        p = np.ascontiguousarray(params, np.float32)
+        nm = np.ascontiguousarray(norm, np.float32)
+        h = np.ascontiguousarray(hull, np.float32)
+        assert p.size == abi.CLOSURE_NPARAMS and nm.size == abi.CLOSURE_NNORM and h.size == 12
+        self._check(self._lib.emerge_cuda_closure_set_params(
+            self._sim, int(model), p.ctypes.data_as(c_void_p), nm.ctypes.data_as(c_void_p),
+            h.ctypes.data_as(c_void_p)))
+
 
 class PinnedBuffer:
     """Page-locked host buffer from the CUDA library (cudaMallocHost)."""
@@ -309,3 +363,42 @@ class DeterministicSimulation(Simulation):
     def __init__(self, config: SimConfig, device: int = 0, lib_path: str | None = None,
                  deterministic: bool = True):
         super().__init__(config, device, lib_path, deterministic=True)
+
+
+# ---------------------------------------------------------------- closure test hooks
+def mlp_loss_grad(params: np.ndarray, x: np.ndarray, t: np.ndarray) -> tuple[float, np.ndarray]:
+    """Device loss and gradient of the closure MLP on one batch (normalised data)."""
+    lib = load_library()
+    p = np.ascontiguousarray(params, np.float32)
+    xx = np.ascontiguousarray(x, np.float32)
+    tt = np.ascontiguousarray(t, np.float32)
+    loss = c_float()
+    grad = np.zeros(abi.CLOSURE_NPARAMS, np.float32)
+    check(lib, lib.emerge_cuda_mlp_loss_grad(p.ctypes.data_as(c_void_p), xx.ctypes.data_as(c_void_p),
+                                             tt.ctypes.data_as(c_void_p), len(xx), byref(loss),
+                                             grad.ctypes.data_as(c_void_p)))
+    return float(loss.value), grad
+
+
+def mlp_adam(params, m, v, grad, step, lr, beta1=0.9, beta2=0.999, eps=1e-8):
+    """One device Adam step; returns updated (params, m, v)."""
+    lib = load_library()
+    p = np.array(params, np.float32)
+    mm = np.array(m, np.float32)
+    vv = np.array(v, np.float32)
+    g = np.ascontiguousarray(grad, np.float32)
+    check(lib, lib.emerge_cuda_mlp_adam(p.ctypes.data_as(c_void_p), mm.ctypes.data_as(c_void_p),
+                                        vv.ctypes.data_as(c_void_p), g.ctypes.data_as(c_void_p),
+                                        len(p), int(step), lr, beta1, beta2, eps))
+    return p, mm, vv
+
+
+def mlp_infer_bf16(params: np.ndarray, x: np.ndarray) -> np.ndarray:
+    """The BF16 tensor-core inference of the closure MLP on normalised inputs."""
+    lib = load_library()
+    p = np.ascontiguousarray(params, np.float32)
+    xx = np.ascontiguousarray(x, np.float32)
+    y = np.zeros((len(xx), 3), np.float32)
+    check(lib, lib.emerge_cuda_mlp_infer_bf16(p.ctypes.data_as(c_void_p), xx.ctypes.data_as(c_void_p),
+                                              len(xx), y.ctypes.data_as(c_void_p)))
+    return y

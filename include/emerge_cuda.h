@@ -359,6 +359,78 @@ emerge_status emerge_cuda_stats(emerge_sim *sim, emerge_stats *out);
  * count every kernel node executed, substep loops included). Synchronises. */
 emerge_status emerge_cuda_kernel_launches(emerge_sim *sim, uint64_t *out);
 
+/* ---- learned return-mapping closure (no counterpart in the reference) --------------
+ * A 6 -> 64 -> 64 -> 64 -> 3 SiLU network replaces the smooth plastic branch of the
+ * Drucker-Prager (sand.rs:156-194, model 0) and NACC (nacc.rs:129-223, model 1) return
+ * mappings inside the particle pass, evaluated on the tensor cores in BF16 with FP32
+ * accumulation.  The exact branch decisions (yield test, DP tip, NACC caps) stay exact;
+ * inputs outside the training box use the plain mapping; a hashed sample of network
+ * evaluations (one in judge_stride) is also run through the plain mapping and the relative
+ * error of the principal Kirchhoff stress is recorded.  Workflow: closure_log (run steps with
+ * the plain mapping while logging), closure_train per model, closure_enable. */
+typedef struct emerge_closure_stats {
+    uint64_t smooth;         /* particles that reached a smooth plastic branch */
+    uint64_t net;            /* of which the network evaluated */
+    uint64_t hull_fallback;  /* of which fell outside the training box (plain mapping) */
+    uint64_t judged;         /* network results also computed by the plain mapping */
+    uint64_t logged[2];      /* samples logged per model (capped at the capacity) */
+    double err_mean;         /* mean relative stress error of the judged results */
+    float err_max;           /* max relative stress error of the judged results */
+    uint32_t pad_;
+} emerge_closure_stats;
+
+typedef struct emerge_closure_train_config {
+    uint32_t epochs;
+    uint32_t batch;          /* <= 65536 */
+    float lr;                /* Adam learning rate */
+    float lr_decay;          /* per-epoch factor (0 = none) */
+    float beta1, beta2, eps; /* Adam */
+    float val_fraction;      /* held-out share, seeded split */
+    uint64_t seed;
+    uint64_t max_samples;    /* 0 = all logged */
+} emerge_closure_train_config;
+
+typedef struct emerge_closure_train_report {
+    uint64_t n_train, n_val;
+    float train_loss;        /* MSE of normalised outputs, last epoch */
+    float val_loss;          /* MSE of normalised outputs, held out, tensor-core inference */
+    float val_err_mean, val_err_p50, val_err_p99, val_err_max;  /* relative stress error */
+    float val_err_trial_mean;  /* the same error when the mapping is skipped (trial state kept) */
+    float seconds;
+    uint32_t steps;          /* Adam steps */
+} emerge_closure_train_report;
+
+/* Log (inputs, targets) of the plain mapping on the smooth branches from the following
+ * steps: up to `capacity` samples per model, one evaluation in `stride` (hashed).
+ * capacity 0 stops logging. */
+emerge_status emerge_cuda_closure_log(emerge_sim *sim, uint64_t capacity, uint32_t stride);
+/* Trains the network of `model` (0 Drucker-Prager, 1 NACC) on its logged samples with the
+ * library's own forward, backward and Adam kernels, then installs it. */
+emerge_status emerge_cuda_closure_train(emerge_sim *sim, int model, const emerge_closure_train_config *cfg,
+                                        emerge_closure_train_report *report);
+/* Turns network inference on or off for the following steps. */
+emerge_status emerge_cuda_closure_enable(emerge_sim *sim, int on, uint32_t judge_stride);
+/* Lifetime counters; reset != 0 zeroes them (the logged counts are kept). */
+emerge_status emerge_cuda_closure_stats(emerge_sim *sim, emerge_closure_stats *out, int reset);
+/* FP32 master parameters (8963 floats: W1[6][64] b1 W2[64][64] b2 W3[64][64] b3 W4[64][3] b4)
+ * and normalisation (in_shift[6] in_scale[6] out_shift[3] out_scale[3]) of a network. */
+emerge_status emerge_cuda_closure_get_params(emerge_sim *sim, int model, float *params, float *norm);
+/* Installs a network: parameters, normalisation as above, and the training box of the
+ * normalised inputs (hull_lo[6] hull_hi[6]). */
+emerge_status emerge_cuda_closure_set_params(emerge_sim *sim, int model, const float *params,
+                                             const float *norm, const float *hull);
+/* Copies up to `max` logged samples of `model` (x: max x 6 raw inputs, t: max x 3 targets);
+ * *n receives the number copied. */
+emerge_status emerge_cuda_closure_get_log(emerge_sim *sim, int model, float *x, float *t, uint64_t max,
+                                          uint64_t *n);
+/* Test hooks on host arrays (they allocate device memory): loss and gradient of the MSE
+ * of normalised outputs over a batch; one Adam step; the BF16 tensor-core inference. */
+emerge_status emerge_cuda_mlp_loss_grad(const float *params, const float *x, const float *t, uint32_t batch,
+                                        float *loss, float *grad);
+emerge_status emerge_cuda_mlp_adam(float *params, float *m, float *v, const float *grad, uint32_t n,
+                                   uint32_t step, float lr, float beta1, float beta2, float eps);
+emerge_status emerge_cuda_mlp_infer_bf16(const float *params, const float *x, uint32_t n, float *y);
+
 #ifdef __cplusplus
 }
 #endif

@@ -40,6 +40,9 @@ C_STRUCTS = {
     "emerge_body_state": abi.BodyStateC,
     "emerge_step_timing": abi.StepTimingC,
     "emerge_stats": abi.StatsC,
+    "emerge_closure_stats": abi.ClosureStatsC,
+    "emerge_closure_train_config": abi.ClosureTrainConfigC,
+    "emerge_closure_train_report": abi.ClosureTrainReportC,
 }
 
 

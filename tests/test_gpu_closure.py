@@ -1,0 +1,102 @@
+"""Learned return-mapping closure on the GPU, checked against the CPU oracle
+(oracle/closure_oracle.py): the training kernels' gradients and Adam step, the BF16
+tensor-core inference, the logged (input, target) pairs of the plain Drucker-Prager
+mapping, and an end-to-end run: log -> train -> infer inside the particle pass, with the
+gain over skipping the mapping and the live judge of the network's stress error."""
+import numpy as np
+import pytest
+
+from emerge_engine_b200 import Simulation
+from emerge_engine_b200.simulation import mlp_adam, mlp_infer_bf16, mlp_loss_grad
+from oracle import closure_oracle as co
+from tests import scenes
+
+pytestmark = pytest.mark.gpu
+
+
+def test_device_gradients_match_oracle(cuda_lib):
+    rng = np.random.default_rng(0)
+    p = co.init_params(1)
+    x = rng.normal(size=(300, 6)).astype(np.float32)
+    t = rng.normal(size=(300, 3)).astype(np.float32)
+    loss, g = mlp_loss_grad(p, x, t)
+    loss_o, g_o = co.loss_and_grad(p.astype(np.float64), x.astype(np.float64), t.astype(np.float64))
+    assert loss == pytest.approx(loss_o, rel=1e-6)
+    assert np.max(np.abs(g - g_o)) <= 1e-5 * np.max(np.abs(g_o))
+
+
+def test_device_adam_matches_oracle(cuda_lib):
+    rng = np.random.default_rng(1)
+    p = co.init_params(2)
+    m = rng.normal(size=p.size).astype(np.float32) * 1e-3
+    v = np.abs(rng.normal(size=p.size)).astype(np.float32) * 1e-6
+    g = rng.normal(size=p.size).astype(np.float32) * 1e-2
+    p1, m1, v1 = mlp_adam(p, m, v, g, 7, 1e-3)
+    p2, m2, v2 = co.adam_step(p.astype(np.float64), m, v, g.astype(np.float64), 7, 1e-3)
+    # FP32 with FMA on the device vs float64: compare against each array's scale
+    assert np.max(np.abs(m1 - m2)) <= 1e-6 * np.max(np.abs(m2))
+    assert np.max(np.abs(v1 - v2)) <= 1e-6 * np.max(np.abs(v2))
+    assert np.max(np.abs(p1 - p2)) <= 1e-6
+
+
+def test_tensor_core_inference_matches_bf16_oracle(cuda_lib):
+    rng = np.random.default_rng(2)
+    p = co.init_params(3)
+    x = rng.normal(size=(1001, 6)).astype(np.float32)  # ragged last warp
+    y = mlp_infer_bf16(p, x)
+    y_bf16 = co.forward_bf16(p, x)
+    y_fp32, _ = co.forward(p.astype(np.float64), x.astype(np.float64))
+    scale = np.max(np.abs(y_fp32))
+    assert np.max(np.abs(y - y_bf16)) <= 2e-3 * scale   # same rounding points
+    assert np.max(np.abs(y - y_fp32)) <= 2e-2 * scale   # BF16 vs FP32
+
+
+@pytest.fixture(scope="module")
+def logged_sim(cuda_lib):
+    sim = scenes.mixed_granular(Simulation, grid_res=256, target_particles=120_000)
+    sim.closure_log(2_000_000, 1)
+    for _ in range(3):
+        sim.step()
+    sim.closure_log(0, 1)
+    return sim
+
+
+def test_logged_pairs_are_the_plain_mapping(logged_sim):
+    st = logged_sim.closure_stats()
+    assert st["logged"][0] > 100_000  # Drucker-Prager particles on the smooth plastic branch
+    x, t = logged_sim.closure_log_samples(0, 200_000)
+    ref, on = co.dp_smooth_targets(x)
+    assert on.mean() > 0.999
+    np.testing.assert_allclose(t[on], ref[on], rtol=1e-4, atol=2e-6)
+
+
+def test_trained_closure_gain_and_live_error(logged_sim, cuda_lib):
+    sim = logged_sim
+    rep = sim.closure_train(0, epochs=30, batch=4096, lr=2e-3, lr_decay=0.93, seed=1)
+    print("closure training", rep)
+    # held out, evaluated by the tensor-core inference itself
+    assert rep["val_err_mean"] <= 2e-3
+    assert rep["val_err_p99"] <= 1e-2
+    # what the network gains over the method without it (the trial state kept)
+    assert rep["val_err_trial_mean"] >= 10.0 * rep["val_err_mean"]
+    params, norm = sim.closure_params(0)
+    assert np.all(np.isfinite(params)) and norm[6:12].min() > 0
+
+    ref = scenes.mixed_granular(Simulation, grid_res=256, target_particles=120_000)
+    for _ in range(3):
+        ref.step()
+    sim.closure_enable(True, judge_stride=16)
+    sim.closure_stats(reset=True)
+    for _ in range(2):
+        sim.step()
+        ref.step()
+    st = sim.closure_stats()
+    print("closure live", st)
+    assert st["net"] > 100_000 and st["judged"] > 1000
+    assert st["err_mean"] <= 2e-3
+    for c, r in (((128.0, 128.0), 200.0), ((64.0, 64.0), 40.0)):
+        a, b = sim.region_state(c, r), ref.region_state(c, r)
+        assert abs(a.count - b.count) <= 2
+        for k in ("avg_speed", "avg_det_f", "avg_density"):
+            assert getattr(a, k) == pytest.approx(getattr(b, k), rel=1e-3), k
+    sim.closure_enable(False)
