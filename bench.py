@@ -27,6 +27,8 @@ import sys
 import threading
 import time
 
+import numpy as np
+
 ROOT = os.path.dirname(os.path.abspath(__file__))
 if ROOT not in sys.path:
     sys.path.insert(0, ROOT)
@@ -48,6 +50,12 @@ WORKLOADS = {
                               desc="mixed granular: seeded blocks 16-128 cells, DruckerPrager / "
                                    "Stomakhin snow / NACC, 4 ppc, 1024^2 grid",
                               material="DP+Snow+NACC", grid_res=1024),
+    "batched_256": dict(builder="batched_scenes", kwargs=dict(n_scenes=256),
+                        desc="256 independent scenes in one batch: grid G ~ U{64..256}, target "
+                             "N ~ logU[4k, 200k] particles (clipped to fit the grid), material "
+                             "uniform over {NewtonianFluid, DruckerPrager, Stomakhin snow, "
+                             "NeoHookean}, 4 ppc block on the floor, SlipBoundary(2), dt=0.05",
+                        material="batched", grid_res=0),
 }
 DEFAULT_WORKLOAD = "dam_break_1m"
 
@@ -254,26 +262,41 @@ def build_scene(sim_cls, workload: str, **kw):
     return getattr(scenes, spec["builder"])(sim_cls, **spec["kwargs"], **kw)
 
 
-def cpu_baseline(workload: str, budget_s: float = 15.0) -> dict:
-    """The CPU oracle (reference step restated in C++) on this host, bounded sample."""
-    from oracle.oracle import OracleSimulation, set_threads
-    threads = set_threads(0)
-    sim = build_scene(OracleSimulation, workload)
-    n = sim.particle_count()
-    sim.step()  # warm-up
-    steps = subs = 0
+def _oracle_scenes(workload: str):
+    from oracle.oracle import OracleSimulation
+    sims = build_scene(OracleSimulation, workload)
+    return sims if isinstance(sims, list) else [sims]
+
+
+def _oracle_run(sims, max_steps: int, budget_s: float):
+    """Steps every scene once per round until max_steps rounds or the time budget;
+    returns (rounds, particle-substeps, substeps, seconds)."""
+    units = subs = rounds = 0
     t0 = time.perf_counter()
-    while True:
-        sim.step()
-        steps += 1
-        subs += sim.last_substeps()
+    while rounds < max_steps:
+        for sim in sims:
+            sim.step()
+            k = sim.last_substeps()
+            subs += k
+            units += sim.particle_count() * k
+        rounds += 1
         if time.perf_counter() - t0 >= budget_s:
             break
-    dt = time.perf_counter() - t0
-    return {"value": n * subs / dt, "unit": UNIT, "cores": threads, "kind": "port",
-            "sample": f"{workload}: {steps} full step(s) = {subs} substeps of {n} particles "
-                      f"after 1 warm-up step, {dt:.1f} s (P2G, density and constitutive "
-                      "update sequential as in the reference; G2P gather on all threads)",
+    return rounds, units, subs, time.perf_counter() - t0
+
+
+def cpu_baseline(workload: str, budget_s: float = 15.0) -> dict:
+    """The CPU oracle (reference step restated in C++) on this host, bounded sample."""
+    from oracle.oracle import set_threads
+    threads = set_threads(0)
+    sims = _oracle_scenes(workload)
+    n = sum(s.particle_count() for s in sims)
+    _oracle_run(sims, 1, budget_s)  # warm-up round
+    rounds, units, subs, dt = _oracle_run(sims, 1 << 30, budget_s)
+    return {"value": units / dt, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"{workload}: {rounds} full step(s) of {len(sims)} scene(s), {subs} substeps, "
+                      f"{n} particles, after 1 warm-up step, {dt:.1f} s (P2G, density and "
+                      "constitutive update sequential as in the reference; G2P gather on all threads)",
             "seconds": dt}
 
 
@@ -282,27 +305,15 @@ def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    from oracle.oracle import OracleSimulation, set_threads
+    from oracle.oracle import set_threads
     threads = set_threads(0)
-    sim = build_scene(OracleSimulation, args.workload)
-    n = sim.particle_count()
+    sims = _oracle_scenes(args.workload)
+    n = sum(s.particle_count() for s in sims)
     # Bounded sample: warm-up and timed steps each stop early once their time budget is
     # spent, so the run ends within a few minutes whatever the workload.
-    t0 = time.perf_counter()
-    for _ in range(args.warmup):
-        sim.step()
-        if time.perf_counter() - t0 >= args.ref_warmup_budget:
-            break
-    subs = steps = 0
-    t0 = time.perf_counter()
-    for _ in range(args.steps):
-        sim.step()
-        steps += 1
-        subs += sim.last_substeps()
-        if time.perf_counter() - t0 >= args.ref_budget:
-            break
-    dt = time.perf_counter() - t0
-    value = n * subs / dt
+    _oracle_run(sims, args.warmup, args.ref_warmup_budget)
+    steps, units, subs, dt = _oracle_run(sims, args.steps, args.ref_budget)
+    value = units / dt
     spec = WORKLOADS[args.workload]
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT,
@@ -311,13 +322,57 @@ def run_reference(args):
         "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic (seeded scene generator, tests/scenes.py)",
         "config": {"workload": args.workload, "description": spec["desc"], "particles": n,
-                   "grid": spec["grid_res"], "substeps": subs},
+                   "scenes": len(sims), "grid": spec["grid_res"], "substeps": subs},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
                          "sample": f"{steps} of {args.steps} full steps ({subs} substeps) of {n} "
-                                   f"particles, {dt:.1f} s (time budget {args.ref_budget:.0f} s)"},
+                                   f"particles in {len(sims)} scene(s), {dt:.1f} s (time budget "
+                                   f"{args.ref_budget:.0f} s)"},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
+
+
+def run_batched(args, spec, rank: int, world: int, dist, local_rank: int) -> dict:
+    """Batched scenes: all scenes of the workload advanced together (one launch per kernel
+    per substep); value = sum over scenes of particles x substeps per second.  Weak scaling:
+    every rank advances its own scenes (seeded per rank)."""
+    from emerge_engine_b200 import Batch, Simulation
+    from emerge_engine_b200.build import build
+    build()
+    sims = build_scene(Simulation, args.workload, device=local_rank, seed=7 + rank)
+    counts = np.array([s.particle_count() for s in sims], dtype=np.int64)
+    batch = Batch(sims)
+    for s in sims:
+        s.close()
+    del sims
+    tune = batch.autotune(steps_per_trial=1) if not args.no_extras else None
+    batch.step(args.warmup)
+    clocks = ClockSampler(local_rank)
+    clocks.start()
+    t_load = time.perf_counter()
+    _, tot0 = batch.substeps()
+    t_begin = time.perf_counter()
+    total_ms = batch.time_steps(args.steps, flush_l2=True)
+    clock_info = clocks.stop(t_begin, time.perf_counter(), t_load)
+    _, tot1 = batch.substeps()
+    units = float(np.sum(counts * (tot1 - tot0).astype(np.int64)))
+    if dist is not None:
+        total_ms, units, _ = reduce_over_ranks(dist, f"cuda:{local_rank}", total_ms, units, 0)
+    value = units / (total_ms / 1000.0)
+    peak, peak_kind = load_peaks()
+    ppc = 4.0
+    b_alg = 156.0 + 24.0 / ppc + 8.0 / ppc  # per particle-substep (fluid scenes add the mass field)
+    achieved = b_alg * value / 1e9
+    out = {"value": value, "ms_per_step": total_ms / args.steps, "clocks": clock_info,
+           "scenes": int(len(counts)), "particles": int(counts.sum()),
+           "substeps_per_step_mean": float(np.mean(tot1 - tot0)) / args.steps,
+           "roofline": {"kernel": "whole substep, all scenes (B_alg = 156 + 32/ppc B per "
+                                  "particle-substep)", "bound": "hbm", "achieved": achieved,
+                        "peak": peak, "unit": "GB/s", "frac": achieved / peak, "traffic": None,
+                        "peak_source": f"{peak_kind} hbm_gbs (MEASURED_PEAKS.json)"},
+           "autotune": tune}
+    batch.close()
+    return out
 
 
 def main():
@@ -355,12 +410,34 @@ def main():
         dist_mod.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
         dist = dist_mod
 
+    spec = WORKLOADS[args.workload]
+    if spec["material"] == "batched":
+        r = run_batched(args, spec, rank, world, dist, local_rank)
+        if rank == 0:
+            line = {
+                "metric": METRIC, "value": r["value"], "unit": UNIT, "n_gpus": world,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": r["ms_per_step"],
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+                "data": "synthetic (seeded scene generator, tests/scenes.py)",
+                "config": {"workload": args.workload, "description": spec["desc"],
+                           "scenes": r["scenes"], "particles_per_gpu": r["particles"],
+                           "substeps_per_step_mean": r["substeps_per_step_mean"],
+                           "l2": "flushed (512 MiB write) before every timed step",
+                           "parallelism": f"replicas x{world}"},
+                "clocks": r["clocks"], "roofline": r["roofline"], "autotune": r["autotune"],
+            }
+            if world == 1 and not args.no_extras:
+                line["cpu_baseline"] = cpu_baseline(args.workload, args.cpu_budget)
+            print(json.dumps(line), flush=True)
+        if dist is not None:
+            dist.destroy_process_group()
+        return
+
     from emerge_engine_b200 import Simulation
     from emerge_engine_b200.abi import OPT_USE_GRAPH
     from emerge_engine_b200.build import build
     build()
 
-    spec = WORKLOADS[args.workload]
     sim = build_scene(Simulation, args.workload, device=local_rank)
     n = sim.particle_count()
     clocks = ClockSampler(local_rank)

@@ -7,4 +7,4 @@ from .config import BodyState, SimConfig, SlipBoundary, SpawnRegion  # noqa: F40
 from .materials import (DruckerPragerMaterial, FallbackMaterial, NaccMaterial,  # noqa: F401
                         NeoHookeanMaterial, NewtonianFluidMaterial, StomakhinMaterial,
                         lame_from_young, to_radians)
-from .simulation import DeterministicSimulation, MaterialRegistry, Simulation  # noqa: F401
+from .simulation import Batch, DeterministicSimulation, MaterialRegistry, Simulation  # noqa: F401

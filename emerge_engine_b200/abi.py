@@ -163,6 +163,13 @@ class ClosureTrainReportC(Structure):
                 ("steps", c_uint32)]
 
 
+class BatchTuneReportC(Structure):
+    """`emerge_batch_tune_report` (include/emerge_cuda.h)."""
+    _fields_ = [("sort_interval", ctypes.c_int32), ("aggregate", ctypes.c_int32), ("n_trials", c_uint32),
+                ("trial_sort_interval", ctypes.c_int32 * 8), ("trial_aggregate", ctypes.c_int32 * 8),
+                ("trial_ms", c_float * 8)]
+
+
 CLOSURE_NPARAMS = 8963  # W1[6][64] b1 W2[64][64] b2 W3[64][64] b3 W4[64][3] b4
 CLOSURE_NNORM = 18      # in_shift[6] in_scale[6] out_shift[3] out_scale[3]
 
@@ -213,6 +220,19 @@ ABI_FUNCTIONS = [
     ("emerge_cuda_mlp_adam", c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_uint32, c_uint32,
                                      c_float, c_float, c_float, c_float]),
     ("emerge_cuda_mlp_infer_bf16", c_int, [c_void_p, c_void_p, c_uint32, c_void_p]),
+    ("emerge_cuda_batch_create", c_int, [POINTER(c_void_p), c_uint32, POINTER(c_void_p)]),
+    ("emerge_cuda_batch_destroy", c_int, [c_void_p]),
+    ("emerge_cuda_batch_last_error", c_char_p, [c_void_p]),
+    ("emerge_cuda_batch_step", c_int, [c_void_p, c_uint32]),
+    ("emerge_cuda_batch_time_steps", c_int, [c_void_p, c_uint32, c_int, POINTER(c_float)]),
+    ("emerge_cuda_batch_scene_count", c_int, [c_void_p, POINTER(c_uint32)]),
+    ("emerge_cuda_batch_particle_count", c_int, [c_void_p, c_uint32, POINTER(c_uint64)]),
+    ("emerge_cuda_batch_read_particles", c_int, [c_void_p, c_uint32, c_void_p, c_uint64]),
+    ("emerge_cuda_batch_region_state", c_int, [c_void_p, c_uint32, c_float, c_float, c_float,
+                                               POINTER(BodyStateC)]),
+    ("emerge_cuda_batch_substeps", c_int, [c_void_p, c_void_p, c_void_p]),
+    ("emerge_cuda_batch_set_option", c_int, [c_void_p, c_int, c_int64]),
+    ("emerge_cuda_batch_autotune", c_int, [c_void_p, c_uint32, POINTER(BatchTuneReportC)]),
 ]
 
 _lib = None

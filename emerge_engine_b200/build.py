@@ -31,6 +31,7 @@ SOURCES = {
     "sort_noalloc.cu": EXACT,
     "sim.cu": EXACT,
     "closure.cu": FAST,
+    "batch.cu": EXACT,
 }
 HEADERS = ["physics.cuh", "device_state.cuh", "kernels.h", "particle_pass.cuh", "closure.cuh", "closure_host.h"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]

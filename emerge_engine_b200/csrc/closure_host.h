@@ -3,9 +3,11 @@
 #pragma once
 
 #include <string>
+#include <vector>
 
 #include "../../include/emerge_cuda.h"
 #include "closure.cuh"
+#include "kernels.h"
 
 namespace emerge {
 
@@ -14,6 +16,22 @@ struct ClosureHost;  // closure.cu: networks, statistics, log buffers, master we
 // Kernel arguments of the closure (all zero when the simulation has none).
 ClosureArgs closure_args(const ClosureHost *c);
 void closure_destroy(ClosureHost *c);
+
+// sim.cu: a simulation's scene description, for building batches (batch.cu).
+struct SimView {
+    emerge_sim_config cfg;
+    std::vector<uint64_t> bounds;
+    std::vector<emerge_material_params> mats;
+    LoadFlagsHost lf;
+    DevConfig dcfg;
+    int deterministic;
+    size_t n;
+    int device;
+};
+SimView sim_view(emerge_sim *s);
+// Byte size of, and carving of, one particle set of capacity `cap` (256-byte pieces).
+size_t particle_set_size(size_t cap);
+DevParticles particle_set_carve(void *base, size_t cap);
 
 // sim.cu: the pieces of a simulation the closure manager uses.
 cudaStream_t sim_stream(emerge_sim *s);

@@ -70,6 +70,8 @@ struct StepState {
     unsigned long long graph_kernels;      // kernels executed inside step graphs
     uint32_t error_flags;
     uint32_t upload_flags;      // k_check_aos: bit 0 contact_group != 0, bit 1 pinned
+    uint32_t active;            // batches: the scene takes part in the running substep
+    uint32_t pad_;
 };
 
 struct GridView {
@@ -87,6 +89,34 @@ __host__ __device__ __forceinline__ int cell_index(int x, int y, int tpd) {
 __host__ __device__ __forceinline__ bool in_domain(int x, int y, int res) {
     return x >= 0 && y >= 0 && x < res && y < res;
 }
+
+// Threads (particles) per CTA of the particle and density passes.
+constexpr int PARTICLE_THREADS = 256;
+
+// One scene of a batch (device memory).  Its particles occupy slots [p0, p0 + n) of the
+// batch's particle arrays (p0 a multiple of the particle-pass CTA size), its particle-pass
+// CTAs are block0 .. block0 + ceil(n / CTA) - 1, its grid tiles tile0 .. tile0 + tpd^2 - 1.
+struct SceneDesc {
+    DevConfig cfg;
+    GridView g;
+    StepState *st;
+    const emerge_material_params *mats;
+    int n_mats;
+    int p0;
+    int n;
+    int block0;
+    int tile0;
+    int density_mode;
+};
+
+// Scene lookup tables of a batch, passed to the batched kernels.
+struct BatchView {
+    const SceneDesc *scenes;
+    const uint16_t *block_scene;  // particle-pass CTA -> scene
+    const uint16_t *tile_scene;   // global grid tile -> scene
+    int n_scenes;
+    int check_active;             // skip scenes whose frame has ended
+};
 
 // Host-side handles of the step kernels (implemented in step_kernels.cu).
 struct StepLaunch {

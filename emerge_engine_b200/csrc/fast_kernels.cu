@@ -5,6 +5,8 @@
 // only in float rounding (summation order of the L2 reductions, FMA, 2-ulp division and
 // square root).  The reference-order mode runs the exact instantiation in step_kernels.cu.
 #define EMERGE_FAST_TU 1  // em_pow: integer exponents by repeated multiplication
+#include <cstring>
+
 #include "particle_pass.cuh"
 
 // Resident CTAs per SM the register allocation is sized for (256 threads each).
@@ -37,6 +39,48 @@ __global__ void __launch_bounds__(THREADS, EMERGE_CLOSURE_CTAS_PER_SM) k_particl
 template <unsigned MASK>
 __global__ void __launch_bounds__(THREADS, EMERGE_DENSITY_CTAS_PER_SM) k_density(DensityKernelArgs a) {
     density_pass<MASK>(a);
+}
+
+// Batched scenes: every CTA finds its scene in the batch's tables; all model sets.
+template <unsigned MASK>
+__global__ void __launch_bounds__(THREADS, EMERGE_PARTICLE_CTAS_PER_SM) k_particle_batch(ParticleKernelArgs a) {
+    particle_pass<MASK, true, false, true>(a);
+}
+template <unsigned MASK>
+__global__ void __launch_bounds__(THREADS, EMERGE_DENSITY_CTAS_PER_SM) k_density_batch(DensityKernelArgs a) {
+    density_pass<MASK, true>(a);
+}
+
+void launch_particle_pass_batch(const DevParticles &P, const BatchView &b, int n_blocks,
+                                const LoadFlagsHost &lf, int mode_g2p, int emit_p2g, int aggregate,
+                                cudaStream_t stream) {
+    if (n_blocks <= 0) return;
+    ParticleKernelArgs a;
+    std::memset(&a, 0, sizeof(a));
+    a.P = P;
+    a.lf.temperature = lf.temperature;
+    a.lf.activation = lf.activation;
+    a.lf.pinned = lf.pinned;
+    a.mode_g2p = mode_g2p;
+    a.project_in = mode_g2p;  // recompute the stored state's projection (where the scene projects)
+    a.emit_p2g = emit_p2g;
+    a.aggregate = aggregate;
+    a.batch = b;
+    k_particle_batch<ALL_MODELS><<<n_blocks, THREADS, 0, stream>>>(a);
+}
+
+void launch_density_pass_batch(const DevParticles &P, const BatchView &b, int n_blocks,
+                               const LoadFlagsHost &lf, int aggregate, cudaStream_t stream) {
+    if (n_blocks <= 0) return;
+    DensityKernelArgs a;
+    std::memset(&a, 0, sizeof(a));
+    a.P = P;
+    a.lf.temperature = lf.temperature;
+    a.lf.activation = lf.activation;
+    a.lf.pinned = lf.pinned;
+    a.aggregate = aggregate;
+    a.batch = b;
+    k_density_batch<ALL_MODELS><<<n_blocks, THREADS, 0, stream>>>(a);
 }
 
 void launch_particle_pass_fast(const ParticleKernelArgs &a, unsigned model_mask, cudaStream_t stream) {

@@ -40,6 +40,20 @@ void launch_mass_scatter(const DevParticles &P, int n, const GridView &g, int fi
 void launch_mass_gather(const DevParticles &P, int lo, int hi, const GridView &g, int write_initial,
                         cudaStream_t stream);
 
+// batched scenes (step_kernels.cu: grid update and controller; fast_kernels.cu: passes)
+void launch_grid_update_batch(const BatchView &b, int n_tiles, cudaStream_t stream);
+void launch_step_begin_batch(const BatchView &b, StepState *batch_st, cudaStream_t stream);
+void launch_substep_begin_batch(const BatchView &b, StepState *batch_st, int use_cond,
+                                unsigned long long handle, int kernels_per_substep, cudaStream_t stream);
+void launch_prime_setup_batch(const BatchView &b, cudaStream_t stream);
+// particle pass (mode_g2p, emit_p2g as launch_particle_pass) and density pass over all
+// CTAs of a batch; lf: union of the scenes' load flags
+void launch_particle_pass_batch(const DevParticles &P, const BatchView &b, int n_blocks,
+                                const LoadFlagsHost &lf, int mode_g2p, int emit_p2g, int aggregate,
+                                cudaStream_t stream);
+void launch_density_pass_batch(const DevParticles &P, const BatchView &b, int n_blocks,
+                               const LoadFlagsHost &lf, int aggregate, cudaStream_t stream);
+
 // det_kernels.cu (reference-order mode)
 void launch_project(const StepLaunch &L);
 void launch_det_records(const StepLaunch &L, int mode, uint32_t invalid_key, uint32_t *keys,
@@ -67,6 +81,15 @@ void launch_sort_keys(const float2 *x, int n, int res, int key_mode, uint32_t *k
 int sort_key_bits(int res, int key_mode);
 // Sorts (keys[0], vals[0]) stably by key; result lands in (keys[r], vals[r]), r returned.
 int radix_sort_pairs(SortScratch &s, int n, int key_bits, cudaStream_t stream);
+// Batched scenes: keys (scene << 20 | tile key) of the compact particle list and the
+// permutation back into each scene's slot range.
+int batch_sort_key_bits(int n_scenes);
+void launch_batch_sort_keys(const SceneDesc *scenes, const int *compact_start, int n_scenes,
+                            const DevParticles &P, int total, uint32_t *keys, uint32_t *vals,
+                            cudaStream_t stream);
+void launch_permute_batch(const DevParticles &src, const DevParticles &dst, const uint32_t *keys,
+                          const uint32_t *vals, const SceneDesc *scenes, const int *compact_start, int total,
+                          cudaStream_t stream);
 // dst[j] = src[perm[j]] for every particle array.
 void launch_permute(const DevParticles &src, const DevParticles &dst, const uint32_t *perm, int n,
                     cudaStream_t stream);

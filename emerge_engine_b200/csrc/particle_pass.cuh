@@ -279,7 +279,7 @@ constexpr unsigned MASK_GRANULAR =
 // after the tile sort) sum their contributions with a segmented shuffle reduction
 // and the segment's first lane issues one reduction per cell.  Tile flags for the
 // grid update are set once per particle (its stencil spans at most 2 x 2 tiles).
-constexpr int THREADS = 256;
+constexpr int THREADS = PARTICLE_THREADS;
 
 struct Payload {
     float2 x;
@@ -478,7 +478,20 @@ struct ParticleKernelArgs {
     int project_in;     // recompute the projection of substep k before G2P (fused pipeline)
     int emit_p2g;       // project for substep k+1 and scatter its P2G (fused pipeline)
     ClosureArgs cl;     // learned closure (kernels instantiated with CLOSURE only)
+    BatchView batch;    // batched scenes (kernels instantiated with BATCH only)
 };
+
+// Scene of this CTA in a batch (nullptr for single-scene kernels); false when the scene
+// does not take part in the running substep (the whole CTA returns).
+template <bool BATCH, class Args>
+__device__ __forceinline__ bool batch_scene(const Args &a, const SceneDesc *&sd) {
+    sd = nullptr;
+    if constexpr (BATCH) {
+        sd = &a.batch.scenes[a.batch.block_scene[blockIdx.x]];
+        if (a.batch.check_active && !sd->st->active) return false;
+    }
+    return true;
+}
 
 // ---------------------------------------------------------------- learned closure
 // Per-lane state carried across the warp-level network evaluation.
@@ -696,21 +709,29 @@ __device__ __forceinline__ void closure_count(const ClosureArgs &cl, int smooth,
 
 // Body of the particle pass (one particle per thread); the kernels that run it are
 // instantiated in step_kernels.cu (reference-order arithmetic) and fast_kernels.cu.
-template <unsigned MASK, bool FAST, bool CLOSURE = false>
+template <unsigned MASK, bool FAST, bool CLOSURE = false, bool BATCH = false>
 __device__ __forceinline__ void particle_pass(const ParticleKernelArgs &a) {
     __shared__ MatP s_mats[MAX_MATERIALS];
     __shared__ uint32_t s_max_speed, s_min_mdt, s_warps_done;
-    for (int k = threadIdx.x; k < a.n_mats; k += THREADS) s_mats[k] = a.mats[k];
+    const SceneDesc *sd;
+    if (!batch_scene<BATCH>(a, sd)) return;
+    // this CTA's scene: the kernel arguments, or the batch's scene table
+    const DevConfig &cfg = [&]() -> const DevConfig & { if constexpr (BATCH) return sd->cfg; else return a.cfg; }();
+    const GridView &g = [&]() -> const GridView & { if constexpr (BATCH) return sd->g; else return a.g; }();
+    const MatP *mats = BATCH ? sd->mats : a.mats;
+    const int n_mats = BATCH ? sd->n_mats : a.n_mats;
+    const int density_mode = BATCH ? sd->density_mode : a.density_mode;
+    StepState *st = BATCH ? sd->st : a.st;
+    const int i = BATCH ? sd->p0 + (static_cast<int>(blockIdx.x) - sd->block0) * THREADS + static_cast<int>(threadIdx.x)
+                        : static_cast<int>(blockIdx.x) * THREADS + static_cast<int>(threadIdx.x);
+    const bool valid = BATCH ? i < sd->p0 + sd->n : i < a.n;
+    for (int k = threadIdx.x; k < n_mats; k += THREADS) s_mats[k] = mats[k];
     if (threadIdx.x == 0) {
         s_max_speed = 0u;            // bits of 0.0f
         s_min_mdt = 0x7f800000u;     // bits of +inf
         s_warps_done = 0u;
     }
-    const DevConfig &cfg = a.cfg;
     const bool pr = cfg.precise_math != 0;
-    StepState *st = a.st;
-    const int i = blockIdx.x * THREADS + threadIdx.x;
-    const bool valid = i < a.n;
     // The particle's state loads and the controller reads are issued together before the
     // barrier that publishes the materials, so their latencies overlap.
     const uint32_t acc_slot = st->acc_slot;
@@ -733,20 +754,20 @@ __device__ __forceinline__ void particle_pass(const ParticleKernelArgs &a) {
         w.judge = 0;
     }
     if (valid) {
-        mp = &s_mats[p.mat < static_cast<uint32_t>(a.n_mats) ? p.mat : 0u];
+        mp = &s_mats[p.mat < static_cast<uint32_t>(n_mats) ? p.mat : 0u];
         if (a.mode_g2p) {
             o = save_fields(p);
             // the stored state is the unprojected post-G2P state S''(k): recompute its
             // projection S'(k) (counted when it was first computed)
-            if (a.project_in) project_state(cfg, p);
-            if (a.density_mode && a.project_in) {
+            if (a.project_in && cfg.project) project_state(cfg, p);
+            if (density_mode && a.project_in) {
                 float d = a.P.rho_dp[i];
                 if (d > F32_EPS) {
                     p.rho = d;
                     p.vol = p.mass / d;
                 }
             }
-            clamped = g2p_particle<FAST>(a.g, cfg, dt, p);
+            clamped = g2p_particle<FAST>(g, cfg, dt, p);
             if constexpr (CLOSURE)
                 closure_prepare<MASK>(*mp, p, dt, pr, a.cl, closure_hash(i, st), w);
             else
@@ -784,7 +805,7 @@ __device__ __forceinline__ void particle_pass(const ParticleKernelArgs &a) {
             pl.v = p.v;
             pl.c = p.c;
             pl.do_ma = true;
-            if (!(a.density_mode && m.model == M_FLUID)) {
+            if (!(density_mode && m.model == M_FLUID)) {
                 pl.tau = combined_kirchhoff_stress<MASK>(m, p, pr);
                 pl.s = -stress_volume(m, p) * KERNEL_D_INVERSE;
                 pl.do_s = true;
@@ -809,10 +830,10 @@ __device__ __forceinline__ void particle_pass(const ParticleKernelArgs &a) {
             atomicAdd(&st->window_blocks, 1ull);
         }
     }
-    if (MASK == MASK_FLUID && a.density_mode)
-        scatter_particle<SC_MA>(a.g, pl, valid, a.aggregate);
+    if (MASK == MASK_FLUID && density_mode)
+        scatter_particle<SC_MA>(g, pl, valid, a.aggregate);
     else
-        scatter_particle<SC_BOTH>(a.g, pl, valid, a.aggregate);
+        scatter_particle<SC_BOTH>(g, pl, valid, a.aggregate);
 }
 
 // ---------------------------------------------------------------- k_density
@@ -847,24 +868,33 @@ struct DensityKernelArgs {
     GridView g;
     LoadFlags lf;
     int aggregate;
+    BatchView batch;    // batched scenes (kernels instantiated with BATCH only)
 };
 
 // estimate_particle_volumes gather (solver/density.rs:50-71) at the projected
 // positions, stored as rho_dp, plus the stress scatter of fluid particles.
-template <unsigned MASK>
+template <unsigned MASK, bool BATCH = false>
 __device__ __forceinline__ void density_pass(const DensityKernelArgs &a) {
     __shared__ MatP s_mats[MAX_MATERIALS];
-    for (int k = threadIdx.x; k < a.n_mats; k += THREADS) s_mats[k] = a.mats[k];
-    const DevConfig &cfg = a.cfg;
+    const SceneDesc *sd;
+    if (!batch_scene<BATCH>(a, sd)) return;
+    if (BATCH && !sd->density_mode) return;  // no material of the scene needs the pass
+    const DevConfig &cfg = [&]() -> const DevConfig & { if constexpr (BATCH) return sd->cfg; else return a.cfg; }();
+    const GridView &g = [&]() -> const GridView & { if constexpr (BATCH) return sd->g; else return a.g; }();
+    const MatP *mats = BATCH ? sd->mats : a.mats;
+    const int n_mats = BATCH ? sd->n_mats : a.n_mats;
+    StepState *st = BATCH ? sd->st : a.st;
+    const int i = BATCH ? sd->p0 + (static_cast<int>(blockIdx.x) - sd->block0) * THREADS + static_cast<int>(threadIdx.x)
+                        : static_cast<int>(blockIdx.x) * THREADS + static_cast<int>(threadIdx.x);
+    const bool valid = BATCH ? i < sd->p0 + sd->n : i < a.n;
+    for (int k = threadIdx.x; k < n_mats; k += THREADS) s_mats[k] = mats[k];
     const bool pr = cfg.precise_math != 0;
-    const int i = blockIdx.x * THREADS + threadIdx.x;
-    const bool valid = i < a.n;
     // Positions at the projected state S'(k): the stored state itself unless the particle
     // pass's projection changed some particle, in which case the full state is loaded and
     // projected again.  Otherwise only what the density gather and the fluid stress read
     // is loaded.
-    const uint32_t acc_slot = a.st->acc_slot;
-    const unsigned long long changed0 = a.st->proj_changed[0], changed1 = a.st->proj_changed[1];
+    const uint32_t acc_slot = st->acc_slot;
+    const unsigned long long changed0 = st->proj_changed[0], changed1 = st->proj_changed[1];
     PState p;
     if (valid) {
         p.x = a.P.x[i];
@@ -881,10 +911,10 @@ __device__ __forceinline__ void density_pass(const DensityKernelArgs &a) {
             project_state(cfg, p);
         }
         const QW w = quadratic_weights(p.x);
-        const bool inside = stencil_inside(w.bx, w.by, a.g.res);
-        const float density = inside ? gather_density<false>(a.g, w) : gather_density<true>(a.g, w);
+        const bool inside = stencil_inside(w.bx, w.by, g.res);
+        const float density = inside ? gather_density<false>(g, w) : gather_density<true>(g, w);
         a.P.rho_dp[i] = density;
-        const MatP &m = s_mats[p.mat < static_cast<uint32_t>(a.n_mats) ? p.mat : 0u];
+        const MatP &m = s_mats[p.mat < static_cast<uint32_t>(n_mats) ? p.mat : 0u];
         if (m.model == M_FLUID) {
             if (!reproject) {  // the fields the fluid stress reads (fluid.rs:135-195)
                 p.c = m_from4(a.P.c[i]);
@@ -908,7 +938,7 @@ __device__ __forceinline__ void density_pass(const DensityKernelArgs &a) {
             pl.do_s = true;
         }
     }
-    scatter_particle<SC_S>(a.g, pl, valid, a.aggregate);
+    scatter_particle<SC_S>(g, pl, valid, a.aggregate);
 }
 
 // Launchers of the fast path's kernels (fast_kernels.cu).

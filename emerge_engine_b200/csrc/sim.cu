@@ -764,6 +764,26 @@ namespace emerge {
 void set_global_error(const char *msg) { g_global_error = msg; }
 
 cudaStream_t sim_stream(emerge_sim *s) { return s->stream; }
+
+SimView sim_view(emerge_sim *s) {
+    SimView v;
+    v.cfg = s->cfg;
+    v.bounds = s->bounds;
+    v.mats = s->mats;
+    v.lf = s->lf;
+    v.dcfg = s->dcfg;
+    v.deterministic = s->deterministic;
+    v.n = s->n;
+    v.device = s->device;
+    return v;
+}
+
+size_t particle_set_size(size_t cap) { return particle_set_bytes(cap); }
+
+DevParticles particle_set_carve(void *base, size_t cap) {
+    Carver c(base);
+    return carve_particles(c, cap);
+}
 ClosureHost *&sim_closure(emerge_sim *s) { return s->closure; }
 void sim_invalidate_graph(emerge_sim *s) { s->graph_dirty = true; }
 emerge_status sim_fail(emerge_sim *s, emerge_status st, const std::string &msg) {

@@ -258,10 +258,8 @@ int radix_sort_pairs(SortScratch &s, int n, int key_bits, cudaStream_t stream) {
     return cur;
 }
 
-__global__ void k_permute(DevParticles src, DevParticles dst, const uint32_t *perm, int n) {
-    int j = blockIdx.x * blockDim.x + threadIdx.x;
-    if (j >= n) return;
-    uint32_t i = perm[j];
+// dst slot j <- src slot i, every particle array.
+__device__ __forceinline__ void copy_slot(const DevParticles &src, uint32_t i, const DevParticles &dst, int j) {
     dst.x[j] = src.x[i];
     dst.v[j] = src.v[i];
     dst.c[j] = src.c[i];
@@ -286,6 +284,74 @@ __global__ void k_permute(DevParticles src, DevParticles dst, const uint32_t *pe
     dst.scalar[j] = src.scalar[i];
     dst.slot_to_index[j] = src.slot_to_index[i];
     dst.rho_dp[j] = src.rho_dp[i];
+}
+
+__global__ void k_permute(DevParticles src, DevParticles dst, const uint32_t *perm, int n) {
+    int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= n) return;
+    copy_slot(src, perm[j], dst, j);
+}
+
+// ---- batched scenes: one sort over all scenes, scene index in the key's high bits ----
+constexpr int BATCH_TILE_KEY_BITS = 20;  // grids up to 1024^2 (128^2 tiles)
+
+// Scene of compact particle index c: compact_start[s] <= c < compact_start[s + 1].
+__device__ __forceinline__ int scene_of(const int *compact_start, int n_scenes, int c) {
+    int lo = 0, hi = n_scenes - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (compact_start[mid] <= c) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+
+__global__ void k_batch_sort_keys(const SceneDesc *scenes, const int *compact_start, int n_scenes,
+                                  DevParticles P, int total, uint32_t *keys, uint32_t *vals) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= total) return;
+    const int s = scene_of(compact_start, n_scenes, c);
+    const SceneDesc &sd = scenes[s];
+    const int slot = sd.p0 + (c - compact_start[s]);
+    const float2 p = P.x[slot];
+    const int res = sd.g.res;
+    const float fx = fminf(fmaxf(floorf(p.x), 0.0f), static_cast<float>(res - 1));
+    const float fy = fminf(fmaxf(floorf(p.y), 0.0f), static_cast<float>(res - 1));
+    const uint32_t cx = static_cast<uint32_t>(fx), cy = static_cast<uint32_t>(fy);
+    keys[c] = (static_cast<uint32_t>(s) << BATCH_TILE_KEY_BITS) |
+              (morton2(cx >> 3, cy >> 3) << 6) | ((cx & 7u) << 3) | (cy & 7u);
+    vals[c] = static_cast<uint32_t>(slot);
+}
+
+__global__ void k_permute_batch(DevParticles src, DevParticles dst, const uint32_t *keys,
+                                const uint32_t *vals, const SceneDesc *scenes, const int *compact_start,
+                                int total) {
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= total) return;
+    const int s = static_cast<int>(keys[j] >> BATCH_TILE_KEY_BITS);
+    copy_slot(src, vals[j], dst, scenes[s].p0 + (j - compact_start[s]));
+}
+
+int batch_sort_key_bits(int n_scenes) {
+    int b = 0;
+    while ((1 << b) < n_scenes) ++b;
+    return BATCH_TILE_KEY_BITS + b;
+}
+
+void launch_batch_sort_keys(const SceneDesc *scenes, const int *compact_start, int n_scenes,
+                            const DevParticles &P, int total, uint32_t *keys, uint32_t *vals,
+                            cudaStream_t stream) {
+    if (total > 0)
+        k_batch_sort_keys<<<(total + 255) / 256, 256, 0, stream>>>(scenes, compact_start, n_scenes, P, total,
+                                                                  keys, vals);
+}
+
+void launch_permute_batch(const DevParticles &src, const DevParticles &dst, const uint32_t *keys,
+                          const uint32_t *vals, const SceneDesc *scenes, const int *compact_start, int total,
+                          cudaStream_t stream) {
+    if (total > 0)
+        k_permute_batch<<<(total + 255) / 256, 256, 0, stream>>>(src, dst, keys, vals, scenes, compact_start,
+                                                                total);
 }
 
 void launch_permute(const DevParticles &src, const DevParticles &dst, const uint32_t *perm, int n,

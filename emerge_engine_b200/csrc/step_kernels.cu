@@ -41,7 +41,30 @@ struct GridKernelArgs {
 };
 
 // Grid::update_velocities (grid/mod.rs:264-291), boundaries (step.rs:150-152,
-// 334-344; forces/boundary/mod.rs:78-101), speed clamp (step.rs:155-165).
+// 334-344; forces/boundary/mod.rs:78-101), speed clamp (step.rs:155-165) for one cell of
+// an active tile, then the accumulators are zeroed for the next scatter.
+__device__ __forceinline__ void grid_update_cell(const GridView &g, const DevConfig &cfg, float dt,
+                                                 int tile, int local) {
+    const int ci = tile * TILE_CELLS + local;
+    const int x = (tile / g.tpd) * TILE + (local >> 3);
+    const int y = (tile % g.tpd) * TILE + (local & 7);
+    float4 acc = g.acc_a[ci];
+    float2 s = g.acc_s[ci];
+    float m = acc.x;
+    float2 mom = v2(acc.y + dt * s.x, acc.z + dt * s.y);
+    if (m > 0.0f) {
+        mom = vdivs(mom, m);
+        mom = vadd(mom, vmuls(cfg.gravity, dt));
+        for (int k = 0; k < cfg.n_bound; ++k) slip_velocity(cfg.bound_t[k], x, y, g.res, mom);
+        float vel_limit = cfg.cell / dt;
+        float spd = vlen(mom);
+        if (spd > vel_limit) mom = vmuls(mom, vel_limit / spd);
+    }
+    g.grid_v[ci] = mom;
+    g.acc_a[ci] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    g.acc_s[ci] = v2(0.0f, 0.0f);
+}
+
 __global__ void __launch_bounds__(256) k_grid_update(GridKernelArgs a) {
     const int tile = blockIdx.x * 4 + (threadIdx.x >> 6);
     const int local = threadIdx.x & 63;
@@ -50,45 +73,48 @@ __global__ void __launch_bounds__(256) k_grid_update(GridKernelArgs a) {
     __syncthreads();
     if (tile >= a.n_tiles || !flag) return;
     if (local == 0) a.g.tile_flag[tile] = 0;
-    const int ci = tile * TILE_CELLS + local;
-    const int x = (tile / a.g.tpd) * TILE + (local >> 3);
-    const int y = (tile % a.g.tpd) * TILE + (local & 7);
-    const float dt = a.st->sub_dt;
-    float4 acc = a.g.acc_a[ci];
-    float2 s = a.g.acc_s[ci];
-    float m = acc.x;
-    float2 mom = v2(acc.y + dt * s.x, acc.z + dt * s.y);
-    if (m > 0.0f) {
-        mom = vdivs(mom, m);
-        mom = vadd(mom, vmuls(a.cfg.gravity, dt));
-        for (int k = 0; k < a.cfg.n_bound; ++k) slip_velocity(a.cfg.bound_t[k], x, y, a.g.res, mom);
-        float vel_limit = a.cfg.cell / dt;
-        float spd = vlen(mom);
-        if (spd > vel_limit) mom = vmuls(mom, vel_limit / spd);
+    grid_update_cell(a.g, a.cfg, a.st->sub_dt, tile, local);
+}
+
+// Batched scenes: global tile t belongs to scene tile_scene[t] (local tile t - tile0).
+// A tile's 64 cells span two warps, so the flag is cleared after a CTA barrier.
+__global__ void __launch_bounds__(256) k_grid_update_batch(BatchView b, int n_tiles) {
+    const int t = blockIdx.x * 4 + (threadIdx.x >> 6);
+    const int local = threadIdx.x & 63;
+    const SceneDesc *sd = nullptr;
+    int tile = 0;
+    uint8_t flag = 0;
+    if (t < n_tiles) {
+        sd = &b.scenes[b.tile_scene[t]];
+        if (sd->st->active) {
+            tile = t - sd->tile0;
+            flag = sd->g.tile_flag[tile];
+        }
     }
-    a.g.grid_v[ci] = mom;
-    a.g.acc_a[ci] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-    a.g.acc_s[ci] = v2(0.0f, 0.0f);
+    __syncthreads();
+    if (!flag) return;
+    if (local == 0) sd->g.tile_flag[tile] = 0;
+    grid_update_cell(sd->g, sd->cfg, sd->st->sub_dt, tile, local);
 }
 
 // ---------------------------------------------------------------- controller
 // Step start (step.rs:29-33).
-__global__ void k_step_begin(StepState *st, DevConfig cfg) {
-    st->remaining = cfg.dt;
-    st->substeps = 0;
-    st->vel_clamp = 0;
-    st->jproj = 0;
-    st->dropped = fmaxf(cfg.dt, 0.0f);
-    st->cont = (cfg.dt > F32_EPS && cfg.max_substeps > 0) ? 1u : 0u;
-    st->total_steps += 1;
+__device__ __forceinline__ void step_begin_state(StepState &s, const DevConfig &cfg) {
+    s.remaining = cfg.dt;
+    s.substeps = 0;
+    s.vel_clamp = 0;
+    s.jproj = 0;
+    s.dropped = fmaxf(cfg.dt, 0.0f);
+    s.cont = (cfg.dt > F32_EPS && cfg.max_substeps > 0) ? 1u : 0u;
+    s.total_steps += 1;
 }
 
+__global__ void k_step_begin(StepState *st, DevConfig cfg) { step_begin_state(*st, cfg); }
+
 // Substep start: choose_substep_dt (step.rs:434-468) from the reduction of slot
-// (parity), loop bookkeeping (step.rs:46-48), and the loop condition
-// (step.rs:34) for the graph's while node.
-__global__ void k_substep_begin(StepState *st, DevConfig cfg, int use_cond,
-                                cudaGraphConditionalHandle handle, int kernels_per_substep) {
-    StepState &s = *st;
+// (parity), loop bookkeeping (step.rs:46-48); returns the loop condition (step.rs:34)
+// for the next substep.
+__device__ __forceinline__ uint32_t substep_begin_state(StepState &s, const DevConfig &cfg) {
     const uint32_t k = s.parity;
     const float rem = s.remaining;
     float dt;
@@ -115,20 +141,74 @@ __global__ void k_substep_begin(StepState *st, DevConfig cfg, int use_cond,
     s.total_substeps += 1;
     s.dropped = fmaxf(rem_after, 0.0f);
     s.cont = (rem_after > F32_EPS && s.substeps < static_cast<uint32_t>(cfg.max_substeps)) ? 1u : 0u;
+    return s.cont;
+}
+
+__global__ void k_substep_begin(StepState *st, DevConfig cfg, int use_cond,
+                                cudaGraphConditionalHandle handle, int kernels_per_substep) {
+    StepState &s = *st;
+    const uint32_t cont = substep_begin_state(s, cfg);
+    s.active = 1u;
     if (use_cond) {
         s.graph_kernels += static_cast<unsigned long long>(kernels_per_substep);
-        cudaGraphSetConditional(handle, s.cont);
+        cudaGraphSetConditional(handle, cont);
     }
 }
 
 // Before a prime pass: the next k_substep_begin reads slot (parity).
-__global__ void k_prime_setup(StepState *st) {
-    const uint32_t k = st->parity;
-    st->max_speed_bits[k] = 0u;
-    st->min_mdt_bits[k] = __float_as_uint(INFINITY);
-    st->jproj_pending[k] = 0ull;
-    st->proj_changed[k] = 0ull;
-    st->acc_slot = k;
+__device__ __forceinline__ void prime_setup_state(StepState &s) {
+    const uint32_t k = s.parity;
+    s.max_speed_bits[k] = 0u;
+    s.min_mdt_bits[k] = __float_as_uint(INFINITY);
+    s.jproj_pending[k] = 0ull;
+    s.proj_changed[k] = 0ull;
+    s.acc_slot = k;
+    s.active = 1u;
+}
+
+__global__ void k_prime_setup(StepState *st) { prime_setup_state(*st); }
+
+// Batched controller, one thread per scene (one CTA).  A scene whose frame has ended
+// (cont == 0) sits out the remaining substeps of the batch's frame (active = 0).
+__global__ void k_step_begin_batch(BatchView b, StepState *batch_st) {
+    int any = 0;
+    for (int s = threadIdx.x; s < b.n_scenes; s += blockDim.x) {
+        const SceneDesc &sd = b.scenes[s];
+        step_begin_state(*sd.st, sd.cfg);
+        any |= sd.st->cont ? 1 : 0;
+    }
+    any = __syncthreads_or(any);
+    if (threadIdx.x == 0) {
+        batch_st->total_steps += 1;
+        batch_st->cont = any ? 1u : 0u;
+    }
+}
+
+__global__ void k_substep_begin_batch(BatchView b, StepState *batch_st, int use_cond,
+                                      cudaGraphConditionalHandle handle, int kernels_per_substep) {
+    int any = 0;
+    for (int s = threadIdx.x; s < b.n_scenes; s += blockDim.x) {
+        StepState &st = *b.scenes[s].st;
+        if (st.cont) {
+            st.active = 1u;
+            any |= substep_begin_state(st, b.scenes[s].cfg) ? 1 : 0;
+        } else {
+            st.active = 0u;
+        }
+    }
+    any = __syncthreads_or(any);
+    if (threadIdx.x == 0) {
+        batch_st->total_substeps += 1;
+        batch_st->cont = any ? 1u : 0u;
+        if (use_cond) {
+            batch_st->graph_kernels += static_cast<unsigned long long>(kernels_per_substep);
+            cudaGraphSetConditional(handle, any ? 1u : 0u);
+        }
+    }
+}
+
+__global__ void k_prime_setup_batch(BatchView b) {
+    for (int s = threadIdx.x; s < b.n_scenes; s += blockDim.x) prime_setup_state(*b.scenes[s].st);
 }
 
 // ---------------------------------------------------------------- queries
@@ -395,6 +475,22 @@ void launch_grid_update(const StepLaunch &L) {
 }
 
 void launch_step_begin(const StepLaunch &L) { k_step_begin<<<1, 1, 0, L.stream>>>(L.st, L.cfg); }
+
+void launch_grid_update_batch(const BatchView &b, int n_tiles, cudaStream_t stream) {
+    if (n_tiles > 0) k_grid_update_batch<<<blocks_for(n_tiles, 4), 256, 0, stream>>>(b, n_tiles);
+}
+void launch_step_begin_batch(const BatchView &b, StepState *batch_st, cudaStream_t stream) {
+    k_step_begin_batch<<<1, 1024, 0, stream>>>(b, batch_st);
+}
+void launch_substep_begin_batch(const BatchView &b, StepState *batch_st, int use_cond,
+                                unsigned long long handle, int kernels_per_substep, cudaStream_t stream) {
+    k_substep_begin_batch<<<1, 1024, 0, stream>>>(b, batch_st, use_cond,
+                                                 static_cast<cudaGraphConditionalHandle>(handle),
+                                                 kernels_per_substep);
+}
+void launch_prime_setup_batch(const BatchView &b, cudaStream_t stream) {
+    k_prime_setup_batch<<<1, 1024, 0, stream>>>(b);
+}
 
 void launch_substep_begin(const StepLaunch &L, int use_cond, unsigned long long handle,
                           int kernels_per_substep) {

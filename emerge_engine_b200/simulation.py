@@ -402,3 +402,79 @@ def mlp_infer_bf16(params: np.ndarray, x: np.ndarray) -> np.ndarray:
     check(lib, lib.emerge_cuda_mlp_infer_bf16(p.ctypes.data_as(c_void_p), xx.ctypes.data_as(c_void_p),
                                               len(xx), y.ctypes.data_as(c_void_p)))
     return y
+
+
+class Batch:
+    """Many independent scenes advanced together (one launch per kernel per substep for
+    all scenes).  Built from simulations set up with the single-scene API; their particles
+    are copied, and they stay independent of the batch."""
+
+    def __init__(self, sims):
+        self._lib = load_library()
+        arr = (c_void_p * len(sims))(*[s._sim for s in sims])
+        ptr = c_void_p()
+        st = self._lib.emerge_cuda_batch_create(arr, len(sims), byref(ptr))
+        if st != abi.OK:
+            raise abi.EmergeError(st, (self._lib.emerge_cuda_batch_last_error(None) or b"").decode())
+        self._b = ptr
+        self.n_scenes = len(sims)
+
+    def _check(self, status: int) -> None:
+        if status != abi.OK:
+            raise abi.EmergeError(status, (self._lib.emerge_cuda_batch_last_error(self._b) or b"").decode())
+
+    def close(self) -> None:
+        if getattr(self, "_b", None):
+            self._lib.emerge_cuda_batch_destroy(self._b)
+            self._b = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def step(self, n: int = 1) -> None:
+        self._check(self._lib.emerge_cuda_batch_step(self._b, int(n)))
+
+    def time_steps(self, n: int, flush_l2: bool = True) -> float:
+        """GPU milliseconds summed over n frames (CUDA events, optional L2 flush before each)."""
+        ms = c_float()
+        self._check(self._lib.emerge_cuda_batch_time_steps(self._b, int(n), 1 if flush_l2 else 0, byref(ms)))
+        return float(ms.value)
+
+    def particle_count(self, scene: int) -> int:
+        n = c_uint64()
+        self._check(self._lib.emerge_cuda_batch_particle_count(self._b, int(scene), byref(n)))
+        return int(n.value)
+
+    def particles(self, scene: int) -> np.ndarray:
+        n = self.particle_count(scene)
+        out = np.zeros(n, dtype=PARTICLE_DTYPE)
+        self._check(self._lib.emerge_cuda_batch_read_particles(self._b, int(scene), out.ctypes.data_as(c_void_p), n))
+        return out
+
+    def region_state(self, scene: int, center, radius: float) -> BodyState:
+        out = BodyStateC()
+        self._check(self._lib.emerge_cuda_batch_region_state(
+            self._b, int(scene), float(center[0]), float(center[1]), float(radius), byref(out)))
+        return BodyState.from_c(out)
+
+    def substeps(self) -> tuple[np.ndarray, np.ndarray]:
+        """Per scene: substeps of the last frame and lifetime substeps."""
+        last = np.zeros(self.n_scenes, np.uint64)
+        total = np.zeros(self.n_scenes, np.uint64)
+        self._check(self._lib.emerge_cuda_batch_substeps(self._b, last.ctypes.data_as(c_void_p),
+                                                         total.ctypes.data_as(c_void_p)))
+        return last, total
+
+    def set_option(self, option: int, value: int) -> None:
+        self._check(self._lib.emerge_cuda_batch_set_option(self._b, int(option), int(value)))
+
+    def autotune(self, steps_per_trial: int = 2) -> dict:
+        rep = abi.BatchTuneReportC()
+        self._check(self._lib.emerge_cuda_batch_autotune(self._b, int(steps_per_trial), byref(rep)))
+        n = rep.n_trials
+        return {"sort_interval": rep.sort_interval, "aggregate": rep.aggregate,
+                "trials": [{"sort_interval": rep.trial_sort_interval[k], "aggregate": rep.trial_aggregate[k],
+                            "ms_per_step": rep.trial_ms[k]} for k in range(n)]}

@@ -431,6 +431,47 @@ emerge_status emerge_cuda_mlp_adam(float *params, float *m, float *v, const floa
                                    uint32_t step, float lr, float beta1, float beta2, float eps);
 emerge_status emerge_cuda_mlp_infer_bf16(const float *params, const float *x, uint32_t n, float *y);
 
+/* ---- batched scenes (no counterpart in the reference) -----------------------------
+ * Many independent scenes advanced together: every substep is one launch per kernel for
+ * all scenes (the passes find their scene from CTA and tile tables), and each scene keeps
+ * its own grid size, materials, boundaries, configuration and CFL substep schedule.  A
+ * batch is built from simulations set up with the single-scene API (their particles are
+ * copied; the simulations stay usable and independent).  Scenes run the fast path. */
+typedef struct emerge_batch emerge_batch;
+
+typedef struct emerge_batch_tune_report {
+    int32_t sort_interval;       /* chosen */
+    int32_t aggregate;           /* chosen P2G warp aggregation */
+    uint32_t n_trials;
+    int32_t trial_sort_interval[8];
+    int32_t trial_aggregate[8];
+    float trial_ms[8];           /* GPU ms per frame of each trial */
+} emerge_batch_tune_report;
+
+emerge_status emerge_cuda_batch_create(emerge_sim *const *sims, uint32_t n_sims, emerge_batch **out);
+emerge_status emerge_cuda_batch_destroy(emerge_batch *batch);
+/* Message for the last failed call on `batch` (or the last failed create when NULL). */
+const char *emerge_cuda_batch_last_error(const emerge_batch *batch);
+/* Simulation::step() for every scene, n_steps times (synchronises at the end). */
+emerge_status emerge_cuda_batch_step(emerge_batch *batch, uint32_t n_steps);
+/* Steps n_steps times, timing each frame with CUDA events on the batch's stream (optionally
+ * writing a buffer larger than L2 before each frame); *ms_total = sum of frame times. */
+emerge_status emerge_cuda_batch_time_steps(emerge_batch *batch, uint32_t n_steps, int flush_l2, float *ms_total);
+emerge_status emerge_cuda_batch_scene_count(const emerge_batch *batch, uint32_t *n);
+emerge_status emerge_cuda_batch_particle_count(const emerge_batch *batch, uint32_t scene, uint64_t *n);
+/* particles() of one scene, reference index order. */
+emerge_status emerge_cuda_batch_read_particles(emerge_batch *batch, uint32_t scene, emerge_particle *out, uint64_t n);
+emerge_status emerge_cuda_batch_region_state(emerge_batch *batch, uint32_t scene, float cx, float cy, float radius,
+                                             emerge_body_state *out);
+/* Per scene: substeps of the last frame (last) and lifetime substeps (total); either may be NULL. */
+emerge_status emerge_cuda_batch_substeps(emerge_batch *batch, uint64_t *last, uint64_t *total);
+/* EMERGE_OPT_USE_GRAPH, EMERGE_OPT_SORT_INTERVAL, EMERGE_OPT_P2G_AGGREGATE. */
+emerge_status emerge_cuda_batch_set_option(emerge_batch *batch, int option, int64_t value);
+/* Times every (sort interval, P2G aggregation) candidate for steps_per_trial frames on the
+ * batch itself and keeps the fastest (the batch advances by 8 x steps_per_trial frames). */
+emerge_status emerge_cuda_batch_autotune(emerge_batch *batch, uint32_t steps_per_trial,
+                                         emerge_batch_tune_report *report);
+
 #ifdef __cplusplus
 }
 #endif

@@ -108,3 +108,41 @@ def mixed_granular(sim_cls, grid_res=1024, target_particles=4_000_000, seed=42, 
         s.rng_seed = (seed * 7919 + x0 * 131 + y0) & 0xFFFFFFFF
         sim.add_body(s)
     return sim
+
+
+def batched_scenes(sim_cls, n_scenes=256, seed=7, grid_range=(64, 256), n_range=(4_000, 200_000),
+                   **sim_kw):
+    """Independent scenes for the batched path: per scene a seeded grid size G ~ U{64..256},
+    a particle target N ~ logU[4k, 200k] and a material uniform over {NewtonianFluid,
+    DruckerPrager sand, Stomakhin snow, NeoHookean}; one square block at 4 particles per cell
+    (seeded jitter) resting on the floor of a G^2 grid, clipped to fit inside the walls (so
+    small grids hold fewer particles than their target).  Returns the list of simulations."""
+    rng = np.random.default_rng(seed)
+    sims = []
+    for k in range(n_scenes):
+        g = int(rng.integers(grid_range[0], grid_range[1] + 1))
+        target = float(np.exp(rng.uniform(np.log(n_range[0]), np.log(n_range[1]))))
+        kind = int(rng.integers(4))
+        cfg = SimConfig.standard(g, 0.05, (0.0, -1.0))
+        t = cfg.boundary_thickness
+        if kind == 0:
+            mat = NewtonianFluidMaterial.low_viscosity(1000.0, 1e4)
+        elif kind == 1:
+            mat = DruckerPragerMaterial.cohesionless(1e5, 0.2)
+        elif kind == 2:
+            mat = StomakhinMaterial.from_young_modulus(1.4e5, 0.2)
+        else:
+            mat = NeoHookeanMaterial.new(400.0, 200.0)
+        sim = sim_cls.empty(cfg, **sim_kw).with_default_material(mat)
+        side = int(min(np.sqrt(target / 4.0), g - 2 * t - 6))
+        s = SpawnRegion.for_sim(cfg)
+        s.spacing = 0.5
+        s.box_size = (side, side)
+        s.box_center = (g / 2.0, t + 2 + side / 2.0)
+        s.position_jitter = 0.4
+        s.rng_seed = (seed * 1000003 + k) & 0xFFFFFFFF
+        if kind == 0:
+            s.mass_override = 1000.0 * 0.25
+        sim.add_body(s)
+        sims.append(sim)
+    return sims

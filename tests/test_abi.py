@@ -43,6 +43,7 @@ C_STRUCTS = {
     "emerge_closure_stats": abi.ClosureStatsC,
     "emerge_closure_train_config": abi.ClosureTrainConfigC,
     "emerge_closure_train_report": abi.ClosureTrainReportC,
+    "emerge_batch_tune_report": abi.BatchTuneReportC,
 }
 
 

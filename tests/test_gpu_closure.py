@@ -32,7 +32,9 @@ def test_device_adam_matches_oracle(cuda_lib):
     v = np.abs(rng.normal(size=p.size)).astype(np.float32) * 1e-6
     g = rng.normal(size=p.size).astype(np.float32) * 1e-2
     p1, m1, v1 = mlp_adam(p, m, v, g, 7, 1e-3)
-    p2, m2, v2 = co.adam_step(p.astype(np.float64), m, v, g.astype(np.float64), 7, 1e-3)
+    f = lambda a: float(np.float32(a))  # the hyper-parameters as the device sees them
+    p2, m2, v2 = co.adam_step(p.astype(np.float64), m, v, g.astype(np.float64), 7, f(1e-3),
+                              beta1=f(0.9), beta2=f(0.999), eps=f(1e-8))
     # FP32 with FMA on the device vs float64: compare against each array's scale
     assert np.max(np.abs(m1 - m2)) <= 1e-6 * np.max(np.abs(m2))
     assert np.max(np.abs(v1 - v2)) <= 1e-6 * np.max(np.abs(v2))
