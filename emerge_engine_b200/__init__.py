@@ -4,7 +4,9 @@
 reference crate's names and semantics; the step runs in libemerge_cuda.so (include/emerge_cuda.h).
 """
 from .config import BodyState, SimConfig, SlipBoundary, SpawnRegion  # noqa: F401
-from .materials import (DruckerPragerMaterial, FallbackMaterial, NaccMaterial,  # noqa: F401
-                        NeoHookeanMaterial, NewtonianFluidMaterial, StomakhinMaterial,
-                        lame_from_young, to_radians)
+from .materials import (BinghamFluidMaterial, CorotatedMaterial,  # noqa: F401
+                        DruckerPragerMaterial, FallbackMaterial, GranularFluidMaterial,
+                        MuIRheologyMaterial, NaccMaterial, NeoHookeanMaterial,
+                        NewtonianFluidMaterial, RankineMaterial, StomakhinMaterial,
+                        ViscoelasticMaterial, VonMisesMaterial, lame_from_young, to_radians)
 from .simulation import Batch, DeterministicSimulation, MaterialRegistry, Simulation  # noqa: F401

@@ -62,6 +62,7 @@ struct emerge_batch {
     int n_blocks = 0, n_tiles = 0, total = 0;
     size_t slots = 0;
     LoadFlagsHost lf;
+    unsigned model_mask = 1u << M_FALLBACK;
     int any_density = 0;
     Buf pbuf, gbuf, tables, sortbuf, region, staging, states, flush;
     DevParticles P[2];
@@ -143,8 +144,11 @@ bool sort_due(const emerge_batch *b) {
 emerge_status prime(emerge_batch *b) {
     const BatchView all = b->view(0);
     launch_prime_setup_batch(all, b->stream);
-    launch_particle_pass_batch(b->P[b->cur], all, b->n_blocks, b->lf, 0, 1, b->aggregate, b->stream);
-    if (b->any_density) launch_density_pass_batch(b->P[b->cur], all, b->n_blocks, b->lf, b->aggregate, b->stream);
+    launch_particle_pass_batch(b->P[b->cur], all, b->n_blocks, b->lf, b->model_mask, 0, 1,
+                               b->aggregate, b->stream);
+    if (b->any_density)
+        launch_density_pass_batch(b->P[b->cur], all, b->n_blocks, b->lf, b->model_mask,
+                                  b->aggregate, b->stream);
     BK(cudaGetLastError());
     b->pending_valid = true;
     return EMERGE_OK;
@@ -154,8 +158,11 @@ void enqueue_substep(emerge_batch *b, int use_cond, unsigned long long handle) {
     const BatchView live = b->view(1);
     launch_substep_begin_batch(live, b->batch_state(), use_cond, handle, 3 + b->any_density, b->stream);
     launch_grid_update_batch(live, b->n_tiles, b->stream);
-    launch_particle_pass_batch(b->P[b->cur], live, b->n_blocks, b->lf, 1, 1, b->aggregate, b->stream);
-    if (b->any_density) launch_density_pass_batch(b->P[b->cur], live, b->n_blocks, b->lf, b->aggregate, b->stream);
+    launch_particle_pass_batch(b->P[b->cur], live, b->n_blocks, b->lf, b->model_mask, 1, 1,
+                               b->aggregate, b->stream);
+    if (b->any_density)
+        launch_density_pass_batch(b->P[b->cur], live, b->n_blocks, b->lf, b->model_mask,
+                                  b->aggregate, b->stream);
 }
 
 emerge_status build_graph(emerge_batch *b) {
@@ -282,8 +289,10 @@ emerge_status emerge_cuda_batch_create(emerge_sim *const *sims, uint32_t n_sims,
         h.n_tiles = h.tpd * h.tpd;
         h.n_mats = static_cast<int>(v.mats.size());
         int dens = v.cfg.recompute_density_each_step ? 1 : 0;
-        for (const auto &m : v.mats)
+        for (const auto &m : v.mats) {
             if (m.model == M_FLUID) dens = 1;  // needs_density_recompute (fluid.rs:261-263)
+            b->model_mask |= model_bits(m);
+        }
         h.density_mode = dens;
         b->any_density |= dens;
         b->lf.temperature |= v.lf.temperature;

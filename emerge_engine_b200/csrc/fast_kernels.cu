@@ -52,8 +52,8 @@ __global__ void __launch_bounds__(THREADS, EMERGE_DENSITY_CTAS_PER_SM) k_density
 }
 
 void launch_particle_pass_batch(const DevParticles &P, const BatchView &b, int n_blocks,
-                                const LoadFlagsHost &lf, int mode_g2p, int emit_p2g, int aggregate,
-                                cudaStream_t stream) {
+                                const LoadFlagsHost &lf, unsigned model_mask, int mode_g2p,
+                                int emit_p2g, int aggregate, cudaStream_t stream) {
     if (n_blocks <= 0) return;
     ParticleKernelArgs a;
     std::memset(&a, 0, sizeof(a));
@@ -66,11 +66,15 @@ void launch_particle_pass_batch(const DevParticles &P, const BatchView &b, int n
     a.emit_p2g = emit_p2g;
     a.aggregate = aggregate;
     a.batch = b;
-    k_particle_batch<ALL_MODELS><<<n_blocks, THREADS, 0, stream>>>(a);
+    if ((model_mask & ~ALL_MODELS) == 0u)
+        k_particle_batch<ALL_MODELS><<<n_blocks, THREADS, 0, stream>>>(a);
+    else
+        k_particle_batch<FULL_MODELS><<<n_blocks, THREADS, 0, stream>>>(a);
 }
 
 void launch_density_pass_batch(const DevParticles &P, const BatchView &b, int n_blocks,
-                               const LoadFlagsHost &lf, int aggregate, cudaStream_t stream) {
+                               const LoadFlagsHost &lf, unsigned model_mask, int aggregate,
+                               cudaStream_t stream) {
     if (n_blocks <= 0) return;
     DensityKernelArgs a;
     std::memset(&a, 0, sizeof(a));
@@ -80,15 +84,21 @@ void launch_density_pass_batch(const DevParticles &P, const BatchView &b, int n_
     a.lf.pinned = lf.pinned;
     a.aggregate = aggregate;
     a.batch = b;
-    k_density_batch<ALL_MODELS><<<n_blocks, THREADS, 0, stream>>>(a);
+    if ((model_mask & ~ALL_MODELS) == 0u)
+        k_density_batch<ALL_MODELS><<<n_blocks, THREADS, 0, stream>>>(a);
+    else
+        k_density_batch<FULL_MODELS><<<n_blocks, THREADS, 0, stream>>>(a);
 }
 
 void launch_particle_pass_fast(const ParticleKernelArgs &a, unsigned model_mask, cudaStream_t stream) {
     const int grid = blocks_for(a.n, THREADS);
     const unsigned plastic = (1u << M_DRUCKER_PRAGER) | (1u << M_NACC);
     if ((a.cl.infer || a.cl.log) && (model_mask & plastic)) {
-        if (covering_mask(model_mask) == MASK_GRANULAR)
+        const unsigned cover = covering_mask(model_mask);
+        if (cover == MASK_GRANULAR)
             k_particle_closure<MASK_GRANULAR><<<grid, THREADS, 0, stream>>>(a);
+        else if (cover == FULL_MODELS)
+            k_particle_closure<FULL_MODELS><<<grid, THREADS, 0, stream>>>(a);
         else
             k_particle_closure<ALL_MODELS><<<grid, THREADS, 0, stream>>>(a);
         return;
@@ -98,7 +108,8 @@ void launch_particle_pass_fast(const ParticleKernelArgs &a, unsigned model_mask,
     case MASK_SOLID: k_particle_fast<MASK_SOLID><<<grid, THREADS, 0, stream>>>(a); break;
     case MASK_SOLID_FLUID: k_particle_fast<MASK_SOLID_FLUID><<<grid, THREADS, 0, stream>>>(a); break;
     case MASK_GRANULAR: k_particle_fast<MASK_GRANULAR><<<grid, THREADS, 0, stream>>>(a); break;
-    default: k_particle_fast<ALL_MODELS><<<grid, THREADS, 0, stream>>>(a); break;
+    case ALL_MODELS: k_particle_fast<ALL_MODELS><<<grid, THREADS, 0, stream>>>(a); break;
+    default: k_particle_fast<FULL_MODELS><<<grid, THREADS, 0, stream>>>(a); break;
     }
 }
 
@@ -109,7 +120,8 @@ void launch_density_pass_fast(const DensityKernelArgs &a, unsigned model_mask, c
     case MASK_SOLID: k_density<MASK_SOLID><<<grid, THREADS, 0, stream>>>(a); break;
     case MASK_SOLID_FLUID: k_density<MASK_SOLID_FLUID><<<grid, THREADS, 0, stream>>>(a); break;
     case MASK_GRANULAR: k_density<MASK_GRANULAR><<<grid, THREADS, 0, stream>>>(a); break;
-    default: k_density<ALL_MODELS><<<grid, THREADS, 0, stream>>>(a); break;
+    case ALL_MODELS: k_density<ALL_MODELS><<<grid, THREADS, 0, stream>>>(a); break;
+    default: k_density<FULL_MODELS><<<grid, THREADS, 0, stream>>>(a); break;
     }
 }
 

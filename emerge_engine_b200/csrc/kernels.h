@@ -47,12 +47,13 @@ void launch_substep_begin_batch(const BatchView &b, StepState *batch_st, int use
                                 unsigned long long handle, int kernels_per_substep, cudaStream_t stream);
 void launch_prime_setup_batch(const BatchView &b, cudaStream_t stream);
 // particle pass (mode_g2p, emit_p2g as launch_particle_pass) and density pass over all
-// CTAs of a batch; lf: union of the scenes' load flags
+// CTAs of a batch; lf: union of the scenes' load flags, model_mask: union of their models
 void launch_particle_pass_batch(const DevParticles &P, const BatchView &b, int n_blocks,
-                                const LoadFlagsHost &lf, int mode_g2p, int emit_p2g, int aggregate,
-                                cudaStream_t stream);
+                                const LoadFlagsHost &lf, unsigned model_mask, int mode_g2p,
+                                int emit_p2g, int aggregate, cudaStream_t stream);
 void launch_density_pass_batch(const DevParticles &P, const BatchView &b, int n_blocks,
-                               const LoadFlagsHost &lf, int aggregate, cudaStream_t stream);
+                               const LoadFlagsHost &lf, unsigned model_mask, int aggregate,
+                               cudaStream_t stream);
 
 // det_kernels.cu (reference-order mode)
 void launch_project(const StepLaunch &L);

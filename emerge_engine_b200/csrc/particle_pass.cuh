@@ -947,10 +947,10 @@ void launch_density_pass_fast(const DensityKernelArgs &a, unsigned model_mask, c
 
 // Smallest instantiated model set that covers the registered models.
 inline unsigned covering_mask(unsigned m) {
-    const unsigned masks[4] = {MASK_FLUID, MASK_SOLID, MASK_SOLID_FLUID, MASK_GRANULAR};
+    const unsigned masks[5] = {MASK_FLUID, MASK_SOLID, MASK_SOLID_FLUID, MASK_GRANULAR, ALL_MODELS};
     for (unsigned c : masks)
         if ((m & ~c) == 0u) return c;
-    return ALL_MODELS;
+    return FULL_MODELS;
 }
 
 template <class Args>

@@ -239,6 +239,34 @@ EM_HD bool dp_project(const MatP &m, float2 sigma_in, float lvs, float q, float2
 
 EM_HD M2 reconstruct(M2 u, float2 s, M2 vt) { return mm(mm(u, mdiag(s)), vt); }
 
+// hencky_strains (matter/materials/utils.rs:58-61)
+EM_HD float2 hencky(float2 sigma, bool pr) {
+    float2 s = vmax2(vabs2(sigma), splat(LOG_CLAMP));
+    return v2(em_log(s.x, pr), em_log(s.y, pr));
+}
+
+// stress_to_hencky (matter/materials/utils.rs:76-83)
+EM_HD float2 stress_to_hencky(float2 tau, float lambda, float mu) {
+    float det = 4.0f * mu * (mu + lambda);
+    float a = 2.0f * mu + lambda;
+    return v2((a * tau.x - lambda * tau.y) / det, (a * tau.y - lambda * tau.x) / det);
+}
+
+// Corotated linear-elastic stress 2 mu (F - R) F^T + lambda (J - 1) J I with moduli already
+// scaled (corotated.rs:61-77, von_mises.rs:94-102, rankine.rs, sand_mui.rs kirchhoff_stress).
+EM_HD M2 corotated_stress(M2 f, float mu, float lambda) {
+    float j = mdet(f);
+    if (j <= MIN_J) return mzero();
+    M2 r = polar(f);
+    return madd(mm(smscale(2.0f * mu, msub(f, r)), mtrans(f)),
+                smscale(lambda * (j - 1.0f) * j, mident()));
+}
+
+// Bingham fluid (bingham.rs): MaterialParams carries the yield stress in compression_limit
+// (bingham.rs params()), so a Fluid slot with compression_limit > 0 is a Bingham fluid.
+// critical_shear_rate is the constructor's 1e-4 (bingham.rs new()).
+EM_HD bool is_bingham(const MatP &m) { return m.model == M_FLUID && m.compression_limit > 0.0f; }
+
 // NaccMaterial::project (nacc.rs:129-223).  params(): hardening_exponent = xi,
 // compression_limit = beta, stretch_limit = M (nacc.rs:309-311).
 EM_HD void nacc_project(const MatP &m, M2 f, float alpha, M2 &f_out, float &alpha_out, bool pr) {
@@ -310,6 +338,17 @@ EM_HD void nacc_project(const MatP &m, M2 f, float alpha, M2 &f_out, float &alph
 #define HAS_MODEL(mask, model) ((((mask) >> (model)) & 1u) != 0u)
 constexpr unsigned ALL_MODELS = (1u << M_FALLBACK) | (1u << M_FLUID) | (1u << M_NEOHOOKEAN) |
                                 (1u << M_SNOW) | (1u << M_DRUCKER_PRAGER) | (1u << M_NACC);
+// Mask bit 12 is not a ConstitutiveModel id: it marks a scene with a Bingham fluid (a Fluid
+// slot with compression_limit > 0), so Newtonian-only kernels leave the Bingham branch out.
+constexpr uint32_t M_BINGHAM_BIT = 12;
+// Every ConstitutiveModel id (materials/mod.rs:53-66) and the Bingham bit.  Kernels for
+// scenes whose models all lie in ALL_MODELS keep the smaller instantiation.
+constexpr unsigned FULL_MODELS = 0x1FFFu;
+
+// Model-mask bits of one material slot.
+EM_HD unsigned model_bits(const MatP &m) {
+    return (1u << m.model) | (is_bingham(m) ? (1u << M_BINGHAM_BIT) : 0u);
+}
 
 // ---------------------------------------------------------------- particle view
 // Registers of one particle while a kernel works on it.
@@ -325,7 +364,7 @@ struct PState {
 };
 
 // MaterialModel::kirchhoff_stress per model.
-template <unsigned MASK = ALL_MODELS>
+template <unsigned MASK = FULL_MODELS>
 EM_HD M2 kirchhoff_stress(const MatP &m, const PState &p, bool pr) {
     const M2 f = p.f;
     switch (m.model) {
@@ -362,6 +401,21 @@ EM_HD M2 kirchhoff_stress(const MatP &m, const PState &p, bool pr) {
             m.eos_stiffness * (em_pow(density / m.rest_density, m.eos_power, pr) - 1.0f),
             m.pressure_floor);
         M2 stress = mdiag(splat(-pressure));
+        if (HAS_MODEL(MASK, M_BINGHAM_BIT) && is_bingham(m)) {  // bingham.rs kirchhoff_stress
+            M2 d = mscale(madd(p.c, mtrans(p.c)), 0.5f);
+            float trace = d.xa.x + d.ya.y;
+            M2 d_dev = msub(d, mdiag(splat(trace * 0.5f)));
+            float dxx = d_dev.xa.x, dyy = d_dev.ya.y, dxy = d_dev.xa.y;
+            float d_sq = dxx * dxx + dyy * dyy + 2.0f * dxy * dxy;
+            float shear_rate = sqrtf(2.0f * d_sq);
+            if (!(shear_rate < 1.0e-4f))
+                stress = madd(stress, mscale(d_dev, m.compression_limit / shear_rate + m.dynamic_viscosity));
+            if (m.surface_tension_coeff != 0.0f) {
+                float j = f.xa.x * f.ya.y - f.xa.y * f.ya.x;
+                stress = madd(stress, mdiag(splat(m.surface_tension_coeff * j)));
+            }
+            return stress;
+        }
         float eff_visc = m.dynamic_viscosity;
         if (m.thermal_viscosity_coeff > 0.0f)
             eff_visc = m.dynamic_viscosity * em_exp(-m.thermal_viscosity_coeff * p.temperature, pr);
@@ -417,22 +471,81 @@ EM_HD M2 kirchhoff_stress(const MatP &m, const PState &p, bool pr) {
     }
         return mzero();
     }
+    case M_COROTATED: {
+        if constexpr (HAS_MODEL(MASK, M_COROTATED)) {  // corotated.rs:61-77
+            float t_scale = 1.0f + m.thermal_expansion * p.temperature;
+            return corotated_stress(f, m.mu * p.h * t_scale, m.lambda * p.h * t_scale);
+        }
+        return mzero();
+    }
+    case M_VON_MISES:
+        if constexpr (HAS_MODEL(MASK, M_VON_MISES)) return corotated_stress(f, m.mu, m.lambda);
+        return mzero();
+    case M_RANKINE:
+        if constexpr (HAS_MODEL(MASK, M_RANKINE)) return corotated_stress(f, m.mu, m.lambda);
+        return mzero();
+    case M_DP_MUI:
+        if constexpr (HAS_MODEL(MASK, M_DP_MUI)) return corotated_stress(f, m.mu, m.lambda);
+        return mzero();
+    case M_VISCOELASTIC: {
+        if constexpr (HAS_MODEL(MASK, M_VISCOELASTIC)) {  // viscoelastic.rs kirchhoff_stress
+        // params(): viscosity in dynamic_viscosity, j_min in volume_ratio_min
+        float j = fminf(fmaxf(f.xa.x * f.ya.y - f.xa.y * f.ya.x, m.volume_ratio_min),
+                        1.0f / m.volume_ratio_min);
+        float t_scale = 1.0f + m.thermal_expansion * p.temperature;
+        float mu = m.mu * t_scale;
+        float lambda = m.lambda * t_scale;
+        M2 b = mm(f, mtrans(f));
+        M2 elastic = madd(smscale(mu, msub(b, mident())), mdiag(splat(lambda * em_log(j, pr))));
+        M2 d = mscale(madd(p.c, mtrans(p.c)), 0.5f);
+        float trace = d.xa.x + d.ya.y;
+        M2 d_dev = msub(d, mdiag(splat(trace * 0.5f)));
+        return madd(elastic, smscale(m.dynamic_viscosity * t_scale, d_dev));
+    }
+        return mzero();
+    }
+    case M_GRANULAR_FLUID: {
+        if constexpr (HAS_MODEL(MASK, M_GRANULAR_FLUID)) {  // granular_fluid.rs kirchhoff_stress
+        float j = fmaxf(mdet(f), MIN_J);
+        float density = fmaxf(m.rest_density / j, 1.0e-6f);
+        float ratio = fmaxf(density / fmaxf(m.rest_density, 1.0e-6f), 1.0e-6f);
+        float pressure = fmaxf(m.eos_stiffness * (em_pow(ratio, m.eos_power, pr) - 1.0f),
+                               m.pressure_floor);
+        M2 r = polar(f);
+        M2 coro = mm(smscale(2.0f * (m.mu * p.h), msub(f, r)), mtrans(f));
+        float tr = coro.xa.x + coro.ya.y;
+        M2 dev_coro = msub(coro, mdiag(splat(tr * 0.5f)));
+        M2 lam_vol = smscale(m.lambda * p.h * (j - 1.0f) * j, mident());
+        return madd(madd(mdiag(splat(-pressure)), dev_coro), lam_vol);
+    }
+        return mzero();
+    }
     default:  // FallbackMaterial: zero stress (materials/mod.rs:362-366)
         return mzero();
     }
 }
 
-// combined_kirchhoff_stress (spacetime/transfer.rs:77-104).  Only NeoHookean has a
-// non-zero activation_scale among the supported models (elastic.rs:271-273).
-template <unsigned MASK = ALL_MODELS>
+// MaterialModel::activation_scale: NeoHookean (elastic.rs:271-273), Corotated and
+// Viscoelastic report active_stress_coeff; every other model 0 (materials/mod.rs:181-183).
+EM_HD float activation_scale(const MatP &m) {
+    return (m.model == M_NEOHOOKEAN || m.model == M_COROTATED || m.model == M_VISCOELASTIC)
+               ? m.active_stress_coeff
+               : 0.0f;
+}
+
+// combined_kirchhoff_stress (spacetime/transfer.rs:77-104): Viscoelastic's active stress
+// is isotropic, every other model's follows the fibre direction.
+template <unsigned MASK = FULL_MODELS>
 EM_HD M2 combined_kirchhoff_stress(const MatP &m, const PState &p, bool pr) {
     M2 tau = kirchhoff_stress<MASK>(m, p, pr);
-    float coeff = (m.model == M_NEOHOOKEAN) ? m.active_stress_coeff : 0.0f;
+    float coeff = activation_scale(m);
     if (p.activation <= 0.0f || coeff <= 0.0f) return tau;
     M2 tau_active;
     float2 n = p.act_dir;
     float len_sq = vdot(n, n);
-    if (len_sq > F32_EPS) {
+    if (m.model == M_VISCOELASTIC) {
+        tau_active = mdiag(splat(p.activation * coeff));
+    } else if (len_sq > F32_EPS) {
         float2 n0 = vdivs(n, sqrtf(len_sq));
         M2 n_outer = m2(vmuls(n0, n0.x), vmuls(n0, n0.y));
         M2 a_mat = mscale(n_outer, p.activation * coeff);
@@ -443,15 +556,16 @@ EM_HD M2 combined_kirchhoff_stress(const MatP &m, const PState &p, bool pr) {
     return madd(tau, tau_active);
 }
 
-// MaterialModel::stress_volume: Fluid uses max(volume, 1e-6) (fluid.rs:193-195),
-// every other supported model the initial volume (materials/mod.rs:114).
+// MaterialModel::stress_volume: Fluid and Bingham use max(volume, 1e-6) (fluid.rs:193-195,
+// bingham.rs min_volume), GranularFluid max(volume, 1e-6) (granular_fluid.rs), every other
+// model the initial volume (materials/mod.rs:114).
 EM_HD float stress_volume(const MatP &m, const PState &p) {
-    if (m.model == M_FLUID) return fmaxf(p.vol, 1.0e-6f);
+    if (m.model == M_FLUID || m.model == M_GRANULAR_FLUID) return fmaxf(p.vol, 1.0e-6f);
     return p.v0;
 }
 
 // MaterialModel::timestep_bound
-template <unsigned MASK = ALL_MODELS>
+template <unsigned MASK = FULL_MODELS>
 EM_HD float timestep_bound(const MatP &m, float density, float h, float cell, float mat_cfl,
                            float visc_cfl, bool pr) {
     switch (m.model) {
@@ -499,6 +613,39 @@ EM_HD float timestep_bound(const MatP &m, float density, float h, float cell, fl
     }
         return INFINITY;
     }
+    case M_COROTATED:  // corotated.rs timestep_bound
+        if constexpr (HAS_MODEL(MASK, M_COROTATED))
+            return elastic_wave_dt(m.lambda, m.mu, h, density, MIN_J, cell, mat_cfl);
+        return INFINITY;
+    case M_GRANULAR_FLUID:  // granular_fluid.rs timestep_bound
+        if constexpr (HAS_MODEL(MASK, M_GRANULAR_FLUID))
+            return elastic_wave_dt(m.lambda, m.mu, h, density, MIN_J, cell, mat_cfl);
+        return INFINITY;
+    case M_VON_MISES:  // von_mises.rs:154-171
+        if constexpr (HAS_MODEL(MASK, M_VON_MISES))
+            return elastic_wave_dt(m.lambda, m.mu, 1.0f, density, MIN_J, cell, mat_cfl);
+        return INFINITY;
+    case M_RANKINE:  // rankine.rs timestep_bound
+        if constexpr (HAS_MODEL(MASK, M_RANKINE))
+            return elastic_wave_dt(m.lambda, m.mu, 1.0f, density, MIN_J, cell, mat_cfl);
+        return INFINITY;
+    case M_DP_MUI:  // sand_mui.rs timestep_bound
+        if constexpr (HAS_MODEL(MASK, M_DP_MUI))
+            return elastic_wave_dt(m.lambda, m.mu, 1.0f, density, MIN_J, cell, mat_cfl);
+        return INFINITY;
+    case M_VISCOELASTIC: {
+        if constexpr (HAS_MODEL(MASK, M_VISCOELASTIC)) {  // viscoelastic.rs timestep_bound
+        float elastic_dt = elastic_wave_dt(m.lambda, m.mu, 1.0f, density, 1.0e-6f, cell, mat_cfl);
+        float viscous_dt = INFINITY;
+        if (m.dynamic_viscosity > 0.0f) {
+            float d = fmaxf(density, 1.0e-6f);
+            float kinematic = m.dynamic_viscosity / d;
+            if (kinematic > F32_EPS) viscous_dt = visc_cfl * cell * cell / kinematic;
+        }
+        return fminf(elastic_dt, viscous_dt);
+    }
+        return INFINITY;
+    }
     default:
         return INFINITY;
     }
@@ -536,7 +683,7 @@ EM_HD void dp_finish(const MatP &m, PState &p, M2 u, float2 sigma, M2 vt, bool p
 }
 
 // MaterialModel::update_particle
-template <unsigned MASK = ALL_MODELS>
+template <unsigned MASK = FULL_MODELS>
 EM_HD void update_particle(const MatP &m, PState &p, float dt, bool pr) {
     switch (m.model) {
     case M_NEOHOOKEAN: {
@@ -608,6 +755,130 @@ EM_HD void update_particle(const MatP &m, PState &p, float dt, bool pr) {
     }
         break;
     }
+    case M_COROTATED:       // corotated.rs update_particle
+    case M_VISCOELASTIC: {  // viscoelastic.rs update_particle
+        if constexpr (HAS_MODEL(MASK, M_COROTATED) || HAS_MODEL(MASK, M_VISCOELASTIC)) {
+        M2 fp_new = madd(mident(), smscale(dt, p.c));
+        p.f = mm(fp_new, p.f);
+        sync_volume_density(p);
+    }
+        break;
+    }
+    case M_VON_MISES: {
+        if constexpr (HAS_MODEL(MASK, M_VON_MISES)) {  // von_mises.rs:108-141
+        // params(): yield_stress in hardening_exponent, H in hardening_modulus
+        M2 f_trial = mm(madd(mident(), smscale(dt, p.c)), p.f);
+        M2 u, vt;
+        float2 sigma;
+        svd2(f_trial, u, sigma, vt);
+        float2 eps = hencky(sigma, pr);
+        float tr = eps.x + eps.y;
+        float2 dev = vsub(eps, splat(tr * 0.5f));
+        float dev_norm = vlen(dev);
+        float kappa = p.q;
+        float effective_yield = m.hardening_exponent + m.hardening_modulus * kappa;
+        float elastic_dev = 2.0f * m.mu * dev_norm;
+        float2 sigma_new = sigma;
+        if (elastic_dev > effective_yield && dev_norm > LOG_CLAMP) {
+            float denom = 2.0f * m.mu + m.hardening_modulus;
+            float gamma = denom > F32_EPS ? (elastic_dev - effective_yield) / denom : 0.0f;
+            p.q = kappa + gamma;
+            float2 eps_proj = vadd(vmuls(dev, effective_yield / elastic_dev), splat(tr * 0.5f));
+            sigma_new = v2(em_exp(eps_proj.x, pr), em_exp(eps_proj.y, pr));
+        }
+        p.f = reconstruct(u, sigma_new, vt);
+        sync_volume_density(p);
+    }
+        break;
+    }
+    case M_RANKINE: {
+        if constexpr (HAS_MODEL(MASK, M_RANKINE)) {  // rankine.rs update_particle
+        // params(): tensile_strength in hardening_exponent, softening_rate in hardening_modulus
+        M2 f_trial = mm(madd(mident(), smscale(dt, p.c)), p.f);
+        M2 u, vt;
+        float2 sigma;
+        svd2(f_trial, u, sigma, vt);
+        float2 eps = hencky(sigma, pr);
+        float a = 2.0f * m.mu + m.lambda;
+        float2 tau = v2(a * eps.x + m.lambda * eps.y, m.lambda * eps.x + a * eps.y);
+        float damage = p.q;
+        float ts = m.hardening_exponent, rate = m.hardening_modulus;
+        float t_eff = fmaxf(ts * em_exp(-rate * damage, pr), ts * 0.05f);  // utils.rs:28
+        bool t1 = tau.x > t_eff, t2 = tau.y > t_eff;
+        float2 sigma_new = sigma;
+        if (t1 || t2) {
+            float2 tau_proj = (t1 && t2) ? splat(t_eff) : (t1 ? v2(t_eff, tau.y) : v2(tau.x, t_eff));
+            float2 eps_proj = stress_to_hencky(tau_proj, m.lambda, m.mu);
+            float2 eps_trial = stress_to_hencky(tau, m.lambda, m.mu);
+            // rankine_damage_saturation_point (utils.rs:43-49)
+            float sat = rate <= 0.0f ? INFINITY : -em_log(0.05f, pr) / rate;
+            p.q = fminf(damage + vlen(vsub(eps_trial, eps_proj)), sat);
+            sigma_new = v2(em_exp(eps_proj.x, pr), em_exp(eps_proj.y, pr));
+        }
+        p.f = reconstruct(u, sigma_new, vt);
+        sync_volume_density(p);
+    }
+        break;
+    }
+    case M_DP_MUI: {
+        if constexpr (HAS_MODEL(MASK, M_DP_MUI)) {  // sand_mui.rs update_particle
+        // params(): mu_static, mu_dynamic, inertial_q in dp_h0, dp_h1, dp_h2
+        const float SQRT_2 = 1.41421356237f;
+        const float mu_s = m.dp_h0, mu_d = m.dp_h1, i0 = m.dp_h2;
+        M2 f_trial = mm(madd(mident(), smscale(dt, p.c)), p.f);
+        M2 u, vt;
+        float2 sigma;
+        svd2(f_trial, u, sigma, vt);
+        float2 eps = hencky(sigma, pr);
+        float tr = eps.x + eps.y;
+        float p_trial = -(m.lambda + m.mu) * tr;
+        float2 dev = vsub(eps, splat(tr * 0.5f));
+        float dev_norm = vlen(dev);
+        float2 sigma_new;
+        float q_new = mu_s;
+        if (p_trial <= 0.0f) {
+            sigma_new = v2(1.0f, 1.0f);
+        } else if (SQRT_2 * m.mu * dev_norm <= mu_s * p_trial || dev_norm < F32_EPS) {
+            sigma_new = sigma;
+        } else {
+            float delta_q = SQRT_2 * m.mu * dev_norm - mu_s * p_trial;
+            float sqrt_p = sqrtf(p_trial);
+            float a = m.mu * dt;
+            float b = p_trial * (mu_d - mu_s) + a * i0 * sqrt_p - delta_q;
+            float c = -delta_q * i0 * sqrt_p;
+            float gamma_dot = fmaxf((-b + sqrtf(b * b - 4.0f * a * c)) / (2.0f * a), 0.0f);
+            if (gamma_dot > F32_EPS) q_new = mu_s + (mu_d - mu_s) / (i0 * sqrt_p / gamma_dot + 1.0f);
+            float delta_gamma = gamma_dot * dt;
+            float2 n_hat = vdivs(dev, dev_norm);
+            float2 eps_new = vsub(eps, vmuls(n_hat, delta_gamma / SQRT_2));
+            sigma_new = v2(em_exp(eps_new.x, pr), em_exp(eps_new.y, pr));
+        }
+        p.f = reconstruct(u, sigma_new, vt);
+        p.q = q_new;
+        sync_volume_density(p);
+    }
+        break;
+    }
+    case M_GRANULAR_FLUID: {
+        if constexpr (HAS_MODEL(MASK, M_GRANULAR_FLUID)) {  // granular_fluid.rs update_particle
+        M2 f_trial = mm(madd(mident(), smscale(dt, p.c)), p.f);
+        if (m.compression_limit > 0.0f || m.stretch_limit > 0.0f) {
+            M2 u, vt;
+            float2 sigma;
+            svd2(f_trial, u, sigma, vt);
+            float lo = 1.0f - m.compression_limit, hi = 1.0f + m.stretch_limit;
+            float2 sigma_c = v2(fclampf(sigma.x, lo, hi), fclampf(sigma.y, lo, hi));
+            float jp_new = p.jp * (sigma.x * sigma.y) / fmaxf(sigma_c.x * sigma_c.y, 1.0e-10f);
+            p.jp = fclampf(jp_new, m.volume_ratio_min, m.volume_ratio_max);
+            p.h = fclampf(em_exp(m.hardening_exponent * (1.0f - p.jp), pr), 0.1f, 7.0f);
+            p.f = mm(mm(u, mdiag(sigma_c)), vt);
+        } else {
+            p.f = f_trial;
+        }
+        sync_volume_density(p);
+    }
+        break;
+    }
     default:
         break;
     }
@@ -625,6 +896,14 @@ EM_HD void init_particle(const MatP &m, emerge_particle &p) {
         break;
     case M_NACC:  // nacc.rs:271-273
         p.log_volume_strain = 0.0f;
+        break;
+    case M_COROTATED:       // corotated.rs init_particle
+    case M_GRANULAR_FLUID:  // granular_fluid.rs init_particle
+        p.hardening_scale = 1.0f;
+        p.plastic_volume_ratio = 1.0f;
+        break;
+    case M_DP_MUI:  // sand_mui.rs init_particle: mu_static in dp_h0
+        p.friction_hardening = m.dp_h0;
         break;
     default:
         break;

@@ -85,8 +85,7 @@ size_t particle_set_bytes(size_t cap) {
 }
 
 bool model_supported(uint32_t m) {
-    return m == M_FALLBACK || m == M_FLUID || m == M_NEOHOOKEAN || m == M_SNOW ||
-           m == M_DRUCKER_PRAGER || m == M_NACC;
+    return m <= M_GRANULAR_FLUID;  // every ConstitutiveModel id (materials/mod.rs:53-66)
 }
 
 // LcgRng (spacetime/solver/mod.rs:154-175)
@@ -282,7 +281,7 @@ StepLaunch make_launch(emerge_sim *s) {
     L.density_mode = density;
     L.use_window = s->use_window;
     L.model_mask = 1u << M_FALLBACK;
-    for (const auto &m : s->mats) L.model_mask |= 1u << m.model;
+    for (const auto &m : s->mats) L.model_mask |= model_bits(m);
     L.fast = s->deterministic ? 0 : 1;
     L.cl = closure_args(s->closure);
     L.stream = s->stream;
@@ -293,9 +292,11 @@ void update_material_flags(emerge_sim *s) {
     s->lf.temperature = 0;
     s->lf.activation = 0;
     for (const auto &m : s->mats) {
-        if (m.model == M_NEOHOOKEAN && m.thermal_expansion != 0.0f) s->lf.temperature = 1;
+        const bool thermal_solid = m.model == M_NEOHOOKEAN || m.model == M_COROTATED ||
+                                   m.model == M_VISCOELASTIC;
+        if (thermal_solid && m.thermal_expansion != 0.0f) s->lf.temperature = 1;
         if (m.model == M_FLUID && m.thermal_viscosity_coeff > 0.0f) s->lf.temperature = 1;
-        if (m.model == M_NEOHOOKEAN && m.active_stress_coeff > 0.0f) s->lf.activation = 1;
+        if (activation_scale(m) > 0.0f) s->lf.activation = 1;
     }
 }
 

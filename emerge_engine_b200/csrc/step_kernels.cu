@@ -454,7 +454,8 @@ void launch_particle_pass(const StepLaunch &L, const LoadFlagsHost &lfh, int mod
     case MASK_SOLID: k_particle<MASK_SOLID><<<grid, THREADS, 0, L.stream>>>(a); break;
     case MASK_SOLID_FLUID: k_particle<MASK_SOLID_FLUID><<<grid, THREADS, 0, L.stream>>>(a); break;
     case MASK_GRANULAR: k_particle<MASK_GRANULAR><<<grid, THREADS, 0, L.stream>>>(a); break;
-    default: k_particle<ALL_MODELS><<<grid, THREADS, 0, L.stream>>>(a); break;
+    case ALL_MODELS: k_particle<ALL_MODELS><<<grid, THREADS, 0, L.stream>>>(a); break;
+    default: k_particle<FULL_MODELS><<<grid, THREADS, 0, L.stream>>>(a); break;
     }
 }
 

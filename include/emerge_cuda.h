@@ -104,8 +104,11 @@ typedef struct emerge_sim_config {
 
 /* MaterialParams (matter/materials/params.rs:10-101, 96 bytes).  `model` carries
  * MaterialModel::constitutive_model() (materials/mod.rs:53-66), NOT params().model:
- * NaccMaterial::params() reports NeoHookean (nacc.rs:300-314).  Supported models:
- * 0 Fallback, 1 Fluid, 2 NeoHookean, 4 Snow, 5 DruckerPrager, 10 Nacc. */
+ * NaccMaterial::params() reports NeoHookean (nacc.rs:300-314).  Every model id 0-11 runs
+ * on the device, each reading its own params() packing.  A Fluid slot with
+ * compression_limit > 0 is a BinghamFluidMaterial (bingham.rs params() puts yield_stress
+ * there); its critical shear rate is the constructor's 1e-4.  Viscoelastic reads
+ * thermal_expansion from the thermal_expansion field, which its params() leaves 0. */
 typedef struct emerge_material_params {
     uint32_t model;
     float lambda;

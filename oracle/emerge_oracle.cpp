@@ -97,6 +97,21 @@ inline float fclamp(float x, float lo, float hi) {
     if (x > hi) x = hi;
     return x;
 }
+
+// Transcendentals.  By default the C library's f32 functions, which is what the Rust
+// reference's f32::exp / ln / powf / sin / sinh call on Linux.  Those are not always
+// correctly rounded (glibc's logf differs from the correctly rounded result in the last
+// bit for a few percent of arguments near 1); with oracle_set_correctly_rounded(1) each
+// is instead evaluated in double and rounded once, which isolates the algorithm from the
+// library's last-bit behaviour.
+int g_correctly_rounded = 0;
+inline float m_exp(float x) { return g_correctly_rounded ? float(std::exp(double(x))) : std::exp(x); }
+inline float m_log(float x) { return g_correctly_rounded ? float(std::log(double(x))) : std::log(x); }
+inline float m_sin(float x) { return g_correctly_rounded ? float(std::sin(double(x))) : std::sin(x); }
+inline float m_sinh(float x) { return g_correctly_rounded ? float(std::sinh(double(x))) : std::sinh(x); }
+inline float m_pow(float x, float y) {
+    return g_correctly_rounded ? float(std::pow(double(x), double(y))) : std::pow(x, y);
+}
 // glam normalize_or_zero: self * (1 / length) when finite and > 0
 inline V2 normalize_or_zero(V2 a) {
     float rcp = 1.0f / length(a);
@@ -232,15 +247,15 @@ using P = oracle_particle;
 // DruckerPragerMaterial::alpha (sand.rs:135-141)
 float dp_alpha(const Mat &m, float q) {
     float phi = m.friction_angle +
-                (m.hardening_peak * q - m.friction_residual) * std::exp(-m.hardening_decay * q);
-    float s = std::sin(phi);
+                (m.hardening_peak * q - m.friction_residual) * m_exp(-m.hardening_decay * q);
+    float s = m_sin(phi);
     return std::sqrt(2.0f / 3.0f) * (2.0f * s) / (3.0f - s);
 }
 
 // DruckerPragerMaterial::project (sand.rs:156-194)
 bool dp_project(const Mat &m, V2 sigma_in, float lvs, float q, V2 &out, float &dq) {
     V2 sigma = vmax(vabs(sigma_in), splat(LOG_CLAMP));
-    V2 eps = v2(std::log(sigma.x) + lvs * 0.5f, std::log(sigma.y) + lvs * 0.5f);
+    V2 eps = v2(m_log(sigma.x) + lvs * 0.5f, m_log(sigma.y) + lvs * 0.5f);
     float trace = eps.x + eps.y;
     V2 dev = sub(eps, splat(trace * 0.5f));
     float dev_norm = length(dev);
@@ -255,7 +270,7 @@ bool dp_project(const Mat &m, V2 sigma_in, float lvs, float q, V2 &out, float &d
     float gamma = dev_norm + ratio * trace * alpha - cohesion_term;
     if (gamma <= 0.0f) return false;
     V2 h = sub(eps, smul(gamma, divs(dev, dev_norm)));
-    out = v2(std::exp(h.x), std::exp(h.y));
+    out = v2(m_exp(h.x), m_exp(h.y));
     dq = gamma;
     return true;
 }
@@ -273,7 +288,7 @@ void nacc_project(const Mat &m, M2 f, float alpha, M2 &f_out, float &alpha_out) 
     V2 sv = sigma;
     V2 sv_sq = mul(sv, sv);
     float sv_sq_trace = sv_sq.x + sv_sq.y;
-    float p0 = m.kappa * (1.0e-5f + std::sinh(xi * fmax_(-alpha, 0.0f)));
+    float p0 = m.kappa * (1.0e-5f + m_sinh(xi * fmax_(-alpha, 0.0f)));
     float j_e_tr = fmax_(sv.x * sv.y, 1.0e-6f);
     V2 s_tr = smul(m.mu * (1.0f / j_e_tr), sub(sv_sq, splat(sv_sq_trace * 0.5f)));
     float psi_kappa = m.kappa * 0.5f * (j_e_tr - 1.0f / j_e_tr);
@@ -281,16 +296,16 @@ void nacc_project(const Mat &m, M2 f, float alpha, M2 &f_out, float &alpha_out) 
     bool hard = m.hardening_enabled != 0;
     if (p_tr > p0) {
         float j_n1 = std::sqrt(fmax_(-2.0f * p0 / m.kappa + 1.0f, 1.0e-8f));
-        float sv_new = std::pow(j_n1, 0.5f);
-        if (hard) alpha += std::log(j_e_tr / j_n1);
+        float sv_new = m_pow(j_n1, 0.5f);
+        if (hard) alpha += m_log(j_e_tr / j_n1);
         f_out = reconstruct(u, splat(sv_new), vt);
         alpha_out = alpha;
         return;
     }
     if (p_tr < -beta * p0) {
         float j_n1 = std::sqrt(fmax_(2.0f * beta * p0 / m.kappa + 1.0f, 1.0e-8f));
-        float sv_new = std::pow(j_n1, 0.5f);
-        if (hard) alpha += std::log(j_e_tr / j_n1);
+        float sv_new = m_pow(j_n1, 0.5f);
+        if (hard) alpha += m_log(j_e_tr / j_n1);
         f_out = reconstruct(u, splat(sv_new), vt);
         alpha_out = alpha;
         return;
@@ -318,7 +333,7 @@ void nacc_project(const Mat &m, M2 f, float alpha, M2 &f_out, float &alpha_out) 
         float p2 = p_c + l2 * dir.x;
         float p_x = ((p_tr - p_c) * (p1 - p_c) > 0.0f) ? p1 : p2;
         float j_e_x = std::sqrt(fmax_(std::fabs(-2.0f * p_x / m.kappa + 1.0f), 1.0e-8f));
-        if (j_e_x > 1.0e-4f) alpha += std::log(j_e_tr / j_e_x);
+        if (j_e_x > 1.0e-4f) alpha += m_log(j_e_tr / j_e_x);
     }
     float scale = std::sqrt(fmax_(-y1 / fmax_(y0, 1.0e-10f), 0.0f)) * (j_e_tr / m.mu);
     V2 b_n1 = add(smul(scale, normalize_or_zero(s_tr)), splat(sv_sq_trace / 2.0f));
@@ -335,7 +350,7 @@ M2 kirchhoff_stress(const Mat &m, const P &p) {
         float j = det(f);
         if (j <= MIN_J) return zero2();
         float t_scale = 1.0f + m.thermal_expansion * p.temperature;
-        float damage_scale = std::exp(-m.damage_softening_rate * p.friction_hardening);
+        float damage_scale = m_exp(-m.damage_softening_rate * p.friction_hardening);
         float mu = m.mu * t_scale * damage_scale;
         float lambda = m.lambda * t_scale * damage_scale;
         M2 b = mm(f, transpose(f));
@@ -343,7 +358,7 @@ M2 kirchhoff_stress(const Mat &m, const P &p) {
         M2 dev_b = msub(b, diag(splat(tr_b * 0.5f)));
         float k = lambda + mu;
         M2 dev_stress = smscale(mu / j, dev_b);
-        M2 vol_stress = smscale(k * std::log(j), ident());
+        M2 vol_stress = smscale(k * m_log(j), ident());
         M2 viscous = zero2();
         if (m.viscosity > 0.0f) {
             M2 c = load_m(p.c);
@@ -358,12 +373,12 @@ M2 kirchhoff_stress(const Mat &m, const P &p) {
     case FLUID: {  // fluid.rs:135-191
         float density = fmin_(fmax_(p.density, m.fluid_min_density), m.rest_density * 2.0f);
         float pressure = fmax_(
-            m.eos_stiffness * (std::pow(density / m.rest_density, m.eos_power) - 1.0f),
+            m.eos_stiffness * (m_pow(density / m.rest_density, m.eos_power) - 1.0f),
             m.pressure_floor);
         M2 stress = diag(splat(-pressure));
         float eff_visc = m.dynamic_viscosity;
         if (m.thermal_viscosity_coeff > 0.0f)
-            eff_visc = m.dynamic_viscosity * std::exp(-m.thermal_viscosity_coeff * p.temperature);
+            eff_visc = m.dynamic_viscosity * m_exp(-m.thermal_viscosity_coeff * p.temperature);
         M2 c = load_m(p.c);
         M2 sym = madd(c, transpose(c));
         float div_v = sym.xa.x + sym.ya.y;
@@ -410,19 +425,98 @@ M2 kirchhoff_stress(const Mat &m, const P &p) {
         M2 vol_stress = smscale(m.kappa * 0.5f * (j * j - 1.0f), ident());
         return madd(dev_stress, vol_stress);
     }
+    case COROTATED: {  // corotated.rs:61-77
+        float j = det(f);
+        if (j <= MIN_J) return zero2();
+        M2 r = polar(f);
+        float h = p.hardening_scale;
+        float t_scale = 1.0f + m.thermal_expansion * p.temperature;
+        float mu_eff = m.mu * h * t_scale;
+        float lambda_eff = m.lambda * h * t_scale;
+        return madd(mm(smscale(2.0f * mu_eff, msub(f, r)), transpose(f)),
+                    smscale(lambda_eff * (j - 1.0f) * j, ident()));
+    }
+    case VON_MISES:    // von_mises.rs:96-104
+    case RANKINE:      // rankine.rs kirchhoff_stress
+    case DP_MUI: {     // sand_mui.rs kirchhoff_stress
+        float j = det(f);
+        if (j <= MIN_J) return zero2();
+        M2 r = polar(f);
+        return madd(mm(smscale(2.0f * m.mu, msub(f, r)), transpose(f)),
+                    smscale(m.lambda * (j - 1.0f) * j, ident()));
+    }
+    case VISCOELASTIC: {  // viscoelastic.rs kirchhoff_stress
+        float j = fmin_(fmax_(f.xa.x * f.ya.y - f.xa.y * f.ya.x, m.j_min), 1.0f / m.j_min);
+        float t_scale = 1.0f + m.thermal_expansion * p.temperature;
+        float mu = m.mu * t_scale;
+        float lambda = m.lambda * t_scale;
+        M2 b = mm(f, transpose(f));
+        M2 elastic = madd(smscale(mu, msub(b, ident())), diag(splat(lambda * m_log(j))));
+        M2 c = load_m(p.c);
+        M2 d = mscale(madd(c, transpose(c)), 0.5f);
+        float trace = d.xa.x + d.ya.y;
+        M2 d_dev = msub(d, diag(splat(trace * 0.5f)));
+        return madd(elastic, smscale(m.viscosity * t_scale, d_dev));
+    }
+    case GRANULAR_FLUID: {  // granular_fluid.rs kirchhoff_stress
+        float j = fmax_(det(f), MIN_J);
+        float density = fmax_(m.rest_density / j, 1.0e-6f);
+        float ratio = fmax_(density / fmax_(m.rest_density, 1.0e-6f), 1.0e-6f);
+        float pressure = fmax_(m.eos_stiffness * (m_pow(ratio, m.eos_power) - 1.0f),
+                               m.pressure_floor);
+        float h = p.hardening_scale;
+        M2 r = polar(f);
+        float mu_eff = m.mu * h;
+        M2 coro = mm(smscale(2.0f * mu_eff, msub(f, r)), transpose(f));
+        float tr = coro.xa.x + coro.ya.y;
+        M2 dev_coro = msub(coro, diag(splat(tr * 0.5f)));
+        M2 lam_vol = smscale(m.lambda * h * (j - 1.0f) * j, ident());
+        return madd(madd(diag(splat(-pressure)), dev_coro), lam_vol);
+    }
     default:  // FallbackMaterial (materials/mod.rs:362-366): zero stress
         return zero2();
     }
 }
 
-// MaterialModel::activation_scale (mod.rs:181-183): NeoHookean overrides it.
+// BinghamFluidMaterial::kirchhoff_stress (bingham.rs): Tait pressure plus the
+// Bingham deviatoric stress with apparent viscosity yield / shear_rate + viscosity.
+M2 bingham_kirchhoff(const Mat &m, const P &p) {
+    float density = fmin_(fmax_(p.density, m.fluid_min_density), m.rest_density * 2.0f);
+    float pressure = fmax_(
+        m.eos_stiffness * (m_pow(density / m.rest_density, m.eos_power) - 1.0f), m.pressure_floor);
+    M2 hydrostatic = diag(splat(-pressure));
+    M2 c = load_m(p.c);
+    M2 d = mscale(madd(c, transpose(c)), 0.5f);
+    float trace = d.xa.x + d.ya.y;
+    M2 d_dev = msub(d, diag(splat(trace * 0.5f)));
+    float dxx = d_dev.xa.x, dyy = d_dev.ya.y, dxy = d_dev.xa.y;
+    float d_sq = dxx * dxx + dyy * dyy + 2.0f * dxy * dxy;
+    float shear_rate = std::sqrt(2.0f * d_sq);
+    M2 deviatoric = zero2();
+    if (!(shear_rate < m.critical_shear_rate)) {
+        float eta_app = m.bingham_yield_stress / shear_rate + m.dynamic_viscosity;
+        deviatoric = mscale(d_dev, eta_app);
+    }
+    M2 surface = zero2();
+    if (m.surface_tension_coeff != 0.0f) {
+        M2 f = load_m(p.f);
+        float j = f.xa.x * f.ya.y - f.xa.y * f.ya.x;
+        surface = diag(splat(m.surface_tension_coeff * j));
+    }
+    return madd(madd(hydrostatic, deviatoric), surface);
+}
+
+// MaterialModel::activation_scale (mod.rs:181-183): NeoHookean, Corotated and
+// Viscoelastic override it.
 inline float activation_scale(const Mat &m) {
-    return m.model == NEOHOOKEAN ? m.active_stress_coeff : 0.0f;
+    return (m.model == NEOHOOKEAN || m.model == COROTATED || m.model == VISCOELASTIC)
+               ? m.active_stress_coeff
+               : 0.0f;
 }
 
 // combined_kirchhoff_stress (spacetime/transfer.rs:77-104)
 M2 combined_kirchhoff_stress(const Mat &m, const P &p) {
-    M2 tau = kirchhoff_stress(m, p);
+    M2 tau = (m.model == FLUID && m.bingham) ? bingham_kirchhoff(m, p) : kirchhoff_stress(m, p);
     float coeff = activation_scale(m);
     if (p.activation <= 0.0f || coeff <= 0.0f) return tau;
     bool isotropic = m.model == VISCOELASTIC;
@@ -447,7 +541,8 @@ M2 combined_kirchhoff_stress(const Mat &m, const P &p) {
 
 // MaterialModel::stress_volume
 inline float stress_volume(const Mat &m, const P &p) {
-    if (m.model == FLUID) return fmax_(p.volume, m.fluid_min_volume);  // fluid.rs:193-195
+    if (m.model == FLUID) return fmax_(p.volume, m.fluid_min_volume);  // fluid.rs:193-195, bingham.rs
+    if (m.model == GRANULAR_FLUID) return fmax_(p.volume, 1.0e-6f);     // granular_fluid.rs
     return p.initial_volume;  // mod.rs:114 default and every other in-scope model
 }
 
@@ -471,7 +566,7 @@ float timestep_bound(const Mat &m, float density, float h, float cell, float mat
         float d = fmax_(density, m.fluid_min_density);
         float ratio = fmax_(d / fmax_(m.rest_density, m.fluid_min_density), MIN_DENSITY_RATIO);
         float dt_bound = INFINITY;
-        float c2 = m.eos_stiffness * m.eos_power * std::pow(ratio, m.eos_power - 1.0f) /
+        float c2 = m.eos_stiffness * m.eos_power * m_pow(ratio, m.eos_power - 1.0f) /
                    fmax_(m.rest_density, m.fluid_min_density);
         if (std::isfinite(c2) && c2 > F32_EPS)
             dt_bound = fmin_(dt_bound, mat_cfl * cell / std::sqrt(c2));
@@ -488,6 +583,23 @@ float timestep_bound(const Mat &m, float density, float h, float cell, float mat
     case NACC: {  // nacc.rs:279-298
         float lambda = m.kappa - m.mu;
         return elastic_wave_dt(lambda, m.mu, h, density, m.nacc_min_density, cell, mat_cfl);
+    }
+    case COROTATED:       // corotated.rs timestep_bound
+    case GRANULAR_FLUID:  // granular_fluid.rs timestep_bound
+        return elastic_wave_dt(m.lambda, m.mu, h, density, MIN_J, cell, mat_cfl);
+    case VON_MISES:  // von_mises.rs, rankine.rs, sand_mui.rs timestep_bound
+    case RANKINE:
+    case DP_MUI:
+        return elastic_wave_dt(m.lambda, m.mu, 1.0f, density, MIN_J, cell, mat_cfl);
+    case VISCOELASTIC: {  // viscoelastic.rs timestep_bound
+        float elastic_dt = elastic_wave_dt(m.lambda, m.mu, 1.0f, density, 1.0e-6f, cell, mat_cfl);
+        float viscous_dt = INFINITY;
+        if (m.viscosity > 0.0f) {
+            float d = fmax_(density, 1.0e-6f);
+            float kinematic = m.viscosity / d;
+            if (kinematic > F32_EPS) viscous_dt = visc_cfl * cell * cell / kinematic;
+        }
+        return fmin_(elastic_dt, viscous_dt);
     }
     default:
         return INFINITY;
@@ -508,9 +620,39 @@ void init_particle(const Mat &m, P &p) {
     case NACC:  // nacc.rs:271-273
         p.log_volume_strain = 0.0f;
         break;
+    case COROTATED:  // corotated.rs init_particle
+        p.hardening_scale = 1.0f;
+        p.plastic_volume_ratio = 1.0f;
+        break;
+    case GRANULAR_FLUID:  // granular_fluid.rs init_particle
+        p.plastic_volume_ratio = 1.0f;
+        p.hardening_scale = 1.0f;
+        break;
+    case DP_MUI:  // sand_mui.rs init_particle
+        p.friction_hardening = m.mu_static;
+        break;
     default:
         break;
     }
+}
+
+// Hencky strains of singular values (utils.rs hencky_strains).
+inline V2 hencky(V2 sigma) {
+    V2 s = vmax(vabs(sigma), splat(LOG_CLAMP));
+    return v2(m_log(s.x), m_log(s.y));
+}
+
+// stress_to_hencky (utils.rs): principal Kirchhoff stress -> Hencky strain.
+inline V2 stress_to_hencky(V2 tau, float lambda, float mu) {
+    float d = 4.0f * mu * (mu + lambda);
+    float a = 2.0f * mu + lambda;
+    return v2((a * tau.x - lambda * tau.y) / d, (a * tau.y - lambda * tau.x) / d);
+}
+
+// rankine_damage_saturation_point (utils.rs)
+inline float rankine_saturation(float softening_rate) {
+    if (softening_rate <= 0.0f) return INFINITY;
+    return -m_log(0.05f) / softening_rate;
 }
 
 // Shared tail of the elastoplastic updates: volume/density from J.
@@ -556,10 +698,10 @@ void update_particle(const Mat &m, P &p, float dt) {
             float new_det = proj.x * proj.y;
             float diff = new_det - prev_det;
             float corrected = diff > 0.0f ? new_det : prev_det + diff * m.volume_correction;
-            p.log_volume_strain += std::log(prev_det) - std::log(corrected);
+            p.log_volume_strain += m_log(prev_det) - m_log(corrected);
             float q_max = 5.0f / fmax_(m.hardening_decay, 1e-6f);
             p.friction_hardening = fmin_(p.friction_hardening + dq, q_max);
-            if (m.dilatancy_angle > 0.0f) p.log_volume_strain += std::sin(m.dilatancy_angle) * dq;
+            if (m.dilatancy_angle > 0.0f) p.log_volume_strain += m_sin(m.dilatancy_angle) * dq;
             new_sigma = proj;
         }
         new_sigma = vabs(new_sigma);
@@ -581,8 +723,134 @@ void update_particle(const Mat &m, P &p, float dt) {
         float jp_new = p.plastic_volume_ratio * (sigma.x * sigma.y) / (sigma_c.x * sigma_c.y);
         p.plastic_volume_ratio = fclamp(jp_new, m.min_plastic_jacobian, m.max_plastic_jacobian);
         p.hardening_scale =
-            fclamp(std::exp(m.hardening_exponent * (1.0f - p.plastic_volume_ratio)), 0.1f, 7.0f);
+            fclamp(m_exp(m.hardening_exponent * (1.0f - p.plastic_volume_ratio)), 0.1f, 7.0f);
         M2 f = mm(mm(u, diag(sigma_c)), vt);
+        store_m(p.f, f);
+        sync_volume_density(p, f);
+        break;
+    }
+    case COROTATED:      // corotated.rs update_particle
+    case VISCOELASTIC: {  // viscoelastic.rs update_particle
+        M2 fp_new = madd(ident(), smscale(dt, load_m(p.c)));
+        M2 f = mm(fp_new, load_m(p.f));
+        store_m(p.f, f);
+        sync_volume_density(p, f);
+        break;
+    }
+    case VON_MISES: {  // von_mises.rs update_particle
+        M2 f_trial = mm(madd(ident(), smscale(dt, load_m(p.c))), load_m(p.f));
+        M2 u, vt;
+        V2 sigma;
+        svd2(f_trial, u, sigma, vt);
+        V2 eps = hencky(sigma);
+        float tr = eps.x + eps.y;
+        V2 dev = sub(eps, splat(tr * 0.5f));
+        float dev_norm = length(dev);
+        float kappa = p.friction_hardening;
+        float effective_yield = m.yield_stress + m.hardening_modulus * kappa;
+        float elastic_dev = 2.0f * m.mu * dev_norm;
+        V2 sigma_new = sigma;
+        if (elastic_dev > effective_yield && dev_norm > LOG_CLAMP) {
+            float denom = 2.0f * m.mu + m.hardening_modulus;
+            float gamma = denom > F32_EPS ? (elastic_dev - effective_yield) / denom : 0.0f;
+            p.friction_hardening = kappa + gamma;
+            V2 eps_proj = add(muls(dev, effective_yield / elastic_dev), splat(tr * 0.5f));
+            sigma_new = v2(m_exp(eps_proj.x), m_exp(eps_proj.y));
+        }
+        M2 f = reconstruct(u, sigma_new, vt);
+        store_m(p.f, f);
+        sync_volume_density(p, f);
+        break;
+    }
+    case RANKINE: {  // rankine.rs update_particle
+        M2 f_trial = mm(madd(ident(), smscale(dt, load_m(p.c))), load_m(p.f));
+        M2 u, vt;
+        V2 sigma;
+        svd2(f_trial, u, sigma, vt);
+        V2 eps = hencky(sigma);
+        float a = 2.0f * m.mu + m.lambda;
+        V2 tau = v2(a * eps.x + m.lambda * eps.y, m.lambda * eps.x + a * eps.y);
+        float damage = p.friction_hardening;
+        float ts = m.tensile_strength;
+        float t_eff = fmax_(ts * m_exp(-m.softening_rate * damage), ts * 0.05f);
+        bool t1 = tau.x > t_eff, t2 = tau.y > t_eff;
+        V2 sigma_new = sigma;
+        if (t1 || t2) {
+            V2 tau_proj = (t1 && t2) ? splat(t_eff) : (t1 ? v2(t_eff, tau.y) : v2(tau.x, t_eff));
+            V2 eps_proj = stress_to_hencky(tau_proj, m.lambda, m.mu);
+            V2 eps_trial = stress_to_hencky(tau, m.lambda, m.mu);
+            p.friction_hardening = fmin_(damage + length(sub(eps_trial, eps_proj)),
+                                         rankine_saturation(m.softening_rate));
+            sigma_new = v2(m_exp(eps_proj.x), m_exp(eps_proj.y));
+        }
+        M2 f = reconstruct(u, sigma_new, vt);
+        store_m(p.f, f);
+        sync_volume_density(p, f);
+        break;
+    }
+    case DP_MUI: {  // sand_mui.rs update_particle
+        const float SQRT_2 = 1.41421356237f;  // std::f32::consts::SQRT_2
+        M2 f_trial = mm(madd(ident(), smscale(dt, load_m(p.c))), load_m(p.f));
+        M2 u, vt;
+        V2 sigma;
+        svd2(f_trial, u, sigma, vt);
+        V2 eps = hencky(sigma);
+        float tr = eps.x + eps.y;
+        float k_2d = m.lambda + m.mu;
+        float p_trial = -k_2d * tr;
+        if (p_trial <= 0.0f) {
+            M2 f = reconstruct(u, v2(1.0f, 1.0f), vt);
+            store_m(p.f, f);
+            p.friction_hardening = m.mu_static;
+            sync_volume_density(p, f);
+            break;
+        }
+        V2 dev = sub(eps, splat(tr * 0.5f));
+        float dev_norm = length(dev);
+        float q_trial = SQRT_2 * m.mu * dev_norm;
+        float q_yield = m.mu_static * p_trial;
+        if (q_trial <= q_yield || dev_norm < F32_EPS) {
+            M2 f = reconstruct(u, sigma, vt);
+            store_m(p.f, f);
+            p.friction_hardening = m.mu_static;
+            sync_volume_density(p, f);
+            break;
+        }
+        float delta_q = q_trial - q_yield;
+        float sqrt_p = std::sqrt(p_trial);
+        float a = m.mu * dt;
+        float b = p_trial * (m.mu_dynamic - m.mu_static) + a * m.inertial_q * sqrt_p - delta_q;
+        float c = -delta_q * m.inertial_q * sqrt_p;
+        float gamma_dot = fmax_((-b + std::sqrt(b * b - 4.0f * a * c)) / (2.0f * a), 0.0f);
+        float mu_i = gamma_dot > F32_EPS
+                         ? m.mu_static + (m.mu_dynamic - m.mu_static) /
+                                             (m.inertial_q * sqrt_p / gamma_dot + 1.0f)
+                         : m.mu_static;
+        float delta_gamma = gamma_dot * dt;
+        V2 n_hat = v2(dev.x / dev_norm, dev.y / dev_norm);
+        V2 eps_new = sub(eps, muls(n_hat, delta_gamma / SQRT_2));
+        M2 f = reconstruct(u, v2(m_exp(eps_new.x), m_exp(eps_new.y)), vt);
+        store_m(p.f, f);
+        p.friction_hardening = mu_i;
+        sync_volume_density(p, f);
+        break;
+    }
+    case GRANULAR_FLUID: {  // granular_fluid.rs update_particle
+        M2 f_trial = mm(madd(ident(), smscale(dt, load_m(p.c))), load_m(p.f));
+        M2 f = f_trial;
+        if (m.compression_limit > 0.0f || m.stretch_limit > 0.0f) {
+            M2 u, vt;
+            V2 sigma;
+            svd2(f_trial, u, sigma, vt);
+            float lo = 1.0f - m.compression_limit, hi = 1.0f + m.stretch_limit;
+            V2 sigma_c = v2(fclamp(sigma.x, lo, hi), fclamp(sigma.y, lo, hi));
+            float jp_new = p.plastic_volume_ratio * (sigma.x * sigma.y) /
+                           fmax_(sigma_c.x * sigma_c.y, 1.0e-10f);
+            p.plastic_volume_ratio = fclamp(jp_new, m.min_plastic_jacobian, m.max_plastic_jacobian);
+            p.hardening_scale =
+                fclamp(m_exp(m.hardening_exponent * (1.0f - p.plastic_volume_ratio)), 0.1f, 7.0f);
+            f = mm(mm(u, diag(sigma_c)), vt);
+        }
         store_m(p.f, f);
         sync_volume_density(p, f);
         break;
@@ -1310,6 +1578,8 @@ void oracle_axis_weights(float d, float w[3]) { axis_weights(d, w); }
 void oracle_kirchhoff(const oracle_material *m, const oracle_particle *p, float tau[4]) {
     store_m(tau, combined_kirchhoff_stress(*m, *p));
 }
+
+void oracle_set_correctly_rounded(int on) { g_correctly_rounded = on ? 1 : 0; }
 
 void oracle_update_particle(const oracle_material *m, oracle_particle *p, float dt) {
     update_particle(*m, *p, dt);

@@ -141,6 +141,22 @@ typedef struct oracle_material {
     float kappa, friction, nacc_cohesion, hardening_factor;
     uint32_t hardening_enabled;
     float nacc_min_density;
+    /* Corotated (corotated.rs:16-27) reuses lambda, mu, thermal_expansion,
+     * active_stress_coeff; VonMises (von_mises.rs:29-38) */
+    float yield_stress, hardening_modulus;
+    /* Rankine (rankine.rs) */
+    float tensile_strength, softening_rate;
+    /* MuIRheology (sand_mui.rs) */
+    float mu_static, mu_dynamic, inertial_q;
+    /* Viscoelastic (viscoelastic.rs) reuses lambda, mu, viscosity, active_stress_coeff,
+     * thermal_expansion */
+    float j_min;
+    /* BinghamFluid (bingham.rs): model FLUID with bingham = 1; reuses the fluid fields */
+    float bingham_yield_stress, critical_shear_rate;
+    uint32_t bingham;
+    /* GranularFluid (granular_fluid.rs) reuses lambda, mu, rest_density, eos_stiffness,
+     * eos_power, pressure_floor and the snow fields hardening_exponent, compression_limit,
+     * stretch_limit, min_plastic_jacobian, max_plastic_jacobian */
 } oracle_material;
 
 typedef struct oracle_sim oracle_sim;
@@ -166,6 +182,9 @@ int oracle_init_with_spawn(oracle_sim *s, const oracle_spawn *spawn);
 /* Raw particle append (active, in order), no density pass. */
 int oracle_push_particles(oracle_sim *s, const oracle_particle *p, uint64_t n);
 void oracle_step(oracle_sim *s, uint32_t n_steps);
+/* 0 (default): exp/log/pow/sin/sinh from the C library, as the Rust reference calls them;
+ * 1: evaluated in double and rounded once to f32 (process-wide switch). */
+void oracle_set_correctly_rounded(int on);
 uint64_t oracle_particle_count(const oracle_sim *s);
 void oracle_read_particles(const oracle_sim *s, oracle_particle *out);
 void oracle_write_particles(oracle_sim *s, const oracle_particle *in);

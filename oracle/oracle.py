@@ -6,6 +6,7 @@ as the parity checker / timed CPU baseline.  `OracleSimulation` has the same met
 """
 from __future__ import annotations
 
+import contextlib
 import ctypes
 import os
 import subprocess
@@ -35,7 +36,12 @@ _MAT_FIELDS = (
 class OracleMaterialC(Structure):
     """`oracle_material` (oracle/emerge_oracle.h)."""
     _fields_ = ([("model", c_uint32)] + [(n, c_float) for n in _MAT_FIELDS]
-                + [("hardening_enabled", c_uint32), ("nacc_min_density", c_float)])
+                + [("hardening_enabled", c_uint32), ("nacc_min_density", c_float)]
+                + [(n, c_float) for n in ("yield_stress", "hardening_modulus", "tensile_strength",
+                                          "softening_rate", "mu_static", "mu_dynamic",
+                                          "inertial_q", "j_min", "bingham_yield_stress",
+                                          "critical_shear_rate")]
+                + [("bingham", c_uint32)])
 
 
 def oracle_material(m: Material) -> OracleMaterialC:
@@ -82,6 +88,7 @@ def lib() -> ctypes.CDLL:
             "oracle_last_timing_us": (None, [c_void_p, P(c_double)]),
             "oracle_set_threads": (c_int, [c_int]),
             "oracle_svd2": (None, [P(c_float), P(c_float), P(c_float), P(c_float)]),
+            "oracle_set_correctly_rounded": (None, [c_int]),
             "oracle_polar": (None, [P(c_float), P(c_float)]),
             "oracle_axis_weights": (None, [c_float, P(c_float)]),
             "oracle_kirchhoff": (None, [P(OracleMaterialC), P(Particle), P(c_float)]),
@@ -243,3 +250,14 @@ class OracleSimulation:
 
 def set_threads(n: int) -> int:
     return int(lib().oracle_set_threads(int(n)))
+
+
+@contextlib.contextmanager
+def correctly_rounded_math():
+    """Within the block the oracle evaluates exp/log/pow/sin/sinh in double and rounds once
+    (oracle_set_correctly_rounded); outside it, the C library's f32 functions."""
+    lib().oracle_set_correctly_rounded(1)
+    try:
+        yield
+    finally:
+        lib().oracle_set_correctly_rounded(0)

@@ -7,9 +7,11 @@ from __future__ import annotations
 
 import numpy as np
 
-from emerge_engine_b200 import (DruckerPragerMaterial, NaccMaterial, NeoHookeanMaterial,
-                                NewtonianFluidMaterial, SimConfig, SlipBoundary, SpawnRegion,
-                                StomakhinMaterial)
+from emerge_engine_b200 import (BinghamFluidMaterial, CorotatedMaterial, DruckerPragerMaterial,
+                                GranularFluidMaterial, MuIRheologyMaterial, NaccMaterial,
+                                NeoHookeanMaterial, NewtonianFluidMaterial, RankineMaterial,
+                                SimConfig, SlipBoundary, SpawnRegion, StomakhinMaterial,
+                                ViscoelasticMaterial, VonMisesMaterial, lame_from_young)
 
 
 def quickstart(sim_cls, **sim_kw):
@@ -146,3 +148,53 @@ def batched_scenes(sim_cls, n_scenes=256, seed=7, grid_range=(64, 256), n_range=
         sim.add_body(s)
         sims.append(sim)
     return sims
+
+
+# One material per constitutive model beyond the core set, with parameters that put it in
+# its plastic / viscous / yield regime within the first frame: (constructor, mass override
+# for 0.5-cell spacing or None, whether particles carry temperature and activation).
+ZOO = {
+    "corotated": (lambda: CorotatedMaterial(*lame_from_young(2e4, 0.3), thermal_expansion=0.02,
+                                            active_stress_coeff=40.0), None, True),
+    "von_mises": (lambda: VonMisesMaterial.with_hardening(*lame_from_young(2e4, 0.3), 60.0, 400.0),
+                  None, False),
+    "rankine": (lambda: RankineMaterial.from_young_modulus(2e4, 0.3, 30.0, 2.0), None, False),
+    "mu_i": (lambda: MuIRheologyMaterial.from_young_modulus(2e4, 0.3), None, False),
+    "viscoelastic": (lambda: ViscoelasticMaterial(*lame_from_young(2e4, 0.3), 4.0,
+                                                  active_stress_coeff=40.0, thermal_expansion=0.02),
+                     None, True),
+    "granular_fluid": (lambda: GranularFluidMaterial.saturated_loam(2e4, 0.3), 1.0 * 0.25, False),
+    "bingham": (lambda: BinghamFluidMaterial.medium_yield(1000.0, 1e4), 1000.0 * 0.25, False),
+}
+
+
+def material_zoo(sim_cls, kind, grid_res=96, seed=3, dt=0.05, gravity=-1.0, **sim_kw):
+    """One model of ZOO in a grid_res^2 grid: a pre-strained 40x24 block (F0 = [[1.04, 0],
+    [0.01, 0.95]], column-major x_axis (1.04, 0.01)) resting on the floor and a disk of
+    radius 10 with seeded random velocities in [-4, 4)^2, both at 4 particles per cell with
+    seeded jitter.  Where the model reads them, every particle gets temperature 1 and every
+    other particle activation 0.5 along (1, 0.3)."""
+    make, mass, active = ZOO[kind]
+    cfg = SimConfig.standard(grid_res, dt, (0.0, gravity))
+    t = cfg.boundary_thickness
+    sim = sim_cls.empty(cfg, **sim_kw).with_default_material(make())
+    a = SpawnRegion.for_sim(cfg)
+    a.spacing, a.box_size = 0.5, (40, 24)
+    a.box_center = (t + 4 + 20.0, t + 1 + 12.0)
+    a.initial_deformation_gradient = (1.04, 0.01, 0.0, 0.95)
+    a.position_jitter, a.rng_seed = 0.3, seed
+    b = SpawnRegion.for_sim(cfg).disk(10.0)
+    b.spacing, b.box_center = 0.5, (grid_res * 0.62, grid_res * 0.6)
+    b.initial_velocity_scale = 8.0
+    b.position_jitter, b.rng_seed = 0.3, seed + 1
+    for s in (a, b):
+        if mass is not None:
+            s.mass_override = mass
+        sim.add_body(s)
+    if active:
+        p = sim.particles()
+        p["temperature"] = 1.0
+        p["activation"][::2] = 0.5
+        p["activation_dir"][::2] = (1.0, 0.3)
+        sim.set_particles(p)
+    return sim
