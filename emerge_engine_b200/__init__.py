@@ -9,4 +9,7 @@ from .materials import (BinghamFluidMaterial, CorotatedMaterial,  # noqa: F401
                         MuIRheologyMaterial, NaccMaterial, NeoHookeanMaterial,
                         NewtonianFluidMaterial, RankineMaterial, StomakhinMaterial,
                         ViscoelasticMaterial, VonMisesMaterial, lame_from_young, to_radians)
+from .fields import (AabbConfinementField, BuoyancyField, ChemotaxisField,  # noqa: F401
+                     CoulombField, GravityWellField, LinearDragField, RadialConfinementField,
+                     UniformElectricField)
 from .simulation import Batch, DeterministicSimulation, MaterialRegistry, Simulation  # noqa: F401

@@ -87,6 +87,13 @@ class SimConfigC(Structure):
 assert ctypes.sizeof(SimConfigC) == 136
 
 
+class ForceFieldC(Structure):
+    """`emerge_force_field` (include/emerge_cuda.h), 48 bytes."""
+    _fields_ = [("kind", c_uint32), ("material_mask", c_uint32), ("material_filter", c_uint32),
+                ("count", c_uint32), ("data_offset", c_uint32), ("n_charges", c_uint32),
+                ("params", c_float * 6)]
+
+
 class MaterialParamsC(Structure):
     """`MaterialParams` (matter/materials/params.rs:10-101), 96 bytes."""
     _fields_ = [(name, c_uint32 if name == "model" else c_float) for name in (
@@ -182,6 +189,8 @@ ABI_FUNCTIONS = [
     ("emerge_cuda_last_global_error", c_char_p, []),
     ("emerge_cuda_set_materials", c_int, [SIM, POINTER(MaterialParamsC), c_uint32]),
     ("emerge_cuda_set_slip_boundaries", c_int, [SIM, POINTER(c_uint64), c_uint32]),
+    ("emerge_cuda_set_force_fields", c_int, [SIM, POINTER(ForceFieldC), c_uint32, POINTER(c_float),
+                                             c_uint64]),
     ("emerge_cuda_add_body", c_int, [SIM, POINTER(SpawnRegionC), POINTER(c_uint32)]),
     ("emerge_cuda_init_with_spawn", c_int, [SIM, POINTER(SpawnRegionC)]),
     ("emerge_cuda_add_particles", c_int, [SIM, c_void_p, c_uint64, c_int]),

@@ -81,6 +81,7 @@ struct GridView {
     float2 *acc_s;
     float2 *grid_v;
     uint8_t *tile_flag;
+    float2 *grid_vpre;  // ASFLIP pre-force velocities (allocated when asflip_blend > 0)
 };
 
 __host__ __device__ __forceinline__ int cell_index(int x, int y, int tpd) {

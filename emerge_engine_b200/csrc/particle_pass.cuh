@@ -151,15 +151,18 @@ __device__ __forceinline__ float2 centre_offset(const QW &w, float2 x) {
     return v2((static_cast<float>(w.bx) - x.x) + 0.5f, (static_cast<float>(w.by) - x.y) + 0.5f);
 }
 
-// Grid velocities of the 3 x 3 stencil; cells outside the domain read as zero.
+// Grid velocities (grid_v, or another float2 grid field) of the 3 x 3 stencil; cells
+// outside the domain read as zero.
 template <bool CHECK>
-__device__ __forceinline__ void load_stencil_v(const GridView &g, const QW &w, float2 (&nv)[3][3]) {
+__device__ __forceinline__ void load_stencil_v(const GridView &g, const QW &w, float2 (&nv)[3][3],
+                                               const float2 *field = nullptr) {
+    const float2 *base = field ? field : g.grid_v;
     int yp[3];
 #pragma unroll
     for (int k = 0; k < 3; ++k) yp[k] = cell_y_part(w.by + k - 1);
 #pragma unroll
     for (int gx = 0; gx < 3; ++gx) {
-        const float2 *row = g.grid_v + cell_x_part(w.bx + gx - 1, g.tpd);
+        const float2 *row = base + cell_x_part(w.bx + gx - 1, g.tpd);
 #pragma unroll
         for (int gy = 0; gy < 3; ++gy) {
             if (CHECK && !in_domain(w.bx + gx - 1, w.by + gy - 1, g.res))
@@ -170,12 +173,46 @@ __device__ __forceinline__ void load_stencil_v(const GridView &g, const QW &w, f
     }
 }
 
-// G2P phase 1 for one particle (transfer/g2p.rs:217-326 with ASFLIP, contact and
-// mixture gated off).  Returns 1 if the speed clamp fired.
+// ASFLIP's PIC gather of the pre-force grid velocities with the G2P weights
+// (transfer/g2p.rs:284-290); cells outside the domain read as zero.
+template <bool FAST>
+__device__ __forceinline__ float2 gather_pre_force(const GridView &g, const QW &w, bool inside) {
+    float2 old_v = v2(0.0f, 0.0f);
+    if constexpr (FAST) {
+        float2 nv[3][3];
+        if (inside)
+            load_stencil_v<false>(g, w, nv, g.grid_vpre);
+        else
+            load_stencil_v<true>(g, w, nv, g.grid_vpre);
+#pragma unroll
+        for (int gx = 0; gx < 3; ++gx) {
+            float2 r;
+            r.x = __fmaf_rn(w.wy[0], nv[gx][0].x, __fmaf_rn(w.wy[1], nv[gx][1].x, w.wy[2] * nv[gx][2].x));
+            r.y = __fmaf_rn(w.wy[0], nv[gx][0].y, __fmaf_rn(w.wy[1], nv[gx][1].y, w.wy[2] * nv[gx][2].y));
+            old_v.x = __fmaf_rn(w.wx[gx], r.x, old_v.x);
+            old_v.y = __fmaf_rn(w.wx[gx], r.y, old_v.y);
+        }
+    } else {
+#pragma unroll
+        for (int gx = 0; gx < 3; ++gx)
+#pragma unroll
+            for (int gy = 0; gy < 3; ++gy) {
+                const float weight = w.wx[gx] * w.wy[gy];
+                const int cx = w.bx + gx - 1, cy = w.by + gy - 1;
+                const float2 pre = (inside || in_domain(cx, cy, g.res)) ? g.grid_vpre[cell_index(cx, cy, g.tpd)]
+                                                                        : v2(0.0f, 0.0f);
+                old_v = vadd(old_v, vmuls(pre, weight));
+            }
+    }
+    return old_v;
+}
+
+// G2P phase 1 for one particle (transfer/g2p.rs:217-326; contact and mixture gated off,
+// ASFLIP compiled in with EXTRAS).  Returns 1 if the speed clamp fired.
 // FAST = false: the reference's cell-by-cell expression order (bit-level parity).
 // FAST = true: the same sums in stencil-offset form with fused multiply-adds:
 //   v' = sum w v_i,  B = v' (x) e + [sum (gx-1) w v_i, sum (gy-1) w v_i].
-template <bool FAST>
+template <bool FAST, bool EXTRAS = false>
 __device__ __forceinline__ int g2p_particle(const GridView &g, const DevConfig &cfg, float dt,
                                             PState &p) {
     QW w = quadratic_weights(p.x);
@@ -242,17 +279,29 @@ __device__ __forceinline__ int g2p_particle(const GridView &g, const DevConfig &
         p.c = mzero();
         return 0;
     }
+    float2 v_store = new_v, v_pos = new_v;
+    if constexpr (EXTRAS) {
+        if (cfg.asflip > 0.0f) {  // g2p.rs:281-296
+            const float2 old_v = gather_pre_force<FAST>(g, w, inside);
+            const float2 diff_vel = vsub(p.v, old_v);
+            const float trace_b = b.xa.x + b.ya.y;
+            const float gamma = trace_b < 0.0f ? 0.0f : 1.0f;
+            v_store = vadd(new_v, svmul(cfg.asflip, diff_vel));
+            v_pos = vadd(new_v, svmul(gamma * cfg.asflip, diff_vel));
+        }
+    }
     const float vel_limit = cfg.cell / dt;
     int clamped = 0;
-    float spd = vlen(new_v);
+    float spd = vlen(v_store);
     if (spd > vel_limit) {
         float scale = vel_limit / spd;
-        new_v = vmuls(new_v, scale);
+        v_store = vmuls(v_store, scale);
+        v_pos = vmuls(v_pos, scale);
         clamped = 1;
     }
-    float2 new_pos = vadd(p.x, vmuls(new_v, dt));
+    float2 new_pos = vadd(p.x, vmuls(v_pos, dt));
     for (int k = 0; k < cfg.n_bound; ++k) new_pos = clamp_position(cfg.bound_t[k], new_pos, g.res);
-    p.v = new_v;
+    p.v = v_store;
     p.c = mscale(mscale(b, KERNEL_D_INVERSE), cfg.apic_blend);
     p.x = new_pos;
     return clamped;
@@ -767,7 +816,7 @@ __device__ __forceinline__ void particle_pass(const ParticleKernelArgs &a) {
                     p.vol = p.mass / d;
                 }
             }
-            clamped = g2p_particle<FAST>(g, cfg, dt, p);
+            clamped = g2p_particle<FAST, HAS_MODEL(MASK, M_EXTRAS_BIT)>(g, cfg, dt, p);
             if constexpr (CLOSURE)
                 closure_prepare<MASK>(*mp, p, dt, pr, a.cl, closure_hash(i, st), w);
             else
@@ -786,6 +835,8 @@ __device__ __forceinline__ void particle_pass(const ParticleKernelArgs &a) {
     }
     if (valid) {
         const MatP &m = *mp;
+        if constexpr (HAS_MODEL(MASK, M_EXTRAS_BIT))
+            if (a.mode_g2p) apply_force_fields(cfg, p, dt);
         if (a.mode_g2p) store_fields(a.P, i, o, p);
         // CFL contribution for the next substep (step.rs:447-466)
         float sp = vlen(p.v);

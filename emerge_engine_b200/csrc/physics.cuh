@@ -338,12 +338,14 @@ EM_HD void nacc_project(const MatP &m, M2 f, float alpha, M2 &f_out, float &alph
 #define HAS_MODEL(mask, model) ((((mask) >> (model)) & 1u) != 0u)
 constexpr unsigned ALL_MODELS = (1u << M_FALLBACK) | (1u << M_FLUID) | (1u << M_NEOHOOKEAN) |
                                 (1u << M_SNOW) | (1u << M_DRUCKER_PRAGER) | (1u << M_NACC);
-// Mask bit 12 is not a ConstitutiveModel id: it marks a scene with a Bingham fluid (a Fluid
-// slot with compression_limit > 0), so Newtonian-only kernels leave the Bingham branch out.
+// Mask bits 12 and 13 are not ConstitutiveModel ids.  Bit 12 marks a scene with a Bingham
+// fluid (a Fluid slot with compression_limit > 0); bit 13 a scene with force fields or
+// ASFLIP.  Kernels instantiated without them leave those branches out.
 constexpr uint32_t M_BINGHAM_BIT = 12;
-// Every ConstitutiveModel id (materials/mod.rs:53-66) and the Bingham bit.  Kernels for
+constexpr uint32_t M_EXTRAS_BIT = 13;
+// Every ConstitutiveModel id (materials/mod.rs:53-66) and both extra bits.  Kernels for
 // scenes whose models all lie in ALL_MODELS keep the smaller instantiation.
-constexpr unsigned FULL_MODELS = 0x1FFFu;
+constexpr unsigned FULL_MODELS = 0x3FFFu;
 
 // Model-mask bits of one material slot.
 EM_HD unsigned model_bits(const MatP &m) {
@@ -929,7 +931,118 @@ struct DevConfig {
     int precise_math;        // evaluate exp/log/sin/sinh/pow in double, round once
     int n_bound;             // slip boundaries in order
     int bound_t[8];
+    float asflip;            // asflip_blend (transfer/g2p.rs:263-296)
+    int n_fields;            // force fields, application order
+    const emerge_force_field *fields;
+    const float *field_data;
 };
+
+// smooth_cutoff (spacetime/solver/cutoff.rs:17-26)
+EM_HD float smooth_cutoff(float r, float r_on, float r_cut) {
+    if (r >= r_cut) return 0.0f;
+    if (r <= r_on) return 1.0f;
+    float x = (r - r_on) / (r_cut - r_on);
+    return 1.0f - 3.0f * x * x + 2.0f * x * x * x;
+}
+
+// Field::acceleration of one built-in force field at a particle (forces/fields/: gravity.rs,
+// buoyancy.rs, drag.rs, confinement.rs, coulomb.rs, em.rs, chemotaxis.rs).  Material charge
+// maps are tables by material id; ids past the table have no charge.
+EM_HD float2 field_acceleration(const emerge_force_field &f, const float *data, const PState &p) {
+    const float *pr = f.params;
+    const float2 x = p.x;
+    switch (f.kind) {
+    case EMERGE_FIELD_GRAVITY_WELL: {
+        float2 acc = v2(0.0f, 0.0f);
+        const float eps2 = pr[1] * pr[1];
+        for (uint32_t k = 0; k < f.count; ++k) {
+            const float *src = data + f.data_offset + 3 * k;
+            const float2 r_vec = vsub(v2(src[0], src[1]), x);  // toward the source
+            const float r2 = vlen2(r_vec);
+            const float r = sqrtf(r2);
+            if (r >= pr[2] || r < F32_EPS) continue;
+            const float norm_s = r2 + eps2;
+            const float force_scale = pr[0] * src[2] / (norm_s * sqrtf(norm_s));
+            if (!isfinite(force_scale)) continue;
+            acc = vadd(acc, vmuls(vmuls(r_vec, force_scale), smooth_cutoff(r, pr[3], pr[2])));
+        }
+        return acc;
+    }
+    case EMERGE_FIELD_BUOYANCY:
+        return vmuls(v2(-pr[1], -pr[2]), pr[0] / fmaxf(p.rho, pr[3]));
+    case EMERGE_FIELD_LINEAR_DRAG:
+        if (f.material_mask != EMERGE_FIELD_ALL_MATERIALS && (f.material_mask & (1u << (p.mat & 31u))) == 0u)
+            return v2(0.0f, 0.0f);
+        return svmul(pr[2], vsub(v2(pr[0], pr[1]), p.v));
+    case EMERGE_FIELD_RADIAL_CONFINEMENT: {
+        const float2 r_vec = vsub(x, v2(pr[0], pr[1]));
+        const float dist = vlen(r_vec);
+        const float overshoot = dist - pr[2];
+        if (overshoot <= 0.0f || dist < F32_EPS) return v2(0.0f, 0.0f);
+        return vmuls(v2(-r_vec.x, -r_vec.y), pr[3] * overshoot / dist);
+    }
+    case EMERGE_FIELD_AABB_CONFINEMENT: {
+        float2 acc = v2(0.0f, 0.0f);
+        if (x.x < pr[0]) acc.x += pr[4] * (pr[0] - x.x);
+        else if (x.x > pr[2]) acc.x -= pr[4] * (x.x - pr[2]);
+        if (x.y < pr[1]) acc.y += pr[4] * (pr[1] - x.y);
+        else if (x.y > pr[3]) acc.y -= pr[4] * (x.y - pr[3]);
+        return acc;
+    }
+    case EMERGE_FIELD_COULOMB: {
+        const float q_p = p.mat < f.n_charges ? data[f.data_offset + 3 * f.count + p.mat] : 0.0f;
+        if (!(fabsf(q_p) > F32_EPS)) return v2(0.0f, 0.0f);
+        float2 acc = v2(0.0f, 0.0f);
+        const float eps2 = pr[1] * pr[1];
+        const float inv_mass = p.mass > F32_EPS ? 1.0f / p.mass : 0.0f;
+        for (uint32_t k = 0; k < f.count; ++k) {
+            const float *src = data + f.data_offset + 3 * k;
+            const float2 r_vec = vsub(x, v2(src[0], src[1]));  // away from the source
+            const float r2 = vlen2(r_vec);
+            const float r = sqrtf(r2);
+            if (r >= pr[2] || r < F32_EPS) continue;
+            const float norm_s = r2 + eps2;
+            const float force_scale = pr[0] * src[2] * q_p / (norm_s * sqrtf(norm_s));
+            if (!isfinite(force_scale)) continue;
+            acc = vadd(acc, vmuls(r_vec, force_scale * smooth_cutoff(r, pr[3], pr[2]) * inv_mass));
+        }
+        return acc;
+    }
+    case EMERGE_FIELD_UNIFORM_ELECTRIC: {
+        const float q = p.mat < f.n_charges ? data[f.data_offset + p.mat] : 0.0f;
+        if (!(fabsf(q) > F32_EPS)) return v2(0.0f, 0.0f);
+        const float inv_mass = p.mass > F32_EPS ? 1.0f / p.mass : 0.0f;
+        return vmuls(v2(pr[0], pr[1]), q * inv_mass);
+    }
+    case EMERGE_FIELD_CHEMOTAXIS: {
+        if (f.material_filter != EMERGE_FIELD_ALL_MATERIALS && p.mat != f.material_filter)
+            return v2(0.0f, 0.0f);
+        const int res = static_cast<int>(f.count);
+        const int ix = f2i(floorf(x.x)), iy = f2i(floorf(x.y));
+        const float *phi = data + f.data_offset;
+        auto at = [&](int xi, int yi) -> float {
+            if (xi < 0 || yi < 0 || xi >= res || yi >= res) return 0.0f;
+            return phi[static_cast<size_t>(xi) * res + yi];
+        };
+        const float2 grad = v2((at(ix + 1, iy) - at(ix - 1, iy)) * 0.5f, (at(ix, iy + 1) - at(ix, iy - 1)) * 0.5f);
+        return svmul(pr[0], grad);
+    }
+    default:
+        return v2(0.0f, 0.0f);
+    }
+}
+
+// Force fields after G2P (step.rs:212-259): v += dt * sum of the accelerations, then the
+// G2P speed clamp again; pinned particles are skipped.
+EM_HD void apply_force_fields(const DevConfig &cfg, PState &p, float dt) {
+    if (cfg.n_fields <= 0 || p.pinned != 0) return;
+    float2 dv = v2(0.0f, 0.0f);
+    for (int k = 0; k < cfg.n_fields; ++k) dv = vadd(dv, field_acceleration(cfg.fields[k], cfg.field_data, p));
+    p.v = vadd(p.v, svmul(dt, dv));
+    const float vel_limit = cfg.cell / dt;
+    const float spd = vlen(p.v);
+    if (spd > vel_limit) p.v = vmuls(p.v, vel_limit / spd);
+}
 
 // affine_cfl_speed_contribution (step.rs:481-488)
 EM_HD float affine_cfl(M2 c, float cell) {

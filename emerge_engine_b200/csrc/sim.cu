@@ -34,6 +34,8 @@ struct Buffer {
     }
 };
 
+inline size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
+
 // Bump allocator over one device allocation, 256-byte aligned pieces.
 struct Carver {
     uintptr_t p;
@@ -125,10 +127,12 @@ struct emerge_sim {
     Buffer gbuf;
     GridView g{};
 
-    // materials / boundaries
+    // materials / boundaries / force fields
     std::vector<emerge_material_params> mats;
     Buffer mbuf;
     std::vector<uint64_t> bounds;
+    int n_fields = 0;
+    Buffer fbuf;  // force field table, then its data
 
     // controller
     Buffer sbuf;
@@ -225,10 +229,7 @@ emerge_status validate_config(const emerge_sim_config &c, std::string &msg) {
         msg = "sleep_threshold > 0 (sleep partition) is not on the device path";
         return EMERGE_ERR_UNSUPPORTED;
     }
-    if (c.asflip_blend > 0.0f) {
-        msg = "asflip_blend > 0 (ASFLIP) is not on the device path";
-        return EMERGE_ERR_UNSUPPORTED;
-    }
+    if (!(c.asflip_blend >= 0.0f)) return bad("asflip_blend must be >= 0");
     if (c.max_substeps_per_step > 0x7fffffffull) {
         msg = "max_substeps_per_step too large";
         return EMERGE_ERR_INVALID_ARG;
@@ -263,7 +264,19 @@ DevConfig make_dev_config(const emerge_sim_config &c, const std::vector<uint64_t
     d.n_bound = static_cast<int>(bounds.size());
     for (size_t k = 0; k < bounds.size() && k < static_cast<size_t>(MAX_BOUNDARIES); ++k)
         d.bound_t[k] = static_cast<int>(bounds[k]);
+    d.asflip = c.asflip_blend;
     return d;
+}
+
+// The simulation's device configuration: config, boundaries and the force-field table.
+void refresh_dev_config(emerge_sim *s) {
+    s->dcfg = make_dev_config(s->cfg, s->bounds, s->dcfg.precise_math);
+    s->dcfg.n_fields = s->n_fields;
+    s->dcfg.fields = s->n_fields ? static_cast<const emerge_force_field *>(s->fbuf.ptr) : nullptr;
+    s->dcfg.field_data = s->n_fields ? reinterpret_cast<const float *>(
+                                           static_cast<const char *>(s->fbuf.ptr) +
+                                           align_up(s->n_fields * sizeof(emerge_force_field), 256))
+                                     : nullptr;
 }
 
 StepLaunch make_launch(emerge_sim *s) {
@@ -282,6 +295,7 @@ StepLaunch make_launch(emerge_sim *s) {
     L.use_window = s->use_window;
     L.model_mask = 1u << M_FALLBACK;
     for (const auto &m : s->mats) L.model_mask |= model_bits(m);
+    if (s->dcfg.n_fields > 0 || s->dcfg.asflip > 0.0f) L.model_mask |= 1u << M_EXTRAS_BIT;
     L.fast = s->deterministic ? 0 : 1;
     L.cl = closure_args(s->closure);
     L.stream = s->stream;
@@ -848,7 +862,9 @@ emerge_status emerge_cuda_create(const emerge_sim_config *config, int device, em
     s->res = static_cast<int>(config->grid_res);
     s->tpd = (s->res + TILE - 1) / TILE;
     size_t cells = static_cast<size_t>(s->tpd) * s->tpd * TILE_CELLS;
-    size_t gbytes = cells * (sizeof(float4) + 2 * sizeof(float2)) + static_cast<size_t>(s->tpd) * s->tpd + 4 * 256;
+    const bool asflip = config->asflip_blend > 0.0f;
+    size_t gbytes = cells * (sizeof(float4) + (asflip ? 3 : 2) * sizeof(float2)) +
+                    static_cast<size_t>(s->tpd) * s->tpd + 5 * 256;
     if (!cuda_ok(s, cudaMalloc(&s->gbuf.ptr, gbytes), "grid alloc", &st)) return bail(st);
     s->gbuf.bytes = gbytes;
     Carver c(s->gbuf.ptr);
@@ -858,6 +874,7 @@ emerge_status emerge_cuda_create(const emerge_sim_config *config, int device, em
     s->g.acc_s = c.take<float2>(cells);
     s->g.grid_v = c.take<float2>(cells);
     s->g.tile_flag = c.take<uint8_t>(static_cast<size_t>(s->tpd) * s->tpd);
+    s->g.grid_vpre = asflip ? c.take<float2>(cells) : nullptr;
     if (!cuda_ok(s, cudaMemsetAsync(s->gbuf.ptr, 0, gbytes, s->stream), "grid clear", &st)) return bail(st);
     if (!cuda_ok(s, cudaMalloc(&s->mbuf.ptr, MAX_MATERIALS * sizeof(emerge_material_params)), "mat alloc", &st))
         return bail(st);
@@ -895,6 +912,7 @@ emerge_status emerge_cuda_destroy(emerge_sim *s) {
     s->detbuf.reset();
     s->gbuf.reset();
     s->mbuf.reset();
+    s->fbuf.reset();
     s->sbuf.reset();
     s->sortbuf.reset();
     s->region_buf.reset();
@@ -937,7 +955,49 @@ emerge_status emerge_cuda_set_slip_boundaries(emerge_sim *s, const uint64_t *thi
         if (thickness[k] + 1 > s->cfg.grid_res)
             return static_cast<emerge_status>(s->fail(EMERGE_ERR_INVALID_ARG, "boundary thickness exceeds grid"));
     s->bounds.assign(thickness, thickness + n);
-    s->dcfg = make_dev_config(s->cfg, s->bounds, s->dcfg.precise_math);
+    refresh_dev_config(s);
+    s->graph_dirty = true;
+    return EMERGE_OK;
+}
+
+emerge_status emerge_cuda_set_force_fields(emerge_sim *s, const emerge_force_field *fields, uint32_t n,
+                                           const float *data, uint64_t n_data) {
+    if (!s || (!fields && n) || (!data && n_data)) return EMERGE_ERR_INVALID_ARG;
+    for (uint32_t k = 0; k < n; ++k) {
+        const emerge_force_field &f = fields[k];
+        uint64_t need = 0;
+        switch (f.kind) {
+        case EMERGE_FIELD_GRAVITY_WELL: need = 3ull * f.count; break;
+        case EMERGE_FIELD_COULOMB: need = 3ull * f.count + f.n_charges; break;
+        case EMERGE_FIELD_UNIFORM_ELECTRIC: need = f.n_charges; break;
+        case EMERGE_FIELD_CHEMOTAXIS: need = static_cast<uint64_t>(f.count) * f.count; break;
+        case EMERGE_FIELD_BUOYANCY:
+        case EMERGE_FIELD_LINEAR_DRAG:
+        case EMERGE_FIELD_RADIAL_CONFINEMENT:
+        case EMERGE_FIELD_AABB_CONFINEMENT: break;
+        default:
+            return static_cast<emerge_status>(
+                s->fail(EMERGE_ERR_UNSUPPORTED, "force field " + std::to_string(k) + ": unknown kind"));
+        }
+        if (static_cast<uint64_t>(f.data_offset) + need > n_data)
+            return static_cast<emerge_status>(
+                s->fail(EMERGE_ERR_INVALID_ARG, "force field " + std::to_string(k) + ": data out of range"));
+    }
+    if (s->stream) CK(cudaStreamSynchronize(s->stream));  // kernels in flight may read the old table
+    s->fbuf.reset();
+    s->n_fields = 0;
+    if (n > 0) {
+        const size_t table = align_up(n * sizeof(emerge_force_field), 256);
+        const size_t bytes = table + std::max<uint64_t>(n_data, 1) * sizeof(float);
+        CK(cudaMalloc(&s->fbuf.ptr, bytes));
+        s->fbuf.bytes = bytes;
+        CK(cudaMemcpy(s->fbuf.ptr, fields, n * sizeof(emerge_force_field), cudaMemcpyHostToDevice));
+        if (n_data)
+            CK(cudaMemcpy(static_cast<char *>(s->fbuf.ptr) + table, data, n_data * sizeof(float),
+                          cudaMemcpyHostToDevice));
+        s->n_fields = static_cast<int>(n);
+    }
+    refresh_dev_config(s);
     s->graph_dirty = true;
     return EMERGE_OK;
 }

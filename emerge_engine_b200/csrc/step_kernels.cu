@@ -52,8 +52,10 @@ __device__ __forceinline__ void grid_update_cell(const GridView &g, const DevCon
     float2 s = g.acc_s[ci];
     float m = acc.x;
     float2 mom = v2(acc.y + dt * s.x, acc.z + dt * s.y);
+    if (m > 0.0f) mom = vdivs(mom, m);
+    // ASFLIP snapshot between normalisation and gravity (step.rs:140-147)
+    if (cfg.asflip > 0.0f) g.grid_vpre[ci] = mom;
     if (m > 0.0f) {
-        mom = vdivs(mom, m);
         mom = vadd(mom, vmuls(cfg.gravity, dt));
         for (int k = 0; k < cfg.n_bound; ++k) slip_velocity(cfg.bound_t[k], x, y, g.res, mom);
         float vel_limit = cfg.cell / dt;

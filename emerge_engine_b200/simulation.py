@@ -18,6 +18,7 @@ from . import abi
 from .abi import (PARTICLE_DTYPE, BodyStateC, MaterialParamsC, StepTimingC, check,
                   load_library)
 from .config import BodyState, SimConfig, SlipBoundary, SpawnRegion
+from .fields import Field, pack_fields
 from .materials import DEVICE_MODELS, FallbackMaterial, Material
 
 MAX_MATERIAL_SLOTS = 64  # materials/registry.rs:6
@@ -72,6 +73,7 @@ class Simulation:
         self._sim = ptr
         self.registry = MaterialRegistry(FallbackMaterial())
         self.boundaries = [SlipBoundary(config.boundary_thickness)]  # lifecycle.rs:29-30
+        self.force_fields: list = []  # (name, field) in application order
         self.last_timing: dict | None = None
         if deterministic:
             self.set_option(abi.OPT_DETERMINISTIC, 1)
@@ -140,6 +142,50 @@ class Simulation:
         mid = self.registry.next_id()
         self.set_material(mid, material)
         return mid
+
+    # ---------------------------------------------------------------- force fields
+    def _upload_fields(self) -> None:
+        table, data = pack_fields([f for _, f in self.force_fields])
+        arr = (abi.ForceFieldC * max(len(table), 1))(*table)
+        d = np.asarray(data if data else [0.0], dtype=np.float32)
+        self._check(self._lib.emerge_cuda_set_force_fields(
+            self._sim, arr, len(table), d.ctypes.data_as(ctypes.POINTER(c_float)), len(data)))
+
+    def add_named_force_field(self, name: str, field: Field) -> None:
+        """lifecycle.rs:374-377."""
+        if not isinstance(field, Field):
+            raise abi.EmergeError(abi.ERR_UNSUPPORTED,
+                                  f"{type(field).__name__} has no device implementation")
+        self.force_fields.append((str(name), field))
+        self._upload_fields()
+
+    def add_force_field(self, field: Field) -> None:
+        """Anonymous field named force_field_N (lifecycle.rs:368-372)."""
+        self.add_named_force_field(f"force_field_{len(self.force_fields)}", field)
+
+    def with_force_field(self, field: Field) -> "Simulation":
+        self.add_force_field(field)
+        return self
+
+    def with_named_force_field(self, name: str, field: Field) -> "Simulation":
+        self.add_named_force_field(name, field)
+        return self
+
+    def remove_force_field(self, name: str) -> bool:
+        """Removes the first field with this name (lifecycle.rs:380-387)."""
+        for k, (n, _) in enumerate(self.force_fields):
+            if n == name:
+                del self.force_fields[k]
+                self._upload_fields()
+                return True
+        return False
+
+    def clear_force_fields(self) -> None:
+        self.force_fields = []
+        self._upload_fields()
+
+    def force_field_names(self) -> list:
+        return [n for n, _ in self.force_fields]
 
     # ---------------------------------------------------------------- boundaries
     def _upload_boundaries(self) -> None:

@@ -94,7 +94,7 @@ typedef struct emerge_sim_config {
     float j_max;
     float sleep_threshold;          /* must be 0: the sleep partition is not on the device path */
     float contact_friction;
-    float asflip_blend;             /* must be 0: ASFLIP is not on the device path */
+    float asflip_blend;             /* ASFLIP FLIP blend (transfer/g2p.rs:263-296); 0 = APIC only */
     float mixture_drag_coefficient;
     uint32_t mixture_pressure_iterations;
     float dx_meters;
@@ -210,6 +210,51 @@ emerge_status emerge_cuda_set_materials(emerge_sim *sim, const emerge_material_p
  * set_boundary_condition :353 replaces). */
 emerge_status emerge_cuda_set_slip_boundaries(emerge_sim *sim, const uint64_t *thickness,
                                               uint32_t n);
+
+/* ---- force fields ------------------------------------------------------------- */
+
+/* Built-in force fields (forces/fields/): per particle v += sub_dt * sum of the
+ * fields' accelerations after G2P, then the G2P speed clamp again (step.rs:212-259).
+ * The reference's Field trait objects can hold arbitrary code; the device runs these
+ * kinds, which cover every built-in field except NBodyGravityField (Barnes-Hut tree
+ * rebuilt per substep) and SpatialDragField (a host function pointer). */
+enum {
+    EMERGE_FIELD_GRAVITY_WELL = 1,       /* gravity.rs: params {G, softening, cutoff, switch_on};
+                                            data: count sources (x, y, mass) */
+    EMERGE_FIELD_BUOYANCY = 2,           /* buoyancy.rs: {fluid_density, gravity.x, gravity.y,
+                                            min_density} */
+    EMERGE_FIELD_LINEAR_DRAG = 3,        /* drag.rs: {target.x, target.y, drag_coefficient};
+                                            material_mask */
+    EMERGE_FIELD_RADIAL_CONFINEMENT = 4, /* confinement.rs: {center.x, center.y, radius, stiffness} */
+    EMERGE_FIELD_AABB_CONFINEMENT = 5,   /* confinement.rs: {min.x, min.y, max.x, max.y, stiffness} */
+    EMERGE_FIELD_COULOMB = 6,            /* coulomb.rs: {k, softening, cutoff, switch_on}; data: count
+                                            sources (x, y, charge), then n_charges charges by
+                                            material id */
+    EMERGE_FIELD_UNIFORM_ELECTRIC = 7,   /* em.rs: {field.x, field.y}; data: n_charges charges by
+                                            material id */
+    EMERGE_FIELD_CHEMOTAXIS = 8          /* chemotaxis.rs: {sensitivity}; material_filter; data:
+                                            count x count potential phi[x * count + y] */
+};
+#define EMERGE_FIELD_ALL_MATERIALS 0xFFFFFFFFu
+
+/* One field (48 bytes).  Material charge maps (HashMap<u32, f32>) are flattened to a table
+ * indexed by material id; ids at or past n_charges have no charge. */
+typedef struct emerge_force_field {
+    uint32_t kind;             /* EMERGE_FIELD_* */
+    uint32_t material_mask;    /* LinearDrag: bit (id & 31) set = applies; ALL_MATERIALS = all */
+    uint32_t material_filter;  /* Chemotaxis: only this material id; ALL_MATERIALS = no filter */
+    uint32_t count;            /* sources (GravityWell, Coulomb) or grid_res (Chemotaxis) */
+    uint32_t data_offset;      /* first float of this field's data in the data array */
+    uint32_t n_charges;        /* Coulomb, UniformElectric */
+    float params[6];
+} emerge_force_field;
+
+/* Replaces the simulation's force fields (Simulation::add_force_field / add_named_force_field /
+ * remove_force_field / clear_force_fields, lifecycle.rs:368-392: the caller keeps the named
+ * list and passes it in application order).  `data` holds every field's sources, charge
+ * tables and potentials; n = 0 clears. */
+emerge_status emerge_cuda_set_force_fields(emerge_sim *sim, const emerge_force_field *fields,
+                                           uint32_t n, const float *data, uint64_t n_data);
 
 /* ---- particles ---------------------------------------------------------------- */
 

@@ -902,13 +902,22 @@ struct Grid {
     std::vector<V2> mom;
     std::vector<uint8_t> touched;
     std::vector<uint32_t> dirty;  // first-touch order (mod.rs:127)
+    std::vector<V2> pre;          // ASFLIP pre-force snapshot, valid at touched cells
 
     void init(size_t r) {
         res = r;
         mass.assign(r * r, 0.0f);
         mom.assign(r * r, v2(0, 0));
         touched.assign(r * r, 0);
+        pre.assign(r * r, v2(0, 0));
         dirty.clear();
+    }
+    // snapshot_velocities / pre_force_velocity_at (grid/mod.rs:300-317): the snapshot's
+    // keys are the dirty cells, which stay touched until the next clear.
+    V2 pre_force_velocity_at(IV2 c) const {
+        uint32_t idx;
+        if (!flat_index(c, idx) || !touched[idx]) return v2(0, 0);
+        return pre[idx];
     }
     // Grid::clear (mod.rs:167-180)
     void clear() {
@@ -966,6 +975,8 @@ struct oracle_sim {
     std::vector<Mat> materials;
     std::vector<size_t> boundaries;  // slip thicknesses, in application order
     Grid grid;
+    std::vector<oracle_force_field> fields;  // force_fields, application order
+    std::vector<float> field_data;
     float last_step_dt = 0.0f;
     size_t last_substeps = 0;
     size_t last_vel_clamp_count = 0;
@@ -1288,6 +1299,9 @@ void grid_update(oracle_sim &s, float dt) {
     V2 grav = v2(s.cfg.gravity[0], s.cfg.gravity[1]);
     for (uint32_t idx : g.dirty)
         if (g.mass[idx] > 0.0f) g.mom[idx] = divs(g.mom[idx], g.mass[idx]);
+    // ASFLIP snapshot between normalisation and gravity (step.rs:140-147)
+    if (s.cfg.asflip_blend > 0.0f)
+        for (uint32_t idx : g.dirty) g.pre[idx] = g.mom[idx];
     for (uint32_t idx : g.dirty)
         if (g.mass[idx] > 0.0f) g.mom[idx] = add(g.mom[idx], muls(grav, dt));
     size_t res = g.res;
@@ -1303,11 +1317,12 @@ void grid_update(oracle_sim &s, float dt) {
     }
 }
 
-// gather_grid_to_particles (transfer/g2p.rs:151-343) with ASFLIP, contact and mixture
-// gated off (asflip_blend = 0, no grip or mixture particles).
+// gather_grid_to_particles (transfer/g2p.rs:151-343) with ASFLIP (g2p.rs:263-296);
+// contact and mixture gated off (no grip or mixture particles).
 size_t g2p(oracle_sim &s, float dt) {
     const float vel_limit = s.cfg.grid_cell_size / dt;
     const float apic_blend = s.cfg.apic_blend;
+    const float asflip_blend = s.cfg.asflip_blend;
     const size_t res = s.grid.res;
     const long n = static_cast<long>(s.active_count);
     std::vector<size_t> clamp_counts(static_cast<size_t>(n > 0 ? n : 0), 0);
@@ -1316,6 +1331,7 @@ size_t g2p(oracle_sim &s, float dt) {
         for (long ii = lo; ii < hi; ++ii) {
             P &q = s.p[static_cast<size_t>(ii)];
             V2 x = load_v(q.x);
+            const V2 v_old = load_v(q.v);
             QW w = quadratic_weights(x);
             V2 new_v = v2(0, 0);
             M2 b = zero2();
@@ -1337,6 +1353,20 @@ size_t g2p(oracle_sim &s, float dt) {
                 continue;
             }
             V2 v_store = new_v, v_pos = new_v;
+            if (asflip_blend > 0.0f) {
+                V2 old_v = v2(0, 0);
+                for (int gx = 0; gx < 3; ++gx)
+                    for (int gy = 0; gy < 3; ++gy) {
+                        float weight = w.wx[gx] * w.wy[gy];
+                        IV2 cell{w.base.x + gx - 1, w.base.y + gy - 1};
+                        old_v = add(old_v, muls(s.grid.pre_force_velocity_at(cell), weight));
+                    }
+                V2 diff_vel = sub(v_old, old_v);
+                float trace_b = b.xa.x + b.ya.y;
+                float gamma = trace_b < 0.0f ? 0.0f : 1.0f;
+                v_store = add(new_v, smul(asflip_blend, diff_vel));
+                v_pos = add(new_v, smul(gamma * asflip_blend, diff_vel));
+            }
             float spd = length(v_store);
             if (spd > vel_limit) {
                 float scale = vel_limit / spd;
@@ -1356,6 +1386,129 @@ size_t g2p(oracle_sim &s, float dt) {
     // Phase 2 (g2p.rs:333-340): sequential constitutive update.
     for (size_t i = 0; i < s.active_count; ++i) update_particle(s.mat(s.p[i].material_id), s.p[i], dt);
     return clamp_count;
+}
+
+// smooth_cutoff (solver/cutoff.rs:17-26)
+float smooth_cutoff(float r, float r_on, float r_cut) {
+    if (r >= r_cut) return 0.0f;
+    if (r <= r_on) return 1.0f;
+    float x = (r - r_on) / (r_cut - r_on);
+    return 1.0f - 3.0f * x * x + 2.0f * x * x * x;
+}
+
+// Charge of a material (HashMap lookup; a missing id has none).
+float field_charge(const oracle_force_field &f, const float *data, uint32_t id, uint32_t skip) {
+    return id < f.n_charges ? data[f.data_offset + skip + id] : 0.0f;
+}
+
+// Field::acceleration of the built-in fields (forces/fields/*.rs).
+V2 field_acceleration(const oracle_force_field &f, const float *data, const P &q, uint32_t id) {
+    const float *pr = f.params;
+    const V2 x = load_v(q.x);
+    switch (f.kind) {
+    case 1: {  // GravityWellField (gravity.rs)
+        V2 acc = v2(0, 0);
+        float eps2 = pr[1] * pr[1];
+        for (uint32_t k = 0; k < f.count; ++k) {
+            const float *src = data + f.data_offset + 3 * k;
+            V2 r_vec = sub(v2(src[0], src[1]), x);
+            float r2 = length_sq(r_vec);
+            float r = std::sqrt(r2);
+            if (r >= pr[2] || r < F32_EPS) continue;
+            float norm_s = r2 + eps2;
+            float force_scale = pr[0] * src[2] / (norm_s * std::sqrt(norm_s));
+            if (!std::isfinite(force_scale)) continue;
+            float sw = smooth_cutoff(r, pr[3], pr[2]);
+            acc = add(acc, muls(muls(r_vec, force_scale), sw));
+        }
+        return acc;
+    }
+    case 2: {  // BuoyancyField (buoyancy.rs)
+        float rho = fmax_(q.density, pr[3]);
+        return muls(v2(-pr[1], -pr[2]), pr[0] / rho);
+    }
+    case 3: {  // LinearDragField (drag.rs)
+        if (f.material_mask != 0xFFFFFFFFu && (f.material_mask & (1u << (id & 31u))) == 0u)
+            return v2(0, 0);
+        return smul(pr[2], sub(v2(pr[0], pr[1]), load_v(q.v)));
+    }
+    case 4: {  // RadialConfinementField (confinement.rs)
+        V2 r_vec = sub(x, v2(pr[0], pr[1]));
+        float dist = length(r_vec);
+        float overshoot = dist - pr[2];
+        if (overshoot <= 0.0f || dist < F32_EPS) return v2(0, 0);
+        return muls(v2(-r_vec.x, -r_vec.y), pr[3] * overshoot / dist);
+    }
+    case 5: {  // AabbConfinementField (confinement.rs)
+        V2 acc = v2(0, 0);
+        if (x.x < pr[0]) acc.x += pr[4] * (pr[0] - x.x);
+        else if (x.x > pr[2]) acc.x -= pr[4] * (x.x - pr[2]);
+        if (x.y < pr[1]) acc.y += pr[4] * (pr[1] - x.y);
+        else if (x.y > pr[3]) acc.y -= pr[4] * (x.y - pr[3]);
+        return acc;
+    }
+    case 6: {  // CoulombField (coulomb.rs)
+        float q_p = field_charge(f, data, id, 3 * f.count);
+        if (!(std::fabs(q_p) > F32_EPS)) return v2(0, 0);
+        V2 acc = v2(0, 0);
+        float eps2 = pr[1] * pr[1];
+        float inv_mass = q.mass > F32_EPS ? 1.0f / q.mass : 0.0f;
+        for (uint32_t k = 0; k < f.count; ++k) {
+            const float *src = data + f.data_offset + 3 * k;
+            V2 r_vec = sub(x, v2(src[0], src[1]));
+            float r2 = length_sq(r_vec);
+            float r = std::sqrt(r2);
+            if (r >= pr[2] || r < F32_EPS) continue;
+            float norm_s = r2 + eps2;
+            float force_scale = pr[0] * src[2] * q_p / (norm_s * std::sqrt(norm_s));
+            if (!std::isfinite(force_scale)) continue;
+            float sw = smooth_cutoff(r, pr[3], pr[2]);
+            acc = add(acc, muls(r_vec, force_scale * sw * inv_mass));
+        }
+        return acc;
+    }
+    case 7: {  // UniformElectricField (em.rs)
+        float qc = field_charge(f, data, id, 0);
+        if (!(std::fabs(qc) > F32_EPS)) return v2(0, 0);
+        float inv_mass = q.mass > F32_EPS ? 1.0f / q.mass : 0.0f;
+        return muls(v2(pr[0], pr[1]), qc * inv_mass);
+    }
+    case 8: {  // ChemotaxisField (chemotaxis.rs)
+        if (f.material_filter != 0xFFFFFFFFu && id != f.material_filter) return v2(0, 0);
+        const int res = static_cast<int>(f.count);
+        const int ix = static_cast<int>(std::floor(x.x)), iy = static_cast<int>(std::floor(x.y));
+        auto phi = [&](int xi, int yi) -> float {
+            if (xi < 0 || yi < 0 || xi >= res || yi >= res) return 0.0f;
+            return data[f.data_offset + static_cast<size_t>(xi) * res + yi];
+        };
+        V2 grad = v2((phi(ix + 1, iy) - phi(ix - 1, iy)) * 0.5f,
+                     (phi(ix, iy + 1) - phi(ix, iy - 1)) * 0.5f);
+        return smul(pr[0], grad);
+    }
+    default:
+        return v2(0, 0);
+    }
+}
+
+// Force fields (step.rs:212-259): v += dt * sum of accelerations, then the speed clamp.
+void apply_force_fields(oracle_sim &s, float dt) {
+    if (s.fields.empty()) return;
+    const float *data = s.field_data.data();
+    for (size_t i = 0; i < s.active_count; ++i) {
+        P &q = s.p[i];
+        if (q.pinned != 0) continue;
+        V2 dv = v2(0, 0);
+        for (const oracle_force_field &f : s.fields) dv = add(dv, field_acceleration(f, data, q, q.material_id));
+        store_v(q.v, add(load_v(q.v), smul(dt, dv)));
+    }
+    const float vel_limit = s.cfg.grid_cell_size / dt;
+    for (size_t i = 0; i < s.active_count; ++i) {
+        P &q = s.p[i];
+        if (q.pinned != 0) continue;
+        V2 v = load_v(q.v);
+        float spd = length(v);
+        if (spd > vel_limit) store_v(q.v, muls(v, vel_limit / spd));
+    }
 }
 
 // Simulation::do_substep (step.rs:62-317) restricted to the gated-on phases.
@@ -1379,6 +1532,7 @@ void do_substep(oracle_sim &s, float sub_dt) {
     t0 = clk::now();
     s.last_vel_clamp_count += g2p(s, sub_dt);
     s.timing[5] += us_since(t0);
+    apply_force_fields(s, sub_dt);
 }
 
 // Simulation::step (step.rs:23-60)
@@ -1580,6 +1734,30 @@ void oracle_kirchhoff(const oracle_material *m, const oracle_particle *p, float 
 }
 
 void oracle_set_correctly_rounded(int on) { g_correctly_rounded = on ? 1 : 0; }
+
+void oracle_field_acceleration(const oracle_force_field *f, const float *data,
+                               const oracle_particle *p, float out[2]) {
+    V2 a = field_acceleration(*f, data, *p, p->material_id);
+    out[0] = a.x;
+    out[1] = a.y;
+}
+
+int oracle_set_force_fields(oracle_sim *s, const oracle_force_field *fields, uint32_t n,
+                            const float *data, uint64_t n_data) {
+    for (uint32_t k = 0; k < n; ++k) {
+        const oracle_force_field &f = fields[k];
+        if (f.kind < 1 || f.kind > 8) return -1;
+        uint64_t need = 0;
+        if (f.kind == 1) need = 3ull * f.count;
+        if (f.kind == 6) need = 3ull * f.count + f.n_charges;
+        if (f.kind == 7) need = f.n_charges;
+        if (f.kind == 8) need = static_cast<uint64_t>(f.count) * f.count;
+        if (static_cast<uint64_t>(f.data_offset) + need > n_data) return -1;
+    }
+    s->fields.assign(fields, fields + n);
+    s->field_data.assign(data, data + n_data);
+    return 0;
+}
 
 void oracle_update_particle(const oracle_material *m, oracle_particle *p, float dt) {
     update_particle(*m, *p, dt);

@@ -159,6 +159,13 @@ typedef struct oracle_material {
      * stretch_limit, min_plastic_jacobian, max_plastic_jacobian */
 } oracle_material;
 
+/* One built-in force field (forces/fields/); kinds and data layout as
+ * emerge_force_field in include/emerge_cuda.h (same 48-byte layout). */
+typedef struct oracle_force_field {
+    uint32_t kind, material_mask, material_filter, count, data_offset, n_charges;
+    float params[6];
+} oracle_force_field;
+
 typedef struct oracle_sim oracle_sim;
 
 /* Simulation::empty (lifecycle.rs:26): validates the config (error -> NULL),
@@ -185,6 +192,13 @@ void oracle_step(oracle_sim *s, uint32_t n_steps);
 /* 0 (default): exp/log/pow/sin/sinh from the C library, as the Rust reference calls them;
  * 1: evaluated in double and rounded once to f32 (process-wide switch). */
 void oracle_set_correctly_rounded(int on);
+/* Replaces the force fields (application order); returns 0, or -1 for an unknown kind or
+ * data out of range. */
+int oracle_set_force_fields(oracle_sim *s, const oracle_force_field *fields, uint32_t n,
+                            const float *data, uint64_t n_data);
+/* Field::acceleration of one field at one particle. */
+void oracle_field_acceleration(const oracle_force_field *f, const float *data,
+                               const oracle_particle *p, float out[2]);
 uint64_t oracle_particle_count(const oracle_sim *s);
 void oracle_read_particles(const oracle_sim *s, oracle_particle *out);
 void oracle_write_particles(oracle_sim *s, const oracle_particle *in);

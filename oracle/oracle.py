@@ -14,8 +14,9 @@ from ctypes import POINTER, Structure, byref, c_double, c_float, c_int, c_uint32
 
 import numpy as np
 
-from emerge_engine_b200.abi import (PARTICLE_DTYPE, BodyStateC, Particle, SimConfigC,
-                                    SpawnRegionC)
+from emerge_engine_b200.abi import (PARTICLE_DTYPE, BodyStateC, ForceFieldC, Particle,
+                                    SimConfigC, SpawnRegionC)
+from emerge_engine_b200.fields import pack_fields
 from emerge_engine_b200.config import BodyState, SimConfig, SlipBoundary, SpawnRegion
 from emerge_engine_b200.materials import FallbackMaterial, Material
 from emerge_engine_b200.simulation import MaterialRegistry
@@ -89,6 +90,9 @@ def lib() -> ctypes.CDLL:
             "oracle_set_threads": (c_int, [c_int]),
             "oracle_svd2": (None, [P(c_float), P(c_float), P(c_float), P(c_float)]),
             "oracle_set_correctly_rounded": (None, [c_int]),
+            "oracle_set_force_fields": (c_int, [c_void_p, P(ForceFieldC), c_uint32, P(c_float),
+                                                c_uint64]),
+            "oracle_field_acceleration": (None, [P(ForceFieldC), P(c_float), P(Particle), P(c_float)]),
             "oracle_polar": (None, [P(c_float), P(c_float)]),
             "oracle_axis_weights": (None, [c_float, P(c_float)]),
             "oracle_kirchhoff": (None, [P(OracleMaterialC), P(Particle), P(c_float)]),
@@ -132,6 +136,7 @@ class OracleSimulation:
             raise ValueError("invalid SimConfig")
         self.registry = MaterialRegistry(FallbackMaterial())
         self.boundaries = [SlipBoundary(config.boundary_thickness)]
+        self.force_fields: list = []
 
     @classmethod
     def empty(cls, config: SimConfig) -> "OracleSimulation":
@@ -178,6 +183,45 @@ class OracleSimulation:
         mid = self.registry.next_id()
         self.set_material(mid, material)
         return mid
+
+    def _upload_fields(self):
+        table, data = pack_fields([f for _, f in self.force_fields])
+        arr = (ForceFieldC * max(len(table), 1))(*table)
+        d = np.asarray(data if data else [0.0], dtype=np.float32)
+        rc = self._lib.oracle_set_force_fields(self._sim, arr, len(table),
+                                               d.ctypes.data_as(POINTER(c_float)), len(data))
+        if rc != 0:
+            raise ValueError("invalid force field")
+
+    def add_named_force_field(self, name, field):
+        self.force_fields.append((str(name), field))
+        self._upload_fields()
+
+    def add_force_field(self, field):
+        self.add_named_force_field(f"force_field_{len(self.force_fields)}", field)
+
+    def with_force_field(self, field):
+        self.add_force_field(field)
+        return self
+
+    def with_named_force_field(self, name, field):
+        self.add_named_force_field(name, field)
+        return self
+
+    def remove_force_field(self, name):
+        for k, (n, _) in enumerate(self.force_fields):
+            if n == name:
+                del self.force_fields[k]
+                self._upload_fields()
+                return True
+        return False
+
+    def clear_force_fields(self):
+        self.force_fields = []
+        self._upload_fields()
+
+    def force_field_names(self):
+        return [n for n, _ in self.force_fields]
 
     def add_boundary_condition(self, b):
         self.boundaries.append(b)

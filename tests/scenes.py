@@ -198,3 +198,46 @@ def material_zoo(sim_cls, kind, grid_res=96, seed=3, dt=0.05, gravity=-1.0, **si
         p["activation_dir"][::2] = (1.0, 0.3)
         sim.set_particles(p)
     return sim
+
+
+def field_scene(sim_cls, asflip=0.0, fields=True, grid_res=96, seed=5, dt=0.05, **sim_kw):
+    """Force fields and ASFLIP: a NeoHookean block (material 0) and a fluid block (material 1,
+    rho0 = 1000 at 4 ppc) in a grid_res^2 grid with gravity (0, -1), every 7th particle
+    pinned, and (fields=True) one field of each device kind in this order: a gravity well
+    with a cutoff, buoyancy, linear drag on material 1, radial and box confinement, a
+    Coulomb source charging material 0, a uniform electric field on material 1 and a
+    chemotaxis ramp phi = x / grid_res.  asflip: SimConfig.asflip_blend."""
+    from emerge_engine_b200 import (AabbConfinementField, BuoyancyField, ChemotaxisField,
+                                    CoulombField, GravityWellField, LinearDragField,
+                                    RadialConfinementField, UniformElectricField)
+    cfg = SimConfig.standard(grid_res, dt, (0.0, -1.0))
+    cfg.asflip_blend = asflip
+    sim = (sim_cls.empty(cfg, **sim_kw)
+           .with_default_material(NeoHookeanMaterial.new(400.0, 200.0))
+           .with_material(1, NewtonianFluidMaterial.low_viscosity(1000.0, 1e4)))
+    a = SpawnRegion.for_sim(cfg)
+    a.spacing, a.box_size, a.box_center = 0.5, (24, 16), (30.0, 20.0)
+    a.position_jitter, a.rng_seed, a.initial_velocity_scale = 0.3, seed, 2.0
+    b = SpawnRegion.for_sim(cfg)
+    b.spacing, b.box_size, b.box_center, b.material_id = 0.5, (20, 20), (grid_res * 0.65, 30.0), 1
+    b.position_jitter, b.rng_seed, b.mass_override = 0.3, seed + 1, 1000.0 * 0.25
+    sim.add_body(a)
+    sim.add_body(b)
+    p = sim.particles()
+    p["pinned"][::7] = 1
+    sim.set_particles(p)
+    if fields:
+        c = grid_res * 0.5
+        chem = ChemotaxisField.new(grid_res, 0.5)
+        chem.sync_from(np.repeat(np.arange(grid_res, dtype=np.float32) / grid_res, grid_res))
+        for f in (GravityWellField.new([((c, c), 40.0), ((c * 0.5, c * 1.5), 15.0)], 0.5, 2.0)
+                  .with_cutoff(grid_res * 0.6),
+                  BuoyancyField.new(2.0, (0.0, -1.0)),
+                  LinearDragField.new((0.5, 0.0), 0.8, 1 << 1),
+                  RadialConfinementField.new((c, c), grid_res * 0.4, 0.3),
+                  AabbConfinementField.new((8.0, 8.0), (grid_res - 8.0, grid_res * 0.6), 0.3),
+                  CoulombField.new([((c, 10.0), 3.0)], {0: 0.5}, 2.0, 1.5).with_cutoff(grid_res * 0.5),
+                  UniformElectricField.for_material((0.3, 0.8), 1, 60.0),
+                  chem):
+            sim.add_force_field(f)
+    return sim
