@@ -28,7 +28,7 @@ __device__ __forceinline__ void count_warp_det(unsigned long long *ctr, bool pre
 __global__ void k_project(DevParticles P, int n, DevConfig cfg, StepState *st) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     bool projected = false;
-    if (i < n) {
+    if (i < n && !(cfg.zones && (P.sleeping[i] & ZB_OUT))) {
         PState p;
         p.x = P.x[i];
         p.v = P.v[i];
@@ -71,8 +71,10 @@ __global__ void k_det_records(DevParticles P, int n, const MatP *mats, int n_mat
     PState p;
     p.x = P.x[s];
     p.mass = P.mass[s];
-    // estimate_particle_volumes_local's AABB filter (density.rs:106-110)
-    const bool skip = filter && (p.x.x < lox || p.x.y < loy || p.x.x > hix || p.x.y > hiy);
+    // estimate_particle_volumes_local's AABB filter (density.rs:106-110); particles outside
+    // the active zone take no part
+    const bool skip = (filter && (p.x.x < lox || p.x.y < loy || p.x.x > hix || p.x.y > hiy)) ||
+                      (cfg.zones && (P.sleeping[s] & ZB_OUT));
     float2 v = v2(0.0f, 0.0f);
     M2 c = mzero(), stress = mzero();
     float stress_coeff = 0.0f;
@@ -144,7 +146,7 @@ __global__ void k_segsum(const uint32_t *keys, const uint32_t *vals, const float
     if (mass_only) {
         g.acc_a[ci].x = m;
     } else {
-        g.acc_a[ci] = make_float4(m, px, py, 0.0f);
+        g.acc_a[ci] = make_float4(m, px, py, 1.0f);  // w > 0: the cell is in the dirty set
     }
     int t = (cx >> 3) * g.tpd + (cy >> 3);
     g.tile_flag[t] = 1;

@@ -26,7 +26,7 @@ void launch_substep_begin(const StepLaunch &L, int use_cond, unsigned long long 
                           int kernels_per_substep);
 void launch_prime_setup(const StepLaunch &L);
 void launch_region_state(const DevParticles &P, int n, float cx, float cy, float r2, void *acc,
-                         cudaStream_t stream);
+                         cudaStream_t stream, int zones = 0);
 size_t region_acc_bytes();
 void region_acc_finalize(const void *acc, emerge_body_state *out);
 void launch_gather_aos(const DevParticles &P, int n, emerge_particle *out, cudaStream_t stream);
@@ -36,9 +36,15 @@ void launch_append_aos(const DevParticles &P, int n_old, int n_new, const emerge
                        cudaStream_t stream);
 void launch_reinit(const DevParticles &P, int n, const MatP *mats, int n_mats, cudaStream_t stream);
 void launch_mass_scatter(const DevParticles &P, int n, const GridView &g, int filter, float lox,
-                         float loy, float hix, float hiy, cudaStream_t stream);
+                         float loy, float hix, float hiy, cudaStream_t stream, int zones = 0);
 void launch_mass_gather(const DevParticles &P, int lo, int hi, const GridView &g, int write_initial,
-                        cudaStream_t stream);
+                        cudaStream_t stream, int zones = 0);
+// sleep partition (step_kernels.cu): wake after P2G, zone bits from the reference index,
+// index remaps after the host's replay of wake / sleep swaps and after add_body
+void launch_wake(const StepLaunch &L, int substep_offset);
+void launch_zone_bits(const DevParticles &P, int n, uint32_t active, cudaStream_t stream);
+void launch_remap_index(const DevParticles &P, int n, const uint32_t *new_of_old, cudaStream_t stream);
+void launch_insert_index(const DevParticles &P, int n_old, int n_new, uint32_t old_active, cudaStream_t stream);
 
 // batched scenes (step_kernels.cu: grid update and controller; fast_kernels.cu: passes)
 void launch_grid_update_batch(const BatchView &b, int n_tiles, cudaStream_t stream);

@@ -429,8 +429,9 @@ __device__ __forceinline__ void scatter_cells(const GridView &g, const ScatterPl
             const float4 t = f4step(r, pl.sy, gy);
             const float wt = w.wx[gx] * w.wy[gy];
             const int ci = xp + yp[gy];
+            // the fourth lane counts scatters: a cell with w > 0 is in the reference's dirty set
             if (SC == SC_MA || (SC == SC_BOTH && do_ma))
-                red_add_v4(&g.acc_a[ci], wm * w.wy[gy], wt * t.x, wt * t.y, 0.0f);
+                red_add_v4(&g.acc_a[ci], wm * w.wy[gy], wt * t.x, wt * t.y, 1.0f);
             if (SC == SC_S || (SC == SC_BOTH && do_s)) red_add_v2(&g.acc_s[ci], wt * t.z, wt * t.w);
         }
     }
@@ -485,7 +486,7 @@ __device__ __forceinline__ void scatter_cells_aggregated(const GridView &g, cons
             const int cx = w.bx + gx - 1, cy = w.by + gy - 1;
             if (head && active && in_domain(cx, cy, g.res)) {
                 const int ci = xp + yp[gy];
-                if (any_ma) red_add_v4(&g.acc_a[ci], mc, ax, ay, 0.0f);
+                if (any_ma) red_add_v4(&g.acc_a[ci], mc, ax, ay, 1.0f);
                 if (any_s) red_add_v2(&g.acc_s[ci], sx, sy);
             }
         }
@@ -773,7 +774,12 @@ __device__ __forceinline__ void particle_pass(const ParticleKernelArgs &a) {
     StepState *st = BATCH ? sd->st : a.st;
     const int i = BATCH ? sd->p0 + (static_cast<int>(blockIdx.x) - sd->block0) * THREADS + static_cast<int>(threadIdx.x)
                         : static_cast<int>(blockIdx.x) * THREADS + static_cast<int>(threadIdx.x);
-    const bool valid = BATCH ? i < sd->p0 + sd->n : i < a.n;
+    const bool in_range = BATCH ? i < sd->p0 + sd->n : i < a.n;
+    // sleep partition: particles outside the active zone take no part in the substep
+    uint32_t zb = 0u;
+    if constexpr (HAS_MODEL(MASK, M_EXTRAS_BIT))
+        if (cfg.zones && in_range) zb = a.P.sleeping[i];
+    const bool valid = in_range && (zb & ZB_OUT) == 0u;
     for (int k = threadIdx.x; k < n_mats; k += THREADS) s_mats[k] = mats[k];
     if (threadIdx.x == 0) {
         s_max_speed = 0u;            // bits of 0.0f
@@ -807,9 +813,11 @@ __device__ __forceinline__ void particle_pass(const ParticleKernelArgs &a) {
         if (a.mode_g2p) {
             o = save_fields(p);
             // the stored state is the unprojected post-G2P state S''(k): recompute its
-            // projection S'(k) (counted when it was first computed)
-            if (a.project_in && cfg.project) project_state(cfg, p);
-            if (density_mode && a.project_in) {
+            // projection S'(k) (counted when it was first computed).  A particle woken after
+            // this substep's P2G was neither projected nor given a density this substep.
+            const bool woken = (zb & ZB_WOKEN) != 0u;
+            if (a.project_in && cfg.project && !woken) project_state(cfg, p);
+            if (density_mode && a.project_in && !woken) {
                 float d = a.P.rho_dp[i];
                 if (d > F32_EPS) {
                     p.rho = d;
@@ -833,11 +841,29 @@ __device__ __forceinline__ void particle_pass(const ParticleKernelArgs &a) {
             closure_count(a.cl, w.smooth, w.kind != 0 ? 1 : 0, (w.smooth && w.kind == 0 && a.cl.infer) ? 1 : 0, err);
         }
     }
+    bool asleep = false;  // sleep scoring at the end of this substep (step.rs:299-315)
     if (valid) {
-        const MatP &m = *mp;
-        if constexpr (HAS_MODEL(MASK, M_EXTRAS_BIT))
-            if (a.mode_g2p) apply_force_fields(cfg, p, dt);
+        if constexpr (HAS_MODEL(MASK, M_EXTRAS_BIT)) {
+            if (a.mode_g2p) {
+                apply_force_fields(cfg, p, dt);
+                if (cfg.sleep_thr > 0.0f && (zb & ZB_FLAG) == 0u) {
+                    const float act = a.lf.activation ? p.activation : a.P.activation[i];
+                    asleep = act == 0.0f && vlen2(p.v) < cfg.sleep_thr * cfg.sleep_thr;
+                }
+            }
+        }
         if (a.mode_g2p) store_fields(a.P, i, o, p);
+        if constexpr (HAS_MODEL(MASK, M_EXTRAS_BIT)) {
+            if (asleep) {
+                a.P.sleeping[i] = ZB_FLAG | ZB_OUT;
+                zone_log(cfg, 2u * static_cast<uint32_t>(st->total_substeps) + 1u, a.P.slot_to_index[i]);
+            } else if (zb & ZB_WOKEN) {
+                a.P.sleeping[i] = zb & ~ZB_WOKEN;
+            }
+        }
+    }
+    if (valid && !asleep) {
+        const MatP &m = *mp;
         // CFL contribution for the next substep (step.rs:447-466)
         float sp = vlen(p.v);
         if (cfg.affine_cfl) sp += affine_cfl(p.c, cfg.cell);
@@ -937,7 +963,9 @@ __device__ __forceinline__ void density_pass(const DensityKernelArgs &a) {
     StepState *st = BATCH ? sd->st : a.st;
     const int i = BATCH ? sd->p0 + (static_cast<int>(blockIdx.x) - sd->block0) * THREADS + static_cast<int>(threadIdx.x)
                         : static_cast<int>(blockIdx.x) * THREADS + static_cast<int>(threadIdx.x);
-    const bool valid = BATCH ? i < sd->p0 + sd->n : i < a.n;
+    bool valid = BATCH ? i < sd->p0 + sd->n : i < a.n;
+    if constexpr (HAS_MODEL(MASK, M_EXTRAS_BIT))
+        if (cfg.zones && valid) valid = (a.P.sleeping[i] & ZB_OUT) == 0u;
     for (int k = threadIdx.x; k < n_mats; k += THREADS) s_mats[k] = mats[k];
     const bool pr = cfg.precise_math != 0;
     // Positions at the projected state S'(k): the stored state itself unless the particle

@@ -935,7 +935,24 @@ struct DevConfig {
     int n_fields;            // force fields, application order
     const emerge_force_field *fields;
     const float *field_data;
+    float sleep_thr;         // sleep_threshold (step.rs:299-315); 0 = no sleep scoring
+    int zones;               // the sleep partition is in use: zone bits live in `sleeping`
+    unsigned long long *zone_log;  // wake / sleep events: (key << 32) | reference index
+    uint32_t *zone_log_count;
+    uint32_t zone_log_cap;
 };
+
+// Bits of DevParticles::sleeping while the sleep partition is in use: bit 0 is
+// Particle::sleeping, bit 1 marks a particle outside the active zone (reference index at or
+// above active_count), bit 2 a particle woken during the running substep.
+constexpr uint32_t ZB_FLAG = 1u, ZB_OUT = 2u, ZB_WOKEN = 4u;
+
+// Records a wake (key = 2 substep) or sleep (key = 2 substep + 1) event of the particle with
+// reference index `index`; the host replays the index swaps in the reference's order.
+__device__ __forceinline__ void zone_log(const DevConfig &cfg, uint32_t key, uint32_t index) {
+    const uint32_t k = atomicAdd(cfg.zone_log_count, 1u);
+    if (k < cfg.zone_log_cap) cfg.zone_log[k] = (static_cast<unsigned long long>(key) << 32) | index;
+}
 
 // smooth_cutoff (spacetime/solver/cutoff.rs:17-26)
 EM_HD float smooth_cutoff(float r, float r_on, float r_cut) {

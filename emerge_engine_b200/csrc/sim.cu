@@ -9,7 +9,9 @@
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
+#include <algorithm>
 #include <cstring>
+#include <functional>
 #include <string>
 #include <vector>
 
@@ -134,6 +136,13 @@ struct emerge_sim {
     int n_fields = 0;
     Buffer fbuf;  // force field table, then its data
 
+    // sleep partition (solver/mod.rs:40-42): reference indices [0, active) are awake
+    uint64_t active = 0;
+    Buffer zbuf;            // event count, event log, index remap table
+    uint32_t zlog_cap = 0;
+    std::vector<uint32_t> pos_of_base, base_of_pos;  // index swaps since the last commit
+    bool perm_dirty = false;
+
     // controller
     Buffer sbuf;
     StepState *d_state = nullptr;
@@ -225,10 +234,6 @@ emerge_status validate_config(const emerge_sim_config &c, std::string &msg) {
         msg = "grid_res above 32768 is not supported by the device grid";
         return EMERGE_ERR_UNSUPPORTED;
     }
-    if (c.sleep_threshold > 0.0f) {
-        msg = "sleep_threshold > 0 (sleep partition) is not on the device path";
-        return EMERGE_ERR_UNSUPPORTED;
-    }
     if (!(c.asflip_blend >= 0.0f)) return bad("asflip_blend must be >= 0");
     if (c.max_substeps_per_step > 0x7fffffffull) {
         msg = "max_substeps_per_step too large";
@@ -268,9 +273,25 @@ DevConfig make_dev_config(const emerge_sim_config &c, const std::vector<uint64_t
     return d;
 }
 
-// The simulation's device configuration: config, boundaries and the force-field table.
+// The sleep partition is in use: sleep scoring is on, or some particle is outside the
+// active zone.
+bool zones_on(const emerge_sim *s) { return s->cfg.sleep_threshold > 0.0f || s->active < s->n; }
+emerge_status drain_zone_log(emerge_sim *s);
+emerge_status commit_perm(emerge_sim *s);
+emerge_status update_zones(emerge_sim *s);
+
+// The simulation's device configuration: config, boundaries, force-field table, sleep
+// partition.
 void refresh_dev_config(emerge_sim *s) {
     s->dcfg = make_dev_config(s->cfg, s->bounds, s->dcfg.precise_math);
+    s->dcfg.sleep_thr = s->cfg.sleep_threshold;
+    s->dcfg.zones = (zones_on(s) && s->zbuf.ptr) ? 1 : 0;
+    if (s->zbuf.ptr) {
+        char *z = static_cast<char *>(s->zbuf.ptr);
+        s->dcfg.zone_log_count = reinterpret_cast<uint32_t *>(z);
+        s->dcfg.zone_log = reinterpret_cast<unsigned long long *>(z + 256);
+        s->dcfg.zone_log_cap = s->zlog_cap;
+    }
     s->dcfg.n_fields = s->n_fields;
     s->dcfg.fields = s->n_fields ? static_cast<const emerge_force_field *>(s->fbuf.ptr) : nullptr;
     s->dcfg.field_data = s->n_fields ? reinterpret_cast<const float *>(
@@ -295,7 +316,7 @@ StepLaunch make_launch(emerge_sim *s) {
     L.use_window = s->use_window;
     L.model_mask = 1u << M_FALLBACK;
     for (const auto &m : s->mats) L.model_mask |= model_bits(m);
-    if (s->dcfg.n_fields > 0 || s->dcfg.asflip > 0.0f) L.model_mask |= 1u << M_EXTRAS_BIT;
+    if (s->dcfg.n_fields > 0 || s->dcfg.asflip > 0.0f || s->dcfg.zones) L.model_mask |= 1u << M_EXTRAS_BIT;
     L.fast = s->deterministic ? 0 : 1;
     L.cl = closure_args(s->closure);
     L.stream = s->stream;
@@ -478,6 +499,13 @@ emerge_status run_host_loop_step(emerge_sim *s, bool timed) {
     CK(cudaMemcpyAsync(s->h_state, s->d_state, sizeof(StepState), cudaMemcpyDeviceToHost, s->stream));
     CK(cudaStreamSynchronize(s->stream));
     while (s->h_state->cont) {
+        // Wake after this substep's P2G (step.rs:107-131), which the previous pass (or the
+        // prime) already scattered.  It runs here, inside the step the substep belongs to,
+        // so that between steps the state is the reference's.
+        if (L.cfg.zones) {
+            launch_wake(L, 1);
+            s->host_launches += 1;
+        }
         CK(cudaEventRecord(s->ev[1], s->stream));
         launch_substep_begin(L, 0, 0ull, 0);
         CK(cudaEventRecord(s->ev[2], s->stream));
@@ -495,6 +523,10 @@ emerge_status run_host_loop_step(emerge_sim *s, bool timed) {
                            s->stream));
         CK(cudaStreamSynchronize(s->stream));
         CK(cudaGetLastError());
+        {
+            emerge_status zst = drain_zone_log(s);
+            if (zst != EMERGE_OK) return zst;
+        }
         float a, b, c, d;
         cudaEventElapsedTime(&a, s->ev[1], s->ev[2]);
         cudaEventElapsedTime(&b, s->ev[2], s->ev[3]);
@@ -518,6 +550,105 @@ emerge_status run_host_loop_step(emerge_sim *s, bool timed) {
         t.density_us = static_cast<uint64_t>(t_dens * 1000.0f);
         t.total_us = static_cast<uint64_t>(tot * 1000.0f);
     }
+    return EMERGE_OK;
+}
+
+// ---------------------------------------------------------------- sleep partition
+// Sizes the event log for the particle capacity (one wake and one sleep per particle per
+// substep at most: the log is drained after every substep) and switches the device
+// configuration to the partition's state.
+emerge_status update_zones(emerge_sim *s) {
+    const bool on = zones_on(s);
+    const uint32_t need = static_cast<uint32_t>(2 * std::max<size_t>(s->cap, 1) + 64);
+    if (on && s->zlog_cap < need) {
+        CK(cudaStreamSynchronize(s->stream));
+        s->zbuf.reset();
+        const size_t bytes = 256 + need * sizeof(unsigned long long) + std::max<size_t>(s->cap, 1) * sizeof(uint32_t);
+        CK(cudaMalloc(&s->zbuf.ptr, bytes));
+        s->zbuf.bytes = bytes;
+        s->zlog_cap = need;
+        CK(cudaMemsetAsync(s->zbuf.ptr, 0, 256, s->stream));
+    }
+    const int want = (on && s->zbuf.ptr) ? 1 : 0;
+    if (want != s->dcfg.zones || (want && s->dcfg.zone_log_cap != s->zlog_cap)) {
+        refresh_dev_config(s);
+        s->graph_dirty = true;
+    }
+    return EMERGE_OK;
+}
+
+void perm_init(emerge_sim *s) {
+    if (s->pos_of_base.size() == s->n) return;
+    s->pos_of_base.resize(s->n);
+    s->base_of_pos.resize(s->n);
+    for (size_t k = 0; k < s->n; ++k) s->pos_of_base[k] = s->base_of_pos[k] = static_cast<uint32_t>(k);
+}
+
+void perm_swap(emerge_sim *s, uint32_t a, uint32_t b) {
+    if (a == b) return;
+    const uint32_t ba = s->base_of_pos[a], bb = s->base_of_pos[b];
+    s->base_of_pos[a] = bb;
+    s->base_of_pos[b] = ba;
+    s->pos_of_base[ba] = b;
+    s->pos_of_base[bb] = a;
+}
+
+// Replays the logged wake / sleep events of the finished substep(s) on the reference
+// indices: per event key in order, wakes in ascending index order swap with the first
+// sleeping particle (particles.rs:252-268), sleeps in descending order with the last active
+// particle (particles.rs:227-245).  The device's indices are updated by commit_perm.
+emerge_status drain_zone_log(emerge_sim *s) {
+    if (!s->dcfg.zones) return EMERGE_OK;
+    uint32_t count = 0;
+    CK(cudaMemcpyAsync(&count, s->dcfg.zone_log_count, sizeof(uint32_t), cudaMemcpyDeviceToHost, s->stream));
+    CK(cudaStreamSynchronize(s->stream));
+    if (count == 0) return EMERGE_OK;
+    if (count > s->zlog_cap)
+        return static_cast<emerge_status>(s->fail(EMERGE_ERR_CUDA, "sleep partition event log overflow"));
+    std::vector<unsigned long long> ev(count);
+    CK(cudaMemcpyAsync(ev.data(), s->dcfg.zone_log, count * sizeof(unsigned long long), cudaMemcpyDeviceToHost,
+                       s->stream));
+    CK(cudaMemsetAsync(s->dcfg.zone_log_count, 0, sizeof(uint32_t), s->stream));
+    CK(cudaStreamSynchronize(s->stream));
+    std::sort(ev.begin(), ev.end());
+    perm_init(s);
+    std::vector<uint32_t> idx;
+    for (size_t a = 0; a < ev.size();) {
+        const uint32_t key = static_cast<uint32_t>(ev[a] >> 32);
+        size_t b = a;
+        idx.clear();
+        for (; b < ev.size() && static_cast<uint32_t>(ev[b] >> 32) == key; ++b)
+            idx.push_back(s->pos_of_base[static_cast<uint32_t>(ev[b])]);
+        if ((key & 1u) == 0u) {  // wake
+            std::sort(idx.begin(), idx.end());
+            for (uint32_t i : idx) {
+                perm_swap(s, i, static_cast<uint32_t>(s->active));
+                s->active += 1;
+            }
+        } else {  // sleep
+            std::sort(idx.begin(), idx.end(), std::greater<uint32_t>());
+            for (uint32_t i : idx) {
+                perm_swap(s, i, static_cast<uint32_t>(s->active - 1));
+                s->active -= 1;
+            }
+        }
+        a = b;
+    }
+    s->perm_dirty = true;
+    return EMERGE_OK;
+}
+
+// Moves the replayed swaps into the device's reference indices.
+emerge_status commit_perm(emerge_sim *s) {
+    if (!s->perm_dirty) return EMERGE_OK;
+    uint32_t *table = reinterpret_cast<uint32_t *>(static_cast<char *>(s->zbuf.ptr) + 256 +
+                                                   s->zlog_cap * sizeof(unsigned long long));
+    CK(cudaMemcpyAsync(table, s->pos_of_base.data(), s->n * sizeof(uint32_t), cudaMemcpyHostToDevice, s->stream));
+    launch_remap_index(s->P[s->cur], static_cast<int>(s->n), table, s->stream);
+    CK(cudaStreamSynchronize(s->stream));
+    CK(cudaGetLastError());
+    for (size_t k = 0; k < s->n; ++k) s->pos_of_base[k] = s->base_of_pos[k] = static_cast<uint32_t>(k);
+    s->perm_dirty = false;
     return EMERGE_OK;
 }
 
@@ -593,7 +724,7 @@ emerge_status run_det_step(emerge_sim *s, bool timed) {
         if (L.density_mode) {  // estimate_particle_volumes(.., false) (density.rs:41-72)
             st = det_scatter(s, L, 0, 0, 0, 0, 0, 0);
             if (st != EMERGE_OK) return st;
-            launch_mass_gather(L.P, 0, L.n, L.g, 0, s->stream);
+            launch_mass_gather(L.P, 0, L.n, L.g, 0, s->stream, L.cfg.zones);
             s->host_launches += 1;
             st = clear_grid(s);
             if (st != EMERGE_OK) return st;
@@ -601,6 +732,10 @@ emerge_status run_det_step(emerge_sim *s, bool timed) {
         CK(cudaEventRecord(s->ev[4], s->stream));
         st = det_scatter(s, L, 1, 0, 0, 0, 0, 0);
         if (st != EMERGE_OK) return st;
+        if (L.cfg.zones) {  // wake after this substep's P2G (step.rs:107-131)
+            launch_wake(L, 0);
+            s->host_launches += 1;
+        }
         CK(cudaEventRecord(s->ev[5], s->stream));
         launch_grid_update(L);
         CK(cudaEventRecord(s->ev[6], s->stream));
@@ -611,6 +746,11 @@ emerge_status run_det_step(emerge_sim *s, bool timed) {
                            s->stream));
         CK(cudaStreamSynchronize(s->stream));
         CK(cudaGetLastError());
+        if (L.cfg.zones) {  // the next substep's records follow the new index order
+            st = drain_zone_log(s);
+            if (st == EMERGE_OK) st = commit_perm(s);
+            if (st != EMERGE_OK) return st;
+        }
         float a, b, c, d, e, f;
         cudaEventElapsedTime(&a, s->ev[1], s->ev[2]);
         cudaEventElapsedTime(&b, s->ev[2], s->ev[3]);
@@ -712,14 +852,26 @@ emerge_status append_particles(emerge_sim *s, const emerge_particle *src, size_t
     if (st != EMERGE_OK) return st;
     for (size_t k = 0; k < count; ++k)
         if (src[k].pinned) s->lf.pinned = 1;
+    st = commit_perm(s);
+    if (st != EMERGE_OK) return st;
     const int n_old = static_cast<int>(s->n), n_new = static_cast<int>(s->n + count);
+    const uint64_t old_active = s->active;
     if (count > 0) {
         CK(cudaMemcpyAsync(s->d_aos, src, count * sizeof(emerge_particle), cudaMemcpyHostToDevice,
                            s->stream));
         launch_append_aos(s->P[s->cur], n_old, n_new, s->d_aos, s->stream);
         s->host_launches += 1;
+        // new particles go before the sleeping zone (particles.rs:389-410)
+        if (old_active < static_cast<uint64_t>(n_old))
+            launch_insert_index(s->P[s->cur], n_old, n_new, static_cast<uint32_t>(old_active), s->stream);
     }
     s->n = static_cast<size_t>(n_new);
+    s->active = old_active + count;
+    s->pos_of_base.clear();
+    s->base_of_pos.clear();
+    st = update_zones(s);
+    if (st != EMERGE_OK) return st;
+    if (s->dcfg.zones) launch_zone_bits(s->P[s->cur], n_new, static_cast<uint32_t>(s->active), s->stream);
     if (volume_mode != 0 && count > 0) {
         // estimate_particle_volumes_local (density.rs:81-144) / estimate_particle_volumes (:41-72)
         int filter = 0;
@@ -746,9 +898,11 @@ emerge_status append_particles(emerge_sim *s, const emerge_particle *src, size_t
             emerge_status dst = det_scatter(s, L, 0, filter, lox, loy, hix, hiy);
             if (dst != EMERGE_OK) return dst;
         } else {
-            launch_mass_scatter(s->P[s->cur], n_new, s->g, filter, lox, loy, hix, hiy, s->stream);
+            launch_mass_scatter(s->P[s->cur], n_new, s->g, filter, lox, loy, hix, hiy, s->stream,
+                                s->dcfg.zones);
         }
-        launch_mass_gather(s->P[s->cur], volume_mode == 1 ? n_old : 0, n_new, s->g, 1, s->stream);
+        launch_mass_gather(s->P[s->cur], volume_mode == 1 ? n_old : 0, n_new, s->g, 1, s->stream,
+                           s->dcfg.zones);
         CK(cudaMemsetAsync(s->g.acc_a, 0, cells * sizeof(float4), s->stream));
         CK(cudaMemsetAsync(s->g.acc_s, 0, cells * sizeof(float2), s->stream));
         CK(cudaMemsetAsync(s->g.tile_flag, 0, static_cast<size_t>(s->tpd) * s->tpd, s->stream));
@@ -913,6 +1067,7 @@ emerge_status emerge_cuda_destroy(emerge_sim *s) {
     s->gbuf.reset();
     s->mbuf.reset();
     s->fbuf.reset();
+    s->zbuf.reset();
     s->sbuf.reset();
     s->sortbuf.reset();
     s->region_buf.reset();
@@ -1080,6 +1235,33 @@ emerge_status emerge_cuda_write_particles(emerge_sim *s, const emerge_particle *
     }
     launch_scatter_aos(s->P[s->cur], static_cast<int>(n), s->d_aos, s->stream);
     s->host_launches += 1;
+    if (s->dcfg.zones) launch_zone_bits(s->P[s->cur], static_cast<int>(n), static_cast<uint32_t>(s->active), s->stream);
+    CK(cudaGetLastError());
+    return invalidate_pending(s);
+}
+
+emerge_status emerge_cuda_active_count(emerge_sim *s, uint64_t *out) {
+    if (!s || !out) return EMERGE_ERR_INVALID_ARG;
+    *out = s->active;
+    return EMERGE_OK;
+}
+
+emerge_status emerge_cuda_replace_particles(emerge_sim *s, const emerge_particle *in, uint64_t n,
+                                            uint64_t active_count) {
+    if (!s || (!in && n)) return EMERGE_ERR_INVALID_ARG;
+    if (active_count > n)
+        return static_cast<emerge_status>(s->fail(EMERGE_ERR_INVALID_ARG, "active_count above the particle count"));
+    if (s->stream) CK(cudaStreamSynchronize(s->stream));
+    s->n = 0;
+    s->active = 0;
+    s->lf.pinned = 0;
+    emerge_status st = append_particles(s, in, n, 0);
+    if (st != EMERGE_OK) return st;
+    s->active = active_count;
+    st = update_zones(s);
+    if (st != EMERGE_OK) return st;
+    if (s->dcfg.zones) launch_zone_bits(s->P[s->cur], static_cast<int>(n), static_cast<uint32_t>(active_count), s->stream);
+    s->graph_dirty = true;
     CK(cudaGetLastError());
     return invalidate_pending(s);
 }
@@ -1097,10 +1279,12 @@ emerge_status emerge_cuda_step(emerge_sim *s, uint32_t n_steps, emerge_step_timi
             st = prime(s);
             if (st != EMERGE_OK) return st;
         }
+        st = update_zones(s);
+        if (st != EMERGE_OK) return st;
         if (s->deterministic) {
             st = run_det_step(s, timing != nullptr);
             if (st != EMERGE_OK) return st;
-        } else if (s->use_graph) {
+        } else if (s->use_graph && !s->dcfg.zones) {
             if (s->graph_dirty || !s->graph_exec) {
                 st = build_graph(s);
                 if (st != EMERGE_OK) return st;
@@ -1123,6 +1307,12 @@ emerge_status emerge_cuda_step(emerge_sim *s, uint32_t n_steps, emerge_step_timi
         }
         CK(cudaMemcpyAsync(s->h_state, s->d_state, sizeof(StepState), cudaMemcpyDeviceToHost, s->stream));
         s->steps_since_sort += 1;
+        if (s->dcfg.zones) {  // the step's wakes and sleeps into the reference indices
+            st = drain_zone_log(s);
+            if (st == EMERGE_OK) st = commit_perm(s);
+            if (st == EMERGE_OK) st = update_zones(s);
+            if (st != EMERGE_OK) return st;
+        }
     }
     CK(cudaGetLastError());
     if (timing) {
@@ -1181,7 +1371,7 @@ emerge_status emerge_cuda_region_state(emerge_sim *s, float cx, float cy, float 
     CK(cudaMemcpyAsync(static_cast<char *>(s->region_buf.ptr) + region_acc_bytes() - 8, &zero_ordered, 4,
                        cudaMemcpyHostToDevice, s->stream));
     launch_region_state(s->P[s->cur], static_cast<int>(s->n), cx, cy, radius * radius, s->region_buf.ptr,
-                        s->stream);
+                        s->stream, s->dcfg.zones);
     s->host_launches += 1;
     CK(cudaMemcpyAsync(acc.data(), s->region_buf.ptr, acc.size(), cudaMemcpyDeviceToHost, s->stream));
     CK(cudaStreamSynchronize(s->stream));

@@ -228,7 +228,7 @@ __device__ __forceinline__ unsigned int float_to_ordered(float f) {
 
 // region_state (queries.rs:125-141) as a device reduction (f64 partial sums).
 __global__ void k_region_state(DevParticles P, int n, float cx, float cy, float r2,
-                               RegionAcc *out) {
+                               RegionAcc *out, int zones) {
     __shared__ double sh[6][256 / 32];
     __shared__ unsigned long long shc[256 / 32];
     __shared__ unsigned int shm[256 / 32];
@@ -238,7 +238,8 @@ __global__ void k_region_state(DevParticles P, int n, float cx, float cy, float 
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         float2 x = P.x[i];
         float2 d = vsub(x, v2(cx, cy));
-        if (vlen2(d) <= r2) {
+        // the spatial hash holds the active zone only (step.rs:53-56)
+        if (vlen2(d) <= r2 && !(zones && (P.sleeping[i] & ZB_OUT))) {
             cnt += 1;
             sx += x.x;
             sy += x.y;
@@ -315,7 +316,7 @@ __global__ void k_gather_aos(DevParticles P, int n, emerge_particle *out) {
     q.activation_dir[0] = ad.x; q.activation_dir[1] = ad.y;
     q.muscle_group_id = P.muscle[s];
     q.contact_group = P.contact[s];
-    q.sleeping = P.sleeping[s];
+    q.sleeping = P.sleeping[s] & ZB_FLAG;
     q.pinned = P.pinned[s];
     q.scalar_field = P.scalar[s];
     q.pad_ = 0;
@@ -394,9 +395,9 @@ __global__ void k_reinit(DevParticles P, int n, const MatP *mats, int n_mats) {
 
 // Mass scatter of estimate_particle_volumes(_local) (density.rs:47-48, 105-120).
 __global__ void k_mass_scatter(DevParticles P, int n, GridView g, int filter, float lox, float loy,
-                               float hix, float hiy) {
+                               float hix, float hiy, int zones) {
     int s = blockIdx.x * blockDim.x + threadIdx.x;
-    if (s >= n) return;
+    if (s >= n || (zones && (P.sleeping[s] & ZB_OUT))) return;
     float2 x = P.x[s];
     if (filter && (x.x < lox || x.y < loy || x.x > hix || x.y > hiy)) return;
     float mass = P.mass[s];
@@ -412,9 +413,9 @@ __global__ void k_mass_scatter(DevParticles P, int n, GridView g, int filter, fl
 
 // Density gather of estimate_particle_volumes(_local) (density.rs:50-71, 122-143)
 // for slots [lo, hi).
-__global__ void k_mass_gather(DevParticles P, int lo, int hi, GridView g, int write_initial) {
+__global__ void k_mass_gather(DevParticles P, int lo, int hi, GridView g, int write_initial, int zones) {
     int s = lo + blockIdx.x * blockDim.x + threadIdx.x;
-    if (s >= hi) return;
+    if (s >= hi || (zones && (P.sleeping[s] & ZB_OUT))) return;
     float2 x = P.x[s];
     float mass = P.mass[s];
     QW w = quadratic_weights(x);
@@ -432,6 +433,70 @@ __global__ void k_mass_gather(DevParticles P, int lo, int hi, GridView g, int wr
         P.vol[s] = vol;
         if (write_initial) P.v0[s] = vol;
     }
+}
+
+// ---------------------------------------------------------------- sleep partition
+// Wake after P2G (step.rs:107-131): a particle outside the active zone whose stencil
+// overlaps a cell of this substep's scatter (acc_a.w > 0) joins the active zone.  `key`
+// is the event key of the substep the P2G belongs to.
+__global__ void k_wake(DevParticles P, int n, GridView g, DevConfig cfg, const StepState *st,
+                       int substep_offset) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= n || !(P.sleeping[s] & ZB_OUT)) return;
+    const QW w = quadratic_weights(P.x[s]);
+    bool hit = false;
+    for (int gx = 0; gx < 3; ++gx)
+        for (int gy = 0; gy < 3; ++gy) {
+            const int cx = w.bx + gx - 1, cy = w.by + gy - 1;
+            if (in_domain(cx, cy, g.res) && g.acc_a[cell_index(cx, cy, g.tpd)].w > 0.0f) hit = true;
+        }
+    if (!hit) return;
+    // The woken particle's G2P reads all 9 stencil cells, some of which this substep's P2G
+    // may not have touched: flag their tiles so the grid update writes their velocity (zero
+    // for an untouched cell, as Grid::velocity_at) instead of leaving an older substep's.
+    mark_tiles(g, w.bx, w.by);
+    P.sleeping[s] = ZB_WOKEN;  // wake_particle clears the flag (particles.rs:252-268)
+    zone_log(cfg, 2u * static_cast<uint32_t>(st->total_substeps + substep_offset), P.slot_to_index[s]);
+}
+
+// Zone bits from the reference index: outside the active zone iff index >= active.
+__global__ void k_zone_bits(DevParticles P, int n, uint32_t active) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= n) return;
+    P.sleeping[s] = (P.sleeping[s] & ZB_FLAG) | (P.slot_to_index[s] >= active ? ZB_OUT : 0u);
+}
+
+// Reference indices after the host replayed wake / sleep swaps: index := new_of_old[index].
+__global__ void k_remap_index(DevParticles P, int n, const uint32_t *new_of_old) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s < n) P.slot_to_index[s] = new_of_old[P.slot_to_index[s]];
+}
+
+// add_body with a sleeping zone (particles.rs:389-410): the new particles (slots [n_old,
+// n_new)) take indices [old_active, old_active + count), the sleeping zone moves up.
+__global__ void k_insert_index(DevParticles P, int n_old, int n_new, uint32_t old_active) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= n_new) return;
+    const uint32_t count = static_cast<uint32_t>(n_new - n_old);
+    if (s >= n_old) {
+        P.slot_to_index[s] = old_active + static_cast<uint32_t>(s - n_old);
+    } else {
+        const uint32_t idx = P.slot_to_index[s];
+        if (idx >= old_active) P.slot_to_index[s] = idx + count;
+    }
+}
+
+void launch_wake(const StepLaunch &L, int substep_offset) {
+    if (L.n > 0) k_wake<<<blocks_for(L.n, 256), 256, 0, L.stream>>>(L.P, L.n, L.g, L.cfg, L.st, substep_offset);
+}
+void launch_zone_bits(const DevParticles &P, int n, uint32_t active, cudaStream_t stream) {
+    if (n > 0) k_zone_bits<<<blocks_for(n, 256), 256, 0, stream>>>(P, n, active);
+}
+void launch_remap_index(const DevParticles &P, int n, const uint32_t *new_of_old, cudaStream_t stream) {
+    if (n > 0) k_remap_index<<<blocks_for(n, 256), 256, 0, stream>>>(P, n, new_of_old);
+}
+void launch_insert_index(const DevParticles &P, int n_old, int n_new, uint32_t old_active, cudaStream_t stream) {
+    if (n_new > 0) k_insert_index<<<blocks_for(n_new, 256), 256, 0, stream>>>(P, n_old, n_new, old_active);
 }
 
 // ---------------------------------------------------------------- launchers
@@ -505,11 +570,11 @@ void launch_substep_begin(const StepLaunch &L, int use_cond, unsigned long long 
 void launch_prime_setup(const StepLaunch &L) { k_prime_setup<<<1, 1, 0, L.stream>>>(L.st); }
 
 void launch_region_state(const DevParticles &P, int n, float cx, float cy, float r2, void *acc,
-                         cudaStream_t stream) {
+                         cudaStream_t stream, int zones) {
     int blocks = blocks_for(n, 256);
     if (blocks > 148 * 8) blocks = 148 * 8;
     if (blocks < 1) blocks = 1;
-    k_region_state<<<blocks, 256, 0, stream>>>(P, n, cx, cy, r2, static_cast<RegionAcc *>(acc));
+    k_region_state<<<blocks, 256, 0, stream>>>(P, n, cx, cy, r2, static_cast<RegionAcc *>(acc), zones);
 }
 
 size_t region_acc_bytes() { return sizeof(RegionAcc); }
@@ -556,12 +621,12 @@ void launch_reinit(const DevParticles &P, int n, const MatP *mats, int n_mats, c
     if (n) k_reinit<<<blocks_for(n, 256), 256, 0, stream>>>(P, n, mats, n_mats);
 }
 void launch_mass_scatter(const DevParticles &P, int n, const GridView &g, int filter, float lox,
-                         float loy, float hix, float hiy, cudaStream_t stream) {
-    if (n) k_mass_scatter<<<blocks_for(n, 256), 256, 0, stream>>>(P, n, g, filter, lox, loy, hix, hiy);
+                         float loy, float hix, float hiy, cudaStream_t stream, int zones) {
+    if (n) k_mass_scatter<<<blocks_for(n, 256), 256, 0, stream>>>(P, n, g, filter, lox, loy, hix, hiy, zones);
 }
 void launch_mass_gather(const DevParticles &P, int lo, int hi, const GridView &g, int write_initial,
-                        cudaStream_t stream) {
-    if (hi > lo) k_mass_gather<<<blocks_for(hi - lo, 256), 256, 0, stream>>>(P, lo, hi, g, write_initial);
+                        cudaStream_t stream, int zones) {
+    if (hi > lo) k_mass_gather<<<blocks_for(hi - lo, 256), 256, 0, stream>>>(P, lo, hi, g, write_initial, zones);
 }
 
 }  // namespace emerge

@@ -14,7 +14,7 @@ from ctypes import byref, c_float, c_uint32, c_uint64, c_void_p
 
 import numpy as np
 
-from . import abi
+from . import abi, lifecycle
 from .abi import (PARTICLE_DTYPE, BodyStateC, MaterialParamsC, StepTimingC, check,
                   load_library)
 from .config import BodyState, SimConfig, SlipBoundary, SpawnRegion
@@ -142,6 +142,40 @@ class Simulation:
         mid = self.registry.next_id()
         self.set_material(mid, material)
         return mid
+
+    # ---------------------------------------------------------------- sleep partition
+    def active_count(self) -> int:
+        """Simulation::active_count (particles.rs:314)."""
+        out = c_uint64()
+        self._check(self._lib.emerge_cuda_active_count(self._sim, byref(out)))
+        return int(out.value)
+
+    def _replace(self, particles: np.ndarray, active: int) -> None:
+        arr = np.ascontiguousarray(particles, dtype=PARTICLE_DTYPE)
+        self._check(self._lib.emerge_cuda_replace_particles(
+            self._sim, arr.ctypes.data_as(c_void_p), len(arr), int(active)))
+
+    def wake_tag(self, tag: int) -> None:
+        self._replace(*lifecycle.wake_tag(self.particles(), self.active_count(), int(tag)))
+
+    def sleep_tag(self, tag: int) -> None:
+        self._replace(*lifecycle.sleep_tag(self.particles(), self.active_count(), int(tag)))
+
+    def remove_particles(self, predicate) -> int:
+        """remove_particles (particles.rs:177-205); returns the number removed."""
+        p, active, removed = lifecycle.remove_particles(self.particles(), self.active_count(), predicate)
+        if removed:
+            self._replace(p, active)
+        return removed
+
+    def retain_particles(self, predicate) -> None:
+        """retain_particles (lifecycle.rs:237-253)."""
+        self._replace(*lifecycle.retain_particles(self.particles(), self.active_count(), predicate))
+
+    def split_particles(self, should_split, jitter: float) -> None:
+        """split_particles (lifecycle.rs:271-310)."""
+        self._replace(*lifecycle.split_particles(self.particles(), self.active_count(), should_split,
+                                                 jitter))
 
     # ---------------------------------------------------------------- force fields
     def _upload_fields(self) -> None:

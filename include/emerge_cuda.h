@@ -92,7 +92,7 @@ typedef struct emerge_sim_config {
     uint64_t max_substeps_per_step;
     float apic_blend;
     float j_max;
-    float sleep_threshold;          /* must be 0: the sleep partition is not on the device path */
+    float sleep_threshold;          /* sleep scoring speed (step.rs:299-315); 0 = off */
     float contact_friction;
     float asflip_blend;             /* ASFLIP FLIP blend (transfer/g2p.rs:263-296); 0 = APIC only */
     float mixture_drag_coefficient;
@@ -210,6 +210,22 @@ emerge_status emerge_cuda_set_materials(emerge_sim *sim, const emerge_material_p
  * set_boundary_condition :353 replaces). */
 emerge_status emerge_cuda_set_slip_boundaries(emerge_sim *sim, const uint64_t *thickness,
                                               uint32_t n);
+
+/* ---- sleep partition ---------------------------------------------------------- */
+
+/* Simulation::active_count (particles.rs:314): reference indices [0, active) are awake.
+ * With SimConfig::sleep_threshold > 0 particles below the speed threshold with zero
+ * activation sleep at the end of every substep and sleeping particles whose stencil meets
+ * a cell of a substep's P2G wake (step.rs:107-131, 299-315); sleep_particle / wake_particle
+ * swap reference indices exactly as the reference (particles.rs:227-268). */
+emerge_status emerge_cuda_active_count(emerge_sim *sim, uint64_t *active_count);
+
+/* Replaces every particle (reference order) and the active-zone size: the write-back of
+ * the reference's particle-set edits that take host predicates (remove_particles
+ * particles.rs:177-205, retain_particles lifecycle.rs:237-253, split_particles :271-310,
+ * wake_tag / sleep_tag particles.rs:271-312), which a shim runs on the host copy. */
+emerge_status emerge_cuda_replace_particles(emerge_sim *sim, const emerge_particle *particles,
+                                            uint64_t n, uint64_t active_count);
 
 /* ---- force fields ------------------------------------------------------------- */
 

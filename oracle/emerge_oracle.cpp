@@ -26,6 +26,7 @@
 #include "emerge_oracle.h"
 
 #include <algorithm>
+#include <functional>
 #include <chrono>
 #include <cmath>
 #include <cstring>
@@ -912,6 +913,11 @@ struct Grid {
         pre.assign(r * r, v2(0, 0));
         dirty.clear();
     }
+    // cell_is_active (grid/mod.rs:231-241): the cell is in the dirty set
+    bool cell_is_active(IV2 c) const {
+        uint32_t idx;
+        return flat_index(c, idx) && touched[idx];
+    }
     // snapshot_velocities / pre_force_velocity_at (grid/mod.rs:300-317): the snapshot's
     // keys are the dirty cells, which stay touched until the next clear.
     V2 pre_force_velocity_at(IV2 c) const {
@@ -1511,6 +1517,54 @@ void apply_force_fields(oracle_sim &s, float dt) {
     }
 }
 
+// sleep_particle (solver/particles.rs:227-245): flag, swap with the last active particle
+// (Particles::swap moves every field, particle.rs:403-429), shrink the active zone.
+void sleep_particle(oracle_sim &s, size_t i) {
+    if (s.p[i].sleeping || s.active_count == 0) return;
+    s.p[i].sleeping = 1;
+    size_t last_active = s.active_count - 1;
+    if (i != last_active) std::swap(s.p[i], s.p[last_active]);
+    s.active_count -= 1;
+}
+
+// wake_particle (solver/particles.rs:252-268): swap with the first sleeping particle.
+void wake_particle(oracle_sim &s, size_t i) {
+    if (!s.p[i].sleeping) return;
+    s.p[i].sleeping = 0;
+    size_t first_sleeping = s.active_count;
+    if (i != first_sleeping) std::swap(s.p[i], s.p[first_sleeping]);
+    s.active_count += 1;
+}
+
+// Wake after P2G (step.rs:107-131): sleeping particles whose stencil overlaps an active
+// cell, woken in ascending index order.
+void wake_touched(oracle_sim &s) {
+    if (s.active_count >= s.p.size()) return;
+    std::vector<size_t> to_wake;
+    for (size_t i = s.active_count; i < s.p.size(); ++i) {
+        QW w = quadratic_weights(load_v(s.p[i].x));
+        bool hit = false;
+        for (int gx = 0; gx < 3 && !hit; ++gx)
+            for (int gy = 0; gy < 3 && !hit; ++gy)
+                hit = s.grid.cell_is_active(IV2{w.base.x + gx - 1, w.base.y + gy - 1});
+        if (hit) to_wake.push_back(i);
+    }
+    for (size_t i : to_wake) wake_particle(s, i);
+}
+
+// Sleep scoring at the end of a substep (step.rs:299-315): active particles with zero
+// activation and speed below the threshold, put to sleep in descending index order.
+void sleep_scoring(oracle_sim &s) {
+    const float threshold = s.cfg.sleep_threshold;
+    if (!(threshold > 0.0f)) return;
+    const float threshold_sq = threshold * threshold;
+    std::vector<size_t> to_sleep;
+    for (size_t i = 0; i < s.active_count; ++i)
+        if (s.p[i].activation == 0.0f && length_sq(load_v(s.p[i].v)) < threshold_sq) to_sleep.push_back(i);
+    std::sort(to_sleep.begin(), to_sleep.end(), std::greater<size_t>());
+    for (size_t i : to_sleep) sleep_particle(s, i);
+}
+
 // Simulation::do_substep (step.rs:62-317) restricted to the gated-on phases.
 void do_substep(oracle_sim &s, float sub_dt) {
     auto t0 = clk::now();
@@ -1525,6 +1579,7 @@ void do_substep(oracle_sim &s, float sub_dt) {
     t0 = clk::now();
     s.grid.clear();
     p2g(s, sub_dt);
+    wake_touched(s);
     s.timing[3] += us_since(t0);
     t0 = clk::now();
     grid_update(s, sub_dt);
@@ -1533,6 +1588,7 @@ void do_substep(oracle_sim &s, float sub_dt) {
     s.last_vel_clamp_count += g2p(s, sub_dt);
     s.timing[5] += us_since(t0);
     apply_force_fields(s, sub_dt);
+    sleep_scoring(s);
 }
 
 // Simulation::step (step.rs:23-60)
@@ -1609,9 +1665,10 @@ int oracle_add_body(oracle_sim *s, const oracle_spawn *spawn, uint32_t *tag_out)
         q.user_tag = tag;
         if (registered) init_particle(s->materials[spawn->material_id], q);
     }
-    // No sleeping partition (sleep_threshold = 0): new particles append at the end.
-    s->p.insert(s->p.end(), np.begin(), np.end());
-    s->active_count = s->p.size();
+    // New particles go before the sleeping zone (particles.rs:389-410): a rotation keeps
+    // [active | new | sleeping].
+    s->p.insert(s->p.begin() + static_cast<long>(old_active), np.begin(), np.end());
+    s->active_count = old_active + np.size();
     estimate_particle_volumes_local(*s, s->active_count, old_active, true);
     if (tag_out) *tag_out = tag;
     return 0;
@@ -1637,6 +1694,32 @@ void oracle_step(oracle_sim *s, uint32_t n_steps) {
 }
 
 uint64_t oracle_particle_count(const oracle_sim *s) { return s->p.size(); }
+
+uint64_t oracle_active_count(const oracle_sim *s) { return s->active_count; }
+
+int oracle_replace_particles(oracle_sim *s, const oracle_particle *p, uint64_t n, uint64_t active_count) {
+    if (active_count > n) return -1;
+    s->p.assign(p, p + n);
+    s->active_count = static_cast<size_t>(active_count);
+    return 0;
+}
+
+// wake_tag / sleep_tag (solver/particles.rs:271-312); the tag's members are the particles
+// carrying the tag.
+void oracle_wake_tag(oracle_sim *s, uint32_t tag) {
+    std::vector<size_t> idx;
+    for (size_t i = 0; i < s->p.size(); ++i)
+        if (s->p[i].user_tag == tag && s->p[i].sleeping) idx.push_back(i);
+    for (size_t i : idx) wake_particle(*s, i);  // ascending
+}
+
+void oracle_sleep_tag(oracle_sim *s, uint32_t tag) {
+    std::vector<size_t> idx;
+    for (size_t i = 0; i < s->p.size(); ++i)
+        if (s->p[i].user_tag == tag && !s->p[i].sleeping) idx.push_back(i);
+    std::sort(idx.begin(), idx.end(), std::greater<size_t>());
+    for (size_t i : idx) sleep_particle(*s, i);
+}
 
 void oracle_read_particles(const oracle_sim *s, oracle_particle *out) {
     std::memcpy(out, s->p.data(), s->p.size() * sizeof(P));

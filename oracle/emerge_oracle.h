@@ -200,6 +200,12 @@ int oracle_set_force_fields(oracle_sim *s, const oracle_force_field *fields, uin
 void oracle_field_acceleration(const oracle_force_field *f, const float *data,
                                const oracle_particle *p, float out[2]);
 uint64_t oracle_particle_count(const oracle_sim *s);
+/* active_count (solver/mod.rs:40-42): particles [0, active_count) are awake. */
+uint64_t oracle_active_count(const oracle_sim *s);
+/* Replaces the particle array (reference order) and the active-zone size. */
+int oracle_replace_particles(oracle_sim *s, const oracle_particle *p, uint64_t n, uint64_t active_count);
+void oracle_wake_tag(oracle_sim *s, uint32_t tag);
+void oracle_sleep_tag(oracle_sim *s, uint32_t tag);
 void oracle_read_particles(const oracle_sim *s, oracle_particle *out);
 void oracle_write_particles(oracle_sim *s, const oracle_particle *in);
 void oracle_region_state(const oracle_sim *s, float cx, float cy, float r,

@@ -16,6 +16,7 @@ import numpy as np
 
 from emerge_engine_b200.abi import (PARTICLE_DTYPE, BodyStateC, ForceFieldC, Particle,
                                     SimConfigC, SpawnRegionC)
+from emerge_engine_b200 import lifecycle
 from emerge_engine_b200.fields import pack_fields
 from emerge_engine_b200.config import BodyState, SimConfig, SlipBoundary, SpawnRegion
 from emerge_engine_b200.materials import FallbackMaterial, Material
@@ -93,6 +94,10 @@ def lib() -> ctypes.CDLL:
             "oracle_set_force_fields": (c_int, [c_void_p, P(ForceFieldC), c_uint32, P(c_float),
                                                 c_uint64]),
             "oracle_field_acceleration": (None, [P(ForceFieldC), P(c_float), P(Particle), P(c_float)]),
+            "oracle_active_count": (c_uint64, [c_void_p]),
+            "oracle_replace_particles": (c_int, [c_void_p, c_void_p, c_uint64, c_uint64]),
+            "oracle_wake_tag": (None, [c_void_p, c_uint32]),
+            "oracle_sleep_tag": (None, [c_void_p, c_uint32]),
             "oracle_polar": (None, [P(c_float), P(c_float)]),
             "oracle_axis_weights": (None, [c_float, P(c_float)]),
             "oracle_kirchhoff": (None, [P(OracleMaterialC), P(Particle), P(c_float)]),
@@ -259,6 +264,36 @@ class OracleSimulation:
         arr = np.ascontiguousarray(particles, dtype=PARTICLE_DTYPE)
         assert len(arr) == self.particle_count()
         self._lib.oracle_write_particles(self._sim, arr.ctypes.data_as(c_void_p))
+
+    # ---------------------------------------------------------------- sleep partition
+    def active_count(self) -> int:
+        return int(self._lib.oracle_active_count(self._sim))
+
+    def _replace(self, particles, active: int) -> None:
+        arr = np.ascontiguousarray(particles, dtype=PARTICLE_DTYPE)
+        if self._lib.oracle_replace_particles(self._sim, arr.ctypes.data_as(c_void_p), len(arr),
+                                              int(active)) != 0:
+            raise ValueError("active count above particle count")
+
+    def wake_tag(self, tag: int) -> None:
+        self._lib.oracle_wake_tag(self._sim, int(tag))
+
+    def sleep_tag(self, tag: int) -> None:
+        self._lib.oracle_sleep_tag(self._sim, int(tag))
+
+    def remove_particles(self, predicate) -> int:
+        p, active, removed = lifecycle.remove_particles(self.particles(), self.active_count(), predicate)
+        if removed:
+            self._replace(p, active)
+        return removed
+
+    def retain_particles(self, predicate) -> None:
+        p, active = lifecycle.retain_particles(self.particles(), self.active_count(), predicate)
+        self._replace(p, active)
+
+    def split_particles(self, should_split, jitter: float) -> None:
+        p, active = lifecycle.split_particles(self.particles(), self.active_count(), should_split, jitter)
+        self._replace(p, active)
 
     def step(self):
         self._lib.oracle_step(self._sim, 1)

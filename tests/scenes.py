@@ -241,3 +241,28 @@ def field_scene(sim_cls, asflip=0.0, fields=True, grid_res=96, seed=5, dt=0.05, 
                   chem):
             sim.add_force_field(f)
     return sim
+
+
+def sleep_scene(sim_cls, threshold=0.05, grid_res=96, seed=9, dt=0.05, **sim_kw):
+    """Sleep partition: NeoHookean (400, 200) at 4 ppc in a grid_res^2 grid, gravity (0, -1),
+    sleep_threshold `threshold`.  Tag 1: a 32 x 10 block resting on the floor (asleep after
+    its first substep); tag 2: a disk of radius 6 launched at (6, -1) toward it (wakes it on
+    contact); tag 3: an 8 x 8 block with activation 0.5, which never sleeps."""
+    cfg = SimConfig.standard(grid_res, dt, (0.0, -1.0))
+    cfg.sleep_threshold = threshold
+    t = cfg.boundary_thickness
+    sim = sim_cls.empty(cfg, **sim_kw).with_default_material(NeoHookeanMaterial.new(400.0, 200.0))
+    a = SpawnRegion.for_sim(cfg)
+    a.spacing, a.box_size, a.box_center = 0.5, (32, 10), (56.0, t + 1 + 5.0)
+    a.position_jitter, a.rng_seed = 0.3, seed
+    b = SpawnRegion.for_sim(cfg).disk(6.0)
+    b.spacing, b.box_center, b.position_jitter, b.rng_seed = 0.5, (30.0, 14.0), 0.3, seed + 1
+    c = SpawnRegion.for_sim(cfg)
+    c.spacing, c.box_size, c.box_center = 0.5, (8, 8), (80.0, 50.0)
+    for s in (a, b, c):
+        sim.add_body(s)
+    p = sim.particles()
+    p["v"][p["user_tag"] == 2] = (6.0, -1.0)
+    p["activation"][p["user_tag"] == 3] = 0.5
+    sim.set_particles(p)
+    return sim
