@@ -50,6 +50,26 @@ WORKLOADS = {
                               desc="mixed granular: seeded blocks 16-128 cells, DruckerPrager / "
                                    "Stomakhin snow / NACC, 4 ppc, 1024^2 grid",
                               material="DP+Snow+NACC", grid_res=1024),
+    "material_zoo_4m": dict(builder="model_blocks",
+                            kwargs=dict(grid_res=1024, target_particles=4_000_000),
+                            desc="the seven further constitutive models at scale: seeded blocks "
+                                 "16-128 cells, each Corotated / VonMises / Rankine / mu(I) / "
+                                 "Viscoelastic / GranularFluid / Bingham, 4 ppc, 1024^2 grid",
+                            material="ZOO7", grid_res=1024),
+    "material_zoo_1m": dict(builder="model_blocks",
+                            kwargs=dict(grid_res=512, target_particles=1_000_000),
+                            desc="material_zoo_4m's generator on a 512^2 grid with 1M particles "
+                                 "(profiling case)",
+                            material="ZOO7", grid_res=512),
+    "fields_asflip_1m": dict(builder="field_dam_break", kwargs=dict(grid_res=1024, column=512),
+                             desc="dam break 1M with ASFLIP (blend 0.5) and three force fields "
+                                  "(gravity well with cutoff, linear drag, radial confinement)",
+                             material="NewtonianFluid+fields", grid_res=1024),
+    "sleep_slab_1m": dict(builder="sleep_slab", kwargs=dict(grid_res=1024, slab=768),
+                          desc="sleep partition: NeoHookean 768 x 384-cell slab at 4 ppc "
+                               "(1.18M particles, asleep after its first substep) and a disk of "
+                               "radius 40 launched into it; units count awake particles only",
+                          material="NeoHookean-sleep", grid_res=1024, active_units=True),
     "batched_256": dict(builder="batched_scenes", kwargs=dict(n_scenes=256),
                         desc="256 independent scenes in one batch: grid G ~ U{64..256}, target "
                              "N ~ logU[4k, 200k] particles (clipped to fit the grid), material "
@@ -65,7 +85,8 @@ DEFAULT_WORKLOAD = "dam_break_1m"
 #   fluid:    read x8 v8 C16 F16 m4 V0 4 V4 rho4 mat4 plastic16 rho_dp4 = 88,
 #             write x8 v8 C16 V4 rho4 = 40, grid 32/4 = 8              -> 136 B
 #   granular: read 84, write x8 v8 C16 F16 V4 rho4 plastic16 = 72, grid 8 -> 164 B
-K_PARTICLE_BYTES = {"NewtonianFluid": 136, "DP+Snow+NACC": 164}
+K_PARTICLE_BYTES = {"NewtonianFluid": 136, "DP+Snow+NACC": 164, "ZOO7": 164,
+                    "NewtonianFluid+fields": 136, "NeoHookean-sleep": 156}
 
 
 def log(*a):
@@ -458,19 +479,24 @@ def main():
     barrier()
     t_begin = time.perf_counter()
     total_ms = 0.0
+    active_units = 0.0  # sleep partition: awake particles x substeps
     for _ in range(args.steps):
         sim.flush_l2()
+        a0 = sim.active_count() if spec.get("active_units") else 0
         sim.event_record(0)
         sim.step()
         sim.event_record(1)
         total_ms += sim.event_elapsed_ms(0, 1)
+        if spec.get("active_units"):
+            active_units += 0.5 * (a0 + sim.active_count()) * sim.last_substeps()
     sim.synchronize()
     clock_info = clocks.stop(t_begin, time.perf_counter(), t_load)
     st1 = sim.stats()
     barrier()
     substeps = st1["substeps"] - st0["substeps"]
     launches = st1["kernel_launches"] - st0["kernel_launches"]
-    units = float(n * substeps)
+    units = active_units if spec.get("active_units") else float(n * substeps)
+    n_eff = units / max(substeps, 1)  # particles a pass works on (awake ones with a partition)
     if dist is not None:
         total_ms, units, launches = reduce_over_ranks(dist, f"cuda:{local_rank}", total_ms, units,
                                                       launches)
@@ -491,7 +517,7 @@ def main():
         sim.set_option(OPT_USE_GRAPH, 1)
         peak, peak_kind = load_peaks()
         per_launch_s = part_us * 1e-6 / max(subs_i, 1)
-        alg_bytes = K_PARTICLE_BYTES[spec["material"]] * n
+        alg_bytes = K_PARTICLE_BYTES[spec["material"]] * n_eff
         achieved = alg_bytes / per_launch_s / 1e9
         traffic = profile_traffic(args.workload)
         extras["roofline"] = {
@@ -511,13 +537,17 @@ def main():
         sub0 = sim.stats()["substeps"]
         sim.synchronize()
         t0 = time.perf_counter()
+        e2e_active = 0.0
         for _ in range(e2e_steps):
             sim.write_particles_raw(host.ptr, n)
+            a0 = sim.active_count() if spec.get("active_units") else 0
             sim.step()
+            if spec.get("active_units"):
+                e2e_active += 0.5 * (a0 + sim.active_count()) * sim.last_substeps()
             sim.read_particles_raw(host.ptr, n)
         e2e_s = time.perf_counter() - t0
         e2e_subs = sim.stats()["substeps"] - sub0
-        e2e_units = float(n * e2e_subs)
+        e2e_units = e2e_active if spec.get("active_units") else float(n * e2e_subs)
         if dist is not None:
             e2e_ms, e2e_units, _ = reduce_over_ranks(dist, f"cuda:{local_rank}", e2e_s * 1e3,
                                                      e2e_units, 0)

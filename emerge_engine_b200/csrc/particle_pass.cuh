@@ -978,6 +978,12 @@ __device__ __forceinline__ void density_pass(const DensityKernelArgs &a) {
     if (valid) {
         p.x = a.P.x[i];
         p.mat = a.P.mat[i];
+        // the fluid stress's own fields, issued with the position so their latency overlaps
+        // the density gather (in a fluid-only scene every particle is a fluid or fallback)
+        if constexpr (MASK == MASK_FLUID) {
+            p.c = m_from4(a.P.c[i]);
+            p.mass = a.P.mass[i];
+        }
     }
     __syncthreads();
     const bool reproject = cfg.project && (acc_slot ? changed1 : changed0) != 0ull;
@@ -996,8 +1002,10 @@ __device__ __forceinline__ void density_pass(const DensityKernelArgs &a) {
         const MatP &m = s_mats[p.mat < static_cast<uint32_t>(n_mats) ? p.mat : 0u];
         if (m.model == M_FLUID) {
             if (!reproject) {  // the fields the fluid stress reads (fluid.rs:135-195)
-                p.c = m_from4(a.P.c[i]);
-                p.mass = a.P.mass[i];
+                if constexpr (MASK != MASK_FLUID) {
+                    p.c = m_from4(a.P.c[i]);
+                    p.mass = a.P.mass[i];
+                }
                 p.f = m.surface_tension_coeff != 0.0f ? m_from4(a.P.f[i]) : mident();
                 p.temperature = a.lf.temperature ? a.P.temperature[i] : 0.0f;
                 p.activation = 0.0f;  // no active stress for fluids

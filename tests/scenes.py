@@ -266,3 +266,70 @@ def sleep_scene(sim_cls, threshold=0.05, grid_res=96, seed=9, dt=0.05, **sim_kw)
     p["activation"][p["user_tag"] == 3] = 0.5
     sim.set_particles(p)
     return sim
+
+
+def model_blocks(sim_cls, grid_res=1024, target_particles=4_000_000, seed=11, gravity=-1.0,
+                 dt=0.05, **sim_kw):
+    """The seven constitutive models beyond the core set at scale: the seeded block partition
+    of mixed_granular (16-128-cell blocks, 4 ppc) with each block's material uniform over
+    ZOO's Corotated, VonMises, Rankine, mu(I), Viscoelastic, GranularFluid and Bingham
+    (temperature and activation left at zero)."""
+    kinds = sorted(ZOO)
+    cfg = SimConfig.standard(grid_res, dt, (0.0, gravity))
+    sim = sim_cls.empty(cfg, **sim_kw).with_default_material(ZOO[kinds[0]][0]())
+    for k in range(1, len(kinds)):
+        sim = sim.with_material(k, ZOO[kinds[k]][0]())
+    rng = np.random.default_rng(seed)
+    for (x0, y0, w, h, _) in granular_blocks(grid_res, target_particles, seed):
+        mid = int(rng.integers(len(kinds)))
+        s = SpawnRegion.for_sim(cfg)
+        s.spacing, s.box_size = 0.5, (w, h)
+        s.box_center = (x0 + w / 2.0, y0 + h / 2.0)
+        s.material_id = mid
+        s.position_jitter = 0.2
+        s.rng_seed = (seed * 7919 + x0 * 131 + y0) & 0xFFFFFFFF
+        mass = ZOO[kinds[mid]][1]
+        if mass is not None:
+            s.mass_override = mass
+        sim.add_body(s)
+    return sim
+
+
+def field_dam_break(sim_cls, grid_res=1024, column=512, asflip=0.5, **sim_kw):
+    """The dam break with ASFLIP (asflip_blend 0.5) and three force fields in this order: a
+    gravity well at the grid centre (G = 0.5, mass 2e4, softening 8, cutoff grid_res / 2),
+    a linear drag toward (0.2, 0) on the fluid (coefficient 0.05) and a radial confinement
+    of radius 0.45 grid_res (stiffness 0.5)."""
+    from emerge_engine_b200 import GravityWellField, LinearDragField, RadialConfinementField
+    sim = dam_break(sim_cls, grid_res=grid_res, column=column, **sim_kw)
+    c = grid_res * 0.5
+    for f in (GravityWellField.point((c, c), 2e4, 0.5, 8.0).with_cutoff(grid_res * 0.5),
+              LinearDragField.new((0.2, 0.0), 0.05, LinearDragField.ALL_MATERIALS),
+              RadialConfinementField.new((c, c), grid_res * 0.45, 0.5)):
+        sim.add_force_field(f)
+    return sim
+
+
+def sleep_slab(sim_cls, grid_res=1024, slab=512, seed=21, threshold=0.05, **sim_kw):
+    """Sleep partition at scale: a NeoHookean (400, 200) slab of slab x slab / 2 cells at
+    4 ppc resting on the floor, which falls asleep after its first substep, and a disk of
+    radius 40 launched into it at (12, -2), which wakes the part it reaches; sleep
+    threshold `threshold`."""
+    cfg = SimConfig.standard(grid_res, 0.05, (0.0, -1.0))
+    cfg.asflip_blend = 0.0
+    cfg.sleep_threshold = threshold
+    sim = sim_cls.empty(cfg, **sim_kw).with_default_material(NeoHookeanMaterial.new(400.0, 200.0))
+    t = cfg.boundary_thickness
+    a = SpawnRegion.for_sim(cfg)
+    a.spacing, a.box_size = 0.5, (slab, slab // 2)
+    a.box_center = (grid_res - t - 4 - slab / 2.0, t + 1 + slab / 4.0)
+    a.position_jitter, a.rng_seed = 0.3, seed
+    b = SpawnRegion.for_sim(cfg).disk(40.0)
+    b.spacing, b.box_center = 0.5, (grid_res - t - 8 - slab - 48.0, t + 60.0)
+    b.position_jitter, b.rng_seed = 0.3, seed + 1
+    sim.add_body(a)
+    tag = sim.add_body(b)
+    p = sim.particles()
+    p["v"][p["user_tag"] == tag] = (12.0, -2.0)
+    sim.set_particles(p)
+    return sim
