@@ -8,7 +8,8 @@ from .materials import (BinghamFluidMaterial, CorotatedMaterial,  # noqa: F401
                         DruckerPragerMaterial, FallbackMaterial, GranularFluidMaterial,
                         MuIRheologyMaterial, NaccMaterial, NeoHookeanMaterial,
                         NewtonianFluidMaterial, RankineMaterial, StomakhinMaterial,
-                        ViscoelasticMaterial, VonMisesMaterial, lame_from_young, to_radians)
+                        ViscoelasticMaterial, VonMisesMaterial, lame_from_young, to_radians,
+                        WithMixturePhase, SOLID_PHASE, FLUID_PHASE, DirectionalContactGrip)
 from .fields import (AabbConfinementField, BuoyancyField, ChemotaxisField,  # noqa: F401
                      CoulombField, GravityWellField, LinearDragField, RadialConfinementField,
                      UniformElectricField)

@@ -27,6 +27,7 @@ SOURCES = {
     "step_kernels.cu": EXACT,
     "fast_kernels.cu": FAST,
     "det_kernels.cu": EXACT,
+    "multifield.cu": EXACT,
     "sort.cu": EXACT,
     "sort_noalloc.cu": EXACT,
     "sim.cu": EXACT,

@@ -255,9 +255,10 @@ emerge_status emerge_cuda_batch_create(emerge_sim *const *sims, uint32_t n_sims,
             g_batch_error = "batch_create: scenes run the fast path (the reference-order mode is per simulation)";
             return EMERGE_ERR_UNSUPPORTED;
         }
-        if (v.dcfg.n_fields > 0 || v.dcfg.asflip > 0.0f || v.cfg.sleep_threshold > 0.0f || v.dcfg.zones) {
-            g_batch_error = "batch_create: scenes with force fields, ASFLIP or a sleep partition run as "
-                            "single simulations";
+        if (v.dcfg.n_fields > 0 || v.dcfg.asflip > 0.0f || v.cfg.sleep_threshold > 0.0f || v.dcfg.zones ||
+            v.dcfg.multi) {
+            g_batch_error = "batch_create: scenes with force fields, ASFLIP, a sleep partition or multi-field "
+                            "contact / mixture run as single simulations";
             return EMERGE_ERR_UNSUPPORTED;
         }
         if (v.cfg.grid_res > 1024) {

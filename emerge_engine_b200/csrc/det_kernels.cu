@@ -64,7 +64,7 @@ __global__ void k_project(DevParticles P, int n, DevConfig cfg, StepState *st) {
 __global__ void k_det_records(DevParticles P, int n, const MatP *mats, int n_mats, DevConfig cfg,
                               const StepState *st, int mode, uint32_t invalid_key, uint32_t *keys,
                               uint32_t *vals, float4 *payload, int filter, float lox, float loy,
-                              float hix, float hiy) {
+                              float hix, float hiy, int pfilter, float4 *points) {
     int s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= n) return;
     const uint32_t hi = P.slot_to_index[s];
@@ -73,8 +73,17 @@ __global__ void k_det_records(DevParticles P, int n, const MatP *mats, int n_mat
     p.mass = P.mass[s];
     // estimate_particle_volumes_local's AABB filter (density.rs:106-110); particles outside
     // the active zone take no part
-    const bool skip = (filter && (p.x.x < lox || p.x.y < loy || p.x.x > hix || p.x.y > hiy)) ||
-                      (cfg.zones && (P.sleeping[s] & ZB_OUT));
+    bool skip = (filter && (p.x.x < lox || p.x.y < loy || p.x.x > hix || p.x.y > hiy)) ||
+                (cfg.zones && (P.sleeping[s] & ZB_OUT));
+    // a field's scatter takes its particles only (p2g.rs:60-66): 1 grip (contact_group != 0),
+    // 2 / 3 the solid / fluid mixture phase
+    const uint32_t cgroup = (pfilter != 0 || points) ? P.contact[s] : 0u;
+    if (pfilter == 1) skip = skip || cgroup == 0u;
+    if (pfilter >= 2) {
+        const uint32_t mat = P.mat[s];
+        const uint32_t ph = cfg.mat_phase[mat < static_cast<uint32_t>(n_mats) ? mat : 0u];
+        skip = skip || ph != static_cast<uint32_t>(pfilter - 1);
+    }
     float2 v = v2(0.0f, 0.0f);
     M2 c = mzero(), stress = mzero();
     float stress_coeff = 0.0f;
@@ -121,12 +130,15 @@ __global__ void k_det_records(DevParticles P, int n, const MatP *mats, int n_mat
                                          svmul(stress_coeff, mv(stress, cell_dist))));
             }
             payload[r] = make_float4(weight * p.mass, mom.x, mom.y, 0.0f);
+            // the contact point cloud (p2g.rs:54-74): position and label of every record
+            if (points) points[r] = make_float4(p.x.x, p.x.y, cgroup != 0u ? 1.0f : -1.0f, 0.0f);
         }
 }
 
 // Sequential per-cell sums over the cell-sorted records (Grid::accumulate order).
 __global__ void k_segsum(const uint32_t *keys, const uint32_t *vals, const float4 *payload, int n_rec,
-                         uint32_t invalid_key, GridView g, int mass_only) {
+                         uint32_t invalid_key, GridView g, int mass_only, float4 *target,
+                         int2 *range, uint32_t *any) {
     int j = blockIdx.x * blockDim.x + threadIdx.x;
     if (j >= n_rec) return;
     uint32_t key = keys[j];
@@ -134,7 +146,8 @@ __global__ void k_segsum(const uint32_t *keys, const uint32_t *vals, const float
     if (j > 0 && keys[j - 1] == key) return;  // not the head of its cell
     float4 first = payload[vals[j]];
     float m = first.x, px = first.y, py = first.z;
-    for (int k = j + 1; k < n_rec && keys[k] == key; ++k) {
+    int k = j + 1;
+    for (; k < n_rec && keys[k] == key; ++k) {
         float4 q = payload[vals[k]];
         m += q.x;
         px += q.y;
@@ -143,6 +156,12 @@ __global__ void k_segsum(const uint32_t *keys, const uint32_t *vals, const float
     int cx = static_cast<int>(key / static_cast<uint32_t>(g.res));
     int cy = static_cast<int>(key % static_cast<uint32_t>(g.res));
     int ci = cell_index(cx, cy, g.tpd);
+    if (range) range[ci] = make_int2(j, k);  // the cell's records, in particle index order
+    if (target) {  // a contact or mixture field
+        target[ci] = make_float4(m, px, py, 1.0f);
+        if (any) *any = 1u;
+        return;
+    }
     if (mass_only) {
         g.acc_a[ci].x = m;
     } else {
@@ -158,18 +177,19 @@ void launch_project(const StepLaunch &L) {
 
 void launch_det_records(const StepLaunch &L, int mode, uint32_t invalid_key, uint32_t *keys,
                         uint32_t *vals, float4 *payload, int filter, float lox, float loy, float hix,
-                        float hiy) {
+                        float hiy, int pfilter, float4 *points) {
     if (L.n)
         k_det_records<<<(L.n + 127) / 128, 128, 0, L.stream>>>(L.P, L.n, L.mats, L.n_mats, L.cfg, L.st,
                                                                mode, invalid_key, keys, vals, payload,
-                                                               filter, lox, loy, hix, hiy);
+                                                               filter, lox, loy, hix, hiy, pfilter, points);
 }
 
 void launch_segsum(const uint32_t *keys, const uint32_t *vals, const float4 *payload, int n_rec,
-                   uint32_t invalid_key, const GridView &g, int mass_only, cudaStream_t stream) {
+                   uint32_t invalid_key, const GridView &g, int mass_only, cudaStream_t stream,
+                   float4 *target, int2 *range, uint32_t *any) {
     if (n_rec)
         k_segsum<<<(n_rec + 255) / 256, 256, 0, stream>>>(keys, vals, payload, n_rec, invalid_key, g,
-                                                          mass_only);
+                                                          mass_only, target, range, any);
 }
 
 }  // namespace emerge

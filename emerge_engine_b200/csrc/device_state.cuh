@@ -71,6 +71,7 @@ struct StepState {
     uint32_t error_flags;
     uint32_t upload_flags;      // k_check_aos: bit 0 contact_group != 0, bit 1 pinned
     uint32_t active;            // batches: the scene takes part in the running substep
+    uint32_t contact_active;    // Grid::has_contact_activity of the running substep
     uint32_t pad_;
 };
 
@@ -82,6 +83,16 @@ struct GridView {
     float2 *grid_v;
     uint8_t *tile_flag;
     float2 *grid_vpre;  // ASFLIP pre-force velocities (allocated when asflip_blend > 0)
+    // multi-field contact and two-phase mixture (allocated when a scene uses them):
+    // per-cell sums {m, px, py, touched} of the grip particles and of each mixture phase,
+    // the resolved velocities G2P reads, the total mass kept past the grid update, each
+    // cell's range in the cell-sorted scatter records, and the pressure solve's scratch
+    float4 *acc_grip, *acc_sol, *acc_flu;
+    float2 *grip_v, *rest_v, *sol_v, *flu_v;
+    float *grid_m;
+    int2 *rec_range;
+    float *mx_as, *mx_af, *mx_k, *mx_rhs, *mx_p[2];
+    uint8_t *mx_sig;
 };
 
 __host__ __device__ __forceinline__ int cell_index(int x, int y, int tpd) {

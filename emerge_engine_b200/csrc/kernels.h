@@ -63,11 +63,20 @@ void launch_density_pass_batch(const DevParticles &P, const BatchView &b, int n_
 
 // det_kernels.cu (reference-order mode)
 void launch_project(const StepLaunch &L);
+// pfilter: 0 every particle, 1 grip particles, 2 / 3 the solid / fluid mixture phase;
+// points (optional): each record's (x, y, contact label) for the contact point cloud
 void launch_det_records(const StepLaunch &L, int mode, uint32_t invalid_key, uint32_t *keys,
                         uint32_t *vals, float4 *payload, int filter = 0, float lox = 0.f,
-                        float loy = 0.f, float hix = 0.f, float hiy = 0.f);
+                        float loy = 0.f, float hix = 0.f, float hiy = 0.f, int pfilter = 0,
+                        float4 *points = nullptr);
+// target (optional): sums go to that field instead of acc_a (and `any` is set); range
+// (optional): each cell's record range
 void launch_segsum(const uint32_t *keys, const uint32_t *vals, const float4 *payload, int n_rec,
-                   uint32_t invalid_key, const GridView &g, int mass_only, cudaStream_t stream);
+                   uint32_t invalid_key, const GridView &g, int mass_only, cudaStream_t stream,
+                   float4 *target = nullptr, int2 *range = nullptr, uint32_t *any = nullptr);
+// multi-field contact and mixture coupling after the grid update (multifield.cu)
+void launch_contact_resolve(const StepLaunch &L, const uint32_t *vals, const float4 *points);
+void launch_mixture_resolve(const StepLaunch &L);
 
 // sort.cu
 // Scratch for a stable LSD radix sort of up to `capacity` (key, value) pairs.

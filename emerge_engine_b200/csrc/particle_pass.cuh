@@ -207,14 +207,24 @@ __device__ __forceinline__ float2 gather_pre_force(const GridView &g, const QW &
     return old_v;
 }
 
-// G2P phase 1 for one particle (transfer/g2p.rs:217-326; contact and mixture gated off,
-// ASFLIP compiled in with EXTRAS).  Returns 1 if the speed clamp fired.
+// The grid velocity a particle of the multi-field scenes reads at a node (g2p.rs:219-238).
+// sel: 1 / 2 a rest / grip particle while contact is active, 3 / 4 a solid / fluid mixture
+// particle; nodes outside the field keep the total velocity.
+__device__ __forceinline__ float2 field_node_v(const GridView &g, int ci, int sel, float2 v) {
+    if (sel <= 2) return g.acc_grip[ci].w > 0.0f ? (sel == 2 ? g.grip_v[ci] : g.rest_v[ci]) : v;
+    const bool mixture = g.acc_sol[ci].w > 0.0f || g.acc_flu[ci].w > 0.0f;
+    return mixture ? (sel == 3 ? g.sol_v[ci] : g.flu_v[ci]) : v;
+}
+
+// G2P phase 1 for one particle (transfer/g2p.rs:217-326; ASFLIP and the multi-field node
+// velocities compiled in with EXTRAS, the latter on the FAST = false path that multi-field
+// scenes run).  Returns 1 if the speed clamp fired.
 // FAST = false: the reference's cell-by-cell expression order (bit-level parity).
 // FAST = true: the same sums in stencil-offset form with fused multiply-adds:
 //   v' = sum w v_i,  B = v' (x) e + [sum (gx-1) w v_i, sum (gy-1) w v_i].
 template <bool FAST, bool EXTRAS = false>
 __device__ __forceinline__ int g2p_particle(const GridView &g, const DevConfig &cfg, float dt,
-                                            PState &p) {
+                                            PState &p, int sel = 0) {
     QW w = quadratic_weights(p.x);
     const bool inside = stencil_inside(w.bx, w.by, g.res);
     float2 new_v = v2(0.0f, 0.0f);
@@ -265,8 +275,12 @@ __device__ __forceinline__ int g2p_particle(const GridView &g, const DevConfig &
                 int cx = w.bx + gx - 1, cy = w.by + gy - 1;
                 float2 dist = vadd(vsub(v2(static_cast<float>(cx), static_cast<float>(cy)), p.x),
                                    splat(0.5f));
-                float2 node_v = (inside || in_domain(cx, cy, g.res)) ? g.grid_v[xp[gx] + yp[gy]]
-                                                                      : v2(0.0f, 0.0f);
+                float2 node_v = v2(0.0f, 0.0f);
+                if (inside || in_domain(cx, cy, g.res)) {
+                    node_v = g.grid_v[xp[gx] + yp[gy]];
+                    if constexpr (EXTRAS)
+                        if (sel != 0) node_v = field_node_v(g, xp[gx] + yp[gy], sel, node_v);
+                }
                 float2 wv = vmuls(node_v, weight);
                 M2 term = m2(vmuls(wv, dist.x), vmuls(wv, dist.y));
                 b = madd(b, term);
@@ -824,7 +838,18 @@ __device__ __forceinline__ void particle_pass(const ParticleKernelArgs &a) {
                     p.vol = p.mass / d;
                 }
             }
-            clamped = g2p_particle<FAST, HAS_MODEL(MASK, M_EXTRAS_BIT)>(g, cfg, dt, p);
+            int sel = 0;  // multi-field node velocities (g2p.rs:219-238)
+            if constexpr (!FAST && HAS_MODEL(MASK, M_EXTRAS_BIT)) {
+                if (cfg.multi) {
+                    if (st->contact_active) {
+                        sel = a.P.contact[i] != 0u ? 2 : 1;
+                    } else {
+                        const uint32_t ph = cfg.mat_phase[p.mat < static_cast<uint32_t>(n_mats) ? p.mat : 0u];
+                        sel = ph == 1u ? 3 : (ph == 2u ? 4 : 0);
+                    }
+                }
+            }
+            clamped = g2p_particle<FAST, HAS_MODEL(MASK, M_EXTRAS_BIT)>(g, cfg, dt, p, sel);
             if constexpr (CLOSURE)
                 closure_prepare<MASK>(*mp, p, dt, pr, a.cl, closure_hash(i, st), w);
             else

@@ -940,6 +940,14 @@ struct DevConfig {
     unsigned long long *zone_log;  // wake / sleep events: (key << 32) | reference index
     uint32_t *zone_log_count;
     uint32_t zone_log_cap;
+    int multi;               // multi-field contact / mixture fields in use
+    float contact_friction;  // SimConfig::contact_friction
+    int grip_on;             // DirectionalContactGrip set
+    float grip_mu_easy, grip_mu_resist;
+    float2 grip_dir;
+    float mix_drag;          // SimConfig::mixture_drag_coefficient
+    int mix_iters;           // SimConfig::mixture_pressure_iterations
+    const uint32_t *mat_phase;  // MixturePhase per material slot: 0 none, 1 solid, 2 fluid
 };
 
 // Bits of DevParticles::sleeping while the sleep partition is in use: bit 0 is

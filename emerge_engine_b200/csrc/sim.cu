@@ -157,6 +157,16 @@ struct emerge_sim {
     bool sorted_once = false;
     unsigned long long fallback_at_sort = 0, blocks_at_sort = 0;
 
+    // multi-field contact (grid/contact.rs) and two-phase mixture (grid/mixture.rs)
+    bool contact_seen = false;       // some particle has contact_group != 0
+    std::vector<uint32_t> phases;    // MixturePhase per material slot: 0 none, 1 solid, 2 fluid
+    int grip_on = 0;                 // Simulation::contact_grip (solver/mod.rs:55)
+    float grip_mu_easy = 0.0f, grip_mu_resist = 0.0f, grip_dir[2] = {0.0f, 0.0f};
+    Buffer mfbuf;                    // the multi-field grid arrays and the phase table
+    Buffer ptsbuf;                   // the contact point cloud, one entry per scatter record
+    size_t pts_cap = 0;
+    float4 *det_points() const { return static_cast<float4 *>(ptsbuf.ptr); }
+
     // reference-order (deterministic) mode
     int deterministic = 0;
     int precise_opt = -1;  // -1: precise math follows `deterministic`
@@ -273,11 +283,22 @@ DevConfig make_dev_config(const emerge_sim_config &c, const std::vector<uint64_t
     return d;
 }
 
+bool mixture_on(const emerge_sim *s) {
+    for (uint32_t ph : s->phases)
+        if (ph != 0) return true;
+    return false;
+}
+// Multi-field scenes run the reference-order pipeline: its cell-sorted scatter records give
+// every contact cell its point cloud in particle index order.
+bool multi_on(const emerge_sim *s) { return s->contact_seen || mixture_on(s); }
+bool det_pipeline(const emerge_sim *s) { return s->deterministic || s->dcfg.multi; }
+
 // The sleep partition is in use: sleep scoring is on, or some particle is outside the
 // active zone.
 bool zones_on(const emerge_sim *s) { return s->cfg.sleep_threshold > 0.0f || s->active < s->n; }
 emerge_status drain_zone_log(emerge_sim *s);
 emerge_status commit_perm(emerge_sim *s);
+emerge_status update_multi(emerge_sim *s);
 emerge_status update_zones(emerge_sim *s);
 
 // The simulation's device configuration: config, boundaries, force-field table, sleep
@@ -292,6 +313,15 @@ void refresh_dev_config(emerge_sim *s) {
         s->dcfg.zone_log = reinterpret_cast<unsigned long long *>(z + 256);
         s->dcfg.zone_log_cap = s->zlog_cap;
     }
+    s->dcfg.multi = (multi_on(s) && s->mfbuf.ptr) ? 1 : 0;
+    s->dcfg.contact_friction = s->cfg.contact_friction;
+    s->dcfg.grip_on = s->grip_on;
+    s->dcfg.grip_mu_easy = s->grip_mu_easy;
+    s->dcfg.grip_mu_resist = s->grip_mu_resist;
+    s->dcfg.grip_dir = make_float2(s->grip_dir[0], s->grip_dir[1]);
+    s->dcfg.mix_drag = s->cfg.mixture_drag_coefficient;
+    s->dcfg.mix_iters = static_cast<int>(s->cfg.mixture_pressure_iterations);
+    s->dcfg.mat_phase = s->mfbuf.ptr ? static_cast<const uint32_t *>(s->mfbuf.ptr) : nullptr;
     s->dcfg.n_fields = s->n_fields;
     s->dcfg.fields = s->n_fields ? static_cast<const emerge_force_field *>(s->fbuf.ptr) : nullptr;
     s->dcfg.field_data = s->n_fields ? reinterpret_cast<const float *>(
@@ -316,8 +346,9 @@ StepLaunch make_launch(emerge_sim *s) {
     L.use_window = s->use_window;
     L.model_mask = 1u << M_FALLBACK;
     for (const auto &m : s->mats) L.model_mask |= model_bits(m);
-    if (s->dcfg.n_fields > 0 || s->dcfg.asflip > 0.0f || s->dcfg.zones) L.model_mask |= 1u << M_EXTRAS_BIT;
-    L.fast = s->deterministic ? 0 : 1;
+    if (s->dcfg.n_fields > 0 || s->dcfg.asflip > 0.0f || s->dcfg.zones || s->dcfg.multi)
+        L.model_mask |= 1u << M_EXTRAS_BIT;
+    L.fast = det_pipeline(s) ? 0 : 1;
     L.cl = closure_args(s->closure);
     L.stream = s->stream;
     return L;
@@ -442,7 +473,7 @@ emerge_status build_graph(emerge_sim *s) {
 emerge_status prime(emerge_sim *s) {
     StepLaunch L = make_launch(s);
     launch_prime_setup(L);
-    if (s->deterministic) {  // CFL reduction only; the substep scatters after dt is known
+    if (det_pipeline(s)) {  // CFL reduction only; the substep scatters after dt is known
         launch_particle_pass(L, s->lf, 0, 0, 0);
         s->host_launches += 2;
         CK(cudaGetLastError());
@@ -679,18 +710,24 @@ int det_key_bits(const emerge_sim *s) {
 }
 
 // Records -> stable sort by cell -> sequential per-cell sums (see det_kernels.cu).
+// A field scatter (pfilter 1 grip, 2 / 3 mixture phases) sums its particles into `target`
+// and sets `any`.  The full scatter can also write the contact point cloud (`points`), each
+// cell's record range and, in `sorted_vals`, the cell-sorted record order they index.
 emerge_status det_scatter(emerge_sim *s, const StepLaunch &L, int mode, int filter, float lox,
-                          float loy, float hix, float hiy) {
+                          float loy, float hix, float hiy, int pfilter = 0, float4 *target = nullptr,
+                          uint32_t *any = nullptr, float4 *points = nullptr, int2 *range = nullptr,
+                          const uint32_t **sorted_vals = nullptr) {
     emerge_status st = ensure_det_scratch(s);
     if (st != EMERGE_OK) return st;
     const uint32_t inv = det_invalid_key(s);
     const int n_rec = 9 * L.n;
     launch_det_records(L, mode, inv, s->det_sort.keys[0], s->det_sort.vals[0], s->det_payload, filter,
-                       lox, loy, hix, hiy);
+                       lox, loy, hix, hiy, pfilter, points);
     int bits = det_key_bits(s);
     int r = radix_sort_pairs(s->det_sort, n_rec, bits, s->stream);
     launch_segsum(s->det_sort.keys[r], s->det_sort.vals[r], s->det_payload, n_rec, inv, s->g,
-                  mode == 0 ? 1 : 0, s->stream);
+                  mode == 0 ? 1 : 0, s->stream, target, range, any);
+    if (sorted_vals) *sorted_vals = s->det_sort.vals[r];
     s->host_launches += 2 + 5 * ((bits + 7) / 8);
     CK(cudaGetLastError());
     return EMERGE_OK;
@@ -704,6 +741,35 @@ emerge_status clear_grid(emerge_sim *s) {
     return EMERGE_OK;
 }
 
+// Contact point cloud storage: one (x, y, label) per scatter record.
+emerge_status ensure_points(emerge_sim *s) {
+    const size_t need = 9 * (s->cap > 0 ? s->cap : 1);
+    if (s->pts_cap >= need) return EMERGE_OK;
+    s->ptsbuf.reset();
+    CK(cudaMalloc(&s->ptsbuf.ptr, need * sizeof(float4)));
+    s->ptsbuf.bytes = need * sizeof(float4);
+    s->pts_cap = need;
+    return EMERGE_OK;
+}
+
+// The per-substep clear of the field sums, the pressure scratch (zero is the pressure of a
+// cell outside the mixture) and the contact flag (Grid::clear, grid/mod.rs:163-176).
+emerge_status clear_multi(emerge_sim *s) {
+    const size_t cells = static_cast<size_t>(s->tpd) * s->tpd * TILE_CELLS;
+    CK(cudaMemsetAsync(s->g.acc_grip, 0, cells * sizeof(float4), s->stream));
+    CK(cudaMemsetAsync(s->g.acc_sol, 0, cells * sizeof(float4), s->stream));
+    CK(cudaMemsetAsync(s->g.acc_flu, 0, cells * sizeof(float4), s->stream));
+    CK(cudaMemsetAsync(s->g.mx_k, 0, cells * sizeof(float), s->stream));
+    CK(cudaMemsetAsync(s->g.mx_p[0], 0, cells * sizeof(float), s->stream));
+    CK(cudaMemsetAsync(s->g.mx_p[1], 0, cells * sizeof(float), s->stream));
+    CK(cudaMemsetAsync(&s->d_state->contact_active, 0, sizeof(uint32_t), s->stream));
+    return EMERGE_OK;
+}
+
+int mixture_launches(const DevConfig &c) {
+    return (c.mix_drag <= 0.0f || c.mix_iters <= 0) ? 1 : 3 + c.mix_iters;
+}
+
 // One Simulation::step in reference order (step.rs:23-60, 62-210), host-driven.
 emerge_status run_det_step(emerge_sim *s, bool timed) {
     StepLaunch L = make_launch(s);
@@ -714,9 +780,19 @@ emerge_status run_det_step(emerge_sim *s, bool timed) {
     CK(cudaMemcpyAsync(s->h_state, s->d_state, sizeof(StepState), cudaMemcpyDeviceToHost, s->stream));
     CK(cudaStreamSynchronize(s->stream));
     emerge_status st = EMERGE_OK;
+    const bool contact = L.cfg.multi && s->contact_seen;
+    const bool mixture = L.cfg.multi && mixture_on(s);
+    if (contact) {
+        st = ensure_points(s);
+        if (st != EMERGE_OK) return st;
+    }
     while (s->h_state->cont) {
         CK(cudaEventRecord(s->ev[1], s->stream));
         launch_substep_begin(L, 0, 0ull, 0);
+        if (L.cfg.multi) {
+            st = clear_multi(s);
+            if (st != EMERGE_OK) return st;
+        }
         CK(cudaEventRecord(s->ev[2], s->stream));
         if (L.cfg.project) launch_project(L);
         CK(cudaEventRecord(s->ev[3], s->stream));
@@ -730,7 +806,20 @@ emerge_status run_det_step(emerge_sim *s, bool timed) {
             if (st != EMERGE_OK) return st;
         }
         CK(cudaEventRecord(s->ev[4], s->stream));
-        st = det_scatter(s, L, 1, 0, 0, 0, 0, 0);
+        // the grip and mixture-phase fields take the same P2G contributions as the total
+        // (p2g.rs:60-66), summed per field in particle index order
+        if (contact) {
+            st = det_scatter(s, L, 1, 0, 0, 0, 0, 0, 1, s->g.acc_grip, &s->d_state->contact_active);
+            if (st != EMERGE_OK) return st;
+        }
+        if (mixture) {
+            st = det_scatter(s, L, 1, 0, 0, 0, 0, 0, 2, s->g.acc_sol);
+            if (st == EMERGE_OK) st = det_scatter(s, L, 1, 0, 0, 0, 0, 0, 3, s->g.acc_flu);
+            if (st != EMERGE_OK) return st;
+        }
+        const uint32_t *sorted_vals = nullptr;
+        st = det_scatter(s, L, 1, 0, 0, 0, 0, 0, 0, nullptr, nullptr, contact ? s->det_points() : nullptr,
+                         contact ? s->g.rec_range : nullptr, &sorted_vals);
         if (st != EMERGE_OK) return st;
         if (L.cfg.zones) {  // wake after this substep's P2G (step.rs:107-131)
             launch_wake(L, 0);
@@ -738,6 +827,14 @@ emerge_status run_det_step(emerge_sim *s, bool timed) {
         }
         CK(cudaEventRecord(s->ev[5], s->stream));
         launch_grid_update(L);
+        if (contact) {  // step.rs:166-183
+            launch_contact_resolve(L, sorted_vals, s->det_points());
+            s->host_launches += 1;
+        }
+        if (mixture) {  // step.rs:185-197
+            launch_mixture_resolve(L);
+            s->host_launches += mixture_launches(L.cfg);
+        }
         CK(cudaEventRecord(s->ev[6], s->stream));
         launch_particle_pass(L, s->lf, 1, 0, 0);
         CK(cudaEventRecord(s->ev[7], s->stream));
@@ -841,11 +938,6 @@ emerge_status spawn_region(emerge_sim *s, const emerge_spawn_region &sp, uint32_
 // (Simulation::new) initial-volume estimate on the device.
 emerge_status append_particles(emerge_sim *s, const emerge_particle *src, size_t count,
                                int volume_mode /*0 none, 1 local, 2 full*/) {
-    for (size_t k = 0; k < count; ++k) {
-        if (src[k].contact_group != 0)
-            return static_cast<emerge_status>(s->fail(
-                EMERGE_ERR_UNSUPPORTED, "contact_group != 0 (multi-field contact) is not on the device path"));
-    }
     if (s->n + count > 0x7fffffffull)
         return static_cast<emerge_status>(s->fail(EMERGE_ERR_INVALID_ARG, "too many particles"));
     emerge_status st = ensure_capacity(s, s->n + count);
@@ -871,6 +963,13 @@ emerge_status append_particles(emerge_sim *s, const emerge_particle *src, size_t
     s->base_of_pos.clear();
     st = update_zones(s);
     if (st != EMERGE_OK) return st;
+    bool contact = false;
+    for (size_t k = 0; k < count && !contact; ++k) contact = src[k].contact_group != 0;
+    if (contact && !s->contact_seen) {
+        s->contact_seen = true;
+        st = update_multi(s);
+        if (st != EMERGE_OK) return st;
+    }
     if (s->dcfg.zones) launch_zone_bits(s->P[s->cur], n_new, static_cast<uint32_t>(s->active), s->stream);
     if (volume_mode != 0 && count > 0) {
         // estimate_particle_volumes_local (density.rs:81-144) / estimate_particle_volumes (:41-72)
@@ -922,6 +1021,59 @@ emerge_status invalidate_pending(emerge_sim *s) {
     CK(cudaMemsetAsync(s->g.acc_s, 0, cells * sizeof(float2), s->stream));
     CK(cudaMemsetAsync(s->g.tile_flag, 0, static_cast<size_t>(s->tpd) * s->tpd, s->stream));
     s->pending_valid = false;
+    return EMERGE_OK;
+}
+
+// Uploads the material phase table (MAX_MATERIALS entries, unset slots 0).
+emerge_status upload_phases(emerge_sim *s) {
+    if (!s->mfbuf.ptr) return EMERGE_OK;
+    std::vector<uint32_t> table(MAX_MATERIALS, 0u);
+    for (size_t k = 0; k < s->phases.size() && k < static_cast<size_t>(MAX_MATERIALS); ++k) table[k] = s->phases[k];
+    CK(cudaMemcpyAsync(s->mfbuf.ptr, table.data(), table.size() * sizeof(uint32_t), cudaMemcpyHostToDevice,
+                       s->stream));
+    CK(cudaStreamSynchronize(s->stream));
+    return EMERGE_OK;
+}
+
+// Switches the multi-field pipeline on (allocating its grid arrays the first time) or off
+// after a change of the particles' contact groups or the materials' phases.
+emerge_status update_multi(emerge_sim *s) {
+    const int was = s->dcfg.multi;
+    if (multi_on(s) && !s->mfbuf.ptr) {
+        const size_t cells = static_cast<size_t>(s->tpd) * s->tpd * TILE_CELLS;
+        const size_t bytes = MAX_MATERIALS * sizeof(uint32_t) +
+                             cells * (3 * sizeof(float4) + 4 * sizeof(float2) + sizeof(float) + sizeof(int2) +
+                                      6 * sizeof(float) + sizeof(uint8_t)) +
+                             20 * 256;
+        CK(cudaMalloc(&s->mfbuf.ptr, bytes));
+        s->mfbuf.bytes = bytes;
+        CK(cudaMemsetAsync(s->mfbuf.ptr, 0, bytes, s->stream));
+        Carver c(s->mfbuf.ptr);
+        c.take<uint32_t>(MAX_MATERIALS);  // the phase table, at the start
+        s->g.acc_grip = c.take<float4>(cells);
+        s->g.acc_sol = c.take<float4>(cells);
+        s->g.acc_flu = c.take<float4>(cells);
+        s->g.grip_v = c.take<float2>(cells);
+        s->g.rest_v = c.take<float2>(cells);
+        s->g.sol_v = c.take<float2>(cells);
+        s->g.flu_v = c.take<float2>(cells);
+        s->g.grid_m = c.take<float>(cells);
+        s->g.rec_range = c.take<int2>(cells);
+        s->g.mx_as = c.take<float>(cells);
+        s->g.mx_af = c.take<float>(cells);
+        s->g.mx_k = c.take<float>(cells);
+        s->g.mx_rhs = c.take<float>(cells);
+        s->g.mx_p[0] = c.take<float>(cells);
+        s->g.mx_p[1] = c.take<float>(cells);
+        s->g.mx_sig = c.take<uint8_t>(cells);
+        emerge_status st = upload_phases(s);
+        if (st != EMERGE_OK) return st;
+    }
+    refresh_dev_config(s);
+    if (s->dcfg.multi != was) {  // the pipelines keep different work pending between steps
+        s->graph_dirty = true;
+        return invalidate_pending(s);
+    }
     return EMERGE_OK;
 }
 
@@ -1157,6 +1309,38 @@ emerge_status emerge_cuda_set_force_fields(emerge_sim *s, const emerge_force_fie
     return EMERGE_OK;
 }
 
+emerge_status emerge_cuda_set_contact_grip(emerge_sim *s, int enabled, float mu_easy, float mu_resist,
+                                          float dir_x, float dir_y) {
+    if (!s) return EMERGE_ERR_INVALID_ARG;
+    if (enabled && !(mu_easy >= 0.0f && mu_easy <= 1.0f && mu_resist >= 0.0f && mu_resist <= 1.0f))
+        return static_cast<emerge_status>(s->fail(EMERGE_ERR_INVALID_ARG, "mu_easy and mu_resist must be in [0.0, 1.0]"));
+    if (enabled && !(std::isfinite(dir_x) && std::isfinite(dir_y)))
+        return static_cast<emerge_status>(s->fail(EMERGE_ERR_INVALID_ARG, "easy direction must be finite"));
+    s->grip_on = enabled ? 1 : 0;
+    s->grip_mu_easy = enabled ? mu_easy : 0.0f;
+    s->grip_mu_resist = enabled ? mu_resist : 0.0f;
+    s->grip_dir[0] = enabled ? dir_x : 0.0f;
+    s->grip_dir[1] = enabled ? dir_y : 0.0f;
+    refresh_dev_config(s);
+    s->graph_dirty = true;
+    return EMERGE_OK;
+}
+
+emerge_status emerge_cuda_set_mixture_phases(emerge_sim *s, const uint32_t *phases, uint32_t count) {
+    if (!s || (!phases && count)) return EMERGE_ERR_INVALID_ARG;
+    if (count > static_cast<uint32_t>(MAX_MATERIALS))
+        return static_cast<emerge_status>(s->fail(EMERGE_ERR_INVALID_ARG, "at most 64 material slots"));
+    for (uint32_t k = 0; k < count; ++k)
+        if (phases[k] > 2u)
+            return static_cast<emerge_status>(
+                s->fail(EMERGE_ERR_INVALID_ARG, "material " + std::to_string(k) + ": phase must be 0, 1 or 2"));
+    if (s->stream) CK(cudaStreamSynchronize(s->stream));  // kernels in flight may read the old table
+    s->phases.assign(phases, phases + count);
+    emerge_status st = upload_phases(s);
+    if (st != EMERGE_OK) return st;
+    return update_multi(s);
+}
+
 emerge_status emerge_cuda_add_body(emerge_sim *s, const emerge_spawn_region *spawn, uint32_t *tag_out) {
     if (!s || !spawn) return EMERGE_ERR_INVALID_ARG;
     std::vector<emerge_particle> ps;
@@ -1214,9 +1398,8 @@ emerge_status emerge_cuda_write_particles(emerge_sim *s, const emerge_particle *
     if (!s || (!in && n)) return EMERGE_ERR_INVALID_ARG;
     if (n != s->n) return static_cast<emerge_status>(s->fail(EMERGE_ERR_INVALID_ARG, "n must equal the particle count"));
     if (n == 0) return EMERGE_OK;
-    // Upload into the staging buffer and check it there (contact groups are not on the
-    // device path; pinned particles switch the pinned load on), so a rejected upload
-    // leaves the simulation's particles untouched.
+    // Upload into the staging buffer and check it there (contact groups switch the
+    // multi-field pipeline on, pinned particles the pinned load).
     CK(cudaMemcpyAsync(s->d_aos, in, n * sizeof(emerge_particle), cudaMemcpyHostToDevice, s->stream));
     CK(cudaMemsetAsync(&s->d_state->upload_flags, 0, sizeof(uint32_t), s->stream));
     launch_check_aos(s->d_aos, static_cast<int>(n), &s->d_state->upload_flags, s->stream);
@@ -1225,9 +1408,11 @@ emerge_status emerge_cuda_write_particles(emerge_sim *s, const emerge_particle *
     CK(cudaStreamSynchronize(s->stream));
     s->host_launches += 1;
     const uint32_t flags = s->h_state->upload_flags;
-    if (flags & 1u)
-        return static_cast<emerge_status>(s->fail(
-            EMERGE_ERR_UNSUPPORTED, "contact_group != 0 (multi-field contact) is not on the device path"));
+    if (((flags & 1u) != 0) != s->contact_seen) {  // the upload replaces every particle
+        s->contact_seen = (flags & 1u) != 0;
+        emerge_status st = update_multi(s);
+        if (st != EMERGE_OK) return st;
+    }
     const int pinned = (flags & 2u) ? 1 : 0;  // the upload replaces every particle
     if (pinned != s->lf.pinned) {
         s->lf.pinned = pinned;
@@ -1255,7 +1440,9 @@ emerge_status emerge_cuda_replace_particles(emerge_sim *s, const emerge_particle
     s->n = 0;
     s->active = 0;
     s->lf.pinned = 0;
+    s->contact_seen = false;
     emerge_status st = append_particles(s, in, n, 0);
+    if (st == EMERGE_OK && !s->contact_seen && s->dcfg.multi) st = update_multi(s);
     if (st != EMERGE_OK) return st;
     s->active = active_count;
     st = update_zones(s);
@@ -1281,7 +1468,7 @@ emerge_status emerge_cuda_step(emerge_sim *s, uint32_t n_steps, emerge_step_timi
         }
         st = update_zones(s);
         if (st != EMERGE_OK) return st;
-        if (s->deterministic) {
+        if (det_pipeline(s)) {
             st = run_det_step(s, timing != nullptr);
             if (st != EMERGE_OK) return st;
         } else if (s->use_graph && !s->dcfg.zones) {

@@ -63,6 +63,7 @@ __device__ __forceinline__ void grid_update_cell(const GridView &g, const DevCon
         if (spd > vel_limit) mom = vmuls(mom, vel_limit / spd);
     }
     g.grid_v[ci] = mom;
+    if (cfg.multi) g.grid_m[ci] = m;  // the contact and mixture resolves read the total mass
     g.acc_a[ci] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
     g.acc_s[ci] = v2(0.0f, 0.0f);
 }

@@ -708,3 +708,72 @@ class BinghamFluidMaterial(Material):
                     fluid_min_volume=self.min_volume,
                     surface_tension_coeff=self.surface_tension_coeff,
                     settling_damping=self.settling_damping)
+
+
+SOLID_PHASE, FLUID_PHASE = 1, 2  # MixturePhase (materials/mod.rs:96-103)
+
+
+class WithMixturePhase(Material):
+    """`WithMixturePhase` (matter/materials/mod.rs:296-357): any material tagged as the solid
+    or fluid phase of a two-phase mixture; every other behaviour is the inner material's."""
+
+    def __init__(self, inner: Material, phase: int):
+        if phase not in (SOLID_PHASE, FLUID_PHASE):
+            raise ValueError("phase must be SOLID_PHASE or FLUID_PHASE")
+        self.inner = inner
+        self.phase = phase
+        self.model = inner.model
+
+    @classmethod
+    def new(cls, inner: Material, phase: int):
+        return cls(inner, phase)
+
+    def mixture_phase(self) -> int:
+        return self.phase
+
+    def constitutive_model(self) -> int:
+        return self.inner.constitutive_model()
+
+    def params(self):
+        return self.inner.params()
+
+    def abi_params(self):
+        return self.inner.abi_params()
+
+    def needs_density_recompute(self) -> bool:
+        return self.inner.needs_density_recompute()
+
+    def oracle_fields(self):
+        return dict(self.inner.oracle_fields(), mixture_phase=self.phase)
+
+
+def mixture_phase_of(m: Material) -> int:
+    """MaterialModel::mixture_phase (materials/mod.rs:170-172): 0 for none."""
+    return m.mixture_phase() if hasattr(m, "mixture_phase") else 0
+
+
+class DirectionalContactGrip:
+    """`DirectionalContactGrip` (spacetime/grid/directional_grip.rs): contact friction that
+    depends on the slip direction; Simulation.with_contact_grip installs it.  Changes made
+    with set_easy_direction / set_friction apply when the simulation is given it again."""
+
+    def __init__(self, mu_easy, mu_resist, easy_direction):
+        self.set_friction(mu_easy, mu_resist)
+        self.set_easy_direction(easy_direction)
+
+    @classmethod
+    def new(cls, mu_easy, mu_resist, easy_direction):
+        return cls(mu_easy, mu_resist, easy_direction)
+
+    def set_friction(self, mu_easy, mu_resist):
+        if not (0.0 <= mu_easy <= 1.0 and 0.0 <= mu_resist <= 1.0):
+            raise ValueError("mu_easy and mu_resist must be in [0.0, 1.0]")
+        self.mu_easy, self.mu_resist = f32(mu_easy), f32(mu_resist)
+
+    def set_easy_direction(self, direction):
+        """glam Vec2::normalize_or_zero in f32 (directional_grip.rs:55-58)."""
+        d = np.array([direction[0], direction[1]], dtype=np.float32)
+        with np.errstate(divide="ignore", over="ignore", invalid="ignore"):
+            rcp = np.float32(1.0) / np.sqrt(d[0] * d[0] + d[1] * d[1], dtype=np.float32)
+        d = d * rcp if np.isfinite(rcp) and rcp > 0.0 else np.zeros(2, dtype=np.float32)
+        self.easy_direction = (float(d[0]), float(d[1]))

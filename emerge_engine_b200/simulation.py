@@ -19,7 +19,7 @@ from .abi import (PARTICLE_DTYPE, BodyStateC, MaterialParamsC, StepTimingC, chec
                   load_library)
 from .config import BodyState, SimConfig, SlipBoundary, SpawnRegion
 from .fields import Field, pack_fields
-from .materials import DEVICE_MODELS, FallbackMaterial, Material
+from .materials import DEVICE_MODELS, FallbackMaterial, Material, mixture_phase_of
 
 MAX_MATERIAL_SLOTS = 64  # materials/registry.rs:6
 
@@ -123,6 +123,8 @@ class Simulation:
         arr = (MaterialParamsC * len(self.registry))(
             *[m.abi_params() for m in self.registry.materials])
         self._check(self._lib.emerge_cuda_set_materials(self._sim, arr, len(self.registry)))
+        phases = (c_uint32 * len(self.registry))(*[mixture_phase_of(m) for m in self.registry.materials])
+        self._check(self._lib.emerge_cuda_set_mixture_phases(self._sim, phases, len(self.registry)))
 
     def with_default_material(self, material: Material) -> "Simulation":
         """lifecycle.rs:107-111 (also re-runs init_particle on every particle)."""
@@ -142,6 +144,20 @@ class Simulation:
         mid = self.registry.next_id()
         self.set_material(mid, material)
         return mid
+
+    # ---------------------------------------------------------------- multi-field contact
+    def set_contact_grip(self, grip) -> None:
+        """Simulation::with_contact_grip (lifecycle.rs:125-131); None removes the grip."""
+        if grip is None:
+            self._check(self._lib.emerge_cuda_set_contact_grip(self._sim, 0, 0.0, 0.0, 0.0, 0.0))
+        else:
+            self._check(self._lib.emerge_cuda_set_contact_grip(
+                self._sim, 1, float(grip.mu_easy), float(grip.mu_resist),
+                grip.easy_direction[0], grip.easy_direction[1]))
+
+    def with_contact_grip(self, grip) -> "Simulation":
+        self.set_contact_grip(grip)
+        return self
 
     # ---------------------------------------------------------------- sleep partition
     def active_count(self) -> int:

@@ -60,7 +60,7 @@ typedef struct emerge_particle {
     float activation;
     float activation_dir[2];
     uint32_t muscle_group_id;
-    uint32_t contact_group;   /* must be 0: multi-field contact is not on the device path */
+    uint32_t contact_group;   /* != 0: in the grip field of multi-field contact */
     uint32_t sleeping;
     uint32_t pinned;
     float scalar_field;
@@ -271,6 +271,31 @@ typedef struct emerge_force_field {
  * tables and potentials; n = 0 clears. */
 emerge_status emerge_cuda_set_force_fields(emerge_sim *sim, const emerge_force_field *fields,
                                            uint32_t n, const float *data, uint64_t n_data);
+
+/* ---- multi-field contact and two-phase mixture ---------------------------------- */
+
+/* Multi-field contact (spacetime/grid/contact.rs) runs when some particle has
+ * contact_group != 0, the two-phase mixture coupling (spacetime/grid/mixture.rs) when some
+ * material slot has a phase; such scenes step through the reference-order pipeline
+ * (EMERGE_OPT_DETERMINISTIC's sums), whose cell-sorted scatter records give each contact
+ * cell its point cloud in particle index order.  After the grid update (step.rs:166-197)
+ * every grip cell gets a logistic-regression interface normal (grid/contact_normal.rs) or
+ * the grip-mass gradient, Coulomb friction or the directional grip, and the overlap
+ * correction; every mixture cell the implicit Darcy drag between the phases and, with
+ * SimConfig::mixture_pressure_iterations > 0, the Jacobi pressure projection.  G2P reads
+ * the resolved velocities (transfer/g2p.rs:219-238). */
+
+/* Simulation::with_contact_grip (lifecycle.rs:125-131): DirectionalContactGrip
+ * (grid/directional_grip.rs) replaces contact_friction with mu_easy / mu_resist by slip
+ * direction.  (dir_x, dir_y) is the grip's stored easy direction, already normalised as
+ * DirectionalContactGrip::new / set_easy_direction store it (normalize_or_zero).
+ * enabled = 0 removes the grip.  mu outside [0, 1] is EMERGE_ERR_INVALID_ARG. */
+emerge_status emerge_cuda_set_contact_grip(emerge_sim *sim, int enabled, float mu_easy, float mu_resist,
+                                          float dir_x, float dir_y);
+/* MaterialModel::mixture_phase per material slot (matter/materials/mod.rs:170-172,
+ * WithMixturePhase :296-357): 0 none, 1 solid, 2 fluid; slots at or past `count` have none.
+ * The caller passes the table again whenever the registry changes. */
+emerge_status emerge_cuda_set_mixture_phases(emerge_sim *sim, const uint32_t *phases, uint32_t count);
 
 /* ---- particles ---------------------------------------------------------------- */
 

@@ -27,6 +27,8 @@
 
 #include <algorithm>
 #include <functional>
+#include <unordered_map>
+#include <utility>
 #include <chrono>
 #include <cmath>
 #include <cstring>
@@ -904,6 +906,17 @@ struct Grid {
     std::vector<uint8_t> touched;
     std::vector<uint32_t> dirty;  // first-touch order (mod.rs:127)
     std::vector<V2> pre;          // ASFLIP pre-force snapshot, valid at touched cells
+    // multi-field contact (grid/contact.rs:10-124): grip field, point cloud, resolution
+    std::vector<float> grip_mass;
+    std::vector<V2> grip_mom, grip_v, rest_v;
+    std::vector<uint8_t> contact_touched;
+    std::vector<uint32_t> contact_dirty;
+    std::unordered_map<uint32_t, std::vector<std::pair<V2, float>>> points;
+    // two-phase mixture (grid/mixture.rs:7-85)
+    std::vector<float> solid_mass, fluid_mass;
+    std::vector<V2> solid_mom, fluid_mom, solid_v, fluid_v;
+    std::vector<uint8_t> mixture_touched;
+    std::vector<uint32_t> mixture_dirty;
 
     void init(size_t r) {
         res = r;
@@ -912,6 +925,70 @@ struct Grid {
         touched.assign(r * r, 0);
         pre.assign(r * r, v2(0, 0));
         dirty.clear();
+        grip_mass.assign(r * r, 0.0f);
+        grip_mom.assign(r * r, v2(0, 0));
+        grip_v.assign(r * r, v2(0, 0));
+        rest_v.assign(r * r, v2(0, 0));
+        contact_touched.assign(r * r, 0);
+        contact_dirty.clear();
+        points.clear();
+        solid_mass.assign(r * r, 0.0f);
+        fluid_mass.assign(r * r, 0.0f);
+        solid_mom.assign(r * r, v2(0, 0));
+        fluid_mom.assign(r * r, v2(0, 0));
+        solid_v.assign(r * r, v2(0, 0));
+        fluid_v.assign(r * r, v2(0, 0));
+        mixture_touched.assign(r * r, 0);
+        mixture_dirty.clear();
+    }
+    bool has_contact_activity() const { return !contact_dirty.empty(); }
+    // add_grip_mass_momentum (contact.rs:41-72)
+    void add_grip(IV2 c, float m, V2 p) {
+        uint32_t idx;
+        if (!flat_index(c, idx)) return;
+        if (contact_touched[idx]) {
+            grip_mass[idx] += m;
+            grip_mom[idx] = ::add(grip_mom[idx], p);
+        } else {
+            contact_touched[idx] = 1;
+            contact_dirty.push_back(idx);
+            grip_mass[idx] = m;
+            grip_mom[idx] = p;
+            grip_v[idx] = rest_v[idx] = v2(0, 0);
+        }
+    }
+    // add_contact_point (contact.rs:74-85): only at cells of the grip field
+    void add_point(IV2 c, V2 x, float label) {
+        uint32_t idx;
+        if (!flat_index(c, idx) || !contact_touched[idx]) return;
+        points[idx].push_back({x, label});
+    }
+    // add_mixture_mass_momentum (mixture.rs:20-58); phase 1 solid, 2 fluid
+    void add_mixture(IV2 c, uint32_t phase, float m, V2 p) {
+        uint32_t idx;
+        if (!flat_index(c, idx)) return;
+        if (!mixture_touched[idx]) {
+            mixture_touched[idx] = 1;
+            mixture_dirty.push_back(idx);
+            solid_mass[idx] = fluid_mass[idx] = 0.0f;
+            solid_mom[idx] = fluid_mom[idx] = v2(0, 0);
+            solid_v[idx] = fluid_v[idx] = v2(0, 0);
+            if (phase == 1) {
+                solid_mass[idx] = m;
+                solid_mom[idx] = p;
+            } else {
+                fluid_mass[idx] = m;
+                fluid_mom[idx] = p;
+            }
+            return;
+        }
+        if (phase == 1) {
+            solid_mass[idx] += m;
+            solid_mom[idx] = ::add(solid_mom[idx], p);
+        } else {
+            fluid_mass[idx] += m;
+            fluid_mom[idx] = ::add(fluid_mom[idx], p);
+        }
     }
     // cell_is_active (grid/mod.rs:231-241): the cell is in the dirty set
     bool cell_is_active(IV2 c) const {
@@ -925,7 +1002,7 @@ struct Grid {
         if (!flat_index(c, idx) || !touched[idx]) return v2(0, 0);
         return pre[idx];
     }
-    // Grid::clear (mod.rs:167-180)
+    // Grid::clear (mod.rs:163-176)
     void clear() {
         for (uint32_t idx : dirty) {
             mass[idx] = 0.0f;
@@ -933,6 +1010,11 @@ struct Grid {
             touched[idx] = 0;
         }
         dirty.clear();
+        for (uint32_t idx : contact_dirty) contact_touched[idx] = 0;
+        contact_dirty.clear();
+        points.clear();
+        for (uint32_t idx : mixture_dirty) mixture_touched[idx] = 0;
+        mixture_dirty.clear();
     }
     // flat_index (mod.rs:89-99)
     bool flat_index(IV2 c, uint32_t &idx) const {
@@ -983,6 +1065,10 @@ struct oracle_sim {
     Grid grid;
     std::vector<oracle_force_field> fields;  // force_fields, application order
     std::vector<float> field_data;
+    // DirectionalContactGrip (grid/directional_grip.rs), if set (lifecycle.rs:125-131)
+    int grip_on = 0;
+    float grip_mu_easy = 0.0f, grip_mu_resist = 0.0f;
+    V2 grip_dir = {0.0f, 0.0f};
     float last_step_dt = 0.0f;
     size_t last_substeps = 0;
     size_t last_vel_clamp_count = 0;
@@ -1294,7 +1380,321 @@ void p2g(oracle_sim &s, float dt) {
                 V2 momentum = smul(weight, add(smul(mass_i, add(v_i, mv(c_i, cell_dist))),
                                                smul(stress_coeff, mv(stress, cell_dist))));
                 s.grid.add(cell, weight * mass_i, momentum);
+                if (q.contact_group != 0) s.grid.add_grip(cell, weight * mass_i, momentum);
+                if (m.mixture_phase != 0) s.grid.add_mixture(cell, m.mixture_phase, weight * mass_i, momentum);
             }
+    }
+}
+
+// gather_contact_point_cloud (p2g.rs:54-74): every active particle adds its position, labelled
+// +1 (grip) or -1, to each stencil cell of the grip field, in index order.
+void gather_contact_point_cloud(oracle_sim &s) {
+    if (!s.grid.has_contact_activity()) return;
+    for (size_t i = 0; i < s.active_count; ++i) {
+        const P &q = s.p[i];
+        V2 x = load_v(q.x);
+        float label = q.contact_group != 0 ? 1.0f : -1.0f;
+        QW w = quadratic_weights(x);
+        for (int gx = 0; gx < 3; ++gx)
+            for (int gy = 0; gy < 3; ++gy) s.grid.add_point(IV2{w.base.x + gx - 1, w.base.y + gy - 1}, x, label);
+    }
+}
+
+// solve3x3 (contact_normal.rs): Cramer's rule, None for |det| <= EPSILON.
+bool solve3x3(const float m[3][3], const float rhs[3], float out[3]) {
+    auto det3 = [](const float a[3][3]) {
+        return a[0][0] * (a[1][1] * a[2][2] - a[1][2] * a[2][1]) -
+               a[0][1] * (a[1][0] * a[2][2] - a[1][2] * a[2][0]) +
+               a[0][2] * (a[1][0] * a[2][1] - a[1][1] * a[2][0]);
+    };
+    float det = det3(m);
+    if (std::fabs(det) <= F32_EPS) return false;
+    for (int col = 0; col < 3; ++col) {
+        float mm_[3][3];
+        for (int r = 0; r < 3; ++r)
+            for (int c = 0; c < 3; ++c) mm_[r][c] = m[r][c];
+        for (int r = 0; r < 3; ++r) mm_[r][col] = rhs[r];
+        out[col] = det3(mm_) / det;
+    }
+    return true;
+}
+
+// glam Vec2::normalize: self * (1 / length)
+inline V2 normalize(V2 a) { return muls(a, 1.0f / length(a)); }
+
+// fit_contact_normal_lr (contact_normal.rs): logistic regression of the point labels on
+// position relative to the node, Newton steps with a small ridge penalty.
+bool fit_contact_normal_lr(const std::vector<std::pair<V2, float>> &points, V2 node_pos, float cell, V2 &out) {
+    bool has_grip = false, has_rest = false;
+    for (const auto &pc : points) {
+        if (pc.second > 0.0f) has_grip = true;
+        if (pc.second < 0.0f) has_rest = true;
+    }
+    if (!has_grip || !has_rest) return false;
+    const float dx2 = cell * cell;
+    const float penalty[3] = {1.0e-7f * dx2, 1.0e-7f * dx2, 0.0f};
+    float beta[3] = {0.0f, 0.0f, 0.0f};
+    bool have_prev = false;
+    V2 prev = v2(0, 0);
+    for (int it = 0; it < 15; ++it) {
+        float m[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+        float rhs[3] = {0, 0, 0};
+        for (const auto &pc : points) {
+            V2 rel = sub(pc.first, node_pos);
+            const float xp[3] = {rel.x, rel.y, 1.0f};
+            float z = fclamp(xp[0] * beta[0] + xp[1] * beta[1] + xp[2] * beta[2], -40.0f, 40.0f);
+            float ez = m_exp(-z);
+            float denom = 1.0f + ez;
+            float f = 2.0f / denom - 1.0f;
+            float sigma = 2.0f * ez / (denom * denom);
+            float sigma_sq = sigma * sigma;
+            for (int k = 0; k < 3; ++k) {
+                for (int l = 0; l < 3; ++l) m[k][l] += sigma_sq * xp[k] * xp[l];
+                rhs[k] += sigma * (pc.second - f) * xp[k];
+            }
+        }
+        for (int k = 0; k < 3; ++k) {
+            m[k][k] += penalty[k];
+            rhs[k] -= penalty[k] * beta[k];
+        }
+        float delta[3];
+        if (!solve3x3(m, rhs, delta)) break;
+        if (!std::isfinite(delta[0]) || !std::isfinite(delta[1]) || !std::isfinite(delta[2])) break;
+        for (int k = 0; k < 3; ++k) beta[k] += delta[k];
+        V2 raw = v2(beta[0], beta[1]);
+        if (length_sq(raw) <= F32_EPS || !finite2(raw)) continue;
+        V2 n = normalize(raw);
+        if (have_prev && 1.0f - dot(n, prev) < 1.0e-5f) {
+            prev = n;
+            break;
+        }
+        prev = n;
+        have_prev = true;
+    }
+    if (!have_prev) return false;
+    float gs = 0.0f, rs = 0.0f;
+    size_t gc = 0, rc = 0;
+    for (const auto &pc : points) {
+        if (pc.second > 0.0f) {
+            gs += dot(sub(pc.first, node_pos), prev);
+            gc += 1;
+        }
+    }
+    for (const auto &pc : points) {
+        if (pc.second < 0.0f) {
+            rs += dot(sub(pc.first, node_pos), prev);
+            rc += 1;
+        }
+    }
+    const float grip_mean = gs / static_cast<float>(gc > 0 ? gc : 1);
+    const float rest_mean = rs / static_cast<float>(rc > 0 ? rc : 1);
+    out = grip_mean < rest_mean ? v2(-prev.x, -prev.y) : prev;
+    return true;
+}
+
+// apply_coulomb_wall (forces/boundary/mod.rs:60-76)
+void apply_coulomb_wall(V2 &v, V2 n, float mu) {
+    float v_n = dot(v, n);
+    if (v_n >= 0.0f) return;
+    float normal_speed = std::fabs(v_n);
+    V2 v_t = sub(v, smul(v_n, n));
+    float v_t_len = length(v_t);
+    float friction_impulse = mu * normal_speed;
+    v = v_t_len > friction_impulse ? muls(v_t, (v_t_len - friction_impulse) / v_t_len) : v2(0, 0);
+}
+
+// Grid::resolve_contact (contact.rs:254-391): per grip cell, the grip and rest velocities
+// after Coulomb friction (or the directional grip) and the overlap correction.
+void resolve_contact(oracle_sim &s, float dt, V2 gravity, float friction, float vel_limit, float cell) {
+    Grid &g = s.grid;
+    const float MIN_MASS_FRACTION = 1.0e-6f;
+    auto clamp_speed = [&](V2 v) {
+        float spd = length(v);
+        return spd > vel_limit ? muls(v, vel_limit / spd) : v;
+    };
+    const size_t res = g.res;
+    auto grip_mass_at = [&](int x, int y) -> float {
+        uint32_t idx;
+        if (!g.flat_index(IV2{x, y}, idx) || !g.contact_touched[idx]) return 0.0f;
+        return g.grip_mass[idx];
+    };
+    for (uint32_t idx : g.contact_dirty) {
+        const int cx = static_cast<int>(idx / res), cy = static_cast<int>(idx % res);
+        V2 node_pos = v2(static_cast<float>(idx / res), static_cast<float>(idx % res));
+        if (!g.touched[idx]) continue;
+        const float total_mass = g.mass[idx];
+        const V2 v_cm = g.mom[idx];  // normalised, gravity, boundaries, clamp
+        const float grip_mass = g.grip_mass[idx];
+        const V2 grip_momentum = g.grip_mom[idx];
+        const float rest_mass = total_mass - grip_mass;
+        if (grip_mass <= MIN_MASS_FRACTION || rest_mass <= MIN_MASS_FRACTION) {
+            g.grip_v[idx] = v_cm;
+            g.rest_v[idx] = v_cm;
+            continue;
+        }
+        V2 v_grip = clamp_speed(add(divs(grip_momentum, grip_mass), muls(gravity, dt)));
+        V2 fit;
+        bool have = false;
+        auto it = g.points.find(idx);
+        static const std::vector<std::pair<V2, float>> none;
+        if (fit_contact_normal_lr(it == g.points.end() ? none : it->second, node_pos, cell, fit) &&
+            finite2(fit))
+            have = true;
+        if (!have) {  // grip_mass_gradient_normal (contact.rs:128-140)
+            auto m = [&](int dx, int dy) { return grip_mass_at(cx + dx, cy + dy); };
+            float gx_ = (m(1, -1) + 2.0f * m(1, 0) + m(1, 1)) - (m(-1, -1) + 2.0f * m(-1, 0) + m(-1, 1));
+            float gy_ = (m(-1, 1) + 2.0f * m(0, 1) + m(1, 1)) - (m(-1, -1) + 2.0f * m(0, -1) + m(1, -1));
+            V2 grad = v2(gx_, gy_);
+            if (length_sq(grad) > F32_EPS) {
+                fit = normalize(grad);
+                have = true;
+            }
+        }
+        V2 v_rel = sub(v_grip, v_cm);
+        if (!have) {
+            g.grip_v[idx] = v_grip;
+            g.rest_v[idx] = clamp_speed(divs(sub(muls(v_cm, total_mass), muls(v_grip, grip_mass)), rest_mass));
+            continue;
+        }
+        const V2 n = v2(-fit.x, -fit.y);
+        if (s.grip_on) {  // DirectionalContactGrip::resolve (directional_grip.rs)
+            V2 tangent = v2(-n.y, n.x);
+            float v_t = dot(v_rel, tangent);
+            float easy_t = dot(s.grip_dir, tangent);
+            float mu = v_t * easy_t >= 0.0f ? s.grip_mu_easy : s.grip_mu_resist;
+            apply_coulomb_wall(v_rel, n, mu);
+        } else {
+            apply_coulomb_wall(v_rel, n, friction);
+        }
+        float max_grip_proj = -INFINITY, min_rest_proj = INFINITY;
+        if (it != g.points.end())
+            for (const auto &pc : it->second) {
+                float proj = dot(pc.first, n);
+                if (pc.second > 0.0f) max_grip_proj = fmax_(max_grip_proj, proj);
+                else if (pc.second < 0.0f) min_rest_proj = fmin_(min_rest_proj, proj);
+            }
+        if (std::isfinite(max_grip_proj) && std::isfinite(min_rest_proj)) {
+            float gap = min_rest_proj - max_grip_proj;
+            if (gap < 0.0f) {
+                const float CORRECTION_RATE = 2.0f;
+                float max_correction_speed = 0.5f * cell;
+                float correction_speed = fmin_(CORRECTION_RATE * (-gap), max_correction_speed);
+                float v_n = dot(v_rel, n);
+                float target_vn = -correction_speed;
+                if (v_n > target_vn) v_rel = add(v_rel, muls(n, target_vn - v_n));
+            }
+        }
+        V2 v_grip_new = clamp_speed(add(v_cm, v_rel));
+        V2 total_momentum = muls(v_cm, total_mass);
+        g.grip_v[idx] = v_grip_new;
+        g.rest_v[idx] = clamp_speed(divs(sub(total_momentum, muls(v_grip_new, grip_mass)), rest_mass));
+    }
+}
+
+// Grid::resolve_mixture_coupling (mixture.rs:87-132) and project_mixture_incompressibility
+// (:150-275): implicit Darcy drag between the phases per node, then Jacobi iterations of a
+// mass-weighted pressure Poisson problem over the mixture nodes.
+void resolve_mixture(oracle_sim &s, float dt, V2 gravity, float drag, float cell, uint32_t iterations) {
+    Grid &g = s.grid;
+    const size_t res = g.res;
+    const float MIN_MASS_FRACTION = 1.0e-6f;
+    if (drag <= 0.0f) {
+        for (uint32_t idx : g.mixture_dirty) {
+            if (!g.touched[idx]) continue;
+            g.solid_v[idx] = g.fluid_v[idx] = g.mom[idx];
+        }
+        return;
+    }
+    for (uint32_t idx : g.mixture_dirty) {
+        if (!g.touched[idx]) continue;
+        const float m_s = g.solid_mass[idx], m_f = g.fluid_mass[idx];
+        if (m_s <= MIN_MASS_FRACTION || m_f <= MIN_MASS_FRACTION) {
+            g.solid_v[idx] = g.fluid_v[idx] = g.mom[idx];
+            continue;
+        }
+        V2 v_s = add(divs(g.solid_mom[idx], m_s), muls(gravity, dt));
+        V2 v_f = add(divs(g.fluid_mom[idx], m_f), muls(gravity, dt));
+        float a = dt * drag / m_s;
+        float b = dt * drag / m_f;
+        float det_ = 1.0f + a + b;
+        g.solid_v[idx] = divs(add(smul(1.0f + b, v_s), smul(a, v_f)), det_);
+        g.fluid_v[idx] = divs(add(smul(b, v_s), smul(1.0f + a, v_f)), det_);
+    }
+    if (iterations == 0) return;
+    const float MIN_MASS = 1.0e-6f;
+    const float h = fmax_(cell, 1.0e-6f);
+    auto pos_of = [&](uint32_t idx) { return IV2{static_cast<int>(idx / res), static_cast<int>(idx % res)}; };
+    auto sv = [&](IV2 c) -> V2 {
+        uint32_t i;
+        return (g.flat_index(c, i) && g.mixture_touched[i]) ? g.solid_v[i] : v2(0, 0);
+    };
+    auto fv = [&](IV2 c) -> V2 {
+        uint32_t i;
+        return (g.flat_index(c, i) && g.mixture_touched[i]) ? g.fluid_v[i] : v2(0, 0);
+    };
+    std::unordered_map<uint32_t, float> alpha_s, alpha_f, mobility, rhs, pressure;
+    std::unordered_map<uint32_t, std::pair<bool, bool>> significant;
+    for (uint32_t idx : g.mixture_dirty) {
+        IV2 pos = pos_of(idx);
+        float m_s = fmax_(g.solid_mass[idx], 0.0f), m_f = fmax_(g.fluid_mass[idx], 0.0f);
+        float n = m_s + m_f > MIN_MASS ? m_f / (m_s + m_f) : 0.0f;
+        float a_s = 1.0f / fmax_(m_s, MIN_MASS);
+        float a_f = 1.0f / fmax_(m_f, MIN_MASS);
+        float k = (1.0f - n) * a_s + n * a_f;
+        const float MIN_SIG = 0.01f;
+        float total_mass = fmax_(m_s + m_f, MIN_MASS);
+        bool solid_sig = m_s / total_mass > MIN_SIG, fluid_sig = m_f / total_mass > MIN_SIG;
+        float vs_r = sv(IV2{pos.x + 1, pos.y}).x, vs_l = sv(IV2{pos.x - 1, pos.y}).x;
+        float vs_u = sv(IV2{pos.x, pos.y + 1}).y, vs_d = sv(IV2{pos.x, pos.y - 1}).y;
+        float div_vs = (vs_r - vs_l) / (2.0f * h) + (vs_u - vs_d) / (2.0f * h);
+        float vf_r = fv(IV2{pos.x + 1, pos.y}).x, vf_l = fv(IV2{pos.x - 1, pos.y}).x;
+        float vf_u = fv(IV2{pos.x, pos.y + 1}).y, vf_d = fv(IV2{pos.x, pos.y - 1}).y;
+        float div_vf = (vf_r - vf_l) / (2.0f * h) + (vf_u - vf_d) / (2.0f * h);
+        float residual = (1.0f - n) * div_vs + n * div_vf;
+        alpha_s[idx] = a_s;
+        alpha_f[idx] = a_f;
+        significant[idx] = {solid_sig, fluid_sig};
+        mobility[idx] = k;
+        rhs[idx] = residual;
+        pressure[idx] = 0.0f;
+    }
+    auto k_or_zero = [&](IV2 c) -> float {
+        uint32_t i;
+        if (!g.flat_index(c, i)) return 0.0f;
+        auto it = mobility.find(i);
+        return it == mobility.end() ? 0.0f : it->second;
+    };
+    auto p_or_zero = [&](const std::unordered_map<uint32_t, float> &p, IV2 c) -> float {
+        uint32_t i;
+        if (!g.flat_index(c, i)) return 0.0f;
+        auto it = p.find(i);
+        return it == p.end() ? 0.0f : it->second;
+    };
+    auto face_k = [](float ki, float kj) { return ki + kj > 1.0e-12f ? 2.0f * ki * kj / (ki + kj) : 0.0f; };
+    for (uint32_t itn = 0; itn < iterations; ++itn) {
+        std::unordered_map<uint32_t, float> next = pressure;
+        for (uint32_t idx : g.mixture_dirty) {
+            IV2 pos = pos_of(idx);
+            float r = rhs[idx], k_i = mobility[idx];
+            float k_r = face_k(k_i, k_or_zero(IV2{pos.x + 1, pos.y}));
+            float k_l = face_k(k_i, k_or_zero(IV2{pos.x - 1, pos.y}));
+            float k_u = face_k(k_i, k_or_zero(IV2{pos.x, pos.y + 1}));
+            float k_d = face_k(k_i, k_or_zero(IV2{pos.x, pos.y - 1}));
+            float k_sum = fmax_(k_r + k_l + k_u + k_d, 1.0e-9f);
+            float p_r = p_or_zero(pressure, IV2{pos.x + 1, pos.y}), p_l = p_or_zero(pressure, IV2{pos.x - 1, pos.y});
+            float p_u = p_or_zero(pressure, IV2{pos.x, pos.y + 1}), p_d = p_or_zero(pressure, IV2{pos.x, pos.y - 1});
+            float weighted = k_r * p_r + k_l * p_l + k_u * p_u + k_d * p_d;
+            next[idx] = (weighted - h * h * r) / k_sum;
+        }
+        pressure = next;
+    }
+    for (uint32_t idx : g.mixture_dirty) {
+        IV2 pos = pos_of(idx);
+        float p_r = p_or_zero(pressure, IV2{pos.x + 1, pos.y}), p_l = p_or_zero(pressure, IV2{pos.x - 1, pos.y});
+        float p_u = p_or_zero(pressure, IV2{pos.x, pos.y + 1}), p_d = p_or_zero(pressure, IV2{pos.x, pos.y - 1});
+        V2 grad_p = v2((p_r - p_l) / (2.0f * h), (p_u - p_d) / (2.0f * h));
+        if (significant[idx].first) g.solid_v[idx] = sub(g.solid_v[idx], smul(alpha_s[idx], grad_p));
+        if (significant[idx].second) g.fluid_v[idx] = sub(g.fluid_v[idx], smul(alpha_f[idx], grad_p));
     }
 }
 
@@ -1321,11 +1721,36 @@ void grid_update(oracle_sim &s, float dt) {
             if (spd > vel_limit) g.mom[idx] = muls(g.mom[idx], vel_limit / spd);
         }
     }
+    // multi-field contact and mixture coupling after the clamp (step.rs:166-197)
+    resolve_contact(s, dt, grav, s.cfg.contact_friction, vel_limit, s.cfg.grid_cell_size);
+    resolve_mixture(s, dt, grav, s.cfg.mixture_drag_coefficient, s.cfg.grid_cell_size,
+                    s.cfg.mixture_pressure_iterations);
 }
 
 // gather_grid_to_particles (transfer/g2p.rs:151-343) with ASFLIP (g2p.rs:263-296);
 // contact and mixture gated off (no grip or mixture particles).
+// The grid velocity a particle reads at a node (g2p.rs:219-238): with contact active, the
+// resolved grip velocity for grip particles and the rest velocity for the others; else a
+// mixture particle's resolved phase velocity; both fall back to the total velocity at nodes
+// outside their field.
+V2 node_velocity(const oracle_sim &s, const P &q, IV2 cell, bool contact_active) {
+    const Grid &g = s.grid;
+    uint32_t idx;
+    if (!g.flat_index(cell, idx)) return v2(0, 0);
+    if (contact_active) {
+        if (!g.contact_touched[idx]) return g.velocity_at(cell);
+        return q.contact_group != 0 ? g.grip_v[idx] : g.rest_v[idx];
+    }
+    const uint32_t phase = s.mat(q.material_id).mixture_phase;
+    if (phase != 0) {
+        if (!g.mixture_touched[idx]) return g.velocity_at(cell);
+        return phase == 1 ? g.solid_v[idx] : g.fluid_v[idx];
+    }
+    return g.velocity_at(cell);
+}
+
 size_t g2p(oracle_sim &s, float dt) {
+    const bool contact_active = s.grid.has_contact_activity();
     const float vel_limit = s.cfg.grid_cell_size / dt;
     const float apic_blend = s.cfg.apic_blend;
     const float asflip_blend = s.cfg.asflip_blend;
@@ -1347,7 +1772,7 @@ size_t g2p(oracle_sim &s, float dt) {
                     IV2 cell{w.base.x + gx - 1, w.base.y + gy - 1};
                     V2 dist = add(sub(v2(static_cast<float>(cell.x), static_cast<float>(cell.y)), x),
                                   splat(0.5f));
-                    V2 node_v = s.grid.velocity_at(cell);
+                    V2 node_v = node_velocity(s, q, cell, contact_active);
                     V2 wv = muls(node_v, weight);
                     M2 term = m2(muls(wv, dist.x), muls(wv, dist.y));
                     b = madd(b, term);
@@ -1579,6 +2004,7 @@ void do_substep(oracle_sim &s, float sub_dt) {
     t0 = clk::now();
     s.grid.clear();
     p2g(s, sub_dt);
+    gather_contact_point_cloud(s);
     wake_touched(s);
     s.timing[3] += us_since(t0);
     t0 = clk::now();
@@ -1817,6 +2243,26 @@ void oracle_kirchhoff(const oracle_material *m, const oracle_particle *p, float 
 }
 
 void oracle_set_correctly_rounded(int on) { g_correctly_rounded = on ? 1 : 0; }
+
+void oracle_set_contact_grip(oracle_sim *s, int on, float mu_easy, float mu_resist, float dir_x,
+                             float dir_y) {
+    s->grip_on = on ? 1 : 0;
+    s->grip_mu_easy = mu_easy;
+    s->grip_mu_resist = mu_resist;
+    V2 d = v2(dir_x, dir_y);
+    s->grip_dir = normalize_or_zero(d);  // DirectionalContactGrip::new normalises
+}
+
+int oracle_fit_contact_normal(const float *points, uint32_t n, float node_x, float node_y,
+                              float cell, float normal[2]) {
+    std::vector<std::pair<V2, float>> pts;
+    for (uint32_t k = 0; k < n; ++k) pts.push_back({v2(points[3 * k], points[3 * k + 1]), points[3 * k + 2]});
+    V2 out;
+    if (!fit_contact_normal_lr(pts, v2(node_x, node_y), cell, out)) return 0;
+    normal[0] = out.x;
+    normal[1] = out.y;
+    return 1;
+}
 
 void oracle_field_acceleration(const oracle_force_field *f, const float *data,
                                const oracle_particle *p, float out[2]) {

@@ -157,6 +157,8 @@ typedef struct oracle_material {
     /* GranularFluid (granular_fluid.rs) reuses lambda, mu, rest_density, eos_stiffness,
      * eos_power, pressure_floor and the snow fields hardening_exponent, compression_limit,
      * stretch_limit, min_plastic_jacobian, max_plastic_jacobian */
+    /* WithMixturePhase (materials/mod.rs:296-357): 0 none, 1 solid, 2 fluid */
+    uint32_t mixture_phase;
 } oracle_material;
 
 /* One built-in force field (forces/fields/); kinds and data layout as
@@ -196,6 +198,14 @@ void oracle_set_correctly_rounded(int on);
  * data out of range. */
 int oracle_set_force_fields(oracle_sim *s, const oracle_force_field *fields, uint32_t n,
                             const float *data, uint64_t n_data);
+/* DirectionalContactGrip (grid/directional_grip.rs) for contact resolution:
+ * on = 0 removes it (Coulomb friction with SimConfig::contact_friction). */
+void oracle_set_contact_grip(oracle_sim *s, int on, float mu_easy, float mu_resist, float dir_x,
+                             float dir_y);
+/* fit_contact_normal_lr (grid/contact_normal.rs) on n points (x, y, label); returns 1 and the
+ * normal, or 0 for no normal. */
+int oracle_fit_contact_normal(const float *points, uint32_t n, float node_x, float node_y,
+                              float cell, float normal[2]);
 /* Field::acceleration of one field at one particle. */
 void oracle_field_acceleration(const oracle_force_field *f, const float *data,
                                const oracle_particle *p, float out[2]);

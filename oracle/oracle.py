@@ -43,7 +43,7 @@ class OracleMaterialC(Structure):
                                           "softening_rate", "mu_static", "mu_dynamic",
                                           "inertial_q", "j_min", "bingham_yield_stress",
                                           "critical_shear_rate")]
-                + [("bingham", c_uint32)])
+                + [("bingham", c_uint32), ("mixture_phase", c_uint32)])
 
 
 def oracle_material(m: Material) -> OracleMaterialC:
@@ -97,6 +97,9 @@ def lib() -> ctypes.CDLL:
             "oracle_active_count": (c_uint64, [c_void_p]),
             "oracle_replace_particles": (c_int, [c_void_p, c_void_p, c_uint64, c_uint64]),
             "oracle_wake_tag": (None, [c_void_p, c_uint32]),
+            "oracle_set_contact_grip": (None, [c_void_p, c_int, c_float, c_float, c_float, c_float]),
+            "oracle_fit_contact_normal": (c_int, [P(c_float), c_uint32, c_float, c_float, c_float,
+                                                  P(c_float)]),
             "oracle_sleep_tag": (None, [c_void_p, c_uint32]),
             "oracle_polar": (None, [P(c_float), P(c_float)]),
             "oracle_axis_weights": (None, [c_float, P(c_float)]),
@@ -274,6 +277,17 @@ class OracleSimulation:
         if self._lib.oracle_replace_particles(self._sim, arr.ctypes.data_as(c_void_p), len(arr),
                                               int(active)) != 0:
             raise ValueError("active count above particle count")
+
+    def with_contact_grip(self, grip):
+        self.set_contact_grip(grip)
+        return self
+
+    def set_contact_grip(self, grip):
+        if grip is None:
+            self._lib.oracle_set_contact_grip(self._sim, 0, 0.0, 0.0, 0.0, 0.0)
+        else:
+            self._lib.oracle_set_contact_grip(self._sim, 1, grip.mu_easy, grip.mu_resist,
+                                              grip.easy_direction[0], grip.easy_direction[1])
 
     def wake_tag(self, tag: int) -> None:
         self._lib.oracle_wake_tag(self._sim, int(tag))

@@ -333,3 +333,56 @@ def sleep_slab(sim_cls, grid_res=1024, slab=512, seed=21, threshold=0.05, **sim_
     p["v"][p["user_tag"] == tag] = (12.0, -2.0)
     sim.set_particles(p)
     return sim
+
+
+def contact_scene(sim_cls, grid_res=96, seed=13, dt=0.05, friction=0.5, grip=None, **sim_kw):
+    """Multi-field contact: a NeoHookean (400, 200) slab on the floor (contact group 0) and a
+    block of the same material with contact_group 1 falling onto it at (1.5, -3), 4 ppc,
+    SimConfig.contact_friction `friction`, optional DirectionalContactGrip `grip`."""
+    cfg = SimConfig.standard(grid_res, dt, (0.0, -1.0))
+    cfg.contact_friction = friction
+    t = cfg.boundary_thickness
+    sim = sim_cls.empty(cfg, **sim_kw).with_default_material(NeoHookeanMaterial.new(400.0, 200.0))
+    if grip is not None:
+        sim.set_contact_grip(grip)
+    a = SpawnRegion.for_sim(cfg)
+    a.spacing, a.box_size, a.box_center = 0.5, (48, 12), (grid_res / 2.0, t + 1 + 6.0)
+    a.position_jitter, a.rng_seed = 0.3, seed
+    b = SpawnRegion.for_sim(cfg)
+    b.spacing, b.box_size, b.box_center = 0.5, (14, 10), (grid_res / 2.0 - 6.0, t + 1 + 12 + 6.0)
+    b.position_jitter, b.rng_seed = 0.3, seed + 1
+    sim.add_body(a)
+    tag = sim.add_body(b)
+    p = sim.particles()
+    g = p["user_tag"] == tag
+    p["contact_group"][g] = 1
+    p["v"][g] = (1.5, -3.0)
+    sim.set_particles(p)
+    return sim
+
+
+def mixture_scene(sim_cls, grid_res=96, seed=17, dt=0.05, drag=5.0, iterations=2, **sim_kw):
+    """Two-phase mixture: a DruckerPrager sand block (solid phase, 1e5 / 0.3, 4 ppc at 1600)
+    on the floor with a block of water (NewtonianFluid 1000 / 1e4, fluid phase, 4 ppc at
+    rho0) resting on part of it, mixture_drag_coefficient `drag`,
+    mixture_pressure_iterations `iterations`."""
+    from emerge_engine_b200 import FLUID_PHASE, SOLID_PHASE, WithMixturePhase
+    cfg = SimConfig.standard(grid_res, dt, (0.0, -1.0))
+    cfg.mixture_drag_coefficient = drag
+    cfg.mixture_pressure_iterations = iterations
+    t = cfg.boundary_thickness
+    sim = (sim_cls.empty(cfg, **sim_kw)
+           .with_default_material(WithMixturePhase(DruckerPragerMaterial.cohesionless(1e5, 0.3),
+                                                   SOLID_PHASE))
+           .with_material(1, WithMixturePhase(NewtonianFluidMaterial.low_viscosity(1000.0, 1e4),
+                                              FLUID_PHASE)))
+    a = SpawnRegion.for_sim(cfg)
+    a.spacing, a.box_size, a.box_center = 0.5, (40, 16), (grid_res / 2.0, t + 1 + 8.0)
+    a.position_jitter, a.rng_seed, a.mass_override = 0.3, seed, 1600.0 * 0.25
+    b = SpawnRegion.for_sim(cfg)
+    b.spacing, b.box_size, b.material_id = 0.5, (20, 10), 1
+    b.box_center = (grid_res / 2.0 - 8.0, t + 1 + 16 + 5.0)
+    b.position_jitter, b.rng_seed, b.mass_override = 0.3, seed + 1, 1000.0 * 0.25
+    sim.add_body(a)
+    sim.add_body(b)
+    return sim

@@ -1,0 +1,104 @@
+"""Multi-field contact and two-phase mixture coupling on the device vs the CPU oracle
+(through the C ABI).
+
+Scenes (tests/scenes.py): contact_scene, a grip block (contact_group 1) thrown onto a slab,
+with SimConfig.contact_friction or a DirectionalContactGrip; mixture_scene, water (fluid
+phase) resting on sand (solid phase) with mixture drag, with and without the Jacobi pressure
+projection.  Both run the reference-order pipeline on the device.
+
+Reference order: after every frame the whole particle array against the oracle with
+correctly rounded math, bit for bit (x and v identical every frame); the contact scene is
+followed for 20 frames (contact starts after about 8), the mixture scene for 4 (its
+resolved phase velocities carry no boundary conditions in the reference, so the scene is
+not meant to run long).  Simulation (the
+default class, single-precision CUDA math): the same frames within the fast bar.
+"""
+import ctypes
+
+import numpy as np
+import pytest
+
+from emerge_engine_b200 import Batch, DeterministicSimulation, DirectionalContactGrip, Simulation
+from emerge_engine_b200.abi import ERR_INVALID_ARG
+from oracle.oracle import OracleSimulation, correctly_rounded_math
+from tests import scenes
+from tests.test_gpu_parity import compare_particles, tol
+
+pytestmark = pytest.mark.gpu
+
+GRIPS = {"friction": None, "grip": DirectionalContactGrip(0.1, 0.9, (1.0, 0.0))}
+
+
+def run_frames(g, c, frames, mode="reference_order"):
+    exact_until = None
+    stats = None
+    for k in range(frames):
+        g.step()
+        c.step()
+        assert g.last_substeps() == c.last_substeps(), k
+        pg, pc = g.particles(), c.particles()
+        same = np.array_equal(pg["x"], pc["x"]) and np.array_equal(pg["v"], pc["v"])
+        if not same and exact_until is None:
+            exact_until = k
+        stats = compare_particles(pg, pc, **tol(mode))
+    return exact_until, stats
+
+
+@pytest.mark.parametrize("which", sorted(GRIPS))
+def test_contact_frames_reference_order(cuda_lib, which):
+    grip = GRIPS[which]
+    g = scenes.contact_scene(DeterministicSimulation, grip=grip)
+    with correctly_rounded_math():
+        c = scenes.contact_scene(OracleSimulation, grip=grip)
+        exact_until, stats = run_frames(g, c, 20)
+    assert exact_until is None, (exact_until, stats)
+
+
+@pytest.mark.parametrize("iterations", [0, 2])
+def test_mixture_frames_reference_order(cuda_lib, iterations):
+    g = scenes.mixture_scene(DeterministicSimulation, iterations=iterations)
+    with correctly_rounded_math():
+        c = scenes.mixture_scene(OracleSimulation, iterations=iterations)
+        exact_until, stats = run_frames(g, c, 4)
+    assert exact_until is None, (exact_until, stats)
+
+
+def test_contact_and_mixture_default_class(cuda_lib):
+    g = scenes.contact_scene(Simulation, grip=GRIPS["grip"])
+    c = scenes.contact_scene(OracleSimulation, grip=GRIPS["grip"])
+    print("contact, default class", run_frames(g, c, 12, "fast"))
+    g = scenes.mixture_scene(Simulation)
+    c = scenes.mixture_scene(OracleSimulation)
+    print("mixture, default class", run_frames(g, c, 3, "fast"))
+
+
+def test_contact_groups_follow_each_upload(cuda_lib):
+    """A write-back that sets contact groups switches the contact fields on; one that clears
+    them switches them off again (particles_mut() edits, lifecycle.rs:233)."""
+    g = scenes.quickstart(DeterministicSimulation)
+    with correctly_rounded_math():
+        c = scenes.quickstart(OracleSimulation)
+        p = g.particles()
+        p["contact_group"][p["x"][:, 1] > np.median(p["x"][:, 1])] = 2
+        for sim in (g, c):
+            sim.set_particles(p)
+        assert run_frames(g, c, 2)[0] is None
+        q = g.particles()
+        q["contact_group"][:] = 0
+        for sim in (g, c):
+            sim.set_particles(q)
+        assert run_frames(g, c, 2)[0] is None
+
+
+def test_grip_and_phase_arguments_are_checked(cuda_lib):
+    sim = scenes.contact_scene(Simulation)
+    lib, h = sim._lib, sim._sim
+    assert lib.emerge_cuda_set_contact_grip(h, 1, 1.5, 0.5, 1.0, 0.0) == ERR_INVALID_ARG
+    assert lib.emerge_cuda_set_contact_grip(h, 1, 0.5, 0.5, float("nan"), 0.0) == ERR_INVALID_ARG
+    bad = (ctypes.c_uint32 * 2)(0, 3)
+    assert lib.emerge_cuda_set_mixture_phases(h, bad, 2) == ERR_INVALID_ARG
+    with pytest.raises(Exception):
+        Batch([scenes.contact_scene(Simulation)])  # multi-field scenes run as single simulations
+    sim.set_contact_grip(None)
+    sim.step()
+    assert np.isfinite(sim.particles()["v"]).all()

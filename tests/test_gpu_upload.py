@@ -1,29 +1,15 @@
 """Particle write-back (`particles_mut()` edits, lifecycle.rs:233) through the C ABI: the
-upload is checked on the device before it replaces anything, and pinned particles follow
-the uploaded flags (G2P zeroes their velocity and affine matrix, transfer/g2p.rs)."""
+upload is checked on the device, and pinned particles follow the uploaded flags (G2P zeroes
+their velocity and affine matrix, transfer/g2p.rs).  Uploaded contact groups are covered by
+test_gpu_contact."""
 import numpy as np
 import pytest
 
 from emerge_engine_b200 import DeterministicSimulation, Simulation
-from emerge_engine_b200.abi import ERR_UNSUPPORTED, EmergeError
 from oracle.oracle import OracleSimulation
 from tests import scenes
 
 pytestmark = pytest.mark.gpu
-
-
-def test_rejected_upload_leaves_particles_untouched(cuda_lib):
-    sim = scenes.quickstart(Simulation)
-    sim.step()
-    before = sim.particles()
-    bad = before.copy()
-    bad["contact_group"][17] = 3
-    bad["x"][:] += 1.0
-    with pytest.raises(EmergeError) as ei:
-        sim.set_particles(bad)
-    assert ei.value.status == ERR_UNSUPPORTED
-    np.testing.assert_array_equal(sim.particles(), before)
-    sim.step()  # still steps from the old state
 
 
 def test_pinned_flags_follow_each_upload(cuda_lib):
