@@ -11,7 +11,7 @@ Default workload: the dam break at ~1M particles (512 x 512-cell water column at
 per cell on a 1024^2 grid).  Inputs are resident in HBM when the timed region starts; L2 is
 flushed (512 MiB device write) before every timed step.  `e2e` repeats the measurement
 through the C ABI with the particle state uploaded from pinned host memory before and read
-back after every step.  `--impl reference` times the CPU oracle (the reference step restated
+back (asynchronously, overlapping the next upload) after every step.  `--impl reference` times the CPU oracle (the reference step restated
 in C++) on the host cores instead.  Under torchrun each rank runs an independent replica
 (replicas only: the single-scene step does not shard), timed on the device, max over ranks.
 """
@@ -70,6 +70,18 @@ WORKLOADS = {
                                "(1.18M particles, asleep after its first substep) and a disk of "
                                "radius 40 launched into it; units count awake particles only",
                           material="NeoHookean-sleep", grid_res=1024, active_units=True),
+    "contact_1m": dict(builder="contact_slab", kwargs=dict(grid_res=1024),
+                       desc="multi-field contact: NeoHookean 896 x 192-cell slab on the floor and a "
+                            "320 x 256-cell grip block (contact_group 1) on it thrown at (1.5, -3), "
+                            "4 ppc, DirectionalContactGrip(0.1, 0.9, (1, 0)); reference-order "
+                            "pipeline (cell-sorted scatters, LR contact normals)",
+                       material="NeoHookean-contact", grid_res=1024),
+    "mixture_1m": dict(builder="mixture_overlap", kwargs=dict(grid_res=1024, side=362, iterations=0),
+                       desc="two-phase mixture without gravity: DruckerPrager sand (solid phase) and "
+                            "water (fluid phase) squares of 362 x 362 cells at 4 ppc each, "
+                            "overlapping, water at (0, -3), drag 5, no pressure projection; "
+                            "reference-order pipeline",
+                       material="DP+NewtonianFluid-mixture", grid_res=1024),
     "batched_256": dict(builder="batched_scenes", kwargs=dict(n_scenes=256),
                         desc="256 independent scenes in one batch: grid G ~ U{64..256}, target "
                              "N ~ logU[4k, 200k] particles (clipped to fit the grid), material "
@@ -85,8 +97,13 @@ DEFAULT_WORKLOAD = "dam_break_1m"
 #   fluid:    read x8 v8 C16 F16 m4 V0 4 V4 rho4 mat4 plastic16 rho_dp4 = 88,
 #             write x8 v8 C16 V4 rho4 = 40, grid 32/4 = 8              -> 136 B
 #   granular: read 84, write x8 v8 C16 F16 V4 rho4 plastic16 = 72, grid 8 -> 164 B
+#   NeoHookean: read x8 v8 C16 F16 m4 V0 4 V4 rho4 mat4 = 68, write x8 v8 C16 F16 V4 rho4 = 56,
+#             contact group 4, grid 8                                  -> 136 + 20 (sleep flag,
+#             field velocities) = 156 B
+#   mixture:  the mean of the granular (164) and fluid (136) particles    -> 150 B
 K_PARTICLE_BYTES = {"NewtonianFluid": 136, "DP+Snow+NACC": 164, "ZOO7": 164,
-                    "NewtonianFluid+fields": 136, "NeoHookean-sleep": 156}
+                    "NewtonianFluid+fields": 136, "NeoHookean-sleep": 156,
+                    "NeoHookean-contact": 156, "DP+NewtonianFluid-mixture": 150}
 
 
 def log(*a):
@@ -509,11 +526,15 @@ def main():
         # CUDA events on the simulation's stream (host-driven substep loop, same kernels).
         sim.set_option(OPT_USE_GRAPH, 0)
         part_us, subs_i = 0.0, 0
+        phase_keys = ("cfl_us", "project_us", "density_us", "p2g_us", "grid_update_us", "g2p_us")
+        phases = dict.fromkeys(phase_keys, 0.0)
         for _ in range(3):
             sim.flush_l2()
             sim.step_n(1, timing=True)
             part_us += sim.last_timing["g2p_us"]
             subs_i += sim.last_substeps()
+            for k in phase_keys:
+                phases[k] += sim.last_timing[k]
         sim.set_option(OPT_USE_GRAPH, 1)
         peak, peak_kind = load_peaks()
         per_launch_s = part_us * 1e-6 / max(subs_i, 1)
@@ -527,11 +548,16 @@ def main():
             "algorithmic_bytes_per_launch": alg_bytes, "launch_us": per_launch_s * 1e6,
             "peak_source": f"{peak_kind} hbm_gbs (MEASURED_PEAKS.json)" if peak_kind == "measured"
             else "fallback 6.65 TB/s"}
+        # where a substep's time goes (host-driven loop, CUDA events between the phases)
+        extras["phases_us_per_substep"] = {k[:-3]: v / max(subs_i, 1) for k, v in phases.items()}
 
         # End to end through the C ABI with host buffers: upload the particle state from
-        # pinned memory, step, read it back, every step.
+        # pinned memory, step, read it back into a second pinned buffer, every step.  The
+        # readback is asynchronous (its own stream), so step k's device-to-host copy overlaps
+        # step k+1's upload; the timed region ends after the last readback has landed.
         from emerge_engine_b200.simulation import PinnedBuffer
         host = PinnedBuffer(n * 128)
+        host_out = PinnedBuffer(n * 128)
         sim.read_particles_raw(host.ptr, n)
         e2e_steps = max(3, min(args.steps, 10))
         sub0 = sim.stats()["substeps"]
@@ -544,7 +570,8 @@ def main():
             sim.step()
             if spec.get("active_units"):
                 e2e_active += 0.5 * (a0 + sim.active_count()) * sim.last_substeps()
-            sim.read_particles_raw(host.ptr, n)
+            sim.read_particles_raw_async(host_out.ptr, n)
+        sim.synchronize()
         e2e_s = time.perf_counter() - t0
         e2e_subs = sim.stats()["substeps"] - sub0
         e2e_units = e2e_active if spec.get("active_units") else float(n * e2e_subs)
@@ -553,9 +580,12 @@ def main():
                                                      e2e_units, 0)
             e2e_s = e2e_ms / 1e3
         host.free()
+        host_out.free()
         extras["e2e"] = {"value": e2e_units / e2e_s, "unit": UNIT,
                          "h2d_bytes_per_step": n * 128, "d2h_bytes_per_step": n * 128,
-                         "steps": e2e_steps, "timing": "host wall clock around the C-ABI calls"}
+                         "steps": e2e_steps, "timing": "host wall clock around the C-ABI calls",
+                         "readback": "emerge_cuda_read_particles_async (copy stream; overlaps "
+                                     "the next step's upload)"}
         if spec["material"] == "DP+Snow+NACC" and not args.no_closure:
             extras["learned_closure"] = closure_ab(sim, n, args.steps, value)
         if world == 1 and rank == 0:

@@ -200,6 +200,7 @@ ABI_FUNCTIONS = [
     ("emerge_cuda_add_particles", c_int, [SIM, c_void_p, c_uint64, c_int]),
     ("emerge_cuda_particle_count", c_int, [SIM, POINTER(c_uint64)]),
     ("emerge_cuda_read_particles", c_int, [SIM, c_void_p, c_uint64]),
+    ("emerge_cuda_read_particles_async", c_int, [SIM, c_void_p, c_uint64]),
     ("emerge_cuda_write_particles", c_int, [SIM, c_void_p, c_uint64]),
     ("emerge_cuda_step", c_int, [SIM, c_uint32, POINTER(StepTimingC)]),
     ("emerge_cuda_last_substeps", c_int, [SIM, POINTER(c_uint64)]),

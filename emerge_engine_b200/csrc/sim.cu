@@ -120,6 +120,11 @@ struct emerge_sim {
     int cur = 0;
     Buffer staging;          // AoS staging (cap * 128 B)
     emerge_particle *d_aos = nullptr;
+    // asynchronous readback: its own AoS staging and stream, so a step's device-to-host copy
+    // overlaps the next step's upload and work
+    cudaStream_t copy_stream = nullptr;
+    cudaEvent_t ev_ready = nullptr, ev_gathered = nullptr;
+    Buffer staging_rb;
     uint32_t next_tag = 1;
     LoadFlagsHost lf;
     std::vector<uint8_t> host_pinned_flag;  // not used for stepping; kept for add/write scans
@@ -368,6 +373,7 @@ void update_material_flags(emerge_sim *s) {
 
 emerge_status ensure_capacity(emerge_sim *s, size_t need) {
     if (need <= s->cap) return EMERGE_OK;
+    if (s->copy_stream) CK(cudaStreamSynchronize(s->copy_stream));  // a readback may read the old sets
     size_t cap = s->cap ? s->cap : 1024;
     while (cap < need) cap *= 2;
     const size_t set_bytes = particle_set_bytes(cap);
@@ -1206,6 +1212,7 @@ emerge_status emerge_cuda_create(const emerge_sim_config *config, int device, em
 emerge_status emerge_cuda_destroy(emerge_sim *s) {
     if (!s) return EMERGE_OK;
     if (s->stream) cudaStreamSynchronize(s->stream);
+    if (s->copy_stream) cudaStreamSynchronize(s->copy_stream);
     destroy_graph(s);
     for (auto &ev : s->ev)
         if (ev) cudaEventDestroy(ev);
@@ -1215,6 +1222,10 @@ emerge_status emerge_cuda_destroy(emerge_sim *s) {
     if (s->h_state) cudaFreeHost(s->h_state);
     s->pbuf.reset();
     s->staging.reset();
+    s->staging_rb.reset();
+    if (s->ev_ready) cudaEventDestroy(s->ev_ready);
+    if (s->ev_gathered) cudaEventDestroy(s->ev_gathered);
+    if (s->copy_stream) cudaStreamDestroy(s->copy_stream);
     s->detbuf.reset();
     s->gbuf.reset();
     s->mbuf.reset();
@@ -1394,6 +1405,36 @@ emerge_status emerge_cuda_read_particles(emerge_sim *s, emerge_particle *out, ui
     return EMERGE_OK;
 }
 
+emerge_status emerge_cuda_read_particles_async(emerge_sim *s, emerge_particle *out, uint64_t n) {
+    if (!s || (!out && n)) return EMERGE_ERR_INVALID_ARG;
+    if (n != s->n) return static_cast<emerge_status>(s->fail(EMERGE_ERR_INVALID_ARG, "n must equal the particle count"));
+    if (n == 0) return EMERGE_OK;
+    if (!s->copy_stream) {
+        CK(cudaStreamCreateWithFlags(&s->copy_stream, cudaStreamNonBlocking));
+        CK(cudaEventCreateWithFlags(&s->ev_ready, cudaEventDisableTiming));
+        CK(cudaEventCreateWithFlags(&s->ev_gathered, cudaEventDisableTiming));
+    }
+    const size_t bytes = s->cap * sizeof(emerge_particle);
+    if (s->staging_rb.bytes < bytes) {
+        CK(cudaStreamSynchronize(s->copy_stream));  // the old buffer may still be copied out
+        s->staging_rb.reset();
+        CK(cudaMalloc(&s->staging_rb.ptr, bytes));
+        s->staging_rb.bytes = bytes;
+    }
+    emerge_particle *rb = static_cast<emerge_particle *>(s->staging_rb.ptr);
+    // gather on the copy stream once the queued steps are done; later work on the
+    // simulation's stream waits for the gather only, not for the copy-out
+    CK(cudaEventRecord(s->ev_ready, s->stream));
+    CK(cudaStreamWaitEvent(s->copy_stream, s->ev_ready, 0));
+    launch_gather_aos(s->P[s->cur], static_cast<int>(n), rb, s->copy_stream);
+    s->host_launches += 1;
+    CK(cudaEventRecord(s->ev_gathered, s->copy_stream));
+    CK(cudaStreamWaitEvent(s->stream, s->ev_gathered, 0));
+    CK(cudaMemcpyAsync(out, rb, n * sizeof(emerge_particle), cudaMemcpyDeviceToHost, s->copy_stream));
+    CK(cudaGetLastError());
+    return EMERGE_OK;
+}
+
 emerge_status emerge_cuda_write_particles(emerge_sim *s, const emerge_particle *in, uint64_t n) {
     if (!s || (!in && n)) return EMERGE_ERR_INVALID_ARG;
     if (n != s->n) return static_cast<emerge_status>(s->fail(EMERGE_ERR_INVALID_ARG, "n must equal the particle count"));
@@ -1545,6 +1586,7 @@ emerge_status emerge_cuda_last_counters(emerge_sim *s, uint64_t *vel_clamp, uint
 emerge_status emerge_cuda_synchronize(emerge_sim *s) {
     if (!s) return EMERGE_ERR_INVALID_ARG;
     CK(cudaStreamSynchronize(s->stream));
+    if (s->copy_stream) CK(cudaStreamSynchronize(s->copy_stream));
     return EMERGE_OK;
 }
 

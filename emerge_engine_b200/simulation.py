@@ -372,6 +372,11 @@ class Simulation:
         """Read back `n` particles into host memory at address `ptr` (AoS, 128 B each)."""
         self._check(self._lib.emerge_cuda_read_particles(self._sim, c_void_p(ptr), int(n)))
 
+    def read_particles_raw_async(self, ptr: int, n: int) -> None:
+        """Enqueue the readback of `n` particles into host memory at `ptr` (AoS, 128 B each);
+        the memory holds them after the next synchronize()."""
+        self._check(self._lib.emerge_cuda_read_particles_async(self._sim, c_void_p(ptr), int(n)))
+
     # ---------------------------------------------------------------- learned closure
     # No counterpart in the reference: a network standing in for the smooth plastic branch
     # of the Drucker-Prager (model 0) and NACC (model 1) return mappings.

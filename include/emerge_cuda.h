@@ -318,6 +318,14 @@ emerge_status emerge_cuda_particle_count(const emerge_sim *sim, uint64_t *n_out)
 /* Simulation::particles() (lifecycle.rs:214): copies all particles, in the
  * reference's index order, into `out` (n must equal the particle count). */
 emerge_status emerge_cuda_read_particles(emerge_sim *sim, emerge_particle *out, uint64_t n);
+/* Asynchronous Simulation::particles() (no reference counterpart: the reference's read is a
+ * borrow of host memory).  Enqueues the copy of every particle into `out` (reference index
+ * order, n = particle count) after the work already queued, and returns at once.  The copy
+ * runs on a stream of its own: later steps and uploads wait only for its device-side
+ * gather, so the device-to-host transfer overlaps them.  `out` is complete after the next
+ * emerge_cuda_synchronize; page-locked memory (emerge_cuda_host_alloc) lets the transfer
+ * run asynchronously.  Successive calls complete in order. */
+emerge_status emerge_cuda_read_particles_async(emerge_sim *sim, emerge_particle *out, uint64_t n);
 /* Simulation::particles_mut() (lifecycle.rs:233) write-back: replaces every
  * particle's state from `in` (reference index order). */
 emerge_status emerge_cuda_write_particles(emerge_sim *sim, const emerge_particle *in, uint64_t n);
@@ -340,7 +348,7 @@ emerge_status emerge_cuda_effective_dt(emerge_sim *sim, float *out);
  * last_sim_time_dropped (:65) of the last step. Synchronises. */
 emerge_status emerge_cuda_last_counters(emerge_sim *sim, uint64_t *vel_clamp_count,
                                         uint64_t *j_projection_count, float *sim_time_dropped);
-/* Blocks until all queued work of `sim` is done. */
+/* Blocks until all queued work of `sim` is done, asynchronous readbacks included. */
 emerge_status emerge_cuda_synchronize(emerge_sim *sim);
 
 /* ---- queries --------------------------------------------------------------------- */

@@ -386,3 +386,59 @@ def mixture_scene(sim_cls, grid_res=96, seed=17, dt=0.05, drag=5.0, iterations=2
     sim.add_body(a)
     sim.add_body(b)
     return sim
+
+
+def contact_slab(sim_cls, grid_res=1024, slab=(896, 192), block=(320, 256), seed=23, **sim_kw):
+    """Multi-field contact at scale: a NeoHookean (400, 200) slab of `slab` cells at 4 ppc on
+    the floor and a grip block (contact_group 1) of `block` cells on top of it, thrown at
+    (1.5, -3), with DirectionalContactGrip(0.1, 0.9, (1, 0)); the two touch from the start."""
+    from emerge_engine_b200 import DirectionalContactGrip
+    cfg = SimConfig.standard(grid_res, 0.05, (0.0, -1.0))
+    t = cfg.boundary_thickness
+    sim = sim_cls.empty(cfg, **sim_kw).with_default_material(NeoHookeanMaterial.new(400.0, 200.0))
+    sim.set_contact_grip(DirectionalContactGrip(0.1, 0.9, (1.0, 0.0)))
+    a = SpawnRegion.for_sim(cfg)
+    a.spacing, a.box_size = 0.5, slab
+    a.box_center = (grid_res / 2.0, t + 1 + slab[1] / 2.0)
+    a.position_jitter, a.rng_seed = 0.3, seed
+    b = SpawnRegion.for_sim(cfg)
+    b.spacing, b.box_size = 0.5, block
+    b.box_center = (grid_res / 2.0 - block[0] / 4.0, t + 1 + slab[1] + block[1] / 2.0 + 0.5)
+    b.position_jitter, b.rng_seed = 0.3, seed + 1
+    sim.add_body(a)
+    tag = sim.add_body(b)
+    p = sim.particles()
+    g = p["user_tag"] == tag
+    p["contact_group"][g] = 1
+    p["v"][g] = (1.5, -3.0)
+    sim.set_particles(p)
+    return sim
+
+
+def mixture_overlap(sim_cls, grid_res=1024, side=362, seed=29, drag=5.0, iterations=2, **sim_kw):
+    """Two-phase mixture at scale, without gravity (the reference's two-phase drag test,
+    tests/solver.rs:1888-1990, at scale): a DruckerPrager sand square (1e5 / 0.3, solid phase)
+    and a water square (NewtonianFluid 1000 / 1e4, fluid phase), `side` cells at 4 ppc each,
+    overlapping in the middle of the domain, the water moving through the sand at (0, -3);
+    particle masses of 125 give the overlap the water's rest density.
+    mixture_drag_coefficient `drag`, mixture_pressure_iterations `iterations`."""
+    from emerge_engine_b200 import FLUID_PHASE, SOLID_PHASE, WithMixturePhase
+    cfg = SimConfig.standard(grid_res, 0.05, (0.0, 0.0))
+    cfg.mixture_drag_coefficient = drag
+    cfg.mixture_pressure_iterations = iterations
+    sim = (sim_cls.empty(cfg, **sim_kw)
+           .with_default_material(WithMixturePhase(DruckerPragerMaterial.cohesionless(1e5, 0.3),
+                                                   SOLID_PHASE))
+           .with_material(1, WithMixturePhase(NewtonianFluidMaterial.low_viscosity(1000.0, 1e4),
+                                              FLUID_PHASE)))
+    tags = []
+    for k in range(2):
+        s = SpawnRegion.for_sim(cfg)
+        s.spacing, s.box_size, s.material_id = 0.5, (side, side), k
+        s.box_center = (grid_res / 2.0, grid_res / 2.0)
+        s.position_jitter, s.rng_seed, s.mass_override = 0.3, seed + k, 125.0
+        tags.append(sim.add_body(s))
+    p = sim.particles()
+    p["v"][p["user_tag"] == tags[1]] = (0.0, -3.0)
+    sim.set_particles(p)
+    return sim
