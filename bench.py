@@ -80,7 +80,7 @@ WORKLOADS = {
                        desc="two-phase mixture without gravity: DruckerPrager sand (solid phase) and "
                             "water (fluid phase) squares of 362 x 362 cells at 4 ppc each, "
                             "overlapping, water at (0, -3), drag 5, no pressure projection; "
-                            "reference-order pipeline",
+                            "fused pipeline (phase sums with the total)",
                        material="DP+NewtonianFluid-mixture", grid_res=1024),
     "batched_256": dict(builder="batched_scenes", kwargs=dict(n_scenes=256),
                         desc="256 independent scenes in one batch: grid G ~ U{64..256}, target "

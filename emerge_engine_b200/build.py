@@ -28,13 +28,15 @@ SOURCES = {
     "fast_kernels.cu": FAST,
     "det_kernels.cu": EXACT,
     "multifield.cu": EXACT,
+    "multifield_fast.cu": FAST,
     "sort.cu": EXACT,
     "sort_noalloc.cu": EXACT,
     "sim.cu": EXACT,
     "closure.cu": FAST,
     "batch.cu": EXACT,
 }
-HEADERS = ["physics.cuh", "device_state.cuh", "kernels.h", "particle_pass.cuh", "closure.cuh", "closure_host.h"]
+HEADERS = ["physics.cuh", "device_state.cuh", "kernels.h", "particle_pass.cuh", "closure.cuh", "closure_host.h",
+           "multifield.cuh"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC,-ffp-contract=off"]
 NVCC = os.environ.get("NVCC", "nvcc")

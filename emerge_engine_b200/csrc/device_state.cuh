@@ -72,7 +72,7 @@ struct StepState {
     uint32_t upload_flags;      // k_check_aos: bit 0 contact_group != 0, bit 1 pinned
     uint32_t active;            // batches: the scene takes part in the running substep
     uint32_t contact_active;    // Grid::has_contact_activity of the running substep
-    uint32_t pad_;
+    uint32_t n_iface;           // fast pipeline: contact cells holding both fields this substep
 };
 
 struct GridView {
@@ -93,7 +93,20 @@ struct GridView {
     int2 *rec_range;
     float *mx_as, *mx_af, *mx_k, *mx_rhs, *mx_p[2];
     uint8_t *mx_sig;
+    // fast pipeline: the fields' P2G sums in the dt-free split ({m, Ax, Ay, w}, {Sx, Sy};
+    // grip, solid, fluid), turned into acc_grip / acc_sol / acc_flu by the grid update; the
+    // contact point cloud as per-base-cell lists (heads indexed x * res + y, one set per
+    // substep parity) of nodes {x, y, label, next} indexed by particle slot; the contact
+    // cells holding both fields (flat indices, StepState::n_iface of them)
+    float4 *fa[3];
+    float2 *fs[3];
+    int *chead[2];
+    float4 *cpts;
+    int *iface;
 };
+
+// StepState::error_flags bits
+constexpr uint32_t ERR_CONTACT_LIST = 1u;  // a contact point-list walk was cut short
 
 __host__ __device__ __forceinline__ int cell_index(int x, int y, int tpd) {
     return (((x >> 3) * tpd + (y >> 3)) << 6) | ((x & 7) << 3) | (y & 7);

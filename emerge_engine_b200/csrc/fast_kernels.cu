@@ -94,7 +94,7 @@ void launch_particle_pass_fast(const ParticleKernelArgs &a, unsigned model_mask,
     const int grid = blocks_for(a.n, THREADS);
     const unsigned plastic = (1u << M_DRUCKER_PRAGER) | (1u << M_NACC);
     if ((a.cl.infer || a.cl.log) && (model_mask & plastic)) {
-        const unsigned cover = covering_mask(model_mask);
+        const unsigned cover = (model_mask & EXTRAS) ? FULL_MODELS : covering_mask(model_mask);
         if (cover == MASK_GRANULAR)
             k_particle_closure<MASK_GRANULAR><<<grid, THREADS, 0, stream>>>(a);
         else if (cover == FULL_MODELS)
@@ -109,6 +109,11 @@ void launch_particle_pass_fast(const ParticleKernelArgs &a, unsigned model_mask,
     case MASK_SOLID_FLUID: k_particle_fast<MASK_SOLID_FLUID><<<grid, THREADS, 0, stream>>>(a); break;
     case MASK_GRANULAR: k_particle_fast<MASK_GRANULAR><<<grid, THREADS, 0, stream>>>(a); break;
     case ALL_MODELS: k_particle_fast<ALL_MODELS><<<grid, THREADS, 0, stream>>>(a); break;
+    case MASK_FLUID_X: k_particle_fast<MASK_FLUID_X><<<grid, THREADS, 0, stream>>>(a); break;
+    case MASK_SOLID_X: k_particle_fast<MASK_SOLID_X><<<grid, THREADS, 0, stream>>>(a); break;
+    case MASK_SOLID_FLUID_X: k_particle_fast<MASK_SOLID_FLUID_X><<<grid, THREADS, 0, stream>>>(a); break;
+    case MASK_GRANULAR_X: k_particle_fast<MASK_GRANULAR_X><<<grid, THREADS, 0, stream>>>(a); break;
+    case ALL_MODELS_X: k_particle_fast<ALL_MODELS_X><<<grid, THREADS, 0, stream>>>(a); break;
     default: k_particle_fast<FULL_MODELS><<<grid, THREADS, 0, stream>>>(a); break;
     }
 }
@@ -121,6 +126,11 @@ void launch_density_pass_fast(const DensityKernelArgs &a, unsigned model_mask, c
     case MASK_SOLID_FLUID: k_density<MASK_SOLID_FLUID><<<grid, THREADS, 0, stream>>>(a); break;
     case MASK_GRANULAR: k_density<MASK_GRANULAR><<<grid, THREADS, 0, stream>>>(a); break;
     case ALL_MODELS: k_density<ALL_MODELS><<<grid, THREADS, 0, stream>>>(a); break;
+    case MASK_FLUID_X: k_density<MASK_FLUID_X><<<grid, THREADS, 0, stream>>>(a); break;
+    case MASK_SOLID_X: k_density<MASK_SOLID_X><<<grid, THREADS, 0, stream>>>(a); break;
+    case MASK_SOLID_FLUID_X: k_density<MASK_SOLID_FLUID_X><<<grid, THREADS, 0, stream>>>(a); break;
+    case MASK_GRANULAR_X: k_density<MASK_GRANULAR_X><<<grid, THREADS, 0, stream>>>(a); break;
+    case ALL_MODELS_X: k_density<ALL_MODELS_X><<<grid, THREADS, 0, stream>>>(a); break;
     default: k_density<FULL_MODELS><<<grid, THREADS, 0, stream>>>(a); break;
     }
 }

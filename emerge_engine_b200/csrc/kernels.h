@@ -77,6 +77,10 @@ void launch_segsum(const uint32_t *keys, const uint32_t *vals, const float4 *pay
 // multi-field contact and mixture coupling after the grid update (multifield.cu)
 void launch_contact_resolve(const StepLaunch &L, const uint32_t *vals, const float4 *points);
 void launch_mixture_resolve(const StepLaunch &L);
+// fast pipeline: contact from the particle pass's base-cell lists (multifield_fast.cu), and
+// the per-substep clear
+void launch_contact_resolve_lists(const StepLaunch &L);
+void launch_multi_clear(const StepLaunch &L);
 
 // sort.cu
 // Scratch for a stable LSD radix sort of up to `capacity` (key, value) pairs.

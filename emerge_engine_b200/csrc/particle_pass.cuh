@@ -217,8 +217,7 @@ __device__ __forceinline__ float2 field_node_v(const GridView &g, int ci, int se
 }
 
 // G2P phase 1 for one particle (transfer/g2p.rs:217-326; ASFLIP and the multi-field node
-// velocities compiled in with EXTRAS, the latter on the FAST = false path that multi-field
-// scenes run).  Returns 1 if the speed clamp fired.
+// velocities compiled in with EXTRAS).  Returns 1 if the speed clamp fired.
 // FAST = false: the reference's cell-by-cell expression order (bit-level parity).
 // FAST = true: the same sums in stencil-offset form with fused multiply-adds:
 //   v' = sum w v_i,  B = v' (x) e + [sum (gx-1) w v_i, sum (gy-1) w v_i].
@@ -235,6 +234,18 @@ __device__ __forceinline__ int g2p_particle(const GridView &g, const DevConfig &
             load_stencil_v<false>(g, w, nv);
         else
             load_stencil_v<true>(g, w, nv);
+        if constexpr (EXTRAS) {
+            if (sel != 0) {
+#pragma unroll
+                for (int gx = 0; gx < 3; ++gx)
+#pragma unroll
+                    for (int gy = 0; gy < 3; ++gy) {
+                        const int cx = w.bx + gx - 1, cy = w.by + gy - 1;
+                        if (inside || in_domain(cx, cy, g.res))
+                            nv[gx][gy] = field_node_v(g, cell_index(cx, cy, g.tpd), sel, nv[gx][gy]);
+                    }
+            }
+        }
         float2 sx = v2(0.0f, 0.0f), sy = v2(0.0f, 0.0f);
 #pragma unroll
         for (int gx = 0; gx < 3; ++gx) {
@@ -329,6 +340,15 @@ constexpr unsigned MASK_SOLID = (1u << M_FALLBACK) | (1u << M_NEOHOOKEAN);
 constexpr unsigned MASK_SOLID_FLUID = MASK_FLUID | MASK_SOLID;
 constexpr unsigned MASK_GRANULAR =
     (1u << M_FALLBACK) | (1u << M_DRUCKER_PRAGER) | (1u << M_SNOW) | (1u << M_NACC);
+// The same sets with the extras (force fields, ASFLIP, sleep zones, multi-field) compiled in.
+constexpr unsigned EXTRAS = 1u << M_EXTRAS_BIT;
+constexpr unsigned MASK_FLUID_X = MASK_FLUID | EXTRAS;
+constexpr unsigned MASK_SOLID_X = MASK_SOLID | EXTRAS;
+constexpr unsigned MASK_SOLID_FLUID_X = MASK_SOLID_FLUID | EXTRAS;
+constexpr unsigned MASK_GRANULAR_X = MASK_GRANULAR | EXTRAS;
+constexpr unsigned ALL_MODELS_X = ALL_MODELS | EXTRAS;
+// The model set without the extras bit.
+__host__ __device__ constexpr unsigned core_mask(unsigned m) { return m & ~EXTRAS; }
 
 // ---------------------------------------------------------------- scatter engine
 // P2G scatter of one particle per thread with vector red.global reductions (native
@@ -353,6 +373,7 @@ struct Payload {
     float s;      // -4 * stress_volume (dt-free stress coefficient)
     bool do_ma;   // scatter mass + affine momentum
     bool do_s;    // scatter stress impulse
+    uint32_t fields;  // multi-field sums it also adds to: bit 0 grip, 1 solid, 2 fluid
 };
 
 // Which channels a scatter call carries: mass + momentum, stress, or per-particle flags.
@@ -424,10 +445,11 @@ __device__ __forceinline__ void mark_tiles(const GridView &g, int bx, int by) {
     }
 }
 
-// One lane's 3 x 3 reductions (no aggregation).  CHECK skips cells outside the domain.
+// One lane's 3 x 3 reductions (no aggregation) into the accumulators A (mass + momentum)
+// and S (stress).  CHECK skips cells outside the domain.
 template <int SC, bool CHECK>
-__device__ __forceinline__ void scatter_cells(const GridView &g, const ScatterPlan &pl,
-                                              bool do_ma, bool do_s) {
+__device__ __forceinline__ void scatter_cells_to(const GridView &g, const ScatterPlan &pl,
+                                                 bool do_ma, bool do_s, float4 *A, float2 *S) {
     const QW &w = pl.w;
     int yp[3];
 #pragma unroll
@@ -445,10 +467,16 @@ __device__ __forceinline__ void scatter_cells(const GridView &g, const ScatterPl
             const int ci = xp + yp[gy];
             // the fourth lane counts scatters: a cell with w > 0 is in the reference's dirty set
             if (SC == SC_MA || (SC == SC_BOTH && do_ma))
-                red_add_v4(&g.acc_a[ci], wm * w.wy[gy], wt * t.x, wt * t.y, 1.0f);
-            if (SC == SC_S || (SC == SC_BOTH && do_s)) red_add_v2(&g.acc_s[ci], wt * t.z, wt * t.w);
+                red_add_v4(&A[ci], wm * w.wy[gy], wt * t.x, wt * t.y, 1.0f);
+            if (SC == SC_S || (SC == SC_BOTH && do_s)) red_add_v2(&S[ci], wt * t.z, wt * t.w);
         }
     }
+}
+
+template <int SC, bool CHECK>
+__device__ __forceinline__ void scatter_cells(const GridView &g, const ScatterPlan &pl,
+                                              bool do_ma, bool do_s) {
+    scatter_cells_to<SC, CHECK>(g, pl, do_ma, do_s, g.acc_a, g.acc_s);
 }
 
 // Warp-aggregated variant: every lane of the warp takes part (inactive lanes add zero).
@@ -500,7 +528,8 @@ __device__ __forceinline__ void scatter_cells_aggregated(const GridView &g, cons
             const int cx = w.bx + gx - 1, cy = w.by + gy - 1;
             if (head && active && in_domain(cx, cy, g.res)) {
                 const int ci = xp + yp[gy];
-                if (any_ma) red_add_v4(&g.acc_a[ci], mc, ax, ay, 1.0f);
+                // the fourth lane counts the segment's scatters, one per particle
+                if (any_ma) red_add_v4(&g.acc_a[ci], mc, ax, ay, static_cast<float>(seg_end - lane));
                 if (any_s) red_add_v2(&g.acc_s[ci], sx, sy);
             }
         }
@@ -523,7 +552,38 @@ __device__ __forceinline__ void scatter_particle(const GridView &g, const Payloa
         else
             scatter_cells<SC, true>(g, pl, p.do_ma, p.do_s);
     }
-    if (active) mark_tiles(g, pl.w.bx, pl.w.by);
+    if (active) {
+        mark_tiles(g, pl.w.bx, pl.w.by);
+        // the multi-field sums of the fast pipeline (p2g.rs:60-66): the same contributions
+        for (uint32_t f = p.fields; f != 0u; f &= f - 1u) {
+            const int k = __ffs(f) - 1;
+            scatter_cells_to<SC, true>(g, pl, p.do_ma, p.do_s, g.fa[k], g.fs[k]);
+        }
+    }
+}
+
+// The multi-field sums a particle adds to on the fast pipeline: the grip field for a
+// contact group (contact.rs:41-72), its material's phase field (mixture.rs:20-58).
+__device__ __forceinline__ uint32_t multi_fields(const DevConfig &cfg, const DevParticles &P, int i,
+                                                 uint32_t mat, int n_mats) {
+    uint32_t f = 0u;
+    if ((cfg.mf_fields & 1) && P.contact[i] != 0u) f |= 1u;
+    if (cfg.mf_fields & 2) {
+        const uint32_t ph = cfg.mat_phase[mat < static_cast<uint32_t>(n_mats) ? mat : 0u];
+        f |= ph == 1u ? 2u : (ph == 2u ? 4u : 0u);
+    }
+    return f;
+}
+
+// The contact point cloud on the fast pipeline (p2g.rs:54-74): every particle that scatters
+// is pushed onto its base cell's list; the cells of its stencil find it in the lists of
+// their 3 x 3 neighbourhood.
+__device__ __forceinline__ void push_contact_point(const GridView &g, float2 x, bool grip, int i,
+                                                   uint32_t slot) {
+    const QW w = quadratic_weights(x);
+    if (!in_domain(w.bx, w.by, g.res)) return;
+    const int prev = atomicExch(&g.chead[slot][w.bx * g.res + w.by], i);
+    g.cpts[i] = make_float4(x.x, x.y, grip ? 1.0f : -1.0f, __int_as_float(prev));
 }
 
 // ---------------------------------------------------------------- k_particle
@@ -815,6 +875,7 @@ __device__ __forceinline__ void particle_pass(const ParticleKernelArgs &a) {
     Payload pl;
     pl.do_ma = false;
     pl.do_s = false;
+    pl.fields = 0u;
     float max_speed = 0.0f;
     float min_mdt = INFINITY;
     int clamped = 0, projected = 0, proj_changed = 0;
@@ -843,7 +904,7 @@ __device__ __forceinline__ void particle_pass(const ParticleKernelArgs &a) {
                 }
             }
             int sel = 0;  // multi-field node velocities (g2p.rs:219-238)
-            if constexpr (!FAST && HAS_MODEL(MASK, M_EXTRAS_BIT)) {
+            if constexpr (HAS_MODEL(MASK, M_EXTRAS_BIT)) {
                 if (cfg.multi) {
                     if (st->contact_active) {
                         sel = a.P.contact[i] != 0u ? 2 : 1;
@@ -916,6 +977,12 @@ __device__ __forceinline__ void particle_pass(const ParticleKernelArgs &a) {
                 pl.s = -stress_volume(m, p) * KERNEL_D_INVERSE;
                 pl.do_s = true;
             }
+            if constexpr (HAS_MODEL(MASK, M_EXTRAS_BIT)) {
+                if (cfg.mf_fast) {
+                    pl.fields = multi_fields(cfg, a.P, i, p.mat, n_mats);
+                    if (cfg.mf_fields & 1) push_contact_point(g, p.x, (pl.fields & 1u) != 0u, i, acc_slot);
+                }
+            }
         }
     }
     count_warp(&st->vel_clamp, clamped != 0);
@@ -936,7 +1003,7 @@ __device__ __forceinline__ void particle_pass(const ParticleKernelArgs &a) {
             atomicAdd(&st->window_blocks, 1ull);
         }
     }
-    if (MASK == MASK_FLUID && density_mode)
+    if (core_mask(MASK) == MASK_FLUID && density_mode)
         scatter_particle<SC_MA>(g, pl, valid, a.aggregate);
     else
         scatter_particle<SC_BOTH>(g, pl, valid, a.aggregate);
@@ -1009,7 +1076,7 @@ __device__ __forceinline__ void density_pass(const DensityKernelArgs &a) {
         p.mat = a.P.mat[i];
         // the fluid stress's own fields, issued with the position so their latency overlaps
         // the density gather (in a fluid-only scene every particle is a fluid or fallback)
-        if constexpr (MASK == MASK_FLUID) {
+        if constexpr (core_mask(MASK) == MASK_FLUID) {
             p.c = m_from4(a.P.c[i]);
             p.mass = a.P.mass[i];
         }
@@ -1019,6 +1086,7 @@ __device__ __forceinline__ void density_pass(const DensityKernelArgs &a) {
     Payload pl;
     pl.do_ma = false;
     pl.do_s = false;
+    pl.fields = 0u;
     if (valid) {
         if (reproject) {
             p = load_state(a.P, i, a.lf);
@@ -1031,7 +1099,7 @@ __device__ __forceinline__ void density_pass(const DensityKernelArgs &a) {
         const MatP &m = s_mats[p.mat < static_cast<uint32_t>(n_mats) ? p.mat : 0u];
         if (m.model == M_FLUID) {
             if (!reproject) {  // the fields the fluid stress reads (fluid.rs:135-195)
-                if constexpr (MASK != MASK_FLUID) {
+                if constexpr (core_mask(MASK) != MASK_FLUID) {
                     p.c = m_from4(a.P.c[i]);
                     p.mass = a.P.mass[i];
                 }
@@ -1052,6 +1120,8 @@ __device__ __forceinline__ void density_pass(const DensityKernelArgs &a) {
             pl.tau = combined_kirchhoff_stress<MASK>(m, p, pr);
             pl.s = -stress_volume(m, p) * KERNEL_D_INVERSE;
             pl.do_s = true;
+            if constexpr (HAS_MODEL(MASK, M_EXTRAS_BIT))
+                if (cfg.mf_fast) pl.fields = multi_fields(cfg, a.P, i, p.mat, n_mats);
         }
     }
     scatter_particle<SC_S>(g, pl, valid, a.aggregate);
@@ -1063,7 +1133,8 @@ void launch_density_pass_fast(const DensityKernelArgs &a, unsigned model_mask, c
 
 // Smallest instantiated model set that covers the registered models.
 inline unsigned covering_mask(unsigned m) {
-    const unsigned masks[5] = {MASK_FLUID, MASK_SOLID, MASK_SOLID_FLUID, MASK_GRANULAR, ALL_MODELS};
+    const unsigned masks[10] = {MASK_FLUID,   MASK_SOLID,   MASK_SOLID_FLUID,   MASK_GRANULAR,   ALL_MODELS,
+                                MASK_FLUID_X, MASK_SOLID_X, MASK_SOLID_FLUID_X, MASK_GRANULAR_X, ALL_MODELS_X};
     for (unsigned c : masks)
         if ((m & ~c) == 0u) return c;
     return FULL_MODELS;

@@ -948,6 +948,8 @@ struct DevConfig {
     float mix_drag;          // SimConfig::mixture_drag_coefficient
     int mix_iters;           // SimConfig::mixture_pressure_iterations
     const uint32_t *mat_phase;  // MixturePhase per material slot: 0 none, 1 solid, 2 fluid
+    int mf_fast;             // multi-field scene on the fast (fused, unordered-sum) pipeline
+    int mf_fields;           // fields in use: bit 0 grip (contact), bit 1 solid + fluid (mixture)
 };
 
 // Bits of DevParticles::sleeping while the sleep partition is in use: bit 0 is

@@ -293,10 +293,11 @@ bool mixture_on(const emerge_sim *s) {
         if (ph != 0) return true;
     return false;
 }
-// Multi-field scenes run the reference-order pipeline: its cell-sorted scatter records give
-// every contact cell its point cloud in particle index order.
+// Multi-field contact or mixture in use.  In the reference-order pipeline the cell-sorted
+// scatter records give every contact cell its point cloud in particle index order; the fast
+// pipeline sums the fields with the total and lists the particles per base cell.
 bool multi_on(const emerge_sim *s) { return s->contact_seen || mixture_on(s); }
-bool det_pipeline(const emerge_sim *s) { return s->deterministic || s->dcfg.multi; }
+bool det_pipeline(const emerge_sim *s) { return s->deterministic != 0; }
 
 // The sleep partition is in use: sleep scoring is on, or some particle is outside the
 // active zone.
@@ -327,6 +328,8 @@ void refresh_dev_config(emerge_sim *s) {
     s->dcfg.mix_drag = s->cfg.mixture_drag_coefficient;
     s->dcfg.mix_iters = static_cast<int>(s->cfg.mixture_pressure_iterations);
     s->dcfg.mat_phase = s->mfbuf.ptr ? static_cast<const uint32_t *>(s->mfbuf.ptr) : nullptr;
+    s->dcfg.mf_fast = (s->dcfg.multi && !s->deterministic) ? 1 : 0;
+    s->dcfg.mf_fields = (s->contact_seen ? 1 : 0) | (mixture_on(s) ? 2 : 0);
     s->dcfg.n_fields = s->n_fields;
     s->dcfg.fields = s->n_fields ? static_cast<const emerge_force_field *>(s->fbuf.ptr) : nullptr;
     s->dcfg.field_data = s->n_fields ? reinterpret_cast<const float *>(
@@ -438,6 +441,23 @@ void destroy_graph(emerge_sim *s) {
     s->graph = nullptr;
 }
 
+// Kernels the fast pipeline adds to a substep for multi-field scenes: the clear, the two
+// contact kernels, the mixture kernels.
+int multi_fast_launches(const DevConfig &c) {
+    if (!c.mf_fast) return 0;
+    int k = 1;
+    if (c.mf_fields & 1) k += 2;
+    if (c.mf_fields & 2) k += (c.mix_drag <= 0.0f || c.mix_iters <= 0) ? 1 : 3 + c.mix_iters;
+    return k;
+}
+
+// After the grid update: contact and mixture coupling (step.rs:166-197) on the fast pipeline.
+void enqueue_multi_resolves(const StepLaunch &L) {
+    if (!L.cfg.mf_fast) return;
+    if (L.cfg.mf_fields & 1) launch_contact_resolve_lists(L);
+    if (L.cfg.mf_fields & 2) launch_mixture_resolve(L);
+}
+
 emerge_status build_graph(emerge_sim *s) {
     destroy_graph(s);
     StepLaunch L = make_launch(s);
@@ -463,11 +483,13 @@ emerge_status build_graph(emerge_sim *s) {
     cudaGraphNode_t wnode;
     CK(cudaGraphAddNode(&wnode, graph, nodes.data(), nn, &cp));
     cudaGraph_t body = cp.conditional.phGraph_out[0];
-    const int kps = 3 + (L.density_mode ? 1 : 0);
+    const int kps = 3 + (L.density_mode ? 1 : 0) + multi_fast_launches(L.cfg);
     CK(cudaStreamBeginCaptureToGraph(s->stream, body, nullptr, nullptr, 0,
                                      cudaStreamCaptureModeThreadLocal));
     launch_substep_begin(L, 1, static_cast<unsigned long long>(handle), kps);
+    if (L.cfg.mf_fast) launch_multi_clear(L);
     launch_grid_update(L);
+    enqueue_multi_resolves(L);
     launch_particle_pass(L, s->lf, 1, L.cfg.project, 1);
     if (L.density_mode) launch_density_pass(L, s->lf);
     CK(cudaStreamEndCapture(s->stream, &body));
@@ -479,6 +501,10 @@ emerge_status build_graph(emerge_sim *s) {
 emerge_status prime(emerge_sim *s) {
     StepLaunch L = make_launch(s);
     launch_prime_setup(L);
+    if (L.cfg.mf_fast) {  // the lists and field sums the prime's scatter fills
+        launch_multi_clear(L);
+        s->host_launches += 1;
+    }
     if (det_pipeline(s)) {  // CFL reduction only; the substep scatters after dt is known
         launch_particle_pass(L, s->lf, 0, 0, 0);
         s->host_launches += 2;
@@ -545,12 +571,14 @@ emerge_status run_host_loop_step(emerge_sim *s, bool timed) {
         }
         CK(cudaEventRecord(s->ev[1], s->stream));
         launch_substep_begin(L, 0, 0ull, 0);
+        if (L.cfg.mf_fast) launch_multi_clear(L);
         CK(cudaEventRecord(s->ev[2], s->stream));
         launch_grid_update(L);
+        enqueue_multi_resolves(L);
         CK(cudaEventRecord(s->ev[3], s->stream));
         launch_particle_pass(L, s->lf, 1, L.cfg.project, 1);
         CK(cudaEventRecord(s->ev[4], s->stream));
-        s->host_launches += 3;
+        s->host_launches += 3 + multi_fast_launches(L.cfg);
         if (L.density_mode) {
             launch_density_pass(L, s->lf);
             s->host_launches += 1;
@@ -1026,6 +1054,11 @@ emerge_status invalidate_pending(emerge_sim *s) {
     CK(cudaMemsetAsync(s->g.acc_a, 0, cells * sizeof(float4), s->stream));
     CK(cudaMemsetAsync(s->g.acc_s, 0, cells * sizeof(float2), s->stream));
     CK(cudaMemsetAsync(s->g.tile_flag, 0, static_cast<size_t>(s->tpd) * s->tpd, s->stream));
+    if (s->mfbuf.ptr)  // the fast pipeline's field sums of the pending scatter
+        for (int f = 0; f < 3; ++f) {
+            CK(cudaMemsetAsync(s->g.fa[f], 0, cells * sizeof(float4), s->stream));
+            CK(cudaMemsetAsync(s->g.fs[f], 0, cells * sizeof(float2), s->stream));
+        }
     s->pending_valid = false;
     return EMERGE_OK;
 }
@@ -1044,13 +1077,15 @@ emerge_status upload_phases(emerge_sim *s) {
 // Switches the multi-field pipeline on (allocating its grid arrays the first time) or off
 // after a change of the particles' contact groups or the materials' phases.
 emerge_status update_multi(emerge_sim *s) {
-    const int was = s->dcfg.multi;
+    const int was = s->dcfg.multi, was_fast = s->dcfg.mf_fast, was_fields = s->dcfg.mf_fields;
     if (multi_on(s) && !s->mfbuf.ptr) {
         const size_t cells = static_cast<size_t>(s->tpd) * s->tpd * TILE_CELLS;
+        const size_t flat = static_cast<size_t>(s->res) * s->res;
         const size_t bytes = MAX_MATERIALS * sizeof(uint32_t) +
                              cells * (3 * sizeof(float4) + 4 * sizeof(float2) + sizeof(float) + sizeof(int2) +
-                                      6 * sizeof(float) + sizeof(uint8_t)) +
-                             20 * 256;
+                                      6 * sizeof(float) + sizeof(uint8_t) +
+                                      3 * (sizeof(float4) + sizeof(float2))) +
+                             3 * flat * sizeof(int) + 30 * 256;
         CK(cudaMalloc(&s->mfbuf.ptr, bytes));
         s->mfbuf.bytes = bytes;
         CK(cudaMemsetAsync(s->mfbuf.ptr, 0, bytes, s->stream));
@@ -1072,11 +1107,19 @@ emerge_status update_multi(emerge_sim *s) {
         s->g.mx_p[0] = c.take<float>(cells);
         s->g.mx_p[1] = c.take<float>(cells);
         s->g.mx_sig = c.take<uint8_t>(cells);
+        for (int f = 0; f < 3; ++f) {
+            s->g.fa[f] = c.take<float4>(cells);
+            s->g.fs[f] = c.take<float2>(cells);
+        }
+        s->g.chead[0] = c.take<int>(flat);
+        s->g.chead[1] = c.take<int>(flat);
+        s->g.iface = c.take<int>(flat);
         emerge_status st = upload_phases(s);
         if (st != EMERGE_OK) return st;
     }
     refresh_dev_config(s);
-    if (s->dcfg.multi != was) {  // the pipelines keep different work pending between steps
+    if (s->dcfg.multi != was || s->dcfg.mf_fast != was_fast || s->dcfg.mf_fields != was_fields) {
+        // the pending scatter was made without (or with other) field sums and point lists
         s->graph_dirty = true;
         return invalidate_pending(s);
     }
@@ -1500,6 +1543,17 @@ emerge_status emerge_cuda_step(emerge_sim *s, uint32_t n_steps, emerge_step_timi
         if (timing) std::memset(timing, 0, sizeof(*timing));
         return EMERGE_OK;
     }
+    if (s->dcfg.mf_fast && (s->dcfg.mf_fields & 1)) {  // the contact lists' nodes, one per slot
+        float4 *before = s->g.cpts;
+        emerge_status st = ensure_points(s);
+        if (st != EMERGE_OK) return st;
+        s->g.cpts = s->det_points();
+        if (s->g.cpts != before) {
+            s->graph_dirty = true;
+            st = invalidate_pending(s);
+            if (st != EMERGE_OK) return st;
+        }
+    }
     for (uint32_t k = 0; k < n_steps; ++k) {
         emerge_status st = maybe_sort(s);
         if (st != EMERGE_OK) return st;
@@ -1553,6 +1607,8 @@ emerge_status emerge_cuda_step(emerge_sim *s, uint32_t n_steps, emerge_step_timi
 static emerge_status sync_state(emerge_sim *s) {
     CK(cudaMemcpyAsync(s->h_state, s->d_state, sizeof(StepState), cudaMemcpyDeviceToHost, s->stream));
     CK(cudaStreamSynchronize(s->stream));
+    if (s->h_state->error_flags & ERR_CONTACT_LIST)
+        return static_cast<emerge_status>(s->fail(EMERGE_ERR_CUDA, "contact point list walk cut short"));
     return EMERGE_OK;
 }
 
@@ -1632,6 +1688,7 @@ emerge_status emerge_cuda_set_option(emerge_sim *s, int option, int64_t value) {
             }
         }
         s->dcfg.precise_math = s->precise_opt >= 0 ? s->precise_opt : s->deterministic;
+        refresh_dev_config(s);  // the multi-field pipeline follows the mode
         s->graph_dirty = true;
         return EMERGE_OK;
     }

@@ -43,8 +43,26 @@ struct GridKernelArgs {
 // Grid::update_velocities (grid/mod.rs:264-291), boundaries (step.rs:150-152,
 // 334-344; forces/boundary/mod.rs:78-101), speed clamp (step.rs:155-165) for one cell of
 // an active tile, then the accumulators are zeroed for the next scatter.
+// The fast pipeline's field sum of one cell: A + dt S as {m, px, py, w} (the form the
+// reference-order scatter writes, w > 0 marking the field), the accumulators zeroed for the
+// next scatter.  Each scatter adds exactly 1 to the w lanes, so for the grip field
+// total_w - grip_w counts the other particles' scatters exactly, whatever the order of the
+// sums: w = 2 marks a cell that also holds other particles, w = 1 a grip-only cell, whose
+// rest mass the reference computes as exactly 0 (its grip and total sums run in the same
+// order), while total - grip here is rounding noise.
+__device__ __forceinline__ bool finalize_field(float4 *fa, float2 *fs, float4 *out, int ci, float dt,
+                                               float total_w) {
+    const float4 a = fa[ci];
+    if (!(a.w > 0.0f)) return false;
+    const float2 s = fs[ci];
+    out[ci] = make_float4(a.x, a.y + dt * s.x, a.z + dt * s.y, total_w > a.w + 0.5f ? 2.0f : 1.0f);
+    fa[ci] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    fs[ci] = v2(0.0f, 0.0f);
+    return true;
+}
+
 __device__ __forceinline__ void grid_update_cell(const GridView &g, const DevConfig &cfg, float dt,
-                                                 int tile, int local) {
+                                                 int tile, int local, uint32_t *contact_active) {
     const int ci = tile * TILE_CELLS + local;
     const int x = (tile / g.tpd) * TILE + (local >> 3);
     const int y = (tile % g.tpd) * TILE + (local & 7);
@@ -63,7 +81,17 @@ __device__ __forceinline__ void grid_update_cell(const GridView &g, const DevCon
         if (spd > vel_limit) mom = vmuls(mom, vel_limit / spd);
     }
     g.grid_v[ci] = mom;
-    if (cfg.multi) g.grid_m[ci] = m;  // the contact and mixture resolves read the total mass
+    if (cfg.multi) {
+        g.grid_m[ci] = m;  // the contact and mixture resolves read the total mass
+        if (cfg.mf_fast) {
+            if ((cfg.mf_fields & 1) && finalize_field(g.fa[0], g.fs[0], g.acc_grip, ci, dt, acc.w))
+                *contact_active = 1u;  // Grid::has_contact_activity
+            if (cfg.mf_fields & 2) {
+                finalize_field(g.fa[1], g.fs[1], g.acc_sol, ci, dt, 0.0f);
+                finalize_field(g.fa[2], g.fs[2], g.acc_flu, ci, dt, 0.0f);
+            }
+        }
+    }
     g.acc_a[ci] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
     g.acc_s[ci] = v2(0.0f, 0.0f);
 }
@@ -76,7 +104,7 @@ __global__ void __launch_bounds__(256) k_grid_update(GridKernelArgs a) {
     __syncthreads();
     if (tile >= a.n_tiles || !flag) return;
     if (local == 0) a.g.tile_flag[tile] = 0;
-    grid_update_cell(a.g, a.cfg, a.st->sub_dt, tile, local);
+    grid_update_cell(a.g, a.cfg, a.st->sub_dt, tile, local, &a.st->contact_active);
 }
 
 // Batched scenes: global tile t belongs to scene tile_scene[t] (local tile t - tile0).
@@ -97,7 +125,7 @@ __global__ void __launch_bounds__(256) k_grid_update_batch(BatchView b, int n_ti
     __syncthreads();
     if (!flag) return;
     if (local == 0) sd->g.tile_flag[tile] = 0;
-    grid_update_cell(sd->g, sd->cfg, sd->st->sub_dt, tile, local);
+    grid_update_cell(sd->g, sd->cfg, sd->st->sub_dt, tile, local, &sd->st->contact_active);
 }
 
 // ---------------------------------------------------------------- controller
@@ -136,6 +164,7 @@ __device__ __forceinline__ uint32_t substep_begin_state(StepState &s, const DevC
     s.min_mdt_bits[k1] = __float_as_uint(INFINITY);
     s.jproj_pending[k1] = 0ull;
     s.proj_changed[k1] = 0ull;
+    s.contact_active = 0u;
     s.acc_slot = k1;
     s.parity = k1;
     const float rem_after = rem - dt;

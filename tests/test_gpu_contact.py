@@ -4,15 +4,17 @@
 Scenes (tests/scenes.py): contact_scene, a grip block (contact_group 1) thrown onto a slab,
 with SimConfig.contact_friction or a DirectionalContactGrip; mixture_scene, water (fluid
 phase) resting on sand (solid phase) with mixture drag, with and without the Jacobi pressure
-projection.  Both run the reference-order pipeline on the device.
+projection.
 
 Reference order: after every frame the whole particle array against the oracle with
 correctly rounded math, bit for bit (x and v identical every frame); the contact scene is
 followed for 20 frames (contact starts after about 8), the mixture scene for 4 (its
 resolved phase velocities carry no boundary conditions in the reference, so the scene is
-not meant to run long).  Simulation (the
-default class, single-precision CUDA math): the same frames within the fast bar.
+not meant to run long).  Simulation (the default class) runs the fused pipeline (field sums
+reduced with the total, point clouds from per-base-cell lists): the same scenes within the
+fast bar.
 """
+import contextlib
 import ctypes
 
 import numpy as np
@@ -63,31 +65,66 @@ def test_mixture_frames_reference_order(cuda_lib, iterations):
     assert exact_until is None, (exact_until, stats)
 
 
-def test_contact_and_mixture_default_class(cuda_lib):
-    g = scenes.contact_scene(Simulation, grip=GRIPS["grip"])
-    c = scenes.contact_scene(OracleSimulation, grip=GRIPS["grip"])
-    print("contact, default class", run_frames(g, c, 12, "fast"))
-    g = scenes.mixture_scene(Simulation)
-    c = scenes.mixture_scene(OracleSimulation)
-    print("mixture, default class", run_frames(g, c, 3, "fast"))
+def run_frames_fast(g, c, frames, strict):
+    """The fast bar per particle for the first `strict` frames; after them the contact
+    decisions (directional friction, overlap correction) may differ with the summation
+    order, and the frames are judged on mass, momentum and region statistics."""
+    for k in range(frames):
+        g.step()
+        c.step()
+        assert g.last_substeps() == c.last_substeps(), k
+        pg, pc = g.particles(), c.particles()
+        if k < strict:
+            compare_particles(pg, pc, **tol("fast"))
+            continue
+        assert pg["mass"].sum(dtype=np.float64) == pc["mass"].sum(dtype=np.float64)
+        m = pc["mass"].astype(np.float64)
+        p_abs = (m * np.linalg.norm(pc["v"].astype(np.float64), axis=1)).sum()
+        dp = (m[:, None] * pg["v"]).sum(0) - (m[:, None] * pc["v"]).sum(0)
+        assert np.linalg.norm(dp) <= 1e-4 * p_abs, k
+    for center, r in (((48.0, 48.0), 96.0), ((42.0, 20.0), 12.0)):  # the 96-cell scene, its contact zone
+        sg, sc = g.region_state(center, r), c.region_state(center, r)
+        assert sg.count == sc.count
+        for key in ("avg_speed", "avg_det_f", "avg_density"):
+            assert getattr(sg, key) == pytest.approx(getattr(sc, key), rel=1e-3, abs=1e-6), key
 
 
-def test_contact_groups_follow_each_upload(cuda_lib):
+@pytest.mark.parametrize("which", sorted(GRIPS))
+def test_contact_fast_pipeline(cuda_lib, which):
+    """Simulation (the default class) runs multi-field scenes on the fused pipeline: field
+    sums reduced with the total, point clouds from per-base-cell lists."""
+    g = scenes.contact_scene(Simulation, grip=GRIPS[which])
+    c = scenes.contact_scene(OracleSimulation, grip=GRIPS[which])
+    run_frames_fast(g, c, 12, strict=9)
+
+
+@pytest.mark.parametrize("iterations", [0, 2])
+def test_mixture_fast_pipeline(cuda_lib, iterations):
+    g = scenes.mixture_scene(Simulation, iterations=iterations)
+    c = scenes.mixture_scene(OracleSimulation, iterations=iterations)
+    print("mixture, fast pipeline 3 frames", run_frames(g, c, 3, "fast"))
+
+
+@pytest.mark.parametrize("mode", ["reference_order", "fast"])
+def test_contact_groups_follow_each_upload(cuda_lib, mode):
     """A write-back that sets contact groups switches the contact fields on; one that clears
     them switches them off again (particles_mut() edits, lifecycle.rs:233)."""
-    g = scenes.quickstart(DeterministicSimulation)
-    with correctly_rounded_math():
+    exact = mode == "reference_order"
+    g = scenes.quickstart(DeterministicSimulation if exact else Simulation)
+    with correctly_rounded_math() if exact else contextlib.nullcontext():
         c = scenes.quickstart(OracleSimulation)
         p = g.particles()
         p["contact_group"][p["x"][:, 1] > np.median(p["x"][:, 1])] = 2
         for sim in (g, c):
             sim.set_particles(p)
-        assert run_frames(g, c, 2)[0] is None
+        first_inexact, _ = run_frames(g, c, 2, mode)
+        assert first_inexact is None or not exact
         q = g.particles()
         q["contact_group"][:] = 0
         for sim in (g, c):
             sim.set_particles(q)
-        assert run_frames(g, c, 2)[0] is None
+        first_inexact, _ = run_frames(g, c, 2, mode)
+        assert first_inexact is None or not exact
 
 
 def test_grip_and_phase_arguments_are_checked(cuda_lib):
