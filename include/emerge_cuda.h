@@ -276,9 +276,10 @@ emerge_status emerge_cuda_set_force_fields(emerge_sim *sim, const emerge_force_f
 
 /* Multi-field contact (spacetime/grid/contact.rs) runs when some particle has
  * contact_group != 0, the two-phase mixture coupling (spacetime/grid/mixture.rs) when some
- * material slot has a phase; such scenes step through the reference-order pipeline
- * (EMERGE_OPT_DETERMINISTIC's sums), whose cell-sorted scatter records give each contact
- * cell its point cloud in particle index order.  After the grid update (step.rs:166-197)
+ * material slot has a phase.  With EMERGE_OPT_DETERMINISTIC the cell-sorted scatter records
+ * give each contact cell its point cloud in particle index order (the reference's sums, bit
+ * for bit); otherwise the fused step sums the fields with the total and gathers each
+ * contact cell's points from per-cell particle lists.  After the grid update (step.rs:166-197)
  * every grip cell gets a logistic-regression interface normal (grid/contact_normal.rs) or
  * the grip-mass gradient, Coulomb friction or the directional grip, and the overlap
  * correction; every mixture cell the implicit Darcy drag between the phases and, with
