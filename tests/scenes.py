@@ -335,12 +335,16 @@ def sleep_slab(sim_cls, grid_res=1024, slab=512, seed=21, threshold=0.05, **sim_
     return sim
 
 
-def contact_scene(sim_cls, grid_res=96, seed=13, dt=0.05, friction=0.5, grip=None, **sim_kw):
+def contact_scene(sim_cls, grid_res=96, seed=13, dt=0.05, friction=0.5, grip=None, asflip=0.0,
+                  sleep=0.0, **sim_kw):
     """Multi-field contact: a NeoHookean (400, 200) slab on the floor (contact group 0) and a
     block of the same material with contact_group 1 falling onto it at (1.5, -3), 4 ppc,
-    SimConfig.contact_friction `friction`, optional DirectionalContactGrip `grip`."""
+    SimConfig.contact_friction `friction`, optional DirectionalContactGrip `grip`,
+    SimConfig.asflip_blend `asflip`, SimConfig.sleep_threshold `sleep`."""
     cfg = SimConfig.standard(grid_res, dt, (0.0, -1.0))
     cfg.contact_friction = friction
+    cfg.asflip_blend = asflip
+    cfg.sleep_threshold = sleep
     t = cfg.boundary_thickness
     sim = sim_cls.empty(cfg, **sim_kw).with_default_material(NeoHookeanMaterial.new(400.0, 200.0))
     if grip is not None:

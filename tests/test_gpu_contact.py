@@ -105,6 +105,35 @@ def test_mixture_fast_pipeline(cuda_lib, iterations):
     print("mixture, fast pipeline 3 frames", run_frames(g, c, 3, "fast"))
 
 
+def combined_scene(sim_cls):
+    """The contact scene with ASFLIP, a linear drag field and the sleep partition on."""
+    from emerge_engine_b200 import LinearDragField
+    sim = scenes.contact_scene(sim_cls, grip=GRIPS["grip"], asflip=0.3, sleep=0.02)
+    sim.add_force_field(LinearDragField.new((0.5, 0.0), 0.05, LinearDragField.ALL_MATERIALS))
+    return sim
+
+
+def test_contact_with_fields_asflip_and_sleep(cuda_lib):
+    """Contact together with the other extras: bit for bit in reference order, within the fast
+    bar on the fused pipeline (which steps it with the host-driven substep loop, as every
+    scene with a sleep partition)."""
+    g = combined_scene(DeterministicSimulation)
+    with correctly_rounded_math():
+        c = combined_scene(OracleSimulation)
+        exact_until, stats = run_frames(g, c, 10)
+    assert exact_until is None, (exact_until, stats)
+    assert g.active_count() == c.active_count()
+    g = combined_scene(Simulation)
+    c = combined_scene(OracleSimulation)
+    for k in range(8):
+        g.step()
+        c.step()
+        assert g.last_substeps() == c.last_substeps(), k
+        assert abs(g.active_count() - c.active_count()) <= 2, k
+    if g.active_count() == c.active_count():
+        compare_particles(g.particles(), c.particles(), **tol("fast"))
+
+
 @pytest.mark.parametrize("mode", ["reference_order", "fast"])
 def test_contact_groups_follow_each_upload(cuda_lib, mode):
     """A write-back that sets contact groups switches the contact fields on; one that clears
