@@ -184,7 +184,7 @@ struct emerge_sim {
     bool pending_valid = false;  // the next substep's P2G (+density) is already on the grid
     int use_graph = 1;
     int use_window = 0;
-    int64_t sort_interval = 8;   // re-sort every N steps; 0 = keep the first sort
+    int64_t sort_interval = 16;  // re-sort every N steps; 0 = keep the first sort
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t graph_exec = nullptr;
     bool graph_dirty = true;

@@ -365,7 +365,7 @@ emerge_status emerge_cuda_region_state(emerge_sim *sim, float cx, float cy, floa
  *   EMERGE_OPT_USE_GRAPH       1 = capture each step in a CUDA graph with a device-side
  *                              substep loop (default), 0 = host-driven substep loop with
  *                              per-phase event timing.
- *   EMERGE_OPT_SORT_INTERVAL   re-sort particles by tile every N steps (default 8;
+ *   EMERGE_OPT_SORT_INTERVAL   re-sort particles by tile every N steps (default 16;
  *                              0 = only before the first step after particles are added;
  *                              see emerge_cuda_sort_now).
  *   EMERGE_OPT_P2G_AGGREGATE   1 = P2G contributions of lanes sharing a base cell are
