@@ -446,10 +446,14 @@ __device__ __forceinline__ void mark_tiles(const GridView &g, int bx, int by) {
 }
 
 // One lane's 3 x 3 reductions (no aggregation) into the accumulators A (mass + momentum)
-// and S (stress).  CHECK skips cells outside the domain.
+// and S (stress), and the same values into up to two more pairs (the multi-field sums; null
+// when unused): one pass over the stencil, so the extra targets cost reductions only.
+// CHECK skips cells outside the domain.
 template <int SC, bool CHECK>
 __device__ __forceinline__ void scatter_cells_to(const GridView &g, const ScatterPlan &pl,
-                                                 bool do_ma, bool do_s, float4 *A, float2 *S) {
+                                                 bool do_ma, bool do_s, float4 *A, float2 *S,
+                                                 float4 *A2 = nullptr, float2 *S2 = nullptr,
+                                                 float4 *A3 = nullptr, float2 *S3 = nullptr) {
     const QW &w = pl.w;
     int yp[3];
 #pragma unroll
@@ -466,9 +470,18 @@ __device__ __forceinline__ void scatter_cells_to(const GridView &g, const Scatte
             const float wt = w.wx[gx] * w.wy[gy];
             const int ci = xp + yp[gy];
             // the fourth lane counts scatters: a cell with w > 0 is in the reference's dirty set
-            if (SC == SC_MA || (SC == SC_BOTH && do_ma))
-                red_add_v4(&A[ci], wm * w.wy[gy], wt * t.x, wt * t.y, 1.0f);
-            if (SC == SC_S || (SC == SC_BOTH && do_s)) red_add_v2(&S[ci], wt * t.z, wt * t.w);
+            if (SC == SC_MA || (SC == SC_BOTH && do_ma)) {
+                const float m = wm * w.wy[gy], ax = wt * t.x, ay = wt * t.y;
+                red_add_v4(&A[ci], m, ax, ay, 1.0f);
+                if (A2) red_add_v4(&A2[ci], m, ax, ay, 1.0f);
+                if (A3) red_add_v4(&A3[ci], m, ax, ay, 1.0f);
+            }
+            if (SC == SC_S || (SC == SC_BOTH && do_s)) {
+                const float sx = wt * t.z, sy = wt * t.w;
+                red_add_v2(&S[ci], sx, sy);
+                if (S2) red_add_v2(&S2[ci], sx, sy);
+                if (S3) red_add_v2(&S3[ci], sx, sy);
+            }
         }
     }
 }
@@ -544,22 +557,35 @@ __device__ __forceinline__ void scatter_particle(const GridView &g, const Payloa
     if (active) pl = make_plan<SC>(p);
     if (aggregate) {
         scatter_cells_aggregated<SC>(g, pl, active, p.do_ma, p.do_s);
-    } else {
         if (!active) return;
-        const QW &w = pl.w;
-        if (stencil_inside(w.bx, w.by, g.res))
-            scatter_cells<SC, false>(g, pl, p.do_ma, p.do_s);
-        else
-            scatter_cells<SC, true>(g, pl, p.do_ma, p.do_s);
-    }
-    if (active) {
-        mark_tiles(g, pl.w.bx, pl.w.by);
         // the multi-field sums of the fast pipeline (p2g.rs:60-66): the same contributions
         for (uint32_t f = p.fields; f != 0u; f &= f - 1u) {
             const int k = __ffs(f) - 1;
             scatter_cells_to<SC, true>(g, pl, p.do_ma, p.do_s, g.fa[k], g.fs[k]);
         }
+    } else {
+        if (!active) return;
+        // up to two multi-field sums (grip, and a mixture phase) take the same contributions
+        float4 *A2 = nullptr, *A3 = nullptr;
+        float2 *S2 = nullptr, *S3 = nullptr;
+        if (p.fields) {
+            const int k2 = __ffs(p.fields) - 1;
+            A2 = g.fa[k2];
+            S2 = g.fs[k2];
+            const uint32_t rest = p.fields & (p.fields - 1u);
+            if (rest) {
+                const int k3 = __ffs(rest) - 1;
+                A3 = g.fa[k3];
+                S3 = g.fs[k3];
+            }
+        }
+        const QW &w = pl.w;
+        if (stencil_inside(w.bx, w.by, g.res))
+            scatter_cells_to<SC, false>(g, pl, p.do_ma, p.do_s, g.acc_a, g.acc_s, A2, S2, A3, S3);
+        else
+            scatter_cells_to<SC, true>(g, pl, p.do_ma, p.do_s, g.acc_a, g.acc_s, A2, S2, A3, S3);
     }
+    mark_tiles(g, pl.w.bx, pl.w.by);
 }
 
 // The multi-field sums a particle adds to on the fast pipeline: the grip field for a
