@@ -78,9 +78,19 @@ __global__ void __launch_bounds__(IFACE_WARPS * 32) k_contact_iface(GridView g, 
 
 }  // namespace
 
+// The interface kernel's grid: four CTAs per SM of the current device (its warps stride over
+// the interface cells, whose count is known only on the device).
+static int iface_blocks() {
+    int dev = 0, sms = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms <= 0)
+        sms = 148;
+    return 4 * sms;
+}
+
 void launch_contact_resolve_lists(const StepLaunch &L) {
     k_contact_cells<<<grid_blocks(L.g), MF_THREADS, 0, L.stream>>>(L.g, L.st);
-    k_contact_iface<<<148 * 4, IFACE_WARPS * 32, 0, L.stream>>>(L.g, L.cfg, L.st, L.n);
+    k_contact_iface<<<iface_blocks(), IFACE_WARPS * 32, 0, L.stream>>>(L.g, L.cfg, L.st, L.n);
 }
 
 }  // namespace emerge
