@@ -226,6 +226,11 @@ __device__ __forceinline__ int g2p_particle(const GridView &g, const DevConfig &
                                             PState &p, int sel = 0) {
     QW w = quadratic_weights(p.x);
     const bool inside = stencil_inside(w.bx, w.by, g.res);
+    // ASFLIP's FLIP residual (g2p.rs:281-290), gathered first so that only the residual is
+    // live across the G2P sums
+    float2 diff_vel = v2(0.0f, 0.0f);
+    if constexpr (EXTRAS)
+        if (cfg.asflip > 0.0f) diff_vel = vsub(p.v, gather_pre_force<FAST>(g, w, inside));
     float2 new_v = v2(0.0f, 0.0f);
     M2 b = mzero();
     if constexpr (FAST) {
@@ -307,8 +312,6 @@ __device__ __forceinline__ int g2p_particle(const GridView &g, const DevConfig &
     float2 v_store = new_v, v_pos = new_v;
     if constexpr (EXTRAS) {
         if (cfg.asflip > 0.0f) {  // g2p.rs:281-296
-            const float2 old_v = gather_pre_force<FAST>(g, w, inside);
-            const float2 diff_vel = vsub(p.v, old_v);
             const float trace_b = b.xa.x + b.ya.y;
             const float gamma = trace_b < 0.0f ? 0.0f : 1.0f;
             v_store = vadd(new_v, svmul(cfg.asflip, diff_vel));
