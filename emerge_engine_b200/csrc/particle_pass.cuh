@@ -894,10 +894,6 @@ __device__ __forceinline__ void particle_pass(const ParticleKernelArgs &a) {
     // barrier that publishes the materials, so their latencies overlap.
     const uint32_t acc_slot = st->acc_slot;
     const float dt = st->sub_dt;
-    // The previous pass counted, in the other slot, the particles whose projection for
-    // this substep changed their stored state; with none, the stored state is its own
-    // projection and the recompute below is skipped.
-    const bool reproject = a.project_in && cfg.project && st->proj_changed[acc_slot ^ 1u] != 0ull;
     PState p;
     if (valid) p = load_state(a.P, i, a.lf);
     __syncthreads();
@@ -924,7 +920,7 @@ __device__ __forceinline__ void particle_pass(const ParticleKernelArgs &a) {
             // projection S'(k) (counted when it was first computed).  A particle woken after
             // this substep's P2G was neither projected nor given a density this substep.
             const bool woken = (zb & ZB_WOKEN) != 0u;
-            if (reproject && !woken) project_state(cfg, p);
+            if (a.project_in && cfg.project && !woken) project_state(cfg, p);
             if (density_mode && a.project_in && !woken) {
                 float d = a.P.rho_dp[i];
                 if (d > F32_EPS) {
