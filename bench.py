@@ -73,8 +73,8 @@ WORKLOADS = {
     "contact_1m": dict(builder="contact_slab", kwargs=dict(grid_res=1024),
                        desc="multi-field contact: NeoHookean 896 x 192-cell slab on the floor and a "
                             "320 x 256-cell grip block (contact_group 1) on it thrown at (1.5, -3), "
-                            "4 ppc, DirectionalContactGrip(0.1, 0.9, (1, 0)); reference-order "
-                            "pipeline (cell-sorted scatters, LR contact normals)",
+                            "4 ppc, DirectionalContactGrip(0.1, 0.9, (1, 0)); fused pipeline (field "
+                            "sums with the total, per-base-cell point lists, LR contact normals)",
                        material="NeoHookean-contact", grid_res=1024),
     "mixture_1m": dict(builder="mixture_overlap", kwargs=dict(grid_res=1024, side=362, iterations=0),
                        desc="two-phase mixture without gravity: DruckerPrager sand (solid phase) and "
