@@ -64,7 +64,7 @@ __global__ void k_project(DevParticles P, int n, DevConfig cfg, StepState *st) {
 __global__ void k_det_records(DevParticles P, int n, const MatP *mats, int n_mats, DevConfig cfg,
                               const StepState *st, int mode, uint32_t invalid_key, uint32_t *keys,
                               uint32_t *vals, float4 *payload, int filter, float lox, float loy,
-                              float hix, float hiy, int pfilter, float4 *points) {
+                              float hix, float hiy, int write_keys, uint8_t *fmask, float4 *points) {
     int s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= n) return;
     const uint32_t hi = P.slot_to_index[s];
@@ -75,14 +75,14 @@ __global__ void k_det_records(DevParticles P, int n, const MatP *mats, int n_mat
     // the active zone take no part
     bool skip = (filter && (p.x.x < lox || p.x.y < loy || p.x.x > hix || p.x.y > hiy)) ||
                 (cfg.zones && (P.sleeping[s] & ZB_OUT));
-    // a field's scatter takes its particles only (p2g.rs:60-66): 1 grip (contact_group != 0),
-    // 2 / 3 the solid / fluid mixture phase
-    const uint32_t cgroup = (pfilter != 0 || points) ? P.contact[s] : 0u;
-    if (pfilter == 1) skip = skip || cgroup == 0u;
-    if (pfilter >= 2) {
+    // the fields the particle's contributions also go to (p2g.rs:60-66): bit 0 grip
+    // (contact_group != 0), bit 1 / 2 the solid / fluid mixture phase
+    const uint32_t cgroup = (fmask || points) ? P.contact[s] : 0u;
+    uint8_t fbits = 0;
+    if (fmask) {
         const uint32_t mat = P.mat[s];
         const uint32_t ph = cfg.mat_phase[mat < static_cast<uint32_t>(n_mats) ? mat : 0u];
-        skip = skip || ph != static_cast<uint32_t>(pfilter - 1);
+        fbits = static_cast<uint8_t>((cgroup != 0u ? 1u : 0u) | (ph == 1u ? 2u : 0u) | (ph == 2u ? 4u : 0u));
     }
     float2 v = v2(0.0f, 0.0f);
     M2 c = mzero(), stress = mzero();
@@ -115,13 +115,16 @@ __global__ void k_det_records(DevParticles P, int n, const MatP *mats, int n_mat
             const uint32_t r = hi * 9u + static_cast<uint32_t>(gx * 3 + gy);
             float weight = w.wx[gx] * w.wy[gy];
             int cx = w.bx + gx - 1, cy = w.by + gy - 1;
-            vals[r] = r;
+            // write_keys = 0: the keys of an earlier call at the same positions are already sorted
+            if (write_keys) vals[r] = r;
             if (skip || !in_domain(cx, cy, cfg.res)) {
-                keys[r] = invalid_key;
+                if (write_keys) keys[r] = invalid_key;
                 payload[r] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
                 continue;
             }
-            keys[r] = static_cast<uint32_t>(cx) * static_cast<uint32_t>(cfg.res) + static_cast<uint32_t>(cy);
+            if (write_keys)
+                keys[r] = static_cast<uint32_t>(cx) * static_cast<uint32_t>(cfg.res) + static_cast<uint32_t>(cy);
+            if (fmask) fmask[r] = fbits;
             float2 mom = v2(0.0f, 0.0f);
             if (mode == 1) {
                 float2 cell_dist = vadd(vsub(v2(static_cast<float>(cx), static_cast<float>(cy)), p.x),
@@ -137,8 +140,7 @@ __global__ void k_det_records(DevParticles P, int n, const MatP *mats, int n_mat
 
 // Sequential per-cell sums over the cell-sorted records (Grid::accumulate order).
 __global__ void k_segsum(const uint32_t *keys, const uint32_t *vals, const float4 *payload, int n_rec,
-                         uint32_t invalid_key, GridView g, int mass_only, float4 *target,
-                         int2 *range, uint32_t *any) {
+                         uint32_t invalid_key, GridView g, int mass_only, int2 *range) {
     int j = blockIdx.x * blockDim.x + threadIdx.x;
     if (j >= n_rec) return;
     uint32_t key = keys[j];
@@ -157,11 +159,6 @@ __global__ void k_segsum(const uint32_t *keys, const uint32_t *vals, const float
     int cy = static_cast<int>(key % static_cast<uint32_t>(g.res));
     int ci = cell_index(cx, cy, g.tpd);
     if (range) range[ci] = make_int2(j, k);  // the cell's records, in particle index order
-    if (target) {  // a contact or mixture field
-        target[ci] = make_float4(m, px, py, 1.0f);
-        if (any) *any = 1u;
-        return;
-    }
     if (mass_only) {
         g.acc_a[ci].x = m;
     } else {
@@ -171,25 +168,70 @@ __global__ void k_segsum(const uint32_t *keys, const uint32_t *vals, const float
     g.tile_flag[t] = 1;
 }
 
+// One field's sums over the same sorted records (add_grip_mass_momentum contact.rs:41-72,
+// add_mixture_mass_momentum mixture.rs:20-58): per cell, the records of the field's particles
+// (fmask & fbit) in particle index order, the first set and the rest added, as the reference
+// does in its own scatter loop.
+__global__ void k_segsum_field(const uint32_t *keys, const uint32_t *vals, const float4 *payload,
+                               const uint8_t *fmask, uint32_t fbit, int n_rec, uint32_t invalid_key,
+                               GridView g, float4 *target, uint32_t *any) {
+    int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= n_rec) return;
+    uint32_t key = keys[j];
+    if (key == invalid_key) return;
+    if (j > 0 && keys[j - 1] == key) return;  // not the head of its cell
+    bool found = false;
+    float m = 0.0f, px = 0.0f, py = 0.0f;
+    for (int k = j; k < n_rec && keys[k] == key; ++k) {
+        const uint32_t r = vals[k];
+        if (!(fmask[r] & fbit)) continue;
+        const float4 q = payload[r];
+        if (!found) {
+            m = q.x;
+            px = q.y;
+            py = q.z;
+            found = true;
+        } else {
+            m += q.x;
+            px += q.y;
+            py += q.z;
+        }
+    }
+    if (!found) return;
+    const int cx = static_cast<int>(key / static_cast<uint32_t>(g.res));
+    const int cy = static_cast<int>(key % static_cast<uint32_t>(g.res));
+    target[cell_index(cx, cy, g.tpd)] = make_float4(m, px, py, 1.0f);
+    if (any) *any = 1u;
+}
+
 void launch_project(const StepLaunch &L) {
     if (L.n) k_project<<<(L.n + 255) / 256, 256, 0, L.stream>>>(L.P, L.n, L.cfg, L.st);
 }
 
 void launch_det_records(const StepLaunch &L, int mode, uint32_t invalid_key, uint32_t *keys,
                         uint32_t *vals, float4 *payload, int filter, float lox, float loy, float hix,
-                        float hiy, int pfilter, float4 *points) {
+                        float hiy, int write_keys, uint8_t *fmask, float4 *points) {
     if (L.n)
         k_det_records<<<(L.n + 127) / 128, 128, 0, L.stream>>>(L.P, L.n, L.mats, L.n_mats, L.cfg, L.st,
                                                                mode, invalid_key, keys, vals, payload,
-                                                               filter, lox, loy, hix, hiy, pfilter, points);
+                                                               filter, lox, loy, hix, hiy, write_keys,
+                                                               fmask, points);
+}
+
+void launch_segsum_field(const uint32_t *keys, const uint32_t *vals, const float4 *payload,
+                         const uint8_t *fmask, uint32_t fbit, int n_rec, uint32_t invalid_key,
+                         const GridView &g, float4 *target, uint32_t *any, cudaStream_t stream) {
+    if (n_rec)
+        k_segsum_field<<<(n_rec + 255) / 256, 256, 0, stream>>>(keys, vals, payload, fmask, fbit, n_rec,
+                                                                invalid_key, g, target, any);
 }
 
 void launch_segsum(const uint32_t *keys, const uint32_t *vals, const float4 *payload, int n_rec,
                    uint32_t invalid_key, const GridView &g, int mass_only, cudaStream_t stream,
-                   float4 *target, int2 *range, uint32_t *any) {
+                   int2 *range) {
     if (n_rec)
         k_segsum<<<(n_rec + 255) / 256, 256, 0, stream>>>(keys, vals, payload, n_rec, invalid_key, g,
-                                                          mass_only, target, range, any);
+                                                          mass_only, range);
 }
 
 }  // namespace emerge

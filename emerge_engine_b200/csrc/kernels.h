@@ -63,17 +63,21 @@ void launch_density_pass_batch(const DevParticles &P, const BatchView &b, int n_
 
 // det_kernels.cu (reference-order mode)
 void launch_project(const StepLaunch &L);
-// pfilter: 0 every particle, 1 grip particles, 2 / 3 the solid / fluid mixture phase;
-// points (optional): each record's (x, y, contact label) for the contact point cloud
+// write_keys = 0 keeps the keys and values of an earlier call at the same positions (already
+// sorted); fmask (optional): each record's fields (bit 0 grip, 1 solid, 2 fluid); points
+// (optional): each record's (x, y, contact label) for the contact point cloud
 void launch_det_records(const StepLaunch &L, int mode, uint32_t invalid_key, uint32_t *keys,
                         uint32_t *vals, float4 *payload, int filter = 0, float lox = 0.f,
-                        float loy = 0.f, float hix = 0.f, float hiy = 0.f, int pfilter = 0,
-                        float4 *points = nullptr);
-// target (optional): sums go to that field instead of acc_a (and `any` is set); range
-// (optional): each cell's record range
+                        float loy = 0.f, float hix = 0.f, float hiy = 0.f, int write_keys = 1,
+                        uint8_t *fmask = nullptr, float4 *points = nullptr);
+// one field's per-cell sums over the sorted records of its particles (fmask & fbit)
+void launch_segsum_field(const uint32_t *keys, const uint32_t *vals, const float4 *payload,
+                         const uint8_t *fmask, uint32_t fbit, int n_rec, uint32_t invalid_key,
+                         const GridView &g, float4 *target, uint32_t *any, cudaStream_t stream);
+// range (optional): each cell's record range
 void launch_segsum(const uint32_t *keys, const uint32_t *vals, const float4 *payload, int n_rec,
                    uint32_t invalid_key, const GridView &g, int mass_only, cudaStream_t stream,
-                   float4 *target = nullptr, int2 *range = nullptr, uint32_t *any = nullptr);
+                   int2 *range = nullptr);
 // multi-field contact and mixture coupling after the grid update (multifield.cu)
 void launch_contact_resolve(const StepLaunch &L, const uint32_t *vals, const float4 *points);
 void launch_mixture_resolve(const StepLaunch &L);

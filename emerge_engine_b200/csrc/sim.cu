@@ -178,7 +178,9 @@ struct emerge_sim {
     Buffer detbuf;
     SortScratch det_sort;
     float4 *det_payload = nullptr;
+    uint8_t *det_fmask = nullptr;   // each record's fields (multi-field scenes)
     size_t det_cap = 0;
+    int det_sorted = 0;             // which key / value buffer holds the last sort's result
 
     // step pipeline
     bool pending_valid = false;  // the next substep's P2G (+density) is already on the grid
@@ -721,13 +723,15 @@ emerge_status ensure_det_scratch(emerge_sim *s) {
     size_t need = 9 * (s->cap > 0 ? s->cap : 1);
     if (s->det_cap >= need) return EMERGE_OK;
     s->detbuf.reset();
-    size_t bytes = sort_scratch_bytes(need) + need * sizeof(float4) + 512;
+    size_t bytes = sort_scratch_bytes(need) + need * (sizeof(float4) + sizeof(uint8_t)) + 1024;
     CK(cudaMalloc(&s->detbuf.ptr, bytes));
     s->detbuf.bytes = bytes;
     sort_scratch_bind(s->det_sort, s->detbuf.ptr, need);
     uintptr_t p = reinterpret_cast<uintptr_t>(s->detbuf.ptr) + sort_scratch_bytes(need);
     p = (p + 255) & ~static_cast<uintptr_t>(255);
     s->det_payload = reinterpret_cast<float4 *>(p);
+    p = (p + need * sizeof(float4) + 255) & ~static_cast<uintptr_t>(255);
+    s->det_fmask = reinterpret_cast<uint8_t *>(p);
     s->det_cap = need;
     return EMERGE_OK;
 }
@@ -744,25 +748,30 @@ int det_key_bits(const emerge_sim *s) {
 }
 
 // Records -> stable sort by cell -> sequential per-cell sums (see det_kernels.cu).
-// A field scatter (pfilter 1 grip, 2 / 3 mixture phases) sums its particles into `target`
-// and sets `any`.  The full scatter can also write the contact point cloud (`points`), each
-// cell's record range and, in `sorted_vals`, the cell-sorted record order they index.
+// reuse_sort: the positions are those of the previous call, whose sorted keys stand (only
+// the payload is written).  The full scatter can also write each record's fields (`fmask`,
+// for det_field_sum), the contact point cloud (`points`), each cell's record range and, in
+// `sorted_vals`, the cell-sorted record order they index.
 emerge_status det_scatter(emerge_sim *s, const StepLaunch &L, int mode, int filter, float lox,
-                          float loy, float hix, float hiy, int pfilter = 0, float4 *target = nullptr,
-                          uint32_t *any = nullptr, float4 *points = nullptr, int2 *range = nullptr,
+                          float loy, float hix, float hiy, bool reuse_sort = false,
+                          uint8_t *fmask = nullptr, float4 *points = nullptr, int2 *range = nullptr,
                           const uint32_t **sorted_vals = nullptr) {
     emerge_status st = ensure_det_scratch(s);
     if (st != EMERGE_OK) return st;
     const uint32_t inv = det_invalid_key(s);
     const int n_rec = 9 * L.n;
     launch_det_records(L, mode, inv, s->det_sort.keys[0], s->det_sort.vals[0], s->det_payload, filter,
-                       lox, loy, hix, hiy, pfilter, points);
+                       lox, loy, hix, hiy, reuse_sort ? 0 : 1, fmask, points);
     int bits = det_key_bits(s);
-    int r = radix_sort_pairs(s->det_sort, n_rec, bits, s->stream);
+    if (!reuse_sort) {
+        s->det_sorted = radix_sort_pairs(s->det_sort, n_rec, bits, s->stream);
+        s->host_launches += 5 * ((bits + 7) / 8);
+    }
+    const int r = s->det_sorted;
     launch_segsum(s->det_sort.keys[r], s->det_sort.vals[r], s->det_payload, n_rec, inv, s->g,
-                  mode == 0 ? 1 : 0, s->stream, target, range, any);
+                  mode == 0 ? 1 : 0, s->stream, range);
     if (sorted_vals) *sorted_vals = s->det_sort.vals[r];
-    s->host_launches += 2 + 5 * ((bits + 7) / 8);
+    s->host_launches += 2;
     CK(cudaGetLastError());
     return EMERGE_OK;
 }
@@ -840,21 +849,26 @@ emerge_status run_det_step(emerge_sim *s, bool timed) {
             if (st != EMERGE_OK) return st;
         }
         CK(cudaEventRecord(s->ev[4], s->stream));
-        // the grip and mixture-phase fields take the same P2G contributions as the total
-        // (p2g.rs:60-66), summed per field in particle index order
-        if (contact) {
-            st = det_scatter(s, L, 1, 0, 0, 0, 0, 0, 1, s->g.acc_grip, &s->d_state->contact_active);
-            if (st != EMERGE_OK) return st;
-        }
-        if (mixture) {
-            st = det_scatter(s, L, 1, 0, 0, 0, 0, 0, 2, s->g.acc_sol);
-            if (st == EMERGE_OK) st = det_scatter(s, L, 1, 0, 0, 0, 0, 0, 3, s->g.acc_flu);
-            if (st != EMERGE_OK) return st;
-        }
+        // P2G at the positions the density scatter sorted, when there was one; the grip and
+        // mixture-phase fields take the same contributions as the total (p2g.rs:60-66),
+        // summed per field over the same sorted records in particle index order
         const uint32_t *sorted_vals = nullptr;
-        st = det_scatter(s, L, 1, 0, 0, 0, 0, 0, 0, nullptr, nullptr, contact ? s->det_points() : nullptr,
-                         contact ? s->g.rec_range : nullptr, &sorted_vals);
+        st = det_scatter(s, L, 1, 0, 0, 0, 0, 0, L.density_mode != 0, (contact || mixture) ? s->det_fmask : nullptr,
+                         contact ? s->det_points() : nullptr, contact ? s->g.rec_range : nullptr, &sorted_vals);
         if (st != EMERGE_OK) return st;
+        const int r = s->det_sorted;
+        const uint32_t inv = det_invalid_key(s);
+        auto field_sum = [&](uint32_t bit, float4 *target, uint32_t *any) {
+            launch_segsum_field(s->det_sort.keys[r], s->det_sort.vals[r], s->det_payload, s->det_fmask, bit,
+                                9 * L.n, inv, s->g, target, any, s->stream);
+            s->host_launches += 1;
+        };
+        if (contact) field_sum(1u, s->g.acc_grip, &s->d_state->contact_active);
+        if (mixture) {
+            field_sum(2u, s->g.acc_sol, nullptr);
+            field_sum(4u, s->g.acc_flu, nullptr);
+        }
+        CK(cudaGetLastError());
         if (L.cfg.zones) {  // wake after this substep's P2G (step.rs:107-131)
             launch_wake(L, 0);
             s->host_launches += 1;
