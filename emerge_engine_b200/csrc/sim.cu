@@ -125,6 +125,12 @@ struct emerge_sim {
     cudaStream_t copy_stream = nullptr;
     cudaEvent_t ev_ready = nullptr, ev_gathered = nullptr;
     Buffer staging_rb;
+    // uploads: their own AoS staging and stream, so a write-back's host-to-device copy
+    // overlaps the work already queued (the step before it)
+    cudaStream_t up_stream = nullptr;
+    cudaEvent_t ev_up_done = nullptr, ev_up_free = nullptr;
+    Buffer staging_up;
+    bool up_used = false;
     uint32_t next_tag = 1;
     LoadFlagsHost lf;
     std::vector<uint8_t> host_pinned_flag;  // not used for stepping; kept for add/write scans
@@ -1270,6 +1276,7 @@ emerge_status emerge_cuda_destroy(emerge_sim *s) {
     if (!s) return EMERGE_OK;
     if (s->stream) cudaStreamSynchronize(s->stream);
     if (s->copy_stream) cudaStreamSynchronize(s->copy_stream);
+    if (s->up_stream) cudaStreamSynchronize(s->up_stream);
     destroy_graph(s);
     for (auto &ev : s->ev)
         if (ev) cudaEventDestroy(ev);
@@ -1280,6 +1287,10 @@ emerge_status emerge_cuda_destroy(emerge_sim *s) {
     s->pbuf.reset();
     s->staging.reset();
     s->staging_rb.reset();
+    s->staging_up.reset();
+    if (s->ev_up_done) cudaEventDestroy(s->ev_up_done);
+    if (s->ev_up_free) cudaEventDestroy(s->ev_up_free);
+    if (s->up_stream) cudaStreamDestroy(s->up_stream);
     if (s->ev_ready) cudaEventDestroy(s->ev_ready);
     if (s->ev_gathered) cudaEventDestroy(s->ev_gathered);
     if (s->copy_stream) cudaStreamDestroy(s->copy_stream);
@@ -1496,11 +1507,30 @@ emerge_status emerge_cuda_write_particles(emerge_sim *s, const emerge_particle *
     if (!s || (!in && n)) return EMERGE_ERR_INVALID_ARG;
     if (n != s->n) return static_cast<emerge_status>(s->fail(EMERGE_ERR_INVALID_ARG, "n must equal the particle count"));
     if (n == 0) return EMERGE_OK;
-    // Upload into the staging buffer and check it there (contact groups switch the
-    // multi-field pipeline on, pinned particles the pinned load).
-    CK(cudaMemcpyAsync(s->d_aos, in, n * sizeof(emerge_particle), cudaMemcpyHostToDevice, s->stream));
+    // Upload into a staging buffer of its own on a stream of its own, so the copy overlaps
+    // the work already queued on the simulation's stream (which waits for it before the
+    // check), then check it there (contact groups switch the multi-field pipeline on,
+    // pinned particles the pinned load).
+    if (!s->up_stream) {
+        CK(cudaStreamCreateWithFlags(&s->up_stream, cudaStreamNonBlocking));
+        CK(cudaEventCreateWithFlags(&s->ev_up_done, cudaEventDisableTiming));
+        CK(cudaEventCreateWithFlags(&s->ev_up_free, cudaEventDisableTiming));
+    }
+    const size_t up_bytes = s->cap * sizeof(emerge_particle);
+    if (s->staging_up.bytes < up_bytes) {
+        CK(cudaStreamSynchronize(s->stream));  // the previous upload's scatter reads the old buffer
+        s->staging_up.reset();
+        CK(cudaMalloc(&s->staging_up.ptr, up_bytes));
+        s->staging_up.bytes = up_bytes;
+        s->up_used = false;
+    }
+    emerge_particle *up = static_cast<emerge_particle *>(s->staging_up.ptr);
+    if (s->up_used) CK(cudaStreamWaitEvent(s->up_stream, s->ev_up_free, 0));  // read by the last scatter
+    CK(cudaMemcpyAsync(up, in, n * sizeof(emerge_particle), cudaMemcpyHostToDevice, s->up_stream));
+    CK(cudaEventRecord(s->ev_up_done, s->up_stream));
+    CK(cudaStreamWaitEvent(s->stream, s->ev_up_done, 0));
     CK(cudaMemsetAsync(&s->d_state->upload_flags, 0, sizeof(uint32_t), s->stream));
-    launch_check_aos(s->d_aos, static_cast<int>(n), &s->d_state->upload_flags, s->stream);
+    launch_check_aos(up, static_cast<int>(n), &s->d_state->upload_flags, s->stream);
     CK(cudaMemcpyAsync(&s->h_state->upload_flags, &s->d_state->upload_flags, sizeof(uint32_t),
                        cudaMemcpyDeviceToHost, s->stream));
     CK(cudaStreamSynchronize(s->stream));
@@ -1516,7 +1546,9 @@ emerge_status emerge_cuda_write_particles(emerge_sim *s, const emerge_particle *
         s->lf.pinned = pinned;
         s->graph_dirty = true;  // the particle kernels' load flags are baked into the graph
     }
-    launch_scatter_aos(s->P[s->cur], static_cast<int>(n), s->d_aos, s->stream);
+    launch_scatter_aos(s->P[s->cur], static_cast<int>(n), up, s->stream);
+    CK(cudaEventRecord(s->ev_up_free, s->stream));
+    s->up_used = true;
     s->host_launches += 1;
     if (s->dcfg.zones) launch_zone_bits(s->P[s->cur], static_cast<int>(n), static_cast<uint32_t>(s->active), s->stream);
     CK(cudaGetLastError());

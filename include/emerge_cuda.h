@@ -328,7 +328,9 @@ emerge_status emerge_cuda_read_particles(emerge_sim *sim, emerge_particle *out, 
  * run asynchronously.  Successive calls complete in order. */
 emerge_status emerge_cuda_read_particles_async(emerge_sim *sim, emerge_particle *out, uint64_t n);
 /* Simulation::particles_mut() (lifecycle.rs:233) write-back: replaces every
- * particle's state from `in` (reference index order). */
+ * particle's state from `in` (reference index order), after the work already queued.  The
+ * host-to-device copy runs on a stream of its own and overlaps that work; the call returns
+ * once `in` has been copied. */
 emerge_status emerge_cuda_write_particles(emerge_sim *sim, const emerge_particle *in, uint64_t n);
 
 /* ---- stepping ------------------------------------------------------------------ */
