@@ -1585,10 +1585,9 @@ emerge_status emerge_cuda_replace_particles(emerge_sim *s, const emerge_particle
 
 emerge_status emerge_cuda_step(emerge_sim *s, uint32_t n_steps, emerge_step_timing *timing) {
     if (!s) return EMERGE_ERR_INVALID_ARG;
-    if (s->n == 0) {
-        if (timing) std::memset(timing, 0, sizeof(*timing));
-        return EMERGE_OK;
-    }
+    // An empty simulation still runs the substep loop (step.rs:34-49): with no particles the
+    // CFL bound leaves the whole frame as one substep, and last_substeps / effective_dt report
+    // it as the reference does; every particle kernel launcher returns at n == 0.
     if (s->dcfg.mf_fast && (s->dcfg.mf_fields & 1)) {  // the contact lists' nodes, one per slot
         float4 *before = s->g.cpts;
         emerge_status st = ensure_points(s);
