@@ -168,3 +168,33 @@ def test_grip_and_phase_arguments_are_checked(cuda_lib):
     sim.set_contact_grip(None)
     sim.step()
     assert np.isfinite(sim.particles()["v"]).all()
+
+
+@pytest.mark.parametrize("mode", ["reference_order", "fast"])
+def test_single_field_scenes(cuda_lib, mode):
+    """Contact with every particle in the grip field (no interface anywhere) and a mixture
+    with one phase only (drag never engages): the resolves must fall back to the total
+    velocity exactly as the reference's do."""
+    exact = mode == "reference_order"
+    cls = DeterministicSimulation if exact else Simulation
+
+    def all_grip(sim_cls):
+        sim = scenes.contact_scene(sim_cls)
+        p = sim.particles()
+        p["contact_group"][:] = 3
+        sim.set_particles(p)
+        return sim
+
+    def one_phase(sim_cls):
+        sim = scenes.mixture_scene(sim_cls)
+        p = sim.particles()
+        p["material_id"][:] = 0  # every particle in the solid phase
+        sim.set_particles(p)
+        return sim
+
+    for build in (all_grip, one_phase):
+        g = build(cls)
+        with correctly_rounded_math() if exact else contextlib.nullcontext():
+            c = build(OracleSimulation)
+            first_inexact, _ = run_frames(g, c, 3, mode)
+        assert first_inexact is None or not exact, build.__name__
