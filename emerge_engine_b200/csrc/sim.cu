@@ -176,6 +176,8 @@ struct emerge_sim {
     Buffer mfbuf;                    // the multi-field grid arrays and the phase table
     Buffer ptsbuf;                   // the contact point cloud, one entry per scatter record
     size_t pts_cap = 0;
+    Buffer listbuf;                  // fast pipeline: the contact list nodes, one per particle slot
+    size_t list_cap = 0;
     float4 *det_points() const { return static_cast<float4 *>(ptsbuf.ptr); }
 
     // reference-order (deterministic) mode
@@ -1590,12 +1592,17 @@ emerge_status emerge_cuda_step(emerge_sim *s, uint32_t n_steps, emerge_step_timi
     // it as the reference does; every particle kernel launcher returns at n == 0.
     if (s->dcfg.mf_fast && (s->dcfg.mf_fields & 1)) {  // the contact lists' nodes, one per slot
         float4 *before = s->g.cpts;
-        emerge_status st = ensure_points(s);
-        if (st != EMERGE_OK) return st;
-        s->g.cpts = s->det_points();
+        if (s->list_cap < s->cap) {
+            CK(cudaStreamSynchronize(s->stream));  // queued kernels may still walk the old nodes
+            s->listbuf.reset();
+            CK(cudaMalloc(&s->listbuf.ptr, std::max<size_t>(s->cap, 1) * sizeof(float4)));
+            s->listbuf.bytes = std::max<size_t>(s->cap, 1) * sizeof(float4);
+            s->list_cap = s->cap;
+        }
+        s->g.cpts = static_cast<float4 *>(s->listbuf.ptr);
         if (s->g.cpts != before) {
             s->graph_dirty = true;
-            st = invalidate_pending(s);
+            emerge_status st = invalidate_pending(s);
             if (st != EMERGE_OK) return st;
         }
     }
