@@ -559,6 +559,12 @@ def main():
         host = PinnedBuffer(n * 128)
         host_out = PinnedBuffer(n * 128)
         sim.read_particles_raw(host.ptr, n)
+        # one untimed round first: the upload and readback paths set up their staging buffers
+        # and streams on first use
+        sim.write_particles_raw(host.ptr, n)
+        sim.step()
+        sim.read_particles_raw_async(host_out.ptr, n)
+        sim.synchronize()
         e2e_steps = max(3, min(args.steps, 10))
         sub0 = sim.stats()["substeps"]
         sim.synchronize()

@@ -427,6 +427,13 @@ emerge_status ensure_capacity(emerge_sim *s, size_t need) {
     CK(cudaMalloc(&s->staging.ptr, cap * sizeof(emerge_particle)));
     s->staging.bytes = cap * sizeof(emerge_particle);
     s->d_aos = static_cast<emerge_particle *>(s->staging.ptr);
+    // the write-back's own staging buffer, sized with the particle sets so that a write-back
+    // does not allocate (a large cudaMalloc can take tens of milliseconds)
+    if (s->up_stream) CK(cudaStreamSynchronize(s->up_stream));
+    s->staging_up.reset();
+    CK(cudaMalloc(&s->staging_up.ptr, cap * sizeof(emerge_particle)));
+    s->staging_up.bytes = cap * sizeof(emerge_particle);
+    s->up_used = false;
     s->sortbuf.reset();
     size_t sb = sort_scratch_bytes(cap);
     CK(cudaMalloc(&s->sortbuf.ptr, sb));
