@@ -377,6 +377,7 @@ struct Payload {
     bool do_ma;   // scatter mass + affine momentum
     bool do_s;    // scatter stress impulse
     uint32_t fields;  // multi-field sums it also adds to: bit 0 grip, 1 solid, 2 fluid
+    bool excl;        // ... and to that (single) field only, not to the total (DevConfig::mf_excl)
 };
 
 // Which channels a scatter call carries: mass + momentum, stress, or per-particle flags.
@@ -496,9 +497,11 @@ __device__ __forceinline__ void scatter_cells(const GridView &g, const ScatterPl
 }
 
 // Warp-aggregated variant: every lane of the warp takes part (inactive lanes add zero).
+// `target`, the same for every active lane: 0 the total, k + 1 multi-field sum k.
 template <int SC>
 __device__ __forceinline__ void scatter_cells_aggregated(const GridView &g, const ScatterPlan &pl,
-                                                         bool active, bool do_ma, bool do_s) {
+                                                         bool active, bool do_ma, bool do_s,
+                                                         unsigned target) {
     const int lane = threadIdx.x & 31;
     const QW &w = pl.w;
     const bool any_ma = SC != SC_S && __ballot_sync(0xffffffffu, active && do_ma) != 0u;
@@ -515,9 +518,10 @@ __device__ __forceinline__ void scatter_cells_aggregated(const GridView &g, cons
         __reduce_max_sync(0xffffffffu, head ? static_cast<unsigned>(seg_end - lane) : 0u));
     if (span <= 1) {
         if (!active) return;
-        if (SC == SC_MA) scatter_cells<SC_MA, true>(g, pl, do_ma, do_s);
-        else if (SC == SC_S) scatter_cells<SC_S, true>(g, pl, do_ma, do_s);
-        else scatter_cells<SC_BOTH, true>(g, pl, do_ma, do_s);
+        if (target)
+            scatter_cells_to<SC, true>(g, pl, do_ma, do_s, g.fa[target - 1], g.fs[target - 1]);
+        else
+            scatter_cells_to<SC, true>(g, pl, do_ma, do_s, g.acc_a, g.acc_s);
         return;
     }
     int yp[3] = {0, 0, 0};
@@ -545,8 +549,14 @@ __device__ __forceinline__ void scatter_cells_aggregated(const GridView &g, cons
             if (head && active && in_domain(cx, cy, g.res)) {
                 const int ci = xp + yp[gy];
                 // the fourth lane counts the segment's scatters, one per particle
-                if (any_ma) red_add_v4(&g.acc_a[ci], mc, ax, ay, static_cast<float>(seg_end - lane));
-                if (any_s) red_add_v2(&g.acc_s[ci], sx, sy);
+                float4 *A = g.acc_a;
+                float2 *S = g.acc_s;
+                if (target) {
+                    A = g.fa[target - 1];
+                    S = g.fs[target - 1];
+                }
+                if (any_ma) red_add_v4(&A[ci], mc, ax, ay, static_cast<float>(seg_end - lane));
+                if (any_s) red_add_v2(&S[ci], sx, sy);
             }
         }
     }
@@ -558,20 +568,38 @@ __device__ __forceinline__ void scatter_particle(const GridView &g, const Payloa
     const bool active = valid && (p.do_ma || p.do_s);
     ScatterPlan pl{};
     if (active) pl = make_plan<SC>(p);
-    if (aggregate) {
-        scatter_cells_aggregated<SC>(g, pl, active, p.do_ma, p.do_s);
+    // Exclusive field sums: a field particle's contributions go to its field's sums only, and
+    // the grid update adds them to the total.  target: 0 the total, k + 1 field k.
+    float4 *A = g.acc_a;
+    float2 *S = g.acc_s;
+    unsigned target = 0u;
+    if (p.excl) {
+        const int k = __ffs(p.fields) - 1;
+        A = g.fa[k];
+        S = g.fs[k];
+        target = static_cast<unsigned>(k) + 1u;
+    }
+    // aggregate 2 (exclusive field sums): the warp aggregates when its active lanes share one
+    // target, a warp that mixes them scatters lane by lane
+    bool agg = aggregate != 0;
+    if (aggregate == 2)
+        agg = __reduce_min_sync(0xffffffffu, active ? target : 4u) >=
+              __reduce_max_sync(0xffffffffu, active ? target : 0u);
+    if (agg) {
+        scatter_cells_aggregated<SC>(g, pl, active, p.do_ma, p.do_s, target);
         if (!active) return;
         // the multi-field sums of the fast pipeline (p2g.rs:60-66): the same contributions
-        for (uint32_t f = p.fields; f != 0u; f &= f - 1u) {
-            const int k = __ffs(f) - 1;
-            scatter_cells_to<SC, true>(g, pl, p.do_ma, p.do_s, g.fa[k], g.fs[k]);
-        }
+        if (!p.excl)
+            for (uint32_t f = p.fields; f != 0u; f &= f - 1u) {
+                const int k = __ffs(f) - 1;
+                scatter_cells_to<SC, true>(g, pl, p.do_ma, p.do_s, g.fa[k], g.fs[k]);
+            }
     } else {
         if (!active) return;
         // up to two multi-field sums (grip, and a mixture phase) take the same contributions
         float4 *A2 = nullptr, *A3 = nullptr;
         float2 *S2 = nullptr, *S3 = nullptr;
-        if (p.fields) {
+        if (p.fields && !p.excl) {
             const int k2 = __ffs(p.fields) - 1;
             A2 = g.fa[k2];
             S2 = g.fs[k2];
@@ -584,9 +612,9 @@ __device__ __forceinline__ void scatter_particle(const GridView &g, const Payloa
         }
         const QW &w = pl.w;
         if (stencil_inside(w.bx, w.by, g.res))
-            scatter_cells_to<SC, false>(g, pl, p.do_ma, p.do_s, g.acc_a, g.acc_s, A2, S2, A3, S3);
+            scatter_cells_to<SC, false>(g, pl, p.do_ma, p.do_s, A, S, A2, S2, A3, S3);
         else
-            scatter_cells_to<SC, true>(g, pl, p.do_ma, p.do_s, g.acc_a, g.acc_s, A2, S2, A3, S3);
+            scatter_cells_to<SC, true>(g, pl, p.do_ma, p.do_s, A, S, A2, S2, A3, S3);
     }
     mark_tiles(g, pl.w.bx, pl.w.by);
 }
@@ -627,7 +655,7 @@ struct ParticleKernelArgs {
     LoadFlags lf;
     int mode_g2p;       // 0: prime pass (no G2P), 1: G2P(k) + P2G(k+1)
     int density_mode;   // fluid stress deferred to k_density; G2P reads rho_dp
-    int aggregate;      // warp-aggregated P2G reductions
+    int aggregate;      // warp-aggregated P2G reductions (2: in warps whose lanes share a target)
     int project_in;     // recompute the projection of substep k before G2P (fused pipeline)
     int emit_p2g;       // project for substep k+1 and scatter its P2G (fused pipeline)
     ClosureArgs cl;     // learned closure (kernels instantiated with CLOSURE only)
@@ -901,6 +929,7 @@ __device__ __forceinline__ void particle_pass(const ParticleKernelArgs &a) {
     pl.do_ma = false;
     pl.do_s = false;
     pl.fields = 0u;
+    pl.excl = false;
     float max_speed = 0.0f;
     float min_mdt = INFINITY;
     int clamped = 0, projected = 0, proj_changed = 0;
@@ -1005,6 +1034,7 @@ __device__ __forceinline__ void particle_pass(const ParticleKernelArgs &a) {
             if constexpr (HAS_MODEL(MASK, M_EXTRAS_BIT)) {
                 if (cfg.mf_fast) {
                     pl.fields = multi_fields(cfg, a.P, i, p.mat, n_mats);
+                    pl.excl = cfg.mf_excl && pl.fields != 0u;
                     if (cfg.mf_fields & 1) push_contact_point(g, p.x, (pl.fields & 1u) != 0u, i, acc_slot);
                 }
             }
@@ -1028,28 +1058,39 @@ __device__ __forceinline__ void particle_pass(const ParticleKernelArgs &a) {
             atomicAdd(&st->window_blocks, 1ull);
         }
     }
+    // aggregate mode 2 (per-warp targets) only where exclusive field sums can occur
+    const int aggregate = HAS_MODEL(MASK, M_EXTRAS_BIT) ? a.aggregate : (a.aggregate ? 1 : 0);
     if (core_mask(MASK) == MASK_FLUID && density_mode)
-        scatter_particle<SC_MA>(g, pl, valid, a.aggregate);
+        scatter_particle<SC_MA>(g, pl, valid, aggregate);
     else
-        scatter_particle<SC_BOTH>(g, pl, valid, a.aggregate);
+        scatter_particle<SC_BOTH>(g, pl, valid, aggregate);
 }
 
 // ---------------------------------------------------------------- k_density
 // Density at a particle: sum of w m over its stencil (solver/density.rs:50-71), as
 // row sums sum_gx wx (sum_gy wy m).  CHECK reads cells outside the domain as zero.
+// `excl_fields`: the fields whose particles scattered into their field only
+// (DevConfig::mf_excl); their masses are part of the cell's total.
 template <bool CHECK>
-__device__ __forceinline__ float gather_density(const GridView &g, const QW &w) {
+__device__ __forceinline__ float gather_density(const GridView &g, const QW &w, int excl_fields) {
     int yp[3];
 #pragma unroll
     for (int k = 0; k < 3; ++k) yp[k] = cell_y_part(w.by + k - 1);
     float density = 0.0f;
 #pragma unroll
     for (int gx = 0; gx < 3; ++gx) {
-        const float4 *row = g.acc_a + cell_x_part(w.bx + gx - 1, g.tpd);
+        const int xp = cell_x_part(w.bx + gx - 1, g.tpd);
+        const float4 *row = g.acc_a + xp;
         float mk[3];
 #pragma unroll
-        for (int gy = 0; gy < 3; ++gy)
-            mk[gy] = (CHECK && !in_domain(w.bx + gx - 1, w.by + gy - 1, g.res)) ? 0.0f : row[yp[gy]].x;
+        for (int gy = 0; gy < 3; ++gy) {
+            const bool out = CHECK && !in_domain(w.bx + gx - 1, w.by + gy - 1, g.res);
+            mk[gy] = out ? 0.0f : row[yp[gy]].x;
+            if (excl_fields && !out) {
+                if (excl_fields & 1) mk[gy] += g.fa[0][xp + yp[gy]].x;
+                if (excl_fields & 2) mk[gy] += g.fa[1][xp + yp[gy]].x + g.fa[2][xp + yp[gy]].x;
+            }
+        }
         const float r = __fmaf_rn(w.wy[0], mk[0], __fmaf_rn(w.wy[1], mk[1], w.wy[2] * mk[2]));
         density = __fmaf_rn(w.wx[gx], r, density);
     }
@@ -1112,6 +1153,7 @@ __device__ __forceinline__ void density_pass(const DensityKernelArgs &a) {
     pl.do_ma = false;
     pl.do_s = false;
     pl.fields = 0u;
+    pl.excl = false;
     if (valid) {
         if (reproject) {
             p = load_state(a.P, i, a.lf);
@@ -1119,7 +1161,11 @@ __device__ __forceinline__ void density_pass(const DensityKernelArgs &a) {
         }
         const QW w = quadratic_weights(p.x);
         const bool inside = stencil_inside(w.bx, w.by, g.res);
-        const float density = inside ? gather_density<false>(g, w) : gather_density<true>(g, w);
+        // (an if statement: a ?: reading cfg here stops this nvcc's front end)
+        int excl = 0;
+        if constexpr (HAS_MODEL(MASK, M_EXTRAS_BIT))
+            if (cfg.mf_excl) excl = cfg.mf_fields;
+        const float density = inside ? gather_density<false>(g, w, excl) : gather_density<true>(g, w, excl);
         a.P.rho_dp[i] = density;
         const MatP &m = s_mats[p.mat < static_cast<uint32_t>(n_mats) ? p.mat : 0u];
         if (m.model == M_FLUID) {
@@ -1145,11 +1191,16 @@ __device__ __forceinline__ void density_pass(const DensityKernelArgs &a) {
             pl.tau = combined_kirchhoff_stress<MASK>(m, p, pr);
             pl.s = -stress_volume(m, p) * KERNEL_D_INVERSE;
             pl.do_s = true;
-            if constexpr (HAS_MODEL(MASK, M_EXTRAS_BIT))
-                if (cfg.mf_fast) pl.fields = multi_fields(cfg, a.P, i, p.mat, n_mats);
+            if constexpr (HAS_MODEL(MASK, M_EXTRAS_BIT)) {
+                if (cfg.mf_fast) {
+                    pl.fields = multi_fields(cfg, a.P, i, p.mat, n_mats);
+                    pl.excl = cfg.mf_excl && pl.fields != 0u;
+                }
+            }
         }
     }
-    scatter_particle<SC_S>(g, pl, valid, a.aggregate);
+    scatter_particle<SC_S>(g, pl, valid,
+                           HAS_MODEL(MASK, M_EXTRAS_BIT) ? a.aggregate : (a.aggregate ? 1 : 0));
 }
 
 // Launchers of the fast path's kernels (fast_kernels.cu).
@@ -1177,7 +1228,7 @@ inline void fill_common(Args &a, const StepLaunch &L, const LoadFlagsHost &lfh) 
     a.lf.temperature = lfh.temperature;
     a.lf.activation = lfh.activation;
     a.lf.pinned = lfh.pinned;
-    a.aggregate = L.use_window;
+    a.aggregate = L.use_window ? (L.cfg.mf_excl ? 2 : 1) : 0;
 }
 
 }  // namespace emerge

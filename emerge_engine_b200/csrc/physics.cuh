@@ -950,6 +950,8 @@ struct DevConfig {
     const uint32_t *mat_phase;  // MixturePhase per material slot: 0 none, 1 solid, 2 fluid
     int mf_fast;             // multi-field scene on the fast (fused, unordered-sum) pipeline
     int mf_fields;           // fields in use: bit 0 grip (contact), bit 1 solid + fluid (mixture)
+    int mf_excl;             // fast pipeline, one kind of field: a field particle scatters into
+                             // its field only, and the grid update adds the fields to the total
 };
 
 // Bits of DevParticles::sleeping while the sleep partition is in use: bit 0 is

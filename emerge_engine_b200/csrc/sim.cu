@@ -340,6 +340,10 @@ void refresh_dev_config(emerge_sim *s) {
     s->dcfg.mat_phase = s->mfbuf.ptr ? static_cast<const uint32_t *>(s->mfbuf.ptr) : nullptr;
     s->dcfg.mf_fast = (s->dcfg.multi && !s->deterministic) ? 1 : 0;
     s->dcfg.mf_fields = (s->contact_seen ? 1 : 0) | (mixture_on(s) ? 2 : 0);
+    // One kind of field: its particles scatter into their field only and the grid update forms
+    // the total.  With both kinds a particle may sit in two fields and scatters into the total
+    // as well.
+    s->dcfg.mf_excl = (s->dcfg.mf_fast && (s->dcfg.mf_fields == 1 || s->dcfg.mf_fields == 2)) ? 1 : 0;
     s->dcfg.n_fields = s->n_fields;
     s->dcfg.fields = s->n_fields ? static_cast<const emerge_force_field *>(s->fbuf.ptr) : nullptr;
     s->dcfg.field_data = s->n_fields ? reinterpret_cast<const float *>(

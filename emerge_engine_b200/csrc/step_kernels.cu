@@ -45,17 +45,17 @@ struct GridKernelArgs {
 // an active tile, then the accumulators are zeroed for the next scatter.
 // The fast pipeline's field sum of one cell: A + dt S as {m, px, py, w} (the form the
 // reference-order scatter writes, w > 0 marking the field), the accumulators zeroed for the
-// next scatter.  Each scatter adds exactly 1 to the w lanes, so for the grip field
-// total_w - grip_w counts the other particles' scatters exactly, whatever the order of the
-// sums: w = 2 marks a cell that also holds other particles, w = 1 a grip-only cell, whose
-// rest mass the reference computes as exactly 0 (its grip and total sums run in the same
-// order), while total - grip here is rounding noise.
+// next scatter.  Each scatter adds exactly 1 to the w lanes, so `rest_w`, the scatters of the
+// particles outside the field, is an exact count whatever the order of the sums: w = 2 marks
+// a cell that also holds other particles, w = 1 a field-only cell, whose rest mass the
+// reference computes as exactly 0 (its field and total sums run in the same order), while
+// total - field here would be rounding noise.
 __device__ __forceinline__ bool finalize_field(float4 *fa, float2 *fs, float4 *out, int ci, float dt,
-                                               float total_w) {
+                                               float rest_w) {
     const float4 a = fa[ci];
     if (!(a.w > 0.0f)) return false;
     const float2 s = fs[ci];
-    out[ci] = make_float4(a.x, a.y + dt * s.x, a.z + dt * s.y, total_w > a.w + 0.5f ? 2.0f : 1.0f);
+    out[ci] = make_float4(a.x, a.y + dt * s.x, a.z + dt * s.y, rest_w > 0.5f ? 2.0f : 1.0f);
     fa[ci] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
     fs[ci] = v2(0.0f, 0.0f);
     return true;
@@ -68,6 +68,17 @@ __device__ __forceinline__ void grid_update_cell(const GridView &g, const DevCon
     const int y = (tile % g.tpd) * TILE + (local & 7);
     float4 acc = g.acc_a[ci];
     float2 s = g.acc_s[ci];
+    const float rest_w = acc.w;  // with exclusive field sums: the scatters of particles in no field
+    if (cfg.mf_excl) {           // the fields' particles scattered into their fields only
+        int k0 = 1, k1 = 2;      // the solid and fluid phases
+        if (cfg.mf_fields & 1) k0 = k1 = 0;  // the grip field
+        for (int k = k0; k <= k1; ++k) {
+            const float4 f = g.fa[k][ci];
+            const float2 fs = g.fs[k][ci];
+            acc = make_float4(acc.x + f.x, acc.y + f.y, acc.z + f.z, acc.w + f.w);
+            s = v2(s.x + fs.x, s.y + fs.y);
+        }
+    }
     float m = acc.x;
     float2 mom = v2(acc.y + dt * s.x, acc.z + dt * s.y);
     if (m > 0.0f) mom = vdivs(mom, m);
@@ -84,8 +95,12 @@ __device__ __forceinline__ void grid_update_cell(const GridView &g, const DevCon
     if (cfg.multi) {
         g.grid_m[ci] = m;  // the contact and mixture resolves read the total mass
         if (cfg.mf_fast) {
-            if ((cfg.mf_fields & 1) && finalize_field(g.fa[0], g.fs[0], g.acc_grip, ci, dt, acc.w))
-                *contact_active = 1u;  // Grid::has_contact_activity
+            if (cfg.mf_fields & 1) {
+                float rest = rest_w;
+                if (!cfg.mf_excl) rest = acc.w - g.fa[0][ci].w;
+                if (finalize_field(g.fa[0], g.fs[0], g.acc_grip, ci, dt, rest))
+                    *contact_active = 1u;  // Grid::has_contact_activity
+            }
             if (cfg.mf_fields & 2) {
                 finalize_field(g.fa[1], g.fs[1], g.acc_sol, ci, dt, 0.0f);
                 finalize_field(g.fa[2], g.fs[2], g.acc_flu, ci, dt, 0.0f);
@@ -478,7 +493,13 @@ __global__ void k_wake(DevParticles P, int n, GridView g, DevConfig cfg, const S
     for (int gx = 0; gx < 3; ++gx)
         for (int gy = 0; gy < 3; ++gy) {
             const int cx = w.bx + gx - 1, cy = w.by + gy - 1;
-            if (in_domain(cx, cy, g.res) && g.acc_a[cell_index(cx, cy, g.tpd)].w > 0.0f) hit = true;
+            if (!in_domain(cx, cy, g.res)) continue;
+            const int ci = cell_index(cx, cy, g.tpd);
+            if (g.acc_a[ci].w > 0.0f) hit = true;
+            // with exclusive field sums, a cell touched by field particles only
+            if (cfg.mf_excl && (((cfg.mf_fields & 1) && g.fa[0][ci].w > 0.0f) ||
+                                ((cfg.mf_fields & 2) && (g.fa[1][ci].w > 0.0f || g.fa[2][ci].w > 0.0f))))
+                hit = true;
         }
     if (!hit) return;
     // The woken particle's G2P reads all 9 stencil cells, some of which this substep's P2G
@@ -563,7 +584,7 @@ void launch_density_pass(const StepLaunch &L, const LoadFlagsHost &lfh) {
     // The density pass scatters two stress components per cell: there the warp-aggregated
     // reductions cost fewer L2 atomics than they add shuffles (dam break 1M: 47.7 -> 42.7 us
     // per launch), unlike the particle pass's mass + momentum scatter (74.5 -> 76.1 us).
-    a.aggregate = 1;
+    a.aggregate = L.cfg.mf_excl ? 2 : 1;
     launch_density_pass_fast(a, L.model_mask, L.stream);
 }
 

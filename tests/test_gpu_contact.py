@@ -114,9 +114,14 @@ def combined_scene(sim_cls):
 
 
 def test_contact_with_fields_asflip_and_sleep(cuda_lib):
-    """Contact together with the other extras: bit for bit in reference order, within the fast
-    bar on the fused pipeline (which steps it with the host-driven substep loop, as every
-    scene with a sleep partition)."""
+    """Contact together with the other extras: bit for bit in reference order.  On the fused
+    pipeline (which steps it with the host-driven substep loop, as every scene with a sleep
+    partition) ASFLIP's position gate, gamma = [trace B >= 0] (g2p.rs:291-296), is a sign
+    decision on rounding noise for the rigidly translating block: with any other summation
+    order a few dozen particles take the other branch from the first frame (about 3e-3 cells
+    apart), and the sleep partition may differ by a particle or two (a particle asleep in one
+    run moves on in the other), so the frames are judged on substep counts, the partition
+    size, mass, momentum and displacement statistics instead of the per-particle bar."""
     g = combined_scene(DeterministicSimulation)
     with correctly_rounded_math():
         c = combined_scene(OracleSimulation)
@@ -130,8 +135,20 @@ def test_contact_with_fields_asflip_and_sleep(cuda_lib):
         c.step()
         assert g.last_substeps() == c.last_substeps(), k
         assert abs(g.active_count() - c.active_count()) <= 2, k
-    if g.active_count() == c.active_count():
-        compare_particles(g.particles(), c.particles(), **tol("fast"))
+    pg, pc = g.particles(), c.particles()
+    assert pg["mass"].sum(dtype=np.float64) == pc["mass"].sum(dtype=np.float64)
+    m = pc["mass"].astype(np.float64)
+    p_abs = (m * np.linalg.norm(pc["v"].astype(np.float64), axis=1)).sum()
+    dp = np.linalg.norm((m[:, None] * pg["v"]).sum(0) - (m[:, None] * pc["v"]).sum(0))
+    dx = np.linalg.norm(pg["x"].astype(np.float64) - pc["x"], axis=1)
+    far = int((dx > 0.25).sum())
+    print("combined scene, fused pipeline: |dp| / sum |p| %.2e, dx p99 %.2e cells, %d particles "
+          "over 0.25 cells (max %.2e)" % (dp / p_abs, np.percentile(dx, 99), far, dx.max()))
+    assert dp <= 1e-3 * p_abs
+    assert np.percentile(dx, 99) <= 0.05
+    # a particle that took the other sleep or contact branch (the partition may differ by two
+    # particles per frame) is followed by its stencil neighbours, not by the whole block
+    assert far <= 16
 
 
 @pytest.mark.parametrize("mode", ["reference_order", "fast"])
