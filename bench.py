@@ -7,8 +7,10 @@ of config.dt = 0.05, with as many CFL-limited substeps as the reference loop tak
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--workload NAME] [--impl ours|reference]
 
-Default workload: the dam break at ~1M particles (512 x 512-cell water column at 4 particles
-per cell on a 1024^2 grid).  Inputs are resident in HBM when the timed region starts; L2 is
+Default workload: the mixed granular scene the metric is quoted on (~4M particles in seeded
+blocks of DruckerPrager sand, Stomakhin snow and NACC soil at 4 particles per cell on a 1024^2
+grid), with the learned return-mapping closure timed on the same scene in the same line
+(`learned_closure`: its rate, its ratio to the plain step and its judged stress error).  Inputs are resident in HBM when the timed region starts; L2 is
 flushed (512 MiB device write) before every timed step.  `e2e` repeats the measurement
 through the C ABI with the particle state uploaded from pinned host memory before and read
 back (asynchronously, overlapping the next upload) after every step.  `--impl reference` times the CPU oracle (the reference step restated
@@ -89,7 +91,7 @@ WORKLOADS = {
                              "NeoHookean}, 4 ppc block on the floor, SlipBoundary(2), dt=0.05",
                         material="batched", grid_res=0),
 }
-DEFAULT_WORKLOAD = "dam_break_1m"
+DEFAULT_WORKLOAD = "mixed_granular_4m"
 
 # Algorithmic bytes per particle of one launch of the fused particle pass (k_particle):
 # the hot state it must read and write once per substep, plus its share of grid traffic
@@ -101,6 +103,9 @@ DEFAULT_WORKLOAD = "dam_break_1m"
 #             contact group 4, grid 8                                  -> 136 + 20 (sleep flag,
 #             field velocities) = 156 B
 #   mixture:  the mean of the granular (164) and fluid (136) particles    -> 150 B
+# k_density per particle (fluid scenes): read x8 mat4 C16 mass4, write rho_dp 4, grid
+# (mass gather 4 B + stress reduction 8 B per cell) / 4 ppc = 3                   -> 39 B
+K_DENSITY_BYTES = 39
 K_PARTICLE_BYTES = {"NewtonianFluid": 136, "DP+Snow+NACC": 164, "ZOO7": 164,
                     "NewtonianFluid+fields": 136, "NeoHookean-sleep": 156,
                     "NeoHookean-contact": 156, "DP+NewtonianFluid-mixture": 150}
@@ -323,19 +328,52 @@ def _oracle_run(sims, max_steps: int, budget_s: float):
     return rounds, units, subs, time.perf_counter() - t0
 
 
-def cpu_baseline(workload: str, budget_s: float = 15.0) -> dict:
-    """The CPU oracle (reference step restated in C++) on this host, bounded sample."""
+def cpu_model() -> str:
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    import platform
+    return platform.processor() or "unknown"
+
+
+def time_oracle(workload: str, warmup_steps: int, warmup_budget_s: float, runs: int,
+                run_budget_s: float, max_steps_per_run: int = 1 << 30) -> dict:
+    """The CPU oracle (the reference step restated in C++) on this host's cores: up to
+    `warmup_steps` warm-up frames (stopping early once `warmup_budget_s` is spent), then
+    `runs` timed runs of whole frames, each run ending after `max_steps_per_run` frames or
+    `run_budget_s` seconds; the value is the median run's particle-substeps per second."""
     from oracle.oracle import set_threads
     threads = set_threads(0)
     sims = _oracle_scenes(workload)
     n = sum(s.particle_count() for s in sims)
-    _oracle_run(sims, 1, budget_s)  # warm-up round
-    rounds, units, subs, dt = _oracle_run(sims, 1 << 30, budget_s)
-    return {"value": units / dt, "unit": UNIT, "cores": threads, "kind": "port",
-            "sample": f"{workload}: {rounds} full step(s) of {len(sims)} scene(s), {subs} substeps, "
-                      f"{n} particles, after 1 warm-up step, {dt:.1f} s (P2G, density and "
-                      "constitutive update sequential as in the reference; G2P gather on all threads)",
-            "seconds": dt}
+    w_rounds, _, _, w_dt = _oracle_run(sims, warmup_steps, warmup_budget_s)
+    rates, frames, subs_total, secs = [], 0, 0, 0.0
+    for _ in range(runs):
+        rounds, units, subs, dt = _oracle_run(sims, max_steps_per_run, run_budget_s)
+        rates.append(units / dt)
+        frames += rounds
+        subs_total += subs
+        secs += dt
+    med = statistics.median(rates)
+    return {"value": med, "unit": UNIT, "cores": threads, "cpu_model": cpu_model(),
+            "kind": "port", "runs": runs, "run_values": rates,
+            "spread": (max(rates) - min(rates)) / med if med > 0 else None,
+            "warmup_steps": w_rounds, "frames": frames, "substeps": subs_total,
+            "particles": n, "scenes": len(sims), "seconds": secs,
+            "sample": f"{workload}: median of {runs} timed runs ({frames} full steps, {subs_total} "
+                      f"substeps of {n} particles in {len(sims)} scene(s), {secs:.1f} s) after "
+                      f"{w_rounds} warm-up step(s) ({w_dt:.1f} s); P2G, density and constitutive "
+                      "update sequential as in the reference, G2P gather on all threads"}
+
+
+def cpu_baseline(workload: str, budget_s: float = 15.0) -> dict:
+    """Bounded sample of the CPU oracle for the cpu_baseline key: warm-up frames (at most 10,
+    within a third of the budget), then the median of 3 timed runs."""
+    return time_oracle(workload, 10, budget_s / 3.0, 3, budget_s / 3.0)
 
 
 def run_reference(args):
@@ -343,31 +381,35 @@ def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    from oracle.oracle import set_threads
-    threads = set_threads(0)
-    sims = _oracle_scenes(args.workload)
-    n = sum(s.particle_count() for s in sims)
-    # Bounded sample: warm-up and timed steps each stop early once their time budget is
+    # Bounded sample: the warm-up and each timed run stop early once their time budget is
     # spent, so the run ends within a few minutes whatever the workload.
-    _oracle_run(sims, args.warmup, args.ref_warmup_budget)
-    steps, units, subs, dt = _oracle_run(sims, args.steps, args.ref_budget)
-    value = units / dt
-    spec = WORKLOADS[args.workload]
+    runs = 3
+    cb = time_oracle(args.workload, max(args.warmup, 1), args.ref_warmup_budget, runs,
+                     args.ref_budget / runs, max(1, -(-args.steps // runs)))
+    value = cb["value"]
+    ms_per_step = cb["seconds"] * 1000.0 / max(cb["frames"], 1)
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT,
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": dt * 1000.0 / max(steps, 1), "higher_is_better": True,
+        "ms_per_step": ms_per_step, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic (seeded scene generator, tests/scenes.py)",
-        "config": {"workload": args.workload, "description": spec["desc"], "particles": n,
-                   "scenes": len(sims), "grid": spec["grid_res"], "substeps": subs},
-        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
-                         "sample": f"{steps} of {args.steps} full steps ({subs} substeps) of {n} "
-                                   f"particles in {len(sims)} scene(s), {dt:.1f} s (time budget "
-                                   f"{args.ref_budget:.0f} s)"},
+        "config": workload_config(args.workload, cb["particles"], args.gpus),
+        "substeps_per_step": cb["substeps"] / max(cb["frames"], 1),
+        "cpu_baseline": {k: cb[k] for k in ("value", "unit", "cores", "cpu_model", "kind", "runs",
+                                             "run_values", "spread", "warmup_steps", "sample")},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
+
+
+def workload_config(workload: str, particles: int, world: int) -> dict:
+    """The `config` object of both arms' lines (identical keys and values for one workload)."""
+    spec = WORKLOADS[workload]
+    return {"workload": workload, "description": spec["desc"], "particles_per_gpu": particles,
+            "grid": spec["grid_res"],
+            "l2": "GPU arm: flushed (512 MiB device write) before every timed step",
+            "parallelism": f"replicas x{world}"}
 
 
 def run_batched(args, spec, rank: int, world: int, dist, local_rank: int) -> dict:
@@ -422,10 +464,11 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-extras", action="store_true",
                     help="skip e2e, roofline instrumentation and CPU baseline (profiling runs)")
-    ap.add_argument("--cpu-budget", type=float, default=15.0)
+    ap.add_argument("--cpu-budget", type=float, default=30.0,
+                    help="cpu_baseline: seconds for the warm-up and for each of the 3 timed runs x 3")
     ap.add_argument("--no-closure", action="store_true",
                     help="skip the learned-closure A/B on scenes with plastic materials")
-    ap.add_argument("--ref-budget", type=float, default=90.0,
+    ap.add_argument("--ref-budget", type=float, default=60.0,
                     help="--impl reference: seconds of timed CPU steps at most")
     ap.add_argument("--ref-warmup-budget", type=float, default=20.0)
     args = ap.parse_args()
@@ -457,11 +500,8 @@ def main():
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": r["ms_per_step"],
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
                 "data": "synthetic (seeded scene generator, tests/scenes.py)",
-                "config": {"workload": args.workload, "description": spec["desc"],
-                           "scenes": r["scenes"], "particles_per_gpu": r["particles"],
-                           "substeps_per_step_mean": r["substeps_per_step_mean"],
-                           "l2": "flushed (512 MiB write) before every timed step",
-                           "parallelism": f"replicas x{world}"},
+                "config": workload_config(args.workload, r["particles"], world),
+                "scenes": r["scenes"], "substeps_per_step_mean": r["substeps_per_step_mean"],
                 "clocks": r["clocks"], "roofline": r["roofline"], "autotune": r["autotune"],
             }
             if world == 1 and not args.no_extras:
@@ -550,6 +590,21 @@ def main():
             else "fallback 6.65 TB/s"}
         # where a substep's time goes (host-driven loop, CUDA events between the phases)
         extras["phases_us_per_substep"] = {k[:-3]: v / max(subs_i, 1) for k, v in phases.items()}
+        extras["phases_note"] = ("p2g and project read 0: the fused particle pass (k_particle) does "
+                                 "the projection and the P2G scatter of substep k+1 together with "
+                                 "the G2P and update of substep k, and is timed as g2p; density is "
+                                 "k_density (fluid scenes only); cfl is the controller")
+        if phases["density_us"] > 0.0:
+            # the density pass: reads x, material, C, mass (88 B of the fluid state are not
+            # needed), writes rho_dp, gathers 9 masses and scatters 9 stress pairs per particle
+            # (12 B per cell at 4 ppc -> 3 B)
+            d_us = phases["density_us"] / max(subs_i, 1)
+            d_bytes = K_DENSITY_BYTES * n_eff
+            d_ach = d_bytes / (d_us * 1e-6) / 1e9
+            extras["roofline_density"] = {
+                "kernel": "k_density (density gather + fluid stress scatter)", "bound": "hbm",
+                "achieved": d_ach, "peak": peak, "unit": "GB/s", "frac": d_ach / peak,
+                "traffic": None, "algorithmic_bytes_per_launch": d_bytes, "launch_us": d_us}
 
         # End to end through the C ABI with host buffers: upload the particle state from
         # pinned memory, step, read it back into a second pinned buffer, every step.  The
@@ -603,11 +658,8 @@ def main():
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic (seeded scene generator, tests/scenes.py)",
-            "config": {"workload": args.workload, "description": spec["desc"],
-                       "particles_per_gpu": n, "grid": spec["grid_res"],
-                       "substeps_per_step": substeps / args.steps,
-                       "l2": "flushed (512 MiB write) before every timed step",
-                       "parallelism": f"replicas x{world}"},
+            "config": workload_config(args.workload, n, world),
+            "substeps_per_step": substeps / args.steps,
             "gpu_launches": launches,
             "clocks": clock_info,
         }

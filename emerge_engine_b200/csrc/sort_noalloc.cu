@@ -8,6 +8,8 @@
 // kernel and stable radix sort over a fixed working array that lives in this
 // library's device image, so it allocates nothing.  The array bounds the input
 // size to EMERGE_SORT_NOALLOC_MAX positions.
+#include <cuda.h>  // CUcontext / CUresult types only; the driver is reached through the runtime
+
 #include <mutex>
 #include <string>
 
@@ -32,7 +34,43 @@ static __device__ __align__(256) unsigned char g_sort_scratch[kScratchBytes];
 
 constexpr int kMaxDevices = 64;
 std::mutex g_setup_mutex;
-void *g_scratch_ptr[kMaxDevices] = {};
+
+// Address of the array on one device, with the id of the context it was looked up in: a
+// context destroyed and created again (cudaDeviceReset) reloads the module, so the cached
+// address is only reused while the device's current context is the same one.
+struct ScratchEntry {
+    void *ptr;
+    unsigned long long ctx_id;
+};
+ScratchEntry g_scratch[kMaxDevices] = {};
+
+using CtxGetCurrentFn = CUresult (*)(CUcontext *);
+using CtxGetIdFn = CUresult (*)(CUcontext, unsigned long long *);
+
+// Id of the calling thread's current context (cuCtxGetId: unique over the process's life,
+// so a re-created context never repeats an old id).  False when there is no current context
+// yet or the driver does not provide the entry points; callers then look the address up.
+bool current_context_id(unsigned long long *id) {
+    static CtxGetCurrentFn get_current = nullptr;
+    static CtxGetIdFn get_id = nullptr;
+    static bool resolved = false;
+    if (!resolved) {  // under g_setup_mutex
+        void *f = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            get_current = reinterpret_cast<CtxGetCurrentFn>(f);
+        f = nullptr;
+        if (cudaGetDriverEntryPoint("cuCtxGetId", &f, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            get_id = reinterpret_cast<CtxGetIdFn>(f);
+        resolved = true;
+    }
+    if (!get_current || !get_id) return false;
+    CUcontext ctx = nullptr;
+    if (get_current(&ctx) != CUDA_SUCCESS || !ctx) return false;
+    return get_id(ctx, id) == CUDA_SUCCESS;
+}
 
 __global__ void k_copy_u32(const uint32_t *src, uint32_t *dst, int n) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -55,18 +93,23 @@ bool device_accessible(const void *p, int dev) {
     return a.type == cudaMemoryTypeDevice && a.device == dev;
 }
 
-// Address of the scratch array on the current device, looked up once per device.
+// Address of the scratch array on the current device, looked up once per device context.
 emerge_status scratch_for_device(int dev, void **out) {
     std::lock_guard<std::mutex> lock(g_setup_mutex);
-    if (!g_scratch_ptr[dev]) {
+    ScratchEntry &entry = g_scratch[dev];
+    unsigned long long id = 0;
+    if (!(entry.ptr && current_context_id(&id) && id == entry.ctx_id)) {
         void *p = nullptr;
         cudaError_t e = cudaGetSymbolAddress(&p, g_sort_scratch);
         if (e != cudaSuccess)
             return fail(EMERGE_ERR_CUDA,
                         std::string("cudaGetSymbolAddress(sort scratch): ") + cudaGetErrorString(e));
-        g_scratch_ptr[dev] = p;
+        // the lookup made the device's context current; 0 (never a valid id) forces a new
+        // lookup on the next call when the id cannot be read
+        entry.ptr = p;
+        entry.ctx_id = current_context_id(&id) ? id : 0ull;
     }
-    *out = g_scratch_ptr[dev];
+    *out = entry.ptr;
     return EMERGE_OK;
 }
 
@@ -90,6 +133,8 @@ extern "C" emerge_status emerge_cuda_sort_keys_noalloc(const float *xy_dev, uint
         return fail(EMERGE_ERR_INVALID_ARG,
                     "sort_keys_noalloc: null or misaligned buffer (xy needs 8-byte, keys/perm "
                     "4-byte alignment)");
+    // an error left pending by the caller's earlier work: not this call's failure
+    const cudaError_t pending = cudaPeekAtLastError();
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess)
@@ -119,7 +164,7 @@ extern "C" emerge_status emerge_cuda_sort_keys_noalloc(const float *xy_dev, uint
     int r = radix_sort_pairs(sc, ni, sort_key_bits(static_cast<int>(grid_res), key_mode), s);
     k_copy_u32<<<blocks, 256, 0, s>>>(sc.vals[r], perm_dev, ni);
     e = cudaPeekAtLastError();
-    if (e != cudaSuccess)
+    if (e != cudaSuccess && e != pending)
         return fail(EMERGE_ERR_CUDA, std::string("sort_keys_noalloc: launch: ") + cudaGetErrorString(e));
     return EMERGE_OK;
 }

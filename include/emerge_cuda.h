@@ -417,11 +417,21 @@ emerge_status emerge_cuda_sort_keys(const float *xy, uint64_t n, uint32_t grid_r
  *   stream    cudaStream_t as void* (NULL = the legacy default stream)
  * The library allocates nothing; it works in one fixed array of about 1 MiB inside its
  * device image, so n is limited to EMERGE_SORT_NOALLOC_MAX and a larger n returns
- * EMERGE_ERR_INVALID_ARG before any device work.  Nothing needs to start at zero (the
- * outputs need no initial contents; the working array is written before it is read).
+ * EMERGE_ERR_INVALID_ARG before any device work.  grid_res must lie in 1..32768 (the
+ * keys then fit in 30 bits) and key_mode be 0 or 1; other values return
+ * EMERGE_ERR_INVALID_ARG, also before any device work.  Nothing needs to start at zero
+ * (the outputs need no initial contents; the working array is written before it is read).
  * Returns once the work is enqueued; results are ready when the stream reaches it.
- * The first call on each device looks up the working array's address
- * (cudaGetSymbolAddress): make that first call before any stream capture begins.
+ * The first call on each device (and the first after that device's context was destroyed,
+ * e.g. by cudaDeviceReset) looks up the working array's address (cudaGetSymbolAddress):
+ * make that first call before any stream capture begins.  With CUDA's lazy module loading
+ * (the default since CUDA 12.2) that first call is also when the driver loads this part of
+ * the library's device image and reserves the fixed array, so a caller whose memory pool
+ * will reserve the whole device should make the first call before the pool does, or set
+ * CUDA_MODULE_LOADING=EAGER.
+ * Launch errors: an error that earlier, unrelated work left pending on the calling thread
+ * is not reported here as this call's failure and stays pending for its owner; a launch
+ * of this call that fails with that same error code cannot be told apart from it.
  * All calls on one device share the one working array, so calls whose work may overlap
  * in time (unordered streams, several host threads) race and corrupt each other's
  * results: order them on one stream or with events. */
