@@ -471,6 +471,10 @@ def main():
     ap.add_argument("--ref-budget", type=float, default=60.0,
                     help="--impl reference: seconds of timed CPU steps at most")
     ap.add_argument("--ref-warmup-budget", type=float, default=20.0)
+    ap.add_argument("--p2g-aggregate", type=int, default=None, choices=[0, 1, 2],
+                    help="EMERGE_OPT_P2G_AGGREGATE for the run (default: the library's)")
+    ap.add_argument("--skip", default="",
+                    help="comma list of parts to leave out: e2e, closure, cpu (roofline and phases stay)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3) if args.impl == "ours" else args.warmup
 
@@ -517,6 +521,10 @@ def main():
     build()
 
     sim = build_scene(Simulation, args.workload, device=local_rank)
+    if args.p2g_aggregate is not None:
+        from emerge_engine_b200.abi import OPT_P2G_AGGREGATE
+        sim.set_option(OPT_P2G_AGGREGATE, args.p2g_aggregate)
+    skip = set(filter(None, args.skip.split(",")))
     n = sim.particle_count()
     clocks = ClockSampler(local_rank)
     clocks.start()
@@ -606,6 +614,7 @@ def main():
                 "achieved": d_ach, "peak": peak, "unit": "GB/s", "frac": d_ach / peak,
                 "traffic": None, "algorithmic_bytes_per_launch": d_bytes, "launch_us": d_us}
 
+    if not args.no_extras and "e2e" not in skip:
         # End to end through the C ABI with host buffers: upload the particle state from
         # pinned memory, step, read it back into a second pinned buffer, every step.  The
         # readback is asynchronous (its own stream), so step k's device-to-host copy overlaps
@@ -647,9 +656,10 @@ def main():
                          "steps": e2e_steps, "timing": "host wall clock around the C-ABI calls",
                          "readback": "emerge_cuda_read_particles_async (copy stream; overlaps "
                                      "the next step's upload)"}
-        if spec["material"] == "DP+Snow+NACC" and not args.no_closure:
+    if not args.no_extras:
+        if spec["material"] == "DP+Snow+NACC" and not args.no_closure and "closure" not in skip:
             extras["learned_closure"] = closure_ab(sim, n, args.steps, value)
-        if world == 1 and rank == 0:
+        if world == 1 and rank == 0 and "cpu" not in skip:
             extras["cpu_baseline"] = cpu_baseline(args.workload, args.cpu_budget)
 
     if rank == 0:

@@ -533,8 +533,10 @@ emerge_status emerge_cuda_batch_set_option(emerge_batch *b, int option, int64_t 
         if (value < 0) return static_cast<emerge_status>(b->fail(EMERGE_ERR_INVALID_ARG, "sort interval < 0"));
         b->sort_interval = value;
         return EMERGE_OK;
-    case EMERGE_OPT_P2G_AGGREGATE:
-        b->aggregate = value != 0;
+    case EMERGE_OPT_P2G_AGGREGATE:  // kernel codes: 1 warp segments, 3 lane pairs / quads
+        if (value < 0 || value > 2)
+            return static_cast<emerge_status>(b->fail(EMERGE_ERR_INVALID_ARG, "P2G aggregation mode must be 0, 1 or 2"));
+        b->aggregate = value == 2 ? 3 : static_cast<int>(value);
         b->graph_dirty = true;
         return EMERGE_OK;
     default: return static_cast<emerge_status>(b->fail(EMERGE_ERR_INVALID_ARG, "option not available for batches"));

@@ -562,12 +562,105 @@ __device__ __forceinline__ void scatter_cells_aggregated(const GridView &g, cons
     }
 }
 
+// Lane-pair aggregation into the total: lanes 2m and 2m + 1 whose particles share a base
+// cell (neighbours in tile-sort order, so usually in one cell) add their contributions with
+// one shuffle per value and the even lane issues the reduction; where all four lanes of an
+// aligned quad share it, a second shuffle folds the two pairs together.  A reduction in L2
+// costs about the same however many lanes of a warp target one cell, so halving (quartering)
+// the lanes that issue them halves (quarters) the scatter's L2 work, for 5 shuffles per cell.
+// Every lane of the warp calls this (inactive lanes add nothing).
+template <int SC>
+__device__ __forceinline__ void scatter_cells_pairs(const GridView &g, const ScatterPlan &pl, bool active,
+                                                    bool do_ma, bool do_s) {
+    const unsigned full = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    const QW &w = pl.w;
+    // a unique key per inactive lane; active keys are the base cell (packed, any int range)
+    const long long key = active ? (static_cast<long long>(w.bx) << 32) | static_cast<uint32_t>(w.by)
+                                 : -1ll - lane;
+    const bool pair = __shfl_xor_sync(full, key, 1) == key;
+    const bool quad = pair && __shfl_xor_sync(full, pair ? key : -100ll - lane, 2) == key;
+    const bool any_pair = __any_sync(full, pair), any_quad = __any_sync(full, quad);
+    const bool issue = active && (!pair || ((lane & 1) == 0 && (!quad || (lane & 2) == 0)));
+    // channels issued by this lane's group: mass + momentum if any member scatters them,
+    // stress likewise (a fluid particle in the density mode pairs with a solid one)
+    const bool ma_self = SC == SC_MA || (SC == SC_BOTH && active && do_ma);
+    const bool s_self = SC == SC_S || (SC == SC_BOTH && active && do_s);
+    int flags = (ma_self ? 1 : 0) | (s_self ? 2 : 0) | (ma_self ? 4 : 0);  // bit 2+: mass-scatter count
+    if (SC == SC_BOTH) {
+        if (any_pair) {
+            const int o = __shfl_xor_sync(full, flags, 1);
+            if (pair) flags = ((flags | o) & 3) | (((flags >> 2) + (o >> 2)) << 2);
+        }
+        if (any_quad) {
+            const int o = __shfl_xor_sync(full, flags, 2);
+            if (quad) flags = ((flags | o) & 3) | (((flags >> 2) + (o >> 2)) << 2);
+        }
+    } else {
+        flags = SC == SC_MA ? (1 | ((quad ? 4 : (pair ? 2 : 1)) << 2)) : 2;
+    }
+    const bool do_a = SC != SC_S && (flags & 1), do_st = SC != SC_MA && (flags & 2);
+    const float count = static_cast<float>(flags >> 2);
+    const bool inside = stencil_inside(w.bx, w.by, g.res);
+    int yp[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) yp[k] = cell_y_part(w.by + k - 1);
+#pragma unroll
+    for (int gx = 0; gx < 3; ++gx) {
+        const int xp = cell_x_part(w.bx + gx - 1, g.tpd);
+        const float4 r = f4step(pl.q, pl.sx, gx);
+        const float wm = w.wx[gx] * pl.m;
+#pragma unroll
+        for (int gy = 0; gy < 3; ++gy) {
+            const float4 t = f4step(r, pl.sy, gy);
+            const float wt = active ? w.wx[gx] * w.wy[gy] : 0.0f;
+            float m = active ? wm * w.wy[gy] : 0.0f, ax = wt * t.x, ay = wt * t.y, sx = wt * t.z, sy = wt * t.w;
+            if (any_pair) {
+                float o0 = 0.0f, o1 = 0.0f, o2 = 0.0f, o3 = 0.0f, o4 = 0.0f;
+                if (SC != SC_S) {
+                    o0 = __shfl_xor_sync(full, m, 1);
+                    o1 = __shfl_xor_sync(full, ax, 1);
+                    o2 = __shfl_xor_sync(full, ay, 1);
+                }
+                if (SC != SC_MA) {
+                    o3 = __shfl_xor_sync(full, sx, 1);
+                    o4 = __shfl_xor_sync(full, sy, 1);
+                }
+                if (pair) { m += o0; ax += o1; ay += o2; sx += o3; sy += o4; }
+            }
+            if (any_quad) {
+                float o0 = 0.0f, o1 = 0.0f, o2 = 0.0f, o3 = 0.0f, o4 = 0.0f;
+                if (SC != SC_S) {
+                    o0 = __shfl_xor_sync(full, m, 2);
+                    o1 = __shfl_xor_sync(full, ax, 2);
+                    o2 = __shfl_xor_sync(full, ay, 2);
+                }
+                if (SC != SC_MA) {
+                    o3 = __shfl_xor_sync(full, sx, 2);
+                    o4 = __shfl_xor_sync(full, sy, 2);
+                }
+                if (quad) { m += o0; ax += o1; ay += o2; sx += o3; sy += o4; }
+            }
+            if (!issue) continue;
+            if (!inside && !in_domain(w.bx + gx - 1, w.by + gy - 1, g.res)) continue;
+            const int ci = xp + yp[gy];
+            if (do_a) red_add_v4(&g.acc_a[ci], m, ax, ay, count);
+            if (do_st) red_add_v2(&g.acc_s[ci], sx, sy);
+        }
+    }
+}
+
 template <int SC>
 __device__ __forceinline__ void scatter_particle(const GridView &g, const Payload &p, bool valid,
                                                  int aggregate) {
     const bool active = valid && (p.do_ma || p.do_s);
     ScatterPlan pl{};
     if (active) pl = make_plan<SC>(p);
+    if (aggregate == 3) {  // lane pairs / quads into the total (no multi-field sums)
+        scatter_cells_pairs<SC>(g, pl, active, p.do_ma, p.do_s);
+        if (active) mark_tiles(g, pl.w.bx, pl.w.by);
+        return;
+    }
     // Exclusive field sums: a field particle's contributions go to its field's sums only, and
     // the grid update adds them to the total.  target: 0 the total, k + 1 field k.
     float4 *A = g.acc_a;
@@ -1059,7 +1152,7 @@ __device__ __forceinline__ void particle_pass(const ParticleKernelArgs &a) {
         }
     }
     // aggregate mode 2 (per-warp targets) only where exclusive field sums can occur
-    const int aggregate = HAS_MODEL(MASK, M_EXTRAS_BIT) ? a.aggregate : (a.aggregate ? 1 : 0);
+    const int aggregate = HAS_MODEL(MASK, M_EXTRAS_BIT) || a.aggregate == 3 ? a.aggregate : (a.aggregate ? 1 : 0);
     if (core_mask(MASK) == MASK_FLUID && density_mode)
         scatter_particle<SC_MA>(g, pl, valid, aggregate);
     else
@@ -1200,7 +1293,7 @@ __device__ __forceinline__ void density_pass(const DensityKernelArgs &a) {
         }
     }
     scatter_particle<SC_S>(g, pl, valid,
-                           HAS_MODEL(MASK, M_EXTRAS_BIT) ? a.aggregate : (a.aggregate ? 1 : 0));
+                           HAS_MODEL(MASK, M_EXTRAS_BIT) || a.aggregate == 3 ? a.aggregate : (a.aggregate ? 1 : 0));
 }
 
 // Launchers of the fast path's kernels (fast_kernels.cu).
@@ -1228,7 +1321,9 @@ inline void fill_common(Args &a, const StepLaunch &L, const LoadFlagsHost &lfh) 
     a.lf.temperature = lfh.temperature;
     a.lf.activation = lfh.activation;
     a.lf.pinned = lfh.pinned;
-    a.aggregate = L.use_window ? (L.cfg.mf_excl ? 2 : 1) : 0;
+    // EMERGE_OPT_P2G_AGGREGATE: 1 warp segments (per-warp targets with exclusive field sums),
+    // 2 lane pairs / quads (scenes without multi-field sums; others use the segments)
+    a.aggregate = L.use_window == 0 ? 0 : (L.use_window == 2 && !L.cfg.mf_fast ? 3 : (L.cfg.mf_excl ? 2 : 1));
 }
 
 }  // namespace emerge

@@ -1736,7 +1736,9 @@ emerge_status emerge_cuda_set_option(emerge_sim *s, int option, int64_t value) {
         s->sort_interval = value;
         return EMERGE_OK;
     case EMERGE_OPT_P2G_AGGREGATE:
-        s->use_window = value != 0;
+        if (value < 0 || value > 2)
+            return static_cast<emerge_status>(s->fail(EMERGE_ERR_INVALID_ARG, "P2G aggregation mode must be 0, 1 or 2"));
+        s->use_window = static_cast<int>(value);
         s->graph_dirty = true;
         return EMERGE_OK;
     case EMERGE_OPT_DETERMINISTIC: {

@@ -584,7 +584,7 @@ void launch_density_pass(const StepLaunch &L, const LoadFlagsHost &lfh) {
     // The density pass scatters two stress components per cell: there the warp-aggregated
     // reductions cost fewer L2 atomics than they add shuffles (dam break 1M: 47.7 -> 42.7 us
     // per launch), unlike the particle pass's mass + momentum scatter (74.5 -> 76.1 us).
-    a.aggregate = L.cfg.mf_excl ? 2 : 1;
+    a.aggregate = L.use_window == 2 && !L.cfg.mf_fast ? 3 : (L.cfg.mf_excl ? 2 : 1);
     launch_density_pass_fast(a, L.model_mask, L.stream);
 }
 

@@ -25,9 +25,20 @@ from tests import scenes
 
 pytestmark = pytest.mark.gpu
 
+class PairsSimulation(Simulation):
+    """The fast path with lane-pair / quad aggregation of the P2G reductions
+    (EMERGE_OPT_P2G_AGGREGATE = 2)."""
+
+    def __init__(self, *a, **kw):
+        super().__init__(*a, **kw)
+        from emerge_engine_b200.abi import OPT_P2G_AGGREGATE
+        self.set_option(OPT_P2G_AGGREGATE, 2)
+
+
 MODES = {
     "reference_order": dict(cls=DeterministicSimulation, x_tol=1e-5, v_tol=1e-5, v_p99=1e-5),
     "fast": dict(cls=Simulation, x_tol=1e-5, v_tol=5e-3, v_p99=1e-4),
+    "fast_pairs": dict(cls=PairsSimulation, x_tol=1e-5, v_tol=5e-3, v_p99=1e-4),
 }
 
 
