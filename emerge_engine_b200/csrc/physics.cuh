@@ -55,9 +55,26 @@ EM_HD float fclampf(float x, float lo, float hi) {
     if (x > hi) x = hi;
     return x;
 }
+// IEEE-rounded square root and division whatever the translation unit's -prec-sqrt /
+// -prec-div flags.  The fast path is compiled with approximate (2-ulp) division and square
+// root; the SVD, the polar decomposition and the return mappings use these instead, because
+// their yield decisions amplify a last-bit difference over tens of substeps (measured on the
+// 160k-particle granular scene over one frame: per-particle velocity error against the
+// oracle, median 3.3e-5 with the approximate operations there and 2.2e-7 with these).  In
+// the reference-order translation units (IEEE flags) they are the plain operators.
+#ifdef __CUDA_ARCH__
+EM_HD float esqrt(float x) { return __fsqrt_rn(x); }
+EM_HD float ediv(float a, float b) { return __fdiv_rn(a, b); }
+#else
+EM_HD float esqrt(float x) { return sqrtf(x); }
+EM_HD float ediv(float a, float b) { return a / b; }
+#endif
+EM_HD float evlen(float2 a) { return esqrt(vdot(a, a)); }
+EM_HD float2 evdivs(float2 a, float s) { return v2(ediv(a.x, s), ediv(a.y, s)); }
+
 // glam normalize_or_zero
 EM_HD float2 normalize_or_zero(float2 a) {
-    float rcp = 1.0f / vlen(a);
+    float rcp = ediv(1.0f, evlen(a));
     if (isfinite(rcp) && rcp > 0.0f) return vmuls(a, rcp);
     return v2(0.0f, 0.0f);
 }
@@ -133,8 +150,8 @@ EM_HD QW quadratic_weights(float2 p) {
 // ---------------------------------------------------------------- svd / polar
 EM_HD float2 orthogonal_complement(float2 v) {  // materials/svd.rs:81-85
     float2 perp = v2(-v.y, v.x);
-    float len = vlen(perp);
-    if (len > 1e-10f) return vdivs(perp, len);
+    float len = evlen(perp);
+    if (len > 1e-10f) return evdivs(perp, len);
     return v2(1.0f, 0.0f);
 }
 
@@ -147,23 +164,23 @@ EM_HD void svd2(M2 f, M2 &u_out, float2 &sigma_out, M2 &vt_out) {
     float c11 = f01 * f01 + f11 * f11;
     float mean = (c00 + c11) * 0.5f;
     float half_diff = (c00 - c11) * 0.5f;
-    float disc = sqrtf(half_diff * half_diff + c01 * c01);
+    float disc = esqrt(half_diff * half_diff + c01 * c01);
     float lambda1 = mean + disc;
     float lambda2 = mean - disc;
     float2 v1;
     if (fabsf(c01) > 1e-10f * fmaxf(c00 + c11, 1e-30f)) {
         float2 raw = v2(c01, lambda1 - c00);
-        v1 = vdivs(raw, vlen(raw));
+        v1 = evdivs(raw, evlen(raw));
     } else {
         v1 = (c00 >= c11) ? v2(1.0f, 0.0f) : v2(0.0f, 1.0f);
     }
     float2 vv2 = v2(-v1.y, v1.x);
     M2 vt = mtrans(m2(v1, vv2));
-    float2 sigma = v2(sqrtf(fmaxf(lambda1, 0.0f)), sqrtf(fmaxf(lambda2, 0.0f)));
+    float2 sigma = v2(esqrt(fmaxf(lambda1, 0.0f)), esqrt(fmaxf(lambda2, 0.0f)));
     float2 fv1 = mv(f, v1);
     float2 fv2 = mv(f, vv2);
-    float2 u1 = (sigma.x > 1e-10f) ? vdivs(fv1, sigma.x) : orthogonal_complement(fv2);
-    float2 u2 = (sigma.y > 1e-10f) ? vdivs(fv2, sigma.y) : orthogonal_complement(u1);
+    float2 u1 = (sigma.x > 1e-10f) ? evdivs(fv1, sigma.x) : orthogonal_complement(fv2);
+    float2 u2 = (sigma.y > 1e-10f) ? evdivs(fv2, sigma.y) : orthogonal_complement(u1);
     M2 u = m2(u1, u2);
     if (mdet(u) < 0.0f) {
         u.ya = v2(-u.ya.x, -u.ya.y);
@@ -178,8 +195,8 @@ EM_HD void svd2(M2 f, M2 &u_out, float2 &sigma_out, M2 &vt_out) {
 EM_HD M2 polar(M2 f) {
     float x = f.xa.x + f.ya.y;
     float y = f.xa.y - f.ya.x;
-    float norm = sqrtf(x * x + y * y);
-    if (norm > F32_EPS) return m2(vdivs(v2(x, y), norm), vdivs(v2(-y, x), norm));
+    float norm = esqrt(x * x + y * y);
+    if (norm > F32_EPS) return m2(evdivs(v2(x, y), norm), evdivs(v2(-y, x), norm));
     return mident();
 }
 
@@ -210,7 +227,7 @@ EM_HD float nacc_kappa(const MatP &m) { return m.lambda + m.mu; }  // inverse of
 EM_HD float dp_alpha(const MatP &m, float q, bool pr) {
     float phi = m.dp_h0 + (m.dp_h1 * q - m.dp_h3) * em_exp(-m.dp_h2 * q, pr);
     float s = em_sin(phi, pr);
-    return sqrtf(2.0f / 3.0f) * (2.0f * s) / (3.0f - s);
+    return ediv(sqrtf(2.0f / 3.0f) * (2.0f * s), 3.0f - s);
 }
 
 // DruckerPragerMaterial::project (sand.rs:156-194); cohesion in stretch_limit (sand.rs:335)
@@ -220,18 +237,18 @@ EM_HD bool dp_project(const MatP &m, float2 sigma_in, float lvs, float q, float2
     float2 eps = v2(em_log(sigma.x, pr) + lvs * 0.5f, em_log(sigma.y, pr) + lvs * 0.5f);
     float trace = eps.x + eps.y;
     float2 dev = vsub(eps, splat(trace * 0.5f));
-    float dev_norm = vlen(dev);
+    float dev_norm = evlen(dev);
     if (dev_norm == 0.0f || trace > 0.0f) {
         out = v2(1.0f, 1.0f);
         dq = dev_norm;
         return true;
     }
-    float ratio = (m.lambda + m.mu) / m.mu;
+    float ratio = ediv(m.lambda + m.mu, m.mu);
     float alpha = dp_alpha(m, q, pr);
-    float cohesion_term = m.stretch_limit / (2.0f * m.mu);
+    float cohesion_term = ediv(m.stretch_limit, 2.0f * m.mu);
     float gamma = dev_norm + ratio * trace * alpha - cohesion_term;
     if (gamma <= 0.0f) return false;
-    float2 h = vsub(eps, svmul(gamma, vdivs(dev, dev_norm)));
+    float2 h = vsub(eps, svmul(gamma, evdivs(dev, dev_norm)));
     out = v2(em_exp(h.x, pr), em_exp(h.y, pr));
     dq = gamma;
     return true;
@@ -282,8 +299,8 @@ EM_HD void nacc_project(const MatP &m, M2 f, float alpha, M2 &f_out, float &alph
     float sv_sq_trace = sv_sq.x + sv_sq.y;
     float p0 = kappa * (1.0e-5f + em_sinh(xi * fmaxf(-alpha, 0.0f), pr));
     float j_e_tr = fmaxf(sv.x * sv.y, 1.0e-6f);
-    float2 s_tr = svmul(m.mu * (1.0f / j_e_tr), vsub(sv_sq, splat(sv_sq_trace * 0.5f)));
-    float psi_kappa = kappa * 0.5f * (j_e_tr - 1.0f / j_e_tr);
+    float2 s_tr = svmul(m.mu * ediv(1.0f, j_e_tr), vsub(sv_sq, splat(sv_sq_trace * 0.5f)));
+    float psi_kappa = kappa * 0.5f * (j_e_tr - ediv(1.0f, j_e_tr));
     float p_tr = -psi_kappa * j_e_tr;
     if (p_tr > p0) {
         float j_n1 = sqrtf(fmaxf(-2.0f * p0 / kappa + 1.0f, 1.0e-8f));
@@ -326,9 +343,9 @@ EM_HD void nacc_project(const MatP &m, M2 f, float alpha, M2 &f_out, float &alph
         float j_e_x = sqrtf(fmaxf(fabsf(-2.0f * p_x / kappa + 1.0f), 1.0e-8f));
         if (j_e_x > 1.0e-4f) alpha += em_log(j_e_tr / j_e_x, pr);
     }
-    float scale = sqrtf(fmaxf(-y1 / fmaxf(y0, 1.0e-10f), 0.0f)) * (j_e_tr / m.mu);
+    float scale = esqrt(fmaxf(ediv(-y1, fmaxf(y0, 1.0e-10f)), 0.0f)) * ediv(j_e_tr, m.mu);
     float2 b_n1 = vadd(svmul(scale, normalize_or_zero(s_tr)), splat(sv_sq_trace / 2.0f));
-    float2 sv_new = v2(sqrtf(fmaxf(b_n1.x, 1.0e-8f)), sqrtf(fmaxf(b_n1.y, 1.0e-8f)));
+    float2 sv_new = v2(esqrt(fmaxf(b_n1.x, 1.0e-8f)), esqrt(fmaxf(b_n1.y, 1.0e-8f)));
     f_out = reconstruct(u, sv_new, vt);
     alpha_out = alpha;
 }
@@ -657,7 +674,7 @@ EM_HD void sync_volume_density(PState &p) {
     float j = fmaxf(mdet(p.f), MIN_J);
     float v = fmaxf(p.v0 * j, 1.0e-6f);
     p.vol = v;
-    p.rho = p.mass / v;
+    p.rho = ediv(p.mass, v);
 }
 
 // DP update after the return map decision (sand.rs:258-318).
@@ -679,7 +696,7 @@ EM_HD void dp_finish(const MatP &m, PState &p, M2 u, float2 sigma, M2 vt, bool p
     new_sigma = vabs2(new_sigma);
     float j_new = new_sigma.x * new_sigma.y;
     if (j_new < m.volume_ratio_min)
-        new_sigma = vmuls(new_sigma, sqrtf(m.volume_ratio_min / fmaxf(j_new, 1e-6f)));
+        new_sigma = vmuls(new_sigma, esqrt(ediv(m.volume_ratio_min, fmaxf(j_new, 1e-6f))));
     p.f = mm(mm(u, mdiag(new_sigma)), vt);
     sync_volume_density(p);
 }
@@ -733,7 +750,7 @@ EM_HD void update_particle(const MatP &m, PState &p, float dt, bool pr) {
         svd2(f_trial, u, sigma, vt);
         float lo = 1.0f - m.compression_limit, hi = 1.0f + m.stretch_limit;
         float2 sigma_c = v2(fclampf(sigma.x, lo, hi), fclampf(sigma.y, lo, hi));
-        float jp_new = p.jp * (sigma.x * sigma.y) / (sigma_c.x * sigma_c.y);
+        float jp_new = ediv(p.jp * (sigma.x * sigma.y), sigma_c.x * sigma_c.y);
         p.jp = fclampf(jp_new, m.volume_ratio_min, m.volume_ratio_max);
         p.h = fclampf(em_exp(m.hardening_exponent * (1.0f - p.jp), pr), 0.1f, 7.0f);
         p.f = mm(mm(u, mdiag(sigma_c)), vt);
