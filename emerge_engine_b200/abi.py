@@ -151,7 +151,8 @@ class ClosureStatsC(Structure):
     """`emerge_closure_stats` (include/emerge_cuda.h)."""
     _fields_ = [("smooth", c_uint64), ("net", c_uint64), ("hull_fallback", c_uint64),
                 ("judged", c_uint64), ("logged", c_uint64 * 2), ("err_mean", ctypes.c_double),
-                ("err_max", c_float), ("pad_", c_uint32)]
+                ("err_max", c_float), ("pad_", c_uint32), ("judge_replaced", c_uint64),
+                ("err_p50", c_float), ("err_p99", c_float)]
 
 
 class ClosureTrainConfigC(Structure):
@@ -227,6 +228,7 @@ ABI_FUNCTIONS = [
                                           POINTER(ClosureTrainReportC)]),
     ("emerge_cuda_closure_enable", c_int, [SIM, c_int, c_uint32]),
     ("emerge_cuda_closure_stats", c_int, [SIM, POINTER(ClosureStatsC), c_int]),
+    ("emerge_cuda_closure_set_mode", c_int, [SIM, c_int, c_float]),
     ("emerge_cuda_closure_get_params", c_int, [SIM, c_int, c_void_p, c_void_p]),
     ("emerge_cuda_closure_get_log", c_int, [SIM, c_int, c_void_p, c_void_p, c_uint64, POINTER(c_uint64)]),
     ("emerge_cuda_closure_set_params", c_int, [SIM, c_int, c_void_p, c_void_p, c_void_p]),
@@ -234,6 +236,7 @@ ABI_FUNCTIONS = [
     ("emerge_cuda_mlp_adam", c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_uint32, c_uint32,
                                      c_float, c_float, c_float, c_float]),
     ("emerge_cuda_mlp_infer_bf16", c_int, [c_void_p, c_void_p, c_uint32, c_void_p]),
+    ("emerge_cuda_mlp_infer_tc", c_int, [c_void_p, c_void_p, c_uint32, c_void_p]),
     ("emerge_cuda_batch_create", c_int, [POINTER(c_void_p), c_uint32, POINTER(c_void_p)]),
     ("emerge_cuda_batch_destroy", c_int, [c_void_p]),
     ("emerge_cuda_batch_last_error", c_char_p, [c_void_p]),

@@ -124,6 +124,23 @@ __global__ void k_pack_net(const float *P, ClosureNet *net) {
     }
 }
 
+// Packs the tcgen05 operand form (closure.cuh): one thread per BF16 element of W1^T
+// (64 x 16), W2^T, W3^T (64 x 64) and W4^T (16 x 64); padding is zero.
+__global__ void k_pack_tc(const float *P, ClosureNet *net) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    constexpr int E1 = CL_H * CL_TC_K1, E2 = CL_H * CL_H, E4 = CL_TC_N4 * CL_H;
+    if (t >= E1 + 2 * E2 + E4) return;
+    int layer, n, k, kdim, off;
+    if (t < E1) { layer = 0; n = t / CL_TC_K1; k = t % CL_TC_K1; kdim = CL_TC_K1; off = CL_TC_OFF_L1; }
+    else if (t < E1 + E2) { layer = 1; n = (t - E1) / CL_H; k = (t - E1) % CL_H; kdim = CL_H; off = CL_TC_OFF_L2; }
+    else if (t < E1 + 2 * E2) { layer = 2; n = (t - E1 - E2) / CL_H; k = (t - E1 - E2) % CL_H; kdim = CL_H; off = CL_TC_OFF_L3; }
+    else { layer = 3; n = (t - E1 - 2 * E2) / CL_H; k = (t - E1 - 2 * E2) % CL_H; kdim = CL_H; off = CL_TC_OFF_L4; }
+    const int K = layer == 0 ? CL_IN : CL_H, N = layer == 3 ? CL_OUT : CL_H;
+    const float *W = P + (layer == 0 ? CL_OFF_W1 : layer == 1 ? CL_OFF_W2 : layer == 2 ? CL_OFF_W3 : CL_OFF_W4);
+    const float v = (k < K && n < N) ? W[k * N + n] : 0.0f;  // W[k][n]: row = input
+    *reinterpret_cast<__nv_bfloat16 *>(net->tc + off + km_offset(n, k, kdim)) = __float2bfloat16_rn(v);
+}
+
 // Tensor-core inference of normalised inputs (test hook and validation).
 __global__ void k_infer(const ClosureNet *net, const float *x, int n, float *y) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -242,16 +259,25 @@ struct ClosureHost {
     DevBuf nets, stats;
     DevBuf log_x[CL_NMODELS], log_t[CL_NMODELS];
     DevBuf params[CL_NMODELS];
+    DevBuf queue;              // CL_NMODELS queues of queue_cap slot indices (deferred mode)
+    size_t queue_cap = 0;
     unsigned long long log_cap = 0;
     uint32_t log_stride = 1, judge_stride = 64;
     int infer = 0, log = 0;
+    int defer = 1;
+    float judge_bar = 1e-3f;
     std::vector<float> norm[CL_NMODELS];  // in_shift[6] in_scale[6] out_shift[3] out_scale[3]
 };
 
-ClosureArgs closure_args(const ClosureHost *c) {
+ClosureArgs closure_args(const ClosureHost *c, size_t n) {
     ClosureArgs a;
     std::memset(&a, 0, sizeof(a));
     if (!c || !c->nets.p) return a;
+    // deferred evaluation needs queues for every particle (re-enable after adding particles)
+    a.defer = c->infer && c->defer && c->queue.p && c->queue_cap >= n ? 1 : 0;
+    for (int m = 0; m < CL_NMODELS; ++m)
+        a.queue[m] = a.defer ? c->queue.as<uint32_t>() + m * c->queue_cap : nullptr;
+    a.judge_bar = c->judge_bar;
     a.nets = c->nets.as<ClosureNet>();
     a.stats = c->stats.as<ClosureStats>();
     for (int m = 0; m < CL_NMODELS; ++m) {
@@ -287,6 +313,7 @@ static emerge_status install_net(emerge_sim *s, ClosureHost *c, int model, const
                                  const float *norm, const float *hull, cudaStream_t st) {
     ClosureNet *net = c->nets.as<ClosureNet>() + model;
     k_pack_net<<<nblk(CL_FRAGS * 32), 256, 0, st>>>(P_dev, net);
+    k_pack_tc<<<nblk(CL_H * CL_TC_K1 + 2 * CL_H * CL_H + CL_TC_N4 * CL_H), 256, 0, st>>>(P_dev, net);
     struct Tail {
         float in_shift[8], in_scale[8], out_shift[4], out_scale[4], hull_lo[8], hull_hi[8];
         int ready, pad_[3];
@@ -349,6 +376,25 @@ emerge_status emerge_cuda_closure_enable(emerge_sim *s, int on, uint32_t judge_s
     if (st != EMERGE_OK) return st;
     c->infer = on ? 1 : 0;
     c->judge_stride = judge_stride;
+    const size_t cap = sim_capacity(s);
+    if (on && c->defer && c->queue_cap < cap) {  // queues for the deferred mode
+        c->queue_cap = 0;
+        if (c->queue.alloc(CL_NMODELS * cap * sizeof(uint32_t)) != cudaSuccess)
+            return sim_fail(s, EMERGE_ERR_OOM, "closure: queue allocation failed");
+        c->queue_cap = cap;
+    }
+    sim_invalidate_graph(s);
+    return EMERGE_OK;
+}
+
+emerge_status emerge_cuda_closure_set_mode(emerge_sim *s, int defer, float judge_bar) {
+    if (!s || !(judge_bar >= 0.0f)) return EMERGE_ERR_INVALID_ARG;
+    ClosureHost *&c = sim_closure(s);
+    emerge_status st = ensure_closure(s, c);
+    if (st != EMERGE_OK) return st;
+    c->defer = defer ? 1 : 0;
+    c->judge_bar = judge_bar;
+    if (c->infer) return emerge_cuda_closure_enable(s, 1, c->judge_stride);  // (re)sizes the queues
     sim_invalidate_graph(s);
     return EMERGE_OK;
 }
@@ -371,6 +417,23 @@ emerge_status emerge_cuda_closure_stats(emerge_sim *s, emerge_closure_stats *out
     out->err_mean = h.judged ? h.err_sum / static_cast<double>(h.judged) : 0.0;
     uint32_t bits = h.err_max_bits;
     std::memcpy(&out->err_max, &bits, sizeof(float));
+    out->judge_replaced = h.judge_replaced;
+    {  // percentiles from the quarter-decade bins (upper bin edge)
+        unsigned long long total = 0ull;
+        for (int b = 0; b < CL_ERR_BINS; ++b) total += h.err_hist[b];
+        auto pct = [&](double q) -> float {
+            if (!total) return 0.0f;
+            unsigned long long acc = 0ull;
+            for (int b = 0; b < CL_ERR_BINS; ++b) {
+                acc += h.err_hist[b];
+                if (static_cast<double>(acc) >= q * static_cast<double>(total))
+                    return static_cast<float>(std::pow(10.0, (b + 1) / 4.0 - 8.0));
+            }
+            return static_cast<float>(std::pow(10.0, CL_ERR_BINS / 4.0 - 8.0));
+        };
+        out->err_p50 = pct(0.5);
+        out->err_p99 = pct(0.99);
+    }
     if (reset) {
         ClosureStats z;
         std::memset(&z, 0, sizeof(z));
@@ -634,6 +697,31 @@ emerge_status emerge_cuda_mlp_infer_bf16(const float *params, const float *x, ui
     k_infer<<<nblk(n), 256>>>(dNet.as<ClosureNet>(), dX.as<float>(), static_cast<int>(n), dY.as<float>());
     if (cudaMemcpy(y, dY.p, static_cast<size_t>(n) * CL_OUT * sizeof(float), cudaMemcpyDeviceToHost) != cudaSuccess)
         return EMERGE_ERR_CUDA;
+    return cudaGetLastError() == cudaSuccess ? EMERGE_OK : EMERGE_ERR_CUDA;
+}
+
+emerge_status emerge_cuda_mlp_infer_tc(const float *params, const float *x, uint32_t n, float *y) {
+    if (!params || !x || !y || n == 0) return EMERGE_ERR_INVALID_ARG;
+    DevBuf dP, dNet, dX, dY, dErr;
+    if (dP.alloc(CL_NPARAMS * sizeof(float)) != cudaSuccess || dNet.alloc(sizeof(ClosureNet)) != cudaSuccess ||
+        dX.alloc(static_cast<size_t>(n) * CL_IN * sizeof(float)) != cudaSuccess ||
+        dY.alloc(static_cast<size_t>(n) * CL_OUT * sizeof(float)) != cudaSuccess ||
+        dErr.alloc(sizeof(uint32_t)) != cudaSuccess)
+        return EMERGE_ERR_OOM;
+    cudaMemcpy(dP.p, params, CL_NPARAMS * sizeof(float), cudaMemcpyHostToDevice);
+    cudaMemcpy(dX.p, x, static_cast<size_t>(n) * CL_IN * sizeof(float), cudaMemcpyHostToDevice);
+    cudaMemset(dNet.p, 0, sizeof(ClosureNet));
+    cudaMemset(dErr.p, 0, sizeof(uint32_t));
+    k_pack_net<<<nblk(CL_FRAGS * 32), 256>>>(dP.as<float>(), dNet.as<ClosureNet>());
+    k_pack_tc<<<nblk(CL_H * CL_TC_K1 + 2 * CL_H * CL_H + CL_TC_N4 * CL_H), 256>>>(dP.as<float>(), dNet.as<ClosureNet>());
+    if (launch_mlp_tiles(dNet.as<ClosureNet>(), dX.as<float>(), static_cast<int>(n), dY.as<float>(),
+                         dErr.as<uint32_t>(), nullptr) != cudaSuccess)
+        return EMERGE_ERR_CUDA;
+    uint32_t err = 0u;
+    if (cudaMemcpy(y, dY.p, static_cast<size_t>(n) * CL_OUT * sizeof(float), cudaMemcpyDeviceToHost) != cudaSuccess ||
+        cudaMemcpy(&err, dErr.p, sizeof(uint32_t), cudaMemcpyDeviceToHost) != cudaSuccess)
+        return EMERGE_ERR_CUDA;
+    if (err) return EMERGE_ERR_TIMEOUT;
     return cudaGetLastError() == cudaSuccess ? EMERGE_OK : EMERGE_ERR_CUDA;
 }
 

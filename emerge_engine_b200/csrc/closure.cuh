@@ -47,10 +47,28 @@ constexpr int CL_OFF_W4 = CL_OFF_B3 + CL_H;
 constexpr int CL_OFF_B4 = CL_OFF_W4 + CL_H * CL_OUT;
 constexpr int CL_NPARAMS = CL_OFF_B4 + CL_OUT;  // 8963
 
+// Weights of one network for the 5th-generation tensor cores (tcgen05.mma, kind::f16): each
+// layer's W^T as a K-major BF16 operand in the no-swizzle core-matrix layout -- element
+// (n, k) of an N x K operand at byte (n / 8) (K / 8) 128 + (k / 8) 128 + (n % 8) 16 + (k % 8) 2,
+// i.e. 8 x 8 core matrices of 128 contiguous bytes, adjacent along K (leading byte offset
+// 128) and K / 8 apart along N (stride byte offset K 16).  Layer 1 pads K from 6 to 16,
+// layer 4 pads N from 3 to 16 (the smallest N of an M = 128 MMA).
+constexpr int CL_TC_K1 = 16, CL_TC_N4 = 16;
+constexpr int CL_TC_BYTES_L1 = CL_H * CL_TC_K1 * 2;   // 2 KB
+constexpr int CL_TC_BYTES_L2 = CL_H * CL_H * 2;       // 8 KB
+constexpr int CL_TC_BYTES_L4 = CL_TC_N4 * CL_H * 2;   // 2 KB
+constexpr int CL_TC_OFF_L1 = 0, CL_TC_OFF_L2 = CL_TC_BYTES_L1, CL_TC_OFF_L3 = CL_TC_OFF_L2 + CL_TC_BYTES_L2,
+              CL_TC_OFF_L4 = CL_TC_OFF_L3 + CL_TC_BYTES_L2, CL_TC_BYTES = CL_TC_OFF_L4 + CL_TC_BYTES_L4;  // 20 KB
+
+__host__ __device__ __forceinline__ uint32_t km_offset(int n, int k, int kdim) {
+    return static_cast<uint32_t>(((n >> 3) * (kdim >> 3) + (k >> 3)) * 128 + (n & 7) * 16 + (k & 7) * 2);
+}
+
 // Inference form of one network (device memory).
 struct ClosureNet {
     uint2 frag[CL_FRAGS][32];       // BF16 pairs, m16n8k16 B-fragment order
     float bias[3 * CL_H + 8];       // b1, b2, b3, b4 (b4 padded to 8)
+    alignas(16) unsigned char tc[CL_TC_BYTES];  // tcgen05 operand form (above)
     float in_shift[8], in_scale[8];  // x_n = (x - shift) * scale
     float out_shift[4], out_scale[4];  // y = y_n * scale + shift
     float hull_lo[8], hull_hi[8];   // box of the normalised training inputs
@@ -261,6 +279,15 @@ __device__ __forceinline__ float2 nacc_principal_stress(const MatP &m, float2 s)
     return v2(m.mu / j * (sq.x - half_tr) + vol, m.mu / j * (sq.y - half_tr) + vol);
 }
 
+// Judged errors are also binned: bin b covers [10^(b/4 - 8), 10^((b+1)/4 - 8)) (a quarter
+// decade from 1e-8 to 1e4), for the percentiles.
+constexpr int CL_ERR_BINS = 48;
+__device__ __forceinline__ int closure_err_bin(float e) {
+    if (!(e > 1e-8f)) return 0;
+    const int b = static_cast<int>(floorf((log10f(e) + 8.0f) * 4.0f));
+    return b < 0 ? 0 : (b >= CL_ERR_BINS ? CL_ERR_BINS - 1 : b);
+}
+
 // Lifetime counters of the closure (device memory).
 struct ClosureStats {
     unsigned long long smooth;        // particles on a smooth plastic branch
@@ -271,6 +298,8 @@ struct ClosureStats {
     double err_sum;                   // sum of judged relative stress errors
     unsigned int err_max_bits;        // max judged relative stress error (float bits)
     unsigned int pad_;
+    unsigned long long judge_replaced;   // judged results above the bar, replaced by the plain one
+    unsigned long long err_hist[CL_ERR_BINS];
 };
 
 // Closure switches and buffers of a particle pass.
@@ -284,6 +313,12 @@ struct ClosureArgs {
     uint32_t judge_stride;    // judge one network evaluation in judge_stride (hashed)
     int infer;                // use installed networks
     int log;                  // record (inputs, targets) of the plain mapping
+    // Deferred evaluation: the particle pass queues the particles the network is to map
+    // (slot indices, one queue per model, counted in StepState::cl_queued) and a tile kernel
+    // evaluates them 128 at a time on tcgen05 and finishes their update and P2G.
+    int defer;
+    uint32_t *queue[CL_NMODELS];
+    float judge_bar;          // judged results with a larger relative stress error use the plain result
 };
 
 }  // namespace emerge

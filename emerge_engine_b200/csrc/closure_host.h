@@ -14,7 +14,7 @@ namespace emerge {
 struct ClosureHost;  // closure.cu: networks, statistics, log buffers, master weights
 
 // Kernel arguments of the closure (all zero when the simulation has none).
-ClosureArgs closure_args(const ClosureHost *c);
+ClosureArgs closure_args(const ClosureHost *c, size_t n);
 void closure_destroy(ClosureHost *c);
 
 // sim.cu: a simulation's scene description, for building batches (batch.cu).
@@ -35,6 +35,7 @@ DevParticles particle_set_carve(void *base, size_t cap);
 
 // sim.cu: the pieces of a simulation the closure manager uses.
 cudaStream_t sim_stream(emerge_sim *s);
+size_t sim_capacity(emerge_sim *s);  // particle capacity of the device storage (at least 1)
 ClosureHost *&sim_closure(emerge_sim *s);
 void sim_invalidate_graph(emerge_sim *s);
 emerge_status sim_fail(emerge_sim *s, emerge_status st, const std::string &msg);

@@ -73,6 +73,7 @@ struct StepState {
     uint32_t active;            // batches: the scene takes part in the running substep
     uint32_t contact_active;    // Grid::has_contact_activity of the running substep
     uint32_t n_iface;           // fast pipeline: contact cells holding both fields this substep
+    uint32_t cl_queued[2][CL_NMODELS];  // learned closure: particles queued per slot and model
 };
 
 struct GridView {
@@ -107,6 +108,7 @@ struct GridView {
 
 // StepState::error_flags bits
 constexpr uint32_t ERR_CONTACT_LIST = 1u;  // a contact point-list walk was cut short
+constexpr uint32_t ERR_CLOSURE_WAIT = 2u;  // a closure tile's tensor-core wait gave up (kernel returned)
 
 __host__ __device__ __forceinline__ int cell_index(int x, int y, int tpd) {
     return (((x >> 3) * tpd + (y >> 3)) << 6) | ((x & 7) << 3) | (y & 7);

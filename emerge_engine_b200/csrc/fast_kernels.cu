@@ -1,9 +1,10 @@
 // fast_kernels.cu -- the fast path's particle and density passes.
 //
-// Compiled with contraction into FMA and approximate division and square root (see
-// build.py): the fused pipeline's default mode, whose results differ from the reference
-// only in float rounding (summation order of the L2 reductions, FMA, 2-ulp division and
-// square root).  The reference-order mode runs the exact instantiation in step_kernels.cu.
+// Compiled with approximate division and square root outside the constitutive math and no
+// implicit contraction (see build.py): the fused pipeline's default mode, whose results
+// differ from the reference only in float rounding (summation order of the L2 reductions,
+// the explicit fused multiply-adds of the stencil sums, 2-ulp division and square root).
+// The reference-order mode runs the exact instantiation in step_kernels.cu.
 #define EMERGE_FAST_TU 1  // em_pow: integer exponents by repeated multiplication
 #include <cstring>
 
@@ -31,7 +32,14 @@ __global__ void __launch_bounds__(THREADS, EMERGE_PARTICLE_CTAS_PER_SM) k_partic
 #endif
 template <unsigned MASK>
 __global__ void __launch_bounds__(THREADS, EMERGE_CLOSURE_CTAS_PER_SM) k_particle_closure(ParticleKernelArgs a) {
-    particle_pass<MASK, true, true>(a);
+    particle_pass<MASK, true, 1>(a);
+}
+
+// The particle pass that queues the network's particles for the tile kernel (no network in
+// this kernel, so it keeps the plain pass's register budget and occupancy).
+template <unsigned MASK>
+__global__ void __launch_bounds__(THREADS, EMERGE_PARTICLE_CTAS_PER_SM) k_particle_closure_queue(ParticleKernelArgs a) {
+    particle_pass<MASK, true, 2>(a);
 }
 
 // estimate_particle_volumes gather (solver/density.rs:50-71) at the projected
@@ -44,7 +52,7 @@ __global__ void __launch_bounds__(THREADS, EMERGE_DENSITY_CTAS_PER_SM) k_density
 // Batched scenes: every CTA finds its scene in the batch's tables; all model sets.
 template <unsigned MASK>
 __global__ void __launch_bounds__(THREADS, EMERGE_PARTICLE_CTAS_PER_SM) k_particle_batch(ParticleKernelArgs a) {
-    particle_pass<MASK, true, false, true>(a);
+    particle_pass<MASK, true, 0, true>(a);
 }
 template <unsigned MASK>
 __global__ void __launch_bounds__(THREADS, EMERGE_DENSITY_CTAS_PER_SM) k_density_batch(DensityKernelArgs a) {
@@ -93,6 +101,16 @@ void launch_density_pass_batch(const DevParticles &P, const BatchView &b, int n_
 void launch_particle_pass_fast(const ParticleKernelArgs &a, unsigned model_mask, cudaStream_t stream) {
     const int grid = blocks_for(a.n, THREADS);
     const unsigned plastic = (1u << M_DRUCKER_PRAGER) | (1u << M_NACC);
+    if (a.cl.defer && a.mode_g2p && (model_mask & plastic) && !(model_mask & EXTRAS)) {
+        const unsigned cover = covering_mask(model_mask);
+        if (cover == MASK_GRANULAR)
+            k_particle_closure_queue<MASK_GRANULAR><<<grid, THREADS, 0, stream>>>(a);
+        else if (cover == ALL_MODELS)
+            k_particle_closure_queue<ALL_MODELS><<<grid, THREADS, 0, stream>>>(a);
+        else
+            k_particle_closure_queue<FULL_MODELS><<<grid, THREADS, 0, stream>>>(a);
+        return;
+    }
     if ((a.cl.infer || a.cl.log) && (model_mask & plastic)) {
         const unsigned cover = (model_mask & EXTRAS) ? FULL_MODELS : covering_mask(model_mask);
         if (cover == MASK_GRANULAR)

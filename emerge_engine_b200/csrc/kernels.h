@@ -16,6 +16,17 @@ struct LoadFlagsHost {
     int pinned = 0;
 };
 
+// closure_tiles.cu: the learned closure's tile kernel (after the particle pass, when the
+// pass queued particles for it: deferred closure, fast path, plastic models, no extras)
+void launch_closure_tiles(const StepLaunch &L, const LoadFlagsHost &lf, int sm_count);
+// test hook: the tile kernel's network on n normalised inputs (closure.cu, emerge_cuda_mlp_infer_tc)
+cudaError_t launch_mlp_tiles(const ClosureNet *net, const float *x, int n, float *y, uint32_t *error,
+                             cudaStream_t stream);
+inline bool closure_tiles_on(const StepLaunch &L) {
+    const unsigned plastic = (1u << M_DRUCKER_PRAGER) | (1u << M_NACC);
+    return L.fast && L.cl.defer && (L.model_mask & plastic) && !(L.model_mask & (1u << M_EXTRAS_BIT));
+}
+
 // step_kernels.cu
 void launch_particle_pass(const StepLaunch &L, const LoadFlagsHost &lf, int mode_g2p,
                           int project_in, int emit_p2g);

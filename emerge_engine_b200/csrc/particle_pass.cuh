@@ -979,11 +979,28 @@ __device__ __forceinline__ void closure_count(const ClosureArgs &cl, int smooth,
             atomicMax(&s->err_max_bits, __float_as_uint(e_max));
         }
     }
+    if (err >= 0.0f) atomicAdd(&cl.stats->err_hist[closure_err_bin(err)], 1ull);
 }
 
 // Body of the particle pass (one particle per thread); the kernels that run it are
 // instantiated in step_kernels.cu (reference-order arithmetic) and fast_kernels.cu.
-template <unsigned MASK, bool FAST, bool CLOSURE = false, bool BATCH = false>
+// Appends the slot of each lane with `want` to queue `model` of the learned closure (one
+// atomic per warp).  Every lane of the warp calls this.
+__device__ __forceinline__ void closure_enqueue(const ClosureArgs &cl, StepState *st, uint32_t slot,
+                                                int model, bool want, int i) {
+    const unsigned ballot = __ballot_sync(0xffffffffu, want);
+    if (!ballot) return;
+    const int lane = threadIdx.x & 31, leader = __ffs(ballot) - 1;
+    uint32_t base = 0u;
+    if (lane == leader) base = atomicAdd(&st->cl_queued[slot][model], static_cast<uint32_t>(__popc(ballot)));
+    base = __shfl_sync(0xffffffffu, base, leader);
+    if (want) cl.queue[model][base + __popc(ballot & ((1u << lane) - 1u))] = static_cast<uint32_t>(i);
+}
+
+// CLOSURE: 0 none; 1 the learned closure evaluated inside the pass (warp-level MMA); 2 the
+// particles the network maps are queued for the tile kernel (closure_tiles.cu), which
+// finishes their update, CFL bound, projection and P2G.
+template <unsigned MASK, bool FAST, int CLOSURE = 0, bool BATCH = false>
 __device__ __forceinline__ void particle_pass(const ParticleKernelArgs &a) {
     __shared__ MatP s_mats[MAX_MATERIALS];
     __shared__ uint32_t s_max_speed, s_min_mdt, s_warps_done;
@@ -1068,7 +1085,8 @@ __device__ __forceinline__ void particle_pass(const ParticleKernelArgs &a) {
                 update_particle<MASK>(*mp, p, dt, pr);
         }
     }
-    if constexpr (CLOSURE) {
+    bool deferred = false;  // CLOSURE == 2: queued for the tile kernel
+    if constexpr (CLOSURE == 1) {
         // learned closure: the network runs for the whole warp (warp-synchronous MMA)
         float y[CL_OUT] = {0.0f, 0.0f, 0.0f};
         float err = -1.0f;
@@ -1076,6 +1094,14 @@ __device__ __forceinline__ void particle_pass(const ParticleKernelArgs &a) {
             closure_evaluate<MASK>(a.cl, w, y);
             if (valid) closure_finish<MASK>(*mp, p, pr, w, y, err);
             closure_count(a.cl, w.smooth, w.kind != 0 ? 1 : 0, (w.smooth && w.kind == 0 && a.cl.infer) ? 1 : 0, err);
+        }
+    } else if constexpr (CLOSURE == 2) {
+        if (a.mode_g2p) {
+            deferred = valid && w.kind != 0;
+            closure_enqueue(a.cl, st, acc_slot, 0, deferred && w.kind == 1, i);
+            closure_enqueue(a.cl, st, acc_slot, 1, deferred && w.kind == 2, i);
+            // smooth-branch and hull counts here; the tile kernel counts the network's results
+            closure_count(a.cl, w.smooth, 0, (w.smooth && w.kind == 0 && a.cl.infer) ? 1 : 0, -1.0f);
         }
     }
     bool asleep = false;  // sleep scoring at the end of this substep (step.rs:299-315)
@@ -1101,13 +1127,16 @@ __device__ __forceinline__ void particle_pass(const ParticleKernelArgs &a) {
     }
     if (valid && !asleep) {
         const MatP &m = *mp;
-        // CFL contribution for the next substep (step.rs:447-466)
+        // CFL contribution for the next substep (step.rs:447-466); a queued particle's
+        // material bound depends on its update, which the tile kernel finishes
         float sp = vlen(p.v);
         if (cfg.affine_cfl) sp += affine_cfl(p.c, cfg.cell);
         max_speed = sp;
-        float mdt = timestep_bound<MASK>(m, p.rho, p.h, cfg.cell, cfg.mat_cfl, cfg.visc_cfl, pr);
-        if (isfinite(mdt) && mdt > 0.0f) min_mdt = mdt;
-        if (a.emit_p2g) {
+        if (!deferred) {
+            float mdt = timestep_bound<MASK>(m, p.rho, p.h, cfg.cell, cfg.mat_cfl, cfg.visc_cfl, pr);
+            if (isfinite(mdt) && mdt > 0.0f) min_mdt = mdt;
+        }
+        if (a.emit_p2g && !deferred) {
             // projection of the next substep (step.rs:67-73) and its P2G payload
             if (cfg.project) {
                 bool ch = false;

@@ -110,6 +110,7 @@ struct emerge_sim {
     emerge_sim_config cfg{};
     DevConfig dcfg{};
     int device = 0;
+    int sm_count = 0;        // streaming multiprocessors of the device (persistent grids)
     cudaStream_t stream = nullptr;
     std::string error;
 
@@ -371,7 +372,7 @@ StepLaunch make_launch(emerge_sim *s) {
     if (s->dcfg.n_fields > 0 || s->dcfg.asflip > 0.0f || s->dcfg.zones || s->dcfg.multi)
         L.model_mask |= 1u << M_EXTRAS_BIT;
     L.fast = det_pipeline(s) ? 0 : 1;
-    L.cl = closure_args(s->closure);
+    L.cl = closure_args(s->closure, s->n);
     L.stream = s->stream;
     return L;
 }
@@ -504,7 +505,7 @@ emerge_status build_graph(emerge_sim *s) {
     cudaGraphNode_t wnode;
     CK(cudaGraphAddNode(&wnode, graph, nodes.data(), nn, &cp));
     cudaGraph_t body = cp.conditional.phGraph_out[0];
-    const int kps = 3 + (L.density_mode ? 1 : 0) + multi_fast_launches(L.cfg);
+    const int kps = 3 + (L.density_mode ? 1 : 0) + multi_fast_launches(L.cfg) + (closure_tiles_on(L) ? 1 : 0);
     CK(cudaStreamBeginCaptureToGraph(s->stream, body, nullptr, nullptr, 0,
                                      cudaStreamCaptureModeThreadLocal));
     launch_substep_begin(L, 1, static_cast<unsigned long long>(handle), kps);
@@ -512,6 +513,7 @@ emerge_status build_graph(emerge_sim *s) {
     launch_grid_update(L);
     enqueue_multi_resolves(L);
     launch_particle_pass(L, s->lf, 1, L.cfg.project, 1);
+    if (closure_tiles_on(L)) launch_closure_tiles(L, s->lf, s->sm_count);
     if (L.density_mode) launch_density_pass(L, s->lf);
     CK(cudaStreamEndCapture(s->stream, &body));
     CK(cudaGraphInstantiate(&s->graph_exec, graph, 0));
@@ -598,6 +600,10 @@ emerge_status run_host_loop_step(emerge_sim *s, bool timed) {
         enqueue_multi_resolves(L);
         CK(cudaEventRecord(s->ev[3], s->stream));
         launch_particle_pass(L, s->lf, 1, L.cfg.project, 1);
+        if (closure_tiles_on(L)) {
+            launch_closure_tiles(L, s->lf, s->sm_count);
+            s->host_launches += 1;
+        }
         CK(cudaEventRecord(s->ev[4], s->stream));
         s->host_launches += 3 + multi_fast_launches(L.cfg);
         if (L.density_mode) {
@@ -1188,6 +1194,7 @@ DevParticles particle_set_carve(void *base, size_t cap) {
     return carve_particles(c, cap);
 }
 ClosureHost *&sim_closure(emerge_sim *s) { return s->closure; }
+size_t sim_capacity(emerge_sim *s) { return std::max<size_t>(s->cap, std::max<size_t>(s->n, 1)); }
 void sim_invalidate_graph(emerge_sim *s) { s->graph_dirty = true; }
 emerge_status sim_fail(emerge_sim *s, emerge_status st, const std::string &msg) {
     return static_cast<emerge_status>(s->fail(st, msg));
@@ -1232,6 +1239,8 @@ emerge_status emerge_cuda_create(const emerge_sim_config *config, int device, em
     emerge_sim *s = new emerge_sim();
     s->cfg = *config;
     s->device = device;
+    if (cudaDeviceGetAttribute(&s->sm_count, cudaDevAttrMultiProcessorCount, device) != cudaSuccess)
+        s->sm_count = 0;  // the persistent grids then assume 148
     s->bounds.push_back(config->boundary_thickness);  // default SlipBoundary (lifecycle.rs:29-30)
     s->dcfg = make_dev_config(s->cfg, s->bounds, 0);
     emerge_material_params fallback;
@@ -1670,6 +1679,9 @@ emerge_status emerge_cuda_step(emerge_sim *s, uint32_t n_steps, emerge_step_timi
 static emerge_status sync_state(emerge_sim *s) {
     CK(cudaMemcpyAsync(s->h_state, s->d_state, sizeof(StepState), cudaMemcpyDeviceToHost, s->stream));
     CK(cudaStreamSynchronize(s->stream));
+    if (s->h_state->error_flags & ERR_CLOSURE_WAIT)
+        return static_cast<emerge_status>(s->fail(EMERGE_ERR_TIMEOUT,
+                                                  "learned closure: a tensor-core wait gave up (tile kernel returned)"));
     if (s->h_state->error_flags & ERR_CONTACT_LIST)
         return static_cast<emerge_status>(s->fail(EMERGE_ERR_CUDA, "contact point list walk cut short"));
     return EMERGE_OK;

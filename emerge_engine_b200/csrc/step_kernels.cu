@@ -179,6 +179,7 @@ __device__ __forceinline__ uint32_t substep_begin_state(StepState &s, const DevC
     s.min_mdt_bits[k1] = __float_as_uint(INFINITY);
     s.jproj_pending[k1] = 0ull;
     s.proj_changed[k1] = 0ull;
+    for (int m = 0; m < CL_NMODELS; ++m) s.cl_queued[k1][m] = 0u;
     s.contact_active = 0u;
     s.acc_slot = k1;
     s.parity = k1;

@@ -398,6 +398,11 @@ class Simulation:
     def closure_enable(self, on: bool = True, judge_stride: int = 64) -> None:
         self._check(self._lib.emerge_cuda_closure_enable(self._sim, 1 if on else 0, int(judge_stride)))
 
+    def closure_set_mode(self, defer: bool = True, judge_bar: float = 1e-3) -> None:
+        """Deferred tensor-core evaluation (tile kernel) or evaluation inside the particle
+        pass, and the judge's replacement bar (emerge_cuda_closure_set_mode)."""
+        self._check(self._lib.emerge_cuda_closure_set_mode(self._sim, 1 if defer else 0, float(judge_bar)))
+
     def closure_stats(self, reset: bool = False) -> dict:
         st = abi.ClosureStatsC()
         self._check(self._lib.emerge_cuda_closure_stats(self._sim, byref(st), 1 if reset else 0))
@@ -492,6 +497,18 @@ def mlp_adam(params, m, v, grad, step, lr, beta1=0.9, beta2=0.999, eps=1e-8):
                                         vv.ctypes.data_as(c_void_p), g.ctypes.data_as(c_void_p),
                                         len(p), int(step), lr, beta1, beta2, eps))
     return p, mm, vv
+
+
+def mlp_infer_tc(params: np.ndarray, x: np.ndarray) -> np.ndarray:
+    """The closure MLP on normalised inputs as the closure's tile kernel evaluates it
+    (tcgen05 tensor cores, 128 rows per tile)."""
+    lib = load_library()
+    p = np.ascontiguousarray(params, np.float32)
+    xx = np.ascontiguousarray(x, np.float32)
+    y = np.zeros((len(xx), 3), np.float32)
+    check(lib, lib.emerge_cuda_mlp_infer_tc(p.ctypes.data_as(c_void_p), xx.ctypes.data_as(c_void_p),
+                                            len(xx), y.ctypes.data_as(c_void_p)))
+    return y
 
 
 def mlp_infer_bf16(params: np.ndarray, x: np.ndarray) -> np.ndarray:

@@ -487,6 +487,8 @@ typedef struct emerge_closure_stats {
     double err_mean;         /* mean relative stress error of the judged results */
     float err_max;           /* max relative stress error of the judged results */
     uint32_t pad_;
+    uint64_t judge_replaced; /* judged results above the judge's bar, replaced by the plain one */
+    float err_p50, err_p99;  /* percentiles of the judged errors (quarter-decade bins: upper edge) */
 } emerge_closure_stats;
 
 typedef struct emerge_closure_train_config {
@@ -522,6 +524,14 @@ emerge_status emerge_cuda_closure_train(emerge_sim *sim, int model, const emerge
 emerge_status emerge_cuda_closure_enable(emerge_sim *sim, int on, uint32_t judge_stride);
 /* Lifetime counters; reset != 0 zeroes them (the logged counts are kept). */
 emerge_status emerge_cuda_closure_stats(emerge_sim *sim, emerge_closure_stats *out, int reset);
+/* How the enabled closure runs.  defer = 1 (default): the particle pass queues the particles
+ * the network maps and a tile kernel evaluates them 128 at a time on the tcgen05 tensor cores
+ * (accumulators in tensor memory) and finishes their update and P2G; the particle pass keeps
+ * the plain pass's register budget.  Scenes with force fields, ASFLIP, a sleep partition or
+ * multi-field sums, and batches, evaluate inside the particle pass (defer = 0: always).
+ * judge_bar: a judged result whose relative stress error exceeds it is replaced by the plain
+ * mapping's (default 1e-3; +inf keeps every network result). */
+emerge_status emerge_cuda_closure_set_mode(emerge_sim *sim, int defer, float judge_bar);
 /* FP32 master parameters (8963 floats: W1[6][64] b1 W2[64][64] b2 W3[64][64] b3 W4[64][3] b4)
  * and normalisation (in_shift[6] in_scale[6] out_shift[3] out_scale[3]) of a network. */
 emerge_status emerge_cuda_closure_get_params(emerge_sim *sim, int model, float *params, float *norm);
@@ -540,6 +550,10 @@ emerge_status emerge_cuda_mlp_loss_grad(const float *params, const float *x, con
 emerge_status emerge_cuda_mlp_adam(float *params, float *m, float *v, const float *grad, uint32_t n,
                                    uint32_t step, float lr, float beta1, float beta2, float eps);
 emerge_status emerge_cuda_mlp_infer_bf16(const float *params, const float *x, uint32_t n, float *y);
+/* The same network evaluated as the closure's tile kernel does it: 128 inputs per tile on the
+ * tcgen05 tensor cores (BF16 operands in shared memory, FP32 accumulators in tensor memory,
+ * SiLU from the hardware tanh).  EMERGE_ERR_TIMEOUT if a bounded wait gave up. */
+emerge_status emerge_cuda_mlp_infer_tc(const float *params, const float *x, uint32_t n, float *y);
 
 /* ---- batched scenes (no counterpart in the reference) -----------------------------
  * Many independent scenes advanced together: every substep is one launch per kernel for

@@ -446,3 +446,24 @@ def mixture_overlap(sim_cls, grid_res=1024, side=362, seed=29, drag=5.0, iterati
     p["v"][p["user_tag"] == tags[1]] = (0.0, -3.0)
     sim.set_particles(p)
     return sim
+
+
+def region_stats64(particles, center, radius):
+    """BodyState statistics (spacetime/solver/query.rs:109-142) of the particles with
+    |x - center|^2 <= radius^2, summed in float64 from a particle array.  Two bit-identical
+    particle sets give identical values, unlike the reference's f32 running sums, whose
+    rounding (~1e-5 relative over 1e5 particles) depends on the iteration order."""
+    x = particles["x"].astype(np.float64)
+    c = np.asarray(center, dtype=np.float64)
+    sel = ((x - c) ** 2).sum(1) <= float(radius) ** 2
+    p = particles[sel]
+    n = int(sel.sum())
+    if n == 0:
+        return dict(count=0)
+    f = p["f"].astype(np.float64)
+    det = f[:, 0] * f[:, 3] - f[:, 2] * f[:, 1]
+    jp = p["plastic_volume_ratio"].astype(np.float64)
+    return dict(count=n, avg_volume_ratio=float(jp.mean()), max_volume_ratio=float(jp.max()),
+                avg_speed=float(np.linalg.norm(p["v"].astype(np.float64), axis=1).mean()),
+                avg_det_f=float(det.mean()), avg_density=float(p["density"].astype(np.float64).mean()),
+                centroid=[float(v) for v in x[sel].mean(0)])

@@ -7,7 +7,7 @@ import numpy as np
 import pytest
 
 from emerge_engine_b200 import Simulation
-from emerge_engine_b200.simulation import mlp_adam, mlp_infer_bf16, mlp_loss_grad
+from emerge_engine_b200.simulation import mlp_adam, mlp_infer_bf16, mlp_infer_tc, mlp_loss_grad
 from oracle import closure_oracle as co
 from tests import scenes
 
@@ -53,6 +53,24 @@ def test_tensor_core_inference_matches_bf16_oracle(cuda_lib):
     assert np.max(np.abs(y - y_fp32)) <= 2e-2 * scale   # BF16 vs FP32
 
 
+@pytest.mark.parametrize("n", [77, 128, 1001, 20_000])
+def test_tile_kernel_inference_matches_bf16_oracle(cuda_lib, n):
+    """The closure's tile kernel (tcgen05.mma, accumulators in tensor memory, 128 rows per
+    tile; partial last tile) against the BF16 emulation of the network: the same rounding
+    points, except SiLU through the hardware tanh (relative error ~2^-11 before the BF16
+    rounding of the activations)."""
+    rng = np.random.default_rng(20 + n)
+    p = co.init_params(4)
+    x = rng.normal(size=(n, 6)).astype(np.float32)
+    y = mlp_infer_tc(p, x)
+    y_bf16 = co.forward_bf16(p, x)
+    y_fp32, _ = co.forward(p.astype(np.float64), x.astype(np.float64))
+    scale = np.max(np.abs(y_fp32))
+    assert np.all(np.isfinite(y))
+    assert np.max(np.abs(y - y_bf16)) <= 3e-3 * scale
+    assert np.max(np.abs(y - y_fp32)) <= 2e-2 * scale
+
+
 @pytest.fixture(scope="module")
 def logged_sim(cuda_lib):
     sim = scenes.mixed_granular(Simulation, grid_res=256, target_particles=120_000)
@@ -93,12 +111,47 @@ def test_trained_closure_gain_and_live_error(logged_sim, cuda_lib):
         sim.step()
         ref.step()
     st = sim.closure_stats()
-    print("closure live", st)
+    print("closure live (tile kernel)", st)
+    # deferred mode (default): the network ran in the tcgen05 tile kernel; judged results
+    # above the judge's bar (1e-3) were replaced by the plain mapping's
     assert st["net"] > 100_000 and st["judged"] > 1000
-    assert st["err_mean"] <= 2e-3
+    assert st["err_mean"] <= 1e-3 and st["err_p50"] <= 1e-3
+    assert st["judge_replaced"] <= 0.05 * st["judged"]
     for c, r in (((128.0, 128.0), 200.0), ((64.0, 64.0), 40.0)):
         a, b = sim.region_state(c, r), ref.region_state(c, r)
         assert abs(a.count - b.count) <= 2
         for k in ("avg_speed", "avg_det_f", "avg_density"):
             assert getattr(a, k) == pytest.approx(getattr(b, k), rel=1e-3), k
     sim.closure_enable(False)
+
+
+def test_deferred_and_inline_closure_agree(logged_sim, cuda_lib):
+    """The tile kernel (deferred mode) and the evaluation inside the particle pass run the
+    same network on the same particles: one frame from one state agrees on mass, momentum and
+    region statistics, and both judge their results against the plain mapping."""
+    src = logged_sim
+    params, norm = src.closure_params(0)
+    hull = np.array([-1e30] * 6 + [1e30] * 6, np.float32)  # the same box for both runs
+    start = src.particles()
+    out = {}
+    for defer in (True, False):
+        sim = scenes.mixed_granular(Simulation, grid_res=256, target_particles=120_000)
+        sim.set_particles(start)
+        sim.set_closure_params(0, params, norm, hull)
+        sim.closure_set_mode(defer=defer, judge_bar=float("inf"))
+        sim.closure_enable(True, judge_stride=8)
+        sim.step()
+        out[defer] = (sim.particles(), sim.closure_stats())
+        sim.close()
+    (pd, sd), (pi, si) = out[True], out[False]
+    print("deferred", sd, "inline", si)
+    assert sd["net"] > 10_000 and si["net"] > 10_000
+    assert sd["net"] == pytest.approx(si["net"], rel=0.02)
+    assert sd["err_mean"] <= 1e-3 and si["err_mean"] <= 2e-3
+    assert pd["mass"].sum(dtype=np.float64) == pi["mass"].sum(dtype=np.float64)
+    m = pd["mass"].astype(np.float64)
+    scale = (m * np.linalg.norm(pi["v"].astype(np.float64), axis=1)).sum()
+    dp = np.linalg.norm((m[:, None] * pd["v"]).sum(0) - (m[:, None] * pi["v"]).sum(0))
+    assert dp <= 1e-3 * scale
+    dx = np.linalg.norm(pd["x"].astype(np.float64) - pi["x"], axis=1)
+    assert np.quantile(dx, 0.99) <= 1e-3
