@@ -231,9 +231,11 @@ void init_params(std::vector<float> &P, uint64_t seed) {
 // (units of mu for Drucker-Prager, of kappa for NACC).
 float stress_rel_err(int model, const float *xraw, const float *y_pred, const float *y_ref) {
     // Drucker-Prager outputs are in units of the trial deviatoric norm s = exp(x[5])
+    // NACC outputs are the plastic correction ln(sv') - ln(sv) of the log singular values
     const float unit = model == 0 ? std::exp(xraw[5]) : 1.0f;
+    const float off0 = model == 0 ? 0.0f : xraw[0], off1 = model == 0 ? 0.0f : xraw[1];
     auto stress = [&](const float *y, float &s0, float &s1) {
-        const float a = std::exp(y[0] * unit), b = std::exp(y[1] * unit), j = a * b;
+        const float a = std::exp(y[0] * unit + off0), b = std::exp(y[1] * unit + off1), j = a * b;
         if (model == 0) {  // tau / mu = 2 (s - 1) s + (lambda / mu) (J - 1) J, lambda/mu = ratio - 1
             const float lam = xraw[3] - 1.0f;
             s0 = 2.0f * (a - 1.0f) * a + lam * (j - 1.0f) * j;
@@ -573,7 +575,8 @@ emerge_status emerge_cuda_closure_train(emerge_sim *s, int model, const emerge_c
             }
             for (int j = 0; j < CL_IN; ++j) xr[j] = X[i * CL_IN + j];
             errs[r] = stress_rel_err(model, xr, yp, &T[i * CL_OUT]);
-            const float y_trial[CL_OUT] = {xr[0], xr[1], 0.0f};  // mapping skipped
+            // the mapping skipped: the trial strains (DP: eps / s; NACC: no correction)
+            const float y_trial[CL_OUT] = {model == 0 ? xr[0] : 0.0f, model == 0 ? xr[1] : 0.0f, 0.0f};
             trial_sum += stress_rel_err(model, xr, y_trial, &T[i * CL_OUT]);
         }
         std::vector<float> sorted = errs;

@@ -7,7 +7,9 @@
 //     cohesion / (2 mu s), ln s -> projected log-strain h / s (sigma' = exp(h)) and the
 //     hardening increment dq / s;
 //   NaccMaterial::project (nacc.rs:129-223), ellipse branch: ln(sv), p0 / kappa, mu / kappa,
-//     beta, M -> projected ln(sv') and the hardening increment d(alpha).
+//     beta, M -> the plastic correction ln(sv') - ln(sv) and the hardening increment
+//     d(alpha) (predicting ln(sv') itself would ask the BF16 network to reproduce the
+//     near-identity part to better than its 2^-8 resolution).
 // The cheap, exact decisions stay exact: the yield test, the DP tip (trace > 0), and the
 // NACC tension / compression caps and elastic test.  Only particles on the smooth plastic
 // branch run the network; inputs outside the training data's box ("hull") use the plain
@@ -185,39 +187,11 @@ __device__ __forceinline__ DpTrial dp_trial(const MatP &m, float2 sigma_in, floa
     t.eps = v2(em_log(sigma.x, pr) + lvs * 0.5f, em_log(sigma.y, pr) + lvs * 0.5f);
     t.trace = t.eps.x + t.eps.y;
     t.dev = vsub(t.eps, splat(t.trace * 0.5f));
-    t.dev_norm = vlen(t.dev);
-    t.ratio = (m.lambda + m.mu) / m.mu;
+    t.dev_norm = evlen(t.dev);  // the arithmetic of dp_project (physics.cuh), so both decide alike
+    t.ratio = ediv(m.lambda + m.mu, m.mu);
     t.alpha = dp_alpha(m, q, pr);
-    t.cohesion = m.stretch_limit / (2.0f * m.mu);
+    t.cohesion = ediv(m.stretch_limit, 2.0f * m.mu);
     t.gamma = t.dev_norm + t.ratio * t.trace * t.alpha - t.cohesion;
-    return t;
-}
-
-// NACC trial quantities (nacc.rs:129-223) in units of kappa.
-struct NaccTrial {
-    float2 sv;
-    float p0, p_tr, y, y1, j_e_tr;
-    int branch;  // 0 elastic, 1 tension cap, 2 compression cap, 3 ellipse (network)
-};
-__device__ __forceinline__ NaccTrial nacc_trial(const MatP &m, float2 sv, float alpha, bool pr) {
-    NaccTrial t;
-    t.sv = sv;
-    const float kappa = nacc_kappa(m);
-    const float xi = m.hardening_exponent, beta = m.compression_limit, mm_ = m.stretch_limit;
-    const float2 sv_sq = vmulv(sv, sv);
-    const float tr = sv_sq.x + sv_sq.y;
-    t.p0 = kappa * (1.0e-5f + em_sinh(xi * fmaxf(-alpha, 0.0f), pr));
-    t.j_e_tr = fmaxf(sv.x * sv.y, 1.0e-6f);
-    const float2 s_tr = svmul(m.mu * (1.0f / t.j_e_tr), vsub(sv_sq, splat(tr * 0.5f)));
-    const float psi_kappa = kappa * 0.5f * (t.j_e_tr - 1.0f / t.j_e_tr);
-    t.p_tr = -psi_kappa * t.j_e_tr;
-    const float y0 = (1.0f + 2.0f * beta) * 2.0f;
-    t.y1 = mm_ * mm_ * (t.p_tr + beta * t.p0) * (t.p_tr - t.p0);
-    t.y = y0 * (s_tr.x * s_tr.x + s_tr.y * s_tr.y) + t.y1;
-    if (t.p_tr > t.p0) t.branch = 1;
-    else if (t.p_tr < -beta * t.p0) t.branch = 2;
-    else if (t.y < 1.0e-4f) t.branch = 0;
-    else t.branch = 3;
     return t;
 }
 
@@ -225,7 +199,7 @@ __device__ __forceinline__ NaccTrial nacc_trial(const MatP &m, float2 sv, float 
 // (the same arithmetic as dp_project / nacc_project): targets for logging, the hull
 // fallback and the judge.
 __device__ __forceinline__ void dp_smooth(const DpTrial &t, float2 &h, float &dq) {
-    h = vsub(t.eps, svmul(t.gamma, vdivs(t.dev, t.dev_norm)));
+    h = vsub(t.eps, svmul(t.gamma, evdivs(t.dev, t.dev_norm)));
     dq = t.gamma;
 }
 
@@ -234,12 +208,10 @@ __device__ __forceinline__ void nacc_smooth(const MatP &m, const NaccTrial &t, f
     const float kappa = nacc_kappa(m);
     const float xi = m.hardening_exponent, beta = m.compression_limit, mm_ = m.stretch_limit;
     const bool hard = xi > 0.0f;
-    const float2 sv = t.sv;
-    const float2 sv_sq = vmulv(sv, sv);
-    const float sv_sq_trace = sv_sq.x + sv_sq.y;
+    const float sv_sq_trace = t.sv_sq_trace;
     const float p0 = t.p0, p_tr = t.p_tr, j_e_tr = t.j_e_tr;
-    const float2 s_tr = svmul(m.mu * (1.0f / j_e_tr), vsub(sv_sq, splat(sv_sq_trace * 0.5f)));
-    const float y0 = (1.0f + 2.0f * beta) * 2.0f;
+    const float2 s_tr = t.s_tr;
+    const float y0 = t.y0;
     const float y1 = t.y1;
     if (hard && p0 > 1.0e-4f && p_tr < p0 - 1.0e-4f && p_tr > -beta * p0 + 1.0e-4f) {
         float p_c = (1.0f - beta) * p0 * 0.5f;
@@ -257,9 +229,9 @@ __device__ __forceinline__ void nacc_smooth(const MatP &m, const NaccTrial &t, f
         float j_e_x = sqrtf(fmaxf(fabsf(-2.0f * p_x / kappa + 1.0f), 1.0e-8f));
         if (j_e_x > 1.0e-4f) alpha += em_log(j_e_tr / j_e_x, pr);
     }
-    float scale = sqrtf(fmaxf(-y1 / fmaxf(y0, 1.0e-10f), 0.0f)) * (j_e_tr / m.mu);
+    float scale = esqrt(fmaxf(ediv(-y1, fmaxf(y0, 1.0e-10f)), 0.0f)) * ediv(j_e_tr, m.mu);
     float2 b_n1 = vadd(svmul(scale, normalize_or_zero(s_tr)), splat(sv_sq_trace / 2.0f));
-    sv_new = v2(sqrtf(fmaxf(b_n1.x, 1.0e-8f)), sqrtf(fmaxf(b_n1.y, 1.0e-8f)));
+    sv_new = v2(esqrt(fmaxf(b_n1.x, 1.0e-8f)), esqrt(fmaxf(b_n1.y, 1.0e-8f)));
     alpha_new = alpha;
 }
 

@@ -34,7 +34,7 @@ constexpr int CT_TMEM_COLS = 64;  // FP32 accumulator columns (the widest layer)
 // Shared memory of one CTA (dynamic, 1 KB aligned).
 struct TileSmem {
     unsigned char a[CT_M * CL_H * 2];            // activations, K-major (K = 64) core matrices
-    unsigned char w[CL_NMODELS][CL_TC_BYTES];    // both networks' weights
+    unsigned char w[CL_TC_BYTES];                // the weights of the network in use (loaded_net)
     float bias[CL_NMODELS][3 * CL_H + 8];
     float in_shift[CL_NMODELS][8], in_scale[CL_NMODELS][8];
     float out_shift[CL_NMODELS][4], out_scale[CL_NMODELS][4];
@@ -43,6 +43,7 @@ struct TileSmem {
     uint32_t tmem_base;
     uint32_t abort;
     uint32_t min_mdt_bits;
+    int loaded_net;                              // network whose weights are in w (-1: none)
 };
 
 // Shared-memory matrix descriptor (tcgen05 "matrix descriptor"): start address, leading
@@ -281,7 +282,7 @@ __device__ __forceinline__ bool tile_mlp(TileSmem &S, TileMma &t, int net, const
         put_row8(S.a, tid, 0, in);
         put_row8(S.a, tid, 8, in + 8);
     }
-    const uint32_t wb = smem_u32(S.w[net]);
+    const uint32_t wb = smem_u32(S.w);
     const float *bias = S.bias[net];
     bool ok = tile_layer(S, t, wb + CL_TC_OFF_L1, 1, CL_H, CL_TC_K1 * 16u);
 #pragma unroll 1
@@ -309,13 +310,24 @@ __device__ __forceinline__ bool tile_mlp(TileSmem &S, TileMma &t, int net, const
     return true;
 }
 
-// Copies both networks' tcgen05 weights, biases and normalisation into shared memory.
+// Copies network `net`'s tcgen05 weights into shared memory if they are not there yet; every
+// thread calls it (CTA barrier).  The MMAs of the previous tile have completed (waited for).
+__device__ __forceinline__ void tile_use_net(TileSmem &S, const ClosureNet *nets, int net) {
+    if (S.loaded_net == net) return;  // CTA-uniform
+    __syncthreads();
+    const uint4 *src = reinterpret_cast<const uint4 *>(nets[net].tc);
+    uint4 *dst = reinterpret_cast<uint4 *>(S.w);
+    for (int k = threadIdx.x; k < CL_TC_BYTES / 16; k += CT_M) dst[k] = src[k];
+    __syncthreads();
+    if (threadIdx.x == 0) S.loaded_net = net;
+    __syncthreads();
+}
+
+// Copies the networks' biases and normalisation into shared memory.
 __device__ __forceinline__ void tile_load_nets(TileSmem &S, const ClosureNet *nets, int n_nets) {
     const int tid = threadIdx.x;
+    if (tid == 0) S.loaded_net = -1;
     for (int net = 0; net < n_nets; ++net) {
-        const uint4 *src = reinterpret_cast<const uint4 *>(nets[net].tc);
-        uint4 *dst = reinterpret_cast<uint4 *>(S.w[net]);
-        for (int k = tid; k < CL_TC_BYTES / 16; k += CT_M) dst[k] = src[k];
         const ClosureNet &nn = nets[net];
         for (int k = tid; k < 3 * CL_H + 8; k += CT_M) S.bias[net][k] = nn.bias[k];
         if (tid < 8) {
@@ -393,10 +405,13 @@ __global__ void __launch_bounds__(CT_M, 1) k_closure_tiles(TileArgs a) {
             mp = &S.mats[p.mat < static_cast<uint32_t>(a.n_mats) ? p.mat : 0u];
             on_branch = tile_prepare<MASK>(*mp, p, dt, pr, model, w);
         }
+        // inputs outside the box of the normalised training inputs use the plain mapping
+        const bool use_net = on_branch && closure_in_hull(cl.nets[model], w.x);
         float xn[CL_IN], y[CL_OUT];
 #pragma unroll
         for (int j = 0; j < CL_IN; ++j)
-            xn[j] = on_branch ? (w.x[j] - S.in_shift[model][j]) * S.in_scale[model][j] : 0.0f;
+            xn[j] = use_net ? (w.x[j] - S.in_shift[model][j]) * S.in_scale[model][j] : 0.0f;
+        tile_use_net(S, a.cl.nets, model);
         if (!tile_mlp(S, t, model, xn, y)) break;  // CTA-uniform
 #pragma unroll
         for (int j = 0; j < CL_OUT; ++j) y[j] = y[j] * S.out_scale[model][j] + S.out_shift[model][j];
@@ -411,7 +426,7 @@ __global__ void __launch_bounds__(CT_M, 1) k_closure_tiles(TileArgs a) {
         float min_mdt = INFINITY;
         if (valid) {
             const MatP &m = *mp;
-            if (on_branch) {
+            if (use_net) {
                 w.judge = (closure_hash(i, st) >> 7) % cl.judge_stride == 0u;
                 PState pn = p;
                 closure_finish<MASK>(m, pn, pr, w, y, err);
@@ -442,9 +457,15 @@ __global__ void __launch_bounds__(CT_M, 1) k_closure_tiles(TileArgs a) {
             pl.s = -stress_volume(m, p) * KERNEL_D_INVERSE;
             pl.do_s = true;
         }
-        // statistics of the network's results (one atomic per warp)
+        // statistics of the queued particles and the network's results (one atomic per warp)
         {
             const unsigned full = 0xffffffffu;
+            const int n_smooth = __reduce_add_sync(full, valid && on_branch ? 1 : 0);
+            const int n_hull = __reduce_add_sync(full, valid && on_branch && !use_net ? 1 : 0);
+            if ((tid & 31) == 0 && n_smooth) {
+                atomicAdd(&cl.stats->smooth, static_cast<unsigned long long>(n_smooth));
+                if (n_hull) atomicAdd(&cl.stats->hull_fallback, static_cast<unsigned long long>(n_hull));
+            }
             const int n_judged = __reduce_add_sync(full, err >= 0.0f ? 1 : 0);
             const int n_rep = __reduce_add_sync(full, replaced);
             float e_sum = err >= 0.0f ? err : 0.0f, e_max = e_sum;
@@ -483,6 +504,7 @@ __global__ void __launch_bounds__(CT_M, 1) k_mlp_tiles(const ClosureNet *net, co
     const int tid = threadIdx.x;
     tile_load_nets(S, net, 1);
     TileMma t = tile_mma_begin(S);
+    tile_use_net(S, net, 0);
     const int tiles = (n + CT_M - 1) / CT_M;
     for (int tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
         const int r = tile * CT_M + tid;
@@ -511,7 +533,8 @@ cudaError_t launch_mlp_tiles(const ClosureNet *net, const float *x, int n, float
 }
 
 // Launches the tile kernel after the particle pass of a substep (same stream).  Persistent
-// CTAs: two per SM, each looping over the tiles both queues hold this substep.
+// CTAs: three per SM (the registers of 3 x 128 threads and about 45 KB of shared memory
+// each), each looping over the tiles both queues hold this substep.
 void launch_closure_tiles(const StepLaunch &L, const LoadFlagsHost &lfh, int sm_count) {
     if (L.n == 0 || !L.cl.defer) return;
     TileArgs a;
@@ -527,7 +550,7 @@ void launch_closure_tiles(const StepLaunch &L, const LoadFlagsHost &lfh, int sm_
     a.lf.pinned = lfh.pinned;
     a.cl = L.cl;
     const size_t smem = sizeof(TileSmem);
-    const int grid = 2 * (sm_count > 0 ? sm_count : 148);
+    const int grid = 3 * (sm_count > 0 ? sm_count : 148);
     const unsigned cover = covering_mask(L.model_mask);
     if (cover == MASK_GRANULAR) {
         cudaFuncSetAttribute(k_closure_tiles<MASK_GRANULAR>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));

@@ -884,7 +884,7 @@ __device__ __forceinline__ void closure_prepare(const MatP &m, PState &p, float 
         float a_new;
         if (cl.log && hash % cl.log_stride == 0u) {
             nacc_smooth(m, t, p.lvs, sv_new, a_new, pr);
-            closure_log(cl, 1, w.x, em_log(sv_new.x, pr), em_log(sv_new.y, pr), a_new - p.lvs);
+            closure_log(cl, 1, w.x, em_log(sv_new.x, pr) - w.x[0], em_log(sv_new.y, pr) - w.x[1], a_new - p.lvs);
         }
         if (cl.infer && closure_in_hull(cl.nets[1], w.x)) {
             w.kind = 2;
@@ -896,6 +896,52 @@ __device__ __forceinline__ void closure_prepare(const MatP &m, PState &p, float 
         return;
     }
     update_particle<MASK>(m, p, dt, pr);
+}
+
+// The update of the deferred mode: the constitutive update of the particle pass, except that
+// a Drucker-Prager or NACC particle on the smooth plastic branch whose network is installed
+// is left unupdated and returned as 1 (Drucker-Prager) or 2 (NACC) for the tile kernel.  The
+// branch decision reuses the trial SVD the update needs anyway (sand.rs:156-194,
+// nacc.rs:129-223); every other particle is updated exactly as update_particle does.
+template <unsigned MASK>
+__device__ __forceinline__ int closure_defer_update(const MatP &m, PState &p, float dt, bool pr,
+                                                    const ClosureArgs &cl) {
+    if (HAS_MODEL(MASK, M_DRUCKER_PRAGER) && m.model == M_DRUCKER_PRAGER && cl.nets[0].ready) {
+        const M2 f_trial = mm(madd(mident(), smscale(dt, p.c)), p.f);
+        M2 u, vt;
+        float2 sigma;
+        svd2(f_trial, u, sigma, vt);
+        // dp_project's decisions in its order: the tip before the friction angle
+        const float2 sg = vmax2(vabs2(sigma), splat(LOG_CLAMP));
+        const float2 eps = v2(em_log(sg.x, pr) + p.lvs * 0.5f, em_log(sg.y, pr) + p.lvs * 0.5f);
+        const float trace = eps.x + eps.y;
+        const float dev_norm = evlen(vsub(eps, splat(trace * 0.5f)));
+        if (dev_norm == 0.0f || trace > 0.0f) {
+            dp_finish(m, p, u, sigma, vt, true, v2(1.0f, 1.0f), dev_norm, pr);
+            return 0;
+        }
+        const float gamma = dev_norm + ediv(m.lambda + m.mu, m.mu) * trace * dp_alpha(m, p.q, pr) -
+                            ediv(m.stretch_limit, 2.0f * m.mu);
+        if (gamma <= 0.0f) {
+            dp_finish(m, p, u, sigma, vt, false, v2(0.0f, 0.0f), 0.0f, pr);
+            return 0;
+        }
+        return 1;
+    }
+    if (HAS_MODEL(MASK, M_NACC) && m.model == M_NACC && cl.nets[1].ready) {
+        M2 u, vt;
+        float2 sv;
+        svd2(p.f, u, sv, vt);
+        const NaccTrial t = nacc_trial(m, sv, p.lvs, pr);
+        if (t.branch == 3) return 2;
+        M2 nf;
+        float na;
+        nacc_project_t(m, p.f, u, vt, t, p.lvs, nf, na, pr);
+        nacc_apply(p, nf, na);
+        return 0;
+    }
+    update_particle<MASK>(m, p, dt, pr);
+    return 0;
 }
 
 // Phase 2 (all 32 lanes): network evaluation for the lanes that asked for it.
@@ -939,8 +985,8 @@ __device__ __forceinline__ void closure_finish(const MatP &m, PState &p, bool pr
             err = vlen(vsub(s_net, s_ref)) / fmaxf(vlen(s_ref), 1e-6f * m.mu);
         }
         dp_finish(m, p, w.u, w.sigma, w.vt, true, proj, dq, pr);
-    } else if (w.kind == 2) {
-        const float2 sv_new = v2(em_exp(y[0], pr), em_exp(y[1], pr));
+    } else if (w.kind == 2) {  // outputs: the plastic correction of ln(sv)
+        const float2 sv_new = v2(em_exp(y[0] + w.x[0], pr), em_exp(y[1] + w.x[1], pr));
         const float a_new = m.hardening_exponent > 0.0f ? p.lvs + y[2] : p.lvs;
         if (w.judge) {
             const NaccTrial t = nacc_trial(m, w.sigma, p.lvs, pr);
@@ -1079,7 +1125,9 @@ __device__ __forceinline__ void particle_pass(const ParticleKernelArgs &a) {
                 }
             }
             clamped = g2p_particle<FAST, HAS_MODEL(MASK, M_EXTRAS_BIT)>(g, cfg, dt, p, sel);
-            if constexpr (CLOSURE)
+            if constexpr (CLOSURE == 2)
+                w.kind = closure_defer_update<MASK>(*mp, p, dt, pr, a.cl);
+            else if constexpr (CLOSURE == 1)
                 closure_prepare<MASK>(*mp, p, dt, pr, a.cl, closure_hash(i, st), w);
             else
                 update_particle<MASK>(*mp, p, dt, pr);
@@ -1096,12 +1144,10 @@ __device__ __forceinline__ void particle_pass(const ParticleKernelArgs &a) {
             closure_count(a.cl, w.smooth, w.kind != 0 ? 1 : 0, (w.smooth && w.kind == 0 && a.cl.infer) ? 1 : 0, err);
         }
     } else if constexpr (CLOSURE == 2) {
-        if (a.mode_g2p) {
+        if (a.mode_g2p) {  // the tile kernel counts the queued particles' statistics
             deferred = valid && w.kind != 0;
             closure_enqueue(a.cl, st, acc_slot, 0, deferred && w.kind == 1, i);
             closure_enqueue(a.cl, st, acc_slot, 1, deferred && w.kind == 2, i);
-            // smooth-branch and hull counts here; the tile kernel counts the network's results
-            closure_count(a.cl, w.smooth, 0, (w.smooth && w.kind == 0 && a.cl.infer) ? 1 : 0, -1.0f);
         }
     }
     bool asleep = false;  // sleep scoring at the end of this substep (step.rs:299-315)

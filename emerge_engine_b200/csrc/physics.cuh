@@ -286,23 +286,45 @@ EM_HD bool is_bingham(const MatP &m) { return m.model == M_FLUID && m.compressio
 
 // NaccMaterial::project (nacc.rs:129-223).  params(): hardening_exponent = xi,
 // compression_limit = beta, stretch_limit = M (nacc.rs:309-311).
-EM_HD void nacc_project(const MatP &m, M2 f, float alpha, M2 &f_out, float &alpha_out, bool pr) {
+// NaccMaterial::project's trial quantities (nacc.rs:129-170), in its expression order, and
+// the branch they select: 0 elastic, 1 the tension cap (p_tr > p0), 2 the compression cap
+// (p_tr < -beta p0), 3 the ellipse (the smooth plastic branch).
+struct NaccTrial {
+    float2 sv, sv_sq, s_tr;
+    float sv_sq_trace, p0, j_e_tr, p_tr, y0, y1, y;
+    int branch;
+};
+EM_HD NaccTrial nacc_trial(const MatP &m, float2 sv, float alpha, bool pr) {
+    NaccTrial t;
     const float kappa = nacc_kappa(m);
-    float xi = m.hardening_exponent;
-    float beta = m.compression_limit;
-    float mm_ = m.stretch_limit;
-    bool hard = xi > 0.0f;
-    M2 u, vt;
-    float2 sv;
-    svd2(f, u, sv, vt);
-    float2 sv_sq = vmulv(sv, sv);
-    float sv_sq_trace = sv_sq.x + sv_sq.y;
-    float p0 = kappa * (1.0e-5f + em_sinh(xi * fmaxf(-alpha, 0.0f), pr));
-    float j_e_tr = fmaxf(sv.x * sv.y, 1.0e-6f);
-    float2 s_tr = svmul(m.mu * ediv(1.0f, j_e_tr), vsub(sv_sq, splat(sv_sq_trace * 0.5f)));
-    float psi_kappa = kappa * 0.5f * (j_e_tr - ediv(1.0f, j_e_tr));
-    float p_tr = -psi_kappa * j_e_tr;
-    if (p_tr > p0) {
+    const float xi = m.hardening_exponent, beta = m.compression_limit, mm_ = m.stretch_limit;
+    t.sv = sv;
+    t.sv_sq = vmulv(sv, sv);
+    t.sv_sq_trace = t.sv_sq.x + t.sv_sq.y;
+    t.p0 = kappa * (1.0e-5f + em_sinh(xi * fmaxf(-alpha, 0.0f), pr));
+    t.j_e_tr = fmaxf(sv.x * sv.y, 1.0e-6f);
+    t.s_tr = svmul(m.mu * ediv(1.0f, t.j_e_tr), vsub(t.sv_sq, splat(t.sv_sq_trace * 0.5f)));
+    const float psi_kappa = kappa * 0.5f * (t.j_e_tr - ediv(1.0f, t.j_e_tr));
+    t.p_tr = -psi_kappa * t.j_e_tr;
+    t.y0 = (1.0f + 2.0f * beta) * 2.0f;
+    t.y1 = mm_ * mm_ * (t.p_tr + beta * t.p0) * (t.p_tr - t.p0);
+    const float s_norm_sq = t.s_tr.x * t.s_tr.x + t.s_tr.y * t.s_tr.y;
+    t.y = t.y0 * s_norm_sq + t.y1;
+    if (t.p_tr > t.p0) t.branch = 1;
+    else if (t.p_tr < -beta * t.p0) t.branch = 2;
+    else if (t.y < 1.0e-4f) t.branch = 0;
+    else t.branch = 3;
+    return t;
+}
+
+// The projection from F's SVD (u, sv, vt) and its trial quantities (nacc.rs:171-223).
+EM_HD void nacc_project_t(const MatP &m, M2 f, M2 u, M2 vt, const NaccTrial &t, float alpha, M2 &f_out,
+                          float &alpha_out, bool pr) {
+    const float kappa = nacc_kappa(m);
+    const float xi = m.hardening_exponent, beta = m.compression_limit, mm_ = m.stretch_limit;
+    const bool hard = xi > 0.0f;
+    const float p0 = t.p0, p_tr = t.p_tr, j_e_tr = t.j_e_tr;
+    if (t.branch == 1) {
         float j_n1 = sqrtf(fmaxf(-2.0f * p0 / kappa + 1.0f, 1.0e-8f));
         float sv_new = em_pow(j_n1, 0.5f, pr);
         if (hard) alpha += em_log(j_e_tr / j_n1, pr);
@@ -310,7 +332,7 @@ EM_HD void nacc_project(const MatP &m, M2 f, float alpha, M2 &f_out, float &alph
         alpha_out = alpha;
         return;
     }
-    if (p_tr < -beta * p0) {
+    if (t.branch == 2) {
         float j_n1 = sqrtf(fmaxf(2.0f * beta * p0 / kappa + 1.0f, 1.0e-8f));
         float sv_new = em_pow(j_n1, 0.5f, pr);
         if (hard) alpha += em_log(j_e_tr / j_n1, pr);
@@ -318,15 +340,12 @@ EM_HD void nacc_project(const MatP &m, M2 f, float alpha, M2 &f_out, float &alph
         alpha_out = alpha;
         return;
     }
-    float y0 = (1.0f + 2.0f * beta) * 2.0f;
-    float y1 = mm_ * mm_ * (p_tr + beta * p0) * (p_tr - p0);
-    float s_norm_sq = s_tr.x * s_tr.x + s_tr.y * s_tr.y;
-    float y = y0 * s_norm_sq + y1;
-    if (y < 1.0e-4f) {
+    if (t.branch == 0) {
         f_out = f;
         alpha_out = alpha;
         return;
     }
+    const float2 s_tr = t.s_tr;
     if (hard && p0 > 1.0e-4f && p_tr < p0 - 1.0e-4f && p_tr > -beta * p0 + 1.0e-4f) {
         float p_c = (1.0f - beta) * p0 * 0.5f;
         float q_tr = sqrtf(2.0f) * vlen(s_tr);
@@ -343,11 +362,24 @@ EM_HD void nacc_project(const MatP &m, M2 f, float alpha, M2 &f_out, float &alph
         float j_e_x = sqrtf(fmaxf(fabsf(-2.0f * p_x / kappa + 1.0f), 1.0e-8f));
         if (j_e_x > 1.0e-4f) alpha += em_log(j_e_tr / j_e_x, pr);
     }
-    float scale = esqrt(fmaxf(ediv(-y1, fmaxf(y0, 1.0e-10f)), 0.0f)) * ediv(j_e_tr, m.mu);
-    float2 b_n1 = vadd(svmul(scale, normalize_or_zero(s_tr)), splat(sv_sq_trace / 2.0f));
+    float scale = esqrt(fmaxf(ediv(-t.y1, fmaxf(t.y0, 1.0e-10f)), 0.0f)) * ediv(j_e_tr, m.mu);
+    float2 b_n1 = vadd(svmul(scale, normalize_or_zero(s_tr)), splat(t.sv_sq_trace / 2.0f));
     float2 sv_new = v2(esqrt(fmaxf(b_n1.x, 1.0e-8f)), esqrt(fmaxf(b_n1.y, 1.0e-8f)));
     f_out = reconstruct(u, sv_new, vt);
     alpha_out = alpha;
+}
+
+// The projection given F's SVD (u, sv, vt), as computed by svd2.
+EM_HD void nacc_project_sv(const MatP &m, M2 f, M2 u, float2 sv, M2 vt, float alpha, M2 &f_out,
+                           float &alpha_out, bool pr) {
+    nacc_project_t(m, f, u, vt, nacc_trial(m, sv, alpha, pr), alpha, f_out, alpha_out, pr);
+}
+
+EM_HD void nacc_project(const MatP &m, M2 f, float alpha, M2 &f_out, float &alpha_out, bool pr) {
+    M2 u, vt;
+    float2 sv;
+    svd2(f, u, sv, vt);
+    nacc_project_sv(m, f, u, sv, vt, alpha, f_out, alpha_out, pr);
 }
 
 // Kernels are specialised on the set of models present in a scene: MASK bit m set

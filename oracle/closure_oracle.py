@@ -149,11 +149,14 @@ def dp_smooth_targets(x):
 
 def principal_stress(model, x, y):
     """Principal Kirchhoff stress of outputs y (log singular values first; Drucker-Prager
-    in units of s = exp(x[:, 5])), scale-free: Drucker-Prager in units of mu, NACC in units
-    of kappa."""
+    in units of s = exp(x[:, 5]), NACC as the correction of x's log singular values),
+    scale-free: Drucker-Prager in units of mu, NACC in units of kappa."""
     unit = np.exp(np.asarray(x[:, 5], np.float64)) if model == 0 else 1.0
-    a = np.exp(np.asarray(y[:, 0], np.float64) * unit)
-    b = np.exp(np.asarray(y[:, 1], np.float64) * unit)
+    # NACC outputs: the plastic correction ln(sv') - ln(sv)
+    off0 = 0.0 if model == 0 else np.asarray(x[:, 0], np.float64)
+    off1 = 0.0 if model == 0 else np.asarray(x[:, 1], np.float64)
+    a = np.exp(np.asarray(y[:, 0], np.float64) * unit + off0)
+    b = np.exp(np.asarray(y[:, 1], np.float64) * unit + off1)
     j = a * b
     if model == 0:
         lam = x[:, 3] - 1.0

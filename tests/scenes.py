@@ -150,6 +150,44 @@ def batched_scenes(sim_cls, n_scenes=256, seed=7, grid_range=(64, 256), n_range=
     return sims
 
 
+def nacc_ellipse(sim_cls, grid_res=256, n_blocks=40, side=24, seed=11, **sim_kw):
+    """NACC soil (NaccMaterial.soft_clay(5e4, 0.3), nacc.rs:93-100) whose particles start on
+    the smooth plastic branch of the projection, the ellipse (nacc.rs:171-223).  The
+    reference's CPU update never advances a NACC particle's F (nacc.rs:255-269), so soil
+    spawned with F = I stays elastic; here each of n_blocks side x side-cell blocks (4
+    particles per cell) gets a seeded pre-deformation F0 = [[1 + e1, g], [0, 1 + e2]] (shear
+    g in [-0.3, 0.3], compressive strains e in [-0.03, 0]) and a seeded hardened state
+    (log_volume_strain alpha in [-0.2, -0.01]: p0 = kappa (1e-5 + sinh(2 |alpha|))), so that
+    about two thirds of the blocks' trial states lie outside the ellipse at moderate
+    pressure.  No gravity; blocks on a lattice."""
+    rng = np.random.default_rng(seed)
+    cfg = SimConfig.standard(grid_res, 0.05, (0.0, 0.0))
+    sim = sim_cls.empty(cfg, **sim_kw).with_default_material(NaccMaterial.soft_clay(5e4, 0.3))
+    per_row = int((grid_res - 8) // (side + 4))
+    alphas = {}
+    for k in range(n_blocks):
+        r, c = divmod(k, per_row)
+        cx = 6 + c * (side + 4) + side / 2.0
+        cy = 6 + r * (side + 4) + side / 2.0
+        if cy + side / 2.0 > grid_res - 6:
+            break
+        s = SpawnRegion.for_sim(cfg)
+        s.spacing = 0.5
+        s.box_size = (side, side)
+        s.box_center = (cx, cy)
+        g, e1, e2 = rng.uniform(-0.3, 0.3), rng.uniform(-0.03, 0.0), rng.uniform(-0.03, 0.0)
+        s.initial_deformation_gradient = (1.0 + e1, 0.0, g, 1.0 + e2)  # x_axis, y_axis columns
+        s.position_jitter = 0.2
+        s.rng_seed = (seed * 7919 + k) & 0xFFFFFFFF
+        tag = sim.add_body(s)
+        alphas[tag] = rng.uniform(-0.2, -0.01)
+    p = sim.particles()
+    for tag, a in alphas.items():
+        p["log_volume_strain"][p["user_tag"] == tag] = a
+    sim.set_particles(p)
+    return sim
+
+
 # One material per constitutive model beyond the core set, with parameters that put it in
 # its plastic / viscous / yield regime within the first frame: (constructor, mass override
 # for 0.5-cell spacing or None, whether particles carry temperature and activation).
