@@ -84,11 +84,13 @@ WORKLOADS = {
                             "overlapping, water at (0, -3), drag 5, no pressure projection; "
                             "fused pipeline (phase sums with the total)",
                        material="DP+NewtonianFluid-mixture", grid_res=1024),
-    "batched_256": dict(builder="batched_scenes", kwargs=dict(n_scenes=256),
-                        desc="256 independent scenes in one batch: grid G ~ U{64..256}, target "
-                             "N ~ logU[4k, 200k] particles (clipped to fit the grid), material "
-                             "uniform over {NewtonianFluid, DruckerPrager, Stomakhin snow, "
-                             "NeoHookean}, 4 ppc block on the floor, SlipBoundary(2), dt=0.05",
+    "batched_256": dict(builder="batched_scenes", kwargs=dict(n_scenes=256, pair_sizes=True),
+                        desc="256 independent scenes in one batch: grid G ~ U{64..256}, "
+                             "N ~ logU[4k, 200k] particles, the two draws paired by rank so every "
+                             "block fits at 4 ppc (~12.8M particles), material uniform over "
+                             "{NewtonianFluid, DruckerPrager, Stomakhin snow, NeoHookean}, block on "
+                             "the floor, SlipBoundary(2), dt=0.05; autotuned tile shape, particles "
+                             "per CTA, sort interval and P2G aggregation (on-disk cache)",
                         material="batched", grid_res=0),
 }
 DEFAULT_WORKLOAD = "mixed_granular_4m"
@@ -463,7 +465,10 @@ def run_batched(args, spec, rank: int, world: int, dist, local_rank: int) -> dic
     for s in sims:
         s.close()
     del sims
-    tune = batch.autotune(steps_per_trial=1) if not args.no_extras else None
+    cache = os.environ.get("EMERGE_CUDA_TUNE_CACHE") or os.path.join(
+        os.path.expanduser("~"), ".cache", "emerge_engine_b200", "batch_tune.txt")
+    os.makedirs(os.path.dirname(cache), exist_ok=True)
+    tune = batch.autotune(steps_per_trial=1, cache_path=cache) if not args.no_extras else None
     batch.step(args.warmup)
     clocks = ClockSampler(local_rank)
     clocks.start()

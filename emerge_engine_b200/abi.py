@@ -33,6 +33,9 @@ OPT_SORT_INTERVAL = 2
 OPT_P2G_AGGREGATE = 3
 OPT_DETERMINISTIC = 4
 OPT_PRECISE_MATH = 5
+OPT_TILE_SHAPE = 7
+OPT_CHUNKS_PER_CTA = 8
+TUNE_MAX_TRIALS = 16
 
 
 class Particle(Structure):
@@ -173,9 +176,12 @@ class ClosureTrainReportC(Structure):
 
 class BatchTuneReportC(Structure):
     """`emerge_batch_tune_report` (include/emerge_cuda.h)."""
-    _fields_ = [("sort_interval", ctypes.c_int32), ("aggregate", ctypes.c_int32), ("n_trials", c_uint32),
-                ("trial_sort_interval", ctypes.c_int32 * 8), ("trial_aggregate", ctypes.c_int32 * 8),
-                ("trial_ms", c_float * 8)]
+    _fields_ = [("sort_interval", c_int32), ("aggregate", c_int32), ("tile_shape", c_int32),
+                ("chunks_per_cta", c_int32), ("n_trials", c_uint32), ("from_cache", c_uint32),
+                ("best_ms", c_float), ("trial_sort_interval", c_int32 * TUNE_MAX_TRIALS),
+                ("trial_aggregate", c_int32 * TUNE_MAX_TRIALS),
+                ("trial_tile_shape", c_int32 * TUNE_MAX_TRIALS),
+                ("trial_chunks", c_int32 * TUNE_MAX_TRIALS), ("trial_ms", c_float * TUNE_MAX_TRIALS)]
 
 
 CLOSURE_NPARAMS = 8963  # W1[6][64] b1 W2[64][64] b2 W3[64][64] b3 W4[64][3] b4
@@ -249,7 +255,7 @@ ABI_FUNCTIONS = [
                                                POINTER(BodyStateC)]),
     ("emerge_cuda_batch_substeps", c_int, [c_void_p, c_void_p, c_void_p]),
     ("emerge_cuda_batch_set_option", c_int, [c_void_p, c_int, c_int64]),
-    ("emerge_cuda_batch_autotune", c_int, [c_void_p, c_uint32, POINTER(BatchTuneReportC)]),
+    ("emerge_cuda_batch_autotune", c_int, [c_void_p, c_uint32, c_char_p, POINTER(BatchTuneReportC)]),
 ]
 
 _lib = None

@@ -9,6 +9,7 @@
 // one scene.  Scenes keep their own grid size, materials, boundaries and configuration;
 // results equal the single-scene step up to float summation order.
 #include <algorithm>
+#include <cstdio>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -76,6 +77,8 @@ struct emerge_batch {
     emerge_material_params *d_mats = nullptr;
     bool pending_valid = false, sorted_once = false;
     int use_graph = 1, aggregate = 0;
+    int tile_shape = 0;   // particle order of the sort (launch_batch_sort_keys)
+    int chunks = 1;       // 256-particle chunks per CTA of the particle and density passes
     int64_t sort_interval = 8;
     uint64_t steps_since_sort = 0;
     cudaGraph_t graph = nullptr;
@@ -125,7 +128,7 @@ emerge_status sort_batch(emerge_batch *b) {
     if (b->total < 2) return EMERGE_OK;
     const int S = static_cast<int>(b->scenes.size());
     launch_batch_sort_keys(b->d_desc, b->d_compact_start, S, b->P[b->cur], b->total, b->sort.keys[0],
-                           b->sort.vals[0], b->stream);
+                           b->sort.vals[0], b->tile_shape, b->stream);
     const int r = radix_sort_pairs(b->sort, b->total, batch_sort_key_bits(S), b->stream);
     launch_permute_batch(b->P[b->cur], b->P[b->cur ^ 1], b->sort.keys[r], b->sort.vals[r], b->d_desc,
                          b->d_compact_start, b->total, b->stream);
@@ -145,10 +148,10 @@ emerge_status prime(emerge_batch *b) {
     const BatchView all = b->view(0);
     launch_prime_setup_batch(all, b->stream);
     launch_particle_pass_batch(b->P[b->cur], all, b->n_blocks, b->lf, b->model_mask, 0, 1,
-                               b->aggregate, b->stream);
+                               b->aggregate, b->chunks, b->stream);
     if (b->any_density)
         launch_density_pass_batch(b->P[b->cur], all, b->n_blocks, b->lf, b->model_mask,
-                                  b->aggregate, b->stream);
+                                  b->aggregate, b->chunks, b->stream);
     BK(cudaGetLastError());
     b->pending_valid = true;
     return EMERGE_OK;
@@ -159,10 +162,10 @@ void enqueue_substep(emerge_batch *b, int use_cond, unsigned long long handle) {
     launch_substep_begin_batch(live, b->batch_state(), use_cond, handle, 3 + b->any_density, b->stream);
     launch_grid_update_batch(live, b->n_tiles, b->stream);
     launch_particle_pass_batch(b->P[b->cur], live, b->n_blocks, b->lf, b->model_mask, 1, 1,
-                               b->aggregate, b->stream);
+                               b->aggregate, b->chunks, b->stream);
     if (b->any_density)
         launch_density_pass_batch(b->P[b->cur], live, b->n_blocks, b->lf, b->model_mask,
-                                  b->aggregate, b->stream);
+                                  b->aggregate, b->chunks, b->stream);
 }
 
 emerge_status build_graph(emerge_batch *b) {
@@ -226,6 +229,79 @@ emerge_status read_states(emerge_batch *b, std::vector<StepState> &out) {
     BK(cudaMemcpyAsync(out.data(), b->d_states, out.size() * sizeof(StepState), cudaMemcpyDeviceToHost, b->stream));
     BK(cudaStreamSynchronize(b->stream));
     return EMERGE_OK;
+}
+
+}  // namespace
+
+namespace {
+
+// One autotuned setting of a batch (and its frame time in GPU ms, 0 when loaded).
+struct TuneChoice {
+    int sort_interval, aggregate, tile_shape, chunks;
+    float ms;
+};
+
+// Cache key: device name and SM count, then each scene's grid size, particle count and model
+// mask, folded into a 64-bit FNV-1a hash (with the scene count in clear text).
+std::string tune_signature(const emerge_batch *b) {
+    cudaDeviceProp prop{};
+    std::string dev = "unknown";
+    if (cudaGetDeviceProperties(&prop, b->device) == cudaSuccess)
+        dev = std::string(prop.name) + "/" + std::to_string(prop.multiProcessorCount);
+    for (char &ch : dev)
+        if (ch == ' ') ch = '_';
+    uint64_t h = 1469598103934665603ull;
+    auto mix = [&](uint64_t v) {
+        for (int k = 0; k < 8; ++k) {
+            h ^= (v >> (8 * k)) & 0xffu;
+            h *= 1099511628211ull;
+        }
+    };
+    for (const SceneHost &sc : b->scenes) {
+        mix(static_cast<uint64_t>(sc.res));
+        mix(static_cast<uint64_t>(sc.n));
+        mix(static_cast<uint64_t>(sc.density_mode));
+    }
+    mix(b->model_mask);
+    char buf[32];
+    std::snprintf(buf, sizeof(buf), "%016llx", static_cast<unsigned long long>(h));
+    return dev + ":" + std::to_string(b->scenes.size()) + ":" + buf;
+}
+
+// The cache is a text file of lines "key sort_interval aggregate tile_shape chunks ms".
+bool cache_lookup(const char *path, const std::string &key, TuneChoice &out) {
+    std::FILE *f = std::fopen(path, "r");
+    if (!f) return false;
+    char k[256];
+    TuneChoice c{};
+    bool found = false;
+    while (std::fscanf(f, "%255s %d %d %d %d %f", k, &c.sort_interval, &c.aggregate, &c.tile_shape, &c.chunks,
+                       &c.ms) == 6) {
+        if (key == k && c.sort_interval >= 0 && (c.aggregate == 0 || c.aggregate == 1) && c.tile_shape >= 0 &&
+            c.tile_shape <= 3 && (c.chunks == 1 || c.chunks == 2 || c.chunks == 4)) {
+            out = c;
+            found = true;  // the last matching line wins
+        }
+    }
+    std::fclose(f);
+    return found;
+}
+
+void cache_store(const char *path, const std::string &key, const TuneChoice &c) {
+    std::vector<std::string> keep;
+    if (std::FILE *f = std::fopen(path, "r")) {
+        char line[512];
+        while (std::fgets(line, sizeof(line), f)) {
+            std::string l(line);
+            if (l.compare(0, key.size() + 1, key + " ") != 0) keep.push_back(l);
+        }
+        std::fclose(f);
+    }
+    std::FILE *f = std::fopen(path, "w");
+    if (!f) return;  // a cache that cannot be written only costs the next batch its trials
+    for (const std::string &l : keep) std::fputs(l.c_str(), f);
+    std::fprintf(f, "%s %d %d %d %d %.6f\n", key.c_str(), c.sort_interval, c.aggregate, c.tile_shape, c.chunks, c.ms);
+    std::fclose(f);
 }
 
 }  // namespace
@@ -539,41 +615,108 @@ emerge_status emerge_cuda_batch_set_option(emerge_batch *b, int option, int64_t 
         b->aggregate = value == 2 ? 3 : static_cast<int>(value);
         b->graph_dirty = true;
         return EMERGE_OK;
+    case EMERGE_OPT_TILE_SHAPE:
+        if (value < 0 || value > 3)
+            return static_cast<emerge_status>(b->fail(EMERGE_ERR_INVALID_ARG, "tile shape must be 0..3"));
+        b->tile_shape = static_cast<int>(value);
+        b->sorted_once = false;  // re-sort in the new order before the next frame
+        return EMERGE_OK;
+    case EMERGE_OPT_CHUNKS_PER_CTA:
+        if (value != 1 && value != 2 && value != 4)
+            return static_cast<emerge_status>(b->fail(EMERGE_ERR_INVALID_ARG, "chunks per CTA must be 1, 2 or 4"));
+        b->chunks = static_cast<int>(value);
+        b->graph_dirty = true;
+        return EMERGE_OK;
     default: return static_cast<emerge_status>(b->fail(EMERGE_ERR_INVALID_ARG, "option not available for batches"));
     }
 }
 
-// Autotuner: times every candidate (sort interval x P2G warp aggregation) for a few frames
-// on the batch itself and keeps the fastest.  Each trial starts from a freshly sorted state.
-emerge_status emerge_cuda_batch_autotune(emerge_batch *b, uint32_t steps_per_trial, emerge_batch_tune_report *rep) {
+// Autotuner.  Four knobs change no result beyond float summation order: the particle order
+// the sort gives each scene (tile shape), the particles each CTA of the particle and density
+// passes takes (256 per chunk, 1, 2 or 4 chunks), the sort interval and the P2G warp
+// aggregation.  Coordinate descent from the current setting: each knob in turn takes every
+// value while the others keep their best so far; each trial re-sorts, runs one untimed frame
+// and times steps_per_trial frames of the batch itself (the trials advance the scenes).  With a cache file, a batch of the same
+// signature (device, SM count, every scene's grid size, particle count and model set) takes
+// the stored choice without trials, and a tuned choice is stored.
+emerge_status emerge_cuda_batch_autotune(emerge_batch *b, uint32_t steps_per_trial, const char *cache_path,
+                                         emerge_batch_tune_report *rep) {
     if (!b || steps_per_trial == 0) return EMERGE_ERR_INVALID_ARG;
-    const int64_t intervals[4] = {1, 4, 8, 16};
-    const int aggs[2] = {0, 1};
     emerge_batch_tune_report r;
     std::memset(&r, 0, sizeof(r));
-    float best = 1e30f;
-    for (int ai = 0; ai < 2; ++ai)
-        for (int ii = 0; ii < 4; ++ii) {
-            b->sort_interval = intervals[ii];
-            b->aggregate = aggs[ai];
+    const std::string key = tune_signature(b);
+    TuneChoice cur{static_cast<int>(b->sort_interval), b->aggregate == 3 ? 0 : b->aggregate, b->tile_shape, b->chunks, 0.0f};
+    if (cache_path && cache_path[0] && cache_lookup(cache_path, key, cur)) {
+        r.from_cache = 1u;
+    } else {
+        float best = 1e30f;
+        auto trial = [&](const TuneChoice &c) -> emerge_status {
+            b->sort_interval = c.sort_interval;
+            b->aggregate = c.aggregate;
+            b->tile_shape = c.tile_shape;
+            b->chunks = c.chunks;
             b->graph_dirty = true;
             b->sorted_once = false;
-            float ms = 0.0f;
-            emerge_status st = emerge_cuda_batch_time_steps(b, steps_per_trial, 0, &ms);
+            // one untimed frame rebuilds the frame graph and re-sorts in the new tile shape
+            emerge_status st = emerge_cuda_batch_step(b, 1);
             if (st != EMERGE_OK) return st;
-            const uint32_t t = r.n_trials++;
-            r.trial_sort_interval[t] = static_cast<int32_t>(intervals[ii]);
-            r.trial_aggregate[t] = aggs[ai];
-            r.trial_ms[t] = ms / steps_per_trial;
-            if (r.trial_ms[t] < best) {
-                best = r.trial_ms[t];
-                r.sort_interval = static_cast<int32_t>(intervals[ii]);
-                r.aggregate = aggs[ai];
+            float ms = 0.0f;
+            st = emerge_cuda_batch_time_steps(b, steps_per_trial, 0, &ms);
+            if (st != EMERGE_OK) return st;
+            const uint32_t t = r.n_trials;
+            if (t < EMERGE_TUNE_MAX_TRIALS) {
+                r.trial_sort_interval[t] = c.sort_interval;
+                r.trial_aggregate[t] = c.aggregate;
+                r.trial_tile_shape[t] = c.tile_shape;
+                r.trial_chunks[t] = c.chunks;
+                r.trial_ms[t] = ms / steps_per_trial;
+                r.n_trials = t + 1;
             }
+            if (ms / steps_per_trial < best) {
+                best = ms / steps_per_trial;
+                cur = c;
+                cur.ms = best;
+            }
+            return EMERGE_OK;
+        };
+        const int shapes[4] = {0, 1, 2, 3}, chunks[3] = {1, 2, 4}, intervals[3] = {4, 8, 16}, aggs[2] = {0, 1};
+        for (int v : shapes) {
+            TuneChoice c = cur;
+            c.tile_shape = v;
+            emerge_status st = trial(c);
+            if (st != EMERGE_OK) return st;
         }
-    b->sort_interval = r.sort_interval;
-    b->aggregate = r.aggregate;
+        for (int v : chunks) {
+            TuneChoice c = cur;
+            c.chunks = v;
+            emerge_status st = trial(c);
+            if (st != EMERGE_OK) return st;
+        }
+        for (int v : intervals) {
+            TuneChoice c = cur;
+            c.sort_interval = v;
+            emerge_status st = trial(c);
+            if (st != EMERGE_OK) return st;
+        }
+        for (int v : aggs) {
+            TuneChoice c = cur;
+            c.aggregate = v;
+            emerge_status st = trial(c);
+            if (st != EMERGE_OK) return st;
+        }
+        if (cache_path && cache_path[0]) cache_store(cache_path, key, cur);
+    }
+    b->sort_interval = cur.sort_interval;
+    b->aggregate = cur.aggregate;
+    b->tile_shape = cur.tile_shape;
+    b->chunks = cur.chunks;
     b->graph_dirty = true;
+    b->sorted_once = false;
+    r.sort_interval = cur.sort_interval;
+    r.aggregate = cur.aggregate;
+    r.tile_shape = cur.tile_shape;
+    r.chunks_per_cta = cur.chunks;
+    r.best_ms = cur.ms;
     if (rep) *rep = r;
     return EMERGE_OK;
 }

@@ -143,6 +143,7 @@ struct BatchView {
     const uint16_t *tile_scene;   // global grid tile -> scene
     int n_scenes;
     int check_active;             // skip scenes whose frame has ended
+    int n_chunks;                 // 256-particle chunks (rows of block_scene)
 };
 
 // Host-side handles of the step kernels (implemented in step_kernels.cu).

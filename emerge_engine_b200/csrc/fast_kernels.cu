@@ -49,19 +49,51 @@ __global__ void __launch_bounds__(THREADS, EMERGE_DENSITY_CTAS_PER_SM) k_density
     density_pass<MASK>(a);
 }
 
-// Batched scenes: every CTA finds its scene in the batch's tables; all model sets.
-template <unsigned MASK>
+// Batched scenes: every chunk of 256 particles finds its scene in the batch's tables; all
+// model sets.  A CTA works through K consecutive chunks (K x 256 particles per CTA, an
+// autotuned choice), with a barrier between chunks so the per-chunk shared state (materials,
+// CFL reduction) starts afresh.
+template <unsigned MASK, int K>
 __global__ void __launch_bounds__(THREADS, EMERGE_PARTICLE_CTAS_PER_SM) k_particle_batch(ParticleKernelArgs a) {
-    particle_pass<MASK, true, 0, true>(a);
+#pragma unroll 1
+    for (int c = 0; c < K; ++c) {
+        const int chunk = static_cast<int>(blockIdx.x) * K + c;
+        if (chunk >= a.batch.n_chunks) break;  // CTA-uniform
+        if (c > 0) __syncthreads();
+        particle_pass<MASK, true, 0, true>(a, chunk);
+    }
 }
-template <unsigned MASK>
+template <unsigned MASK, int K>
 __global__ void __launch_bounds__(THREADS, EMERGE_DENSITY_CTAS_PER_SM) k_density_batch(DensityKernelArgs a) {
-    density_pass<MASK, true>(a);
+#pragma unroll 1
+    for (int c = 0; c < K; ++c) {
+        const int chunk = static_cast<int>(blockIdx.x) * K + c;
+        if (chunk >= a.batch.n_chunks) break;
+        if (c > 0) __syncthreads();
+        density_pass<MASK, true>(a, chunk);
+    }
+}
+
+template <int K>
+void batch_particle_launch(const ParticleKernelArgs &a, unsigned model_mask, cudaStream_t stream) {
+    const int grid = (a.batch.n_chunks + K - 1) / K;
+    if ((model_mask & ~ALL_MODELS) == 0u)
+        k_particle_batch<ALL_MODELS, K><<<grid, THREADS, 0, stream>>>(a);
+    else
+        k_particle_batch<FULL_MODELS, K><<<grid, THREADS, 0, stream>>>(a);
+}
+template <int K>
+void batch_density_launch(const DensityKernelArgs &a, unsigned model_mask, cudaStream_t stream) {
+    const int grid = (a.batch.n_chunks + K - 1) / K;
+    if ((model_mask & ~ALL_MODELS) == 0u)
+        k_density_batch<ALL_MODELS, K><<<grid, THREADS, 0, stream>>>(a);
+    else
+        k_density_batch<FULL_MODELS, K><<<grid, THREADS, 0, stream>>>(a);
 }
 
 void launch_particle_pass_batch(const DevParticles &P, const BatchView &b, int n_blocks,
                                 const LoadFlagsHost &lf, unsigned model_mask, int mode_g2p,
-                                int emit_p2g, int aggregate, cudaStream_t stream) {
+                                int emit_p2g, int aggregate, int chunks, cudaStream_t stream) {
     if (n_blocks <= 0) return;
     ParticleKernelArgs a;
     std::memset(&a, 0, sizeof(a));
@@ -74,15 +106,15 @@ void launch_particle_pass_batch(const DevParticles &P, const BatchView &b, int n
     a.emit_p2g = emit_p2g;
     a.aggregate = aggregate;
     a.batch = b;
-    if ((model_mask & ~ALL_MODELS) == 0u)
-        k_particle_batch<ALL_MODELS><<<n_blocks, THREADS, 0, stream>>>(a);
-    else
-        k_particle_batch<FULL_MODELS><<<n_blocks, THREADS, 0, stream>>>(a);
+    a.batch.n_chunks = n_blocks;
+    if (chunks >= 4) batch_particle_launch<4>(a, model_mask, stream);
+    else if (chunks == 2) batch_particle_launch<2>(a, model_mask, stream);
+    else batch_particle_launch<1>(a, model_mask, stream);
 }
 
 void launch_density_pass_batch(const DevParticles &P, const BatchView &b, int n_blocks,
                                const LoadFlagsHost &lf, unsigned model_mask, int aggregate,
-                               cudaStream_t stream) {
+                               int chunks, cudaStream_t stream) {
     if (n_blocks <= 0) return;
     DensityKernelArgs a;
     std::memset(&a, 0, sizeof(a));
@@ -92,10 +124,10 @@ void launch_density_pass_batch(const DevParticles &P, const BatchView &b, int n_
     a.lf.pinned = lf.pinned;
     a.aggregate = aggregate;
     a.batch = b;
-    if ((model_mask & ~ALL_MODELS) == 0u)
-        k_density_batch<ALL_MODELS><<<n_blocks, THREADS, 0, stream>>>(a);
-    else
-        k_density_batch<FULL_MODELS><<<n_blocks, THREADS, 0, stream>>>(a);
+    a.batch.n_chunks = n_blocks;
+    if (chunks >= 4) batch_density_launch<4>(a, model_mask, stream);
+    else if (chunks == 2) batch_density_launch<2>(a, model_mask, stream);
+    else batch_density_launch<1>(a, model_mask, stream);
 }
 
 void launch_particle_pass_fast(const ParticleKernelArgs &a, unsigned model_mask, cudaStream_t stream) {

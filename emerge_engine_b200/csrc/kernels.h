@@ -65,12 +65,13 @@ void launch_substep_begin_batch(const BatchView &b, StepState *batch_st, int use
 void launch_prime_setup_batch(const BatchView &b, cudaStream_t stream);
 // particle pass (mode_g2p, emit_p2g as launch_particle_pass) and density pass over all
 // CTAs of a batch; lf: union of the scenes' load flags, model_mask: union of their models
+// chunks: 256-particle chunks per CTA (1, 2 or 4)
 void launch_particle_pass_batch(const DevParticles &P, const BatchView &b, int n_blocks,
                                 const LoadFlagsHost &lf, unsigned model_mask, int mode_g2p,
-                                int emit_p2g, int aggregate, cudaStream_t stream);
+                                int emit_p2g, int aggregate, int chunks, cudaStream_t stream);
 void launch_density_pass_batch(const DevParticles &P, const BatchView &b, int n_blocks,
                                const LoadFlagsHost &lf, unsigned model_mask, int aggregate,
-                               cudaStream_t stream);
+                               int chunks, cudaStream_t stream);
 
 // det_kernels.cu (reference-order mode)
 void launch_project(const StepLaunch &L);
@@ -116,11 +117,14 @@ void launch_sort_keys(const float2 *x, int n, int res, int key_mode, uint32_t *k
 int sort_key_bits(int res, int key_mode);
 // Sorts (keys[0], vals[0]) stably by key; result lands in (keys[r], vals[r]), r returned.
 int radix_sort_pairs(SortScratch &s, int n, int key_bits, cudaStream_t stream);
-// Batched scenes: keys (scene << 20 | tile key) of the compact particle list and the
-// permutation back into each scene's slot range.
+// Batched scenes: keys (scene << 20 | spatial key) of the compact particle list and the
+// permutation back into each scene's slot range.  `shape`, the order the sort gives each
+// scene's particles (what patch of grid a CTA's chunk covers): 0 8 x 8-cell tiles in Morton
+// order, cells row by row inside; 1 the same tiles, cells in Morton order inside; 2 16 x 16
+// blocks in Morton order, each as four 16 x 4 strips; 3 the same blocks as four 4 x 16 strips.
 int batch_sort_key_bits(int n_scenes);
 void launch_batch_sort_keys(const SceneDesc *scenes, const int *compact_start, int n_scenes,
-                            const DevParticles &P, int total, uint32_t *keys, uint32_t *vals,
+                            const DevParticles &P, int total, uint32_t *keys, uint32_t *vals, int shape,
                             cudaStream_t stream);
 void launch_permute_batch(const DevParticles &src, const DevParticles &dst, const uint32_t *keys,
                           const uint32_t *vals, const SceneDesc *scenes, const int *compact_start, int total,

@@ -758,10 +758,10 @@ struct ParticleKernelArgs {
 // Scene of this CTA in a batch (nullptr for single-scene kernels); false when the scene
 // does not take part in the running substep (the whole CTA returns).
 template <bool BATCH, class Args>
-__device__ __forceinline__ bool batch_scene(const Args &a, const SceneDesc *&sd) {
+__device__ __forceinline__ bool batch_scene(const Args &a, const SceneDesc *&sd, int blk) {
     sd = nullptr;
     if constexpr (BATCH) {
-        sd = &a.batch.scenes[a.batch.block_scene[blockIdx.x]];
+        sd = &a.batch.scenes[a.batch.block_scene[blk]];
         if (a.batch.check_active && !sd->st->active) return false;
     }
     return true;
@@ -1046,12 +1046,14 @@ __device__ __forceinline__ void closure_enqueue(const ClosureArgs &cl, StepState
 // CLOSURE: 0 none; 1 the learned closure evaluated inside the pass (warp-level MMA); 2 the
 // particles the network maps are queued for the tile kernel (closure_tiles.cu), which
 // finishes their update, CFL bound, projection and P2G.
+// blk: the 256-particle chunk this CTA works on (blockIdx.x; batched CTAs may take several
+// chunks in turn, see k_particle_batch).
 template <unsigned MASK, bool FAST, int CLOSURE = 0, bool BATCH = false>
-__device__ __forceinline__ void particle_pass(const ParticleKernelArgs &a) {
+__device__ __forceinline__ void particle_pass(const ParticleKernelArgs &a, int blk = blockIdx.x) {
     __shared__ MatP s_mats[MAX_MATERIALS];
     __shared__ uint32_t s_max_speed, s_min_mdt, s_warps_done;
     const SceneDesc *sd;
-    if (!batch_scene<BATCH>(a, sd)) return;
+    if (!batch_scene<BATCH>(a, sd, blk)) return;
     // this CTA's scene: the kernel arguments, or the batch's scene table
     const DevConfig &cfg = [&]() -> const DevConfig & { if constexpr (BATCH) return sd->cfg; else return a.cfg; }();
     const GridView &g = [&]() -> const GridView & { if constexpr (BATCH) return sd->g; else return a.g; }();
@@ -1059,8 +1061,8 @@ __device__ __forceinline__ void particle_pass(const ParticleKernelArgs &a) {
     const int n_mats = BATCH ? sd->n_mats : a.n_mats;
     const int density_mode = BATCH ? sd->density_mode : a.density_mode;
     StepState *st = BATCH ? sd->st : a.st;
-    const int i = BATCH ? sd->p0 + (static_cast<int>(blockIdx.x) - sd->block0) * THREADS + static_cast<int>(threadIdx.x)
-                        : static_cast<int>(blockIdx.x) * THREADS + static_cast<int>(threadIdx.x);
+    const int i = BATCH ? sd->p0 + (blk - sd->block0) * THREADS + static_cast<int>(threadIdx.x)
+                        : blk * THREADS + static_cast<int>(threadIdx.x);
     const bool in_range = BATCH ? i < sd->p0 + sd->n : i < a.n;
     // sleep partition: particles outside the active zone take no part in the substep
     uint32_t zb = 0u;
@@ -1281,18 +1283,18 @@ struct DensityKernelArgs {
 // estimate_particle_volumes gather (solver/density.rs:50-71) at the projected
 // positions, stored as rho_dp, plus the stress scatter of fluid particles.
 template <unsigned MASK, bool BATCH = false>
-__device__ __forceinline__ void density_pass(const DensityKernelArgs &a) {
+__device__ __forceinline__ void density_pass(const DensityKernelArgs &a, int blk = blockIdx.x) {
     __shared__ MatP s_mats[MAX_MATERIALS];
     const SceneDesc *sd;
-    if (!batch_scene<BATCH>(a, sd)) return;
+    if (!batch_scene<BATCH>(a, sd, blk)) return;
     if (BATCH && !sd->density_mode) return;  // no material of the scene needs the pass
     const DevConfig &cfg = [&]() -> const DevConfig & { if constexpr (BATCH) return sd->cfg; else return a.cfg; }();
     const GridView &g = [&]() -> const GridView & { if constexpr (BATCH) return sd->g; else return a.g; }();
     const MatP *mats = BATCH ? sd->mats : a.mats;
     const int n_mats = BATCH ? sd->n_mats : a.n_mats;
     StepState *st = BATCH ? sd->st : a.st;
-    const int i = BATCH ? sd->p0 + (static_cast<int>(blockIdx.x) - sd->block0) * THREADS + static_cast<int>(threadIdx.x)
-                        : static_cast<int>(blockIdx.x) * THREADS + static_cast<int>(threadIdx.x);
+    const int i = BATCH ? sd->p0 + (blk - sd->block0) * THREADS + static_cast<int>(threadIdx.x)
+                        : blk * THREADS + static_cast<int>(threadIdx.x);
     bool valid = BATCH ? i < sd->p0 + sd->n : i < a.n;
     if constexpr (HAS_MODEL(MASK, M_EXTRAS_BIT))
         if (cfg.zones && valid) valid = (a.P.sleeping[i] & ZB_OUT) == 0u;

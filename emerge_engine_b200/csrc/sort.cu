@@ -307,7 +307,7 @@ __device__ __forceinline__ int scene_of(const int *compact_start, int n_scenes, 
 }
 
 __global__ void k_batch_sort_keys(const SceneDesc *scenes, const int *compact_start, int n_scenes,
-                                  DevParticles P, int total, uint32_t *keys, uint32_t *vals) {
+                                  DevParticles P, int total, uint32_t *keys, uint32_t *vals, int shape) {
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= total) return;
     const int s = scene_of(compact_start, n_scenes, c);
@@ -318,8 +318,16 @@ __global__ void k_batch_sort_keys(const SceneDesc *scenes, const int *compact_st
     const float fx = fminf(fmaxf(floorf(p.x), 0.0f), static_cast<float>(res - 1));
     const float fy = fminf(fmaxf(floorf(p.y), 0.0f), static_cast<float>(res - 1));
     const uint32_t cx = static_cast<uint32_t>(fx), cy = static_cast<uint32_t>(fy);
-    keys[c] = (static_cast<uint32_t>(s) << BATCH_TILE_KEY_BITS) |
-              (morton2(cx >> 3, cy >> 3) << 6) | ((cx & 7u) << 3) | (cy & 7u);
+    uint32_t k;  // spatial key below 2^20 for grids up to 1024^2
+    if (shape == 1)
+        k = (morton2(cx >> 3, cy >> 3) << 6) | morton2(cx & 7u, cy & 7u);
+    else if (shape == 2)  // 16 x 16 blocks, four 16 x 4 strips each
+        k = (morton2(cx >> 4, cy >> 4) << 8) | (((cy >> 2) & 3u) << 6) | ((cx & 15u) << 2) | (cy & 3u);
+    else if (shape == 3)  // 16 x 16 blocks, four 4 x 16 strips each
+        k = (morton2(cx >> 4, cy >> 4) << 8) | (((cx >> 2) & 3u) << 6) | ((cy & 15u) << 2) | (cx & 3u);
+    else
+        k = (morton2(cx >> 3, cy >> 3) << 6) | ((cx & 7u) << 3) | (cy & 7u);
+    keys[c] = (static_cast<uint32_t>(s) << BATCH_TILE_KEY_BITS) | k;
     vals[c] = static_cast<uint32_t>(slot);
 }
 
@@ -339,11 +347,11 @@ int batch_sort_key_bits(int n_scenes) {
 }
 
 void launch_batch_sort_keys(const SceneDesc *scenes, const int *compact_start, int n_scenes,
-                            const DevParticles &P, int total, uint32_t *keys, uint32_t *vals,
+                            const DevParticles &P, int total, uint32_t *keys, uint32_t *vals, int shape,
                             cudaStream_t stream) {
     if (total > 0)
         k_batch_sort_keys<<<(total + 255) / 256, 256, 0, stream>>>(scenes, compact_start, n_scenes, P, total,
-                                                                  keys, vals);
+                                                                  keys, vals, shape);
 }
 
 void launch_permute_batch(const DevParticles &src, const DevParticles &dst, const uint32_t *keys,

@@ -589,10 +589,17 @@ class Batch:
     def set_option(self, option: int, value: int) -> None:
         self._check(self._lib.emerge_cuda_batch_set_option(self._b, int(option), int(value)))
 
-    def autotune(self, steps_per_trial: int = 2) -> dict:
+    def autotune(self, steps_per_trial: int = 2, cache_path: str | None = None) -> dict:
+        """Tile shape, particles per CTA, sort interval and P2G aggregation for this batch
+        (emerge_cuda_batch_autotune); `cache_path`: the tuning cache file (None = none)."""
         rep = abi.BatchTuneReportC()
-        self._check(self._lib.emerge_cuda_batch_autotune(self._b, int(steps_per_trial), byref(rep)))
+        path = cache_path.encode() if cache_path else None
+        self._check(self._lib.emerge_cuda_batch_autotune(self._b, int(steps_per_trial), path, byref(rep)))
         n = rep.n_trials
         return {"sort_interval": rep.sort_interval, "aggregate": rep.aggregate,
-                "trials": [{"sort_interval": rep.trial_sort_interval[k], "aggregate": rep.trial_aggregate[k],
+                "tile_shape": rep.tile_shape, "chunks_per_cta": rep.chunks_per_cta,
+                "particles_per_cta": 256 * rep.chunks_per_cta, "from_cache": bool(rep.from_cache),
+                "best_ms_per_step": rep.best_ms,
+                "trials": [{"tile_shape": rep.trial_tile_shape[k], "chunks_per_cta": rep.trial_chunks[k],
+                            "sort_interval": rep.trial_sort_interval[k], "aggregate": rep.trial_aggregate[k],
                             "ms_per_step": rep.trial_ms[k]} for k in range(n)]}

@@ -389,7 +389,14 @@ enum {
     EMERGE_OPT_SORT_INTERVAL = 2,
     EMERGE_OPT_P2G_AGGREGATE = 3,
     EMERGE_OPT_DETERMINISTIC = 4,
-    EMERGE_OPT_PRECISE_MATH = 5
+    EMERGE_OPT_PRECISE_MATH = 5,
+    EMERGE_OPT_TILE_SHAPE = 7,      /* batches: the particle order the sort gives each scene (what
+                                     * patch of grid a CTA covers): 0 8 x 8-cell tiles in Morton
+                                     * order, cells row by row (default); 1 the same tiles, cells
+                                     * in Morton order; 2 16 x 16 blocks of four 16 x 4 strips;
+                                     * 3 16 x 16 blocks of four 4 x 16 strips */
+    EMERGE_OPT_CHUNKS_PER_CTA = 8   /* batches: particles per CTA of the particle and density
+                                     * passes, in chunks of 256: 1 (default), 2 or 4 */
 };
 emerge_status emerge_cuda_set_option(emerge_sim *sim, int option, int64_t value);
 
@@ -563,13 +570,20 @@ emerge_status emerge_cuda_mlp_infer_tc(const float *params, const float *x, uint
  * copied; the simulations stay usable and independent).  Scenes run the fast path. */
 typedef struct emerge_batch emerge_batch;
 
+#define EMERGE_TUNE_MAX_TRIALS 16
 typedef struct emerge_batch_tune_report {
     int32_t sort_interval;       /* chosen */
-    int32_t aggregate;           /* chosen P2G warp aggregation */
+    int32_t aggregate;           /* chosen P2G warp aggregation (0 / 1) */
+    int32_t tile_shape;          /* chosen EMERGE_OPT_TILE_SHAPE */
+    int32_t chunks_per_cta;      /* chosen EMERGE_OPT_CHUNKS_PER_CTA */
     uint32_t n_trials;
-    int32_t trial_sort_interval[8];
-    int32_t trial_aggregate[8];
-    float trial_ms[8];           /* GPU ms per frame of each trial */
+    uint32_t from_cache;         /* 1: taken from the cache file, no trials run */
+    float best_ms;               /* GPU ms per frame of the chosen setting (0 from the cache) */
+    int32_t trial_sort_interval[EMERGE_TUNE_MAX_TRIALS];
+    int32_t trial_aggregate[EMERGE_TUNE_MAX_TRIALS];
+    int32_t trial_tile_shape[EMERGE_TUNE_MAX_TRIALS];
+    int32_t trial_chunks[EMERGE_TUNE_MAX_TRIALS];
+    float trial_ms[EMERGE_TUNE_MAX_TRIALS];  /* GPU ms per frame of each trial */
 } emerge_batch_tune_report;
 
 emerge_status emerge_cuda_batch_create(emerge_sim *const *sims, uint32_t n_sims, emerge_batch **out);
@@ -589,11 +603,18 @@ emerge_status emerge_cuda_batch_region_state(emerge_batch *batch, uint32_t scene
                                              emerge_body_state *out);
 /* Per scene: substeps of the last frame (last) and lifetime substeps (total); either may be NULL. */
 emerge_status emerge_cuda_batch_substeps(emerge_batch *batch, uint64_t *last, uint64_t *total);
-/* EMERGE_OPT_USE_GRAPH, EMERGE_OPT_SORT_INTERVAL, EMERGE_OPT_P2G_AGGREGATE. */
+/* EMERGE_OPT_USE_GRAPH, EMERGE_OPT_SORT_INTERVAL, EMERGE_OPT_P2G_AGGREGATE,
+ * EMERGE_OPT_TILE_SHAPE, EMERGE_OPT_CHUNKS_PER_CTA. */
 emerge_status emerge_cuda_batch_set_option(emerge_batch *batch, int option, int64_t value);
-/* Times every (sort interval, P2G aggregation) candidate for steps_per_trial frames on the
- * batch itself and keeps the fastest (the batch advances by 8 x steps_per_trial frames). */
-emerge_status emerge_cuda_batch_autotune(emerge_batch *batch, uint32_t steps_per_trial,
+/* Autotuner (no reference counterpart): picks the tile shape, the particles per CTA, the
+ * sort interval and the P2G warp aggregation for this batch by coordinate descent -- each knob
+ * in turn takes every value (4 + 3 + 3 + 2 trials; each re-sorts, runs one untimed frame
+ * and times steps_per_trial frames), keeping the fastest -- and applies the result; the batch advances by those
+ * frames.  None of the knobs changes a result beyond float summation order.  cache_path
+ * (NULL or "" = none): a text file of tuned settings keyed by the batch's signature (device
+ * name, SM count, every scene's grid size, particle count and model set); a hit applies the
+ * stored setting without trials, a tuned setting is stored. */
+emerge_status emerge_cuda_batch_autotune(emerge_batch *batch, uint32_t steps_per_trial, const char *cache_path,
                                          emerge_batch_tune_report *report);
 
 #ifdef __cplusplus

@@ -113,18 +113,33 @@ def mixed_granular(sim_cls, grid_res=1024, target_particles=4_000_000, seed=42, 
 
 
 def batched_scenes(sim_cls, n_scenes=256, seed=7, grid_range=(64, 256), n_range=(4_000, 200_000),
-                   **sim_kw):
+                   pair_sizes=False, **sim_kw):
     """Independent scenes for the batched path: per scene a seeded grid size G ~ U{64..256},
     a particle target N ~ logU[4k, 200k] and a material uniform over {NewtonianFluid,
     DruckerPrager sand, Stomakhin snow, NeoHookean}; one square block at 4 particles per cell
     (seeded jitter) resting on the floor of a G^2 grid, clipped to fit inside the walls (so
-    small grids hold fewer particles than their target).  Returns the list of simulations."""
+    small grids hold fewer particles than their target).  With pair_sizes, the drawn grid
+    sizes and particle counts are paired by rank (the largest count with the largest grid),
+    which keeps both distributions as drawn and lets every block fit at 4 particles per cell:
+    256 scenes then hold the ~12.8M particles the two distributions give (mean N ~ 50k).
+    Returns the list of simulations."""
     rng = np.random.default_rng(seed)
-    sims = []
+    draws = []
     for k in range(n_scenes):
         g = int(rng.integers(grid_range[0], grid_range[1] + 1))
         target = float(np.exp(rng.uniform(np.log(n_range[0]), np.log(n_range[1]))))
         kind = int(rng.integers(4))
+        draws.append((g, target, kind))
+    if pair_sizes:
+        gs = sorted(d[0] for d in draws)
+        ns = sorted(d[1] for d in draws)
+        order = np.argsort([d[0] for d in draws], kind="stable")
+        paired = list(draws)
+        for rank, k in enumerate(order):
+            paired[k] = (gs[rank], ns[rank], draws[k][2])
+        draws = paired
+    sims = []
+    for k, (g, target, kind) in enumerate(draws):
         cfg = SimConfig.standard(g, 0.05, (0.0, -1.0))
         t = cfg.boundary_thickness
         if kind == 0:

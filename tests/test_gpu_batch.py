@@ -98,12 +98,45 @@ def test_batch_matches_single_scenes(cuda_lib):
     assert int(total.sum()) >= steps * len(singles)
 
 
-def test_autotune_picks_a_candidate(cuda_lib):
+def test_autotune_picks_the_fastest_trial_and_caches_it(cuda_lib, tmp_path):
     batch = Batch(scenes.batched_scenes(Simulation, n_scenes=12, seed=5, grid_range=(64, 128),
                                         n_range=(2_000, 20_000)))
-    rep = batch.autotune(steps_per_trial=1)
-    assert len(rep["trials"]) == 8
+    cache = str(tmp_path / "tune.txt")
+    rep = batch.autotune(steps_per_trial=1, cache_path=cache)
+    assert not rep["from_cache"] and len(rep["trials"]) == 12
+    assert {t["tile_shape"] for t in rep["trials"]} == {0, 1, 2, 3}
+    assert {t["chunks_per_cta"] for t in rep["trials"]} == {1, 2, 4}
     best = min(rep["trials"], key=lambda t: t["ms_per_step"])
-    assert (rep["sort_interval"], rep["aggregate"]) == (best["sort_interval"], best["aggregate"])
+    assert rep["best_ms_per_step"] == pytest.approx(best["ms_per_step"])
+    chosen = (rep["tile_shape"], rep["chunks_per_cta"], rep["sort_interval"], rep["aggregate"])
+    assert chosen == (best["tile_shape"], best["chunks_per_cta"], best["sort_interval"], best["aggregate"])
     batch.step(2)
     assert np.all(np.isfinite(batch.particles(0)["x"]))
+    # a batch of the same signature takes the stored choice without trials
+    again = Batch(scenes.batched_scenes(Simulation, n_scenes=12, seed=5, grid_range=(64, 128),
+                                        n_range=(2_000, 20_000)))
+    rep2 = again.autotune(steps_per_trial=1, cache_path=cache)
+    assert rep2["from_cache"] and len(rep2["trials"]) == 0
+    assert (rep2["tile_shape"], rep2["chunks_per_cta"], rep2["sort_interval"], rep2["aggregate"]) == chosen
+
+
+@pytest.mark.parametrize("shape,chunks", [(1, 2), (2, 4), (3, 1)])
+def test_tile_shapes_and_chunks_change_no_result_beyond_summation_order(cuda_lib, shape, chunks):
+    """Every tuned setting runs the same physics: one frame of the mixed set against the
+    default setting, at the batch-vs-single bars."""
+    from emerge_engine_b200.abi import OPT_CHUNKS_PER_CTA, OPT_TILE_SHAPE
+    sources = mixed_set()
+    a, b = Batch(sources), Batch(sources)  # both copy the same start state
+    for k in range(a.n_scenes):
+        np.testing.assert_array_equal(b.particles(k), a.particles(k))
+    b.set_option(OPT_TILE_SHAPE, shape)
+    b.set_option(OPT_CHUNKS_PER_CTA, chunks)
+    a.step(1)
+    b.step(1)
+    la, _ = a.substeps()
+    lb, _ = b.substeps()
+    for k in range(a.n_scenes):
+        pa, pb = a.particles(k), b.particles(k)
+        assert la[k] == lb[k], k
+        assert pa["mass"].sum(dtype=np.float64) == pb["mass"].sum(dtype=np.float64)
+        assert np.abs(pa["x"].astype(np.float64) - pb["x"]).max() <= 1e-3, k
