@@ -455,11 +455,24 @@ def workload_config(workload: str, particles: int, world: int) -> dict:
 def run_batched(args, spec, rank: int, world: int, dist, local_rank: int) -> dict:
     """Batched scenes: all scenes of the workload advanced together (one launch per kernel
     per substep); value = sum over scenes of particles x substeps per second.  Weak scaling:
-    every rank advances its own scenes (seeded per rank)."""
+    one fixed list of 256 x N seeded scenes is placed on the N ranks by
+    sharding.shard_scenes (longest-processing-time first on particle counts), and each rank
+    advances its share as one batch, with no collective on the data path."""
     from emerge_engine_b200 import Batch, Simulation
     from emerge_engine_b200.build import build
+    from emerge_engine_b200.sharding import shard_loads, shard_scenes
+    from tests import scenes as scene_lib
     build()
-    sims = build_scene(Simulation, args.workload, device=local_rank, seed=7 + rank)
+    kw = dict(WORKLOADS[args.workload]["kwargs"])
+    kw["n_scenes"] = kw.get("n_scenes", 256) * world
+    draws = scene_lib.batched_scene_draws(
+        **{k: v for k, v in kw.items() if k in ("n_scenes", "seed", "pair_sizes")})
+    costs = scene_lib.batched_scene_particles(draws)
+    shards = shard_scenes(costs, world)
+    placement = {"scenes_total": len(draws), "particles_total": int(sum(costs)),
+                 "rank_particles": [int(x) for x in shard_loads(costs, shards)],
+                 "method": "LPT on particle counts (emerge_engine_b200.sharding)"}
+    sims = scene_lib.batched_scenes(Simulation, only=shards[rank], device=local_rank, **kw)
     counts = np.array([s.particle_count() for s in sims], dtype=np.int64)
     batch = Batch(sims)
     for s in sims:
@@ -493,7 +506,7 @@ def run_batched(args, spec, rank: int, world: int, dist, local_rank: int) -> dic
                                   "particle-substep)", "bound": "hbm", "achieved": achieved,
                         "peak": peak, "unit": "GB/s", "frac": achieved / peak, "traffic": None,
                         "peak_source": f"{peak_kind} hbm_gbs (MEASURED_PEAKS.json)"},
-           "autotune": tune}
+           "autotune": tune, "placement": placement}
     batch.close()
     return out
 
@@ -550,6 +563,7 @@ def main():
                 "config": workload_config(args.workload, r["particles"], world),
                 "scenes": r["scenes"], "substeps_per_step_mean": r["substeps_per_step_mean"],
                 "clocks": r["clocks"], "roofline": r["roofline"], "autotune": r["autotune"],
+                "placement": r["placement"],
             }
             if world == 1 and not args.no_extras:
                 line["cpu_baseline"] = cpu_baseline(args.workload, args.cpu_budget)

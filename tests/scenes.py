@@ -112,17 +112,13 @@ def mixed_granular(sim_cls, grid_res=1024, target_particles=4_000_000, seed=42, 
     return sim
 
 
-def batched_scenes(sim_cls, n_scenes=256, seed=7, grid_range=(64, 256), n_range=(4_000, 200_000),
-                   pair_sizes=False, **sim_kw):
-    """Independent scenes for the batched path: per scene a seeded grid size G ~ U{64..256},
-    a particle target N ~ logU[4k, 200k] and a material uniform over {NewtonianFluid,
-    DruckerPrager sand, Stomakhin snow, NeoHookean}; one square block at 4 particles per cell
-    (seeded jitter) resting on the floor of a G^2 grid, clipped to fit inside the walls (so
-    small grids hold fewer particles than their target).  With pair_sizes, the drawn grid
-    sizes and particle counts are paired by rank (the largest count with the largest grid),
-    which keeps both distributions as drawn and lets every block fit at 4 particles per cell:
-    256 scenes then hold the ~12.8M particles the two distributions give (mean N ~ 50k).
-    Returns the list of simulations."""
+def batched_scene_draws(n_scenes=256, seed=7, grid_range=(64, 256), n_range=(4_000, 200_000),
+                        pair_sizes=False):
+    """The seeded per-scene draws of batched_scenes: (grid size G, particle target, material
+    kind) per scene.  With pair_sizes, the drawn grid sizes and particle counts are paired by
+    rank (the largest count with the largest grid), which keeps both distributions as drawn
+    and lets every block fit at 4 particles per cell: 256 scenes then hold the ~12.8M
+    particles the two distributions give (mean N ~ 50k)."""
     rng = np.random.default_rng(seed)
     draws = []
     for k in range(n_scenes):
@@ -138,8 +134,32 @@ def batched_scenes(sim_cls, n_scenes=256, seed=7, grid_range=(64, 256), n_range=
         for rank, k in enumerate(order):
             paired[k] = (gs[rank], ns[rank], draws[k][2])
         draws = paired
+    return draws
+
+
+def _block_side(g, target, thickness=2):
+    return int(min(np.sqrt(target / 4.0), g - 2 * thickness - 6))
+
+
+def batched_scene_particles(draws):
+    """Particles each drawn scene spawns (4 per cell of its side x side block)."""
+    return [4 * _block_side(g, t) ** 2 for g, t, _ in draws]
+
+
+def batched_scenes(sim_cls, n_scenes=256, seed=7, grid_range=(64, 256), n_range=(4_000, 200_000),
+                   pair_sizes=False, only=None, **sim_kw):
+    """Independent scenes for the batched path: per scene a seeded grid size G ~ U{64..256},
+    a particle target N ~ logU[4k, 200k] and a material uniform over {NewtonianFluid,
+    DruckerPrager sand, Stomakhin snow, NeoHookean}; one square block at 4 particles per cell
+    (seeded jitter) resting on the floor of a G^2 grid, clipped to fit inside the walls (so
+    small grids hold fewer particles than their target).  pair_sizes: see
+    batched_scene_draws.  only: the indices of the scenes to build (a rank's share of one
+    fixed list; each scene's seeds depend on its index only).  Returns the simulations."""
+    draws = batched_scene_draws(n_scenes, seed, grid_range, n_range, pair_sizes)
+    keep = range(n_scenes) if only is None else only
     sims = []
-    for k, (g, target, kind) in enumerate(draws):
+    for k in keep:
+        g, target, kind = draws[k]
         cfg = SimConfig.standard(g, 0.05, (0.0, -1.0))
         t = cfg.boundary_thickness
         if kind == 0:
@@ -151,7 +171,7 @@ def batched_scenes(sim_cls, n_scenes=256, seed=7, grid_range=(64, 256), n_range=
         else:
             mat = NeoHookeanMaterial.new(400.0, 200.0)
         sim = sim_cls.empty(cfg, **sim_kw).with_default_material(mat)
-        side = int(min(np.sqrt(target / 4.0), g - 2 * t - 6))
+        side = _block_side(g, target, t)
         s = SpawnRegion.for_sim(cfg)
         s.spacing = 0.5
         s.box_size = (side, side)
