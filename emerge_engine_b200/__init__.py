@@ -11,6 +11,6 @@ from .materials import (BinghamFluidMaterial, CorotatedMaterial,  # noqa: F401
                         ViscoelasticMaterial, VonMisesMaterial, lame_from_young, to_radians,
                         WithMixturePhase, SOLID_PHASE, FLUID_PHASE, DirectionalContactGrip)
 from .fields import (AabbConfinementField, BuoyancyField, ChemotaxisField,  # noqa: F401
-                     CoulombField, GravityWellField, LinearDragField, RadialConfinementField,
-                     UniformElectricField)
+                     CoulombField, GravityWellField, LinearDragField, NBodyGravityField,
+                     RadialConfinementField, UniformElectricField, orbit)
 from .simulation import Batch, DeterministicSimulation, MaterialRegistry, Simulation  # noqa: F401

@@ -198,6 +198,7 @@ ABI_FUNCTIONS = [
     ("emerge_cuda_set_slip_boundaries", c_int, [SIM, POINTER(c_uint64), c_uint32]),
     ("emerge_cuda_set_force_fields", c_int, [SIM, POINTER(ForceFieldC), c_uint32, POINTER(c_float),
                                              c_uint64]),
+    ("emerge_cuda_field_accelerations", c_int, [SIM, POINTER(c_float), c_uint64]),
     ("emerge_cuda_set_contact_grip", c_int, [SIM, c_int, c_float, c_float, c_float, c_float]),
     ("emerge_cuda_set_mixture_phases", c_int, [SIM, POINTER(c_uint32), c_uint32]),
     ("emerge_cuda_active_count", c_int, [SIM, POINTER(c_uint64)]),

@@ -42,6 +42,7 @@ SOURCES = {
     "closure.cu": FAST,
     "closure_tiles.cu": FAST,
     "batch.cu": EXACT,
+    "nbody.cu": EXACT,
 }
 HEADERS = ["physics.cuh", "device_state.cuh", "kernels.h", "particle_pass.cuh", "closure.cuh", "closure_host.h",
            "multifield.cuh"]

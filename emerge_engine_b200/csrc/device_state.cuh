@@ -109,6 +109,7 @@ struct GridView {
 // StepState::error_flags bits
 constexpr uint32_t ERR_CONTACT_LIST = 1u;  // a contact point-list walk was cut short
 constexpr uint32_t ERR_CLOSURE_WAIT = 2u;  // a closure tile's tensor-core wait gave up (kernel returned)
+constexpr uint32_t ERR_NBODY_SKIPPED = 4u; // an n-body node seen as far had no center of mass
 
 __host__ __device__ __forceinline__ int cell_index(int x, int y, int tpd) {
     return (((x >> 3) * tpd + (y >> 3)) << 6) | ((x & 7) << 3) | (y & 7);

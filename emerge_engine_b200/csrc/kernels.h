@@ -28,9 +28,39 @@ inline bool closure_tiles_on(const StepLaunch &L) {
 }
 
 // step_kernels.cu
+// nbody.cu: NBodyGravityField's quadtree (NBodyView), rebuilt each substep.
+struct SortScratch;
+struct NBodyBounds {
+    uint32_t lo[2], hi[2];          // order-preserving bits of the bodies' min / max x, y
+    uint32_t all_lo[2], all_hi[2];  // ... of every particle's position
+    uint32_t n_bodies;              // particles of positive mass
+};
+struct NBodyTreeHost {
+    int depth = -1;          // max_depth; -1: no NBodyGravityField
+    int max_bodies = 0;      // max_bodies_per_node
+    float theta_max = 0.0f;  // largest theta over the NBody fields (which nodes may be far)
+    float4 *root = nullptr;
+    float4 *body = nullptr;
+    uint2 *range = nullptr;
+    float4 *com = nullptr;
+    NBodyBounds *bounds = nullptr;
+};
+// Builds the tree over the n particles of P on `stream` (the key sort uses `sort`, which
+// must hold n entries); returns the kernels launched.
+int launch_nbody_build(const NBodyTreeHost &t, const DevParticles &P, int n, SortScratch &sort,
+                       cudaStream_t stream);
+// The kernels launch_nbody_build launches for n particles.
+inline int nbody_build_kernels(int depth, int n) {
+    const int bits = 2 * depth + 1;
+    return 3 + (n > 0 ? 2 : 0) + (n > 1 ? 5 * ((bits + 7) / 8) : 0);
+}
+
+// split: 0 one pass; 1 / 2 its G2P and fields halves (ParticleKernelArgs::split)
 void launch_particle_pass(const StepLaunch &L, const LoadFlagsHost &lf, int mode_g2p,
-                          int project_in, int emit_p2g);
+                          int project_in, int emit_p2g, int split = 0);
 void launch_density_pass(const StepLaunch &L, const LoadFlagsHost &lf);
+// Sum of the force fields' accelerations per particle, out[reference index] (n-body tree built).
+void launch_field_accelerations(const StepLaunch &L, const LoadFlagsHost &lf, float2 *out);
 void launch_grid_update(const StepLaunch &L);
 void launch_step_begin(const StepLaunch &L);
 void launch_substep_begin(const StepLaunch &L, int use_cond, unsigned long long handle,

@@ -1,0 +1,258 @@
+// nbody.cu -- NBodyGravityField's Barnes-Hut quadtree (forces/fields/n_body.rs:63-283),
+// rebuilt on the device once per substep, between the G2P half and the fields half of the
+// particle pass (the reference's prepare() after G2P, step.rs:221-226).
+//
+// The reference inserts the particles of positive mass one at a time in index order into a
+// pointer quadtree.  Its shape does not depend on that order: a node below max_depth is
+// split exactly when more than max_bodies_per_node bodies fall into it.  The device
+// therefore builds it in four data-parallel steps:
+//   1. bounds   the bodies' bounding box (the root box, n_body.rs:228-247) and that of every
+//               particle (where the field is evaluated), by warp reductions and atomics;
+//   2. keys     each body's quadrant path from the root (2 bits per level, the boxes'
+//               centers computed as the reference's insertion computes them) written at its
+//               reference index, so that the stable radix sort keeps index order among
+//               equal paths; particles without mass sort behind every body;
+//   3. ranges   after the sort, each body's slot at every level opens or closes a run of
+//               equal path prefixes: the bodies of every node, in insertion order;
+//   4. centers  each node's total mass and center of mass, folded over its run in
+//               insertion order with the reference's incremental update (MassProps::add,
+//               n_body.rs:96-107), one thread per node.  A node that no particle can see as
+//               far (its width over the largest distance to any particle is at least theta)
+//               is never asked for its center and is not folded: typically the root and
+//               its four children, whose folds would be the longest.
+// The fold and every box center use the reference's operations in the same order with
+// IEEE rounding, so the tree -- and the field's accelerations -- match the reference bit
+// for bit on both pipelines.
+#include "device_state.cuh"
+#include "kernels.h"
+
+namespace emerge {
+
+namespace {
+
+constexpr int NB_THREADS = 256;
+constexpr float EMPTY_TREE_HALF_SIZE = 1000.0f;  // n_body.rs:38
+constexpr float AABB_PADDING_RATIO = 0.1f;       // n_body.rs:42
+constexpr float AABB_PADDING_MIN = 1.0f;         // n_body.rs:46
+
+// Order-preserving map of a float to uint (for atomicMin / atomicMax) and back.
+__device__ __forceinline__ uint32_t ord_bits(float f) {
+    const uint32_t b = __float_as_uint(f);
+    return (b & 0x80000000u) ? ~b : (b | 0x80000000u);
+}
+__device__ __forceinline__ float ord_float(uint32_t u) {
+    return __uint_as_float((u & 0x80000000u) ? (u & 0x7fffffffu) : ~u);
+}
+
+__device__ __forceinline__ uint32_t warp_min_u(uint32_t v) {
+    for (int o = 16; o > 0; o >>= 1) v = min(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
+__device__ __forceinline__ uint32_t warp_max_u(uint32_t v) {
+    for (int o = 16; o > 0; o >>= 1) v = max(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
+
+__global__ void k_nb_reset(NBodyBounds *b) {
+    if (threadIdx.x == 0) {
+        for (int k = 0; k < 2; ++k) {
+            b->lo[k] = 0xffffffffu;
+            b->hi[k] = 0u;
+            b->all_lo[k] = 0xffffffffu;
+            b->all_hi[k] = 0u;
+        }
+        b->n_bodies = 0u;
+    }
+}
+
+// Step 1.  A NaN coordinate is left out of its minimum and maximum, as f32::min / max do.
+__global__ void k_nb_bounds(const float2 *x, const float *mass, int n, NBodyBounds *b) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    float2 p = make_float2(0.0f, 0.0f);
+    float m = 0.0f;
+    if (i < n) {
+        p = x[i];
+        m = mass[i];
+    }
+    const bool body = i < n && m > 0.0f;
+    const uint32_t ox = ord_bits(p.x), oy = ord_bits(p.y);
+    const bool fx = i < n && p.x == p.x, fy = i < n && p.y == p.y;
+    const uint32_t lo_x = warp_min_u(fx && body ? ox : 0xffffffffu), hi_x = warp_max_u(fx && body ? ox : 0u);
+    const uint32_t lo_y = warp_min_u(fy && body ? oy : 0xffffffffu), hi_y = warp_max_u(fy && body ? oy : 0u);
+    const uint32_t alo_x = warp_min_u(fx ? ox : 0xffffffffu), ahi_x = warp_max_u(fx ? ox : 0u);
+    const uint32_t alo_y = warp_min_u(fy ? oy : 0xffffffffu), ahi_y = warp_max_u(fy ? oy : 0u);
+    const uint32_t nb = __popc(__ballot_sync(0xffffffffu, body));
+    if ((threadIdx.x & 31) == 0) {
+        if (nb) {
+            atomicMin(&b->lo[0], lo_x);
+            atomicMax(&b->hi[0], hi_x);
+            atomicMin(&b->lo[1], lo_y);
+            atomicMax(&b->hi[1], hi_y);
+            atomicAdd(&b->n_bodies, nb);
+        }
+        atomicMin(&b->all_lo[0], alo_x);
+        atomicMax(&b->all_hi[0], ahi_x);
+        atomicMin(&b->all_lo[1], alo_y);
+        atomicMax(&b->all_hi[1], ahi_y);
+    }
+}
+
+// Quadtree::build's root box (n_body.rs:217-256): the bodies' box padded by 10 % of its
+// width plus height and one cell, then squared about its center.
+__device__ __forceinline__ float4 nb_root(const NBodyBounds &b) {
+    if (b.n_bodies == 0u) return make_float4(0.0f, 0.0f, EMPTY_TREE_HALF_SIZE, 0.0f);
+    float min_x = b.lo[0] == 0xffffffffu ? 3.40282347e38f : ord_float(b.lo[0]);
+    float min_y = b.lo[1] == 0xffffffffu ? 3.40282347e38f : ord_float(b.lo[1]);
+    float max_x = b.hi[0] == 0u ? -3.40282347e38f : ord_float(b.hi[0]);
+    float max_y = b.hi[1] == 0u ? -3.40282347e38f : ord_float(b.hi[1]);
+    const float pad = __fadd_rn(__fmul_rn(__fadd_rn(__fsub_rn(max_x, min_x), __fsub_rn(max_y, min_y)),
+                                          AABB_PADDING_RATIO),
+                                AABB_PADDING_MIN);
+    min_x = __fsub_rn(min_x, pad);
+    min_y = __fsub_rn(min_y, pad);
+    max_x = __fadd_rn(max_x, pad);
+    max_y = __fadd_rn(max_y, pad);
+    const float cx = __fmul_rn(__fadd_rn(min_x, max_x), 0.5f);
+    const float cy = __fmul_rn(__fadd_rn(min_y, max_y), 0.5f);
+    const float half = __fmul_rn(fmaxf(__fsub_rn(max_x, min_x), __fsub_rn(max_y, min_y)), 0.5f);
+    return make_float4(cx, cy, half, 0.0f);
+}
+
+// One level down (Aabb2::quadrant_of / quadrant_aabb, n_body.rs:74-91): quadrant bit 0 =
+// right (x >= center.x), bit 1 = bottom (y < center.y); the child's center moves by a
+// quarter of the parent's size.
+__device__ __forceinline__ uint32_t nb_descend(float2 p, float2 &c, float &half) {
+    const uint32_t q = (p.x >= c.x ? 1u : 0u) | (p.y < c.y ? 2u : 0u);
+    half = __fmul_rn(half, 0.5f);
+    c.x = (q & 1u) ? __fadd_rn(c.x, half) : __fsub_rn(c.x, half);
+    c.y = (q & 2u) ? __fsub_rn(c.y, half) : __fadd_rn(c.y, half);
+    return q;
+}
+
+// Step 2.  keys / vals are indexed by reference index: the radix sort is stable, so bodies of
+// equal path stay in insertion (index) order.
+__global__ void k_nb_keys(const float2 *x, const float *mass, const uint32_t *slot_to_index, int n,
+                          const NBodyBounds *b, int depth, float4 *root_out, uint32_t *keys,
+                          uint32_t *vals) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const float4 rt = nb_root(*b);
+    if (i == 0) root_out[0] = rt;
+    if (i >= n) return;
+    const uint32_t ref = slot_to_index[i];
+    if (ref >= static_cast<uint32_t>(n)) return;
+    uint32_t key = 1u << (2 * depth);  // no mass: behind every body
+    if (mass[i] > 0.0f) {
+        const float2 p = x[i];
+        float2 c = make_float2(rt.x, rt.y);
+        float half = rt.z;
+        key = 0u;
+        for (int d = 0; d < depth; ++d) key = (key << 2) | nb_descend(p, c, half);
+    }
+    keys[ref] = key;
+    vals[ref] = static_cast<uint32_t>(i);
+}
+
+// Step 3.  range must be zero before (an empty slot keeps [0, 0)).
+__global__ void k_nb_ranges(const uint32_t *keys, const uint32_t *vals, const float2 *x, const float *mass,
+                            const uint32_t *slot_to_index, int n, const NBodyBounds *b, int depth, float4 *body,
+                            uint2 *range) {
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    const int nb = static_cast<int>(b->n_bodies);
+    if (j >= nb || j >= n) return;
+    const uint32_t key = keys[j];
+    const uint32_t slot = vals[j];
+    if ((key >> (2 * depth)) != 0u || slot >= static_cast<uint32_t>(n)) return;  // not a body's key
+    const float2 p = x[slot];
+    body[j] = make_float4(p.x, p.y, mass[slot], __uint_as_float(slot_to_index[slot]));
+    const uint32_t prev = j > 0 ? keys[j - 1] : 0u, next = j + 1 < nb ? keys[j + 1] : 0u;
+    for (int d = 0; d <= depth; ++d) {
+        const int shift = 2 * (depth - d);
+        const uint32_t pd = key >> shift;
+        const int s = nbody_level_offset(d) + static_cast<int>(pd);
+        if (j == 0 || (prev >> shift) != pd) range[s].x = static_cast<uint32_t>(j);
+        if (j + 1 == nb || (next >> shift) != pd) range[s].y = static_cast<uint32_t>(j + 1);
+    }
+}
+
+// Step 4.  com.w = 1 marks a folded node (an empty one included: it is never far).
+__global__ void k_nb_centers(const uint2 *range, const float4 *body, const float4 *root, const NBodyBounds *b,
+                             int depth, float theta_max, float4 *com) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= nbody_slots(depth)) return;
+    int d = 0;
+    while (s >= nbody_level_offset(d + 1)) ++d;
+    const uint32_t pre = static_cast<uint32_t>(s - nbody_level_offset(d));
+    const uint2 rg = range[s];
+    if (rg.y <= rg.x) {
+        com[s] = make_float4(0.0f, 0.0f, 0.0f, 1.0f);
+        return;
+    }
+    // the node's box, as the traversal computes it
+    const float4 rt = root[0];
+    float2 c = make_float2(rt.x, rt.y);
+    float half = rt.z;
+    for (int l = 0; l < d; ++l) {
+        const uint32_t q = (pre >> (2 * (d - 1 - l))) & 3u;
+        half = __fmul_rn(half, 0.5f);
+        c.x = (q & 1u) ? __fadd_rn(c.x, half) : __fsub_rn(c.x, half);
+        c.y = (q & 2u) ? __fsub_rn(c.y, half) : __fadd_rn(c.y, half);
+    }
+    // far for some particle only if the farthest particle is beyond width / theta (with a
+    // relative margin far above the rounding of the traversal's distance and quotient)
+    if (b->all_lo[0] != 0xffffffffu && b->all_lo[1] != 0xffffffffu) {
+        const double ax = ord_float(b->all_lo[0]), bx = ord_float(b->all_hi[0]);
+        const double ay = ord_float(b->all_lo[1]), by = ord_float(b->all_hi[1]);
+        const double dx = fmax(fabs(ax - c.x), fabs(bx - c.x)), dy = fmax(fabs(ay - c.y), fabs(by - c.y));
+        const double dmax = sqrt(dx * dx + dy * dy);
+        if (dmax * static_cast<double>(theta_max) <= 2.0 * static_cast<double>(half) * (1.0 - 1e-4)) {
+            com[s] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+            return;
+        }
+    }
+    float tm = 0.0f, cx = 0.0f, cy = 0.0f;
+    for (uint32_t j = rg.x; j < rg.y; ++j) {
+        const float4 q = body[j];
+        const float nt = __fadd_rn(tm, q.z);
+        if (nt > 0.0f) {
+            cx = __fdiv_rn(__fadd_rn(__fmul_rn(cx, tm), __fmul_rn(q.x, q.z)), nt);
+            cy = __fdiv_rn(__fadd_rn(__fmul_rn(cy, tm), __fmul_rn(q.y, q.z)), nt);
+            tm = nt;
+        }
+    }
+    com[s] = make_float4(cx, cy, tm, 1.0f);
+}
+
+}  // namespace
+
+int launch_nbody_build(const NBodyTreeHost &t, const DevParticles &P, int n, SortScratch &sort,
+                       cudaStream_t stream) {
+    const int slots = nbody_slots(t.depth);
+    const int gb = (n + NB_THREADS - 1) / NB_THREADS;
+    k_nb_reset<<<1, 32, 0, stream>>>(t.bounds);
+    int kernels = 1;
+    if (n > 0) {
+        k_nb_bounds<<<gb, NB_THREADS, 0, stream>>>(P.x, P.mass, n, t.bounds);
+        kernels += 1;
+    }
+    k_nb_keys<<<gb > 0 ? gb : 1, NB_THREADS, 0, stream>>>(P.x, P.mass, P.slot_to_index, n, t.bounds, t.depth,
+                                                          t.root, sort.keys[0], sort.vals[0]);
+    kernels += 1;
+    int r = 0;
+    if (n > 1) {
+        const int bits = 2 * t.depth + 1;
+        r = radix_sort_pairs(sort, n, bits, stream);
+        kernels += 5 * ((bits + 7) / 8);
+    }
+    cudaMemsetAsync(t.range, 0, static_cast<size_t>(slots) * sizeof(uint2), stream);
+    if (n > 0) {
+        k_nb_ranges<<<gb, NB_THREADS, 0, stream>>>(sort.keys[r], sort.vals[r], P.x, P.mass, P.slot_to_index, n,
+                                                   t.bounds, t.depth, t.body, t.range);
+        kernels += 1;
+    }
+    k_nb_centers<<<(slots + NB_THREADS - 1) / NB_THREADS, NB_THREADS, 0, stream>>>(t.range, t.body, t.root,
+                                                                                    t.bounds, t.depth,
+                                                                                    t.theta_max, t.com);
+    return kernels + 1;
+}
+
+}  // namespace emerge

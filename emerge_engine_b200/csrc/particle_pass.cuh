@@ -751,6 +751,10 @@ struct ParticleKernelArgs {
     int aggregate;      // warp-aggregated P2G reductions (2: in warps whose lanes share a target)
     int project_in;     // recompute the projection of substep k before G2P (fused pipeline)
     int emit_p2g;       // project for substep k+1 and scatter its P2G (fused pipeline)
+    int split;          // 0: one pass; 1: G2P half (no fields, sleep scoring, CFL or P2G);
+                        // 2: fields half (fields, sleep scoring, CFL, projection, P2G of the
+                        // state the G2P half stored) -- the passes NBodyGravityField's tree
+                        // build runs between
     ClosureArgs cl;     // learned closure (kernels instantiated with CLOSURE only)
     BatchView batch;    // batched scenes (kernels instantiated with BATCH only)
 };
@@ -1134,6 +1138,7 @@ __device__ __forceinline__ void particle_pass(const ParticleKernelArgs &a, int b
             else
                 update_particle<MASK>(*mp, p, dt, pr);
         }
+        if (a.split == 2) o = save_fields(p);
     }
     bool deferred = false;  // CLOSURE == 2: queued for the tile kernel
     if constexpr (CLOSURE == 1) {
@@ -1155,15 +1160,15 @@ __device__ __forceinline__ void particle_pass(const ParticleKernelArgs &a, int b
     bool asleep = false;  // sleep scoring at the end of this substep (step.rs:299-315)
     if (valid) {
         if constexpr (HAS_MODEL(MASK, M_EXTRAS_BIT)) {
-            if (a.mode_g2p) {
-                apply_force_fields(cfg, p, dt);
+            if (a.split == 0 ? a.mode_g2p != 0 : a.split == 2) {
+                apply_force_fields(cfg, p, dt, cfg.nbody.body ? a.P.slot_to_index[i] : 0xFFFFFFFFu);
                 if (cfg.sleep_thr > 0.0f && (zb & ZB_FLAG) == 0u) {
                     const float act = a.lf.activation ? p.activation : a.P.activation[i];
                     asleep = act == 0.0f && vlen2(p.v) < cfg.sleep_thr * cfg.sleep_thr;
                 }
             }
         }
-        if (a.mode_g2p) store_fields(a.P, i, o, p);
+        if (a.mode_g2p || a.split == 2) store_fields(a.P, i, o, p);
         if constexpr (HAS_MODEL(MASK, M_EXTRAS_BIT)) {
             if (asleep) {
                 a.P.sleeping[i] = ZB_FLAG | ZB_OUT;
@@ -1173,7 +1178,7 @@ __device__ __forceinline__ void particle_pass(const ParticleKernelArgs &a, int b
             }
         }
     }
-    if (valid && !asleep) {
+    if (valid && !asleep && a.split != 1) {
         const MatP &m = *mp;
         // CFL contribution for the next substep (step.rs:447-466); a queued particle's
         // material bound depends on its update, which the tile kernel finishes
@@ -1218,7 +1223,7 @@ __device__ __forceinline__ void particle_pass(const ParticleKernelArgs &a, int b
     // block's last warp to arrive publishes the block's result (one global atomic each).
     max_speed = warp_max(max_speed);
     min_mdt = warp_min(min_mdt);
-    if ((threadIdx.x & 31) == 0) {
+    if ((threadIdx.x & 31) == 0 && a.split != 1) {
         atomicMax(&s_max_speed, __float_as_uint(max_speed));  // non-negative: ordered as uint
         atomicMin(&s_min_mdt, __float_as_uint(min_mdt));      // positive or +inf
         __threadfence_block();

@@ -962,6 +962,28 @@ EM_HD void init_particle(const MatP &m, emerge_particle &p) {
 }
 
 // ---------------------------------------------------------------- solver pieces
+// NBodyGravityField's Barnes-Hut quadtree (forces/fields/n_body.rs:63-283), rebuilt on the
+// device every substep (nbody.cu).  The tree is stored as the complete quadtree of `depth`
+// levels: the node of level d whose quadrant path from the root is `pre` (2 bits per level,
+// quadrant 0 first) is slot (4^d - 1) / 3 + pre.  A node exists when its parent holds more
+// than max_bodies bodies; it is a leaf when it holds at most max_bodies or sits at level
+// `depth` -- the tree the reference's one-at-a-time insertion builds, which does not depend
+// on the insertion order.  The bodies of a slot are a contiguous run of `body`, in reference
+// index order (the insertion order).
+constexpr int NBODY_MAX_DEPTH = 10;
+struct NBodyView {
+    int depth;             // max_depth (0..NBODY_MAX_DEPTH)
+    int max_bodies;        // max_bodies_per_node
+    const float4 *root;    // {center.x, center.y, half size, 0} of the root box
+    const float4 *body;    // bodies in tree order: x, y, mass, reference index (as bits)
+    const uint2 *range;    // per slot: [first, end) into body
+    const float4 *com;     // per slot: center of mass x, y, total mass; w = 1 if computed
+    uint32_t *error;       // StepState::error_flags (a far node without its center of mass)
+};
+
+__host__ __device__ __forceinline__ int nbody_level_offset(int d) { return ((1 << (2 * d)) - 1) / 3; }
+__host__ __device__ __forceinline__ int nbody_slots(int depth) { return nbody_level_offset(depth + 1); }
+
 struct DevConfig {
     int res;                 // grid_res
     float cell;              // grid_cell_size
@@ -1001,6 +1023,7 @@ struct DevConfig {
     int mf_fields;           // fields in use: bit 0 grip (contact), bit 1 solid + fluid (mixture)
     int mf_excl;             // fast pipeline, one kind of field: a field particle scatters into
                              // its field only, and the grid update adds the fields to the total
+    NBodyView nbody;         // NBodyGravityField's tree (body == nullptr: no such field)
 };
 
 // Bits of DevParticles::sleeping while the sleep partition is in use: bit 0 is
@@ -1110,12 +1133,108 @@ EM_HD float2 field_acceleration(const emerge_force_field &f, const float *data, 
     }
 }
 
+// Plummer-softened pull of mass m at offset r (n_body.rs:180-189, 199-207): zero when the
+// scale is not finite.
+EM_HD float2 nbody_pull(float2 r, float m, float g, float eps2) {
+    const float ns = vdot(r, r) + eps2;
+    const float scale = ediv(g * m, ns * esqrt(ns));
+    return isfinite(scale) ? vmuls(r, scale) : v2(0.0f, 0.0f);
+}
+
+// NBodyGravityField::acceleration (n_body.rs:178-208, 347-360) of the particle with reference
+// index `self` at `pos`: the reference's recursion walked depth first with an explicit
+// stack, each node's children summed into their own accumulator in quadrant order so that
+// every addition is the reference's.  A node is far when the particle is at least the
+// softening length from its box center, it holds mass, and its width over that distance is
+// below theta; far nodes pull with their center of mass, leaves with each body but the
+// particle itself and those closer than the softening length.
+__device__ __forceinline__ float2 nbody_acceleration(const NBodyView &nb, const emerge_force_field &f, float2 pos,
+                                                     uint32_t self) {
+    const float g = f.params[0], soft = f.params[1], theta = f.params[2];
+    const float eps2 = soft * soft;
+    if (!nb.body) return v2(0.0f, 0.0f);
+    const float4 rt = nb.root[0];
+    float2 ctr[NBODY_MAX_DEPTH + 1];
+    float2 acc[NBODY_MAX_DEPTH + 1];
+    int d = 0;
+    uint32_t pre = 0u;
+    float2 c = v2(rt.x, rt.y);
+    float half = rt.z;
+    for (;;) {
+        // first visit of node (d, pre): box center c, half size `half`
+        const int slot = nbody_level_offset(d) + static_cast<int>(pre);
+        const uint2 rg = nb.range[slot];
+        float2 r;
+        const float dist = evlen(vsub(pos, c));
+        bool far = false;
+        if (!(dist < soft) && rg.y > rg.x) far = ediv(half * 2.0f, dist) < theta;
+        if (far) {
+            const float4 cm = nb.com[slot];
+            if (cm.w == 0.0f) atomicOr(nb.error, 4u);  // ERR_NBODY_SKIPPED (device_state.cuh)
+            r = nbody_pull(vsub(v2(cm.x, cm.y), pos), cm.z, g, eps2);
+        } else if (d >= nb.depth || rg.y - rg.x <= static_cast<uint32_t>(nb.max_bodies)) {
+            r = v2(0.0f, 0.0f);
+            for (uint32_t j = rg.x; j < rg.y; ++j) {
+                const float4 b = nb.body[j];
+                if (__float_as_uint(b.w) == self) continue;
+                const float2 rv = vsub(v2(b.x, b.y), pos);
+                if (vdot(rv, rv) < eps2) continue;
+                r = vadd(r, nbody_pull(rv, b.z, g, eps2));
+            }
+        } else {  // internal: descend into quadrant 0 (left, top)
+            ctr[d] = c;
+            acc[d] = v2(0.0f, 0.0f);
+            half *= 0.5f;
+            c = v2(c.x - half, c.y + half);
+            ++d;
+            pre <<= 2;
+            continue;
+        }
+        // return r to the parent; move to the next sibling, or finish the parent
+        for (;;) {
+            if (d == 0) return r;
+            const uint32_t q = pre & 3u;
+            pre >>= 2;
+            --d;
+            acc[d] = vadd(acc[d], r);
+            if (q < 3u) {
+                const uint32_t nq = q + 1u;
+                const float quarter = half;  // the children's half size
+                c = v2((nq & 1u) ? ctr[d].x + quarter : ctr[d].x - quarter,
+                       (nq & 2u) ? ctr[d].y - quarter : ctr[d].y + quarter);
+                ++d;
+                pre = (pre << 2) | nq;
+                break;
+            }
+            r = acc[d];
+            half *= 2.0f;
+        }
+    }
+}
+
+// Sum of the force fields' accelerations at a particle, in application order (step.rs:
+// 232-236).  `self`: the particle's reference index (NBodyGravityField skips the particle's
+// own body).
+EM_HD float2 force_field_sum(const DevConfig &cfg, const PState &p, uint32_t self) {
+    float2 dv = v2(0.0f, 0.0f);
+    for (int k = 0; k < cfg.n_fields; ++k) {
+        const emerge_force_field &f = cfg.fields[k];
+#ifdef __CUDA_ARCH__
+        if (f.kind == EMERGE_FIELD_NBODY_GRAVITY) {
+            dv = vadd(dv, nbody_acceleration(cfg.nbody, f, p.x, self));
+            continue;
+        }
+#endif
+        dv = vadd(dv, field_acceleration(f, cfg.field_data, p));
+    }
+    return dv;
+}
+
 // Force fields after G2P (step.rs:212-259): v += dt * sum of the accelerations, then the
 // G2P speed clamp again; pinned particles are skipped.
-EM_HD void apply_force_fields(const DevConfig &cfg, PState &p, float dt) {
+EM_HD void apply_force_fields(const DevConfig &cfg, PState &p, float dt, uint32_t self = 0xFFFFFFFFu) {
     if (cfg.n_fields <= 0 || p.pinned != 0) return;
-    float2 dv = v2(0.0f, 0.0f);
-    for (int k = 0; k < cfg.n_fields; ++k) dv = vadd(dv, field_acceleration(cfg.fields[k], cfg.field_data, p));
+    const float2 dv = force_field_sum(cfg, p, self);
     p.v = vadd(p.v, svmul(dt, dv));
     const float vel_limit = cfg.cell / dt;
     const float spd = vlen(p.v);

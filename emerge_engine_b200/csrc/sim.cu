@@ -147,6 +147,10 @@ struct emerge_sim {
     std::vector<uint64_t> bounds;
     int n_fields = 0;
     Buffer fbuf;  // force field table, then its data
+    NBodyTreeHost nb;        // NBodyGravityField's tree (nb.depth < 0: none)
+    Buffer nbbuf;            // its arrays, sized for nb_cap particles and nb_alloc_depth
+    size_t nb_cap = 0;
+    int nb_alloc_depth = -1;
 
     // sleep partition (solver/mod.rs:40-42): reference indices [0, active) are awake
     uint64_t active = 0;
@@ -345,6 +349,16 @@ void refresh_dev_config(emerge_sim *s) {
     // the total.  With both kinds a particle may sit in two fields and scatters into the total
     // as well.
     s->dcfg.mf_excl = (s->dcfg.mf_fast && (s->dcfg.mf_fields == 1 || s->dcfg.mf_fields == 2)) ? 1 : 0;
+    s->dcfg.nbody = NBodyView{};
+    if (s->nb.depth >= 0 && s->nbbuf.ptr) {
+        s->dcfg.nbody.depth = s->nb.depth;
+        s->dcfg.nbody.max_bodies = s->nb.max_bodies;
+        s->dcfg.nbody.root = s->nb.root;
+        s->dcfg.nbody.body = s->nb.body;
+        s->dcfg.nbody.range = s->nb.range;
+        s->dcfg.nbody.com = s->nb.com;
+        s->dcfg.nbody.error = &s->d_state->error_flags;
+    }
     s->dcfg.n_fields = s->n_fields;
     s->dcfg.fields = s->n_fields ? static_cast<const emerge_force_field *>(s->fbuf.ptr) : nullptr;
     s->dcfg.field_data = s->n_fields ? reinterpret_cast<const float *>(
@@ -480,6 +494,55 @@ void enqueue_multi_resolves(const StepLaunch &L) {
     if (L.cfg.mf_fields & 2) launch_mixture_resolve(L);
 }
 
+bool nbody_live(const emerge_sim *s) { return s->nb.depth >= 0 && s->nbbuf.ptr != nullptr; }
+
+// Kernels a substep's particle pass takes beyond the one pass: with an NBodyGravityField, the
+// tree build and the fields half.
+int nbody_extra_kernels(const emerge_sim *s) {
+    return nbody_live(s) ? nbody_build_kernels(s->nb.depth, static_cast<int>(s->n)) + 1 : 0;
+}
+
+// The particle pass of a substep (G2P of substep k, fields, CFL bound, and with emit_p2g the
+// projection and P2G of k + 1).  With an NBodyGravityField the fields need the tree of every
+// particle's post-G2P position (step.rs:221-226): the pass runs as its G2P half, the tree
+// build, and its fields half.
+void launch_particle_pass_fields(emerge_sim *s, const StepLaunch &L, int project_in, int emit_p2g) {
+    if (!nbody_live(s)) {
+        launch_particle_pass(L, s->lf, 1, project_in, emit_p2g);
+        return;
+    }
+    launch_particle_pass(L, s->lf, 1, project_in, 0, 1);
+    launch_nbody_build(s->nb, L.P, L.n, s->sort, L.stream);
+    launch_particle_pass(L, s->lf, 0, 0, emit_p2g, 2);
+}
+
+// The tree's arrays for the current capacity and depth (allocated before a step).
+emerge_status nbody_prepare(emerge_sim *s) {
+    if (s->nb.depth < 0) return EMERGE_OK;
+    if (s->nbbuf.ptr && s->nb_cap >= s->cap && s->nb_alloc_depth == s->nb.depth) return EMERGE_OK;
+    CK(cudaStreamSynchronize(s->stream));  // queued kernels may still read the old arrays
+    s->nbbuf.reset();
+    const size_t cap = std::max<size_t>(s->cap, 1);
+    const size_t slots = static_cast<size_t>(nbody_slots(s->nb.depth));
+    const size_t b_bounds = align_up(sizeof(NBodyBounds), 256), b_root = 256;
+    const size_t b_body = align_up(cap * sizeof(float4), 256), b_range = align_up(slots * sizeof(uint2), 256);
+    const size_t b_com = align_up(slots * sizeof(float4), 256);
+    const size_t bytes = b_bounds + b_root + b_body + b_range + b_com;
+    CK(cudaMalloc(&s->nbbuf.ptr, bytes));
+    s->nbbuf.bytes = bytes;
+    char *p = static_cast<char *>(s->nbbuf.ptr);
+    s->nb.bounds = reinterpret_cast<NBodyBounds *>(p);
+    s->nb.root = reinterpret_cast<float4 *>(p + b_bounds);
+    s->nb.body = reinterpret_cast<float4 *>(p + b_bounds + b_root);
+    s->nb.range = reinterpret_cast<uint2 *>(p + b_bounds + b_root + b_body);
+    s->nb.com = reinterpret_cast<float4 *>(p + b_bounds + b_root + b_body + b_range);
+    s->nb_cap = cap;
+    s->nb_alloc_depth = s->nb.depth;
+    refresh_dev_config(s);
+    s->graph_dirty = true;
+    return EMERGE_OK;
+}
+
 emerge_status build_graph(emerge_sim *s) {
     destroy_graph(s);
     StepLaunch L = make_launch(s);
@@ -505,14 +568,15 @@ emerge_status build_graph(emerge_sim *s) {
     cudaGraphNode_t wnode;
     CK(cudaGraphAddNode(&wnode, graph, nodes.data(), nn, &cp));
     cudaGraph_t body = cp.conditional.phGraph_out[0];
-    const int kps = 3 + (L.density_mode ? 1 : 0) + multi_fast_launches(L.cfg) + (closure_tiles_on(L) ? 1 : 0);
+    const int kps = 3 + (L.density_mode ? 1 : 0) + multi_fast_launches(L.cfg) + (closure_tiles_on(L) ? 1 : 0) +
+                    nbody_extra_kernels(s);
     CK(cudaStreamBeginCaptureToGraph(s->stream, body, nullptr, nullptr, 0,
                                      cudaStreamCaptureModeThreadLocal));
     launch_substep_begin(L, 1, static_cast<unsigned long long>(handle), kps);
     if (L.cfg.mf_fast) launch_multi_clear(L);
     launch_grid_update(L);
     enqueue_multi_resolves(L);
-    launch_particle_pass(L, s->lf, 1, L.cfg.project, 1);
+    launch_particle_pass_fields(s, L, L.cfg.project, 1);
     if (closure_tiles_on(L)) launch_closure_tiles(L, s->lf, s->sm_count);
     if (L.density_mode) launch_density_pass(L, s->lf);
     CK(cudaStreamEndCapture(s->stream, &body));
@@ -599,7 +663,8 @@ emerge_status run_host_loop_step(emerge_sim *s, bool timed) {
         launch_grid_update(L);
         enqueue_multi_resolves(L);
         CK(cudaEventRecord(s->ev[3], s->stream));
-        launch_particle_pass(L, s->lf, 1, L.cfg.project, 1);
+        launch_particle_pass_fields(s, L, L.cfg.project, 1);
+        s->host_launches += nbody_extra_kernels(s);
         if (closure_tiles_on(L)) {
             launch_closure_tiles(L, s->lf, s->sm_count);
             s->host_launches += 1;
@@ -909,9 +974,9 @@ emerge_status run_det_step(emerge_sim *s, bool timed) {
             s->host_launches += mixture_launches(L.cfg);
         }
         CK(cudaEventRecord(s->ev[6], s->stream));
-        launch_particle_pass(L, s->lf, 1, 0, 0);
+        launch_particle_pass_fields(s, L, 0, 0);
         CK(cudaEventRecord(s->ev[7], s->stream));
-        s->host_launches += 2;
+        s->host_launches += 2 + nbody_extra_kernels(s);
         CK(cudaMemcpyAsync(s->h_state, s->d_state, sizeof(StepState), cudaMemcpyDeviceToHost,
                            s->stream));
         CK(cudaStreamSynchronize(s->stream));
@@ -1383,6 +1448,23 @@ emerge_status emerge_cuda_set_force_fields(emerge_sim *s, const emerge_force_fie
         case EMERGE_FIELD_LINEAR_DRAG:
         case EMERGE_FIELD_RADIAL_CONFINEMENT:
         case EMERGE_FIELD_AABB_CONFINEMENT: break;
+        case EMERGE_FIELD_NBODY_GRAVITY: {
+            // NBodyGravityField::new asserts theta in (0, 1] (n_body.rs:306-311)
+            const float theta = f.params[2], depth = f.params[3], maxb = f.params[4];
+            if (!(theta > 0.0f && theta <= 1.0f))
+                return static_cast<emerge_status>(
+                    s->fail(EMERGE_ERR_INVALID_ARG, "force field " + std::to_string(k) + ": theta must be in (0, 1]"));
+            if (!(maxb >= 0.0f && maxb <= 2147483647.0f && maxb == std::floor(maxb)) || !(depth >= 0.0f) ||
+                depth != std::floor(depth))
+                return static_cast<emerge_status>(s->fail(
+                    EMERGE_ERR_INVALID_ARG,
+                    "force field " + std::to_string(k) + ": max_depth and max_bodies_per_node must be non-negative integers"));
+            if (depth > static_cast<float>(NBODY_MAX_DEPTH))
+                return static_cast<emerge_status>(
+                    s->fail(EMERGE_ERR_UNSUPPORTED, "force field " + std::to_string(k) + ": max_depth above " +
+                                                        std::to_string(NBODY_MAX_DEPTH)));
+            break;
+        }
         default:
             return static_cast<emerge_status>(
                 s->fail(EMERGE_ERR_UNSUPPORTED, "force field " + std::to_string(k) + ": unknown kind"));
@@ -1391,7 +1473,30 @@ emerge_status emerge_cuda_set_force_fields(emerge_sim *s, const emerge_force_fie
             return static_cast<emerge_status>(
                 s->fail(EMERGE_ERR_INVALID_ARG, "force field " + std::to_string(k) + ": data out of range"));
     }
+    // NBody fields share one tree: the same max_depth and max_bodies_per_node
+    NBodyTreeHost tree;
+    for (uint32_t k = 0; k < n; ++k) {
+        const emerge_force_field &f = fields[k];
+        if (f.kind != EMERGE_FIELD_NBODY_GRAVITY) continue;
+        const int depth = static_cast<int>(f.params[3]), maxb = static_cast<int>(f.params[4]);
+        if (tree.depth >= 0 && (tree.depth != depth || tree.max_bodies != maxb))
+            return static_cast<emerge_status>(s->fail(
+                EMERGE_ERR_UNSUPPORTED, "n-body fields with different max_depth or max_bodies_per_node"));
+        tree.depth = depth;
+        tree.max_bodies = maxb;
+        tree.theta_max = std::max(tree.theta_max, f.params[2]);
+    }
     if (s->stream) CK(cudaStreamSynchronize(s->stream));  // kernels in flight may read the old table
+    if (tree.depth < 0) {
+        s->nbbuf.reset();
+        s->nb = NBodyTreeHost{};
+        s->nb_cap = 0;
+        s->nb_alloc_depth = -1;
+    } else {
+        s->nb.depth = tree.depth;
+        s->nb.max_bodies = tree.max_bodies;
+        s->nb.theta_max = tree.theta_max;
+    }
     s->fbuf.reset();
     s->n_fields = 0;
     if (n > 0) {
@@ -1408,6 +1513,27 @@ emerge_status emerge_cuda_set_force_fields(emerge_sim *s, const emerge_force_fie
     refresh_dev_config(s);
     s->graph_dirty = true;
     return EMERGE_OK;
+}
+
+static emerge_status sync_state(emerge_sim *s);
+
+emerge_status emerge_cuda_field_accelerations(emerge_sim *s, float *out, uint64_t n) {
+    if (!s || (!out && n)) return EMERGE_ERR_INVALID_ARG;
+    if (n != s->n)
+        return static_cast<emerge_status>(s->fail(EMERGE_ERR_INVALID_ARG, "n must equal the particle count"));
+    if (n == 0) return EMERGE_OK;
+    emerge_status st = nbody_prepare(s);
+    if (st != EMERGE_OK) return st;
+    StepLaunch L = make_launch(s);
+    if (nbody_live(s)) launch_nbody_build(s->nb, L.P, L.n, s->sort, s->stream);
+    float2 *d_out = nullptr;
+    CK(cudaMalloc(&d_out, n * sizeof(float2)));
+    launch_field_accelerations(L, s->lf, d_out);
+    cudaError_t e = cudaMemcpyAsync(out, d_out, n * sizeof(float2), cudaMemcpyDeviceToHost, s->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
+    cudaFree(d_out);
+    CK(e);
+    return sync_state(s);
 }
 
 emerge_status emerge_cuda_set_contact_grip(emerge_sim *s, int enabled, float mu_easy, float mu_resist,
@@ -1626,6 +1752,10 @@ emerge_status emerge_cuda_step(emerge_sim *s, uint32_t n_steps, emerge_step_timi
             if (st != EMERGE_OK) return st;
         }
     }
+    {
+        emerge_status st = nbody_prepare(s);
+        if (st != EMERGE_OK) return st;
+    }
     for (uint32_t k = 0; k < n_steps; ++k) {
         emerge_status st = maybe_sort(s);
         if (st != EMERGE_OK) return st;
@@ -1684,6 +1814,8 @@ static emerge_status sync_state(emerge_sim *s) {
                                                   "learned closure: a tensor-core wait gave up (tile kernel returned)"));
     if (s->h_state->error_flags & ERR_CONTACT_LIST)
         return static_cast<emerge_status>(s->fail(EMERGE_ERR_CUDA, "contact point list walk cut short"));
+    if (s->h_state->error_flags & ERR_NBODY_SKIPPED)
+        return static_cast<emerge_status>(s->fail(EMERGE_ERR_CUDA, "n-body field: a far node had no center of mass"));
     return EMERGE_OK;
 }
 

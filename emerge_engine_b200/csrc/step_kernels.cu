@@ -551,13 +551,33 @@ void launch_insert_index(const DevParticles &P, int n_old, int n_new, uint32_t o
     if (n_new > 0) k_insert_index<<<blocks_for(n_new, 256), 256, 0, stream>>>(P, n_old, n_new, old_active);
 }
 
+// Field::acceleration summed over the force fields for every particle at its current state,
+// written in reference index order (the dv of step.rs:232-236 before the dt factor).
+__global__ void k_field_accelerations(DevParticles P, int n, LoadFlags lf, DevConfig cfg, float2 *out) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const PState p = load_state(P, i, lf);
+    const uint32_t ref = P.slot_to_index[i];
+    if (ref < static_cast<uint32_t>(n)) out[ref] = force_field_sum(cfg, p, ref);
+}
+
 // ---------------------------------------------------------------- launchers
 
+void launch_field_accelerations(const StepLaunch &L, const LoadFlagsHost &lfh, float2 *out) {
+    if (L.n == 0) return;
+    LoadFlags lf;
+    lf.temperature = lfh.temperature;
+    lf.activation = lfh.activation;
+    lf.pinned = lfh.pinned;
+    k_field_accelerations<<<blocks_for(L.n, 256), 256, 0, L.stream>>>(L.P, L.n, lf, L.cfg, out);
+}
+
 void launch_particle_pass(const StepLaunch &L, const LoadFlagsHost &lfh, int mode_g2p,
-                          int project_in, int emit_p2g) {
+                          int project_in, int emit_p2g, int split) {
     if (L.n == 0) return;
     ParticleKernelArgs a;
     fill_common(a, L, lfh);
+    a.split = split;
     a.mode_g2p = mode_g2p;
     a.density_mode = L.density_mode;
     a.project_in = project_in;

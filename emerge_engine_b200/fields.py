@@ -6,8 +6,9 @@ charge table or potential to `data` and returns the table entry).  The fields ap
 G2P: v += sub_dt * (sum of the fields' accelerations), then the G2P speed clamp
 (spacetime/solver/step.rs:212-259).
 
-Not on the device: `NBodyGravityField` (a Barnes-Hut quadtree rebuilt per substep) and
-`SpatialDragField` (a host function pointer).
+`NBodyGravityField` is the particles' own gravity through a Barnes-Hut quadtree, rebuilt on
+the device every substep between the G2P half and the fields half of the particle pass.
+Not on the device: `SpatialDragField` (a host function pointer).
 """
 from __future__ import annotations
 
@@ -21,7 +22,8 @@ ALL_MATERIALS = 0xFFFFFFFF
 FADE_ONSET_RATIO = f32(0.85)  # forces/fields/mod.rs:10
 
 GRAVITY_WELL, BUOYANCY, LINEAR_DRAG, RADIAL_CONFINEMENT, AABB_CONFINEMENT = 1, 2, 3, 4, 5
-COULOMB, UNIFORM_ELECTRIC, CHEMOTAXIS = 6, 7, 8
+COULOMB, UNIFORM_ELECTRIC, CHEMOTAXIS, NBODY_GRAVITY = 6, 7, 8, 9
+NBODY_MAX_DEPTH = 10  # the device tree's limit (the reference takes any usize)
 
 
 def _entry(kind, params=(), **kw) -> ForceFieldC:
@@ -242,6 +244,73 @@ class ChemotaxisField(Field):
                    material_filter=ALL_MATERIALS if self.material_filter is None else self.material_filter)
         data += self.phi.tolist()
         return e
+
+
+class NBodyGravityField(Field):
+    """`NBodyGravityField` (forces/fields/n_body.rs:287-361): Plummer-softened gravity of every
+    particle of positive mass on every particle, a = G M r / (|r|^2 + eps^2)^(3/2), through a
+    Barnes-Hut quadtree rebuilt each substep from the post-G2P positions; a node whose width
+    over its distance is below theta pulls with its center of mass.  max_depth (default 8)
+    and max_bodies_per_node (default 4) shape the tree; the device takes max_depth up to 10,
+    and all NBody fields of one simulation share both."""
+
+    def __init__(self, gravitational_constant, softening, theta):
+        theta = f32(theta)
+        if not (theta > 0.0 and theta <= 1.0):  # NBodyGravityField::new's assertion
+            raise ValueError(f"theta must be in (0, 1]; got {float(theta)}. "
+                             "0.5 is a common Barnes-Hut trade-off value in practice.")
+        self.gravitational_constant = f32(gravitational_constant)
+        self.softening = f32(softening)
+        self.theta = theta
+        self.max_depth = 8
+        self.max_bodies_per_node = 4
+
+    @classmethod
+    def new(cls, gravitational_constant, softening, theta):
+        return cls(gravitational_constant, softening, theta)
+
+    def pack(self, data):
+        depth, maxb = int(self.max_depth), int(self.max_bodies_per_node)
+        if depth < 0 or maxb < 0:
+            raise ValueError("max_depth and max_bodies_per_node must be non-negative")
+        return _entry(NBODY_GRAVITY, (self.gravitational_constant, self.softening, self.theta,
+                                      depth, maxb))
+
+
+class orbit:
+    """Orbit helpers for bodies under NBodyGravityField (n_body.rs:366-429), f32 like the
+    reference; units are grid cells and cells/s, g the field's gravitational_constant."""
+    _EPS = float(np.finfo(np.float32).eps)
+
+    @staticmethod
+    def circular_velocity(g, central_mass, orbit_radius):
+        if f32(orbit_radius) <= orbit._EPS:
+            return f32(0.0)
+        return f32(np.sqrt(f32(g) * f32(central_mass) / f32(orbit_radius)))
+
+    @staticmethod
+    def circular_velocity_softened(g, central_mass, orbit_radius, softening):
+        r, e = f32(orbit_radius), f32(softening)
+        norm_s = r * r + e * e
+        if norm_s <= orbit._EPS:
+            return f32(0.0)
+        return f32(r * np.sqrt(f32(g) * f32(central_mass) / (norm_s * np.sqrt(norm_s))))
+
+    @staticmethod
+    def escape_velocity(g, central_mass, distance):
+        if f32(distance) <= orbit._EPS:
+            return f32(0.0)
+        return f32(np.sqrt(f32(2.0) * f32(g) * f32(central_mass) / f32(distance)))
+
+    @staticmethod
+    def elliptical_velocity(g, central_mass, distance, eccentricity, at_periapsis):
+        d = f32(distance)
+        if d <= orbit._EPS:
+            return f32(0.0)
+        mu = f32(g) * f32(central_mass)
+        sign = f32(1.0) if at_periapsis else f32(-1.0)
+        semimajor = d / (f32(1.0) - f32(eccentricity) * sign)
+        return f32(np.sqrt(max(mu * (f32(2.0) / d - f32(1.0) / semimajor), f32(0.0))))
 
 
 def pack_fields(fields) -> tuple:

@@ -237,6 +237,15 @@ class Simulation:
     def force_field_names(self) -> list:
         return [n for n, _ in self.force_fields]
 
+    def field_accelerations(self) -> np.ndarray:
+        """(n, 2) float32: the fields' summed Field::acceleration per particle, reference index
+        order, at the current state (the n-body tree built from the current positions)."""
+        n = self.particle_count()
+        out = np.zeros((max(n, 1), 2), dtype=np.float32)
+        self._check(self._lib.emerge_cuda_field_accelerations(
+            self._sim, out.ctypes.data_as(ctypes.POINTER(c_float)), n))
+        return out[:n]
+
     # ---------------------------------------------------------------- boundaries
     def _upload_boundaries(self) -> None:
         arr = (c_uint64 * max(len(self.boundaries), 1))(*[b.thickness for b in self.boundaries])

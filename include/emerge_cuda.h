@@ -232,8 +232,8 @@ emerge_status emerge_cuda_replace_particles(emerge_sim *sim, const emerge_partic
 /* Built-in force fields (forces/fields/): per particle v += sub_dt * sum of the
  * fields' accelerations after G2P, then the G2P speed clamp again (step.rs:212-259).
  * The reference's Field trait objects can hold arbitrary code; the device runs these
- * kinds, which cover every built-in field except NBodyGravityField (Barnes-Hut tree
- * rebuilt per substep) and SpatialDragField (a host function pointer). */
+ * kinds, which cover every built-in field except SpatialDragField (a host function
+ * pointer). */
 enum {
     EMERGE_FIELD_GRAVITY_WELL = 1,       /* gravity.rs: params {G, softening, cutoff, switch_on};
                                             data: count sources (x, y, mass) */
@@ -248,8 +248,17 @@ enum {
                                             material id */
     EMERGE_FIELD_UNIFORM_ELECTRIC = 7,   /* em.rs: {field.x, field.y}; data: n_charges charges by
                                             material id */
-    EMERGE_FIELD_CHEMOTAXIS = 8          /* chemotaxis.rs: {sensitivity}; material_filter; data:
+    EMERGE_FIELD_CHEMOTAXIS = 8,         /* chemotaxis.rs: {sensitivity}; material_filter; data:
                                             count x count potential phi[x * count + y] */
+    EMERGE_FIELD_NBODY_GRAVITY = 9       /* n_body.rs: {G, softening, theta, max_depth,
+                                            max_bodies_per_node}: the particles' own Plummer-softened
+                                            gravity through a Barnes-Hut quadtree over every
+                                            particle of positive mass, rebuilt on the device each
+                                            substep after G2P.  theta in (0, 1]; max_depth an
+                                            integer in 0..10 (the reference takes any usize);
+                                            max_bodies_per_node a non-negative integer.  All
+                                            NBody fields of a simulation share max_depth and
+                                            max_bodies_per_node (one tree) */
 };
 #define EMERGE_FIELD_ALL_MATERIALS 0xFFFFFFFFu
 
@@ -271,6 +280,11 @@ typedef struct emerge_force_field {
  * tables and potentials; n = 0 clears. */
 emerge_status emerge_cuda_set_force_fields(emerge_sim *sim, const emerge_force_field *fields,
                                            uint32_t n, const float *data, uint64_t n_data);
+/* Field::acceleration (forces/fields/force_field.rs) summed over the simulation's fields in
+ * application order, for every particle at its current state: out[2 i], out[2 i + 1] for
+ * reference index i (n = the particle count).  NBodyGravityField builds its tree from the
+ * current positions first, as prepare() does. */
+emerge_status emerge_cuda_field_accelerations(emerge_sim *sim, float *out, uint64_t n);
 
 /* ---- multi-field contact and two-phase mixture ---------------------------------- */
 

@@ -1921,15 +1921,167 @@ V2 field_acceleration(const oracle_force_field &f, const float *data, const P &q
     }
 }
 
-// Force fields (step.rs:212-259): v += dt * sum of accelerations, then the speed clamp.
+// ---- NBodyGravityField (forces/fields/n_body.rs): Barnes-Hut quadtree ----
+// A pointer-free restatement of the reference's Node / Quadtree: nodes in one vector,
+// children as four consecutive entries, built by inserting the bodies one at a time in
+// index order (n_body.rs:143-175, 210-256) so that every node's MassProps accumulates in
+// the reference's order.
+struct NbNode {
+    V2 center;
+    float half;               // Aabb2 half size (square: both components equal)
+    size_t depth;
+    float mass = 0.0f;        // MassProps (n_body.rs:94-107)
+    V2 com = {0.0f, 0.0f};
+    std::vector<uint32_t> bodies;  // positions in the snapshot
+    int64_t child = -1;       // first of the four children, -1 = none
+};
+
+struct NbTree {
+    std::vector<NbNode> nodes;
+    std::vector<V2> pos;          // snapshot: particles of positive mass, index order
+    std::vector<float> mass;
+    std::vector<uint32_t> index;  // their particle indices
+    size_t max_depth = 8;
+    size_t max_bodies = 4;
+};
+
+// MassProps::add (n_body.rs:96-107)
+void nb_mass_add(NbNode &n, V2 p, float m) {
+    const float nt = n.mass + m;
+    if (nt > 0.0f) {
+        n.com = divs(add(muls(n.com, n.mass), muls(p, m)), nt);
+        n.mass = nt;
+    }
+}
+
+// Aabb2::quadrant_of (n_body.rs:74-78): bit 0 right, bit 1 bottom.
+size_t nb_quadrant(const NbNode &n, V2 p) {
+    return static_cast<size_t>(p.x >= n.center.x) | (static_cast<size_t>(p.y < n.center.y) << 1);
+}
+
+// Node::insert (n_body.rs:143-175)
+void nb_insert(NbTree &t, size_t node, uint32_t b) {
+    nb_mass_add(t.nodes[node], t.pos[b], t.mass[b]);
+    {
+        NbNode &n = t.nodes[node];
+        if (n.depth >= t.max_depth || (n.bodies.size() < t.max_bodies && n.child < 0)) {
+            n.bodies.push_back(b);
+            return;
+        }
+    }
+    if (t.nodes[node].child < 0) {
+        // quadrant_aabb (n_body.rs:80-91): the children's centers a quarter of the size away
+        const V2 c = t.nodes[node].center;
+        const float quarter = t.nodes[node].half * 0.5f;
+        const size_t depth = t.nodes[node].depth + 1;
+        const size_t first = t.nodes.size();
+        for (size_t q = 0; q < 4; ++q) {
+            NbNode ch;
+            const float xs = (q & 1) == 0 ? -1.0f : 1.0f, ys = (q & 2) == 0 ? 1.0f : -1.0f;
+            ch.center = add(c, v2(xs * quarter, ys * quarter));
+            ch.half = quarter;
+            ch.depth = depth;
+            t.nodes.push_back(std::move(ch));
+        }
+        t.nodes[node].child = static_cast<int64_t>(first);
+        std::vector<uint32_t> existing;
+        existing.swap(t.nodes[node].bodies);
+        for (uint32_t e : existing) nb_insert(t, first + nb_quadrant(t.nodes[node], t.pos[e]), e);
+    }
+    nb_insert(t, static_cast<size_t>(t.nodes[node].child) + nb_quadrant(t.nodes[node], t.pos[b]), b);
+}
+
+// NBodyGravityField::prepare + Quadtree::build (n_body.rs:210-256, 332-345): every particle of
+// positive mass, the root box their bounding box padded and squared.
+void nb_build(NbTree &t, const std::vector<P> &ps, size_t max_depth, size_t max_bodies) {
+    t = NbTree{};
+    t.max_depth = max_depth;
+    t.max_bodies = max_bodies;
+    for (size_t i = 0; i < ps.size(); ++i) {
+        if (!(ps[i].mass > 0.0f)) continue;
+        t.pos.push_back(load_v(ps[i].x));
+        t.mass.push_back(ps[i].mass);
+        t.index.push_back(static_cast<uint32_t>(i));
+    }
+    NbNode root;
+    root.depth = 0;
+    if (t.pos.empty()) {
+        root.center = v2(0.0f, 0.0f);
+        root.half = 1000.0f;  // EMPTY_TREE_HALF_SIZE
+        t.nodes.push_back(std::move(root));
+        return;
+    }
+    float min_x = std::numeric_limits<float>::max(), min_y = min_x;
+    float max_x = std::numeric_limits<float>::lowest(), max_y = max_x;
+    for (V2 p : t.pos) {
+        min_x = fmin_(min_x, p.x);
+        min_y = fmin_(min_y, p.y);
+        max_x = fmax_(max_x, p.x);
+        max_y = fmax_(max_y, p.y);
+    }
+    const float pad = ((max_x - min_x) + (max_y - min_y)) * 0.1f + 1.0f;  // AABB_PADDING_RATIO, _MIN
+    min_x -= pad;
+    min_y -= pad;
+    max_x += pad;
+    max_y += pad;
+    root.center = v2((min_x + max_x) * 0.5f, (min_y + max_y) * 0.5f);
+    root.half = fmax_(max_x - min_x, max_y - min_y) * 0.5f;
+    t.nodes.push_back(std::move(root));
+    for (uint32_t b = 0; b < t.pos.size(); ++b) nb_insert(t, 0, b);
+}
+
+// Plummer pull (n_body.rs:180-189, 199-207): zero when the scale is not finite.
+V2 nb_pull(V2 r, float m, float g, float eps2) {
+    const float ns = length_sq(r) + eps2;
+    const float scale = g * m / (ns * std::sqrt(ns));
+    return std::isfinite(scale) ? muls(r, scale) : v2(0.0f, 0.0f);
+}
+
+// Node::acceleration_on (n_body.rs:177-214) with is_far_enough (n_body.rs:131-141).
+V2 nb_accel(const NbTree &t, size_t node, size_t self, V2 pos, float g, float soft, float theta) {
+    const NbNode &n = t.nodes[node];
+    const float eps2 = soft * soft;
+    const float dist = length(sub(pos, n.center));
+    const bool far = !(dist < soft || n.mass <= 0.0f) && (n.half * 2.0f) / dist < theta;
+    if (far) return nb_pull(sub(n.com, pos), n.mass, g, eps2);
+    if (n.child < 0) {
+        V2 total = v2(0.0f, 0.0f);
+        for (uint32_t b : n.bodies) {
+            if (t.index[b] == self) continue;
+            const V2 r = sub(t.pos[b], pos);
+            if (length_sq(r) < eps2) continue;
+            total = add(total, nb_pull(r, t.mass[b], g, eps2));
+        }
+        return total;
+    }
+    V2 total = v2(0.0f, 0.0f);
+    for (size_t q = 0; q < 4; ++q)
+        total = add(total, nb_accel(t, static_cast<size_t>(n.child) + q, self, pos, g, soft, theta));
+    return total;
+}
+
+// Force fields (step.rs:212-259): prepare() of every field (the n-body trees), then
+// v += dt * sum of accelerations, then the speed clamp.
 void apply_force_fields(oracle_sim &s, float dt) {
     if (s.fields.empty()) return;
     const float *data = s.field_data.data();
+    std::vector<NbTree> trees(s.fields.size());
+    for (size_t k = 0; k < s.fields.size(); ++k) {
+        const oracle_force_field &f = s.fields[k];
+        if (f.kind == 9)
+            nb_build(trees[k], s.p, static_cast<size_t>(f.params[3]), static_cast<size_t>(f.params[4]));
+    }
     for (size_t i = 0; i < s.active_count; ++i) {
         P &q = s.p[i];
         if (q.pinned != 0) continue;
         V2 dv = v2(0, 0);
-        for (const oracle_force_field &f : s.fields) dv = add(dv, field_acceleration(f, data, q, q.material_id));
+        for (size_t k = 0; k < s.fields.size(); ++k) {
+            const oracle_force_field &f = s.fields[k];
+            if (f.kind == 9)  // NBodyGravityField (n_body.rs:347-360)
+                dv = add(dv, nb_accel(trees[k], 0, i, load_v(q.x), f.params[0], f.params[1], f.params[2]));
+            else
+                dv = add(dv, field_acceleration(f, data, q, q.material_id));
+        }
         store_v(q.v, add(load_v(q.v), smul(dt, dv)));
     }
     const float vel_limit = s.cfg.grid_cell_size / dt;
@@ -2271,11 +2423,40 @@ void oracle_field_acceleration(const oracle_force_field *f, const float *data,
     out[1] = a.y;
 }
 
+void oracle_field_accelerations(oracle_sim *s, float *out) {
+    const float *data = s->field_data.data();
+    std::vector<NbTree> trees(s->fields.size());
+    for (size_t k = 0; k < s->fields.size(); ++k) {
+        const oracle_force_field &f = s->fields[k];
+        if (f.kind == 9)
+            nb_build(trees[k], s->p, static_cast<size_t>(f.params[3]), static_cast<size_t>(f.params[4]));
+    }
+    for (size_t i = 0; i < s->p.size(); ++i) {
+        const P &q = s->p[i];
+        V2 dv = v2(0, 0);
+        for (size_t k = 0; k < s->fields.size(); ++k) {
+            const oracle_force_field &f = s->fields[k];
+            if (f.kind == 9)
+                dv = add(dv, nb_accel(trees[k], 0, i, load_v(q.x), f.params[0], f.params[1], f.params[2]));
+            else
+                dv = add(dv, field_acceleration(f, data, q, q.material_id));
+        }
+        out[2 * i] = dv.x;
+        out[2 * i + 1] = dv.y;
+    }
+}
+
 int oracle_set_force_fields(oracle_sim *s, const oracle_force_field *fields, uint32_t n,
                             const float *data, uint64_t n_data) {
     for (uint32_t k = 0; k < n; ++k) {
         const oracle_force_field &f = fields[k];
-        if (f.kind < 1 || f.kind > 8) return -1;
+        if (f.kind < 1 || f.kind > 9) return -1;
+        if (f.kind == 9) {  // theta in (0, 1] (n_body.rs:306-311); integral depth and leaf size
+            const float theta = f.params[2], depth = f.params[3], maxb = f.params[4];
+            if (!(theta > 0.0f && theta <= 1.0f)) return -1;
+            if (!(depth >= 0.0f && depth <= 24.0f && depth == std::floor(depth))) return -1;
+            if (!(maxb >= 0.0f && maxb <= 2147483647.0f && maxb == std::floor(maxb))) return -1;
+        }
         uint64_t need = 0;
         if (f.kind == 1) need = 3ull * f.count;
         if (f.kind == 6) need = 3ull * f.count + f.n_charges;

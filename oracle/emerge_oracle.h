@@ -198,6 +198,9 @@ void oracle_set_correctly_rounded(int on);
  * data out of range. */
 int oracle_set_force_fields(oracle_sim *s, const oracle_force_field *fields, uint32_t n,
                             const float *data, uint64_t n_data);
+/* The fields' summed Field::acceleration for every particle (out[2 i], out[2 i + 1]), the
+ * n-body trees built from the current positions (n_body.rs:332-360). */
+void oracle_field_accelerations(oracle_sim *s, float *out);
 /* DirectionalContactGrip (grid/directional_grip.rs) for contact resolution:
  * on = 0 removes it (Coulomb friction with SimConfig::contact_friction). */
 void oracle_set_contact_grip(oracle_sim *s, int on, float mu_easy, float mu_resist, float dir_x,

@@ -94,6 +94,7 @@ def lib() -> ctypes.CDLL:
             "oracle_set_force_fields": (c_int, [c_void_p, P(ForceFieldC), c_uint32, P(c_float),
                                                 c_uint64]),
             "oracle_field_acceleration": (None, [P(ForceFieldC), P(c_float), P(Particle), P(c_float)]),
+            "oracle_field_accelerations": (None, [c_void_p, P(c_float)]),
             "oracle_active_count": (c_uint64, [c_void_p]),
             "oracle_replace_particles": (c_int, [c_void_p, c_void_p, c_uint64, c_uint64]),
             "oracle_wake_tag": (None, [c_void_p, c_uint32]),
@@ -230,6 +231,14 @@ class OracleSimulation:
 
     def force_field_names(self):
         return [n for n, _ in self.force_fields]
+
+    def field_accelerations(self) -> np.ndarray:
+        """(n, 2) float32: the fields' summed Field::acceleration per particle at the current
+        state (n-body trees built from the current positions, n_body.rs:332-360)."""
+        n = self.particle_count()
+        out = np.zeros((max(n, 1), 2), dtype=np.float32)
+        self._lib.oracle_field_accelerations(self._sim, out.ctypes.data_as(POINTER(c_float)))
+        return out[:n]
 
     def add_boundary_condition(self, b):
         self.boundaries.append(b)

@@ -316,6 +316,71 @@ def field_scene(sim_cls, asflip=0.0, fields=True, grid_res=96, seed=5, dt=0.05, 
     return sim
 
 
+def nbody_points(n, seed=13, layout="blobs", grid_res=128):
+    """Particle set for NBodyGravityField accelerations: positions and masses in reference
+    index order.  layout "blobs": three Gaussian clusters of different widths; "uniform":
+    uniform in the grid's interior; "clustered": 90 % of the particles within 0.05 cells of
+    one point (leaves at the tree's maximum depth hold many bodies), the rest uniform;
+    "duplicates": positions on a coarse lattice so that many coincide.  Masses are seeded in
+    [0.1, 1]; every 11th particle has none (not a body, but still evaluated)."""
+    from emerge_engine_b200.abi import PARTICLE_DTYPE
+    rng = np.random.default_rng(seed)
+    lo, hi = 4.0, grid_res - 4.0
+    if layout == "blobs":
+        centers = np.array([[0.3, 0.35], [0.7, 0.6], [0.45, 0.75]]) * grid_res
+        widths = np.array([4.0, 9.0, 2.0])
+        k = rng.integers(0, 3, n)
+        x = centers[k] + rng.normal(size=(n, 2)) * widths[k, None]
+    elif layout == "uniform":
+        x = rng.uniform(lo, hi, (n, 2))
+    elif layout == "clustered":
+        x = rng.uniform(lo, hi, (n, 2))
+        m = rng.random(n) < 0.9
+        x[m] = grid_res * 0.4 + rng.uniform(-0.05, 0.05, (int(m.sum()), 2))
+    elif layout == "duplicates":
+        x = np.floor(rng.uniform(lo, hi, (n, 2)) / 4.0) * 4.0
+    else:
+        raise ValueError(layout)
+    p = np.zeros(n, dtype=PARTICLE_DTYPE)
+    p["x"] = np.clip(x, lo, hi).astype(np.float32)
+    p["mass"] = rng.uniform(0.1, 1.0, n).astype(np.float32)
+    p["mass"][::11] = 0.0
+    p["f"] = np.array([1.0, 0.0, 0.0, 1.0], dtype=np.float32)
+    p["initial_volume"] = 0.25
+    p["volume"] = 0.25
+    p["density"] = 1.0
+    return p
+
+
+def nbody_field(G=20.0, softening=1.0, theta=0.5, max_depth=8, max_bodies=4):
+    from emerge_engine_b200 import NBodyGravityField
+    f = NBodyGravityField.new(G, softening, theta)
+    f.max_depth = max_depth
+    f.max_bodies_per_node = max_bodies
+    return f
+
+
+def nbody_scene(sim_cls, grid_res=128, seed=13, dt=0.05, G=20.0, softening=1.0, theta=0.5,
+                max_depth=8, max_bodies=4, pinned_every=0, **sim_kw):
+    """Self-gravitating clumps: three NeoHookean (400, 200) blocks at 4 ppc with seeded jitter
+    and initial velocities in a grid_res^2 grid without gravity, pulled together by
+    NBodyGravityField(G, softening, theta) (tree shape max_depth, max_bodies); every
+    pinned_every-th particle pinned (0: none)."""
+    cfg = SimConfig.standard(grid_res, dt, (0.0, 0.0))
+    sim = sim_cls.empty(cfg, **sim_kw).with_default_material(NeoHookeanMaterial.new(400.0, 200.0))
+    for k, (cx, cy, side) in enumerate(((0.3, 0.4, 18), (0.68, 0.55, 14), (0.5, 0.75, 10))):
+        s = SpawnRegion.for_sim(cfg)
+        s.spacing, s.box_size, s.box_center = 0.5, (side, side), (grid_res * cx, grid_res * cy)
+        s.position_jitter, s.rng_seed, s.initial_velocity_scale = 0.3, seed + k, 1.0
+        sim.add_body(s)
+    if pinned_every:
+        p = sim.particles()
+        p["pinned"][::pinned_every] = 1
+        sim.set_particles(p)
+    sim.add_force_field(nbody_field(G, softening, theta, max_depth, max_bodies))
+    return sim
+
+
 def sleep_scene(sim_cls, threshold=0.05, grid_res=96, seed=9, dt=0.05, **sim_kw):
     """Sleep partition: NeoHookean (400, 200) at 4 ppc in a grid_res^2 grid, gravity (0, -1),
     sleep_threshold `threshold`.  Tag 1: a 32 x 10 block resting on the floor (asleep after

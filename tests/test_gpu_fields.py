@@ -84,3 +84,100 @@ def test_field_api_on_the_device(cuda_lib):
     assert np.isfinite(sim.particles()["v"]).all()
     with pytest.raises(Exception):
         Batch([scenes.field_scene(Simulation)])  # fields run as single simulations
+
+
+# ---------------------------------------------------------------- NBodyGravityField
+NBODY_CASES = [  # layout, particles, G, softening, theta, max_depth, max_bodies_per_node
+    ("blobs", 20_000, 20.0, 1.0, 0.5, 8, 4),
+    ("uniform", 50_000, 5.0, 0.5, 1.0, 8, 4),
+    ("blobs", 30_000, 20.0, 2.0, 0.3, 10, 1),
+    ("clustered", 40_000, 10.0, 0.01, 0.7, 6, 2),
+    ("duplicates", 25_000, 1.0, 1.0, 0.5, 8, 0),
+    ("uniform", 3_000, 3.0, 0.5, 0.5, 0, 4),
+    ("blobs", 1, 3.0, 0.5, 0.5, 8, 4),
+]
+
+
+def _with_points(cls, p, field):
+    from emerge_engine_b200 import SimConfig
+    sim = cls.empty(SimConfig.standard(128, 0.05, (0.0, 0.0)))
+    sim.add_particles(p)
+    sim.add_force_field(field)
+    return sim
+
+
+@pytest.mark.parametrize("cls", [Simulation, DeterministicSimulation])
+@pytest.mark.parametrize("layout,n,g,soft,theta,depth,maxb", NBODY_CASES)
+def test_nbody_accelerations_match_the_oracle_bit_for_bit(cuda_lib, cls, layout, n, g, soft, theta, depth, maxb):
+    """The device tree (built from sorted quadrant paths, centers of mass folded in insertion
+    order) and its stack traversal against the oracle's one-at-a-time insertion and
+    recursion: identical bits on both pipelines, for any tree shape."""
+    p = scenes.nbody_points(n, seed=n + depth, layout=layout)
+    field = scenes.nbody_field(g, soft, theta, depth, maxb)
+    got = _with_points(cls, p, field).field_accelerations()
+    want = _with_points(OracleSimulation, p, field).field_accelerations()
+    np.testing.assert_array_equal(got.view(np.uint32), want.view(np.uint32))
+
+
+def test_nbody_with_other_fields_in_order(cuda_lib):
+    from emerge_engine_b200 import LinearDragField, RadialConfinementField
+    p = scenes.nbody_points(10_000, seed=2, layout="blobs")
+    p["v"] = np.float32(0.5)
+    out = []
+    for cls in (Simulation, OracleSimulation):
+        sim = _with_points(cls, p, RadialConfinementField.new((64.0, 64.0), 30.0, 0.3))
+        sim.add_force_field(scenes.nbody_field(G=8.0))
+        sim.add_force_field(LinearDragField.new((1.0, 0.0), 0.4, LinearDragField.ALL_MATERIALS))
+        out.append(sim.field_accelerations())
+    np.testing.assert_array_equal(out[0].view(np.uint32), out[1].view(np.uint32))
+
+
+def test_nbody_parameters_are_checked(cuda_lib):
+    from emerge_engine_b200.abi import EmergeError
+    sim = scenes.nbody_scene(Simulation)
+    with pytest.raises(EmergeError):  # above the device tree's depth limit
+        sim.add_force_field(scenes.nbody_field(max_depth=11))
+    sim.clear_force_fields()
+    sim.add_force_field(scenes.nbody_field(max_depth=6))
+    with pytest.raises(EmergeError):  # two trees of different shape
+        sim.add_force_field(scenes.nbody_field(max_depth=7))
+    sim.clear_force_fields()
+    sim.add_force_field(scenes.nbody_field(max_depth=6, theta=0.4))
+    sim.add_force_field(scenes.nbody_field(max_depth=6, theta=0.9, G=2.0))  # one tree, two fields
+    sim.step()
+    assert np.all(np.isfinite(sim.particles()["x"]))
+
+
+@pytest.mark.parametrize("pinned_every", [0, 5])
+def test_nbody_scene_one_frame_reference_order(cuda_lib, pinned_every):
+    g = scenes.nbody_scene(DeterministicSimulation, pinned_every=pinned_every)
+    g.step()
+    with correctly_rounded_math():
+        c = scenes.nbody_scene(OracleSimulation, pinned_every=pinned_every)
+        c.step()
+    assert g.last_substeps() == c.last_substeps()
+    print("nbody reference order 1 frame", compare_particles(g.particles(), c.particles(), **tol("reference_order")))
+
+
+def test_nbody_scene_fast(cuda_lib):
+    g = scenes.nbody_scene(Simulation, dt=1e-3)
+    c = scenes.nbody_scene(OracleSimulation, dt=1e-3)
+    g.step()
+    c.step()
+    assert g.last_substeps() == c.last_substeps() == 1
+    print("nbody fast 1 substep", compare_particles(g.particles(), c.particles(), **tol("fast")))
+    g = scenes.nbody_scene(Simulation)
+    c = scenes.nbody_scene(OracleSimulation)
+    g.step_n(5)
+    c.step_n(5)
+    pg, pc = g.particles(), c.particles()
+    assert pg["mass"].sum(dtype=np.float64) == pc["mass"].sum(dtype=np.float64)
+    m = pc["mass"].astype(np.float64)
+    p_abs = (m * np.linalg.norm(pc["v"].astype(np.float64), axis=1)).sum()
+    dp = (m[:, None] * pg["v"]).sum(0) - (m[:, None] * pc["v"]).sum(0)
+    assert np.linalg.norm(dp) <= 1e-3 * p_abs
+    for center, r in (((64.0, 64.0), 128.0), ((38.0, 51.0), 14.0), ((87.0, 70.0), 12.0)):
+        sg, sc = g.region_state(center, r), c.region_state(center, r)
+        assert sg.count == sc.count
+        for k in ("avg_speed", "avg_det_f"):
+            assert getattr(sg, k) == pytest.approx(getattr(sc, k), rel=1e-3, abs=1e-6), (k, center)
