@@ -40,19 +40,23 @@ struct NBodyTreeHost {
     int max_bodies = 0;      // max_bodies_per_node
     float theta_max = 0.0f;  // largest theta over the NBody fields (which nodes may be far)
     float4 *root = nullptr;
-    float4 *body = nullptr;
+    float4 *bdata = nullptr;     // per particle slot (cap)
+    uint2 *path = nullptr;       // per reference index: full quadrant path (or none), slot (cap)
+    uint32_t *order = nullptr;   // (depth + 1) levels of `stride` entries
+    size_t stride = 0;
     uint2 *range = nullptr;
     float4 *com = nullptr;
     NBodyBounds *bounds = nullptr;
 };
-// Builds the tree over the n particles of P on `stream` (the key sort uses `sort`, which
-// must hold n entries); returns the kernels launched.
-int launch_nbody_build(const NBodyTreeHost &t, const DevParticles &P, int n, SortScratch &sort,
-                       cudaStream_t stream);
+// Builds the tree over the n particles of P on `stream` (the level sorts use `sort`, which
+// must hold n entries).
+void launch_nbody_build(const NBodyTreeHost &t, const DevParticles &P, int n, SortScratch &sort,
+                        cudaStream_t stream);
 // The kernels launch_nbody_build launches for n particles.
 inline int nbody_build_kernels(int depth, int n) {
-    const int bits = 2 * depth + 1;
-    return 3 + (n > 0 ? 2 : 0) + (n > 1 ? 5 * ((bits + 7) / 8) : 0);
+    int k = 4;  // reset, bounds, paths, centers
+    for (int d = 0; d <= depth; ++d) k += 2 + (n > 1 ? 5 * ((2 * d + 1 + 7) / 8) : 0);
+    return k;
 }
 
 // split: 0 one pass; 1 / 2 its G2P and fields halves (ParticleKernelArgs::split)

@@ -4,25 +4,28 @@
 //
 // The reference inserts the particles of positive mass one at a time in index order into a
 // pointer quadtree.  Its shape does not depend on that order: a node below max_depth is
-// split exactly when more than max_bodies_per_node bodies fall into it.  The device
-// therefore builds it in four data-parallel steps:
+// split exactly when more than max_bodies_per_node bodies fall into it.  What depends on the
+// order is the arithmetic: each node folds its center of mass body by body in insertion
+// order (MassProps::add, n_body.rs:96-107), and a leaf sums its bodies in the order it
+// holds them.  The device builds the tree in data-parallel steps:
 //   1. bounds   the bodies' bounding box (the root box, n_body.rs:228-247) and that of every
 //               particle (where the field is evaluated), by warp reductions and atomics;
-//   2. keys     each body's quadrant path from the root (2 bits per level, the boxes'
-//               centers computed as the reference's insertion computes them) written at its
-//               reference index, so that the stable radix sort keeps index order among
-//               equal paths; particles without mass sort behind every body;
-//   3. ranges   after the sort, each body's slot at every level opens or closes a run of
-//               equal path prefixes: the bodies of every node, in insertion order;
-//   4. centers  each node's total mass and center of mass, folded over its run in
-//               insertion order with the reference's incremental update (MassProps::add,
-//               n_body.rs:96-107), one thread per node.  A node that no particle can see as
-//               far (its width over the largest distance to any particle is at least theta)
-//               is never asked for its center and is not folded: typically the root and
-//               its four children, whose folds would be the longest.
-// The fold and every box center use the reference's operations in the same order with
-// IEEE rounding, so the tree -- and the field's accelerations -- match the reference bit
-// for bit on both pipelines.
+//   2. paths    each body's quadrant path from the root (2 bits per level, the boxes'
+//               centers computed as the reference's insertion computes them), stored at
+//               its reference index;
+//   3. levels   for every level d, a stable radix sort of the path prefixes of length d
+//               taken in reference index order: the level's body order, in which every
+//               level-d node is one run with its bodies in insertion order; particles
+//               without mass sort behind every body.  The run boundaries give each slot's
+//               range;
+//   4. centers  each node's total mass and center of mass, folded over its run in its
+//               level's order with the reference's operations, one thread per node.  A
+//               node that no particle can see as far (its width over the largest distance
+//               to any particle is at least theta) is never asked for its center and is not
+//               folded: typically the root and its four children, whose folds are longest.
+// Every fold and box center uses the reference's operations in the same order with IEEE
+// rounding, so the tree -- and the field's accelerations -- match the reference bit for bit
+// on both pipelines.
 #include "device_state.cuh"
 #include "kernels.h"
 
@@ -129,54 +132,55 @@ __device__ __forceinline__ uint32_t nb_descend(float2 p, float2 &c, float &half)
     return q;
 }
 
-// Step 2.  keys / vals are indexed by reference index: the radix sort is stable, so bodies of
-// equal path stay in insertion (index) order.
-__global__ void k_nb_keys(const float2 *x, const float *mass, const uint32_t *slot_to_index, int n,
-                          const NBodyBounds *b, int depth, float4 *root_out, uint32_t *keys,
-                          uint32_t *vals) {
+// Step 2.  path[ref] = {quadrant path of D levels, or 1 << 2D without mass; particle slot}.
+__global__ void k_nb_paths(const float2 *x, const float *mass, const uint32_t *slot_to_index, int n,
+                           const NBodyBounds *b, int depth, float4 *root_out, float4 *bdata, uint2 *path) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const float4 rt = nb_root(*b);
     if (i == 0) root_out[0] = rt;
     if (i >= n) return;
     const uint32_t ref = slot_to_index[i];
+    const float2 p = x[i];
+    const float m = mass[i];
+    bdata[i] = make_float4(p.x, p.y, m, __uint_as_float(ref));
     if (ref >= static_cast<uint32_t>(n)) return;
-    uint32_t key = 1u << (2 * depth);  // no mass: behind every body
-    if (mass[i] > 0.0f) {
-        const float2 p = x[i];
+    uint32_t key = 1u << (2 * depth);
+    if (m > 0.0f) {
         float2 c = make_float2(rt.x, rt.y);
         float half = rt.z;
         key = 0u;
         for (int d = 0; d < depth; ++d) key = (key << 2) | nb_descend(p, c, half);
     }
-    keys[ref] = key;
-    vals[ref] = static_cast<uint32_t>(i);
+    path[ref] = make_uint2(key, static_cast<uint32_t>(i));
 }
 
-// Step 3.  range must be zero before (an empty slot keeps [0, 0)).
-__global__ void k_nb_ranges(const uint32_t *keys, const uint32_t *vals, const float2 *x, const float *mass,
-                            const uint32_t *slot_to_index, int n, const NBodyBounds *b, int depth, float4 *body,
-                            uint2 *range) {
+// Step 3, before the sort of level d: keys in reference index order.
+__global__ void k_nb_level_keys(const uint2 *path, int n, int depth, int d, uint32_t *keys, uint32_t *vals) {
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= n) return;
+    const uint2 pv = path[r];
+    keys[r] = (pv.x >> (2 * depth)) != 0u ? (1u << (2 * d)) : (pv.x >> (2 * (depth - d)));
+    vals[r] = pv.y;
+}
+
+// Step 3, after the sort: the level's order and its slots' runs (range zeroed before).
+__global__ void k_nb_level_ranges(const uint32_t *keys, const uint32_t *vals, int n, const NBodyBounds *b, int d,
+                                  uint32_t *order, uint2 *range) {
     const int j = blockIdx.x * blockDim.x + threadIdx.x;
     const int nb = static_cast<int>(b->n_bodies);
     if (j >= nb || j >= n) return;
-    const uint32_t key = keys[j];
-    const uint32_t slot = vals[j];
-    if ((key >> (2 * depth)) != 0u || slot >= static_cast<uint32_t>(n)) return;  // not a body's key
-    const float2 p = x[slot];
-    body[j] = make_float4(p.x, p.y, mass[slot], __uint_as_float(slot_to_index[slot]));
-    const uint32_t prev = j > 0 ? keys[j - 1] : 0u, next = j + 1 < nb ? keys[j + 1] : 0u;
-    for (int d = 0; d <= depth; ++d) {
-        const int shift = 2 * (depth - d);
-        const uint32_t pd = key >> shift;
-        const int s = nbody_level_offset(d) + static_cast<int>(pd);
-        if (j == 0 || (prev >> shift) != pd) range[s].x = static_cast<uint32_t>(j);
-        if (j + 1 == nb || (next >> shift) != pd) range[s].y = static_cast<uint32_t>(j + 1);
-    }
+    const uint32_t key = keys[j], v = vals[j];
+    const bool ok = (key >> (2 * d)) == 0u && v < static_cast<uint32_t>(n);  // a body's key
+    order[j] = ok ? v : 0u;  // every entry of the level's body range names a valid slot
+    if (!ok) return;
+    const int s = nbody_level_offset(d) + static_cast<int>(key);
+    if (j == 0 || keys[j - 1] != key) range[s].x = static_cast<uint32_t>(j);
+    if (j + 1 == nb || keys[j + 1] != key) range[s].y = static_cast<uint32_t>(j + 1);
 }
 
 // Step 4.  com.w = 1 marks a folded node (an empty one included: it is never far).
-__global__ void k_nb_centers(const uint2 *range, const float4 *body, const float4 *root, const NBodyBounds *b,
-                             int depth, float theta_max, float4 *com) {
+__global__ void k_nb_centers(const uint2 *range, const float4 *bdata, const uint32_t *order, size_t stride,
+                             const float4 *root, const NBodyBounds *b, int depth, float theta_max, float4 *com) {
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= nbody_slots(depth)) return;
     int d = 0;
@@ -209,9 +213,10 @@ __global__ void k_nb_centers(const uint2 *range, const float4 *body, const float
             return;
         }
     }
+    const uint32_t *ord = order + static_cast<size_t>(d) * stride;
     float tm = 0.0f, cx = 0.0f, cy = 0.0f;
     for (uint32_t j = rg.x; j < rg.y; ++j) {
-        const float4 q = body[j];
+        const float4 q = bdata[ord[j]];
         const float nt = __fadd_rn(tm, q.z);
         if (nt > 0.0f) {
             cx = __fdiv_rn(__fadd_rn(__fmul_rn(cx, tm), __fmul_rn(q.x, q.z)), nt);
@@ -224,35 +229,23 @@ __global__ void k_nb_centers(const uint2 *range, const float4 *body, const float
 
 }  // namespace
 
-int launch_nbody_build(const NBodyTreeHost &t, const DevParticles &P, int n, SortScratch &sort,
-                       cudaStream_t stream) {
+void launch_nbody_build(const NBodyTreeHost &t, const DevParticles &P, int n, SortScratch &sort,
+                        cudaStream_t stream) {
     const int slots = nbody_slots(t.depth);
-    const int gb = (n + NB_THREADS - 1) / NB_THREADS;
+    const int gb = n > 0 ? (n + NB_THREADS - 1) / NB_THREADS : 1;
     k_nb_reset<<<1, 32, 0, stream>>>(t.bounds);
-    int kernels = 1;
-    if (n > 0) {
-        k_nb_bounds<<<gb, NB_THREADS, 0, stream>>>(P.x, P.mass, n, t.bounds);
-        kernels += 1;
-    }
-    k_nb_keys<<<gb > 0 ? gb : 1, NB_THREADS, 0, stream>>>(P.x, P.mass, P.slot_to_index, n, t.bounds, t.depth,
-                                                          t.root, sort.keys[0], sort.vals[0]);
-    kernels += 1;
-    int r = 0;
-    if (n > 1) {
-        const int bits = 2 * t.depth + 1;
-        r = radix_sort_pairs(sort, n, bits, stream);
-        kernels += 5 * ((bits + 7) / 8);
-    }
+    k_nb_bounds<<<gb, NB_THREADS, 0, stream>>>(P.x, P.mass, n, t.bounds);
+    k_nb_paths<<<gb, NB_THREADS, 0, stream>>>(P.x, P.mass, P.slot_to_index, n, t.bounds, t.depth, t.root, t.bdata,
+                                              t.path);
     cudaMemsetAsync(t.range, 0, static_cast<size_t>(slots) * sizeof(uint2), stream);
-    if (n > 0) {
-        k_nb_ranges<<<gb, NB_THREADS, 0, stream>>>(sort.keys[r], sort.vals[r], P.x, P.mass, P.slot_to_index, n,
-                                                   t.bounds, t.depth, t.body, t.range);
-        kernels += 1;
+    for (int d = 0; d <= t.depth; ++d) {
+        k_nb_level_keys<<<gb, NB_THREADS, 0, stream>>>(t.path, n, t.depth, d, sort.keys[0], sort.vals[0]);
+        const int r = radix_sort_pairs(sort, n, 2 * d + 1, stream);
+        k_nb_level_ranges<<<gb, NB_THREADS, 0, stream>>>(sort.keys[r], sort.vals[r], n, t.bounds, d,
+                                                         t.order + static_cast<size_t>(d) * t.stride, t.range);
     }
-    k_nb_centers<<<(slots + NB_THREADS - 1) / NB_THREADS, NB_THREADS, 0, stream>>>(t.range, t.body, t.root,
-                                                                                    t.bounds, t.depth,
-                                                                                    t.theta_max, t.com);
-    return kernels + 1;
+    k_nb_centers<<<(slots + NB_THREADS - 1) / NB_THREADS, NB_THREADS, 0, stream>>>(
+        t.range, t.bdata, t.order, t.stride, t.root, t.bounds, t.depth, t.theta_max, t.com);
 }
 
 }  // namespace emerge

@@ -968,16 +968,20 @@ EM_HD void init_particle(const MatP &m, emerge_particle &p) {
 // quadrant 0 first) is slot (4^d - 1) / 3 + pre.  A node exists when its parent holds more
 // than max_bodies bodies; it is a leaf when it holds at most max_bodies or sits at level
 // `depth` -- the tree the reference's one-at-a-time insertion builds, which does not depend
-// on the insertion order.  The bodies of a slot are a contiguous run of `body`, in reference
-// index order (the insertion order).
+// on the insertion order.  Level d keeps its own order of the bodies, sorted by the level's
+// path prefix and, within a node, by reference index (the insertion order): the bodies of a
+// level-d slot are the run [first, end) of that order, so a leaf sums its bodies, and a node
+// folds its center of mass, in the reference's order.
 constexpr int NBODY_MAX_DEPTH = 10;
 struct NBodyView {
     int depth;             // max_depth (0..NBODY_MAX_DEPTH)
     int max_bodies;        // max_bodies_per_node
     const float4 *root;    // {center.x, center.y, half size, 0} of the root box
-    const float4 *body;    // bodies in tree order: x, y, mass, reference index (as bits)
-    const uint2 *range;    // per slot: [first, end) into body
-    const float4 *com;     // per slot: center of mass x, y, total mass; w = 1 if computed
+    const float4 *bdata;   // per particle slot: x, y, mass, reference index (as bits)
+    const uint32_t *order; // level d's body order (particle slots) at order + d * stride
+    size_t stride;
+    const uint2 *range;    // per tree slot: [first, end) into its level's order
+    const float4 *com;     // per tree slot: center of mass x, y, total mass; w = 1 if computed
     uint32_t *error;       // StepState::error_flags (a far node without its center of mass)
 };
 
@@ -1152,7 +1156,7 @@ __device__ __forceinline__ float2 nbody_acceleration(const NBodyView &nb, const 
                                                      uint32_t self) {
     const float g = f.params[0], soft = f.params[1], theta = f.params[2];
     const float eps2 = soft * soft;
-    if (!nb.body) return v2(0.0f, 0.0f);
+    if (!nb.bdata) return v2(0.0f, 0.0f);
     const float4 rt = nb.root[0];
     float2 ctr[NBODY_MAX_DEPTH + 1];
     float2 acc[NBODY_MAX_DEPTH + 1];
@@ -1174,8 +1178,9 @@ __device__ __forceinline__ float2 nbody_acceleration(const NBodyView &nb, const 
             r = nbody_pull(vsub(v2(cm.x, cm.y), pos), cm.z, g, eps2);
         } else if (d >= nb.depth || rg.y - rg.x <= static_cast<uint32_t>(nb.max_bodies)) {
             r = v2(0.0f, 0.0f);
+            const uint32_t *ord = nb.order + static_cast<size_t>(d) * nb.stride;
             for (uint32_t j = rg.x; j < rg.y; ++j) {
-                const float4 b = nb.body[j];
+                const float4 b = nb.bdata[ord[j]];
                 if (__float_as_uint(b.w) == self) continue;
                 const float2 rv = vsub(v2(b.x, b.y), pos);
                 if (vdot(rv, rv) < eps2) continue;

@@ -350,11 +350,13 @@ void refresh_dev_config(emerge_sim *s) {
     // as well.
     s->dcfg.mf_excl = (s->dcfg.mf_fast && (s->dcfg.mf_fields == 1 || s->dcfg.mf_fields == 2)) ? 1 : 0;
     s->dcfg.nbody = NBodyView{};
-    if (s->nb.depth >= 0 && s->nbbuf.ptr) {
+    if (s->nb.depth >= 0 && s->nbbuf.ptr && s->nb_alloc_depth == s->nb.depth) {
         s->dcfg.nbody.depth = s->nb.depth;
         s->dcfg.nbody.max_bodies = s->nb.max_bodies;
         s->dcfg.nbody.root = s->nb.root;
-        s->dcfg.nbody.body = s->nb.body;
+        s->dcfg.nbody.bdata = s->nb.bdata;
+        s->dcfg.nbody.order = s->nb.order;
+        s->dcfg.nbody.stride = s->nb.stride;
         s->dcfg.nbody.range = s->nb.range;
         s->dcfg.nbody.com = s->nb.com;
         s->dcfg.nbody.error = &s->d_state->error_flags;
@@ -494,7 +496,9 @@ void enqueue_multi_resolves(const StepLaunch &L) {
     if (L.cfg.mf_fields & 2) launch_mixture_resolve(L);
 }
 
-bool nbody_live(const emerge_sim *s) { return s->nb.depth >= 0 && s->nbbuf.ptr != nullptr; }
+bool nbody_live(const emerge_sim *s) {
+    return s->nb.depth >= 0 && s->nbbuf.ptr != nullptr && s->nb_alloc_depth == s->nb.depth;
+}
 
 // Kernels a substep's particle pass takes beyond the one pass: with an NBodyGravityField, the
 // tree build and the fields half.
@@ -524,18 +528,29 @@ emerge_status nbody_prepare(emerge_sim *s) {
     s->nbbuf.reset();
     const size_t cap = std::max<size_t>(s->cap, 1);
     const size_t slots = static_cast<size_t>(nbody_slots(s->nb.depth));
+    const size_t stride = align_up(cap, 64);
     const size_t b_bounds = align_up(sizeof(NBodyBounds), 256), b_root = 256;
-    const size_t b_body = align_up(cap * sizeof(float4), 256), b_range = align_up(slots * sizeof(uint2), 256);
-    const size_t b_com = align_up(slots * sizeof(float4), 256);
-    const size_t bytes = b_bounds + b_root + b_body + b_range + b_com;
+    const size_t b_bdata = align_up(cap * sizeof(float4), 256), b_path = align_up(cap * sizeof(uint2), 256);
+    const size_t b_order = static_cast<size_t>(s->nb.depth + 1) * stride * sizeof(uint32_t);
+    const size_t b_range = align_up(slots * sizeof(uint2), 256), b_com = align_up(slots * sizeof(float4), 256);
+    const size_t bytes = b_bounds + b_root + b_bdata + b_path + b_order + b_range + b_com;
     CK(cudaMalloc(&s->nbbuf.ptr, bytes));
     s->nbbuf.bytes = bytes;
     char *p = static_cast<char *>(s->nbbuf.ptr);
     s->nb.bounds = reinterpret_cast<NBodyBounds *>(p);
-    s->nb.root = reinterpret_cast<float4 *>(p + b_bounds);
-    s->nb.body = reinterpret_cast<float4 *>(p + b_bounds + b_root);
-    s->nb.range = reinterpret_cast<uint2 *>(p + b_bounds + b_root + b_body);
-    s->nb.com = reinterpret_cast<float4 *>(p + b_bounds + b_root + b_body + b_range);
+    p += b_bounds;
+    s->nb.root = reinterpret_cast<float4 *>(p);
+    p += b_root;
+    s->nb.bdata = reinterpret_cast<float4 *>(p);
+    p += b_bdata;
+    s->nb.path = reinterpret_cast<uint2 *>(p);
+    p += b_path;
+    s->nb.order = reinterpret_cast<uint32_t *>(p);
+    s->nb.stride = stride;
+    p += b_order;
+    s->nb.range = reinterpret_cast<uint2 *>(p);
+    p += b_range;
+    s->nb.com = reinterpret_cast<float4 *>(p);
     s->nb_cap = cap;
     s->nb_alloc_depth = s->nb.depth;
     refresh_dev_config(s);
@@ -1496,6 +1511,8 @@ emerge_status emerge_cuda_set_force_fields(emerge_sim *s, const emerge_force_fie
         s->nb.depth = tree.depth;
         s->nb.max_bodies = tree.max_bodies;
         s->nb.theta_max = tree.theta_max;
+        if (s->nb_alloc_depth != tree.depth) s->nbbuf.reset();  // reallocated for the new depth
+        s->nb_alloc_depth = s->nbbuf.ptr ? tree.depth : -1;
     }
     s->fbuf.reset();
     s->n_fields = 0;
