@@ -384,9 +384,12 @@ emerge_status emerge_cuda_region_state(emerge_sim *sim, float cx, float cy, floa
  *   EMERGE_OPT_SORT_INTERVAL   re-sort particles by tile every N steps (default 16;
  *                              0 = only before the first step after particles are added;
  *                              see emerge_cuda_sort_now).
- *   EMERGE_OPT_P2G_AGGREGATE   1 = P2G contributions of lanes sharing a base cell are
- *                              summed in the warp before one global reduction per cell
- *                              (default), 0 = one global reduction per contribution.
+ *   EMERGE_OPT_P2G_AGGREGATE   0 = one global reduction per contribution (default, the
+ *                              fastest measured: reductions in L2 cost less than combining
+ *                              contributions first); 1 = contributions of lanes sharing a
+ *                              base cell are summed in the warp before one global reduction
+ *                              per cell; 2 = lane pairs and quads sharing a base cell are
+ *                              summed first.
  *   EMERGE_OPT_DETERMINISTIC   1 = reference-order mode: every grid cell sums its P2G and
  *                              density contributions sequentially in the reference's
  *                              particle index order (transfer/p2g.rs:16-23), so results
