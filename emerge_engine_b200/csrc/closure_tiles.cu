@@ -28,6 +28,11 @@ namespace emerge {
 
 namespace {
 
+// Resident tile CTAs per SM (the persistent grid is this many per SM): registers bound it,
+// 65,536 / (128 threads x the kernel's registers).
+#ifndef EMERGE_CLOSURE_TILE_CTAS_PER_SM
+#define EMERGE_CLOSURE_TILE_CTAS_PER_SM 3
+#endif
 constexpr int CT_M = 128;         // rows (particles) per tile = TMEM lanes = threads
 constexpr int CT_TMEM_COLS = 64;  // FP32 accumulator columns (the widest layer)
 
@@ -364,7 +369,7 @@ struct TileArgs {
 };
 
 template <unsigned MASK>
-__global__ void __launch_bounds__(CT_M, 1) k_closure_tiles(TileArgs a) {
+__global__ void __launch_bounds__(CT_M, EMERGE_CLOSURE_TILE_CTAS_PER_SM) k_closure_tiles(TileArgs a) {
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     TileSmem &S = *reinterpret_cast<TileSmem *>(smem_raw);
     const int tid = threadIdx.x;
@@ -550,7 +555,7 @@ void launch_closure_tiles(const StepLaunch &L, const LoadFlagsHost &lfh, int sm_
     a.lf.pinned = lfh.pinned;
     a.cl = L.cl;
     const size_t smem = sizeof(TileSmem);
-    const int grid = 3 * (sm_count > 0 ? sm_count : 148);
+    const int grid = EMERGE_CLOSURE_TILE_CTAS_PER_SM * (sm_count > 0 ? sm_count : 148);
     const unsigned cover = covering_mask(L.model_mask);
     if (cover == MASK_GRANULAR) {
         cudaFuncSetAttribute(k_closure_tiles<MASK_GRANULAR>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));

@@ -151,6 +151,52 @@ def test_contact_with_fields_asflip_and_sleep(cuda_lib):
     assert far <= 16
 
 
+def test_contact_with_fields_and_sleep_per_particle(cuda_lib):
+    """The combined scene without ASFLIP (whose position gate is the sign decision above), on
+    the fused pipeline: every particle within the fast bar for 3 frames, with the same
+    partition size as the oracle's, so a field-sum routing error cannot hide under the
+    aggregate statistics."""
+    from emerge_engine_b200 import LinearDragField
+
+    def build(sim_cls):
+        sim = scenes.contact_scene(sim_cls, grip=GRIPS["grip"], asflip=0.0, sleep=0.02)
+        sim.add_force_field(LinearDragField.new((0.5, 0.0), 0.05, LinearDragField.ALL_MATERIALS))
+        return sim
+
+    g, c = build(Simulation), build(OracleSimulation)
+    for k in range(3):
+        g.step()
+        c.step()
+        assert g.last_substeps() == c.last_substeps(), k
+        assert g.active_count() == c.active_count(), k
+        compare_particles(g.particles(), c.particles(), **tol("fast"))
+
+
+class _AggregatedSimulation(Simulation):
+    """The fused pipeline with warp-aggregated P2G (EMERGE_OPT_P2G_AGGREGATE = 1): with one
+    kind of field a warp whose lanes all target one array (the total, or one field's sums)
+    aggregates, and a warp mixing field and non-field particles scatters lane by lane."""
+
+    def __init__(self, *a, **kw):
+        super().__init__(*a, **kw)
+        from emerge_engine_b200.abi import OPT_P2G_AGGREGATE
+        self.set_option(OPT_P2G_AGGREGATE, 1)
+
+
+@pytest.mark.parametrize("scene", ["contact", "mixture"])
+def test_aggregated_field_scatter(cuda_lib, scene):
+    """Per-warp target selection on single-kind field scenes: the contact block lands on the
+    slab (warps along the interface mix grip and slab particles), the water sits on the sand
+    (warps along the interface mix the phases), against the oracle at the fast bar."""
+    if scene == "contact":
+        g, c = scenes.contact_scene(_AggregatedSimulation), scenes.contact_scene(OracleSimulation)
+        frames = 10
+    else:
+        g, c = scenes.mixture_scene(_AggregatedSimulation), scenes.mixture_scene(OracleSimulation)
+        frames = 3
+    print(scene, "aggregated, fast pipeline", run_frames(g, c, frames, "fast"))
+
+
 @pytest.mark.parametrize("mode", ["reference_order", "fast"])
 def test_contact_groups_follow_each_upload(cuda_lib, mode):
     """A write-back that sets contact groups switches the contact fields on; one that clears

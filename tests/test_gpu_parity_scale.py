@@ -7,7 +7,7 @@ What the bars are and why:
     particles (dam break, one frame) and 4,033,816 particles (mixed granular, one substep),
     and the whole particle array after 10 and 100 frames.
   * Fast path: its P2G sums run in L2 in an order that changes from run to run, and its
-    arithmetic contracts into FMA.  The reference itself, given the same particles in another
+    stencil sums use explicit FMAs.  The reference itself, given the same particles in another
     index order (its P2G sums in particle order, transfer/p2g.rs:16-23), moves by a per-
     particle velocity error of p99 ~1.1e-5 after one dam-break frame and ~1.1e-3 after one
     frame of granular plasticity (34 substeps of yield decisions).  So a 1e-5 bar
