@@ -660,7 +660,8 @@ def main():
             subs_i += sim.last_substeps()
             for k in phase_keys:
                 phases[k] += sim.last_timing[k]
-        sim.set_option(OPT_USE_GRAPH, 1)
+        if os.environ.get("EMERGE_CUDA_USE_GRAPH", "1") != "0":  # else keep the host loop
+            sim.set_option(OPT_USE_GRAPH, 1)
         peak, peak_kind = load_peaks()
         per_launch_s = part_us * 1e-6 / max(subs_i, 1)
         alg_bytes = K_PARTICLE_BYTES[spec["material"]] * n_eff
