@@ -244,6 +244,7 @@ ABI_FUNCTIONS = [
                                      c_float, c_float, c_float, c_float]),
     ("emerge_cuda_mlp_infer_bf16", c_int, [c_void_p, c_void_p, c_uint32, c_void_p]),
     ("emerge_cuda_mlp_infer_tc", c_int, [c_void_p, c_void_p, c_uint32, c_void_p]),
+    ("emerge_cuda_silu_fast", c_int, [c_void_p, c_uint32, c_void_p]),
     ("emerge_cuda_batch_create", c_int, [POINTER(c_void_p), c_uint32, POINTER(c_void_p)]),
     ("emerge_cuda_batch_destroy", c_int, [c_void_p]),
     ("emerge_cuda_batch_last_error", c_char_p, [c_void_p]),

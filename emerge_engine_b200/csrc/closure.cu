@@ -728,4 +728,17 @@ emerge_status emerge_cuda_mlp_infer_tc(const float *params, const float *x, uint
     return cudaGetLastError() == cudaSuccess ? EMERGE_OK : EMERGE_ERR_CUDA;
 }
 
+emerge_status emerge_cuda_silu_fast(const float *x, uint32_t n, float *y) {
+    if (!x || !y || n == 0) return EMERGE_ERR_INVALID_ARG;
+    DevBuf dX, dY;
+    if (dX.alloc(static_cast<size_t>(n) * sizeof(float)) != cudaSuccess ||
+        dY.alloc(static_cast<size_t>(n) * sizeof(float)) != cudaSuccess)
+        return EMERGE_ERR_OOM;
+    if (cudaMemcpy(dX.p, x, static_cast<size_t>(n) * sizeof(float), cudaMemcpyHostToDevice) != cudaSuccess ||
+        launch_silu_fast(dX.as<float>(), static_cast<int>(n), dY.as<float>(), nullptr) != cudaSuccess ||
+        cudaMemcpy(y, dY.p, static_cast<size_t>(n) * sizeof(float), cudaMemcpyDeviceToHost) != cudaSuccess)
+        return EMERGE_ERR_CUDA;
+    return EMERGE_OK;
+}
+
 }  // extern "C"

@@ -151,6 +151,12 @@ __device__ __forceinline__ float silu_fast(float z) {
     return 0.5f * z * (1.0f + t);
 }
 
+// Test hook: y = silu_fast(x), elementwise.
+__global__ void k_silu_fast(const float *x, int n, float *y) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) y[i] = silu_fast(x[i]);
+}
+
 // Writes 8 consecutive BF16 values of row `r` starting at K index k0 (a multiple of 8) into
 // the activation tile (K = 64 layout).
 __device__ __forceinline__ void put_row8(unsigned char *a, int r, int k0, const float *v) {
@@ -540,6 +546,11 @@ cudaError_t launch_mlp_tiles(const ClosureNet *net, const float *x, int n, float
 // Launches the tile kernel after the particle pass of a substep (same stream).  Persistent
 // CTAs: three per SM (the registers of 3 x 128 threads and about 45 KB of shared memory
 // each), each looping over the tiles both queues hold this substep.
+cudaError_t launch_silu_fast(const float *x, int n, float *y, cudaStream_t stream) {
+    if (n > 0) k_silu_fast<<<(n + 255) / 256, 256, 0, stream>>>(x, n, y);
+    return cudaGetLastError();
+}
+
 void launch_closure_tiles(const StepLaunch &L, const LoadFlagsHost &lfh, int sm_count) {
     if (L.n == 0 || !L.cl.defer) return;
     TileArgs a;

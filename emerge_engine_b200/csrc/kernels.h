@@ -22,6 +22,8 @@ void launch_closure_tiles(const StepLaunch &L, const LoadFlagsHost &lf, int sm_c
 // test hook: the tile kernel's network on n normalised inputs (closure.cu, emerge_cuda_mlp_infer_tc)
 cudaError_t launch_mlp_tiles(const ClosureNet *net, const float *x, int n, float *y, uint32_t *error,
                              cudaStream_t stream);
+// The tile kernel's SiLU on n values (device pointers; test hook).
+cudaError_t launch_silu_fast(const float *x, int n, float *y, cudaStream_t stream);
 inline bool closure_tiles_on(const StepLaunch &L) {
     const unsigned plastic = (1u << M_DRUCKER_PRAGER) | (1u << M_NACC);
     return L.fast && L.cl.defer && (L.model_mask & plastic) && !(L.model_mask & (1u << M_EXTRAS_BIT));

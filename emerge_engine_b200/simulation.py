@@ -520,6 +520,15 @@ def mlp_infer_tc(params: np.ndarray, x: np.ndarray) -> np.ndarray:
     return y
 
 
+def silu_fast(x: np.ndarray) -> np.ndarray:
+    """The closure tile kernel's SiLU (hardware tanh) on float32 values."""
+    lib = load_library()
+    xx = np.ascontiguousarray(x, np.float32).ravel()
+    y = np.zeros_like(xx)
+    check(lib, lib.emerge_cuda_silu_fast(xx.ctypes.data_as(c_void_p), len(xx), y.ctypes.data_as(c_void_p)))
+    return y
+
+
 def mlp_infer_bf16(params: np.ndarray, x: np.ndarray) -> np.ndarray:
     """The BF16 tensor-core inference of the closure MLP on normalised inputs."""
     lib = load_library()

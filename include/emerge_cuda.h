@@ -578,6 +578,9 @@ emerge_status emerge_cuda_mlp_infer_bf16(const float *params, const float *x, ui
  * tcgen05 tensor cores (BF16 operands in shared memory, FP32 accumulators in tensor memory,
  * SiLU from the hardware tanh).  EMERGE_ERR_TIMEOUT if a bounded wait gave up. */
 emerge_status emerge_cuda_mlp_infer_tc(const float *params, const float *x, uint32_t n, float *y);
+/* Test hook (no reference counterpart): the tile kernel's SiLU, z (1 + tanh(z / 2)) / 2 with
+ * the hardware tanh, on n host values. */
+emerge_status emerge_cuda_silu_fast(const float *x, uint32_t n, float *y);
 
 /* ---- batched scenes (no counterpart in the reference) -----------------------------
  * Many independent scenes advanced together: every substep is one launch per kernel for

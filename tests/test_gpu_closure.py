@@ -53,6 +53,24 @@ def test_tensor_core_inference_matches_bf16_oracle(cuda_lib):
     assert np.max(np.abs(y - y_fp32)) <= 2e-2 * scale   # BF16 vs FP32
 
 
+def test_silu_through_hardware_tanh_meets_its_bound(cuda_lib):
+    """SiLU(z) = z sigma(z) = z (1 + tanh(z / 2)) / 2 with tanh.approx.f32 (relative error
+    about 2^-11 of tanh): against the exp-based float64 SiLU, the error is bounded by
+    2^-11 (|silu| + |z| / 2) -- the second term where 1 + tanh cancels for z << 0 -- over
+    z in [-30, 30], and at 0 it is exact."""
+    from emerge_engine_b200.simulation import silu_fast
+    z = np.concatenate([np.linspace(-30.0, 30.0, 200_001), [0.0, -1e-30, 1e-30]]).astype(np.float32)
+    y = silu_fast(z).astype(np.float64)
+    zd = z.astype(np.float64)
+    ref = zd / (1.0 + np.exp(-zd))
+    err = np.abs(y - ref)
+    bound = 2.0 ** -11 * (np.abs(ref) + 0.5 * np.abs(zd)) + 1e-37
+    assert np.all(err <= bound), float((err / bound).max())
+    assert y[-3] == 0.0
+    # the rounding the network applies next (BF16, 2^-9) is the larger error
+    assert np.median(err[np.abs(ref) > 1e-3] / np.abs(ref[np.abs(ref) > 1e-3])) < 2.0 ** -9
+
+
 @pytest.mark.parametrize("n", [77, 128, 1001, 20_000])
 def test_tile_kernel_inference_matches_bf16_oracle(cuda_lib, n):
     """The closure's tile kernel (tcgen05.mma, accumulators in tensor memory, 128 rows per
