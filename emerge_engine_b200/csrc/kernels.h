@@ -77,6 +77,8 @@ void launch_region_state(const DevParticles &P, int n, float cx, float cy, float
 size_t region_acc_bytes();
 void region_acc_finalize(const void *acc, emerge_body_state *out);
 void launch_gather_aos(const DevParticles &P, int n, emerge_particle *out, cudaStream_t stream);
+// *dst_mapped = *src by a one-thread kernel (dst: pinned host memory's device address).
+void launch_copy_word_to_host(const uint32_t *src, uint32_t *dst_mapped, cudaStream_t stream);
 void launch_scatter_aos(const DevParticles &P, int n, const emerge_particle *in, cudaStream_t stream);
 void launch_check_aos(const emerge_particle *in, int n, uint32_t *flags, cudaStream_t stream);
 void launch_append_aos(const DevParticles &P, int n_old, int n_new, const emerge_particle *in,

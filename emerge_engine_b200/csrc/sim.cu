@@ -163,6 +163,7 @@ struct emerge_sim {
     Buffer sbuf;
     StepState *d_state = nullptr;
     StepState *h_state = nullptr;  // pinned mirror
+    StepState *h_state_dev = nullptr;  // its device address (nullptr: not mapped)
     Buffer region_buf;
 
     // sort
@@ -1358,6 +1359,10 @@ emerge_status emerge_cuda_create(const emerge_sim_config *config, int device, em
     if (!cuda_ok(s, cudaMalloc(&s->sbuf.ptr, sizeof(StepState)), "state alloc", &st)) return bail(st);
     s->d_state = static_cast<StepState *>(s->sbuf.ptr);
     if (!cuda_ok(s, cudaMallocHost(&s->h_state, sizeof(StepState)), "pinned alloc", &st)) return bail(st);
+    if (cudaHostGetDevicePointer(reinterpret_cast<void **>(&s->h_state_dev), s->h_state, 0) != cudaSuccess) {
+        s->h_state_dev = nullptr;  // an unmapped mirror: its words are read back with copies
+        (void)cudaGetLastError();
+    }
     std::memset(s->h_state, 0, sizeof(StepState));
     s->h_state->last_step_dt = config->dt;
     s->h_state->min_mdt_bits[0] = s->h_state->min_mdt_bits[1] = 0x7f800000u;
@@ -1696,8 +1701,16 @@ emerge_status emerge_cuda_write_particles(emerge_sim *s, const emerge_particle *
     CK(cudaStreamWaitEvent(s->stream, s->ev_up_done, 0));
     CK(cudaMemsetAsync(&s->d_state->upload_flags, 0, sizeof(uint32_t), s->stream));
     launch_check_aos(up, static_cast<int>(n), &s->d_state->upload_flags, s->stream);
-    CK(cudaMemcpyAsync(&s->h_state->upload_flags, &s->d_state->upload_flags, sizeof(uint32_t),
-                       cudaMemcpyDeviceToHost, s->stream));
+    // The flags come back by a store into the mapped mirror, not by a copy: a device-to-host
+    // copy here would queue behind a readback still in flight (emerge_cuda_read_particles_async
+    // of the previous step) and hold this call up until it lands.
+    if (s->h_state_dev) {
+        launch_copy_word_to_host(&s->d_state->upload_flags, &s->h_state_dev->upload_flags, s->stream);
+        s->host_launches += 1;
+    } else {
+        CK(cudaMemcpyAsync(&s->h_state->upload_flags, &s->d_state->upload_flags, sizeof(uint32_t),
+                           cudaMemcpyDeviceToHost, s->stream));
+    }
     CK(cudaStreamSynchronize(s->stream));
     s->host_launches += 1;
     const uint32_t flags = s->h_state->upload_flags;

@@ -679,6 +679,14 @@ void region_acc_finalize(const void *acc, emerge_body_state *out) {
     out->pad_ = 0;
 }
 
+// One word from device memory into pinned host memory through its device address: a store
+// from the SM, not a copy, so it does not queue behind device-to-host copies in flight.
+__global__ void k_copy_word_to_host(const uint32_t *src, uint32_t *dst_mapped) { *dst_mapped = *src; }
+
+void launch_copy_word_to_host(const uint32_t *src, uint32_t *dst_mapped, cudaStream_t stream) {
+    k_copy_word_to_host<<<1, 1, 0, stream>>>(src, dst_mapped);
+}
+
 void launch_gather_aos(const DevParticles &P, int n, emerge_particle *out, cudaStream_t stream) {
     if (n) k_gather_aos<<<blocks_for(n, 256), 256, 0, stream>>>(P, n, out);
 }

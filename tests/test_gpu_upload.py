@@ -81,3 +81,30 @@ def test_async_readback_returns_the_state_it_was_queued_after(cuda_lib):
     finally:
         for b in bufs:
             b.free()
+
+
+@pytest.mark.parametrize("scene", ["quickstart", "dam_break"])
+def test_async_readback_into_pinned_and_pageable_memory(cuda_lib, scene):
+    """Two readbacks in flight at once, one into pinned and one into pageable memory: both
+    give particles() bit for bit (240 particles, and 60,001 particles of a dam break)."""
+    from emerge_engine_b200.abi import PARTICLE_DTYPE
+    from emerge_engine_b200.simulation import PinnedBuffer
+    g = scenes.quickstart(Simulation) if scene == "quickstart" else scenes.dam_break(
+        Simulation, grid_res=512, column=128)
+    if scene == "dam_break":
+        p = g.particles()
+        g._replace(p[:60_001], min(g.active_count(), 60_001))
+    g.step()
+    n = g.particle_count()
+    want = g.particles()
+    pinned = PinnedBuffer(n * 128)
+    pageable = np.zeros(n, dtype=PARTICLE_DTYPE)
+    try:
+        g.read_particles_raw_async(pinned.ptr, n)
+        g.read_particles_raw_async(pageable.ctypes.data, n)
+        g.synchronize()
+        np.testing.assert_array_equal(pinned.as_particles(n), want)
+        np.testing.assert_array_equal(pageable, want)
+    finally:
+        pinned.free()
+
