@@ -598,7 +598,8 @@ typedef struct emerge_batch_tune_report {
     int32_t chunks_per_cta;      /* chosen EMERGE_OPT_CHUNKS_PER_CTA */
     uint32_t n_trials;
     uint32_t from_cache;         /* 1: taken from the cache file, no trials run */
-    float best_ms;               /* GPU ms per frame of the chosen setting (0 from the cache) */
+    float best_ms;               /* GPU ms per frame of the chosen setting (from the cache: as
+                                    stored when it was tuned) */
     int32_t trial_sort_interval[EMERGE_TUNE_MAX_TRIALS];
     int32_t trial_aggregate[EMERGE_TUNE_MAX_TRIALS];
     int32_t trial_tile_shape[EMERGE_TUNE_MAX_TRIALS];
