@@ -736,7 +736,9 @@ def main():
                          "readback": "emerge_cuda_read_particles_async (copy stream; overlaps "
                                      "the next step's upload)"}
     if not args.no_extras:
-        if spec["material"] == "DP+Snow+NACC" and not args.no_closure and "closure" not in skip:
+        # the closure's A/B (training included) on one GPU only: a scaling run's ranks would each
+        # repeat it, holding every GPU for minutes outside the timed region
+        if spec["material"] == "DP+Snow+NACC" and not args.no_closure and "closure" not in skip and world == 1:
             extras["learned_closure"] = closure_ab(sim, n, args.steps, value)
         if world == 1 and rank == 0 and "cpu" not in skip:
             extras["cpu_baseline"] = cpu_baseline(args.workload, args.cpu_budget)
