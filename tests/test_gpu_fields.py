@@ -181,3 +181,36 @@ def test_nbody_scene_fast(cuda_lib):
         assert sg.count == sc.count
         for k in ("avg_speed", "avg_det_f"):
             assert getattr(sg, k) == pytest.approx(getattr(sc, k), rel=1e-3, abs=1e-6), (k, center)
+
+
+def test_nbody_with_the_sleep_partition_reference_order(cuda_lib):
+    """The tree inserts the bodies in reference index order, which the sleep partition
+    changes every substep (a sleeping particle swaps with the last awake one): with sleep on,
+    the reference-order mode stays within the reference-order bar of the oracle frame by
+    frame, with the same partition size."""
+    def build_cfg(cls):
+        from emerge_engine_b200 import NeoHookeanMaterial, SimConfig, SpawnRegion
+        cfg = SimConfig.standard(128, 0.05, (0.0, 0.0))
+        cfg.sleep_threshold = 0.05
+        sim = cls.empty(cfg).with_default_material(NeoHookeanMaterial.new(400.0, 200.0))
+        for k, (cx, cy, side, v) in enumerate(((0.3, 0.4, 18, 0.0), (0.68, 0.55, 14, 1.0))):
+            sp = SpawnRegion.for_sim(cfg)
+            sp.spacing, sp.box_size, sp.box_center = 0.5, (side, side), (128 * cx, 128 * cy)
+            sp.position_jitter, sp.rng_seed, sp.initial_velocity_scale = 0.3, 30 + k, v
+            sim.add_body(sp)
+        sim.add_force_field(scenes.nbody_field(G=0.5))
+        return sim
+
+    g = build_cfg(DeterministicSimulation)
+    fewest_awake = None
+    with correctly_rounded_math():
+        c = build_cfg(OracleSimulation)
+        for k in range(4):
+            g.step()
+            c.step()
+            assert g.last_substeps() == c.last_substeps(), k
+            assert g.active_count() == c.active_count(), k
+            compare_particles(g.particles(), c.particles(), **tol("reference_order"))
+            fewest_awake = min(fewest_awake or c.active_count(), c.active_count())
+    assert fewest_awake < c.particle_count()  # part of the scene slept: the partition was in use
+
