@@ -461,6 +461,21 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+# The parity bar the measured path meets (the fast path; tests/test_gpu_parity_scale.py holds
+# it against the oracle).  The reference-order mode (DeterministicSimulation) is bit identical
+# to the oracle on the same scenes.
+PARITY = {
+    "path": "fast (P2G summed by L2 reductions in a run-to-run order)",
+    "bars": {"dam_break_1m, one frame": "x <= 1e-5, v p50 <= 1e-5, p99 <= 3e-5, max <= 2e-3",
+             "mixed_granular_4m, one substep": "v <= 1e-5 per particle",
+             "100 frames (dam break 262k, granular 160k)": "region statistics within max(1e-3, 2x the "
+                                                            "reference's own reordering distance)",
+             "always": "mass exact, momentum within 1e-6 of the total |momentum|"},
+    "reference_order_mode": "bit identical to the oracle (1M dam break frame, 4M granular substep)",
+    "tests": "tests/test_gpu_parity_scale.py, tests/test_gpu_parity.py",
+}
+
+
 def workload_config(workload: str, particles: int, world: int) -> dict:
     """The `config` object of both arms' lines (identical keys and values for one workload)."""
     spec = WORKLOADS[workload]
@@ -753,6 +768,7 @@ def main():
             "substeps_per_step": substeps / args.steps,
             "gpu_launches": launches,
             "clocks": clock_info,
+            "parity": PARITY,
         }
         line.update(extras)
         print(json.dumps(line), flush=True)
