@@ -51,8 +51,8 @@ struct NBodyTreeHost {
     NBodyBounds *bounds = nullptr;
 };
 // Builds the tree over the n particles of P on `stream` (the level sorts use `sort`, which
-// must hold n entries).
-void launch_nbody_build(const NBodyTreeHost &t, const DevParticles &P, int n, SortScratch &sort,
+// must hold n entries); exact: centers of mass folded in insertion order (reference order).
+void launch_nbody_build(const NBodyTreeHost &t, const DevParticles &P, int n, SortScratch &sort, bool exact,
                         cudaStream_t stream);
 // The kernels launch_nbody_build launches for n particles.
 inline int nbody_build_kernels(int depth, int n) {

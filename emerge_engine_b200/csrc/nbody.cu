@@ -18,14 +18,17 @@
 //               level-d node is one run with its bodies in insertion order; particles
 //               without mass sort behind every body.  The run boundaries give each slot's
 //               range;
-//   4. centers  each node's total mass and center of mass, folded over its run in its
-//               level's order with the reference's operations, one thread per node.  A
+//   4. centers  each node's total mass and center of mass, one warp per node: in the
+//               reference-order mode folded over its run in its level's order with the
+//               reference's operations; in the fast pipeline as the lanes' sums Σm x / Σm.  A
 //               node that no particle can see as far (its width over the largest distance
 //               to any particle is at least theta) is never asked for its center and is not
 //               folded: typically the root and its four children, whose folds are longest.
-// Every fold and box center uses the reference's operations in the same order with IEEE
-// rounding, so the tree -- and the field's accelerations -- match the reference bit for bit
-// on both pipelines.
+// Every box center, and in the reference-order mode every fold, uses the reference's
+// operations in the same order with IEEE rounding, so the tree -- and the field's
+// accelerations -- match the reference bit for bit there; the fast pipeline's centers of mass
+// differ from the reference's in the last bits only (a serial fold of a large node costs one
+// dependent correctly rounded division per body).
 #include "device_state.cuh"
 #include "kernels.h"
 
@@ -178,17 +181,22 @@ __global__ void k_nb_level_ranges(const uint32_t *keys, const uint32_t *vals, in
     if (j + 1 == nb || keys[j + 1] != key) range[s].y = static_cast<uint32_t>(j + 1);
 }
 
-// Step 4.  com.w = 1 marks a folded node (an empty one included: it is never far).
+// Step 4.  One warp per node; com.w = 1 marks a folded node (an empty one included: it is
+// never far).  The fold is serial in insertion order; the warp's lanes load the next 32
+// bodies of the node's run together (and the 32 after them while these are folded), and
+// every lane runs the same fold on the values broadcast from the lane that loaded them.
 __global__ void k_nb_centers(const uint2 *range, const float4 *bdata, const uint32_t *order, size_t stride,
-                             const float4 *root, const NBodyBounds *b, int depth, float theta_max, float4 *com) {
-    const int s = blockIdx.x * blockDim.x + threadIdx.x;
-    if (s >= nbody_slots(depth)) return;
+                             const float4 *root, const NBodyBounds *b, int depth, float theta_max, int exact,
+                             float4 *com) {
+    const int s = static_cast<int>((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+    const int lane = threadIdx.x & 31;
+    if (s >= nbody_slots(depth)) return;  // warp-uniform
     int d = 0;
     while (s >= nbody_level_offset(d + 1)) ++d;
     const uint32_t pre = static_cast<uint32_t>(s - nbody_level_offset(d));
     const uint2 rg = range[s];
     if (rg.y <= rg.x) {
-        com[s] = make_float4(0.0f, 0.0f, 0.0f, 1.0f);
+        if (lane == 0) com[s] = make_float4(0.0f, 0.0f, 0.0f, 1.0f);
         return;
     }
     // the node's box, as the traversal computes it
@@ -209,27 +217,55 @@ __global__ void k_nb_centers(const uint2 *range, const float4 *bdata, const uint
         const double dx = fmax(fabs(ax - c.x), fabs(bx - c.x)), dy = fmax(fabs(ay - c.y), fabs(by - c.y));
         const double dmax = sqrt(dx * dx + dy * dy);
         if (dmax * static_cast<double>(theta_max) <= 2.0 * static_cast<double>(half) * (1.0 - 1e-4)) {
-            com[s] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+            if (lane == 0) com[s] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
             return;
         }
     }
     const uint32_t *ord = order + static_cast<size_t>(d) * stride;
+    if (!exact) {
+        // fast pipeline: the mass-weighted mean as sums over the lanes (Σm x / Σm), in the
+        // warp's order rather than the insertion order -- the same quantity, rounded
+        // differently, like the fast pipeline's P2G sums
+        float sm = 0.0f, sx = 0.0f, sy = 0.0f;
+        for (uint32_t j = rg.x + lane; j < rg.y; j += 32u) {
+            const float4 q = bdata[ord[j]];
+            sm += q.z;
+            sx = __fmaf_rn(q.z, q.x, sx);
+            sy = __fmaf_rn(q.z, q.y, sy);
+        }
+        for (int o = 16; o > 0; o >>= 1) {
+            sm += __shfl_xor_sync(0xffffffffu, sm, o);
+            sx += __shfl_xor_sync(0xffffffffu, sx, o);
+            sy += __shfl_xor_sync(0xffffffffu, sy, o);
+        }
+        if (lane == 0) com[s] = sm > 0.0f ? make_float4(__fdiv_rn(sx, sm), __fdiv_rn(sy, sm), sm, 1.0f)
+                                          : make_float4(0.0f, 0.0f, 0.0f, 1.0f);
+        return;
+    }
     float tm = 0.0f, cx = 0.0f, cy = 0.0f;
-    for (uint32_t j = rg.x; j < rg.y; ++j) {
-        const float4 q = bdata[ord[j]];
-        const float nt = __fadd_rn(tm, q.z);
-        if (nt > 0.0f) {
-            cx = __fdiv_rn(__fadd_rn(__fmul_rn(cx, tm), __fmul_rn(q.x, q.z)), nt);
-            cy = __fdiv_rn(__fadd_rn(__fmul_rn(cy, tm), __fmul_rn(q.y, q.z)), nt);
-            tm = nt;
+    float4 next = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    if (rg.x + lane < rg.y) next = bdata[ord[rg.x + lane]];
+    for (uint32_t j0 = rg.x; j0 < rg.y; j0 += 32u) {
+        const float4 q = next;
+        if (j0 + 32u + lane < rg.y) next = bdata[ord[j0 + 32u + lane]];
+        const int cnt = static_cast<int>(min(32u, rg.y - j0));
+        for (int k = 0; k < cnt; ++k) {
+            const float qx = __shfl_sync(0xffffffffu, q.x, k), qy = __shfl_sync(0xffffffffu, q.y, k);
+            const float qm = __shfl_sync(0xffffffffu, q.z, k);
+            const float nt = __fadd_rn(tm, qm);
+            if (nt > 0.0f) {
+                cx = __fdiv_rn(__fadd_rn(__fmul_rn(cx, tm), __fmul_rn(qx, qm)), nt);
+                cy = __fdiv_rn(__fadd_rn(__fmul_rn(cy, tm), __fmul_rn(qy, qm)), nt);
+                tm = nt;
+            }
         }
     }
-    com[s] = make_float4(cx, cy, tm, 1.0f);
+    if (lane == 0) com[s] = make_float4(cx, cy, tm, 1.0f);
 }
 
 }  // namespace
 
-void launch_nbody_build(const NBodyTreeHost &t, const DevParticles &P, int n, SortScratch &sort,
+void launch_nbody_build(const NBodyTreeHost &t, const DevParticles &P, int n, SortScratch &sort, bool exact,
                         cudaStream_t stream) {
     const int slots = nbody_slots(t.depth);
     const int gb = n > 0 ? (n + NB_THREADS - 1) / NB_THREADS : 1;
@@ -244,8 +280,9 @@ void launch_nbody_build(const NBodyTreeHost &t, const DevParticles &P, int n, So
         k_nb_level_ranges<<<gb, NB_THREADS, 0, stream>>>(sort.keys[r], sort.vals[r], n, t.bounds, d,
                                                          t.order + static_cast<size_t>(d) * t.stride, t.range);
     }
-    k_nb_centers<<<(slots + NB_THREADS - 1) / NB_THREADS, NB_THREADS, 0, stream>>>(
-        t.range, t.bdata, t.order, t.stride, t.root, t.bounds, t.depth, t.theta_max, t.com);
+    const long long threads = static_cast<long long>(slots) * 32;  // one warp per node
+    k_nb_centers<<<static_cast<int>((threads + NB_THREADS - 1) / NB_THREADS), NB_THREADS, 0, stream>>>(
+        t.range, t.bdata, t.order, t.stride, t.root, t.bounds, t.depth, t.theta_max, exact ? 1 : 0, t.com);
 }
 
 }  // namespace emerge

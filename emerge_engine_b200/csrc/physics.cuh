@@ -1146,21 +1146,33 @@ EM_HD float2 nbody_pull(float2 r, float m, float g, float eps2) {
 }
 
 // NBodyGravityField::acceleration (n_body.rs:178-208, 347-360) of the particle with reference
-// index `self` at `pos`: the reference's recursion walked depth first with an explicit
-// stack, each node's children summed into their own accumulator in quadrant order so that
-// every addition is the reference's.  A node is far when the particle is at least the
-// softening length from its box center, it holds mass, and its width over that distance is
-// below theta; far nodes pull with their center of mass, leaves with each body but the
-// particle itself and those closer than the softening length.
+// index `self` at `pos`.  A node is far when the particle is at least the softening length
+// from its box center, it holds mass, and its width over that distance is below theta; far
+// nodes pull with their center of mass, leaves with each body but the particle itself and
+// those closer than the softening length, and an internal node sums its four children in
+// quadrant order (the reference's recursion).
+//
+// The lanes that call it together walk the tree together, depth first: the warp opens a node
+// when any lane needs it opened, so neighbouring particles (tile-sorted) share one walk and a
+// leaf's bodies are read once for all of them.  Each lane keeps the reference's arithmetic:
+// a lane that stops at a node (far for it, or a leaf) adds that node's value to its parent's
+// accumulator at once -- where its own recursion would -- and sits out the node's subtree
+// (`skip`); a lane that opens a node accumulates its children into the node's own level and
+// adds the total when the walk leaves the node.  So every lane makes the additions of its
+// own recursion, in the same order, whatever its neighbours need.
 __device__ __forceinline__ float2 nbody_acceleration(const NBodyView &nb, const emerge_force_field &f, float2 pos,
                                                      uint32_t self) {
     const float g = f.params[0], soft = f.params[1], theta = f.params[2];
     const float eps2 = soft * soft;
     if (!nb.bdata) return v2(0.0f, 0.0f);
+    const unsigned mask = __activemask();
     const float4 rt = nb.root[0];
     float2 ctr[NBODY_MAX_DEPTH + 1];
     float2 acc[NBODY_MAX_DEPTH + 1];
-    int d = 0;
+    float2 result = v2(0.0f, 0.0f);
+    uint32_t opened = 0u;  // bit d: this lane opened the path's node at depth d
+    int skip = -1;         // depth of the node whose subtree this lane sits out (-1: none)
+    int d = 0;             // the walk's position (the same in every lane)
     uint32_t pre = 0u;
     float2 c = v2(rt.x, rt.y);
     float half = rt.z;
@@ -1168,40 +1180,60 @@ __device__ __forceinline__ float2 nbody_acceleration(const NBodyView &nb, const 
         // first visit of node (d, pre): box center c, half size `half`
         const int slot = nbody_level_offset(d) + static_cast<int>(pre);
         const uint2 rg = nb.range[slot];
-        float2 r;
-        const float dist = evlen(vsub(pos, c));
-        bool far = false;
-        if (!(dist < soft) && rg.y > rg.x) far = ediv(half * 2.0f, dist) < theta;
-        if (far) {
-            const float4 cm = nb.com[slot];
-            if (cm.w == 0.0f) atomicOr(nb.error, 4u);  // ERR_NBODY_SKIPPED (device_state.cuh)
-            r = nbody_pull(vsub(v2(cm.x, cm.y), pos), cm.z, g, eps2);
-        } else if (d >= nb.depth || rg.y - rg.x <= static_cast<uint32_t>(nb.max_bodies)) {
-            r = v2(0.0f, 0.0f);
-            const uint32_t *ord = nb.order + static_cast<size_t>(d) * nb.stride;
-            for (uint32_t j = rg.x; j < rg.y; ++j) {
-                const float4 b = nb.bdata[ord[j]];
-                if (__float_as_uint(b.w) == self) continue;
-                const float2 rv = vsub(v2(b.x, b.y), pos);
-                if (vdot(rv, rv) < eps2) continue;
-                r = vadd(r, nbody_pull(rv, b.z, g, eps2));
+        const bool leaf = d >= nb.depth || rg.y - rg.x <= static_cast<uint32_t>(nb.max_bodies);
+        const bool part = skip < 0;
+        bool need_open = false;
+        if (part) {
+            const float dist = evlen(vsub(pos, c));
+            bool far = false;
+            if (!(dist < soft) && rg.y > rg.x) far = ediv(half * 2.0f, dist) < theta;
+            float2 r = v2(0.0f, 0.0f);
+            if (far) {
+                const float4 cm = nb.com[slot];
+                if (cm.w == 0.0f) atomicOr(nb.error, 4u);  // ERR_NBODY_SKIPPED (device_state.cuh)
+                r = nbody_pull(vsub(v2(cm.x, cm.y), pos), cm.z, g, eps2);
+            } else if (leaf) {
+                const uint32_t *ord = nb.order + static_cast<size_t>(d) * nb.stride;
+                for (uint32_t j = rg.x; j < rg.y; ++j) {
+                    const float4 bd = nb.bdata[ord[j]];
+                    if (__float_as_uint(bd.w) == self) continue;
+                    const float2 rv = vsub(v2(bd.x, bd.y), pos);
+                    if (vdot(rv, rv) < eps2) continue;
+                    r = vadd(r, nbody_pull(rv, bd.z, g, eps2));
+                }
+            } else {
+                need_open = true;
             }
-        } else {  // internal: descend into quadrant 0 (left, top)
+            if (!need_open) {  // this lane's value of the node: to its parent now
+                if (d == 0) result = r;
+                else acc[d - 1] = vadd(acc[d - 1], r);
+            }
+        }
+        if (__any_sync(mask, need_open)) {  // the walk descends into quadrant 0 (left, top)
+            if (part && !need_open) skip = d;
+            if (need_open) {
+                acc[d] = v2(0.0f, 0.0f);
+                opened |= 1u << d;
+            }
             ctr[d] = c;
-            acc[d] = v2(0.0f, 0.0f);
             half *= 0.5f;
             c = v2(c.x - half, c.y + half);
             ++d;
             pre <<= 2;
             continue;
         }
-        // return r to the parent; move to the next sibling, or finish the parent
+        // the walk leaves node (d, pre): finish it, move to its next sibling or leave its parent
         for (;;) {
-            if (d == 0) return r;
+            if (opened & (1u << d)) {  // this lane opened it: its children's total goes up
+                opened &= ~(1u << d);
+                if (d == 0) result = acc[0];
+                else acc[d - 1] = vadd(acc[d - 1], acc[d]);
+            }
+            if (skip == d) skip = -1;
+            if (d == 0) return result;
             const uint32_t q = pre & 3u;
             pre >>= 2;
             --d;
-            acc[d] = vadd(acc[d], r);
             if (q < 3u) {
                 const uint32_t nq = q + 1u;
                 const float quarter = half;  // the children's half size
@@ -1211,7 +1243,6 @@ __device__ __forceinline__ float2 nbody_acceleration(const NBodyView &nb, const 
                 pre = (pre << 2) | nq;
                 break;
             }
-            r = acc[d];
             half *= 2.0f;
         }
     }

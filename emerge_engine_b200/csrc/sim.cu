@@ -517,7 +517,7 @@ void launch_particle_pass_fields(emerge_sim *s, const StepLaunch &L, int project
         return;
     }
     launch_particle_pass(L, s->lf, 1, project_in, 0, 1);
-    launch_nbody_build(s->nb, L.P, L.n, s->sort, L.stream);
+    launch_nbody_build(s->nb, L.P, L.n, s->sort, det_pipeline(s), L.stream);
     launch_particle_pass(L, s->lf, 0, 0, emit_p2g, 2);
 }
 
@@ -1547,7 +1547,7 @@ emerge_status emerge_cuda_field_accelerations(emerge_sim *s, float *out, uint64_
     emerge_status st = nbody_prepare(s);
     if (st != EMERGE_OK) return st;
     StepLaunch L = make_launch(s);
-    if (nbody_live(s)) launch_nbody_build(s->nb, L.P, L.n, s->sort, s->stream);
+    if (nbody_live(s)) launch_nbody_build(s->nb, L.P, L.n, s->sort, det_pipeline(s), s->stream);
     float2 *d_out = nullptr;
     CK(cudaMalloc(&d_out, n * sizeof(float2)));
     launch_field_accelerations(L, s->lf, d_out);

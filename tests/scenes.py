@@ -361,15 +361,16 @@ def nbody_field(G=20.0, softening=1.0, theta=0.5, max_depth=8, max_bodies=4):
 
 
 def nbody_scene(sim_cls, grid_res=128, seed=13, dt=0.05, G=20.0, softening=1.0, theta=0.5,
-                max_depth=8, max_bodies=4, pinned_every=0, **sim_kw):
-    """Self-gravitating clumps: three NeoHookean (400, 200) blocks at 4 ppc with seeded jitter
-    and initial velocities in a grid_res^2 grid without gravity, pulled together by
-    NBodyGravityField(G, softening, theta) (tree shape max_depth, max_bodies); every
-    pinned_every-th particle pinned (0: none)."""
+                max_depth=8, max_bodies=4, pinned_every=0, scale=1, **sim_kw):
+    """Self-gravitating clumps: three NeoHookean (400, 200) blocks (sides 18, 14, 10 cells,
+    times `scale`) at 4 ppc with seeded jitter and initial velocities in a grid_res^2 grid
+    without gravity, pulled together by NBodyGravityField(G, softening, theta) (tree shape
+    max_depth, max_bodies); every pinned_every-th particle pinned (0: none)."""
     cfg = SimConfig.standard(grid_res, dt, (0.0, 0.0))
     sim = sim_cls.empty(cfg, **sim_kw).with_default_material(NeoHookeanMaterial.new(400.0, 200.0))
     for k, (cx, cy, side) in enumerate(((0.3, 0.4, 18), (0.68, 0.55, 14), (0.5, 0.75, 10))):
         s = SpawnRegion.for_sim(cfg)
+        side = side * scale
         s.spacing, s.box_size, s.box_center = 0.5, (side, side), (grid_res * cx, grid_res * cy)
         s.position_jitter, s.rng_seed, s.initial_velocity_scale = 0.3, seed + k, 1.0
         sim.add_body(s)

@@ -106,17 +106,36 @@ def _with_points(cls, p, field):
     return sim
 
 
+def assert_fast_nbody_close(got, want):
+    """The fast pipeline's centers of mass are lane sums (sum m x / sum m), not the
+    reference's body-by-body fold: the same tree, the same open/far decisions (they depend on
+    box centers only), centers of mass that differ by the two summations' rounding (a
+    node's fold over ~10^4 bodies rounds by ~1e-4 of a cell itself).  Far pulls largely
+    cancel in an even distribution, so the bar is on the field's scale: every particle within
+    2e-4 of the RMS |a| (the Barnes-Hut approximation itself is ~4e-3 at the median)."""
+    got, want = got.astype(np.float64), want.astype(np.float64)
+    mag = np.linalg.norm(want, axis=1)
+    rms = np.sqrt((mag ** 2).mean()) if mag.size else 0.0
+    err = np.linalg.norm(got - want, axis=1)
+    assert np.all(err <= 2e-4 * rms), (err.max(), rms)
+    return float(err.max() / rms) if rms > 0 else 0.0
+
+
 @pytest.mark.parametrize("cls", [Simulation, DeterministicSimulation])
 @pytest.mark.parametrize("layout,n,g,soft,theta,depth,maxb", NBODY_CASES)
-def test_nbody_accelerations_match_the_oracle_bit_for_bit(cuda_lib, cls, layout, n, g, soft, theta, depth, maxb):
-    """The device tree (built from sorted quadrant paths, centers of mass folded in insertion
-    order) and its stack traversal against the oracle's one-at-a-time insertion and
-    recursion: identical bits on both pipelines, for any tree shape."""
+def test_nbody_accelerations_match_the_oracle(cuda_lib, cls, layout, n, g, soft, theta, depth, maxb):
+    """The device tree (built from sorted quadrant paths) and its traversal against the
+    oracle's one-at-a-time insertion and recursion, for any tree shape: in the reference-order
+    mode (centers of mass folded in insertion order) identical bits; on the fast pipeline
+    within its bar."""
     p = scenes.nbody_points(n, seed=n + depth, layout=layout)
     field = scenes.nbody_field(g, soft, theta, depth, maxb)
     got = _with_points(cls, p, field).field_accelerations()
     want = _with_points(OracleSimulation, p, field).field_accelerations()
-    np.testing.assert_array_equal(got.view(np.uint32), want.view(np.uint32))
+    if cls is DeterministicSimulation:
+        np.testing.assert_array_equal(got.view(np.uint32), want.view(np.uint32))
+    else:
+        print("nbody fast accelerations", layout, n, "max error / RMS |a|", assert_fast_nbody_close(got, want))
 
 
 def test_nbody_with_other_fields_in_order(cuda_lib):
@@ -124,12 +143,13 @@ def test_nbody_with_other_fields_in_order(cuda_lib):
     p = scenes.nbody_points(10_000, seed=2, layout="blobs")
     p["v"] = np.float32(0.5)
     out = []
-    for cls in (Simulation, OracleSimulation):
+    for cls in (DeterministicSimulation, Simulation, OracleSimulation):
         sim = _with_points(cls, p, RadialConfinementField.new((64.0, 64.0), 30.0, 0.3))
         sim.add_force_field(scenes.nbody_field(G=8.0))
         sim.add_force_field(LinearDragField.new((1.0, 0.0), 0.4, LinearDragField.ALL_MATERIALS))
         out.append(sim.field_accelerations())
-    np.testing.assert_array_equal(out[0].view(np.uint32), out[1].view(np.uint32))
+    np.testing.assert_array_equal(out[0].view(np.uint32), out[2].view(np.uint32))
+    assert_fast_nbody_close(out[1], out[2])
 
 
 def test_nbody_parameters_are_checked(cuda_lib):
