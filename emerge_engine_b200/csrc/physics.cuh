@@ -983,6 +983,7 @@ struct NBodyView {
     const uint2 *range;    // per tree slot: [first, end) into its level's order
     const float4 *com;     // per tree slot: center of mass x, y, total mass; w = 1 if computed
     uint32_t *error;       // StepState::error_flags (a far node without its center of mass)
+    int fast;              // pulls by the approximate reciprocal square root (fast pipeline)
 };
 
 __host__ __device__ __forceinline__ int nbody_level_offset(int d) { return ((1 << (2 * d)) - 1) / 3; }
@@ -1145,6 +1146,16 @@ EM_HD float2 nbody_pull(float2 r, float m, float g, float eps2) {
     return isfinite(scale) ? vmuls(r, scale) : v2(0.0f, 0.0f);
 }
 
+// The same pull on the fast pipeline: g m / ns^1.5 as g m (1/sqrt ns)^3 with the hardware's
+// approximate reciprocal square root (a few ulp, where the division and square root above
+// are correctly rounded); ns = 0 gives an infinite scale and no pull, as above.
+__device__ __forceinline__ float2 nbody_pull_fast(float2 r, float m, float g, float eps2) {
+    const float ns = vdot(r, r) + eps2;
+    const float inv = rsqrtf(ns);
+    const float scale = (g * m) * (inv * inv * inv);
+    return isfinite(scale) ? vmuls(r, scale) : v2(0.0f, 0.0f);
+}
+
 // NBodyGravityField::acceleration (n_body.rs:178-208, 347-360) of the particle with reference
 // index `self` at `pos`.  A node is far when the particle is at least the softening length
 // from its box center, it holds mass, and its width over that distance is below theta; far
@@ -1191,7 +1202,8 @@ __device__ __forceinline__ float2 nbody_acceleration(const NBodyView &nb, const 
             if (far) {
                 const float4 cm = nb.com[slot];
                 if (cm.w == 0.0f) atomicOr(nb.error, 4u);  // ERR_NBODY_SKIPPED (device_state.cuh)
-                r = nbody_pull(vsub(v2(cm.x, cm.y), pos), cm.z, g, eps2);
+                const float2 rv = vsub(v2(cm.x, cm.y), pos);
+                r = nb.fast ? nbody_pull_fast(rv, cm.z, g, eps2) : nbody_pull(rv, cm.z, g, eps2);
             } else if (leaf) {
                 const uint32_t *ord = nb.order + static_cast<size_t>(d) * nb.stride;
                 for (uint32_t j = rg.x; j < rg.y; ++j) {
@@ -1199,7 +1211,7 @@ __device__ __forceinline__ float2 nbody_acceleration(const NBodyView &nb, const 
                     if (__float_as_uint(bd.w) == self) continue;
                     const float2 rv = vsub(v2(bd.x, bd.y), pos);
                     if (vdot(rv, rv) < eps2) continue;
-                    r = vadd(r, nbody_pull(rv, bd.z, g, eps2));
+                    r = vadd(r, nb.fast ? nbody_pull_fast(rv, bd.z, g, eps2) : nbody_pull(rv, bd.z, g, eps2));
                 }
             } else {
                 need_open = true;

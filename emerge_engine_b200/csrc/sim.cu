@@ -361,6 +361,7 @@ void refresh_dev_config(emerge_sim *s) {
         s->dcfg.nbody.range = s->nb.range;
         s->dcfg.nbody.com = s->nb.com;
         s->dcfg.nbody.error = &s->d_state->error_flags;
+        s->dcfg.nbody.fast = det_pipeline(s) ? 0 : 1;
     }
     s->dcfg.n_fields = s->n_fields;
     s->dcfg.fields = s->n_fields ? static_cast<const emerge_force_field *>(s->fbuf.ptr) : nullptr;
