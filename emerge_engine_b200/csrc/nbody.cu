@@ -18,17 +18,20 @@
 //               level-d node is one run with its bodies in insertion order; particles
 //               without mass sort behind every body.  The run boundaries give each slot's
 //               range;
-//   4. centers  each node's total mass and center of mass, one warp per node: in the
-//               reference-order mode folded over its run in its level's order with the
-//               reference's operations; in the fast pipeline as the lanes' sums Σm x / Σm.  A
-//               node that no particle can see as far (its width over the largest distance
-//               to any particle is at least theta) is never asked for its center and is not
+//   4. centers  each node's total mass and center of mass, one warp per node, folded over
+//               its run in its level's order with the reference's operations.  A node that
+//               no particle can see as far (its width over the largest distance to any
+//               particle is at least theta) is never asked for its center and is not
 //               folded: typically the root and its four children, whose folds are longest.
-// Every box center, and in the reference-order mode every fold, uses the reference's
-// operations in the same order with IEEE rounding, so the tree -- and the field's
-// accelerations -- match the reference bit for bit there; the fast pipeline's centers of mass
-// differ from the reference's in the last bits only (a serial fold of a large node costs one
-// dependent correctly rounded division per body).
+// The fast pipeline needs neither the insertion order nor the serial folds: it sorts once by
+// the full path (every node is then one run of that single order at every level), the
+// deepest level's nodes sum Σm, Σm x and Σm y over their bodies (a warp each), and every
+// node above adds its four children's sums (one launch per level of more than 256 nodes,
+// one CTA for the rest), so no chain is longer than a node's four children.
+// In the reference-order mode every box center and fold uses the reference's operations in
+// the same order with IEEE rounding, so the tree -- and the field's accelerations -- match
+// the reference bit for bit; the fast pipeline's tree has the same nodes, ranges and box
+// centers, and centers of mass that differ from the reference's in the last bits only.
 #include "device_state.cuh"
 #include "kernels.h"
 
@@ -186,8 +189,7 @@ __global__ void k_nb_level_ranges(const uint32_t *keys, const uint32_t *vals, in
 // bodies of the node's run together (and the 32 after them while these are folded), and
 // every lane runs the same fold on the values broadcast from the lane that loaded them.
 __global__ void k_nb_centers(const uint2 *range, const float4 *bdata, const uint32_t *order, size_t stride,
-                             const float4 *root, const NBodyBounds *b, int depth, float theta_max, int exact,
-                             float4 *com) {
+                             const float4 *root, const NBodyBounds *b, int depth, float theta_max, float4 *com) {
     const int s = static_cast<int>((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
     const int lane = threadIdx.x & 31;
     if (s >= nbody_slots(depth)) return;  // warp-uniform
@@ -222,26 +224,6 @@ __global__ void k_nb_centers(const uint2 *range, const float4 *bdata, const uint
         }
     }
     const uint32_t *ord = order + static_cast<size_t>(d) * stride;
-    if (!exact) {
-        // fast pipeline: the mass-weighted mean as sums over the lanes (Σm x / Σm), in the
-        // warp's order rather than the insertion order -- the same quantity, rounded
-        // differently, like the fast pipeline's P2G sums
-        float sm = 0.0f, sx = 0.0f, sy = 0.0f;
-        for (uint32_t j = rg.x + lane; j < rg.y; j += 32u) {
-            const float4 q = bdata[ord[j]];
-            sm += q.z;
-            sx = __fmaf_rn(q.z, q.x, sx);
-            sy = __fmaf_rn(q.z, q.y, sy);
-        }
-        for (int o = 16; o > 0; o >>= 1) {
-            sm += __shfl_xor_sync(0xffffffffu, sm, o);
-            sx += __shfl_xor_sync(0xffffffffu, sx, o);
-            sy += __shfl_xor_sync(0xffffffffu, sy, o);
-        }
-        if (lane == 0) com[s] = sm > 0.0f ? make_float4(__fdiv_rn(sx, sm), __fdiv_rn(sy, sm), sm, 1.0f)
-                                          : make_float4(0.0f, 0.0f, 0.0f, 1.0f);
-        return;
-    }
     float tm = 0.0f, cx = 0.0f, cy = 0.0f;
     float4 next = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
     if (rg.x + lane < rg.y) next = bdata[ord[rg.x + lane]];
@@ -263,6 +245,83 @@ __global__ void k_nb_centers(const uint2 *range, const float4 *bdata, const uint
     if (lane == 0) com[s] = make_float4(cx, cy, tm, 1.0f);
 }
 
+// Fast pipeline, step 3: the ranges of every level from one sort by the full path (a
+// level-d node's bodies are one run of that order at every level, in path order rather than
+// insertion order).  `order` is shared by all levels.
+__global__ void k_nb_ranges_all(const uint32_t *keys, const uint32_t *vals, int n, const NBodyBounds *b, int depth,
+                                uint32_t *order, uint2 *range) {
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    const int nb = static_cast<int>(b->n_bodies);
+    if (j >= nb || j >= n) return;
+    const uint32_t key = keys[j], v = vals[j];
+    const bool ok = (key >> (2 * depth)) == 0u && v < static_cast<uint32_t>(n);  // a body's key
+    order[j] = ok ? v : 0u;
+    if (!ok) return;
+    const uint32_t kp = j > 0 ? keys[j - 1] : 0xffffffffu, kn = j + 1 < nb ? keys[j + 1] : 0xffffffffu;
+    for (int d = 0; d <= depth; ++d) {
+        const int sh = 2 * (depth - d);
+        const uint32_t kd = key >> sh;
+        const int s = nbody_level_offset(d) + static_cast<int>(kd);
+        if (j == 0 || (kp >> sh) != kd) range[s].x = static_cast<uint32_t>(j);
+        if (j + 1 == nb || (kn >> sh) != kd) range[s].y = static_cast<uint32_t>(j + 1);
+    }
+}
+
+// Fast pipeline, step 4, bottom up.  The deepest level's nodes (one warp each) sum their
+// bodies' m, m x and m y into com as raw sums {Σm x, Σm y, Σm, 1}.
+__global__ void k_nb_sums_leaf(const uint2 *range, const float4 *bdata, const uint32_t *order, int depth,
+                               float4 *com) {
+    const long long wid = (static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    const int count = 1 << (2 * depth);
+    if (wid >= count) return;  // warp-uniform
+    const int s = nbody_level_offset(depth) + static_cast<int>(wid);
+    const uint2 rg = range[s];
+    float sm = 0.0f, sx = 0.0f, sy = 0.0f;
+    for (uint32_t j = rg.x + lane; j < rg.y; j += 32u) {
+        const float4 q = bdata[order[j]];
+        sm += q.z;
+        sx = __fmaf_rn(q.z, q.x, sx);
+        sy = __fmaf_rn(q.z, q.y, sy);
+    }
+    if (rg.y - rg.x > 1u)
+        for (int o = 16; o > 0; o >>= 1) {
+            sm += __shfl_xor_sync(0xffffffffu, sm, o);
+            sx += __shfl_xor_sync(0xffffffffu, sx, o);
+            sy += __shfl_xor_sync(0xffffffffu, sy, o);
+        }
+    if (lane == 0) com[s] = make_float4(sx, sy, sm, 1.0f);
+}
+
+__device__ __forceinline__ float4 nb_finish(float4 r) {
+    return r.z > 0.0f ? make_float4(__fdiv_rn(r.x, r.z), __fdiv_rn(r.y, r.z), r.z, 1.0f)
+                      : make_float4(0.0f, 0.0f, 0.0f, 1.0f);
+}
+
+// Levels d_from down to d_to: each node sums its four children's raw sums and turns the
+// children's into their centers of mass (it is their only reader).  A launch covering more
+// than one level is a single CTA (the barrier orders the levels); finish_root finishes slot 0.
+__global__ void k_nb_sums_up(float4 *com, int d_from, int d_to, int finish_root) {
+    for (int d = d_from; d >= d_to; --d) {
+        const int count = 1 << (2 * d), base = nbody_level_offset(d), cbase = nbody_level_offset(d + 1);
+        for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < count; p += gridDim.x * blockDim.x) {
+            float4 t = make_float4(0.0f, 0.0f, 0.0f, 1.0f);
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const int cs = cbase + 4 * p + q;
+                const float4 c = com[cs];
+                t.x += c.x;
+                t.y += c.y;
+                t.z += c.z;
+                com[cs] = nb_finish(c);
+            }
+            com[base + p] = t;
+        }
+        __syncthreads();
+    }
+    if (finish_root && blockIdx.x == 0 && threadIdx.x == 0) com[0] = nb_finish(com[0]);
+}
+
 }  // namespace
 
 void launch_nbody_build(const NBodyTreeHost &t, const DevParticles &P, int n, SortScratch &sort, bool exact,
@@ -274,6 +333,21 @@ void launch_nbody_build(const NBodyTreeHost &t, const DevParticles &P, int n, So
     k_nb_paths<<<gb, NB_THREADS, 0, stream>>>(P.x, P.mass, P.slot_to_index, n, t.bounds, t.depth, t.root, t.bdata,
                                               t.path);
     cudaMemsetAsync(t.range, 0, static_cast<size_t>(slots) * sizeof(uint2), stream);
+    if (!exact) {
+        // one sort by the full path; every node's center of mass from its children's sums
+        k_nb_level_keys<<<gb, NB_THREADS, 0, stream>>>(t.path, n, t.depth, t.depth, sort.keys[0], sort.vals[0]);
+        const int r = radix_sort_pairs(sort, n, 2 * t.depth + 1, stream);
+        k_nb_ranges_all<<<gb, NB_THREADS, 0, stream>>>(sort.keys[r], sort.vals[r], n, t.bounds, t.depth, t.order,
+                                                       t.range);
+        const long long lthreads = (1ll << (2 * t.depth)) * 32;  // one warp per deepest node
+        k_nb_sums_leaf<<<static_cast<int>((lthreads + NB_THREADS - 1) / NB_THREADS), NB_THREADS, 0, stream>>>(
+            t.range, t.bdata, t.order, t.depth, t.com);
+        int d = t.depth - 1;
+        for (; d >= 0 && (1 << (2 * d)) > NB_THREADS; --d)  // one launch per wide level
+            k_nb_sums_up<<<((1 << (2 * d)) + NB_THREADS - 1) / NB_THREADS, NB_THREADS, 0, stream>>>(t.com, d, d, 0);
+        k_nb_sums_up<<<1, NB_THREADS, 0, stream>>>(t.com, d, 0, 1);  // the narrow levels and the root
+        return;
+    }
     for (int d = 0; d <= t.depth; ++d) {
         k_nb_level_keys<<<gb, NB_THREADS, 0, stream>>>(t.path, n, t.depth, d, sort.keys[0], sort.vals[0]);
         const int r = radix_sort_pairs(sort, n, 2 * d + 1, stream);
@@ -282,7 +356,7 @@ void launch_nbody_build(const NBodyTreeHost &t, const DevParticles &P, int n, So
     }
     const long long threads = static_cast<long long>(slots) * 32;  // one warp per node
     k_nb_centers<<<static_cast<int>((threads + NB_THREADS - 1) / NB_THREADS), NB_THREADS, 0, stream>>>(
-        t.range, t.bdata, t.order, t.stride, t.root, t.bounds, t.depth, t.theta_max, exact ? 1 : 0, t.com);
+        t.range, t.bdata, t.order, t.stride, t.root, t.bounds, t.depth, t.theta_max, t.com);
 }
 
 }  // namespace emerge

@@ -357,7 +357,8 @@ void refresh_dev_config(emerge_sim *s) {
         s->dcfg.nbody.root = s->nb.root;
         s->dcfg.nbody.bdata = s->nb.bdata;
         s->dcfg.nbody.order = s->nb.order;
-        s->dcfg.nbody.stride = s->nb.stride;
+        // the fast pipeline's build leaves one body order for all levels
+        s->dcfg.nbody.stride = det_pipeline(s) ? s->nb.stride : 0;
         s->dcfg.nbody.range = s->nb.range;
         s->dcfg.nbody.com = s->nb.com;
         s->dcfg.nbody.error = &s->d_state->error_flags;
