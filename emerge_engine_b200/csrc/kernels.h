@@ -36,6 +36,7 @@ struct NBodyBounds {
     uint32_t lo[2], hi[2];          // order-preserving bits of the bodies' min / max x, y
     uint32_t all_lo[2], all_hi[2];  // ... of every particle's position
     uint32_t n_bodies;              // particles of positive mass
+    uint32_t walk_next;             // k_nb_walk's next particle
 };
 struct NBodyTreeHost {
     int depth = -1;          // max_depth; -1: no NBodyGravityField
@@ -49,13 +50,27 @@ struct NBodyTreeHost {
     uint2 *range = nullptr;
     float4 *com = nullptr;
     NBodyBounds *bounds = nullptr;
+    int n_fields = 0;            // NBody fields (one walk and one accel block each)
+    float2 *accel = nullptr;     // n_fields blocks of `stride` float2 (per particle slot)
+    int walk_ctas = 0;           // resident CTAs of k_nb_walk on the device (its grid)
 };
 // Builds the tree over the n particles of P on `stream` (the level sorts use `sort`, which
 // must hold n entries); exact: centers of mass folded in insertion order (reference order).
 void launch_nbody_build(const NBodyTreeHost &t, const DevParticles &P, int n, SortScratch &sort, bool exact,
                         cudaStream_t stream);
+// Every particle's acceleration from each NBody field of `cfg` (the tree built), into
+// t.accel; particles outside the sleep partition's active zone are skipped unless
+// all_particles.
+void launch_nbody_walk(const NBodyTreeHost &t, const DevConfig &cfg, const DevParticles &P, int n,
+                       bool all_particles, cudaStream_t stream);
+// Resident CTAs of the walk kernel on the current device (queried outside graph capture).
+int nbody_walk_ctas();
 // The kernels launch_nbody_build launches for n particles.
-inline int nbody_build_kernels(int depth, int n) {
+inline int nbody_build_kernels(int depth, int n, bool exact) {
+    if (!exact) {  // reset, bounds, paths, keys, one sort, ranges, leaf sums, the levels above
+        const int wide = depth - 5 > 0 ? depth - 5 : 0;
+        return 6 + (n > 1 ? 5 * ((2 * depth + 1 + 7) / 8) : 0) + 1 + wide + 1;
+    }
     int k = 4;  // reset, bounds, paths, centers
     for (int d = 0; d <= depth; ++d) k += 2 + (n > 1 ? 5 * ((2 * d + 1 + 7) / 8) : 0);
     return k;

@@ -32,6 +32,8 @@
 // the same order with IEEE rounding, so the tree -- and the field's accelerations -- match
 // the reference bit for bit; the fast pipeline's tree has the same nodes, ranges and box
 // centers, and centers of mass that differ from the reference's in the last bits only.
+#include <algorithm>
+
 #include "device_state.cuh"
 #include "kernels.h"
 
@@ -71,6 +73,7 @@ __global__ void k_nb_reset(NBodyBounds *b) {
             b->all_hi[k] = 0u;
         }
         b->n_bodies = 0u;
+        b->walk_next = 0u;
     }
 }
 
@@ -322,7 +325,55 @@ __global__ void k_nb_sums_up(float4 *com, int d_from, int d_to, int finish_root)
     if (finish_root && blockIdx.x == 0 && threadIdx.x == 0) com[0] = nb_finish(com[0]);
 }
 
+// The tree walk of every particle (nbody_acceleration) at its stored position, one warp per
+// 32 consecutive particles (tile-sort neighbours, which share most of their walk), the warps
+// taking the next 32 from a counter as they finish: walks differ in length by orders of
+// magnitude between a clump's core and its outskirts, and a fixed grid would wait for its
+// slowest CTAs.
+__global__ void __launch_bounds__(NB_THREADS) k_nb_walk(NBodyView nb, const emerge_force_field *fields,
+                                                        int n_fields, const float2 *x,
+                                                        const uint32_t *slot_to_index, const uint32_t *sleeping,
+                                                        int zones, int n, NBodyBounds *b, float2 *accel) {
+    const int lane = threadIdx.x & 31;
+    for (;;) {
+        uint32_t base = 0u;
+        if (lane == 0) base = atomicAdd(&b->walk_next, 32u);
+        base = __shfl_sync(0xffffffffu, base, 0);
+        if (base >= static_cast<uint32_t>(n)) return;  // warp-uniform
+        const int i = static_cast<int>(base) + lane;
+        bool want = i < n;
+        if (want && zones) want = (sleeping[i] & ZB_OUT) == 0u;
+        if (want) {
+            const float2 pos = x[i];
+            const uint32_t self = slot_to_index[i];
+            int kn = 0;
+            for (int k = 0; k < n_fields; ++k) {
+                const emerge_force_field f = fields[k];
+                if (f.kind != EMERGE_FIELD_NBODY_GRAVITY) continue;
+                accel[static_cast<size_t>(kn) * nb.accel_stride + i] = nbody_acceleration(nb, f, pos, self);
+                ++kn;
+            }
+        }
+    }
+}
+
 }  // namespace
+
+int nbody_walk_ctas() {
+    int sms = 148, per_sm = 1, dev = 0;
+    if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_nb_walk, NB_THREADS, 0) != cudaSuccess) per_sm = 1;
+    return sms * std::max(per_sm, 1);
+}
+
+void launch_nbody_walk(const NBodyTreeHost &t, const DevConfig &cfg, const DevParticles &P, int n,
+                       bool all_particles, cudaStream_t stream) {
+    if (n <= 0) return;
+    const int warps = (n + 31) / 32;
+    const int grid = std::max(1, std::min((warps + NB_THREADS / 32 - 1) / (NB_THREADS / 32), std::max(t.walk_ctas, 1)));
+    k_nb_walk<<<grid, NB_THREADS, 0, stream>>>(cfg.nbody, cfg.fields, cfg.n_fields, P.x, P.slot_to_index,
+                                               P.sleeping, all_particles ? 0 : cfg.zones, n, t.bounds, t.accel);
+}
 
 void launch_nbody_build(const NBodyTreeHost &t, const DevParticles &P, int n, SortScratch &sort, bool exact,
                         cudaStream_t stream) {

@@ -1161,7 +1161,7 @@ __device__ __forceinline__ void particle_pass(const ParticleKernelArgs &a, int b
     if (valid) {
         if constexpr (HAS_MODEL(MASK, M_EXTRAS_BIT)) {
             if (a.split == 0 ? a.mode_g2p != 0 : a.split == 2) {
-                apply_force_fields(cfg, p, dt, cfg.nbody.bdata ? a.P.slot_to_index[i] : 0xFFFFFFFFu);
+                apply_force_fields(cfg, p, dt, i);
                 if (cfg.sleep_thr > 0.0f && (zb & ZB_FLAG) == 0u) {
                     const float act = a.lf.activation ? p.activation : a.P.activation[i];
                     asleep = act == 0.0f && vlen2(p.v) < cfg.sleep_thr * cfg.sleep_thr;

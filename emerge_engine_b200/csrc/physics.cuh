@@ -984,6 +984,9 @@ struct NBodyView {
     const float4 *com;     // per tree slot: center of mass x, y, total mass; w = 1 if computed
     uint32_t *error;       // StepState::error_flags (a far node without its center of mass)
     int fast;              // pulls by the approximate reciprocal square root (fast pipeline)
+    const float2 *accel;   // the walk's result per NBody field k and particle slot i, at
+                           // accel[k * accel_stride + i] (written before the fields half)
+    size_t accel_stride;
 };
 
 __host__ __device__ __forceinline__ int nbody_level_offset(int d) { return ((1 << (2 * d)) - 1) / 3; }
@@ -1156,6 +1159,27 @@ __device__ __forceinline__ float2 nbody_pull_fast(float2 r, float m, float g, fl
     return isfinite(scale) ? vmuls(r, scale) : v2(0.0f, 0.0f);
 }
 
+// The reference's far test of a node holding bodies (n_body.rs:184-187): with dist = |pos -
+// center| correctly rounded, the node is far when !(dist < softening) and (2 half) / dist,
+// correctly rounded, is below theta.  Both comparisons are first made from s = |pos -
+// center|^2 (the same rounded value the distance's square root takes) and the hardware's
+// approximate 1/sqrt(s), whose error (a few ulp, ~1e-6 at most) is far inside the 1e-5
+// relative margins below: outside the margins the outcome is certain, and the correctly
+// rounded square root and division run only inside them (or for non-finite inputs, whose
+// comparisons are all false).
+__device__ __forceinline__ bool nbody_far(float2 dv, float half, float soft, float theta) {
+    const float s = vdot(dv, dv);
+    const float s2 = soft * soft;
+    if (s < s2 * 0.99999f) return false;  // dist < soft for certain
+    const float q = (half * 2.0f) * rsqrtf(s);
+    if (s > s2 * 1.00001f) {              // dist >= soft for certain
+        if (q < theta * 0.99999f) return true;
+        if (q > theta * 1.00001f) return false;
+    }
+    const float dist = esqrt(s);
+    return !(dist < soft) && ediv(half * 2.0f, dist) < theta;
+}
+
 // NBodyGravityField::acceleration (n_body.rs:178-208, 347-360) of the particle with reference
 // index `self` at `pos`.  A node is far when the particle is at least the softening length
 // from its box center, it holds mass, and its width over that distance is below theta; far
@@ -1195,9 +1219,7 @@ __device__ __forceinline__ float2 nbody_acceleration(const NBodyView &nb, const 
         const bool part = skip < 0;
         bool need_open = false;
         if (part) {
-            const float dist = evlen(vsub(pos, c));
-            bool far = false;
-            if (!(dist < soft) && rg.y > rg.x) far = ediv(half * 2.0f, dist) < theta;
+            const bool far = rg.y > rg.x && nbody_far(vsub(pos, c), half, soft, theta);
             float2 r = v2(0.0f, 0.0f);
             if (far) {
                 const float4 cm = nb.com[slot];
@@ -1261,18 +1283,19 @@ __device__ __forceinline__ float2 nbody_acceleration(const NBodyView &nb, const 
 }
 
 // Sum of the force fields' accelerations at a particle, in application order (step.rs:
-// 232-236).  `self`: the particle's reference index (NBodyGravityField skips the particle's
-// own body).
-EM_HD float2 force_field_sum(const DevConfig &cfg, const PState &p, uint32_t self) {
+// 232-236).  `slot`: the particle's slot; an NBodyGravityField's value is the tree walk's
+// (k_nb_walk, run for every particle before this sum is formed).
+EM_HD float2 force_field_sum(const DevConfig &cfg, const PState &p, int slot) {
     float2 dv = v2(0.0f, 0.0f);
+    int kn = 0;  // NBody fields met so far
     for (int k = 0; k < cfg.n_fields; ++k) {
         const emerge_force_field &f = cfg.fields[k];
-#ifdef __CUDA_ARCH__
         if (f.kind == EMERGE_FIELD_NBODY_GRAVITY) {
-            dv = vadd(dv, nbody_acceleration(cfg.nbody, f, p.x, self));
+            if (cfg.nbody.accel)
+                dv = vadd(dv, cfg.nbody.accel[static_cast<size_t>(kn) * cfg.nbody.accel_stride + slot]);
+            ++kn;
             continue;
         }
-#endif
         dv = vadd(dv, field_acceleration(f, cfg.field_data, p));
     }
     return dv;
@@ -1280,9 +1303,9 @@ EM_HD float2 force_field_sum(const DevConfig &cfg, const PState &p, uint32_t sel
 
 // Force fields after G2P (step.rs:212-259): v += dt * sum of the accelerations, then the
 // G2P speed clamp again; pinned particles are skipped.
-EM_HD void apply_force_fields(const DevConfig &cfg, PState &p, float dt, uint32_t self = 0xFFFFFFFFu) {
+EM_HD void apply_force_fields(const DevConfig &cfg, PState &p, float dt, int slot) {
     if (cfg.n_fields <= 0 || p.pinned != 0) return;
-    const float2 dv = force_field_sum(cfg, p, self);
+    const float2 dv = force_field_sum(cfg, p, slot);
     p.v = vadd(p.v, svmul(dt, dv));
     const float vel_limit = cfg.cell / dt;
     const float spd = vlen(p.v);

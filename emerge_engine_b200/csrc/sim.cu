@@ -150,6 +150,7 @@ struct emerge_sim {
     NBodyTreeHost nb;        // NBodyGravityField's tree (nb.depth < 0: none)
     Buffer nbbuf;            // its arrays, sized for nb_cap particles and nb_alloc_depth
     size_t nb_cap = 0;
+    int nb_alloc_fields = 0;  // NBody fields the accel blocks were allocated for
     int nb_alloc_depth = -1;
 
     // sleep partition (solver/mod.rs:40-42): reference indices [0, active) are awake
@@ -363,6 +364,8 @@ void refresh_dev_config(emerge_sim *s) {
         s->dcfg.nbody.com = s->nb.com;
         s->dcfg.nbody.error = &s->d_state->error_flags;
         s->dcfg.nbody.fast = det_pipeline(s) ? 0 : 1;
+        s->dcfg.nbody.accel = s->nb.accel;
+        s->dcfg.nbody.accel_stride = s->nb.stride;
     }
     s->dcfg.n_fields = s->n_fields;
     s->dcfg.fields = s->n_fields ? static_cast<const emerge_force_field *>(s->fbuf.ptr) : nullptr;
@@ -504,15 +507,15 @@ bool nbody_live(const emerge_sim *s) {
 }
 
 // Kernels a substep's particle pass takes beyond the one pass: with an NBodyGravityField, the
-// tree build and the fields half.
+// tree build, the walk and the fields half.
 int nbody_extra_kernels(const emerge_sim *s) {
-    return nbody_live(s) ? nbody_build_kernels(s->nb.depth, static_cast<int>(s->n)) + 1 : 0;
+    return nbody_live(s) ? nbody_build_kernels(s->nb.depth, static_cast<int>(s->n), det_pipeline(s)) + 2 : 0;
 }
 
 // The particle pass of a substep (G2P of substep k, fields, CFL bound, and with emit_p2g the
 // projection and P2G of k + 1).  With an NBodyGravityField the fields need the tree of every
 // particle's post-G2P position (step.rs:221-226): the pass runs as its G2P half, the tree
-// build, and its fields half.
+// build, the walk (each particle's n-body acceleration) and its fields half.
 void launch_particle_pass_fields(emerge_sim *s, const StepLaunch &L, int project_in, int emit_p2g) {
     if (!nbody_live(s)) {
         launch_particle_pass(L, s->lf, 1, project_in, emit_p2g);
@@ -520,13 +523,16 @@ void launch_particle_pass_fields(emerge_sim *s, const StepLaunch &L, int project
     }
     launch_particle_pass(L, s->lf, 1, project_in, 0, 1);
     launch_nbody_build(s->nb, L.P, L.n, s->sort, det_pipeline(s), L.stream);
+    launch_nbody_walk(s->nb, L.cfg, L.P, L.n, false, L.stream);
     launch_particle_pass(L, s->lf, 0, 0, emit_p2g, 2);
 }
 
 // The tree's arrays for the current capacity and depth (allocated before a step).
 emerge_status nbody_prepare(emerge_sim *s) {
     if (s->nb.depth < 0) return EMERGE_OK;
-    if (s->nbbuf.ptr && s->nb_cap >= s->cap && s->nb_alloc_depth == s->nb.depth) return EMERGE_OK;
+    if (s->nbbuf.ptr && s->nb_cap >= s->cap && s->nb_alloc_depth == s->nb.depth &&
+        s->nb_alloc_fields == s->nb.n_fields)
+        return EMERGE_OK;
     CK(cudaStreamSynchronize(s->stream));  // queued kernels may still read the old arrays
     s->nbbuf.reset();
     const size_t cap = std::max<size_t>(s->cap, 1);
@@ -536,7 +542,8 @@ emerge_status nbody_prepare(emerge_sim *s) {
     const size_t b_bdata = align_up(cap * sizeof(float4), 256), b_path = align_up(cap * sizeof(uint2), 256);
     const size_t b_order = static_cast<size_t>(s->nb.depth + 1) * stride * sizeof(uint32_t);
     const size_t b_range = align_up(slots * sizeof(uint2), 256), b_com = align_up(slots * sizeof(float4), 256);
-    const size_t bytes = b_bounds + b_root + b_bdata + b_path + b_order + b_range + b_com;
+    const size_t b_accel = static_cast<size_t>(std::max(s->nb.n_fields, 1)) * stride * sizeof(float2);
+    const size_t bytes = b_bounds + b_root + b_bdata + b_path + b_order + b_range + b_com + b_accel;
     CK(cudaMalloc(&s->nbbuf.ptr, bytes));
     s->nbbuf.bytes = bytes;
     char *p = static_cast<char *>(s->nbbuf.ptr);
@@ -554,8 +561,12 @@ emerge_status nbody_prepare(emerge_sim *s) {
     s->nb.range = reinterpret_cast<uint2 *>(p);
     p += b_range;
     s->nb.com = reinterpret_cast<float4 *>(p);
+    p += b_com;
+    s->nb.accel = reinterpret_cast<float2 *>(p);
+    s->nb.walk_ctas = nbody_walk_ctas();
     s->nb_cap = cap;
     s->nb_alloc_depth = s->nb.depth;
+    s->nb_alloc_fields = s->nb.n_fields;
     refresh_dev_config(s);
     s->graph_dirty = true;
     return EMERGE_OK;
@@ -1507,6 +1518,7 @@ emerge_status emerge_cuda_set_force_fields(emerge_sim *s, const emerge_force_fie
         tree.depth = depth;
         tree.max_bodies = maxb;
         tree.theta_max = std::max(tree.theta_max, f.params[2]);
+        ++tree.n_fields;
     }
     if (s->stream) CK(cudaStreamSynchronize(s->stream));  // kernels in flight may read the old table
     if (tree.depth < 0) {
@@ -1518,7 +1530,9 @@ emerge_status emerge_cuda_set_force_fields(emerge_sim *s, const emerge_force_fie
         s->nb.depth = tree.depth;
         s->nb.max_bodies = tree.max_bodies;
         s->nb.theta_max = tree.theta_max;
-        if (s->nb_alloc_depth != tree.depth) s->nbbuf.reset();  // reallocated for the new depth
+        s->nb.n_fields = tree.n_fields;
+        if (s->nb_alloc_depth != tree.depth || s->nb_alloc_fields != tree.n_fields)
+            s->nbbuf.reset();  // reallocated for the new depth or field count
         s->nb_alloc_depth = s->nbbuf.ptr ? tree.depth : -1;
     }
     s->fbuf.reset();
@@ -1549,7 +1563,10 @@ emerge_status emerge_cuda_field_accelerations(emerge_sim *s, float *out, uint64_
     emerge_status st = nbody_prepare(s);
     if (st != EMERGE_OK) return st;
     StepLaunch L = make_launch(s);
-    if (nbody_live(s)) launch_nbody_build(s->nb, L.P, L.n, s->sort, det_pipeline(s), s->stream);
+    if (nbody_live(s)) {
+        launch_nbody_build(s->nb, L.P, L.n, s->sort, det_pipeline(s), s->stream);
+        launch_nbody_walk(s->nb, L.cfg, L.P, L.n, true, s->stream);
+    }
     float2 *d_out = nullptr;
     CK(cudaMalloc(&d_out, n * sizeof(float2)));
     launch_field_accelerations(L, s->lf, d_out);

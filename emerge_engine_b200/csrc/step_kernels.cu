@@ -558,7 +558,7 @@ __global__ void k_field_accelerations(DevParticles P, int n, LoadFlags lf, DevCo
     if (i >= n) return;
     const PState p = load_state(P, i, lf);
     const uint32_t ref = P.slot_to_index[i];
-    if (ref < static_cast<uint32_t>(n)) out[ref] = force_field_sum(cfg, p, ref);
+    if (ref < static_cast<uint32_t>(n)) out[ref] = force_field_sum(cfg, p, i);
 }
 
 // ---------------------------------------------------------------- launchers
