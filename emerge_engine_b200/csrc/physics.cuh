@@ -1194,7 +1194,8 @@ __device__ __forceinline__ bool nbody_far(float2 dv, float half, float soft, flo
 // accumulator at once -- where its own recursion would -- and sits out the node's subtree
 // (`skip`); a lane that opens a node accumulates its children into the node's own level and
 // adds the total when the walk leaves the node.  So every lane makes the additions of its
-// own recursion, in the same order, whatever its neighbours need.
+// own recursion, in the same order, whatever its neighbours need.  The fast pipeline adds
+// every value into one running sum instead (the same terms, another order).
 __device__ __forceinline__ float2 nbody_acceleration(const NBodyView &nb, const emerge_force_field &f, float2 pos,
                                                      uint32_t self) {
     const float g = f.params[0], soft = f.params[1], theta = f.params[2];
@@ -1215,6 +1216,9 @@ __device__ __forceinline__ float2 nbody_acceleration(const NBodyView &nb, const 
         // first visit of node (d, pre): box center c, half size `half`
         const int slot = nbody_level_offset(d) + static_cast<int>(pre);
         const uint2 rg = nb.range[slot];
+        // the center of mass is loaded with the range (one wait instead of two in a row),
+        // whether or not the node turns out far
+        const float4 cm = nb.com[slot];
         const bool leaf = d >= nb.depth || rg.y - rg.x <= static_cast<uint32_t>(nb.max_bodies);
         const bool part = skip < 0;
         bool need_open = false;
@@ -1222,7 +1226,6 @@ __device__ __forceinline__ float2 nbody_acceleration(const NBodyView &nb, const 
             const bool far = rg.y > rg.x && nbody_far(vsub(pos, c), half, soft, theta);
             float2 r = v2(0.0f, 0.0f);
             if (far) {
-                const float4 cm = nb.com[slot];
                 if (cm.w == 0.0f) atomicOr(nb.error, 4u);  // ERR_NBODY_SKIPPED (device_state.cuh)
                 const float2 rv = vsub(v2(cm.x, cm.y), pos);
                 r = nb.fast ? nbody_pull_fast(rv, cm.z, g, eps2) : nbody_pull(rv, cm.z, g, eps2);
@@ -1239,13 +1242,14 @@ __device__ __forceinline__ float2 nbody_acceleration(const NBodyView &nb, const 
                 need_open = true;
             }
             if (!need_open) {  // this lane's value of the node: to its parent now
-                if (d == 0) result = r;
+                if (nb.fast) result = vadd(result, r);  // fast pipeline: one running sum
+                else if (d == 0) result = r;
                 else acc[d - 1] = vadd(acc[d - 1], r);
             }
         }
         if (__any_sync(mask, need_open)) {  // the walk descends into quadrant 0 (left, top)
             if (part && !need_open) skip = d;
-            if (need_open) {
+            if (need_open && !nb.fast) {
                 acc[d] = v2(0.0f, 0.0f);
                 opened |= 1u << d;
             }
