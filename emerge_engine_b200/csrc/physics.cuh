@@ -1202,6 +1202,8 @@ __device__ __forceinline__ float2 nbody_acceleration(const NBodyView &nb, const 
     const float eps2 = soft * soft;
     if (!nb.bdata) return v2(0.0f, 0.0f);
     const unsigned mask = __activemask();
+    const bool full = mask == 0xffffffffu;
+    const uint32_t lane = threadIdx.x & 31u;
     const float4 rt = nb.root[0];
     float2 ctr[NBODY_MAX_DEPTH + 1];
     float2 acc[NBODY_MAX_DEPTH + 1];
@@ -1221,16 +1223,45 @@ __device__ __forceinline__ float2 nbody_acceleration(const NBodyView &nb, const 
         const float4 cm = nb.com[slot];
         const bool leaf = d >= nb.depth || rg.y - rg.x <= static_cast<uint32_t>(nb.max_bodies);
         const bool part = skip < 0;
-        bool need_open = false;
+        bool need_open = false, need_leaf = false;
+        float2 r = v2(0.0f, 0.0f);
         if (part) {
             const bool far = rg.y > rg.x && nbody_far(vsub(pos, c), half, soft, theta);
-            float2 r = v2(0.0f, 0.0f);
             if (far) {
                 if (cm.w == 0.0f) atomicOr(nb.error, 4u);  // ERR_NBODY_SKIPPED (device_state.cuh)
                 const float2 rv = vsub(v2(cm.x, cm.y), pos);
                 r = nb.fast ? nbody_pull_fast(rv, cm.z, g, eps2) : nbody_pull(rv, cm.z, g, eps2);
             } else if (leaf) {
-                const uint32_t *ord = nb.order + static_cast<size_t>(d) * nb.stride;
+                need_leaf = true;
+            } else {
+                need_open = true;
+            }
+        }
+        if (leaf) {
+            // the leaf's bodies in order, summed by the lanes that stop here: for a large leaf
+            // (only the deepest level holds more than max_bodies_per_node) a full warp loads
+            // the next 32 (one per lane) and passes each to every lane; otherwise the lanes
+            // load them one by one
+            const uint32_t *ord = nb.order + static_cast<size_t>(d) * nb.stride;
+            if (full && rg.y - rg.x > 8u) {
+                if (__any_sync(0xffffffffu, need_leaf)) {
+                    for (uint32_t j0 = rg.x; j0 < rg.y; j0 += 32u) {
+                        float4 q = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+                        if (j0 + lane < rg.y) q = nb.bdata[ord[j0 + lane]];
+                        const int cnt = static_cast<int>(min(32u, rg.y - j0));
+                        for (int k = 0; k < cnt; ++k) {
+                            const float bx = __shfl_sync(0xffffffffu, q.x, k);
+                            const float by = __shfl_sync(0xffffffffu, q.y, k);
+                            const float bm = __shfl_sync(0xffffffffu, q.z, k);
+                            const float bw = __shfl_sync(0xffffffffu, q.w, k);
+                            if (!need_leaf || __float_as_uint(bw) == self) continue;
+                            const float2 rv = vsub(v2(bx, by), pos);
+                            if (vdot(rv, rv) < eps2) continue;
+                            r = vadd(r, nb.fast ? nbody_pull_fast(rv, bm, g, eps2) : nbody_pull(rv, bm, g, eps2));
+                        }
+                    }
+                }
+            } else if (need_leaf) {
                 for (uint32_t j = rg.x; j < rg.y; ++j) {
                     const float4 bd = nb.bdata[ord[j]];
                     if (__float_as_uint(bd.w) == self) continue;
@@ -1238,14 +1269,12 @@ __device__ __forceinline__ float2 nbody_acceleration(const NBodyView &nb, const 
                     if (vdot(rv, rv) < eps2) continue;
                     r = vadd(r, nb.fast ? nbody_pull_fast(rv, bd.z, g, eps2) : nbody_pull(rv, bd.z, g, eps2));
                 }
-            } else {
-                need_open = true;
             }
-            if (!need_open) {  // this lane's value of the node: to its parent now
-                if (nb.fast) result = vadd(result, r);  // fast pipeline: one running sum
-                else if (d == 0) result = r;
-                else acc[d - 1] = vadd(acc[d - 1], r);
-            }
+        }
+        if (part && !need_open) {  // this lane's value of the node: to its parent now
+            if (nb.fast) result = vadd(result, r);  // fast pipeline: one running sum
+            else if (d == 0) result = r;
+            else acc[d - 1] = vadd(acc[d - 1], r);
         }
         if (__any_sync(mask, need_open)) {  // the walk descends into quadrant 0 (left, top)
             if (part && !need_open) skip = d;
