@@ -697,9 +697,9 @@ def main():
         if "nbody" in spec["material"]:
             extras["roofline"]["note"] = (
                 "with NBodyGravityField the pass runs as two halves around the Barnes-Hut tree "
-                "build, and the timed g2p phase holds both halves, the build and each particle's "
-                "tree walk (latency-bound pointer chasing, not streaming): the fraction is of "
-                "k_particle's streaming bytes only")
+                "build and walk (k_nb_walk), and the timed g2p phase holds all of them; the walk "
+                "(three quarters of a substep) is bound by instruction issue on an L1/L2-resident "
+                "tree, not by HBM: the fraction is of k_particle's streaming bytes only")
         # where a substep's time goes (host-driven loop, CUDA events between the phases)
         extras["phases_us_per_substep"] = {k[:-3]: v / max(subs_i, 1) for k, v in phases.items()}
         extras["phases_note"] = ("p2g and project read 0: the fused particle pass (k_particle) does "
