@@ -94,18 +94,47 @@ __global__ void k_nb_bounds(const float2 *x, const float *mass, int n, NBodyBoun
     const uint32_t alo_x = warp_min_u(fx ? ox : 0xffffffffu), ahi_x = warp_max_u(fx ? ox : 0u);
     const uint32_t alo_y = warp_min_u(fy ? oy : 0xffffffffu), ahi_y = warp_max_u(fy ? oy : 0u);
     const uint32_t nb = __popc(__ballot_sync(0xffffffffu, body));
+    // the CTA's warps combine in shared memory and one thread per CTA issues the atomics
+    // (every warp issuing them made the 9 words a point of contention)
+    constexpr int W = NB_THREADS / 32;
+    __shared__ uint32_t sv[9][W];
+    const int w = static_cast<int>(threadIdx.x >> 5);
     if ((threadIdx.x & 31) == 0) {
-        if (nb) {
-            atomicMin(&b->lo[0], lo_x);
-            atomicMax(&b->hi[0], hi_x);
-            atomicMin(&b->lo[1], lo_y);
-            atomicMax(&b->hi[1], hi_y);
-            atomicAdd(&b->n_bodies, nb);
+        sv[0][w] = lo_x;
+        sv[1][w] = hi_x;
+        sv[2][w] = lo_y;
+        sv[3][w] = hi_y;
+        sv[4][w] = nb;
+        sv[5][w] = alo_x;
+        sv[6][w] = ahi_x;
+        sv[7][w] = alo_y;
+        sv[8][w] = ahi_y;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        uint32_t v[9] = {sv[0][0], sv[1][0], sv[2][0], sv[3][0], sv[4][0], sv[5][0], sv[6][0], sv[7][0], sv[8][0]};
+        for (int k = 1; k < W; ++k) {
+            v[0] = min(v[0], sv[0][k]);
+            v[1] = max(v[1], sv[1][k]);
+            v[2] = min(v[2], sv[2][k]);
+            v[3] = max(v[3], sv[3][k]);
+            v[4] += sv[4][k];
+            v[5] = min(v[5], sv[5][k]);
+            v[6] = max(v[6], sv[6][k]);
+            v[7] = min(v[7], sv[7][k]);
+            v[8] = max(v[8], sv[8][k]);
         }
-        atomicMin(&b->all_lo[0], alo_x);
-        atomicMax(&b->all_hi[0], ahi_x);
-        atomicMin(&b->all_lo[1], alo_y);
-        atomicMax(&b->all_hi[1], ahi_y);
+        if (v[4]) {
+            atomicMin(&b->lo[0], v[0]);
+            atomicMax(&b->hi[0], v[1]);
+            atomicMin(&b->lo[1], v[2]);
+            atomicMax(&b->hi[1], v[3]);
+            atomicAdd(&b->n_bodies, v[4]);
+        }
+        atomicMin(&b->all_lo[0], v[5]);
+        atomicMax(&b->all_hi[0], v[6]);
+        atomicMin(&b->all_lo[1], v[7]);
+        atomicMax(&b->all_hi[1], v[8]);
     }
 }
 
