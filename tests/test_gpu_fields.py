@@ -152,6 +152,23 @@ def test_nbody_with_other_fields_in_order(cuda_lib):
     assert_fast_nbody_close(out[1], out[2])
 
 
+def test_two_nbody_fields_share_one_tree(cuda_lib):
+    """Two NBody fields of one tree shape with their own G, softening and theta, a drag field
+    between them: each field's walk has its own result block and the sum keeps the
+    application order -- identical bits in the reference-order mode, the fast bar otherwise."""
+    from emerge_engine_b200 import LinearDragField
+    p = scenes.nbody_points(20_000, seed=9, layout="blobs")
+    p["v"] = np.float32(0.25)
+    out = []
+    for cls in (DeterministicSimulation, Simulation, OracleSimulation):
+        sim = _with_points(cls, p, scenes.nbody_field(G=6.0, softening=0.8, theta=0.4, max_depth=7, max_bodies=3))
+        sim.add_force_field(LinearDragField.new((0.5, 0.0), 0.3, LinearDragField.ALL_MATERIALS))
+        sim.add_force_field(scenes.nbody_field(G=2.0, softening=1.5, theta=0.9, max_depth=7, max_bodies=3))
+        out.append(sim.field_accelerations())
+    np.testing.assert_array_equal(out[0].view(np.uint32), out[2].view(np.uint32))
+    assert_fast_nbody_close(out[1], out[2])
+
+
 def test_nbody_parameters_are_checked(cuda_lib):
     from emerge_engine_b200.abi import EmergeError
     sim = scenes.nbody_scene(Simulation)
