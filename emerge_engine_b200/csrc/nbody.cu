@@ -388,10 +388,16 @@ __global__ void __launch_bounds__(NB_THREADS) k_nb_walk(NBodyView nb, const emer
 
 }  // namespace
 
+// Resident walk CTAs per SM the grid is sized for (0: as many as fit).
+#ifndef EMERGE_NB_WALK_CTAS_PER_SM
+#define EMERGE_NB_WALK_CTAS_PER_SM 0
+#endif
+
 int nbody_walk_ctas() {
     int sms = 148, per_sm = 1, dev = 0;
     if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_nb_walk, NB_THREADS, 0) != cudaSuccess) per_sm = 1;
+    if (EMERGE_NB_WALK_CTAS_PER_SM > 0) per_sm = std::min(per_sm, EMERGE_NB_WALK_CTAS_PER_SM);
     return sms * std::max(per_sm, 1);
 }
 
