@@ -1212,11 +1212,12 @@ __device__ __forceinline__ float2 nbody_acceleration(const NBodyView &nb, const 
     int skip = -1;         // depth of the node whose subtree this lane sits out (-1: none)
     int d = 0;             // the walk's position (the same in every lane)
     uint32_t pre = 0u;
+    int base = 0;          // nbody_level_offset(d), kept as the walk moves
     float2 c = v2(rt.x, rt.y);
     float half = rt.z;
     for (;;) {
         // first visit of node (d, pre): box center c, half size `half`
-        const int slot = nbody_level_offset(d) + static_cast<int>(pre);
+        const int slot = base + static_cast<int>(pre);
         const uint2 rg = nb.range[slot];
         // the center of mass is loaded with the range (one wait instead of two in a row),
         // whether or not the node turns out far
@@ -1286,6 +1287,7 @@ __device__ __forceinline__ float2 nbody_acceleration(const NBodyView &nb, const 
             half *= 0.5f;
             c = v2(c.x - half, c.y + half);
             ++d;
+            base = 4 * base + 1;
             pre <<= 2;
             continue;
         }
@@ -1310,6 +1312,7 @@ __device__ __forceinline__ float2 nbody_acceleration(const NBodyView &nb, const 
                 pre = (pre << 2) | nq;
                 break;
             }
+            base = (base - 1) >> 2;
             half *= 2.0f;
         }
     }
